@@ -1,0 +1,126 @@
+/*
+ * semtex_b200 -- C ABI of the B200 spectral-element--Fourier hot path.
+ *
+ * The reference (Semtex) has no FFI; its boundary for this path is the C++
+ * class API of Domain / Field / ModalMatrixSys / AuxField and integrate().
+ * Each entry point below replaces one of those calls (file:line given in the
+ * reference tree) with plain pointers and sizes.
+ *
+ * Conventions
+ *  - Every call returns 0 on success or a STX_E* code; stx_last_error()
+ *    gives the message of the last failure on the calling thread.  (The
+ *    reference prints and exits instead: veclib/util.c:24-46.)
+ *  - Field data use the reference plane layout:
+ *      data[k*plane_size + e*np*np + i*np + j]
+ *    (src/auxfield.cpp:45-68); in Fourier space plane 0 = Re mode 0,
+ *    plane 1 = Nyquist, planes 2m, 2m+1 = Re, Im of mode m.
+ *  - Pointers named d_* are device pointers on the context's device; h_*
+ *    are host pointers.  Device work runs asynchronously on the context's
+ *    stream unless the call says it synchronises.
+ *  - One host thread per context at a time.
+ */
+#ifndef SEMTEX_B200_H
+#define SEMTEX_B200_H
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+#define STX_OK 0
+#define STX_EINVAL 1       /* bad argument or shape                         */
+#define STX_ESESSION 2     /* session file / token / mesh error             */
+#define STX_ENUMERIC 3     /* matrix not positive definite, singular hii    */
+#define STX_ECUDA 4        /* CUDA runtime error                            */
+#define STX_ENOCONV 5      /* PCG reached STEP_MAX (solution still written) */
+#define STX_EUNSUPPORTED 6 /* feature outside this library's scope          */
+
+#define STX_DIRECT 0 /* SolverKind DIRECT  (src/matrix.h:6-9) */
+#define STX_JACPCG 1 /* SolverKind JACPCG                     */
+
+#define STX_FORWARD 1  /* femlib/cfemdef.h FORWARD */
+#define STX_INVERSE -1 /* femlib/cfemdef.h INVERSE */
+
+typedef struct stx_context stx_context;
+typedef struct stx_modal stx_modal;
+typedef struct stx_dns stx_dns;
+
+/* Message of the last failed call on this thread ("" if none). */
+const char* stx_last_error(void);
+
+/* Read a FEML session, build mesh, geometry and numbering for every field,
+ * upload them to `device`, work on `stream` (a cudaStream_t, or NULL for a
+ * stream the context creates).  `overrides` holds "NAME=expr" token
+ * assignments separated by ';' (or NULL).
+ * Replaces the construction sequence FEML -> Mesh -> Geometry::set ->
+ * Element -> BCmgr -> Domain (elliptic/drive.cpp:145-216,
+ * dns/drive.cpp:157-248). */
+int stx_context_create(const char* session_path, const char* overrides, int device,
+                       void* stream, stx_context** out);
+int stx_context_destroy(stx_context* ctx);
+
+/* Geometry::nP/nZ/nElmt/planeSize (src/geometry.h:29-44). */
+int stx_context_geometry(const stx_context* ctx, int* np, int* nz, int* nel, int* plane_size);
+/* Field names as in <FIELDS>, NUL terminated, e.g. "uvwp" (Domain::field). */
+int stx_context_fields(const stx_context* ctx, char* buf, int len);
+/* Femlib::value (femlib/femlib.h:191-210) for a token or expression. */
+int stx_token(const stx_context* ctx, const char* expr, double* value);
+/* NumberSys sizes for a field (src/numbersys.h:44-46). */
+int stx_numbering(const stx_context* ctx, char field, int* nglobal, int* nsolve, int* nband);
+/* Element node locations, host buffers of nel*np*np (Element::_xmesh). */
+int stx_mesh_coords(const stx_context* ctx, double* h_x, double* h_y);
+/* Number of geometry families (elements sharing condensed matrices). */
+int stx_mesh_families(const stx_context* ctx, int* nfamily);
+
+/* AuxField = "function" (src/auxfield.cpp:198-220): evaluate an expression of
+ * x, y, z, t and tokens at every node of every plane into host memory
+ * h_out[nz*nel*np*np] (physical space, unpadded planes). */
+int stx_field_evaluate(const stx_context* ctx, const char* expr, double t, double* h_out);
+
+/* Evaluate a field's boundary values at time t in physical space on every
+ * plane and Fourier-transform them (Field::evaluateBoundaries +
+ * Field::bTransform, src/field.cpp:160-243).  Synchronises. */
+int stx_field_bc_evaluate(stx_context* ctx, char field, double t);
+
+/* ModalMatrixSys(lambda2, beta, base, nmodes, elmt, bsys, method)
+ * (src/matrix.cpp:33-105): one condensed, Cholesky-factored (DIRECT) or
+ * diagonally preconditioned (JACPCG) system per Fourier mode, with mode
+ * constant (beta*k)^2.  Setup runs on the host cores in FP64 and uploads;
+ * systems with equal constants and numbering are shared, as the reference's
+ * MatrixSys cache shares them (src/matrix.cpp:85-97). */
+int stx_modal_create(stx_context* ctx, char field, double lambda2, double beta, int base_mode,
+                     int num_modes, int method, stx_modal** out);
+int stx_modal_destroy(stx_modal* sys);
+/* Band width and solve size of one mode (MatrixSys::_nband/_nsolve). */
+int stx_modal_info(const stx_modal* sys, int mode, int* nsolve, int* nband);
+
+/* Field::solve(f, MMS) (src/field.cpp:598-809) on device data: d_forcing is
+ * the Fourier-space forcing (not modified), d_unknown receives the solution
+ * (and holds the PCG initial guess on entry).  Uses the field's BC values
+ * from the last stx_field_bc_evaluate.  For JACPCG, `tol_rel` and
+ * `step_max` are TOL_REL / STEP_MAX; `iterations` (nz ints, may be NULL)
+ * receives the per-plane iteration counts and the call synchronises. */
+int stx_field_solve(stx_modal* sys, const double* d_forcing, double* d_unknown, double tol_rel,
+                    int step_max, int* iterations);
+
+/* AuxField::transform(sign) (src/auxfield.cpp:1157-1194) in place on nz
+ * device planes of plane_size doubles. */
+int stx_transform(stx_context* ctx, double* d_data, int sign);
+
+/* Whole elliptic solve from host memory (elliptic/drive.cpp:61-96 with
+ * elliptic/helmholtz.cpp:29-52): copy the physical-space forcing in, forward
+ * transform, zero Nyquist, solve every mode, inverse transform, copy the
+ * physical-space solution out.  Synchronises. */
+int stx_elliptic_solve_host(stx_modal* sys, const double* h_forcing, double* h_solution);
+
+/* Synchronise the context's stream. */
+int stx_sync(stx_context* ctx);
+
+/* Device scratch the context owns: returns a device pointer to at least
+ * `bytes` bytes (grown on demand; freed with the context). */
+int stx_context_scratch(stx_context* ctx, unsigned long long bytes, void** d_ptr);
+
+#ifdef __cplusplus
+}
+#endif
+
+#endif /* SEMTEX_B200_H */

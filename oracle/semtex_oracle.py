@@ -1,0 +1,1114 @@
+"""CPU oracle for the Semtex spectral-element--Fourier hot path (TEST INFRASTRUCTURE).
+
+This module is the checker, not the product.  Only ``tests/``,
+``__graft_entry__.smoke()`` and ``bench.py``'s CPU-baseline leg import it.
+It restates, in numpy/scipy, the reference algorithm of the path that the
+CUDA library accelerates:
+
+* FEML session reading and token evaluation  (src/feml.cpp:64-330,
+  femlib/initial.y:138-249, femlib/defaults.h:10-96)
+* straight-sided quad meshing with a Coons patch (src/mesh.cpp:723-882)
+* GLL quadrature and derivative operators     (femlib/polylib.c:312-575)
+* element geometric factors                    (src/element.cpp:1253-1408)
+* elemental Helmholtz matrix / operator        (src/element.cpp:1411-1622)
+* static condensation                          (src/element.cpp:131-214)
+* banded Cholesky boundary system              (src/matrix.cpp:132-267)
+* Field::solve DIRECT / JACPCG                 (src/field.cpp:598-809)
+* z-direction real DFT, packed Re0,Nyq,Re1,Im1 (femlib/fourier.c:40-165)
+* the DNS velocity-correction step             (dns/integrate.cpp:66-289,
+  dns/nonlinear.cpp:198-381)
+
+The banded factorisation and solve call LAPACK dpbtrf/dpbtrs through scipy,
+the same routines the reference calls (src/matrix.cpp:252, src/field.cpp:693).
+
+Node numbering is this module's own (connectivity + reverse Cuthill--McKee).
+It differs from the reference `enumerate` output, which changes nothing but
+round-off, except for the singular k=0 pressure problem, whose pinned node
+(src/matrix.cpp:160-162) is the highest-numbered solve node: the pressure is
+then determined up to a constant that depends on the numbering.
+"""
+
+from __future__ import annotations
+
+import math
+import os
+import re
+from dataclasses import dataclass, field as dfield
+
+import numpy as np
+import scipy.linalg as sla
+from scipy.sparse import csr_matrix
+from scipy.sparse.csgraph import reverse_cuthill_mckee
+
+EPSDP = 6.0e-14          # veclib/cveclib.h:58
+EPSSP = 6.0e-7
+
+# ---------------------------------------------------------------------------
+# Tokens and expressions (femlib/defaults.h, femlib/initial.y)
+# ---------------------------------------------------------------------------
+
+DEFAULT_TOKENS = {
+    "E": 2.71828182845904523536, "DEG": 57.29577951308232087721,
+    "PI": 3.14159265358979323844, "TWOPI": 6.28318530717958647688,
+    "EULER": 0.57721566490153286061, "GOLDEN": 1.61803398874989484820,
+    "t": 0.0, "D_T": 0.01, "TOL_REL": 1.0e-8, "TOL_ABS": 1.0e-8,
+    "TOL_POS": 1.0e-5, "z": 0.0, "BETA": 1.0, "LAMBDA2": 0.0,
+    "KINVIS": 1.0, "REFVIS": 1.0, "RHO": 1.0, "GRAVITY": 9.81,
+    "X_SHIFT": 0.0, "Y_SHIFT": 0.0, "X_SCALE": 1.0, "Y_SCALE": 1.0,
+    "SVV_MN": -1, "SVV_EPSN": 0.0, "SVV_MZ": -1, "SVV_EPSZ": 0.0,
+    "ITERATIVE": 0, "TBCS": 0, "CYLINDRICAL": 0, "VERBOSE": 0,
+    "CHKPOINT": 1, "IO_FLD": 500, "IO_HIS": 10, "IO_CFL": 50, "IO_MDL": 50,
+    "N_P": 5, "N_TIME": 2, "N_STEP": 1, "N_Z": 1, "I_PROC": 0, "N_PROC": 1,
+    "STEP_MAX": 500, "NR_MAX": 20, "FFX": 0.0, "FFY": 0.0, "FFZ": 0.0,
+}
+
+_FUNCS = {
+    "cos": np.cos, "sin": np.sin, "tan": np.tan, "exp": np.exp,
+    "sinh": np.sinh, "cosh": np.cosh, "tanh": np.tanh, "abs": np.abs,
+    "floor": np.floor, "ceil": np.ceil, "acos": np.arccos, "asin": np.arcsin,
+    "atan": np.arctan, "log": np.log, "log10": np.log10, "sqrt": np.sqrt,
+    "int": np.rint, "sgn": np.sign,
+    "heav": lambda x: np.where(np.asarray(x) >= 0.0, 1.0, 0.0),
+}
+
+
+class Tokens(dict):
+    """Token table with the reference defaults and its expression grammar.
+
+    Grammar of femlib/initial.y:196-249: '^' is right-associative power with
+    higher precedence than unary minus, which python's '**' shares.
+    """
+
+    def __init__(self):
+        super().__init__(DEFAULT_TOKENS)
+
+    def evaluate(self, expr: str, **variables):
+        src = expr.strip().replace("^", "**")
+        if "&" in src or "~" in src:
+            raise ValueError(f"operator not supported by the oracle: {expr}")
+        names = dict(_FUNCS)
+        names.update(self)
+        names.update(variables)
+        return eval(src, {"__builtins__": {}}, names)  # noqa: S307 (test oracle)
+
+    def assign(self, line: str):
+        name, expr = line.split("=", 1)
+        self[name.strip()] = float(self.evaluate(expr))
+
+    def ivalue(self, name):
+        return int(round(float(self[name])))
+
+
+# ---------------------------------------------------------------------------
+# FEML session (src/feml.cpp, src/mesh.cpp:129-470, src/bcmgr.cpp:100-110)
+# ---------------------------------------------------------------------------
+
+@dataclass
+class Session:
+    name: str
+    tokens: Tokens
+    fields: str
+    groups: dict                 # group char -> descriptor string
+    bcs: dict                    # group char -> {field: (kind, expr)}
+    nodes: np.ndarray            # [Nn, 3]
+    elements: np.ndarray         # [nel, 4] zero-based node ids (CCW)
+    surfaces: list               # (elmt, side, 'B', group) | (elmt, side, 'P', (me, ms))
+    user: list = dfield(default_factory=list)
+
+
+def _section(text: str, name: str):
+    m = re.search(r"<\s*" + name + r"\b([^>]*)>(.*?)</\s*" + name + r"\s*>",
+                  text, re.S | re.I)
+    if not m:
+        return None, None
+    return m.group(1), m.group(2)
+
+
+def _lines(body: str):
+    out = []
+    for ln in body.splitlines():
+        s = ln.strip()
+        if s and not s.startswith("#"):
+            out.append(s)
+    return out
+
+
+def read_session(path: str, overrides: dict | None = None) -> Session:
+    """Read a FEML session file (src/feml.cpp:64-330, src/mesh.cpp:129-470)."""
+    text = open(path).read()
+    tok = Tokens()
+    _, body = _section(text, "TOKENS")
+    if body:
+        for ln in body.splitlines():
+            if "=" in ln and not ln.strip().startswith("#"):
+                tok.assign(ln)
+    for k, v in (overrides or {}).items():
+        tok[k] = float(v)
+    if tok.ivalue("IO_FLD") > tok.ivalue("N_STEP"):
+        tok["IO_FLD"] = tok["N_STEP"]
+    if tok.ivalue("N_TIME") > 3:
+        tok["N_TIME"] = 3
+    _, body = _section(text, "FIELDS")
+    fields = "".join(body.split())
+    groups = {}
+    _, body = _section(text, "GROUPS")
+    if body:
+        for ln in _lines(body):
+            parts = ln.split()
+            groups[parts[1]] = parts[2]
+    bcs = {}
+    _, body = _section(text, "BCS")
+    if body:
+        lines = _lines(body)
+        i = 0
+        while i < len(lines):
+            parts = lines[i].split()
+            g, nf = parts[1], int(parts[2])
+            entry = {}
+            for j in range(nf):
+                m = re.match(r"<\s*([A-Z])\s*>\s*(\w)\s*=?\s*(.*?)\s*</\s*[A-Z]\s*>",
+                             lines[i + 1 + j])
+                kind, fname, expr = m.group(1), m.group(2), m.group(3)
+                entry[fname] = (kind, expr)
+            bcs[g] = entry
+            i += 1 + nf
+    _, body = _section(text, "NODES")
+    nodes = np.array([[float(v) for v in ln.split()[1:4]] for ln in _lines(body)])
+    _, body = _section(text, "ELEMENTS")
+    elems = []
+    for ln in _lines(body):
+        m = re.match(r"(\d+)\s*<\s*Q\s*>\s*(\d+)\s+(\d+)\s+(\d+)\s+(\d+)", ln)
+        elems.append([int(m.group(k)) - 1 for k in range(2, 6)])
+    surfaces = []
+    _, body = _section(text, "SURFACES")
+    if body:
+        for ln in _lines(body):
+            m = re.match(r"\d+\s+(\d+)\s+(\d+)\s*<\s*([BP])\s*>\s*(.*?)\s*</", ln)
+            e, s, kind, rest = int(m.group(1)) - 1, int(m.group(2)) - 1, m.group(3), m.group(4)
+            if kind == "B":
+                surfaces.append((e, s, "B", rest.strip()))
+            else:
+                me, ms = rest.split()
+                surfaces.append((e, s, "P", (int(me) - 1, int(ms) - 1)))
+    _, curves = _section(text, "CURVES")
+    if curves and _lines(curves):
+        raise NotImplementedError("curved sides are outside the oracle's scope")
+    _, body = _section(text, "USER")
+    user = _lines(body) if body else []
+    name = os.path.basename(path)
+    return Session(name, tok, fields, groups, bcs, nodes, np.array(elems, int),
+                   surfaces, user)
+
+
+# ---------------------------------------------------------------------------
+# GLL quadrature (femlib/polylib.c:312-575): zeros, weights, derivative matrix
+# ---------------------------------------------------------------------------
+
+def _legendre(n, x):
+    p0, p1 = np.ones_like(x), x.copy()
+    if n == 0:
+        return p0
+    for k in range(2, n + 1):
+        p0, p1 = p1, ((2 * k - 1) * x * p1 - (k - 1) * p0) / k
+    return p1
+
+
+def gll(np_: int):
+    """GLL points z, weights w, derivative D[i,j] = h_j'(z_i) (row-major)."""
+    N = np_ - 1
+    if np_ == 2:
+        z = np.array([-1.0, 1.0])
+    else:
+        # interior points: zeros of P_N'(x) via the Jacobi P^{(1,1)}_{N-1}
+        # companion (Golub--Welsch) eigenvalues, then Newton polish.
+        n = N - 1
+        k = np.arange(1, n)
+        b = np.sqrt(k * (k + 2.0) / ((2 * k + 1.0) * (2 * k + 3.0)))
+        J = np.diag(b, 1) + np.diag(b, -1)
+        zi = np.sort(np.linalg.eigvalsh(J)) if n > 1 else np.array([0.0])
+        for _ in range(6):
+            # P_N'(x) = N (x P_N - P_{N-1}) / (x^2 - 1)
+            pn, pn1 = _legendre(N, zi), _legendre(N - 1, zi)
+            d1 = N * (zi * pn - pn1) / (zi * zi - 1.0)
+            d2 = (2 * zi * d1 - N * (N + 1) * pn) / (1.0 - zi * zi)
+            zi = zi - d1 / d2
+        z = np.concatenate([[-1.0], zi, [1.0]])
+    PN = _legendre(N, z)
+    w = 2.0 / (N * (N + 1) * PN * PN)
+    D = np.zeros((np_, np_))
+    for i in range(np_):
+        for j in range(np_):
+            if i != j:
+                D[i, j] = PN[i] / (PN[j] * (z[i] - z[j]))
+    D[0, 0] = -N * (N + 1) / 4.0
+    D[N, N] = N * (N + 1) / 4.0
+    return z, w, D
+
+
+# ---------------------------------------------------------------------------
+# Mesh and element geometry
+# ---------------------------------------------------------------------------
+
+class Mesh:
+    """Element node locations and connectivity for straight-sided quads."""
+
+    def __init__(self, S: Session, np_: int):
+        self.S, self.np = S, np_
+        self.nel = len(S.elements)
+        self.z, self.w, self.D = gll(np_)
+        nel, z = self.nel, self.z
+        tok = S.tokens
+        x = np.zeros((nel, np_, np_))
+        y = np.zeros((nel, np_, np_))
+        for e in range(nel):
+            P = S.nodes[S.elements[e], :2]
+            # side k runs from vertex k to vertex k+1 (src/mesh.cpp:804-844):
+            # Coons patch of straight sides == bilinear map of the 4 vertices.
+            r = z[None, :]
+            s = z[:, None]
+            for arr, c in ((x, 0), (y, 1)):
+                arr[e] = 0.25 * ((1 - r) * (1 - s) * P[0, c] + (1 + r) * (1 - s) * P[1, c]
+                                 + (1 + r) * (1 + s) * P[2, c] + (1 - r) * (1 + s) * P[3, c])
+        if abs(tok["X_SHIFT"]) > EPSDP:
+            x += tok["X_SHIFT"]
+        if abs(tok["Y_SHIFT"]) > EPSDP:
+            y += tok["Y_SHIFT"]
+        if abs(tok["X_SCALE"] - 1.0) > EPSDP:
+            x *= tok["X_SCALE"]
+        if abs(tok["Y_SCALE"] - 1.0) > EPSDP:
+            y *= tok["Y_SCALE"]
+        self.x, self.y = x, y
+        self._factors()
+        self._connect()
+
+    # -- src/element.cpp:1253-1408 (Element::mapping)
+    def _factors(self):
+        D, w = self.D, self.w
+        x, y = self.x, self.y
+        dxdr = x @ D.T
+        dxds = D @ x
+        dydr = y @ D.T
+        dyds = D @ y
+        jac = dxdr * dyds - dxds * dydr
+        if jac.min() < 4 * EPSDP:
+            raise ValueError("Jacobian of element nonpositive")
+        WW = np.outer(w, w)[None]
+        self.Q1 = (dxds * dxds + dyds * dyds) / jac * WW
+        self.Q2 = (dxdr * dxdr + dydr * dydr) / jac * WW
+        self.Q3 = (-dydr * dyds - dxdr * dxds) / jac * WW
+        self.Q4 = jac * WW
+        self.drdx = dyds / jac
+        self.drdy = -dxds / jac
+        self.dsdx = -dydr / jac
+        self.dsdy = dxdr / jac
+        eps = 4 * EPSDP
+        for nm in ("drdx", "drdy", "dsdx", "dsdy", "Q3"):
+            a = getattr(self, nm)
+            for e in range(self.nel):
+                if np.linalg.norm(a[e]) < eps:
+                    a[e] = 0.0
+
+    # -- element-boundary node traverse (femlib/mapping.c:46-132)
+    def emap(self):
+        n = self.np
+        em = [0]
+        k = 0
+        for _ in range(1, n):
+            k += 1
+            em.append(k)
+        for _ in range(1, n):
+            k += n
+            em.append(k)
+        for _ in range(1, n):
+            k -= 1
+            em.append(k)
+        for _ in range(1, n - 1):
+            k -= n
+            em.append(k)
+        for i in range(1, n - 1):
+            for j in range(1, n - 1):
+                em.append(i * n + j)
+        return np.array(em, int)
+
+    def _connect(self):
+        """Side mates: shared vertex pairs (internal) or <P> surfaces."""
+        S = self.S
+        nel = self.nel
+        self.mate = {}
+        key = {}
+        for e in range(nel):
+            for s in range(4):
+                a, b = S.elements[e][s], S.elements[e][(s + 1) % 4]
+                key.setdefault((a, b), []).append((e, s))
+        for e in range(nel):
+            for s in range(4):
+                a, b = S.elements[e][s], S.elements[e][(s + 1) % 4]
+                for (me, ms) in key.get((b, a), []):
+                    self.mate[(e, s)] = (me, ms)
+        self.group = {}
+        for (e, s, kind, val) in S.surfaces:
+            if kind == "B":
+                self.group[(e, s)] = val
+            else:
+                self.mate[(e, s)] = val
+                self.mate[val] = (e, s)
+
+    def side_nodes(self, s):
+        """Row-major indices of the np nodes of side s, CCW (src/element.h:162)."""
+        n = self.np
+        if s == 0:
+            return [j for j in range(n)]
+        if s == 1:
+            return [i * n + n - 1 for i in range(n)]
+        if s == 2:
+            return [(n - 1) * n + (n - 1 - j) for j in range(n)]
+        return [(n - 1 - i) * n for i in range(n)]
+
+
+class Numbering:
+    """Global numbering of element-boundary nodes for one field.
+
+    Role of the `.num` NumberSys (src/numbersys.h, src/bcmgr.cpp:586-826):
+    btog[e, i] for the 4(np-1) boundary nodes of element e in emap order,
+    bmask (1 = essential), solve nodes numbered first, RCM-ordered.
+    """
+
+    def __init__(self, M: Mesh, fld: str, rcm: bool = True):
+        S, n, nel = M.S, M.np, M.nel
+        nm = n - 1
+        next_ = 4 * nm
+        parent = list(range(len(S.nodes)))
+
+        def find(a):
+            while parent[a] != a:
+                parent[a] = parent[parent[a]]
+                a = parent[a]
+            return a
+
+        for (e, s), (me, ms) in M.mate.items():
+            a, b = S.elements[e][s], S.elements[e][(s + 1) % 4]
+            c, d = S.elements[me][ms], S.elements[me][(ms + 1) % 4]
+            for u, v in ((a, d), (b, c)):
+                ru, rv = find(u), find(v)
+                if ru != rv:
+                    parent[max(ru, rv)] = min(ru, rv)
+        gid = -np.ones((nel, next_), int)
+        vid = {}
+        nxt = 0
+        for e in range(nel):
+            for s in range(4):
+                r = find(S.elements[e][s])
+                if r not in vid:
+                    vid[r] = nxt
+                    nxt += 1
+                gid[e, s * nm] = vid[r]
+        done = {}
+        for e in range(nel):
+            for s in range(4):
+                if (e, s) in done:
+                    ids = done[(e, s)]
+                else:
+                    ids = list(range(nxt, nxt + nm - 1))
+                    nxt += nm - 1
+                    if (e, s) in M.mate:
+                        done[M.mate[(e, s)]] = ids[::-1]
+                gid[e, s * nm + 1: s * nm + nm] = ids
+        nglobal = nxt
+        ess = np.zeros(nglobal, bool)
+        for (e, s), g in M.group.items():
+            if (e, s) in M.mate:
+                continue
+            bc = S.bcs.get(g, {}).get(fld)
+            if bc and bc[0] == "D":
+                for t in range(n):
+                    ess[gid[e, (s * nm + t) % next_]] = True
+        solve_nodes = np.where(~ess)[0]
+        ess_nodes = np.where(ess)[0]
+        nsolve = len(solve_nodes)
+        order = solve_nodes
+        if rcm and nsolve > 1:
+            loc = -np.ones(nglobal, int)
+            loc[solve_nodes] = np.arange(nsolve)
+            rows, cols = [], []
+            for e in range(nel):
+                g = loc[gid[e]]
+                g = np.unique(g[g >= 0])
+                rr, cc = np.meshgrid(g, g)
+                rows.append(rr.ravel())
+                cols.append(cc.ravel())
+            A = csr_matrix((np.ones(sum(len(r) for r in rows)),
+                            (np.concatenate(rows), np.concatenate(cols))),
+                           shape=(nsolve, nsolve))
+            perm = reverse_cuthill_mckee(A, symmetric_mode=True)
+            order = solve_nodes[perm]
+        newid = np.empty(nglobal, int)
+        newid[order] = np.arange(nsolve)
+        newid[ess_nodes] = nsolve + np.arange(len(ess_nodes))
+        self.btog = newid[gid]
+        self.bmask = ess[gid].astype(int)
+        self.emask = self.bmask.any(axis=1).astype(int)
+        self.nglobal, self.nsolve = nglobal, nsolve
+        bw = 0
+        for e in range(nel):
+            g = self.btog[e][self.btog[e] < nsolve]
+            if len(g):
+                bw = max(bw, g.max() - g.min())
+        self.nband = bw + 1
+        em = M.emap()
+        mass = np.zeros(nglobal)
+        for e in range(nel):
+            np.add.at(mass, self.btog[e], M.Q4[e].ravel()[em[:next_]])
+        self.imass = 1.0 / mass
+
+
+# ---------------------------------------------------------------------------
+# Elemental operators (src/element.cpp:521-565, 1411-1622)
+# ---------------------------------------------------------------------------
+
+def helmholtz_matrix(M: Mesh, e: int, lambda2: float, betak2: float):
+    """Full np^2 x np^2 elemental Helmholtz matrix, HelmholtzRow semantics.
+
+    H[(i,j),(m,n)] = d_im sum_q Q1[i,q] D[q,j] D[q,n]
+                   + d_jn sum_p Q2[p,j] D[p,i] D[p,m]
+                   + Q3[i,n] D[n,j] D[i,m] + Q3[m,j] D[j,n] D[m,i]
+                   + d_im d_jn Q4[i,j] (lambda2 + betak2)
+    """
+    n, D = M.np, M.D
+    Q1, Q2, Q3, Q4 = M.Q1[e], M.Q2[e], M.Q3[e], M.Q4[e]
+    I = np.eye(n)
+    T1 = np.einsum("im,iq,qj,qn->ijmn", I, Q1, D, D)
+    T2 = np.einsum("jn,pj,pi,pm->ijmn", I, Q2, D, D)
+    T3 = np.einsum("in,nj,im->ijmn", Q3, D, D) + np.einsum("mj,jn,mi->ijmn", Q3, D, D)
+    T4 = np.einsum("im,jn,ij->ijmn", I, I, Q4) * (lambda2 + betak2)
+    return (T1 + T2 + T3 + T4).reshape(n * n, n * n)
+
+
+def helmholtz_op(M: Mesh, u, lambda2, betak2):
+    """Batched Element::HelmholtzOp over all elements; u: [nel, np, np]."""
+    D = M.D
+    R = u @ D.T
+    S = D @ u
+    R2 = M.Q1 * R + M.Q3 * S
+    S2 = M.Q2 * S + M.Q3 * R
+    return M.Q4 * u * (lambda2 + betak2) + D.T @ S2 + R2 @ D
+
+
+def grad(M: Mesh, u, direction):
+    """Element::grad x (0) or y (1) derivative of plane data u [nel,np,np]."""
+    ur = u @ M.D.T
+    us = M.D @ u
+    if direction == 0:
+        return ur * M.drdx + us * M.dsdx
+    return ur * M.drdy + us * M.dsdy
+
+
+# ---------------------------------------------------------------------------
+# Boundary conditions (src/condition.cpp, src/boundary.cpp, src/field.cpp)
+# ---------------------------------------------------------------------------
+
+class BoundarySystem:
+    """Boundary edges (BCtriples) of one field with their kinds."""
+
+    def __init__(self, M: Mesh, N: Numbering, fld: str):
+        self.M, self.N, self.fld = M, N, fld
+        S = M.S
+        self.edges = []      # (e, s, kind, expr)
+        for (e, s), g in sorted(M.group.items()):
+            if (e, s) in M.mate:
+                continue
+            bc = S.bcs.get(g, {}).get(fld)
+            if bc is None:
+                raise ValueError(f"no BC for field {fld} in group {g}")
+            self.edges.append((e, s, bc[0], bc[1]))
+        n = M.np
+        self.area = []
+        for (e, s, _, _) in self.edges:
+            idx = M.side_nodes(s)
+            xs, ys = M.x[e].ravel()[idx], M.y[e].ravel()[idx]
+            # straight side: |dx/dl| along the side times the GLL weight
+            L = math.hypot(xs[-1] - xs[0], ys[-1] - ys[0])
+            self.area.append(0.5 * L * M.w)
+        self.nline = len(self.edges) * n
+
+    def evaluate_physical(self, tok: Tokens, z: float, t: float):
+        """BC line (values along each edge) in physical space at plane z."""
+        out = np.zeros((len(self.edges), self.M.np))
+        for b, (e, s, kind, expr) in enumerate(self.edges):
+            if kind in ("D", "N"):
+                idx = self.M.side_nodes(s)
+                xs, ys = self.M.x[e].ravel()[idx], self.M.y[e].ravel()[idx]
+                val = tok.evaluate(expr, x=xs, y=ys, z=z, t=t)
+                out[b] = np.broadcast_to(np.asarray(val, float), (self.M.np,))
+        return out
+
+    def get_essential(self, line, tgt):
+        """Field::getEssential -> Essential::set (src/condition.cpp:80-101)."""
+        nm = self.M.np - 1
+        for b, (e, s, kind, _) in enumerate(self.edges):
+            if kind == "D":
+                g = [self.N.btog[e, (s * nm + t) % (4 * nm)] for t in range(nm + 1)]
+                tgt[g] = line[b]
+
+    def natural_sum(self, line, tgt):
+        """Natural::sum (src/condition.cpp:192-219): <h, w> into tgt."""
+        nm = self.M.np - 1
+        for b, (e, s, kind, _) in enumerate(self.edges):
+            if kind == "N":
+                g = [self.N.btog[e, (s * nm + t) % (4 * nm)] for t in range(nm + 1)]
+                np.add.at(tgt, g, line[b] * self.area[b])
+
+
+# ---------------------------------------------------------------------------
+# Modal matrix systems and Field::solve (src/matrix.cpp, src/field.cpp)
+# ---------------------------------------------------------------------------
+
+class MatrixSys:
+    """Statically condensed, banded-Cholesky Helmholtz system of one mode."""
+
+    def __init__(self, M: Mesh, N: Numbering, lambda2: float, betak2: float,
+                 method: str = "DIRECT", mixed_bc: bool = False):
+        self.M, self.N = M, N
+        self.lambda2, self.betak2, self.method = lambda2, betak2, method
+        n = M.np
+        next_ = 4 * (n - 1)
+        em = M.emap()
+        singular = (lambda2 + betak2) < EPSSP and (N.nglobal == N.nsolve) and not mixed_bc
+        self.nsolve = N.nsolve - 1 if singular else N.nsolve
+        self.nglobal = N.nglobal
+        nel = M.nel
+        if method == "DIRECT":
+            kd = N.nband - 1
+            ns = self.nsolve
+            AB = np.zeros((kd + 1, ns))         # LAPACK upper band storage
+            self.hbi = np.zeros((nel, next_, (n - 2) ** 2))
+            self.hii = np.zeros((nel, (n - 2) ** 2, (n - 2) ** 2))
+            for e in range(nel):
+                H = helmholtz_matrix(M, e, lambda2, betak2)[np.ix_(em, em)]
+                hbb = H[:next_, :next_]
+                hbi = H[:next_, next_:]
+                hii = H[next_:, next_:]
+                if hii.size:
+                    hii_inv = np.linalg.inv(hii)
+                    hbi_c = hbi @ hii_inv
+                    hbb = hbb - hbi_c @ hbi.T
+                else:
+                    hii_inv, hbi_c = hii, hbi
+                self.hbi[e], self.hii[e] = hbi_c, hii_inv
+                g = N.btog[e]
+                for i in range(next_):
+                    m = g[i]
+                    if m >= ns:
+                        continue
+                    for k in range(next_):
+                        nn = g[k]
+                        if nn < ns and nn >= m:
+                            AB[kd + m - nn, nn] += hbb[i, k]
+            self.factor = sla.cholesky_banded(AB, lower=False) if ns else AB
+        else:
+            npts = N.nglobal + nel * (n - 2) ** 2
+            pc = np.zeros(npts)
+            for e in range(nel):
+                H = helmholtz_matrix(M, e, lambda2, betak2)
+                dg = np.diag(H)[em]
+                np.add.at(pc, N.btog[e], dg[:next_])
+                pc[N.nglobal + e * (n - 2) ** 2: N.nglobal + (e + 1) * (n - 2) ** 2] = dg[next_:]
+            self.PC = 1.0 / pc
+            self.npts = npts
+
+
+def solve_plane(M: Mesh, N: Numbering, B: BoundarySystem, MS: MatrixSys,
+                forcing, unknown, bcline, tol_rel=1e-8, step_max=500):
+    """One plane of Field::solve (src/field.cpp:598-809).
+
+    forcing, unknown: [nel, np, np]; returns new unknown (forcing unchanged).
+    """
+    n, nel = M.np, M.nel
+    next_ = 4 * (n - 1)
+    em = M.emap()
+    lam, bk2 = MS.lambda2, MS.betak2
+    nsolve, nglobal = MS.nsolve, MS.nglobal
+    # -- constrain: f <- -(M f + H g)              (src/field.cpp:812-852)
+    gvec = np.zeros(nglobal)
+    B.get_essential(bcline, gvec)
+    F = M.Q4 * forcing
+    if N.emask.any():
+        u = np.zeros_like(F)
+        flat = u.reshape(nel, -1)
+        flat[:, em[:next_]] = gvec[N.btog]
+        HG = helmholtz_op(M, u, lam, bk2)
+        F = F + HG * N.emask[:, None, None]
+    F = -F
+    Fe = F.reshape(nel, -1)[:, em]                    # emap (boundary-major)
+    if MS.method == "DIRECT":
+        # -- buildRHS with static condensation     (src/field.cpp:943-1009)
+        RHS = np.zeros(nglobal)
+        Fb = Fe[:, :next_] - np.einsum("eij,ej->ei", MS.hbi, Fe[:, next_:])
+        np.add.at(RHS, N.btog, Fb)
+        B.natural_sum(bcline, RHS)
+        RHS[nsolve:] = 0.0
+        if nsolve:
+            RHS[:nsolve] = sla.cho_solve_banded((MS.factor, False), RHS[:nsolve])
+        # -- global2localSC                         (src/element.cpp:368-407)
+        ub = RHS[N.btog]
+        ui = np.einsum("eij,ej->ei", MS.hii, Fe[:, next_:]) - np.einsum("eji,ej->ei", MS.hbi, ub)
+        out = np.zeros((nel, n * n))
+        out[:, em[:next_]] = ub
+        out[:, em[next_:]] = ui
+    else:
+        out = _jacpcg(M, N, B, MS, Fe, unknown, bcline, gvec, tol_rel, step_max)
+    # -- impose essential values                    (src/field.cpp:1106-1124)
+    gvec = np.zeros(nglobal)
+    B.get_essential(bcline, gvec)
+    mask = N.bmask.astype(bool)
+    bnd = out[:, em[:next_]]
+    bnd[mask] = gvec[N.btog][mask]
+    out[:, em[:next_]] = bnd
+    return out.reshape(nel, n, n)
+
+
+def _global_op(M, N, MS, xg):
+    """Field::HelmholtzOperator (src/field.cpp:855-940) on global vector xg."""
+    n, nel = M.np, M.nel
+    next_, nint = 4 * (n - 1), (n - 2) ** 2
+    em = M.emap()
+    P = np.zeros((nel, n * n))
+    P[:, em[:next_]] = xg[N.btog]
+    P[:, em[next_:]] = xg[N.nglobal:].reshape(nel, nint)
+    HP = helmholtz_op(M, P.reshape(nel, n, n), MS.lambda2, MS.betak2).reshape(nel, -1)
+    y = np.zeros_like(xg)
+    np.add.at(y, N.btog, HP[:, em[:next_]])
+    y[N.nglobal:] = HP[:, em[next_:]].ravel()
+    return y
+
+
+def _jacpcg(M, N, B, MS, Fe, unknown, bcline, gvec, tol_rel, step_max):
+    """Jacobi-PCG branch of Field::solve (src/field.cpp:711-805)."""
+    n, nel = M.np, M.nel
+    next_, nint = 4 * (n - 1), (n - 2) ** 2
+    em = M.emap()
+    nglobal, nsolve = MS.nglobal, MS.nsolve
+    npts = MS.npts
+    r = np.zeros(npts)
+    np.add.at(r, N.btog, Fe[:, :next_])
+    r[nglobal:] = Fe[:, next_:].ravel()
+    B.natural_sum(bcline, r)
+    r[nsolve:nglobal] = 0.0
+    epsb2 = (tol_rel * math.sqrt(r @ r)) ** 2
+    x = np.zeros(npts)
+    x[:nglobal] = gvec
+    uf = unknown.reshape(nel, -1)[:, em]
+    xb = np.zeros(nglobal)
+    xb[N.btog] = uf[:, :next_]                 # local2global (last write wins)
+    x[:nglobal] = xb
+    x[nglobal:] = uf[:, next_:].ravel()
+    x[nsolve:nglobal] = 0.0
+    p = _global_op(M, N, MS, x)
+    p[nsolve:nglobal] = 0.0
+    r[nsolve:nglobal] = 0.0
+    r = r - p
+    r2 = r @ r
+    i = 0
+    rho2 = 0.0
+    while r2 > epsb2:
+        i += 1
+        if i >= step_max:
+            break
+        z = MS.PC * r
+        rho1 = r @ z
+        p = z.copy() if i == 1 else z + (rho1 / rho2) * p
+        q = _global_op(M, N, MS, p)
+        q[nsolve:nglobal] = 0.0
+        alpha = rho1 / (p @ q)
+        x = x + alpha * p
+        r = r - alpha * q
+        rho2 = rho1
+        r2 = r @ r
+    out = np.zeros((nel, n * n))
+    out[:, em[:next_]] = x[N.btog]
+    out[:, em[next_:]] = x[nglobal:].reshape(nel, nint)
+    return out
+
+
+# ---------------------------------------------------------------------------
+# z-direction real DFT (femlib/fourier.c:40-165; src/auxfield.cpp:1157-1194)
+# ---------------------------------------------------------------------------
+
+def dft_forward(phys):
+    """[nz, ...] physical planes -> packed Fourier planes, scaled by 1/nz."""
+    nz = phys.shape[0]
+    if nz == 1:
+        return phys.copy()
+    if nz == 2:
+        out = phys.copy()
+        out[1] = 0.0
+        return out
+    c = np.fft.rfft(phys, axis=0) / nz
+    out = np.empty_like(phys)
+    out[0] = c[0].real
+    out[1] = c[nz // 2].real
+    out[2::2] = c[1:nz // 2].real
+    out[3::2] = c[1:nz // 2].imag
+    return out
+
+
+def dft_inverse(four):
+    nz = four.shape[0]
+    if nz == 1:
+        return four.copy()
+    if nz == 2:
+        out = four.copy()
+        out[1] = four[0]
+        return out
+    c = np.zeros((nz // 2 + 1,) + four.shape[1:], complex)
+    c[0] = four[0]
+    c[nz // 2] = four[1]
+    c[1:nz // 2] = four[2::2] + 1j * four[3::2]
+    return np.fft.irfft(c * nz, n=nz, axis=0)
+
+
+# ---------------------------------------------------------------------------
+# Field files (src/misc.cpp:106-180, src/auxfield.cpp:1021-1113)
+# ---------------------------------------------------------------------------
+
+def write_field(path, session_name, np_, nz, nel, step, time, dt, kinvis, beta,
+                fields: dict):
+    hdr = [
+        f"{session_name:<25s} Session",
+        f"{'Thu Jan 01 00:00:00 1970':<25s} Created",
+        f"{f'{np_} {np_} {nz} {nel}':<25s} Nr, Ns, Nz, Elements",
+        f"{step:<25d} Step",
+        f"{time:<25.6g} Time",
+        f"{dt:<25.6g} Time step",
+        f"{kinvis:<25.6g} Kinvis",
+        f"{beta:<25.6g} Beta",
+        f"{''.join(fields.keys()):<25s} Fields written",
+        f"{'binary IEEE little-endian':<25s} Format",
+    ]
+    with open(path, "wb") as f:
+        f.write(("\n".join(hdr) + "\n").encode())
+        for v in fields.values():
+            f.write(np.ascontiguousarray(v, dtype="<f8").tobytes())
+
+
+def read_field(path):
+    with open(path, "rb") as f:
+        lines = [f.readline().decode() for _ in range(10)]
+        np_, _, nz, nel = (int(v) for v in lines[2].split()[:4])
+        names = lines[8].split()[0]
+        hdr = {"np": np_, "nz": nz, "nel": nel, "step": int(lines[3].split()[0]),
+               "time": float(lines[4].split()[0])}
+        out = {}
+        for c in names:
+            out[c] = np.frombuffer(f.read(8 * np_ * np_ * nz * nel), "<f8").reshape(
+                nz, nel, np_, np_).copy()
+    return hdr, out
+
+
+# ---------------------------------------------------------------------------
+# Drivers
+# ---------------------------------------------------------------------------
+
+class Problem:
+    """Mesh + numbering + boundary systems for every field of a session."""
+
+    def __init__(self, S: Session, rcm: bool = True):
+        self.S = S
+        tok = S.tokens
+        self.np = tok.ivalue("N_P")
+        self.nz = tok.ivalue("N_Z")
+        if self.nz > 1 and self.nz % 2:
+            raise ValueError("N_Z must be even")
+        self.M = Mesh(S, self.np)
+        self.nel = self.M.nel
+        self.N, self.B = {}, {}
+        for c in S.fields:
+            self.N[c] = Numbering(self.M, c, rcm)
+            self.B[c] = BoundarySystem(self.M, self.N[c], c)
+        self.dz = 2 * math.pi / tok["BETA"] / self.nz
+
+    def evaluate(self, expr, t=0.0):
+        """AuxField = function, physical space (src/auxfield.cpp:198-220)."""
+        M = self.M
+        out = np.empty((self.nz, self.nel, self.np, self.np))
+        for k in range(self.nz):
+            val = self.S.tokens.evaluate(expr, x=M.x, y=M.y, z=k * self.dz, t=t)
+            out[k] = np.broadcast_to(np.asarray(val, float), M.x.shape)
+        return out
+
+    def bc_lines(self, c, t=0.0):
+        """Fourier-transformed BC lines [nz, nedge, np] (src/field.cpp:62-160)."""
+        B = self.B[c]
+        phys = np.stack([B.evaluate_physical(self.S.tokens, k * self.dz, t)
+                         for k in range(self.nz)])
+        return dft_forward(phys)
+
+    def modal_systems(self, c, lambda2, method="DIRECT", cache=None):
+        """ModalMatrixSys (src/matrix.cpp:33-105): one MatrixSys per mode."""
+        beta = self.S.tokens["BETA"]
+        nmodes = (self.nz + 1) // 2
+        out = []
+        for m in range(nmodes):
+            bk2 = (beta * m) ** 2
+            key = (c, round(lambda2, 14), round(bk2, 14), method)
+            if cache is not None and key in cache:
+                out.append(cache[key])
+                continue
+            ms = MatrixSys(self.M, self.N[c], lambda2, bk2, method)
+            if cache is not None:
+                cache[key] = ms
+            out.append(ms)
+        return out
+
+    def solve(self, c, forcing, unknown, systems, bclines, tol_rel=1e-8, step_max=500):
+        """Field::solve over all planes; forcing in Fourier space."""
+        out = unknown.copy()
+        for k in range(self.nz):
+            if k == 1:
+                continue
+            out[k] = solve_plane(self.M, self.N[c], self.B[c], systems[k >> 1],
+                                 forcing[k], unknown[k], bclines[k], tol_rel, step_max)
+        return out
+
+
+def elliptic(path: str, overrides: dict | None = None, forcing_phys=None):
+    """elliptic driver (elliptic/drive.cpp:61-96, elliptic/helmholtz.cpp:29-52).
+
+    Returns (problem, solution in physical space [nz, nel, np, np]).
+    forcing_phys overrides the USER 'forcing' string (the `.frc` path).
+    """
+    S = read_session(path, overrides)
+    P = Problem(S)
+    c = S.fields[0]
+    tok = S.tokens
+    if forcing_phys is None:
+        fstr = None
+        for ln in S.user:
+            parts = ln.split(None, 1)
+            if parts and parts[0].upper() == "FORCING":
+                fstr = parts[1].split()[0]
+        forcing_phys = P.evaluate(fstr) if fstr else np.zeros((P.nz, P.nel, P.np, P.np))
+    F = dft_forward(forcing_phys)
+    if P.nz > 1:
+        F[1] = 0.0
+    systems = P.modal_systems(c, tok["LAMBDA2"], "JACPCG" if tok.ivalue("ITERATIVE") else "DIRECT")
+    u0 = np.zeros_like(F)
+    U = P.solve(c, F, u0, systems, P.bc_lines(c), tok["TOL_REL"], tok.ivalue("STEP_MAX"))
+    if P.nz > 1:
+        U[1] = 0.0
+    return P, dft_inverse(U)
+
+
+def exact_field(P: Problem, which: str = "EXACT", t: float = 0.0):
+    for ln in P.S.user:
+        parts = ln.split(None, 1)
+        if parts and parts[0].upper() == which:
+            return P.evaluate(parts[1].split()[0], t)
+    raise KeyError(which)
+
+
+# ---------------------------------------------------------------------------
+# DNS time step (dns/integrate.cpp:66-289, dns/nonlinear.cpp:198-381)
+# ---------------------------------------------------------------------------
+
+SS_COEFF = {1: [1.0, -1.0], 2: [1.5, -2.0, 0.5],
+            3: [11.0 / 6.0, -3.0, 1.5, -1.0 / 3.0]}      # src/integration.cpp:99-133
+EX_COEFF = {1: [1.0], 2: [2.0, -1.0], 3: [3.0, -3.0, 1.0]}  # src/integration.cpp:136-164
+
+
+def fourier_grad_z(P: Problem, u):
+    """AuxField::gradient(2) on Fourier data (src/auxfield.cpp:651-672)."""
+    beta = P.S.tokens["BETA"]
+    out = np.empty_like(u)
+    out[0] = 0.0
+    out[1] = 0.0
+    for m in range(1, P.nz // 2):
+        out[2 * m] = -beta * m * u[2 * m + 1]
+        out[2 * m + 1] = beta * m * u[2 * m]
+    return out
+
+
+def plane_grad(P: Problem, u, d):
+    if d == 2:
+        return fourier_grad_z(P, u)
+    return grad(P.M, u, d)
+
+
+def smooth(P: Problem, c: str, u):
+    """Field::smooth (src/field.cpp:282-327), per plane."""
+    M, N = P.M, P.N[c]
+    next_ = 4 * (P.np - 1)
+    em = M.emap()[:next_]
+    out = u.copy()
+    wq = M.Q4.reshape(P.nel, -1)[:, em]
+    for k in range(u.shape[0]):
+        flat = out[k].reshape(P.nel, -1)
+        ds = np.zeros(N.nglobal)
+        np.add.at(ds, N.btog, wq * flat[:, em])
+        ds *= N.imass
+        flat[:, em] = ds[N.btog]
+    return out
+
+
+class DNS:
+    """Velocity-correction DNS on a Problem (Cartesian, periodic / Dirichlet).
+
+    State is kept in Fourier space as [nz, nel, np, np] arrays per field,
+    with the reference's multi-level storage Us/Uf (dns/integrate.cpp:94-136).
+    """
+
+    def __init__(self, P: Problem, ic: dict | None = None, t0: float = 0.0,
+                 dealias: bool = False):
+        if dealias:
+            raise NotImplementedError("3/2-rule products are not in the oracle")
+        self.P = P
+        S = P.S
+        tok = S.tokens
+        self.ncom = len(S.fields) - 1
+        self.ndim = 3 if P.nz > 1 else 2
+        self.nord = tok.ivalue("N_TIME")
+        self.dt = tok["D_T"]
+        self.nu = tok["KINVIS"]
+        self.vel = S.fields[:self.ncom]
+        self.pname = S.fields[self.ncom]
+        if any(kind == "H" for g in S.bcs.values() for (kind, _) in g.values()):
+            raise NotImplementedError("high-order pressure BCs are not in the oracle")
+        shape = (P.nz, P.nel, P.np, P.np)
+        self.u = {}
+        for c in S.fields:
+            if ic and c in ic:
+                phys = ic[c]
+            else:
+                phys = np.zeros(shape)
+            f = dft_forward(phys)
+            if P.nz > 1:
+                f[1] = 0.0
+            self.u[c] = f
+        self.Us = [[np.zeros(shape) for _ in range(self.ncom)] for _ in range(self.nord)]
+        self.Uf = [[np.zeros(shape) for _ in range(self.ncom)] for _ in range(self.nord)]
+        self.step, self.time = 0, t0
+        self.toggle = 1
+        self.cache = {}
+        lam = SS_COEFF[self.nord][0] / (self.dt * self.nu)
+        self.vsys = {c: P.modal_systems(c, lam, "DIRECT", self.cache) for c in self.vel}
+        self.psys = P.modal_systems(self.pname, 0.0, "DIRECT", self.cache)
+
+    def nonlinear(self):
+        """altSkewSymmetric, Cartesian branch (dns/nonlinear.cpp:198-381)."""
+        P = self.P
+        U = [self.u[c].copy() for c in self.vel]
+        Uphys = [dft_inverse(self.u[c]) for c in self.vel]
+        N = []
+        for i in range(self.ncom):
+            n = np.zeros_like(U[0])
+            for j in range(self.ndim):
+                if self.toggle:
+                    if j == 2:
+                        tmp = dft_inverse(fourier_grad_z(P, U[i]))
+                    else:
+                        tmp = grad(P.M, Uphys[i], j)
+                    n -= Uphys[j] * tmp
+                else:
+                    tmp = Uphys[i] * Uphys[j]
+                    if j == 2:
+                        tmp = dft_inverse(fourier_grad_z(P, dft_forward(tmp)))
+                    else:
+                        tmp = grad(P.M, tmp, j)
+                    n -= tmp
+            n = dft_forward(n)
+            N.append(smooth(P, self.vel[0], n))
+        self.toggle = 1 - self.toggle
+        return U, N
+
+    def advance(self, nsteps: int = 1):
+        P = self.P
+        tok = P.S.tokens
+        for _ in range(nsteps):
+            U, N = self.nonlinear()
+            self.Us[0] = U
+            self.Uf[0] = N
+            self.step += 1
+            self.time += self.dt
+            # -- waveProp (dns/integrate.cpp:204-239)
+            Je = min(self.step, self.nord)
+            alpha = SS_COEFF[Je]
+            beta = [b * self.dt for b in EX_COEFF[Je]]
+            uhat = []
+            for i in range(self.ncom):
+                h = np.zeros_like(U[0])
+                for q in range(Je):
+                    h += -alpha[q + 1] * self.Us[q][i]
+                    h += beta[q] * self.Uf[q][i]
+                uhat.append(h)
+            self.Uf = [self.Uf[-1]] + self.Uf[:-1]          # rollm(Uf)
+            # -- setPForce (dns/integrate.cpp:242-257)
+            div = np.zeros_like(U[0])
+            for i in range(self.ndim):
+                div += plane_grad(P, uhat[i], i)
+            div /= self.dt
+            pc = self.pname
+            self.u[pc] = P.solve(pc, div, self.u[pc], self.psys,
+                                 P.bc_lines(pc, self.time), tok["TOL_REL"])
+            # -- project (dns/integrate.cpp:260-289)
+            a = -1.0 / (self.dt * self.nu)
+            b = 1.0 / self.nu
+            forc = []
+            for i in range(self.ncom):
+                f = a * uhat[i]
+                if i < self.ndim:
+                    f = f + b * plane_grad(P, self.u[pc], i)
+                forc.append(f)
+            self.Us[0] = [self.u[c] for c in self.vel]
+            self.Us = [self.Us[-1]] + self.Us[:-1]          # rollm(Us)
+            # -- viscous substep (dns/integrate.cpp:186-193, 328-356)
+            for i, c in enumerate(self.vel):
+                if self.step < self.nord:
+                    lam = SS_COEFF[Je][0] / (self.dt * self.nu)
+                    sysi = P.modal_systems(c, lam, "JACPCG", self.cache)
+                else:
+                    sysi = self.vsys[c]
+                self.u[c] = P.solve(c, forc[i], self.u[c], sysi,
+                                    P.bc_lines(c, self.time), tok["TOL_REL"],
+                                    tok.ivalue("STEP_MAX"))
+
+    def physical(self):
+        out = {}
+        for c, v in self.u.items():
+            f = v.copy()
+            if self.P.nz > 1:
+                f[1] = 0.0
+            out[c] = dft_inverse(f)
+        return out
+
+
+def user_functions(S: Session):
+    """USER-section 'name = expr' lines (as `compare` reads them)."""
+    out = {}
+    for ln in S.user:
+        if "=" in ln:
+            name, expr = ln.split("=", 1)
+            out[name.strip()] = expr.strip()
+    return out
+
+
+def dns_session(path: str, overrides: dict | None = None, nsteps: int | None = None):
+    """Run `dns` with the USER solution at t=0 as restart (test/testregress)."""
+    S = read_session(path, overrides)
+    P = Problem(S)
+    funcs = user_functions(S)
+    ic = {c: P.evaluate(funcs[c], 0.0) for c in S.fields if c in funcs}
+    D = DNS(P, ic)
+    D.advance(S.tokens.ivalue("N_STEP") if nsteps is None else nsteps)
+    return D
+
+
+def compare_errors(D: DNS, noise: float = 1e-12):
+    """`compare -n` ∞-norm errors vs the USER solution (utility/compare.cpp:197-232)."""
+    P = D.P
+    funcs = user_functions(P.S)
+    t = float(f"{D.time:.6g}")
+    out = {}
+    for c, ph in D.physical().items():
+        ex = P.evaluate(funcs[c], t) if c in funcs else np.zeros_like(ph)
+        err = np.abs(ex - ph).max()
+        out[c] = "noise-level" if err < noise else f"{err:.4e}"
+    return out

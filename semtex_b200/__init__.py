@@ -1,0 +1,252 @@
+"""semtex_b200: B200-native spectral-element--Fourier Helmholtz solve and DNS step.
+
+Python mirror of the reference's C++ API for the hot path, over the C ABI of
+``libsemtex_b200.so`` (include/semtex_b200.h):
+
+* :class:`Context`  -- FEML session + mesh + numbering on one GPU
+  (the FEML/Mesh/Element/BCmgr/Domain construction, elliptic/drive.cpp:145-216)
+* :class:`ModalMatrixSys` -- per-mode condensed systems (src/matrix.h:55-71)
+* :class:`Field`    -- device field data in the reference plane layout with
+  ``solve`` (src/field.h:27) and ``transform`` (src/auxfield.h:61)
+* :func:`elliptic`  -- the `elliptic` driver (elliptic/drive.cpp:61-96)
+
+Device memory is held in torch tensors (plumbing only); every numerical
+operation runs in the library's CUDA kernels.  There is no CPU fallback.
+"""
+
+from __future__ import annotations
+
+import ctypes as C
+import os
+
+import numpy as np
+
+from . import _lib
+from ._lib import FORWARD, INVERSE, STX_DIRECT, STX_JACPCG, StxError, check, lib
+from .fieldfile import read_field, write_field
+
+DIRECT, JACPCG = STX_DIRECT, STX_JACPCG
+
+__all__ = ["Context", "ModalMatrixSys", "Field", "elliptic", "read_field", "write_field",
+           "FORWARD", "INVERSE", "DIRECT", "JACPCG", "StxError"]
+
+
+def _torch():
+    import torch
+    if not torch.cuda.is_available():
+        raise RuntimeError("semtex_b200 needs a CUDA device (no CPU fallback)")
+    return torch
+
+
+class Context:
+    """A session on one GPU: mesh, geometry, numbering and BC storage."""
+
+    def __init__(self, session: str, overrides: dict | str | None = None, device: int = 0,
+                 stream: int | None = None):
+        if isinstance(overrides, dict):
+            overrides = ";".join(f"{k}={v}" for k, v in overrides.items())
+        self._h = C.c_void_p()
+        check(lib().stx_context_create(session.encode(), overrides.encode() if overrides else None,
+                                       device, C.c_void_p(stream) if stream else None,
+                                       C.byref(self._h)))
+        self.session = session
+        self.device = device
+        np_, nz, nel, ps = C.c_int(), C.c_int(), C.c_int(), C.c_int()
+        check(lib().stx_context_geometry(self._h, C.byref(np_), C.byref(nz), C.byref(nel), C.byref(ps)))
+        self.np, self.nz, self.nel, self.plane_size = np_.value, nz.value, nel.value, ps.value
+        buf = C.create_string_buffer(64)
+        check(lib().stx_context_fields(self._h, buf, 64))
+        self.fields = buf.value.decode()
+
+    @property
+    def handle(self):
+        return self._h
+
+    def close(self):
+        if self._h:
+            check(lib().stx_context_destroy(self._h))
+            self._h = C.c_void_p()
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    def token(self, expr: str) -> float:
+        v = C.c_double()
+        check(lib().stx_token(self._h, expr.encode(), C.byref(v)))
+        return v.value
+
+    def numbering(self, field: str):
+        a, b, c = C.c_int(), C.c_int(), C.c_int()
+        check(lib().stx_numbering(self._h, field.encode(), C.byref(a), C.byref(b), C.byref(c)))
+        return {"nglobal": a.value, "nsolve": b.value, "nband": c.value}
+
+    def families(self) -> int:
+        v = C.c_int()
+        check(lib().stx_mesh_families(self._h, C.byref(v)))
+        return v.value
+
+    def mesh_coords(self):
+        n = self.nel * self.np * self.np
+        x, y = np.empty(n), np.empty(n)
+        check(lib().stx_mesh_coords(self._h, x.ctypes.data, y.ctypes.data))
+        s = (self.nel, self.np, self.np)
+        return x.reshape(s), y.reshape(s)
+
+    def evaluate(self, expr: str, t: float = 0.0) -> np.ndarray:
+        """AuxField = "function" in physical space, [nz, nel, np, np]."""
+        out = np.empty((self.nz, self.nel, self.np, self.np))
+        check(lib().stx_field_evaluate(self._h, expr.encode(), t, out.ctypes.data))
+        return out
+
+    def bc_evaluate(self, field: str, t: float = 0.0):
+        check(lib().stx_field_bc_evaluate(self._h, field.encode(), t))
+
+    def sync(self):
+        check(lib().stx_sync(self._h))
+
+    # -- device field storage in the reference layout
+    def new_field(self, name: str = "f"):
+        return Field(self, name)
+
+
+class Field:
+    """Device data of one field, [nz, plane_size] doubles (AuxField storage)."""
+
+    def __init__(self, ctx: Context, name: str):
+        torch = _torch()
+        self.ctx, self.name = ctx, name
+        self.data = torch.zeros((ctx.nz, ctx.plane_size), dtype=torch.float64,
+                                device=f"cuda:{ctx.device}")
+
+    def ptr(self):
+        return C.c_void_p(self.data.data_ptr())
+
+    def load_physical(self, a: np.ndarray):
+        """Set from physical-space [nz, nel, np, np] host data (no transform)."""
+        torch = _torch()
+        n = self.ctx.nel * self.ctx.np ** 2
+        self.data.zero_()
+        self.data[:, :n] = torch.from_numpy(np.ascontiguousarray(a).reshape(self.ctx.nz, n)).to(self.data.device)
+        return self
+
+    def to_numpy(self) -> np.ndarray:
+        n = self.ctx.nel * self.ctx.np ** 2
+        self.ctx.sync()
+        return self.data[:, :n].cpu().numpy().reshape(self.ctx.nz, self.ctx.nel, self.ctx.np, self.ctx.np)
+
+    def transform(self, sign: int):
+        """AuxField::transform (src/auxfield.cpp:1157)."""
+        check(lib().stx_transform(self.ctx.handle, self.ptr(), sign))
+        return self
+
+    def zero_nyquist(self):
+        if self.ctx.nz > 1:
+            self.data[1].zero_()
+        return self
+
+    def solve(self, forcing: "Field", system: "ModalMatrixSys", tol_rel: float | None = None,
+              step_max: int | None = None):
+        """Field::solve(f, MMS) (src/field.cpp:598-809); forcing in Fourier space."""
+        ctx = self.ctx
+        tol = ctx.token("TOL_REL") if tol_rel is None else tol_rel
+        smax = int(ctx.token("STEP_MAX")) if step_max is None else step_max
+        iters = (C.c_int * ctx.nz)()
+        rc = lib().stx_field_solve(system.handle, forcing.ptr(), self.ptr(), tol, smax, iters)
+        if rc == _lib.STX_ENOCONV:
+            import warnings
+            warnings.warn("Field::solve: step limit exceeded")
+        else:
+            check(rc)
+        self.iterations = list(iters)
+        return self
+
+
+class ModalMatrixSys:
+    """ModalMatrixSys(lambda2, beta, base, nmodes, ..., method) for one field."""
+
+    def __init__(self, ctx: Context, field: str, lambda2: float, beta: float | None = None,
+                 base_mode: int = 0, num_modes: int | None = None, method: int = DIRECT):
+        self.ctx = ctx
+        beta = ctx.token("BETA") if beta is None else beta
+        num_modes = (ctx.nz + 1) // 2 if num_modes is None else num_modes
+        self._h = C.c_void_p()
+        check(lib().stx_modal_create(ctx.handle, field.encode(), lambda2, beta, base_mode, num_modes,
+                                     method, C.byref(self._h)))
+        self.field, self.lambda2, self.beta, self.method = field, lambda2, beta, method
+        self.num_modes = num_modes
+
+    @property
+    def handle(self):
+        return self._h
+
+    def info(self, mode: int):
+        a, b = C.c_int(), C.c_int()
+        check(lib().stx_modal_info(self._h, mode, C.byref(a), C.byref(b)))
+        return {"nsolve": a.value, "nband": b.value}
+
+    def close(self):
+        if self._h and self.ctx._h:
+            check(lib().stx_modal_destroy(self._h))
+        self._h = C.c_void_p()
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    def solve_host(self, forcing_phys: np.ndarray, out: np.ndarray | None = None) -> np.ndarray:
+        """Whole elliptic solve from/to host memory (stx_elliptic_solve_host)."""
+        ctx = self.ctx
+        shape = (ctx.nz, ctx.nel, ctx.np, ctx.np)
+        f = np.ascontiguousarray(forcing_phys, dtype=np.float64)
+        if f.shape != shape:
+            raise ValueError(f"forcing shape {f.shape} != {shape}")
+        if out is None:
+            out = np.empty(shape)
+        check(lib().stx_elliptic_solve_host(self._h, C.c_void_p(f.ctypes.data),
+                                            C.c_void_p(out.ctypes.data)))
+        return out
+
+
+def _user_value(session: str, key: str):
+    txt = open(session).read()
+    import re
+    m = re.search(r"<USER>(.*?)</USER>", txt, re.S | re.I)
+    if not m:
+        return None
+    for ln in m.group(1).splitlines():
+        parts = ln.split(None, 1)
+        if parts and parts[0].upper() == key.upper():
+            return parts[1].split()[0]
+    return None
+
+
+def elliptic(session: str, overrides=None, iterative: bool = False, device: int = 0,
+             write: bool = False):
+    """The `elliptic` driver: solve the session's Helmholtz problem on the GPU.
+
+    Forcing comes from ``session.frc`` if present, else the USER ``forcing``
+    string, else zero (elliptic/drive.cpp:258-354).  Returns the physical
+    solution [nz, nel, np, np]; with ``write`` also writes ``session.fld``.
+    """
+    ctx = Context(session, overrides, device)
+    c = ctx.fields[0]
+    frc = session + ".frc"
+    if os.path.exists(frc):
+        _, flds = read_field(frc)
+        forcing = next(iter(flds.values()))
+    else:
+        fs = _user_value(session, "forcing")
+        forcing = ctx.evaluate(fs) if fs else np.zeros((ctx.nz, ctx.nel, ctx.np, ctx.np))
+    sys_ = ModalMatrixSys(ctx, c, ctx.token("LAMBDA2"), method=JACPCG if iterative else DIRECT)
+    u = sys_.solve_host(forcing)
+    if write:
+        write_field(session + ".fld", os.path.basename(session), ctx.np, ctx.nz, ctx.nel, 1, 0.0,
+                    ctx.token("D_T"), ctx.token("KINVIS"), ctx.token("BETA"), {c: u})
+    sys_.close()
+    ctx.close()
+    return u

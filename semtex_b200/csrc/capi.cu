@@ -1,0 +1,519 @@
+// C ABI of the library: context, modal systems, solves, transforms.
+//
+// Host code here owns the session, mesh and numbering (FP64 setup on the
+// host cores) and the device copies the kernels read.  Errors are reported
+// as status codes with a thread-local message instead of the reference's
+// print-and-exit (veclib/util.c:24-46).
+#include <cuda_runtime.h>
+
+#include <cmath>
+#include <cstring>
+#include <map>
+#include <memory>
+#include <mutex>
+#include <stdexcept>
+#include <string>
+#include <thread>
+#include <vector>
+
+#include "../../include/semtex_b200.h"
+#include "host/helmsys.hpp"
+#include "host/mesh.hpp"
+#include "host/session.hpp"
+#include "kernels/helmholtz.cuh"
+#include "stx_internal.hpp"
+
+namespace {
+
+thread_local std::string g_last_error;
+
+struct StxError : std::runtime_error {
+  int code;
+  StxError(int c, const std::string& m) : std::runtime_error(m), code(c) {}
+};
+
+void cuda_check(cudaError_t e, const char* what) {
+  if (e != cudaSuccess)
+    throw StxError(STX_ECUDA, std::string(what) + ": " + cudaGetErrorString(e));
+}
+
+template <class F>
+int guarded(F&& f) {
+  try {
+    f();
+    g_last_error.clear();
+    return STX_OK;
+  } catch (const StxError& e) {
+    g_last_error = e.what();
+    return e.code;
+  } catch (const std::exception& e) {
+    g_last_error = e.what();
+    const std::string m = e.what();
+    if (m.find("positive definite") != std::string::npos || m.find("singular") != std::string::npos)
+      return STX_ENUMERIC;
+    if (m.find("not supported") != std::string::npos) return STX_EUNSUPPORTED;
+    return STX_ESESSION;
+  }
+}
+
+}  // namespace
+
+namespace stx {
+
+void* DeviceArena::alloc(size_t bytes) {
+  void* p = nullptr;
+  if (bytes == 0) bytes = 8;
+  cuda_check(cudaMalloc(&p, bytes), "cudaMalloc");
+  ptrs.push_back(p);
+  return p;
+}
+
+DeviceArena::~DeviceArena() {
+  for (void* p : ptrs) cudaFree(p);
+}
+
+void host_dft_forward(std::vector<double>& a, int nz, int n) {
+  // Same contract as the device z_transform, for short BC lines.
+  if (nz < 2) return;
+  if (nz == 2) {
+    for (int i = 0; i < n; ++i) a[n + i] = 0.0;
+    return;
+  }
+  std::vector<double> out(a.size(), 0.0);
+  const int half = nz / 2;
+  for (int i = 0; i < n; ++i)
+    for (int q = 0; q < nz; ++q) {
+      const int kf = q == 0 ? 0 : (q == 1 ? half : q / 2);
+      const bool im = q >= 2 && (q & 1);
+      double v = 0;
+      for (int k = 0; k < nz; ++k) {
+        const double th = 2.0 * M_PI * ((static_cast<long>(kf) * k) % nz) / nz;
+        v += a[static_cast<size_t>(k) * n + i] * (im ? -std::sin(th) : std::cos(th));
+      }
+      out[static_cast<size_t>(q) * n + i] = v / nz;
+    }
+  a.swap(out);
+}
+
+}  // namespace stx
+
+using namespace stx;
+
+template <class T>
+static T* upload(DeviceArena& A, const std::vector<T>& v) {
+  T* p = static_cast<T*>(A.alloc(sizeof(T) * v.size()));
+  if (!v.empty()) cuda_check(cudaMemcpy(p, v.data(), sizeof(T) * v.size(), cudaMemcpyHostToDevice), "upload");
+  return p;
+}
+
+extern "C" {
+
+const char* stx_last_error(void) { return g_last_error.c_str(); }
+
+int stx_context_create(const char* session_path, const char* overrides, int device, void* stream,
+                       stx_context** out) {
+  return guarded([&] {
+    if (!session_path || !out) throw StxError(STX_EINVAL, "null argument");
+    *out = nullptr;
+    auto ctx = std::make_unique<stx_context>();
+    ctx->S = read_session(session_path, overrides ? overrides : "");
+    if (ctx->S.tokens.ivalue("CYLINDRICAL"))
+      throw StxError(STX_EUNSUPPORTED, "cylindrical coordinates are not supported");
+    ctx->M = build_mesh(ctx->S);
+    ctx->device = device;
+    cuda_check(cudaSetDevice(device), "cudaSetDevice");
+    if (stream) {
+      ctx->stream = static_cast<cudaStream_t>(stream);
+      ctx->own_stream = false;
+    } else {
+      cuda_check(cudaStreamCreateWithFlags(&ctx->stream, cudaStreamNonBlocking), "stream");
+      ctx->own_stream = true;
+    }
+    const Mesh& M = ctx->M;
+    DeviceArena& A = ctx->arena;
+    DevGeom& g = ctx->dg;
+    g.np = M.np;
+    g.nel = M.nel;
+    g.nz = M.nz;
+    g.npnp = M.npnp;
+    g.next = M.next;
+    g.nint = M.nint;
+    g.plane_size = M.plane_size;
+    g.D = upload(A, M.q.D);
+    g.Q1 = upload(A, M.Q1);
+    g.Q2 = upload(A, M.Q2);
+    g.Q3 = upload(A, M.Q3);
+    g.Q4 = upload(A, M.Q4);
+    g.drdx = upload(A, M.drdx);
+    g.drdy = upload(A, M.drdy);
+    g.dsdx = upload(A, M.dsdx);
+    g.dsdy = upload(A, M.dsdy);
+    g.emap = upload(A, M.emap);
+    g.pmap = upload(A, M.pmap);
+    g.family = upload(A, M.family);
+    std::vector<double> tw(2 * std::max(1, M.nz));
+    for (int m = 0; m < M.nz; ++m) {
+      tw[m] = std::cos(2.0 * M_PI * m / M.nz);
+      tw[M.nz + m] = std::sin(2.0 * M_PI * m / M.nz);
+    }
+    ctx->d_twiddle = upload(A, tw);
+    for (char c : ctx->S.fields) {
+      FieldDev& F = ctx->fields[c];
+      F.N = build_numbering(ctx->S, M, c);
+      const Numbering& N = F.N;
+      DevNumbering& d = F.dn;
+      d.nglobal = N.nglobal;
+      d.nsolve = N.nsolve;
+      d.nband = N.nband;
+      d.btog = upload(A, N.btog);
+      d.bmask = upload(A, N.bmask);
+      d.emask = upload(A, N.emask);
+      d.imass = upload(A, N.imass);
+      d.nedge = static_cast<int>(N.edges.size());
+      std::vector<int> gid, kind;
+      std::vector<double> area;
+      for (const auto& E : N.edges) {
+        for (int t = 0; t < M.np; ++t) {
+          gid.push_back(N.btog[E.elmt * M.next + (E.side * (M.np - 1) + t) % M.next]);
+          area.push_back(E.area[t]);
+        }
+        kind.push_back(E.kind);
+      }
+      d.edge_gid = upload(A, gid);
+      d.edge_kind = upload(A, kind);
+      d.edge_area = upload(A, area);
+      F.nline = d.nedge * M.np;
+      F.d_lines = static_cast<double*>(A.alloc(sizeof(double) * std::max(1, F.nline) * M.nz));
+      cuda_check(cudaMemset(F.d_lines, 0, sizeof(double) * std::max(1, F.nline) * M.nz), "memset");
+    }
+    *out = ctx.release();
+    for (char c : (*out)->S.fields) stx_field_bc_evaluate(*out, c, 0.0);
+    if (!g_last_error.empty()) {
+      std::string m = g_last_error;
+      stx_context_destroy(*out);
+      *out = nullptr;
+      throw StxError(STX_ESESSION, m);
+    }
+  });
+}
+
+int stx_context_destroy(stx_context* ctx) {
+  return guarded([&] {
+    if (!ctx) return;
+    cudaSetDevice(ctx->device);
+    cudaStreamSynchronize(ctx->stream);
+    for (auto* m : ctx->modals) delete m;
+    ctx->modals.clear();
+    if (ctx->own_stream) cudaStreamDestroy(ctx->stream);
+    delete ctx;
+  });
+}
+
+int stx_context_geometry(const stx_context* ctx, int* np, int* nz, int* nel, int* plane_size) {
+  return guarded([&] {
+    if (!ctx) throw StxError(STX_EINVAL, "null context");
+    if (np) *np = ctx->M.np;
+    if (nz) *nz = ctx->M.nz;
+    if (nel) *nel = ctx->M.nel;
+    if (plane_size) *plane_size = ctx->M.plane_size;
+  });
+}
+
+int stx_context_fields(const stx_context* ctx, char* buf, int len) {
+  return guarded([&] {
+    if (!ctx || !buf) throw StxError(STX_EINVAL, "null argument");
+    if (static_cast<int>(ctx->S.fields.size()) + 1 > len) throw StxError(STX_EINVAL, "buffer too small");
+    std::strcpy(buf, ctx->S.fields.c_str());
+  });
+}
+
+int stx_token(const stx_context* ctx, const char* expr, double* value) {
+  return guarded([&] {
+    if (!ctx || !expr || !value) throw StxError(STX_EINVAL, "null argument");
+    *value = ctx->S.tokens.value(expr);
+  });
+}
+
+int stx_numbering(const stx_context* ctx, char field, int* nglobal, int* nsolve, int* nband) {
+  return guarded([&] {
+    auto it = ctx->fields.find(field);
+    if (it == ctx->fields.end()) throw StxError(STX_EINVAL, std::string("no field ") + field);
+    if (nglobal) *nglobal = it->second.N.nglobal;
+    if (nsolve) *nsolve = it->second.N.nsolve;
+    if (nband) *nband = it->second.N.nband;
+  });
+}
+
+int stx_mesh_coords(const stx_context* ctx, double* h_x, double* h_y) {
+  return guarded([&] {
+    if (!ctx) throw StxError(STX_EINVAL, "null context");
+    if (h_x) std::memcpy(h_x, ctx->M.x.data(), sizeof(double) * ctx->M.x.size());
+    if (h_y) std::memcpy(h_y, ctx->M.y.data(), sizeof(double) * ctx->M.y.size());
+  });
+}
+
+int stx_mesh_families(const stx_context* ctx, int* nfamily) {
+  return guarded([&] {
+    if (!ctx || !nfamily) throw StxError(STX_EINVAL, "null argument");
+    *nfamily = ctx->M.nfamily;
+  });
+}
+
+int stx_field_evaluate(const stx_context* ctx, const char* expr, double t, double* h_out) {
+  return guarded([&] {
+    if (!ctx || !expr || !h_out) throw StxError(STX_EINVAL, "null argument");
+    const Mesh& M = ctx->M;
+    const double dz = 2.0 * M_PI / ctx->S.tokens.value("BETA") / M.nz;
+    std::map<std::string, double> vars;
+    vars["t"] = t;
+    for (int k = 0; k < M.nz; ++k) {
+      vars["z"] = k * dz;
+      for (int i = 0; i < M.nplane; ++i) {
+        vars["x"] = M.x[i];
+        vars["y"] = M.y[i];
+        h_out[static_cast<size_t>(k) * M.nplane + i] = ctx->S.tokens.eval(expr, &vars);
+      }
+    }
+  });
+}
+
+int stx_field_bc_evaluate(stx_context* ctx, char field, double t) {
+  return guarded([&] {
+    if (!ctx) throw StxError(STX_EINVAL, "null context");
+    auto it = ctx->fields.find(field);
+    if (it == ctx->fields.end()) throw StxError(STX_EINVAL, std::string("no field ") + field);
+    FieldDev& F = it->second;
+    const Mesh& M = ctx->M;
+    const int nz = M.nz, np = M.np;
+    if (F.nline == 0) return;
+    const double dz = 2.0 * M_PI / ctx->S.tokens.value("BETA") / nz;
+    std::vector<double> line(static_cast<size_t>(F.nline) * nz, 0.0);
+    std::map<std::string, double> vars;
+    vars["t"] = t;
+    for (int k = 0; k < nz; ++k) {
+      vars["z"] = k * dz;
+      for (size_t b = 0; b < F.N.edges.size(); ++b) {
+        const BoundaryEdge& E = F.N.edges[b];
+        for (int q = 0; q < np; ++q) {
+          vars["x"] = E.x[q];
+          vars["y"] = E.y[q];
+          line[static_cast<size_t>(k) * F.nline + b * np + q] = ctx->S.tokens.eval(E.expr, &vars);
+        }
+      }
+    }
+    host_dft_forward(line, nz, F.nline);
+    cuda_check(cudaMemcpyAsync(F.d_lines, line.data(), sizeof(double) * line.size(),
+                               cudaMemcpyHostToDevice, ctx->stream),
+               "bc upload");
+    cuda_check(cudaStreamSynchronize(ctx->stream), "bc sync");
+  });
+}
+
+int stx_modal_create(stx_context* ctx, char field, double lambda2, double beta, int base_mode,
+                     int num_modes, int method, stx_modal** out) {
+  return guarded([&] {
+    if (!ctx || !out) throw StxError(STX_EINVAL, "null argument");
+    *out = nullptr;
+    auto it = ctx->fields.find(field);
+    if (it == ctx->fields.end()) throw StxError(STX_EINVAL, std::string("no field ") + field);
+    if (method != STX_DIRECT && method != STX_JACPCG) throw StxError(STX_EINVAL, "unknown method");
+    const int nmode_total = (ctx->M.nz + 1) / 2;
+    if (base_mode != 0 || num_modes != nmode_total)
+      throw StxError(STX_EINVAL, "a single-device context holds all modes: base 0, nz/2 modes");
+    cudaSetDevice(ctx->device);
+    const Numbering& N = it->second.N;
+    auto sys = std::make_unique<stx_modal>();
+    sys->ctx = ctx;
+    sys->field = field;
+    sys->method = method;
+    // -- share storage with an existing system of equal constants/numbering
+    for (auto* o : ctx->modals)
+      if (o->method == method && std::fabs(o->lambda2 - lambda2) < 6e-14 &&
+          std::fabs(o->beta - beta) < 6e-14 && ctx->fields.at(o->field).N.same_as(N)) {
+        sys->store = o->store;
+        break;
+      }
+    sys->lambda2 = lambda2;
+    sys->beta = beta;
+    if (!sys->store) {
+      auto st = std::make_shared<ModalStore>();
+      const Mesh& M = ctx->M;
+      std::vector<ModeSystem> modes(num_modes);
+      std::vector<std::string> errs(num_modes);
+      unsigned nth = std::max(1u, std::min<unsigned>(std::thread::hardware_concurrency(), num_modes));
+      std::vector<std::thread> pool;
+      for (unsigned w = 0; w < nth; ++w)
+        pool.emplace_back([&, w] {
+          for (int m = static_cast<int>(w); m < num_modes; m += nth) {
+            try {
+              const double bk = beta * (base_mode + m);
+              modes[m] = build_mode_system(M, N, lambda2, bk * bk, method);
+            } catch (const std::exception& e) {
+              errs[m] = e.what();
+            }
+          }
+        });
+      for (auto& th : pool) th.join();
+      for (auto& e : errs)
+        if (!e.empty()) throw StxError(STX_ENUMERIC, e);
+      DevModal& d = st->dm;
+      d.nmodes = num_modes;
+      d.method = method;
+      d.nfamily = M.nfamily;
+      d.nband = N.nband;
+      std::vector<double> lam(num_modes), bk2(num_modes);
+      std::vector<int> ns(num_modes);
+      int nsmax = 0;
+      for (int m = 0; m < num_modes; ++m) {
+        lam[m] = modes[m].lambda2;
+        bk2[m] = modes[m].betak2;
+        ns[m] = modes[m].nsolve;
+        nsmax = std::max(nsmax, ns[m]);
+      }
+      st->nsolve = ns;
+      d.ns_stride = nsmax;
+      d.lambda2 = upload(st->arena, lam);
+      d.betak2 = upload(st->arena, bk2);
+      d.nsolve = upload(st->arena, ns);
+      if (method == STX_DIRECT) {
+        std::vector<double> hbi, hii, fwd, bwd;
+        const size_t band = static_cast<size_t>(nsmax) * N.nband;
+        for (int m = 0; m < num_modes; ++m) {
+          hbi.insert(hbi.end(), modes[m].hbi.begin(), modes[m].hbi.end());
+          hii.insert(hii.end(), modes[m].hii.begin(), modes[m].hii.end());
+          auto f = modes[m].fwd, b = modes[m].bwd;
+          f.resize(band, 0.0);
+          b.resize(band, 0.0);
+          fwd.insert(fwd.end(), f.begin(), f.end());
+          bwd.insert(bwd.end(), b.begin(), b.end());
+          modes[m] = ModeSystem();
+        }
+        d.hbi = upload(st->arena, hbi);
+        d.hii = upload(st->arena, hii);
+        d.fwd = upload(st->arena, fwd);
+        d.bwd = upload(st->arena, bwd);
+        d.pc = nullptr;
+        d.npts = 0;
+      } else {
+        std::vector<double> pc;
+        d.npts = N.nglobal + M.nel * M.nint;
+        for (int m = 0; m < num_modes; ++m) pc.insert(pc.end(), modes[m].pc.begin(), modes[m].pc.end());
+        d.pc = upload(st->arena, pc);
+        d.hbi = d.hii = d.fwd = d.bwd = nullptr;
+      }
+      sys->store = st;
+    }
+    ctx->modals.push_back(sys.get());
+    *out = sys.release();
+  });
+}
+
+int stx_modal_destroy(stx_modal* sys) {
+  return guarded([&] {
+    if (!sys) return;
+    auto& v = sys->ctx->modals;
+    for (auto it = v.begin(); it != v.end(); ++it)
+      if (*it == sys) {
+        v.erase(it);
+        break;
+      }
+    cudaSetDevice(sys->ctx->device);
+    cudaStreamSynchronize(sys->ctx->stream);
+    delete sys;
+  });
+}
+
+int stx_modal_info(const stx_modal* sys, int mode, int* nsolve, int* nband) {
+  return guarded([&] {
+    if (!sys || mode < 0 || mode >= sys->store->dm.nmodes) throw StxError(STX_EINVAL, "bad mode");
+    if (nsolve) *nsolve = sys->store->nsolve[mode];
+    if (nband) *nband = sys->store->dm.nband;
+  });
+}
+
+int stx_field_solve(stx_modal* sys, const double* d_forcing, double* d_unknown, double tol_rel,
+                    int step_max, int* iterations) {
+  return guarded([&] {
+    if (!sys || !d_forcing || !d_unknown) throw StxError(STX_EINVAL, "null argument");
+    stx_context* ctx = sys->ctx;
+    FieldDev& F = ctx->fields.at(sys->field);
+    cudaSetDevice(ctx->device);
+    if (sys->method == STX_DIRECT) {
+      double* work = ctx->workspace(helmholtz_workspace_doubles(ctx->dg, F.dn));
+      cuda_check(helmholtz_direct_solve(ctx->dg, F.dn, sys->store->dm, d_forcing, d_unknown,
+                                        F.d_lines, F.nline, work, ctx->stream),
+                 "direct solve");
+    } else {
+      double* work = ctx->workspace(jacpcg_workspace_doubles(ctx->dg, F.dn));
+      std::vector<int> it(ctx->M.nz, -1);
+      cudaError_t e = helmholtz_jacpcg_solve(ctx->dg, F.dn, sys->store->dm, d_forcing, d_unknown,
+                                             F.d_lines, F.nline, tol_rel, step_max, work,
+                                             it.data(), ctx->stream);
+      if (iterations) std::memcpy(iterations, it.data(), sizeof(int) * it.size());
+      if (e == cudaErrorNotReady) throw StxError(STX_ENOCONV, "Field::solve: step limit exceeded");
+      cuda_check(e, "jacpcg solve");
+    }
+  });
+}
+
+int stx_transform(stx_context* ctx, double* d_data, int sign) {
+  return guarded([&] {
+    if (!ctx || !d_data) throw StxError(STX_EINVAL, "null argument");
+    if (sign != STX_FORWARD && sign != STX_INVERSE) throw StxError(STX_EINVAL, "bad sign");
+    cudaSetDevice(ctx->device);
+    cuda_check(z_transform(d_data, ctx->M.nz, ctx->M.plane_size, sign, ctx->d_twiddle, nullptr,
+                           ctx->stream),
+               "transform");
+  });
+}
+
+int stx_elliptic_solve_host(stx_modal* sys, const double* h_forcing, double* h_solution) {
+  return guarded([&] {
+    if (!sys || !h_forcing || !h_solution) throw StxError(STX_EINVAL, "null argument");
+    stx_context* ctx = sys->ctx;
+    const Mesh& M = ctx->M;
+    cudaSetDevice(ctx->device);
+    const size_t nplane = M.nplane, ps = M.plane_size, nz = M.nz;
+    if (!ctx->d_io) {
+      ctx->d_io = static_cast<double*>(ctx->arena.alloc(sizeof(double) * 2 * ps * nz));
+      cuda_check(cudaMemset(ctx->d_io, 0, sizeof(double) * 2 * ps * nz), "memset io");
+    }
+    double* dF = ctx->d_io;
+    double* dU = ctx->d_io + ps * nz;
+    for (size_t k = 0; k < nz; ++k)
+      cuda_check(cudaMemcpyAsync(dF + k * ps, h_forcing + k * nplane, sizeof(double) * nplane,
+                                 cudaMemcpyHostToDevice, ctx->stream),
+                 "forcing h2d");
+    cuda_check(z_transform(dF, M.nz, M.plane_size, STX_FORWARD, ctx->d_twiddle, nullptr, ctx->stream),
+               "forward transform");
+    if (nz > 1) cuda_check(cudaMemsetAsync(dF + ps, 0, sizeof(double) * ps, ctx->stream), "nyquist");
+    cuda_check(cudaMemsetAsync(dU, 0, sizeof(double) * ps * nz, ctx->stream), "zero solution");
+    const double tol = ctx->S.tokens.value("TOL_REL");
+    const int smax = ctx->S.tokens.ivalue("STEP_MAX");
+    int rc = stx_field_solve(sys, dF, dU, tol, smax, nullptr);
+    if (rc != STX_OK) throw StxError(rc, g_last_error);
+    cuda_check(z_transform(dU, M.nz, M.plane_size, STX_INVERSE, ctx->d_twiddle, nullptr, ctx->stream),
+               "inverse transform");
+    for (size_t k = 0; k < nz; ++k)
+      cuda_check(cudaMemcpyAsync(h_solution + k * nplane, dU + k * ps, sizeof(double) * nplane,
+                                 cudaMemcpyDeviceToHost, ctx->stream),
+                 "solution d2h");
+    cuda_check(cudaStreamSynchronize(ctx->stream), "sync");
+  });
+}
+
+int stx_sync(stx_context* ctx) {
+  return guarded([&] {
+    if (!ctx) throw StxError(STX_EINVAL, "null context");
+    cuda_check(cudaStreamSynchronize(ctx->stream), "sync");
+  });
+}
+
+int stx_context_scratch(stx_context* ctx, unsigned long long bytes, void** d_ptr) {
+  return guarded([&] {
+    if (!ctx || !d_ptr) throw StxError(STX_EINVAL, "null argument");
+    *d_ptr = ctx->scratch(bytes);
+  });
+}
+
+}  // extern "C"

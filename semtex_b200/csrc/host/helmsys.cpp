@@ -1,0 +1,196 @@
+#include "helmsys.hpp"
+
+#include <cmath>
+#include <stdexcept>
+#include <string>
+
+namespace stx {
+
+namespace {
+constexpr double kEpsSP = 6.0e-7;
+
+// In-place inverse of a dense n x n matrix by Gauss--Jordan with partial
+// pivoting (the role of getrf + getri at src/element.cpp:197-211).
+void invert(int n, double* A) {
+  std::vector<int> piv(n);
+  for (int i = 0; i < n; ++i) piv[i] = i;
+  std::vector<double> B(static_cast<size_t>(n) * 2 * n, 0.0);
+  for (int i = 0; i < n; ++i) {
+    for (int j = 0; j < n; ++j) B[i * 2 * n + j] = A[i * n + j];
+    B[i * 2 * n + n + i] = 1.0;
+  }
+  for (int c = 0; c < n; ++c) {
+    int p = c;
+    for (int r = c + 1; r < n; ++r)
+      if (std::fabs(B[r * 2 * n + c]) > std::fabs(B[p * 2 * n + c])) p = r;
+    if (B[p * 2 * n + c] == 0.0) throw std::runtime_error("matrix hii is singular");
+    if (p != c)
+      for (int j = 0; j < 2 * n; ++j) std::swap(B[p * 2 * n + j], B[c * 2 * n + j]);
+    const double d = 1.0 / B[c * 2 * n + c];
+    for (int j = 0; j < 2 * n; ++j) B[c * 2 * n + j] *= d;
+    for (int r = 0; r < n; ++r) {
+      if (r == c) continue;
+      const double f = B[r * 2 * n + c];
+      if (f == 0.0) continue;
+      for (int j = 0; j < 2 * n; ++j) B[r * 2 * n + j] -= f * B[c * 2 * n + j];
+    }
+  }
+  for (int i = 0; i < n; ++i)
+    for (int j = 0; j < n; ++j) A[i * n + j] = B[i * 2 * n + n + j];
+}
+}  // namespace
+
+void element_helmholtz(const Mesh& M, int e, double lambda2, double betak2, double* H) {
+  const int n = M.np, nn = M.npnp;
+  const double* D = M.q.D.data();
+  const double* Q1 = &M.Q1[e * nn];
+  const double* Q2 = &M.Q2[e * nn];
+  const double* Q3 = &M.Q3[e * nn];
+  const double* Q4 = &M.Q4[e * nn];
+  const double hcon = lambda2 + betak2;
+  for (int k = 0; k < nn * nn; ++k) H[k] = 0.0;
+  // row (i,j), column (m,n) -- HelmholtzRow (src/element.cpp:1443-1480)
+  for (int i = 0; i < n; ++i)
+    for (int j = 0; j < n; ++j) {
+      double* row = H + (i * n + j) * nn;
+      for (int c = 0; c < n; ++c) {
+        double s = 0;
+        for (int q = 0; q < n; ++q) s += Q1[i * n + q] * D[q * n + j] * D[q * n + c];
+        row[i * n + c] += s;
+      }
+      for (int m = 0; m < n; ++m) {
+        double s = 0;
+        for (int p = 0; p < n; ++p) s += Q2[p * n + j] * D[p * n + i] * D[p * n + m];
+        row[m * n + j] += s;
+      }
+      for (int m = 0; m < n; ++m)
+        for (int c = 0; c < n; ++c) {
+          row[m * n + c] += Q3[i * n + c] * D[c * n + j] * D[i * n + m];
+          row[m * n + c] += Q3[m * n + j] * D[j * n + c] * D[m * n + i];
+        }
+      row[i * n + j] += Q4[i * n + j] * hcon;
+    }
+}
+
+ModeSystem build_mode_system(const Mesh& M, const Numbering& N, double lambda2,
+                             double betak2, int method) {
+  ModeSystem S;
+  S.lambda2 = lambda2;
+  S.betak2 = betak2;
+  S.method = method;
+  S.nglobal = N.nglobal;
+  S.singular = (lambda2 + betak2) < kEpsSP && N.nglobal == N.nsolve;
+  S.nsolve = S.singular ? N.nsolve - 1 : N.nsolve;
+  S.nband = N.nband;
+  const int nn = M.npnp, next = M.next, nint = M.nint, nel = M.nel;
+  std::vector<double> H(static_cast<size_t>(nn) * nn);
+
+  if (method == kJacPCG) {
+    S.pc.assign(N.nglobal + static_cast<size_t>(nel) * nint, 0.0);
+    for (int e = 0; e < nel; ++e) {
+      element_helmholtz(M, e, lambda2, betak2, H.data());
+      for (int i = 0; i < next; ++i)
+        S.pc[N.btog[e * next + i]] += H[static_cast<size_t>(M.emap[i]) * nn + M.emap[i]];
+      for (int i = 0; i < nint; ++i) {
+        const int r = M.emap[next + i];
+        S.pc[N.nglobal + static_cast<size_t>(e) * nint + i] = H[static_cast<size_t>(r) * nn + r];
+      }
+    }
+    for (auto& v : S.pc) v = 1.0 / v;
+    return S;
+  }
+
+  // -- per-family static condensation (Element::HelmholtzSC)
+  const int nf = M.nfamily;
+  S.hbi.assign(static_cast<size_t>(nf) * next * nint, 0.0);
+  S.hii.assign(static_cast<size_t>(nf) * nint * nint, 0.0);
+  std::vector<double> hbb_all(static_cast<size_t>(nf) * next * next);
+  for (int f = 0; f < nf; ++f) {
+    element_helmholtz(M, M.family_rep[f], lambda2, betak2, H.data());
+    double* hbb = &hbb_all[static_cast<size_t>(f) * next * next];
+    double* hbi = &S.hbi[static_cast<size_t>(f) * next * nint];
+    double* hii = &S.hii[static_cast<size_t>(f) * nint * nint];
+    std::vector<double> bi(static_cast<size_t>(next) * nint);
+    for (int a = 0; a < next; ++a)
+      for (int b = 0; b < next; ++b)
+        hbb[a * next + b] = H[static_cast<size_t>(M.emap[a]) * nn + M.emap[b]];
+    for (int a = 0; a < next; ++a)
+      for (int b = 0; b < nint; ++b)
+        bi[static_cast<size_t>(a) * nint + b] = H[static_cast<size_t>(M.emap[a]) * nn + M.emap[next + b]];
+    for (int a = 0; a < nint; ++a)
+      for (int b = 0; b < nint; ++b)
+        hii[a * nint + b] = H[static_cast<size_t>(M.emap[next + a]) * nn + M.emap[next + b]];
+    if (nint) {
+      invert(nint, hii);
+      for (int a = 0; a < next; ++a)
+        for (int b = 0; b < nint; ++b) {
+          double s = 0;
+          for (int k = 0; k < nint; ++k) s += bi[static_cast<size_t>(a) * nint + k] * hii[k * nint + b];
+          hbi[static_cast<size_t>(a) * nint + b] = s;
+        }
+      for (int a = 0; a < next; ++a)
+        for (int b = 0; b < next; ++b) {
+          double s = 0;
+          for (int k = 0; k < nint; ++k)
+            s += hbi[static_cast<size_t>(a) * nint + k] * bi[static_cast<size_t>(b) * nint + k];
+          hbb[a * next + b] -= s;
+        }
+    }
+  }
+
+  // -- banded assembly over the first nsolve global nodes (src/matrix.cpp:218-232)
+  const int ns = S.nsolve, nb = S.nband, kd = nb - 1;
+  std::vector<double> A(static_cast<size_t>(ns) * nb, 0.0);  // A[j*nb + t] = A(j-kd+t, j)
+  for (int e = 0; e < nel; ++e) {
+    const double* hbb = &hbb_all[static_cast<size_t>(M.family[e]) * next * next];
+    for (int a = 0; a < next; ++a) {
+      const int m = N.btog[e * next + a];
+      if (m >= ns) continue;
+      for (int b = 0; b < next; ++b) {
+        const int c = N.btog[e * next + b];
+        if (c < ns && c >= m) {
+          if (c - m > kd) throw std::runtime_error("numbering bandwidth exceeded");
+          A[static_cast<size_t>(c) * nb + kd - (c - m)] += hbb[a * next + b];
+        }
+      }
+    }
+  }
+  // -- banded Cholesky A = U^T U, U stored in place as columns (dpbtrf "U")
+  for (int j = 0; j < ns; ++j) {
+    double* cj = &A[static_cast<size_t>(j) * nb];
+    const int i0 = std::max(0, j - kd);
+    for (int i = i0; i < j; ++i) {
+      const double* ci = &A[static_cast<size_t>(i) * nb];
+      double s = cj[kd - (j - i)];
+      const int k0 = std::max(i0, i - kd);
+      for (int k = k0; k < i; ++k) s -= ci[kd - (i - k)] * cj[kd - (j - k)];
+      cj[kd - (j - i)] = s / ci[kd];
+    }
+    double d = cj[kd];
+    for (int k = i0; k < j; ++k) d -= cj[kd - (j - k)] * cj[kd - (j - k)];
+    if (!(d > 0.0))
+      throw std::runtime_error("failed to factor Helmholtz matrix (not positive definite)");
+    cj[kd] = std::sqrt(d);
+  }
+  S.fwd.assign(static_cast<size_t>(ns) * nb, 0.0);
+  S.bwd.assign(static_cast<size_t>(ns) * nb, 0.0);
+  for (int j = 0; j < ns; ++j)
+    for (int t = 0; t < nb; ++t) {
+      double v = A[static_cast<size_t>(j) * nb + t];
+      if (j - kd + t < 0) v = 0.0;
+      S.fwd[static_cast<size_t>(j) * nb + t] = (t == kd) ? 1.0 / v : v;
+    }
+  // bwd row r: entries U[i][i+kd-t] for i = ns-1-r, column c = i+kd-t
+  for (int r = 0; r < ns; ++r) {
+    const int i = ns - 1 - r;
+    for (int t = 0; t < nb; ++t) {
+      const int c = i + kd - t;
+      double v = 0.0;
+      if (c < ns) v = A[static_cast<size_t>(c) * nb + kd - (c - i)];
+      S.bwd[static_cast<size_t>(r) * nb + t] = (t == kd) ? 1.0 / v : v;
+    }
+  }
+  return S;
+}
+
+}  // namespace stx

@@ -1,0 +1,477 @@
+#include "mesh.hpp"
+
+#include <algorithm>
+#include <cmath>
+#include <map>
+#include <numeric>
+#include <queue>
+#include <stdexcept>
+
+namespace stx {
+
+namespace {
+constexpr double kEpsDP = 6.0e-14;  // veclib/cveclib.h:58
+
+void legendre(int n, double x, double& pn, double& pn1) {
+  double p0 = 1.0, p1 = x;
+  if (n == 0) {
+    pn = 1.0;
+    pn1 = 0.0;
+    return;
+  }
+  for (int k = 2; k <= n; ++k) {
+    double p2 = ((2 * k - 1) * x * p1 - (k - 1) * p0) / k;
+    p0 = p1;
+    p1 = p2;
+  }
+  pn = p1;
+  pn1 = p0;
+}
+}  // namespace
+
+Quadrature gll(int np) {
+  if (np < 2) throw std::runtime_error("need > 2 knots for element edges");
+  Quadrature Q;
+  Q.np = np;
+  const int N = np - 1;
+  Q.z.resize(np);
+  Q.w.resize(np);
+  Q.D.assign(np * np, 0.0);
+  // Lobatto nodes: Newton iteration on (x P_N - P_{N-1}) from the
+  // Chebyshev--Gauss--Lobatto points (roots of (1-x^2) P_N'(x)).
+  for (int j = 0; j < np; ++j) {
+    double x = -std::cos(M_PI * j / N);
+    for (int it = 0; it < 100; ++it) {
+      double pn, pn1;
+      legendre(N, x, pn, pn1);
+      double dx = (x * pn - pn1) / (np * pn);
+      x -= dx;
+      if (std::fabs(dx) < 1e-17) break;
+    }
+    Q.z[j] = x;
+  }
+  Q.z[0] = -1.0;
+  Q.z[N] = 1.0;
+  std::vector<double> PN(np);
+  for (int j = 0; j < np; ++j) {
+    double pn, pn1;
+    legendre(N, Q.z[j], pn, pn1);
+    PN[j] = pn;
+    Q.w[j] = 2.0 / (N * (N + 1) * pn * pn);
+  }
+  for (int i = 0; i < np; ++i)
+    for (int j = 0; j < np; ++j)
+      if (i != j) Q.D[i * np + j] = PN[i] / (PN[j] * (Q.z[i] - Q.z[j]));
+  Q.D[0] = -N * (N + 1) / 4.0;
+  Q.D[N * np + N] = N * (N + 1) / 4.0;
+  return Q;
+}
+
+void Mesh::side_nodes(int s, int* idx) const {
+  const int n = np;
+  for (int t = 0; t < n; ++t) {
+    switch (s) {
+      case 0: idx[t] = t; break;
+      case 1: idx[t] = t * n + n - 1; break;
+      case 2: idx[t] = (n - 1) * n + (n - 1 - t); break;
+      default: idx[t] = (n - 1 - t) * n; break;
+    }
+  }
+}
+
+Mesh build_mesh(const Session& S) {
+  if (S.has_curves) throw std::runtime_error("curved element sides are not supported");
+  Mesh M;
+  M.np = S.tokens.ivalue("N_P");
+  M.nz = S.tokens.ivalue("N_Z");
+  if (M.nz > 1 && (M.nz & 1)) throw std::runtime_error("N_Z must be even");
+  M.nel = static_cast<int>(S.elements.size());
+  if (M.nel < 1) throw std::runtime_error("at least 1 element needed");
+  const int n = M.np, nel = M.nel;
+  M.npnp = n * n;
+  M.next = 4 * (n - 1);
+  M.nint = (n - 2) * (n - 2);
+  M.nplane = nel * M.npnp;
+  M.plane_size = M.nplane + (M.nplane % 2);  // src/geometry.cpp:105-108
+  M.q = gll(n);
+  const auto& z = M.q.z;
+  const auto& w = M.q.w;
+  const auto& D = M.q.D;
+
+  // -- boundary-major traverse (femlib/mapping.c:97-115)
+  M.emap.resize(M.npnp);
+  M.pmap.resize(M.npnp);
+  {
+    int k = 0, v = 0;
+    M.emap[0] = 0;
+    for (int i = 1; i < n; ++i) M.emap[++k] = v += 1;
+    for (int i = 1; i < n; ++i) M.emap[++k] = v += n;
+    for (int i = 1; i < n; ++i) M.emap[++k] = v -= 1;
+    for (int i = 1; i < n - 1; ++i) M.emap[++k] = v -= n;
+    ++k;
+    for (int i = 1; i < n - 1; ++i)
+      for (int j = 1; j < n - 1; ++j) M.emap[k++] = i * n + j;
+    for (int i = 0; i < M.npnp; ++i) M.pmap[M.emap[i]] = i;
+  }
+
+  // -- node locations: bilinear (Coons patch of straight sides)
+  const double xs = S.tokens.value("X_SHIFT"), ys = S.tokens.value("Y_SHIFT");
+  const double xc = S.tokens.value("X_SCALE"), yc = S.tokens.value("Y_SCALE");
+  M.x.resize(M.nplane);
+  M.y.resize(M.nplane);
+  for (int e = 0; e < nel; ++e) {
+    const auto& v = S.elements[e];
+    double P[4][2];
+    for (int c = 0; c < 4; ++c) {
+      P[c][0] = S.nodes[v[c]][0];
+      P[c][1] = S.nodes[v[c]][1];
+    }
+    for (int i = 0; i < n; ++i)
+      for (int j = 0; j < n; ++j) {
+        const double r = z[j], s = z[i];
+        const double a = (1 - r) * (1 - s), b = (1 + r) * (1 - s), c = (1 + r) * (1 + s),
+                     d = (1 - r) * (1 + s);
+        double X = 0.25 * (a * P[0][0] + b * P[1][0] + c * P[2][0] + d * P[3][0]);
+        double Y = 0.25 * (a * P[0][1] + b * P[1][1] + c * P[2][1] + d * P[3][1]);
+        if (std::fabs(xs) > kEpsDP) X += xs;
+        if (std::fabs(ys) > kEpsDP) Y += ys;
+        if (std::fabs(xc - 1.0) > kEpsDP) X *= xc;
+        if (std::fabs(yc - 1.0) > kEpsDP) Y *= yc;
+        M.x[e * M.npnp + i * n + j] = X;
+        M.y[e * M.npnp + i * n + j] = Y;
+      }
+  }
+
+  // -- geometric factors (src/element.cpp:1307-1407)
+  for (auto* v : {&M.Q1, &M.Q2, &M.Q3, &M.Q4, &M.drdx, &M.drdy, &M.dsdx, &M.dsdy})
+    v->assign(M.nplane, 0.0);
+  for (int e = 0; e < nel; ++e) {
+    const double* X = &M.x[e * M.npnp];
+    const double* Y = &M.y[e * M.npnp];
+    for (int i = 0; i < n; ++i)
+      for (int j = 0; j < n; ++j) {
+        double xr = 0, xs_ = 0, yr = 0, ys_ = 0;
+        for (int k = 0; k < n; ++k) {
+          xr += X[i * n + k] * D[j * n + k];
+          yr += Y[i * n + k] * D[j * n + k];
+          xs_ += D[i * n + k] * X[k * n + j];
+          ys_ += D[i * n + k] * Y[k * n + j];
+        }
+        const double jac = xr * ys_ - xs_ * yr;
+        if (jac < 4 * kEpsDP)
+          throw std::runtime_error("Jacobian of element " + std::to_string(e + 1) + " nonpositive");
+        const double WW = w[i] * w[j];
+        const int ij = e * M.npnp + i * n + j;
+        M.Q1[ij] = (xs_ * xs_ + ys_ * ys_) / jac * WW;
+        M.Q2[ij] = (xr * xr + yr * yr) / jac * WW;
+        M.Q3[ij] = (-yr * ys_ - xr * xs_) / jac * WW;
+        M.Q4[ij] = jac * WW;
+        M.drdx[ij] = ys_ / jac;
+        M.drdy[ij] = -xs_ / jac;
+        M.dsdx[ij] = -yr / jac;
+        M.dsdy[ij] = xr / jac;
+      }
+    // null-mapping: vectors below 4*EPSDP in 2-norm are exactly zero
+    for (auto* v : {&M.drdx, &M.drdy, &M.dsdx, &M.dsdy, &M.Q3}) {
+      double s = 0;
+      for (int k = 0; k < M.npnp; ++k) s += (*v)[e * M.npnp + k] * (*v)[e * M.npnp + k];
+      if (std::sqrt(s) < 4 * kEpsDP)
+        std::fill(v->begin() + e * M.npnp, v->begin() + (e + 1) * M.npnp, 0.0);
+    }
+  }
+
+  // -- side connectivity: shared vertex pairs, then <P> periodic mates
+  M.mate.assign(nel * 4, {-1, -1});
+  M.group.assign(nel * 4, 0);
+  std::map<std::pair<int, int>, std::vector<int>> sides;
+  for (int e = 0; e < nel; ++e)
+    for (int s = 0; s < 4; ++s)
+      sides[{S.elements[e][s], S.elements[e][(s + 1) % 4]}].push_back(e * 4 + s);
+  for (int e = 0; e < nel; ++e)
+    for (int s = 0; s < 4; ++s) {
+      auto it = sides.find({S.elements[e][(s + 1) % 4], S.elements[e][s]});
+      if (it != sides.end()) {
+        int o = it->second.front();
+        M.mate[e * 4 + s] = {o / 4, o % 4};
+      }
+    }
+  for (const auto& sf : S.surfaces) {
+    if (sf.elmt < 0 || sf.elmt >= nel || sf.side < 0 || sf.side > 3)
+      throw std::runtime_error("surface element/side out of range");
+    if (sf.kind == 'B') {
+      M.group[sf.elmt * 4 + sf.side] = sf.group;
+    } else {
+      if (sf.mate_elmt < 0 || sf.mate_elmt >= nel || sf.mate_side < 0 || sf.mate_side > 3)
+        throw std::runtime_error("periodic mate out of range");
+      M.mate[sf.elmt * 4 + sf.side] = {sf.mate_elmt, sf.mate_side};
+      M.mate[sf.mate_elmt * 4 + sf.mate_side] = {sf.elmt, sf.side};
+    }
+  }
+
+  // -- geometry families: elements whose Q1..Q4 agree to EPSDP share
+  //    condensed matrices (the role of Family::adopt, femlib/family.c:185).
+  M.family.assign(nel, -1);
+  for (int e = 0; e < nel; ++e) {
+    for (int f = 0; f < M.nfamily && M.family[e] < 0; ++f) {
+      const int r = M.family_rep[f];
+      bool same = true;
+      for (const auto* v : {&M.Q1, &M.Q2, &M.Q3, &M.Q4}) {
+        for (int k = 0; k < M.npnp && same; ++k)
+          same = std::fabs((*v)[e * M.npnp + k] - (*v)[r * M.npnp + k]) <= kEpsDP;
+        if (!same) break;
+      }
+      if (same) M.family[e] = f;
+    }
+    if (M.family[e] < 0) {
+      M.family[e] = M.nfamily++;
+      M.family_rep.push_back(e);
+    }
+  }
+  return M;
+}
+
+namespace {
+
+// Reverse Cuthill--McKee from `root` over a symmetric adjacency (CSR).
+void rcm_from(int root, const std::vector<int>& xadj, const std::vector<int>& adj,
+              const std::vector<int>& deg, std::vector<int>& order, std::vector<char>& seen) {
+  std::queue<int> Qu;
+  Qu.push(root);
+  seen[root] = 1;
+  std::vector<int> nb;
+  while (!Qu.empty()) {
+    int v = Qu.front();
+    Qu.pop();
+    order.push_back(v);
+    nb.clear();
+    for (int k = xadj[v]; k < xadj[v + 1]; ++k)
+      if (!seen[adj[k]]) {
+        nb.push_back(adj[k]);
+        seen[adj[k]] = 1;
+      }
+    std::sort(nb.begin(), nb.end(), [&](int a, int b) { return deg[a] < deg[b] || (deg[a] == deg[b] && a < b); });
+    for (int u : nb) Qu.push(u);
+  }
+}
+
+int bfs_far(int root, const std::vector<int>& xadj, const std::vector<int>& adj,
+            const std::vector<int>& deg, int& depth) {
+  const int n = static_cast<int>(deg.size());
+  std::vector<int> lev(n, -1);
+  std::queue<int> Qu;
+  Qu.push(root);
+  lev[root] = 0;
+  int last = root;
+  while (!Qu.empty()) {
+    int v = Qu.front();
+    Qu.pop();
+    if (lev[v] > lev[last] || (lev[v] == lev[last] && deg[v] < deg[last])) last = v;
+    for (int k = xadj[v]; k < xadj[v + 1]; ++k)
+      if (lev[adj[k]] < 0) {
+        lev[adj[k]] = lev[v] + 1;
+        Qu.push(adj[k]);
+      }
+  }
+  depth = lev[last];
+  return last;
+}
+
+}  // namespace
+
+Numbering build_numbering(const Session& S, const Mesh& M, char field, int rcm_roots) {
+  const int n = M.np, nel = M.nel, nm = n - 1, next = M.next;
+  Numbering N;
+  N.field = field;
+  // -- vertex identification: union of periodic vertex pairs
+  std::vector<int> parent(S.nodes.size());
+  std::iota(parent.begin(), parent.end(), 0);
+  auto find = [&](int a) {
+    while (parent[a] != a) a = parent[a] = parent[parent[a]];
+    return a;
+  };
+  for (int e = 0; e < nel; ++e)
+    for (int s = 0; s < 4; ++s) {
+      auto m = M.mate[e * 4 + s];
+      if (m[0] < 0) continue;
+      int a = S.elements[e][s], b = S.elements[e][(s + 1) % 4];
+      int c = S.elements[m[0]][m[1]], d = S.elements[m[0]][(m[1] + 1) % 4];
+      for (auto pr : {std::make_pair(a, d), std::make_pair(b, c)}) {
+        int ru = find(pr.first), rv = find(pr.second);
+        if (ru != rv) parent[std::max(ru, rv)] = std::min(ru, rv);
+      }
+    }
+  std::vector<int> gid(nel * next, -1);
+  std::map<int, int> vid;
+  int nxt = 0;
+  for (int e = 0; e < nel; ++e)
+    for (int s = 0; s < 4; ++s) {
+      int r = find(S.elements[e][s]);
+      auto it = vid.find(r);
+      if (it == vid.end()) it = vid.emplace(r, nxt++).first;
+      gid[e * next + s * nm] = it->second;
+    }
+  std::vector<int> edge_first(nel * 4, -1);
+  for (int e = 0; e < nel; ++e)
+    for (int s = 0; s < 4; ++s) {
+      const int es = e * 4 + s;
+      int base;
+      bool reversed = false;
+      auto m = M.mate[es];
+      if (edge_first[es] >= 0) {
+        base = edge_first[es];
+        reversed = true;
+      } else {
+        base = nxt;
+        nxt += nm - 1;
+        if (m[0] >= 0) edge_first[m[0] * 4 + m[1]] = base;
+      }
+      for (int t = 1; t < nm; ++t)
+        gid[e * next + s * nm + t] = reversed ? base + (nm - 1 - t) : base + (t - 1);
+    }
+  const int nglobal = nxt;
+  // -- essential nodes (Mesh::buildMask semantics, src/mesh.cpp:1226-1326),
+  //    applied to every copy of a global node.
+  std::vector<char> ess(nglobal, 0);
+  for (int e = 0; e < nel; ++e)
+    for (int s = 0; s < 4; ++s) {
+      const int es = e * 4 + s;
+      if (M.mate[es][0] >= 0) continue;
+      char g = M.group[es];
+      if (!g) continue;
+      auto gi = S.bcs.find(g);
+      if (gi == S.bcs.end()) throw std::runtime_error(std::string("no BCs for group ") + g);
+      auto bi = gi->second.find(field);
+      if (bi == gi->second.end())
+        throw std::runtime_error(std::string("no BC for field ") + field + " in group " + g);
+      const BCSpec& bc = bi->second;
+      if (bc.kind == 'D') {
+        for (int t = 0; t <= nm; ++t) ess[gid[e * next + (s * nm + t) % next]] = 1;
+      } else if (bc.kind != 'N') {
+        throw std::runtime_error(std::string("boundary condition kind <") + bc.kind +
+                                 "> is not supported");
+      }
+      BoundaryEdge E;
+      E.elmt = e;
+      E.side = s;
+      E.kind = bc.kind;
+      E.expr = bc.expr;
+      std::vector<int> idx(n);
+      M.side_nodes(s, idx.data());
+      E.x.resize(n);
+      E.y.resize(n);
+      for (int t = 0; t < n; ++t) {
+        E.x[t] = M.x[e * M.npnp + idx[t]];
+        E.y[t] = M.y[e * M.npnp + idx[t]];
+      }
+      const double L = std::hypot(E.x[n - 1] - E.x[0], E.y[n - 1] - E.y[0]);
+      E.area.resize(n);
+      for (int t = 0; t < n; ++t) E.area[t] = 0.5 * L * M.q.w[t];
+      N.edges.push_back(E);
+    }
+  // -- solve nodes first, RCM-ordered; essential nodes last
+  std::vector<int> loc(nglobal, -1), solve_nodes;
+  for (int g = 0; g < nglobal; ++g)
+    if (!ess[g]) {
+      loc[g] = static_cast<int>(solve_nodes.size());
+      solve_nodes.push_back(g);
+    }
+  const int ns = static_cast<int>(solve_nodes.size());
+  std::vector<int> order;
+  if (ns > 1) {
+    std::vector<std::vector<int>> nbr(ns);
+    for (int e = 0; e < nel; ++e) {
+      std::vector<int> v;
+      for (int i = 0; i < next; ++i)
+        if (loc[gid[e * next + i]] >= 0) v.push_back(loc[gid[e * next + i]]);
+      std::sort(v.begin(), v.end());
+      v.erase(std::unique(v.begin(), v.end()), v.end());
+      for (int a : v)
+        for (int b : v)
+          if (a != b) nbr[a].push_back(b);
+    }
+    std::vector<int> xadj(ns + 1, 0), adj, deg(ns);
+    for (int a = 0; a < ns; ++a) {
+      auto& v = nbr[a];
+      std::sort(v.begin(), v.end());
+      v.erase(std::unique(v.begin(), v.end()), v.end());
+      deg[a] = static_cast<int>(v.size());
+      xadj[a + 1] = xadj[a] + deg[a];
+      adj.insert(adj.end(), v.begin(), v.end());
+    }
+    // candidate roots: pseudo-peripheral node of each component plus a spread
+    std::vector<int> cand;
+    {
+      int depth = 0;
+      int r = bfs_far(0, xadj, adj, deg, depth);
+      for (int it = 0; it < 4; ++it) {
+        int d2 = 0;
+        int r2 = bfs_far(r, xadj, adj, deg, d2);
+        if (d2 <= depth) break;
+        depth = d2;
+        r = r2;
+      }
+      cand.push_back(r);
+      for (int k = 1; k < rcm_roots; ++k) cand.push_back(static_cast<int>((static_cast<long>(k) * ns) / rcm_roots));
+    }
+    auto bandwidth = [&](const std::vector<int>& ord) {
+      std::vector<int> pos(ns);
+      for (int k = 0; k < ns; ++k) pos[ord[ns - 1 - k]] = k;  // reversed
+      int bw = 0;
+      for (int a = 0; a < ns; ++a)
+        for (int k = xadj[a]; k < xadj[a + 1]; ++k) bw = std::max(bw, std::abs(pos[a] - pos[adj[k]]));
+      return bw;
+    };
+    int best_bw = -1;
+    for (int root : cand) {
+      std::vector<int> ord;
+      std::vector<char> seen(ns, 0);
+      rcm_from(root, xadj, adj, deg, ord, seen);
+      for (int a = 0; a < ns; ++a)
+        if (!seen[a]) rcm_from(a, xadj, adj, deg, ord, seen);
+      int bw = bandwidth(ord);
+      if (best_bw < 0 || bw < best_bw) {
+        best_bw = bw;
+        order.assign(ord.rbegin(), ord.rend());
+      }
+    }
+  } else if (ns == 1) {
+    order.push_back(0);
+  }
+  std::vector<int> newid(nglobal);
+  for (int k = 0; k < ns; ++k) newid[solve_nodes[order[k]]] = k;
+  int ne = ns;
+  for (int g = 0; g < nglobal; ++g)
+    if (ess[g]) newid[g] = ne++;
+  N.nglobal = nglobal;
+  N.nsolve = ns;
+  N.btog.resize(nel * next);
+  N.bmask.resize(nel * next);
+  N.emask.assign(nel, 0);
+  for (int k = 0; k < nel * next; ++k) {
+    N.btog[k] = newid[gid[k]];
+    N.bmask[k] = ess[gid[k]];
+    if (N.bmask[k]) N.emask[k / next] = 1;
+  }
+  int bw = 0;
+  for (int e = 0; e < nel; ++e) {
+    int lo = nglobal, hi = -1;
+    for (int i = 0; i < next; ++i) {
+      int g = N.btog[e * next + i];
+      if (g < ns) {
+        lo = std::min(lo, g);
+        hi = std::max(hi, g);
+      }
+    }
+    if (hi >= 0) bw = std::max(bw, hi - lo);
+  }
+  N.nband = bw + 1;
+  // -- inverse boundary mass (src/bcmgr.cpp:813-825)
+  N.imass.assign(nglobal, 0.0);
+  for (int e = 0; e < nel; ++e)
+    for (int i = 0; i < next; ++i)
+      N.imass[N.btog[e * next + i]] += M.Q4[e * M.npnp + M.emap[i]];
+  for (auto& v : N.imass) v = 1.0 / v;
+  return N;
+}
+
+}  // namespace stx

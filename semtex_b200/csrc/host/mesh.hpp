@@ -1,0 +1,71 @@
+// Spectral-element mesh, geometry and global numbering (host-side setup).
+//
+// Element node placement follows Mesh::meshElmt (src/mesh.cpp:767-882),
+// straight sides with a Coons patch; geometric factors follow
+// Element::mapping (src/element.cpp:1253-1408); GLL operators restate
+// femlib/polylib.c:312-575; the boundary-major element traverse restates
+// femlib/mapping.c:46-132.  Numbering plays the role of the `.num`
+// NumberSys (src/numbersys.h, src/bcmgr.cpp:586-826): btog, bmask, emask,
+// nglobal / nsolve / nband and the inverse boundary mass (imass).  The
+// ordering is this library's own reverse Cuthill--McKee.
+#pragma once
+
+#include <array>
+#include <string>
+#include <vector>
+
+#include "session.hpp"
+
+namespace stx {
+
+struct Quadrature {
+  int np = 0;
+  std::vector<double> z, w, D;  // D[i*np+j] = h_j'(z_i), row-major
+};
+Quadrature gll(int np);
+
+struct Mesh {
+  int np = 0, nel = 0, nz = 1;
+  int npnp = 0, next = 0, nint = 0;
+  int nplane = 0, plane_size = 0;   // nel*np*np and its even round-up
+  Quadrature q;
+  std::vector<int> emap, pmap;      // boundary-major permutation and inverse
+  std::vector<double> x, y;         // [nel*npnp] node locations
+  std::vector<double> Q1, Q2, Q3, Q4, drdx, drdy, dsdx, dsdy;  // [nel*npnp]
+  std::vector<std::array<int, 2>> mate;  // [nel*4] (elmt, side) or (-1,-1)
+  std::vector<char> group;               // [nel*4] boundary group or 0
+  std::vector<int> family;               // element -> geometry family
+  std::vector<int> family_rep;           // family -> representative element
+  int nfamily = 0;
+
+  // Row-major node indices of side s in CCW traverse (src/element.h:162-170).
+  void side_nodes(int s, int* idx) const;
+};
+
+Mesh build_mesh(const Session& S);
+
+struct BoundaryEdge {
+  int elmt = 0, side = 0;
+  char kind = 0;              // 'D' or 'N' (others rejected)
+  std::string expr;
+  std::vector<double> area;   // np quadrature-weighted side lengths
+  std::vector<double> x, y;   // np node locations along the side
+};
+
+struct Numbering {
+  char field = 0;
+  int nglobal = 0, nsolve = 0, nband = 0;
+  std::vector<int> btog, bmask;  // [nel*next]
+  std::vector<int> emask;        // [nel]
+  std::vector<double> imass;     // [nglobal]
+  std::vector<BoundaryEdge> edges;
+  bool same_as(const Numbering& o) const {
+    return nglobal == o.nglobal && nsolve == o.nsolve && btog == o.btog;
+  }
+};
+
+// rcm_roots: number of trial roots for the reverse Cuthill--McKee search
+// (the role of enumerate's optimisation levels, utility/enumerate.cpp:706-832).
+Numbering build_numbering(const Session& S, const Mesh& M, char field, int rcm_roots = 48);
+
+}  // namespace stx

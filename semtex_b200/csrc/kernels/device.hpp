@@ -1,0 +1,57 @@
+// Device-resident data shared by the hot-path kernels.
+//
+// Field storage keeps the reference plane layout (src/auxfield.cpp:45-68,
+// src/geometry.cpp:105-108): data[k*plane_size + e*np*np + i*np + j], i = s
+// row, j = r column; in Fourier space plane 0 = Re mode 0, plane 1 = Nyquist,
+// planes 2m / 2m+1 = Re / Im of mode m (femlib/fourier.c:56-63).
+#pragma once
+
+#include <cuda_runtime.h>
+#include <cstdint>
+
+namespace stx {
+
+struct DevGeom {
+  int np, nel, nz, npnp, next, nint, plane_size;
+  const double* D;      // [np*np] derivative matrix
+  const double* Q1;     // [nel*npnp] geometric factors
+  const double* Q2;
+  const double* Q3;
+  const double* Q4;
+  const double* drdx;
+  const double* drdy;
+  const double* dsdx;
+  const double* dsdy;
+  const int* emap;      // [npnp] boundary-major traverse
+  const int* pmap;      // [npnp] inverse of emap
+  const int* family;    // [nel] geometry family
+};
+
+struct DevNumbering {
+  int nglobal, nsolve, nband;
+  const int* btog;      // [nel*next]
+  const int* bmask;     // [nel*next]
+  const int* emask;     // [nel]
+  const double* imass;  // [nglobal]
+  int nedge;            // boundary edges with a BC
+  const int* edge_gid;  // [nedge*np] global id of each edge node
+  const int* edge_kind; // [nedge]  'D' or 'N'
+  const double* edge_area;  // [nedge*np]
+};
+
+// A ModalMatrixSys on the device: one MatrixSys per locally held mode.
+struct DevModal {
+  int nmodes, method, nfamily;
+  int nband, ns_stride;           // band width, row stride between modes' factors
+  const double* lambda2;          // [nmodes]
+  const double* betak2;           // [nmodes]
+  const int* nsolve;              // [nmodes]
+  const double* hbi;              // [nmodes][nfamily][next][nint]
+  const double* hii;              // [nmodes][nfamily][nint][nint]
+  const double* fwd;              // [nmodes][ns_stride][nband]
+  const double* bwd;              // [nmodes][ns_stride][nband]
+  const double* pc;               // JACPCG: [nmodes][npts]
+  int npts;
+};
+
+}  // namespace stx

@@ -1,0 +1,598 @@
+// Condensed direct Helmholtz solve for all Fourier planes of a field.
+//
+// Device restatement of Field::solve DIRECT (src/field.cpp:598-709):
+//   1. essential values g into a globally numbered vector per plane
+//      (Field::getEssential, src/field.cpp:1078-1103);
+//   2. per (element, plane): F = -(M f + H g) (Field::constrain,
+//      src/field.cpp:812-852), boundary-major gather, condensation
+//      F_b -= (h_bi h_ii^-1) F_i and direct-stiffness scatter-sum into the
+//      boundary RHS (Element::local2globalSumSC, src/element.cpp:326-365);
+//   3. natural-BC edge integrals <h, w> (Natural::sum, src/condition.cpp:192);
+//   4. banded Cholesky forward / backward solves per mode, Re and Im planes
+//      of a mode sharing one factor read (Lapack::pbtrs, src/field.cpp:693);
+//   5. per (element, plane): interior recovery u_i = h_ii^-1 F_i -
+//      (h_ii^-1 h_ib) u_b (Element::global2localSC, src/element.cpp:368-407)
+//      and imposition of essential values (Field::setEssential,
+//      src/field.cpp:1106-1124).
+#include "helmholtz.cuh"
+
+#include <algorithm>
+#include <vector>
+
+namespace stx {
+
+namespace {
+
+// Plane index k of a locally held mode m and RHS slot r (0 = Re, 1 = Im).
+__device__ __forceinline__ int plane_of(int m, int r) { return 2 * m + r; }
+
+// Constrained forcing -(Q4 f + [emask] H g) of element e in boundary-major
+// order, left in sF (length npnp).  Uses blockDim.x >= npnp.
+__device__ void constrained_forcing(const DevGeom& g, const DevNumbering& N,
+                                    const double* __restrict__ fplane,
+                                    const double* __restrict__ Gplane, double hcon,
+                                    int e, double* su, double* sR, double* sS,
+                                    double* sF, const double* sD) {
+  const int np = g.np, nn = g.npnp, t = threadIdx.x;
+  const int i = t / np, j = t - (t / np) * np;
+  double F = 0.0;
+  if (t < nn) F = g.Q4[e * nn + t] * fplane[e * nn + t];
+  if (N.emask && N.emask[e]) {
+    if (t < nn) su[t] = 0.0;
+    __syncthreads();
+    if (t < g.next) su[g.emap[t]] = Gplane[N.btog[e * g.next + t]];
+    __syncthreads();
+    double r = 0.0, s = 0.0;
+    if (t < nn) {
+      for (int k = 0; k < np; ++k) {
+        r += su[i * np + k] * sD[j * np + k];  // (u D^T)[i][j]
+        s += sD[i * np + k] * su[k * np + j];  // (D u)[i][j]
+      }
+      const double q1 = g.Q1[e * nn + t], q2 = g.Q2[e * nn + t], q3 = g.Q3[e * nn + t];
+      sR[t] = q1 * r + q3 * s;
+      sS[t] = q2 * s + q3 * r;
+    }
+    __syncthreads();
+    if (t < nn) {
+      double h = g.Q4[e * nn + t] * su[t] * hcon;
+      for (int k = 0; k < np; ++k) {
+        h += sD[k * np + i] * sS[k * np + j];  // D^T S'
+        h += sR[i * np + k] * sD[k * np + j];  // R' D
+      }
+      F += h;
+    }
+  }
+  if (t < nn) sF[g.pmap[t]] = -F;
+  __syncthreads();
+}
+
+__global__ void k_essential(DevGeom g, DevNumbering N, const double* __restrict__ lines,
+                            int nline, double* __restrict__ G, int gstride, int nz) {
+  const int idx = blockIdx.x * blockDim.x + threadIdx.x;
+  const int k = blockIdx.y;
+  if (k >= nz || idx >= N.nedge * g.np) return;
+  const int b = idx / g.np;
+  if (N.edge_kind[b] != 'D') return;
+  G[static_cast<size_t>(k) * gstride + N.edge_gid[idx]] = lines[static_cast<size_t>(k) * nline + idx];
+}
+
+__global__ void k_natural(DevGeom g, DevNumbering N, const double* __restrict__ lines,
+                          int nline, double* __restrict__ R, int rstride, int nz) {
+  const int idx = blockIdx.x * blockDim.x + threadIdx.x;
+  const int k = blockIdx.y;
+  if (k >= nz || (nz > 1 && k == 1) || idx >= N.nedge * g.np) return;
+  const int b = idx / g.np;
+  if (N.edge_kind[b] != 'N') return;
+  atomicAdd(&R[static_cast<size_t>(k) * rstride + N.edge_gid[idx]],
+            lines[static_cast<size_t>(k) * nline + idx] * N.edge_area[idx]);
+}
+
+__global__ void k_condense(DevGeom g, DevNumbering N, DevModal S,
+                           const double* __restrict__ F, const double* __restrict__ G,
+                           int gstride, double* __restrict__ R, int rstride) {
+  extern __shared__ double smem[];
+  const int nn = g.npnp;
+  double* sD = smem;
+  double* su = sD + g.np * g.np;
+  double* sR = su + nn;
+  double* sS = sR + nn;
+  double* sF = sS + nn;
+  const int e = blockIdx.x;
+  const int k = blockIdx.y;
+  if (g.nz > 1 && k == 1) return;  // Nyquist plane is never solved
+  const int m = k >> 1;
+  for (int t = threadIdx.x; t < g.np * g.np; t += blockDim.x) sD[t] = g.D[t];
+  __syncthreads();
+  constrained_forcing(g, N, F + static_cast<size_t>(k) * g.plane_size,
+                      G ? G + static_cast<size_t>(k) * gstride : nullptr,
+                      S.lambda2[m] + S.betak2[m], e, su, sR, sS, sF, sD);
+  const int t = threadIdx.x;
+  if (t < g.next) {
+    const double* hbi = S.hbi + (static_cast<size_t>(m) * S.nfamily + g.family[e]) * g.next * g.nint;
+    double v = sF[t];
+    const double* row = hbi + static_cast<size_t>(t) * g.nint;
+    for (int b = 0; b < g.nint; ++b) v -= row[b] * sF[g.next + b];
+    atomicAdd(&R[static_cast<size_t>(k) * rstride + N.btog[e * g.next + t]], v);
+  }
+}
+
+__global__ void k_recover(DevGeom g, DevNumbering N, DevModal S,
+                          const double* __restrict__ F, const double* __restrict__ G,
+                          int gstride, const double* __restrict__ R, int rstride,
+                          double* __restrict__ U) {
+  extern __shared__ double smem[];
+  const int nn = g.npnp;
+  double* sD = smem;
+  double* su = sD + g.np * g.np;
+  double* sR = su + nn;
+  double* sS = sR + nn;
+  double* sF = sS + nn;
+  double* sub = sF + nn;
+  const int e = blockIdx.x;
+  const int k = blockIdx.y;
+  if (g.nz > 1 && k == 1) return;
+  const int m = k >> 1;
+  for (int t = threadIdx.x; t < g.np * g.np; t += blockDim.x) sD[t] = g.D[t];
+  __syncthreads();
+  const double* Gp = G ? G + static_cast<size_t>(k) * gstride : nullptr;
+  constrained_forcing(g, N, F + static_cast<size_t>(k) * g.plane_size, Gp,
+                      S.lambda2[m] + S.betak2[m], e, su, sR, sS, sF, sD);
+  const int t = threadIdx.x;
+  const int nsolve = S.nsolve[m];
+  const double* Rp = R + static_cast<size_t>(k) * rstride;
+  double* Up = U + static_cast<size_t>(k) * g.plane_size + static_cast<size_t>(e) * nn;
+  if (t < g.next) {
+    const int gi = N.btog[e * g.next + t];
+    const double ub = gi < nsolve ? Rp[gi] : 0.0;
+    sub[t] = ub;
+    Up[g.emap[t]] = (N.bmask[e * g.next + t] && Gp) ? Gp[gi] : ub;
+  }
+  __syncthreads();
+  if (t < g.nint) {
+    const size_t fm = static_cast<size_t>(m) * S.nfamily + g.family[e];
+    const double* hii = S.hii + fm * g.nint * g.nint + static_cast<size_t>(t) * g.nint;
+    const double* hbi = S.hbi + fm * g.next * g.nint;
+    double v = 0.0;
+    for (int c = 0; c < g.nint; ++c) v += hii[c] * sF[g.next + c];
+    for (int a = 0; a < g.next; ++a) v -= hbi[static_cast<size_t>(a) * g.nint + t] * sub[a];
+    Up[g.emap[g.next + t]] = v;
+  }
+}
+
+// Banded lower-triangular solve L z = c, in place, for the planes of one mode
+// per block.  Row j of L is contiguous: L[j*nband + t] multiplies z[j-kd+t],
+// t = kd holds 1/L[j][j].  `reversed` addresses vector entry r at n-1-r.
+// Rows are processed in blocks of 32: all warps form the contributions of
+// already-solved columns, then warp 0 finishes the block's 32x32 triangle.
+__global__ void k_band_solve(DevModal S, const double* __restrict__ Lall,
+                             double* __restrict__ R, int rstride, int nz, int reversed) {
+  __shared__ double acc[32][2];
+  __shared__ double tri[32][33];
+  __shared__ double rdiag[32];
+  const int m = blockIdx.x;
+  const int n = S.nsolve[m];
+  const int nb = S.nband, kd = nb - 1;
+  const double* L = Lall + static_cast<size_t>(m) * S.ns_stride * nb;
+  const int nr = (nz > 1 && m > 0) ? 2 : 1;
+  double* z0 = R + static_cast<size_t>(plane_of(m, 0)) * rstride;
+  double* z1 = R + static_cast<size_t>(plane_of(m, 1)) * rstride;
+  const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31, nwarp = blockDim.x >> 5;
+  auto at = [&](int r) { return reversed ? n - 1 - r : r; };
+  for (int j0 = 0; j0 < n; j0 += 32) {
+    const int bn = min(32, n - j0);
+    for (int rr = warp; rr < bn; rr += nwarp) {
+      const int j = j0 + rr;
+      const double* Lj = L + static_cast<size_t>(j) * nb;
+      const int tlo = max(0, kd - j);
+      const int thi = kd - rr;  // columns < j0
+      double s0 = 0.0, s1 = 0.0;
+      for (int t = tlo + lane; t < thi; t += 32) {
+        const int c = at(j - kd + t);
+        const double l = Lj[t];
+        s0 += l * z0[c];
+        if (nr > 1) s1 += l * z1[c];
+      }
+      for (int o = 16; o; o >>= 1) {
+        s0 += __shfl_xor_sync(0xffffffffu, s0, o);
+        s1 += __shfl_xor_sync(0xffffffffu, s1, o);
+      }
+      if (lane == 0) {
+        acc[rr][0] = z0[at(j)] - s0;
+        acc[rr][1] = nr > 1 ? z1[at(j)] - s1 : 0.0;
+        rdiag[rr] = Lj[kd];
+      }
+      if (lane < rr) tri[rr][lane] = (rr - lane <= kd) ? Lj[kd - rr + lane] : 0.0;
+    }
+    __syncthreads();
+    if (warp == 0) {
+      double a0 = lane < bn ? acc[lane][0] : 0.0;
+      double a1 = lane < bn ? acc[lane][1] : 0.0;
+      for (int s = 0; s < bn; ++s) {
+        double y0 = a0 * rdiag[s], y1 = a1 * rdiag[s];
+        y0 = __shfl_sync(0xffffffffu, y0, s);
+        y1 = __shfl_sync(0xffffffffu, y1, s);
+        if (lane > s && lane < bn) {
+          const double l = tri[lane][s];
+          a0 -= l * y0;
+          a1 -= l * y1;
+        }
+        if (lane == s) {
+          z0[at(j0 + s)] = y0;
+          if (nr > 1) z1[at(j0 + s)] = y1;
+        }
+      }
+    }
+    __syncthreads();
+  }
+}
+
+
+// ---------------------------------------------------------------------------
+// Jacobi-PCG (Field::solve JACPCG, src/field.cpp:711-805): all planes iterate
+// in lockstep, each with its own scalars and stopping test, so every plane
+// takes exactly the iterations the reference loop takes for it.
+// Global vectors per plane: [0, nglobal) element-boundary nodes, then nel
+// blocks of nint interior nodes in boundary-major order.
+// ---------------------------------------------------------------------------
+
+struct PcgScalars {
+  double rho1, rho2, r2, eps, dotp;
+  int iter, active, hit_max, solved;
+};
+
+// y = H x (Field::HelmholtzOperator, src/field.cpp:855-940) per (element,
+// plane); y's boundary part must be zero on entry.
+__global__ void k_global_op(DevGeom g, DevNumbering N, DevModal S, const double* __restrict__ X,
+                            double* __restrict__ Y, int vstride, const PcgScalars* sc) {
+  extern __shared__ double smem[];
+  const int nn = g.npnp, np = g.np;
+  double* sD = smem;
+  double* su = sD + np * np;
+  double* sR = su + nn;
+  double* sS = sR + nn;
+  const int e = blockIdx.x, k = blockIdx.y, t = threadIdx.x;
+  if (!sc[k].active) return;
+  const int m = k >> 1;
+  const double hcon = S.lambda2[m] + S.betak2[m];
+  const double* x = X + static_cast<size_t>(k) * vstride;
+  double* y = Y + static_cast<size_t>(k) * vstride;
+  for (int q = t; q < np * np; q += blockDim.x) sD[q] = g.D[q];
+  if (t < g.next) su[g.emap[t]] = x[N.btog[e * g.next + t]];
+  if (t < g.nint) su[g.emap[g.next + t]] = x[N.nglobal + static_cast<size_t>(e) * g.nint + t];
+  __syncthreads();
+  const int i = t / np, j = t - (t / np) * np;
+  if (t < nn) {
+    double r = 0.0, s = 0.0;
+    for (int q = 0; q < np; ++q) {
+      r += su[i * np + q] * sD[j * np + q];
+      s += sD[i * np + q] * su[q * np + j];
+    }
+    const double q1 = g.Q1[e * nn + t], q2 = g.Q2[e * nn + t], q3 = g.Q3[e * nn + t];
+    sR[t] = q1 * r + q3 * s;
+    sS[t] = q2 * s + q3 * r;
+  }
+  __syncthreads();
+  if (t < nn) {
+    double h = g.Q4[e * nn + t] * su[t] * hcon;
+    for (int q = 0; q < np; ++q) {
+      h += sD[q * np + i] * sS[q * np + j];
+      h += sR[i * np + q] * sD[q * np + j];
+    }
+    const int b = g.pmap[t];
+    if (b < g.next)
+      atomicAdd(&y[N.btog[e * g.next + b]], h);
+    else
+      y[N.nglobal + static_cast<size_t>(e) * g.nint + (b - g.next)] = h;
+  }
+}
+
+// r = assembled constrained forcing (buildRHS without condensation).
+__global__ void k_pcg_rhs(DevGeom g, DevNumbering N, DevModal S, const double* __restrict__ F,
+                          const double* __restrict__ G, int gstride, double* __restrict__ Rv,
+                          int vstride) {
+  extern __shared__ double smem[];
+  const int nn = g.npnp;
+  double* sD = smem;
+  double* su = sD + g.np * g.np;
+  double* sR = su + nn;
+  double* sS = sR + nn;
+  double* sF = sS + nn;
+  const int e = blockIdx.x, k = blockIdx.y;
+  if (g.nz > 1 && k == 1) return;
+  const int m = k >> 1;
+  for (int t = threadIdx.x; t < g.np * g.np; t += blockDim.x) sD[t] = g.D[t];
+  __syncthreads();
+  constrained_forcing(g, N, F + static_cast<size_t>(k) * g.plane_size,
+                      G ? G + static_cast<size_t>(k) * gstride : nullptr,
+                      S.lambda2[m] + S.betak2[m], e, su, sR, sS, sF, sD);
+  const int t = threadIdx.x;
+  double* r = Rv + static_cast<size_t>(k) * vstride;
+  if (t < g.next) atomicAdd(&r[N.btog[e * g.next + t]], sF[t]);
+  if (t < g.nint) r[N.nglobal + static_cast<size_t>(e) * g.nint + t] = sF[g.next + t];
+}
+
+// x <- local2global(unknown) boundary + interior (Field::local2global).
+__global__ void k_local2global(DevGeom g, DevNumbering N, const double* __restrict__ U,
+                               double* __restrict__ X, int vstride) {
+  const int e = blockIdx.x, k = blockIdx.y, t = threadIdx.x;
+  if (g.nz > 1 && k == 1) return;
+  const double* u = U + static_cast<size_t>(k) * g.plane_size + static_cast<size_t>(e) * g.npnp;
+  double* x = X + static_cast<size_t>(k) * vstride;
+  if (t < g.next) x[N.btog[e * g.next + t]] = u[g.emap[t]];
+  if (t < g.nint) x[N.nglobal + static_cast<size_t>(e) * g.nint + t] = u[g.emap[g.next + t]];
+}
+
+// unknown <- global2local(x), essential values imposed from G.
+__global__ void k_global2local(DevGeom g, DevNumbering N, const double* __restrict__ X, int vstride,
+                               const double* __restrict__ G, int gstride, double* __restrict__ U) {
+  const int e = blockIdx.x, k = blockIdx.y, t = threadIdx.x;
+  if (g.nz > 1 && k == 1) return;
+  double* u = U + static_cast<size_t>(k) * g.plane_size + static_cast<size_t>(e) * g.npnp;
+  const double* x = X + static_cast<size_t>(k) * vstride;
+  if (t < g.next) {
+    const int gi = N.btog[e * g.next + t];
+    u[g.emap[t]] = (G && N.bmask[e * g.next + t]) ? G[static_cast<size_t>(k) * gstride + gi] : x[gi];
+  }
+  if (t < g.nint) u[g.emap[g.next + t]] = x[N.nglobal + static_cast<size_t>(e) * g.nint + t];
+}
+
+// Zero entries [lo, hi) of each plane's vector; lo = lo_mode[mode] if given.
+__global__ void k_zero_range(double* V, int vstride, int lo, const int* lo_mode, int hi, int nz) {
+  const int k = blockIdx.y;
+  if (k >= nz) return;
+  const int l = lo_mode ? lo_mode[k >> 1] : lo;
+  for (int i = l + blockIdx.x * blockDim.x + threadIdx.x; i < hi; i += gridDim.x * blockDim.x)
+    V[static_cast<size_t>(k) * vstride + i] = 0.0;
+}
+
+// out[k] += sum_i a[k][i] * b[k][i] over active (or all, if force) planes.
+__global__ void k_dot(const double* __restrict__ A, const double* __restrict__ B, int n, int vstride,
+                      double* out, const PcgScalars* sc, int force) {
+  const int k = blockIdx.y;
+  if (!force && !sc[k].active) return;
+  double s = 0.0;
+  const double* a = A + static_cast<size_t>(k) * vstride;
+  const double* b = B + static_cast<size_t>(k) * vstride;
+  for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) s += a[i] * b[i];
+  for (int o = 16; o; o >>= 1) s += __shfl_xor_sync(0xffffffffu, s, o);
+  __shared__ double ws[32];
+  if ((threadIdx.x & 31) == 0) ws[threadIdx.x >> 5] = s;
+  __syncthreads();
+  if (threadIdx.x < 32) {
+    s = threadIdx.x < (blockDim.x >> 5) ? ws[threadIdx.x] : 0.0;
+    for (int o = 16; o; o >>= 1) s += __shfl_xor_sync(0xffffffffu, s, o);
+    if (threadIdx.x == 0) atomicAdd(&out[k], s);
+  }
+}
+
+// r -= p on solved planes.
+__global__ void k_sub(double* __restrict__ R, const double* __restrict__ P, int n, int vstride,
+                      const PcgScalars* sc) {
+  const int k = blockIdx.y;
+  if (!sc[k].solved) return;
+  for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x)
+    R[static_cast<size_t>(k) * vstride + i] -= P[static_cast<size_t>(k) * vstride + i];
+}
+
+// Per-plane scalar bookkeeping.
+__global__ void k_pcg_init(PcgScalars* sc, const double* bb, const double* rr, double tol, int nz) {
+  const int k = threadIdx.x;
+  if (k >= nz) return;
+  PcgScalars s{};
+  const bool solved = !(nz > 1 && k == 1);
+  const double e = tol * sqrt(bb[k]);
+  s.eps = e * e;
+  s.r2 = rr[k];
+  s.iter = 0;
+  s.solved = solved;
+  s.active = solved ? 1 : 0;
+  s.hit_max = 0;
+  sc[k] = s;
+}
+
+// Loop head `while (r2 > epsb2 && ++i < StepMax)`.
+__global__ void k_pcg_head(PcgScalars* sc, int step_max, int nz, int* any_active) {
+  const int k = threadIdx.x;
+  if (k >= nz) return;
+  PcgScalars& s = sc[k];
+  if (s.active) {
+    if (s.r2 > s.eps) {
+      s.iter += 1;
+      if (s.iter >= step_max) {
+        s.active = 0;
+        s.hit_max = 1;
+      }
+    } else {
+      s.active = 0;
+    }
+  }
+  if (s.active) atomicOr(any_active, 1);
+}
+
+// z = PC r ; (after rho1 computed) p = z + beta p.
+__global__ void k_pcg_precond(const double* __restrict__ PC, int npts, const double* __restrict__ R,
+                              double* __restrict__ Z, int vstride, const PcgScalars* sc) {
+  const int k = blockIdx.y;
+  if (!sc[k].active) return;
+  const double* pc = PC + static_cast<size_t>(k >> 1) * npts;
+  for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < npts; i += gridDim.x * blockDim.x)
+    Z[static_cast<size_t>(k) * vstride + i] = pc[i] * R[static_cast<size_t>(k) * vstride + i];
+}
+
+__global__ void k_pcg_dir(const double* __restrict__ Z, double* __restrict__ P, int n, int vstride,
+                          PcgScalars* sc, const double* rho1) {
+  const int k = blockIdx.y;
+  if (!sc[k].active) return;
+  const double beta = sc[k].iter == 1 ? 0.0 : rho1[k] / sc[k].rho2;
+  for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
+    const size_t o = static_cast<size_t>(k) * vstride + i;
+    P[o] = sc[k].iter == 1 ? Z[o] : Z[o] + beta * P[o];
+  }
+}
+
+__global__ void k_pcg_step(double* __restrict__ X, double* __restrict__ R, const double* __restrict__ P,
+                           const double* __restrict__ Q, int n, int vstride, const PcgScalars* sc,
+                           const double* rho1, const double* dotp) {
+  const int k = blockIdx.y;
+  if (!sc[k].active) return;
+  const double alpha = rho1[k] / dotp[k];
+  for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
+    const size_t o = static_cast<size_t>(k) * vstride + i;
+    X[o] += alpha * P[o];
+    R[o] -= alpha * Q[o];
+  }
+}
+
+__global__ void k_pcg_tail(PcgScalars* sc, const double* rho1, const double* r2, int nz) {
+  const int k = threadIdx.x;
+  if (k >= nz || !sc[k].active) return;
+  sc[k].rho2 = rho1[k];
+  sc[k].r2 = r2[k];
+}
+
+}  // namespace
+
+size_t helmholtz_workspace_doubles(const DevGeom& g, const DevNumbering& N) {
+  const size_t stride = (static_cast<size_t>(N.nglobal) + 31) / 32 * 32;
+  return 2 * stride * g.nz;
+}
+
+cudaError_t helmholtz_direct_solve(const DevGeom& g, const DevNumbering& N, const DevModal& S,
+                                   const double* F, double* U, const double* lines, int nline,
+                                   double* work, cudaStream_t st) {
+  const int rstride = (N.nglobal + 31) / 32 * 32;
+  double* R = work;
+  double* G = work + static_cast<size_t>(rstride) * g.nz;
+  const int nz = g.nz;
+  cudaError_t err = cudaMemsetAsync(work, 0, sizeof(double) * 2 * static_cast<size_t>(rstride) * nz, st);
+  if (err != cudaSuccess) return err;
+  const bool has_ess = N.nglobal > N.nsolve;
+  const int nedge_nodes = N.nedge * g.np;
+  if (has_ess && nedge_nodes) {
+    dim3 grid((nedge_nodes + 127) / 128, nz);
+    k_essential<<<grid, 128, 0, st>>>(g, N, lines, nline, G, rstride, nz);
+  }
+  const int threads = ((g.npnp + 31) / 32) * 32 < 64 ? 64 : ((g.npnp + 31) / 32) * 32;
+  const size_t shm = sizeof(double) * (static_cast<size_t>(g.np) * g.np + 5 * g.npnp);
+  dim3 egrid(g.nel, nz);
+  k_condense<<<egrid, threads, shm, st>>>(g, N, S, F, has_ess ? G : nullptr, rstride, R, rstride);
+  if (nedge_nodes) {
+    dim3 grid((nedge_nodes + 127) / 128, nz);
+    k_natural<<<grid, 128, 0, st>>>(g, N, lines, nline, R, rstride, nz);
+  }
+  k_band_solve<<<S.nmodes, 256, 0, st>>>(S, S.fwd, R, rstride, nz, 0);
+  k_band_solve<<<S.nmodes, 256, 0, st>>>(S, S.bwd, R, rstride, nz, 1);
+  k_recover<<<egrid, threads, shm + sizeof(double) * g.next, st>>>(g, N, S, F, has_ess ? G : nullptr,
+                                                                   rstride, R, rstride, U);
+  return cudaGetLastError();
+}
+
+}  // namespace stx
+
+namespace stx {
+
+size_t jacpcg_workspace_doubles(const DevGeom& g, const DevNumbering& N) {
+  const size_t npts = static_cast<size_t>(N.nglobal) + static_cast<size_t>(g.nel) * g.nint;
+  const size_t vs = (npts + 31) / 32 * 32;
+  const size_t gs = (static_cast<size_t>(N.nglobal) + 31) / 32 * 32;
+  // 5 vectors + essential values + scalars (rho1, dotp, r2, bb, flag) + PcgScalars
+  return (5 * vs + gs) * g.nz + 8 * static_cast<size_t>(g.nz) + 8 * static_cast<size_t>(g.nz) + 64;
+}
+
+cudaError_t helmholtz_jacpcg_solve(const DevGeom& g, const DevNumbering& N, const DevModal& S,
+                                   const double* F, double* U, const double* lines, int nline,
+                                   double tol_rel, int step_max, double* work, int* iters,
+                                   cudaStream_t st) {
+  const int nz = g.nz;
+  const int npts = N.nglobal + g.nel * g.nint;
+  const int vs = (npts + 31) / 32 * 32;
+  const int gs = (N.nglobal + 31) / 32 * 32;
+  double* r = work;
+  double* p = r + static_cast<size_t>(vs) * nz;
+  double* q = p + static_cast<size_t>(vs) * nz;
+  double* x = q + static_cast<size_t>(vs) * nz;
+  double* z = x + static_cast<size_t>(vs) * nz;
+  double* G = z + static_cast<size_t>(vs) * nz;
+  double* scal = G + static_cast<size_t>(gs) * nz;   // 8*nz doubles
+  double* rho1 = scal;
+  double* dotp = scal + nz;
+  double* r2 = scal + 2 * nz;
+  double* bb = scal + 3 * nz;
+  int* flag = reinterpret_cast<int*>(scal + 4 * nz);
+  PcgScalars* sc = reinterpret_cast<PcgScalars*>(scal + 8 * nz);
+  const int nzero_lo = N.nsolve;
+  const int nzt = std::min(1024, (nz + 31) / 32 * 32);  // one thread per plane
+  cudaError_t err;
+  // The per-mode pinned node of a singular system moves nsolve down by one.
+  // S.nsolve is on the device; zero [nsolve_m, nglobal) per plane.
+  err = cudaMemsetAsync(work, 0, sizeof(double) * ((5 * static_cast<size_t>(vs) + gs) * nz + 8 * nz), st);
+  if (err != cudaSuccess) return err;
+  const bool has_ess = N.nglobal > N.nsolve;
+  const int nedge_nodes = N.nedge * g.np;
+  if (has_ess && nedge_nodes) {
+    dim3 grid((nedge_nodes + 127) / 128, nz);
+    k_essential<<<grid, 128, 0, st>>>(g, N, lines, nline, G, gs, nz);
+  }
+  const int threads = ((g.npnp + 31) / 32) * 32 < 64 ? 64 : ((g.npnp + 31) / 32) * 32;
+  const size_t shm = sizeof(double) * (static_cast<size_t>(g.np) * g.np + 5 * g.npnp);
+  dim3 egrid(g.nel, nz);
+  k_pcg_rhs<<<egrid, threads, shm, st>>>(g, N, S, F, has_ess ? G : nullptr, gs, r, vs);
+  if (nedge_nodes) {
+    dim3 grid((nedge_nodes + 127) / 128, nz);
+    k_natural<<<grid, 128, 0, st>>>(g, N, lines, nline, r, vs, nz);
+  }
+  const dim3 vgrid(std::min(1024, (npts + 255) / 256), nz);
+  const dim3 zgrid(std::max(1, std::min(64, (N.nglobal + 255) / 256)), nz);
+  k_zero_range<<<zgrid, 256, 0, st>>>(r, vs, nzero_lo, S.nsolve, N.nglobal, nz);
+  k_dot<<<vgrid, 256, 0, st>>>(r, r, npts, vs, bb, sc, 1);
+  // x = local2global(unknown) with essential part zeroed; r -= H x
+  k_local2global<<<egrid, threads, 0, st>>>(g, N, U, x, vs);
+  k_zero_range<<<zgrid, 256, 0, st>>>(x, vs, nzero_lo, S.nsolve, N.nglobal, nz);
+  // all solved planes active for the first operator apply
+  k_pcg_init<<<1, nzt, 0, st>>>(sc, bb, bb, tol_rel, nz);
+  k_global_op<<<egrid, threads, shm, st>>>(g, N, S, x, p, vs, sc);
+  k_zero_range<<<zgrid, 256, 0, st>>>(p, vs, nzero_lo, S.nsolve, N.nglobal, nz);
+  k_sub<<<vgrid, 256, 0, st>>>(r, p, npts, vs, sc);
+  k_dot<<<vgrid, 256, 0, st>>>(r, r, npts, vs, r2, sc, 1);
+  k_pcg_init<<<1, nzt, 0, st>>>(sc, bb, r2, tol_rel, nz);
+  // -- iterations
+  std::vector<int> hflag(1);
+  for (int it = 0; it < step_max + 1; ++it) {
+    cudaMemsetAsync(flag, 0, sizeof(int), st);
+    k_pcg_head<<<1, nzt, 0, st>>>(sc, step_max, nz, flag);
+    if ((it & 7) == 0) {
+      cudaMemcpyAsync(hflag.data(), flag, sizeof(int), cudaMemcpyDeviceToHost, st);
+      err = cudaStreamSynchronize(st);
+      if (err != cudaSuccess) return err;
+      if (!hflag[0]) break;
+    }
+    k_pcg_precond<<<vgrid, 256, 0, st>>>(S.pc, S.npts, r, z, vs, sc);
+    cudaMemsetAsync(rho1, 0, sizeof(double) * nz, st);
+    k_dot<<<vgrid, 256, 0, st>>>(r, z, npts, vs, rho1, sc, 0);
+    k_pcg_dir<<<vgrid, 256, 0, st>>>(z, p, npts, vs, sc, rho1);
+    cudaMemsetAsync(q, 0, sizeof(double) * static_cast<size_t>(vs) * nz, st);
+    k_global_op<<<egrid, threads, shm, st>>>(g, N, S, p, q, vs, sc);
+    k_zero_range<<<zgrid, 256, 0, st>>>(q, vs, nzero_lo, S.nsolve, N.nglobal, nz);
+    cudaMemsetAsync(dotp, 0, sizeof(double) * nz, st);
+    k_dot<<<vgrid, 256, 0, st>>>(p, q, npts, vs, dotp, sc, 0);
+    k_pcg_step<<<vgrid, 256, 0, st>>>(x, r, p, q, npts, vs, sc, rho1, dotp);
+    cudaMemsetAsync(r2, 0, sizeof(double) * nz, st);
+    k_dot<<<vgrid, 256, 0, st>>>(r, r, npts, vs, r2, sc, 0);
+    k_pcg_tail<<<1, nzt, 0, st>>>(sc, rho1, r2, nz);
+  }
+  k_global2local<<<egrid, threads, 0, st>>>(g, N, x, vs, has_ess ? G : nullptr, gs, U);
+  std::vector<PcgScalars> hs(nz);
+  cudaMemcpyAsync(hs.data(), sc, sizeof(PcgScalars) * nz, cudaMemcpyDeviceToHost, st);
+  err = cudaStreamSynchronize(st);
+  if (err != cudaSuccess) return err;
+  bool hit = false;
+  for (int k = 0; k < nz; ++k) {
+    iters[k] = hs[k].solved ? hs[k].iter : -1;
+    hit = hit || hs[k].hit_max;
+  }
+  err = cudaGetLastError();
+  if (err != cudaSuccess) return err;
+  return hit ? cudaErrorNotReady : cudaSuccess;
+}
+
+}  // namespace stx

@@ -1,0 +1,37 @@
+// Launchers of the hot-path kernels (all asynchronous on the given stream).
+#pragma once
+
+#include <cstddef>
+
+#include "device.hpp"
+
+namespace stx {
+
+// Doubles of scratch the direct solve needs: boundary RHS and essential
+// values, one padded globally numbered vector each per plane.
+size_t helmholtz_workspace_doubles(const DevGeom& g, const DevNumbering& N);
+
+// Field::solve DIRECT over all planes: F (Fourier forcing, reference plane
+// layout) -> U.  `lines` holds the Fourier-space BC values [nz][nline].
+// U's Nyquist plane (k = 1) is left untouched, as in the reference.
+cudaError_t helmholtz_direct_solve(const DevGeom& g, const DevNumbering& N, const DevModal& S,
+                                   const double* F, double* U, const double* lines, int nline,
+                                   double* work, cudaStream_t st);
+
+// Field::solve JACPCG over all planes (src/field.cpp:711-805).  U holds the
+// initial guess on entry.  Iterations per plane are written to `iters`
+// (host array, nz entries, -1 for planes not solved).  Returns
+// cudaErrorNotReady if a plane reached STEP_MAX, after finishing all planes.
+size_t jacpcg_workspace_doubles(const DevGeom& g, const DevNumbering& N);
+cudaError_t helmholtz_jacpcg_solve(const DevGeom& g, const DevNumbering& N, const DevModal& S,
+                                   const double* F, double* U, const double* lines, int nline,
+                                   double tol_rel, int step_max, double* work, int* iters,
+                                   cudaStream_t st);
+
+// AuxField::transform (src/auxfield.cpp:1157-1194, femlib/fourier.c:40-165)
+// of nz planes in place: sign +1 forward (scaled by 1/nz), -1 inverse.
+// `twiddle` holds cos/sin(2 pi m / nz), m < nz, as [2][nz].
+cudaError_t z_transform(double* data, int nz, int plane_size, int sign, const double* twiddle,
+                        double* work, cudaStream_t st);
+
+}  // namespace stx

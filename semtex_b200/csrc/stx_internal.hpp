@@ -1,0 +1,99 @@
+// Internal definitions of the opaque C-ABI handles.
+#pragma once
+
+#include <cuda_runtime.h>
+
+#include <map>
+#include <memory>
+#include <stdexcept>
+#include <string>
+#include <vector>
+
+#include "host/mesh.hpp"
+#include "host/session.hpp"
+#include "kernels/device.hpp"
+
+namespace stx {
+
+// Device allocations freed together.
+struct DeviceArena {
+  std::vector<void*> ptrs;
+  void* alloc(size_t bytes);
+  DeviceArena() = default;
+  DeviceArena(const DeviceArena&) = delete;
+  DeviceArena& operator=(const DeviceArena&) = delete;
+  ~DeviceArena();
+};
+
+struct FieldDev {
+  Numbering N;
+  DevNumbering dn{};
+  double* d_lines = nullptr;  // [nz][nline] Fourier-space BC values
+  int nline = 0;
+};
+
+struct ModalStore {
+  DeviceArena arena;
+  DevModal dm{};
+  std::vector<int> nsolve;
+};
+
+void host_dft_forward(std::vector<double>& a, int nz, int n);
+
+}  // namespace stx
+
+struct stx_modal;
+
+struct stx_context {
+  int device = 0;
+  cudaStream_t stream = nullptr;
+  bool own_stream = false;
+  stx::Session S;
+  stx::Mesh M;
+  std::map<char, stx::FieldDev> fields;
+  stx::DeviceArena arena;
+  stx::DevGeom dg{};
+  double* d_twiddle = nullptr;
+  double* d_io = nullptr;
+  std::vector<stx_modal*> modals;
+
+  // Solver workspace, grown on demand (synchronises before regrowing).
+  double* d_work = nullptr;
+  size_t work_doubles = 0;
+  double* workspace(size_t n) {
+    if (n > work_doubles) {
+      cudaStreamSynchronize(stream);
+      if (d_work) cudaFree(d_work);
+      d_work = nullptr;
+      if (cudaMalloc(&d_work, sizeof(double) * n) != cudaSuccess)
+        throw std::runtime_error("cudaMalloc of solver workspace failed");
+      work_doubles = n;
+    }
+    return d_work;
+  }
+  void* d_scratch = nullptr;
+  size_t scratch_bytes = 0;
+  void* scratch(size_t n) {
+    if (n > scratch_bytes) {
+      cudaStreamSynchronize(stream);
+      if (d_scratch) cudaFree(d_scratch);
+      d_scratch = nullptr;
+      if (cudaMalloc(&d_scratch, n) != cudaSuccess)
+        throw std::runtime_error("cudaMalloc of scratch failed");
+      scratch_bytes = n;
+    }
+    return d_scratch;
+  }
+  ~stx_context() {
+    if (d_work) cudaFree(d_work);
+    if (d_scratch) cudaFree(d_scratch);
+  }
+};
+
+struct stx_modal {
+  stx_context* ctx = nullptr;
+  char field = 0;
+  int method = 0;
+  double lambda2 = 0, beta = 0;
+  std::shared_ptr<stx::ModalStore> store;
+};

@@ -1,0 +1,107 @@
+"""FEML session writer for rectangular quad meshes (the role of `rectmesh`).
+
+Produces the session files the benchmarks and tests run: an nx x ny grid of
+quads on [x0,x1] x [y0,y1], optional periodic pairing in x and/or y, one
+boundary group per remaining side kind, tokens and a USER section.
+"""
+
+from __future__ import annotations
+
+import numpy as np
+
+
+def rect_session(path, nx, ny, x=(0.0, 1.0), y=(0.0, 1.0), tokens=None, fields="c",
+                 periodic_x=False, periodic_y=False, bcs=None, user=None, xs=None, ys=None,
+                 wall_group="w"):
+    """Write a session file.
+
+    bcs: {group_char: {field: "<D> value" | "<N> value" | "<H>"}} applied to
+    every non-periodic boundary side (group `wall_group`), or None for no BCs.
+    xs / ys: explicit node coordinates along x / y (length nx+1 / ny+1).
+    """
+    xs = np.linspace(x[0], x[1], nx + 1) if xs is None else np.asarray(xs, float)
+    ys = np.linspace(y[0], y[1], ny + 1) if ys is None else np.asarray(ys, float)
+    lines = []
+    if user:
+        lines.append("<USER>")
+        lines += [f"\t{u}" for u in user]
+        lines.append("</USER>\n")
+    lines.append("<FIELDS>")
+    lines.append("\t" + " ".join(fields))
+    lines.append("</FIELDS>\n")
+    lines.append("<TOKENS>")
+    for k, v in (tokens or {}).items():
+        lines.append(f"\t{k} = {v}")
+    lines.append("</TOKENS>\n")
+    if bcs:
+        lines.append(f"<GROUPS NUMBER={len(bcs)}>")
+        for i, g in enumerate(bcs):
+            lines.append(f"\t{i + 1}\t{g}\twall")
+        lines.append("</GROUPS>\n")
+        lines.append(f"<BCS NUMBER={len(bcs)}>")
+        for i, (g, spec) in enumerate(bcs.items()):
+            lines.append(f"\t{i + 1}\t{g}\t{len(spec)}")
+            for f, s in spec.items():
+                kind, _, val = s.partition(" ")
+                tag = kind.strip("<>")
+                lines.append(f"\t\t<{tag}>\t{f} = {val.strip() or 0}\t</{tag}>")
+        lines.append("</BCS>\n")
+    nn = (nx + 1) * (ny + 1)
+    lines.append(f"<NODES NUMBER={nn}>")
+
+    def nid(i, j):
+        return j * (nx + 1) + i + 1
+
+    for j in range(ny + 1):
+        for i in range(nx + 1):
+            lines.append(f"\t{nid(i, j)}\t{xs[i]:.17g}\t{ys[j]:.17g}\t0")
+    lines.append("</NODES>\n")
+    lines.append(f"<ELEMENTS NUMBER={nx * ny}>")
+
+    def eid(i, j):
+        return j * nx + i + 1
+
+    for j in range(ny):
+        for i in range(nx):
+            lines.append(f"\t{eid(i, j)}\t<Q>\t{nid(i, j)} {nid(i + 1, j)} {nid(i + 1, j + 1)} "
+                         f"{nid(i, j + 1)}\t</Q>")
+    lines.append("</ELEMENTS>\n")
+    surf = []
+    # side 1 = bottom (y0), 2 = right (x1), 3 = top (y1), 4 = left (x0)
+    for i in range(nx):
+        if periodic_y:
+            surf.append((eid(i, 0), 1, f"<P>\t{eid(i, ny - 1)} 3\t</P>"))
+        elif bcs:
+            surf.append((eid(i, 0), 1, f"<B>\t{wall_group}\t</B>"))
+            surf.append((eid(i, ny - 1), 3, f"<B>\t{wall_group}\t</B>"))
+    for j in range(ny):
+        if periodic_x:
+            surf.append((eid(0, j), 4, f"<P>\t{eid(nx - 1, j)} 2\t</P>"))
+        elif bcs:
+            surf.append((eid(0, j), 4, f"<B>\t{wall_group}\t</B>"))
+            surf.append((eid(nx - 1, j), 2, f"<B>\t{wall_group}\t</B>"))
+    lines.append(f"<SURFACES NUMBER={len(surf)}>")
+    for k, (e, s, body) in enumerate(surf):
+        lines.append(f"\t{k + 1}\t{e}\t{s}\t{body}")
+    lines.append("</SURFACES>")
+    with open(path, "w") as f:
+        f.write("\n".join(lines) + "\n")
+    return path
+
+
+def helmholtz_session(path, n, np_, nz=1, lambda2=1.0, beta=1.0, extra=None, user=None, xs=None, ys=None):
+    """Dirichlet-zero Helmholtz problem on [0,1]^2 (configs c1, c2, c4)."""
+    tok = {"N_P": np_, "N_Z": nz, "LAMBDA2": lambda2, "BETA": beta, "TOL_REL": 1e-12}
+    tok.update(extra or {})
+    return rect_session(path, n, n, tokens=tok, fields="c", bcs={"w": {"c": "<D> 0.0"}},
+                        user=user, xs=xs, ys=ys)
+
+
+def taylor_green_session(path, n, np_, nz, re=1600.0, dt=1e-3, nstep=200, extra=None):
+    """3D-periodic Taylor--Green vortex on [0, 2 pi]^3 (config c3)."""
+    tok = {"N_P": np_, "N_Z": nz, "BETA": 1, "KINVIS": f"1.0/{re}", "D_T": dt, "N_TIME": 3,
+           "N_STEP": nstep, "TOL_REL": 1e-13}
+    tok.update(extra or {})
+    user = ["u = sin(x)*cos(y)*cos(z)", "v = -cos(x)*sin(y)*cos(z)", "w = 0", "p = 0"]
+    return rect_session(path, n, n, x=(0.0, 2 * np.pi), y=(0.0, 2 * np.pi), tokens=tok,
+                        fields="uvwp", periodic_x=True, periodic_y=True, user=user)

@@ -1,0 +1,97 @@
+"""GPU parity of the condensed Helmholtz solve against the oracle (FP64).
+
+Bar: relative L2 difference <= 1e-10 between the CUDA path (through the C
+ABI) and the oracle's restatement of Field::solve on the same session and
+forcing; plus agreement with the analytic solutions the sessions carry.
+"""
+import os
+
+import numpy as np
+import pytest
+
+import semtex_oracle as O
+import semtex_b200 as S
+from semtex_b200 import sessions
+
+from conftest import SESSIONS
+
+pytestmark = pytest.mark.gpu
+TOL = 1e-10
+
+
+def rel_l2(a, b):
+    return np.linalg.norm(a - b) / max(np.linalg.norm(b), 1e-300)
+
+
+@pytest.mark.parametrize("name", ["helmholtz1", "poisson1", "laplace1", "laplace4", "laplace3"])
+@pytest.mark.parametrize("iterative", [False, True])
+def test_reference_sessions(name, iterative):
+    path = os.path.join(SESSIONS, name)
+    ov = {"ITERATIVE": 1, "TOL_REL": 1e-14} if iterative else None
+    u = S.elliptic(path, overrides=ov, iterative=iterative)
+    P, U = O.elliptic(path, ov)
+    assert rel_l2(u, U) < (1e-9 if iterative else TOL)
+
+
+def _random_case(tmp_path, n, np_, nz, seed, perturb=0.0):
+    rng = np.random.default_rng(seed)
+    xs = ys = None
+    if perturb:
+        xs = np.linspace(0, 1, n + 1)
+        ys = np.linspace(0, 1, n + 1)
+        xs[1:-1] += perturb * rng.uniform(-1, 1, n - 1) / n
+        ys[1:-1] += perturb * rng.uniform(-1, 1, n - 1) / n
+    p = sessions.helmholtz_session(str(tmp_path / f"r{seed}"), n, np_, nz=nz, lambda2=1.0, beta=1.0,
+                                   xs=xs, ys=ys)
+    ctx = S.Context(p)
+    x, y = ctx.mesh_coords()
+    f = rng.uniform(-1, 1, (nz, n * n, np_, np_))
+    return p, ctx, f
+
+
+@pytest.mark.parametrize("n,np_,nz,perturb", [(4, 6, 8, 0.0), (5, 7, 6, 0.3), (3, 11, 4, 0.0), (6, 5, 1, 0.25)])
+def test_random_forcing_fourier(tmp_path, n, np_, nz, perturb):
+    p, ctx, f = _random_case(tmp_path, n, np_, nz, seed=n * 100 + np_, perturb=perturb)
+    sysm = S.ModalMatrixSys(ctx, "c", 1.0)
+    u = sysm.solve_host(f)
+    P, U = O.elliptic(p, forcing_phys=f)
+    assert rel_l2(u, U) < TOL
+    if perturb:
+        assert ctx.families() > 1
+
+
+def test_two_calls_in_a_row_identical(tmp_path):
+    p, ctx, f = _random_case(tmp_path, 4, 6, 8, seed=7)
+    sysm = S.ModalMatrixSys(ctx, "c", 1.0)
+    u1 = sysm.solve_host(f).copy()
+    u2 = sysm.solve_host(f)
+    assert rel_l2(u1, u2) < 1e-14
+
+
+def test_device_solve_and_transform(tmp_path):
+    import torch
+    p, ctx, f = _random_case(tmp_path, 4, 6, 8, seed=11)
+    F = ctx.new_field("f").load_physical(f)
+    F.transform(S.FORWARD)
+    fo = O.dft_forward(f)
+    got = F.to_numpy()
+    assert rel_l2(got, fo) < 1e-14
+    F.zero_nyquist()
+    U = ctx.new_field("c")
+    sysm = S.ModalMatrixSys(ctx, "c", 1.0)
+    U.solve(F, sysm)
+    U.transform(S.INVERSE)
+    P, Uo = O.elliptic(p, forcing_phys=f)
+    assert rel_l2(U.to_numpy(), Uo) < TOL
+
+
+def test_transform_roundtrip_odd_factors(tmp_path):
+    p = sessions.helmholtz_session(str(tmp_path / "t"), 2, 5, nz=12)
+    ctx = S.Context(p)
+    rng = np.random.default_rng(3)
+    f = rng.standard_normal((12, 4, 5, 5))
+    F = ctx.new_field().load_physical(f)
+    F.transform(S.FORWARD)
+    assert rel_l2(F.to_numpy(), O.dft_forward(f)) < 1e-14
+    F.transform(S.INVERSE)
+    assert rel_l2(F.to_numpy(), f) < 1e-14
