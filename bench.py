@@ -1,0 +1,341 @@
+"""Benchmark: batched 2D x Fourier Helmholtz solve, Helmholtz DOF/s on B200.
+
+Workload (the configuration the headline metric is quoted on): 16x16
+uniform quads on [0,1]^2, GLL order N=10 (N_P=11), N_Z=64 planes (modes
+k=0..31), per-mode constant lambda^2 + (beta k)^2 with LAMBDA2=1, BETA=1,
+Dirichlet u=0 on the x/y edges, forcing i.i.d. uniform[-1,1] per unique node
+from seed 20261203.  One step = one full condensed direct solve of every
+mode (elliptic/helmholtz.cpp:29-52, src/field.cpp:598-709) in plain FP64.
+DOF per step = unique nodes per plane x N_Z = 25921 x 64.
+
+value: device time of the solve with the Fourier forcing resident in HBM
+(CUDA events on the library stream, L2 flushed between steps).
+e2e:   the public host-buffer call stx_elliptic_solve_host (pinned forcing
+in, forward FFT, solve, inverse FFT, solution out), wall clock.
+
+Usage: python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference]
+"""
+
+from __future__ import annotations
+
+import argparse
+import json
+import os
+import statistics
+import subprocess
+import sys
+import tempfile
+import time
+
+import numpy as np
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, ROOT)
+
+WORKLOAD = dict(n=16, np_=11, nz=64, lambda2=1.0, beta=1.0, seed=20261203)
+METRIC = "Helmholtz DOF/s (batched 2D x Fourier, plain FP64 direct)"
+UNIT = "DOF/s"
+
+
+def make_session(d):
+    from semtex_b200 import sessions
+    w = WORKLOAD
+    return sessions.helmholtz_session(os.path.join(d, "c2"), w["n"], w["np_"], nz=w["nz"],
+                                      lambda2=w["lambda2"], beta=w["beta"])
+
+
+def forcing_per_unique_node(x, y, nz, seed):
+    """U[-1,1] per unique (x, y, z) node, identical on coincident element copies."""
+    key = np.round(x * 1e9).astype(np.int64) * 4000000007 + np.round(y * 1e9).astype(np.int64)
+    uniq, inv = np.unique(key.ravel(), return_inverse=True)
+    rng = np.random.default_rng(seed)
+    vals = rng.uniform(-1.0, 1.0, (nz, len(uniq)))
+    return vals[:, inv].reshape((nz,) + x.shape), len(uniq)
+
+
+def dist_init():
+    ws = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    if ws > 1:
+        import torch.distributed as dist
+        import datetime
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=120))
+    return ws, rank, local
+
+
+def clocks_start():
+    try:
+        f = open(os.path.join(tempfile.gettempdir(), f"clk_{os.getpid()}.csv"), "w")
+        p = subprocess.Popen(
+            ["nvidia-smi", "--query-gpu=index,clocks.sm,clocks.max.sm,power.draw,"
+             "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+             "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap",
+             "--format=csv,noheader,nounits", "-lms", "200"], stdout=f, stderr=subprocess.DEVNULL)
+        return p, f
+    except Exception:
+        return None, None
+
+
+def clocks_stop(p, f, gpu_index):
+    if p is None:
+        return None
+    p.terminate()
+    p.wait(timeout=10)
+    f.close()
+    sm, mx, reasons = [], None, set()
+    names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+    for ln in open(f.name):
+        parts = [s.strip() for s in ln.split(",")]
+        if len(parts) < 8 or parts[0] != str(gpu_index):
+            continue
+        try:
+            sm.append(float(parts[1]))
+            mx = float(parts[2])
+        except ValueError:
+            continue
+        for nm, v in zip(names, parts[4:8]):
+            if v.lower() == "active":
+                reasons.add(nm)
+    os.unlink(f.name)
+    if not sm:
+        return None
+    return {"sm_mhz": statistics.median(sm), "sm_max_mhz": mx, "reasons": sorted(reasons),
+            "samples": len(sm)}
+
+
+def measured_peaks():
+    p = os.path.join(ROOT, "MEASURED_PEAKS.json")
+    if os.path.exists(p):
+        d = json.load(open(p))
+        return d.get("hbm_gbs", 6650.0), "measured"
+    return 6650.0, "fallback"
+
+
+def load_profile_traffic():
+    """DRAM bytes per launch of the banded sweep from the committed ncu summary."""
+    p = os.path.join(ROOT, "profiles", "band_solve_c2.json")
+    if os.path.exists(p):
+        return json.load(open(p)).get("dram_bytes_per_launch")
+    return None
+
+
+# ---------------------------------------------------------------------------
+# CPU arms (the oracle restatement of the reference path; the reference itself
+# does not build here)
+# ---------------------------------------------------------------------------
+
+def _oracle_plane_worker(args):
+    """Oracle solves of `planes`, each repeated `nrep` times after a one-off setup.
+
+    Returns per-repetition seconds (summed over this worker's planes)."""
+    session, planes, seed, nrep = args
+    from threadpoolctl import threadpool_limits
+    sys.path.insert(0, os.path.join(ROOT, "oracle"))
+    import semtex_oracle as O
+    with threadpool_limits(1):
+        S = O.read_session(session)
+        P = O.Problem(S)
+        c = "c"
+        f, _ = forcing_per_unique_node(P.M.x, P.M.y, P.nz, seed)
+        F = O.dft_forward(f)
+        bl = P.bc_lines(c)
+        beta = S.tokens["BETA"]
+        systems = {k: O.MatrixSys(P.M, P.N[c], S.tokens["LAMBDA2"], (beta * (k >> 1)) ** 2)
+                   for k in planes}
+        out = []
+        for _ in range(nrep):
+            t0 = time.perf_counter()
+            for k in planes:
+                O.solve_plane(P.M, P.N[c], P.B[c], systems[k], F[k], np.zeros_like(F[k]), bl[k])
+            out.append(time.perf_counter() - t0)
+    return out
+
+
+def cpu_sample(session, planes, workers, seed, nrep=1):
+    """Oracle solves of `planes` spread over `workers` spawned processes.
+
+    Returns the per-repetition wall time of the slowest worker."""
+    if workers <= 1:
+        return _oracle_plane_worker((session, planes, seed, nrep))
+    import multiprocessing as mp
+    ctx = mp.get_context("spawn")
+    chunks = [planes[i::workers] for i in range(workers)]
+    chunks = [c for c in chunks if c]
+    with ctx.Pool(len(chunks)) as pool:
+        res = pool.map(_oracle_plane_worker, [(session, ch, seed, nrep) for ch in chunks])
+    return [max(r[i] for r in res) for i in range(nrep)]
+
+
+def run_reference(args):
+    ws, rank, _ = int(os.environ.get("WORLD_SIZE", "1")), int(os.environ.get("RANK", "0")), 0
+    if rank != 0:
+        return
+    w = WORKLOAD
+    cores = os.cpu_count() or 1
+    with tempfile.TemporaryDirectory() as d:
+        session = make_session(d)
+        sys.path.insert(0, os.path.join(ROOT, "oracle"))
+        import semtex_oracle as O
+        S = O.read_session(session)
+        P = O.Problem(S)
+        _, nuniq = forcing_per_unique_node(P.M.x, P.M.y, 1, w["seed"])
+        planes = [k for k in range(w["nz"]) if k != 1][: max(cores, 1)]
+        reps = cpu_sample(session, planes, cores, w["seed"], args.warmup + args.steps)
+        times = reps[args.warmup:]
+    tot = sum(times)
+    value = nuniq * len(planes) * len(times) / tot
+    line = {
+        "impl": "reference", "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": ws,
+        "steps": args.steps, "warmup": args.warmup, "ms_per_step": 1e3 * tot / len(times),
+        "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f64",
+        "data": "synthetic", "config": config_block(),
+        "cpu_baseline": {"value": value, "unit": UNIT, "cores": cores, "kind": "port",
+                         "sample": f"{len(planes)} of {w['nz'] - 1} solved planes per step, one "
+                                   f"process per core; condensed-system setup excluded"},
+        "e2e": {"value": value, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
+    }
+    print(json.dumps(line))
+
+
+def config_block():
+    w = WORKLOAD
+    return {"workload": "c2: batched 2D x Fourier Helmholtz, 16x16 quads, N_P=11, N_Z=64, "
+                        "lambda2=1+k^2, Dirichlet 0, U[-1,1] forcing",
+            "elements": w["n"] * w["n"], "np": w["np_"], "nz": w["nz"],
+            "solver": "static condensation + banded Cholesky per mode (FP64)",
+            "l2": "flushed between timed steps (256 MB write)", "parallelism": "replicas"}
+
+
+# ---------------------------------------------------------------------------
+# GPU arm
+# ---------------------------------------------------------------------------
+
+def run_ours(args):
+    import ctypes as C
+    import torch
+    ws, rank, local = dist_init()
+    torch.cuda.set_device(local)
+    import semtex_b200 as S
+    from semtex_b200 import _lib
+    w = WORKLOAD
+    d = tempfile.mkdtemp()
+    session = make_session(d)
+    t0 = time.perf_counter()
+    ctx = S.Context(session, device=local)
+    x, y = ctx.mesh_coords()
+    f, nuniq = forcing_per_unique_node(x, y, ctx.nz, w["seed"])
+    sysm = S.ModalMatrixSys(ctx, "c", w["lambda2"], w["beta"])
+    setup_s = time.perf_counter() - t0
+    dof = nuniq * ctx.nz
+    F = ctx.new_field("f").load_physical(f).transform(S.FORWARD).zero_nyquist()
+    U = ctx.new_field("c")
+    stream = ctx.torch_stream()
+    flush = torch.empty(256 * 1024 * 1024 // 4, dtype=torch.float32, device=f"cuda:{local}")
+    nb = sysm.info(1)["nband"]
+    ns = [sysm.info(m)["nsolve"] for m in range(sysm.num_modes)]
+    phase = (C.c_float * 4)()
+    launches = C.c_int()
+
+    def solve_profiled():
+        _lib.check(_lib.lib().stx_field_solve_profiled(sysm.handle, F.ptr(), U.ptr(), phase,
+                                                       C.byref(launches)))
+        return list(phase)
+
+    for _ in range(args.warmup):
+        solve_profiled()
+    if ws > 1:
+        torch.distributed.barrier()
+    torch.cuda.synchronize()
+    clk_p, clk_f = clocks_start()
+    phases = []
+    t_total = 0.0
+    for _ in range(args.steps):
+        with torch.cuda.stream(stream):
+            flush.fill_(1.0)
+        ph = solve_profiled()
+        phases.append(ph)
+        t_total += sum(ph) / 1e3
+    torch.cuda.synchronize()
+    if ws > 1:
+        t = torch.tensor([t_total], device=f"cuda:{local}")
+        torch.distributed.all_reduce(t, op=torch.distributed.ReduceOp.MAX)
+        torch.distributed.barrier()
+        t_total = t.item()
+    # -- end to end through the host-buffer call
+    fh = torch.from_numpy(np.ascontiguousarray(f)).pin_memory()
+    uh = torch.empty_like(fh).pin_memory()
+    for _ in range(max(1, args.warmup)):
+        _lib.check(_lib.lib().stx_elliptic_solve_host(sysm.handle, C.c_void_p(fh.data_ptr()),
+                                                      C.c_void_p(uh.data_ptr())))
+    if ws > 1:
+        torch.distributed.barrier()
+    e0 = time.perf_counter()
+    for _ in range(args.steps):
+        _lib.check(_lib.lib().stx_elliptic_solve_host(sysm.handle, C.c_void_p(fh.data_ptr()),
+                                                      C.c_void_p(uh.data_ptr())))
+    e_total = time.perf_counter() - e0
+    if ws > 1:
+        t = torch.tensor([e_total], device=f"cuda:{local}")
+        torch.distributed.all_reduce(t, op=torch.distributed.ReduceOp.MAX)
+        e_total = t.item()
+    clocks = clocks_stop(clk_p, clk_f, local)
+    if rank != 0:
+        if ws > 1:
+            torch.distributed.destroy_process_group()
+        return
+    ph = np.array(phases)
+    band_ms = ph[:, 1] + ph[:, 2]
+    # algorithmic bytes of both banded sweeps: every factor entry once per sweep
+    # plus the RHS vectors read and written (Re and Im planes of each mode).
+    nr = [1] + [2] * (len(ns) - 1)
+    band_bytes = 2 * sum(8 * n * nb + 2 * 8 * n * r for n, r in zip(ns, nr))
+    peak, kind = measured_peaks()
+    achieved = band_bytes / (band_ms.mean() / 1e3) / 1e9
+    traffic = load_profile_traffic()
+    # CPU baseline: the oracle on one core over a bounded sample of planes
+    cpu = None
+    if not args.no_cpu_baseline:
+        planes = [0, 2, 3, 20, 21, 62, 63]
+        secs = cpu_sample(session, planes, 1, w["seed"], 3)
+        cpu = {"value": nuniq * len(planes) / min(secs), "unit": UNIT, "cores": 1, "kind": "port",
+               "sample": f"{len(planes)} of {w['nz'] - 1} solved planes (modes 0,1,10,31), "
+                         "oracle restatement: per-element condensation + LAPACK dpbtrs, 1 thread"}
+    line = {
+        "metric": METRIC, "value": dof * args.steps * ws / t_total, "unit": UNIT, "n_gpus": ws,
+        "steps": args.steps, "warmup": args.warmup, "ms_per_step": 1e3 * t_total / args.steps,
+        "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f64",
+        "data": "synthetic", "config": config_block(),
+        "e2e": {"value": dof * args.steps * ws / e_total, "unit": UNIT,
+                "h2d_bytes_per_step": int(fh.numel() * 8), "d2h_bytes_per_step": int(uh.numel() * 8)},
+        "roofline": {"bound": "hbm", "kernel": "k_band_solve (forward + backward sweeps)",
+                     "achieved": achieved, "peak": peak, "unit": "GB/s", "frac": achieved / peak,
+                     "peak_kind": kind, "traffic": traffic,
+                     "algorithmic_bytes_per_step": band_bytes},
+        "phases_ms": {"condense": float(ph[:, 0].mean()), "band_fwd": float(ph[:, 1].mean()),
+                      "band_bwd": float(ph[:, 2].mean()), "recover": float(ph[:, 3].mean())},
+        "setup_s": setup_s, "nband": nb, "nsolve": max(ns), "families": ctx.families(),
+        "gpu_launches": int(launches.value) * args.steps,
+        "clocks": clocks, "cpu_baseline": cpu,
+    }
+    print(json.dumps(line))
+    if ws > 1:
+        torch.distributed.destroy_process_group()
+
+
+def main():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=20)
+    ap.add_argument("--warmup", type=int, default=3)
+    ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
+    ap.add_argument("--no-cpu-baseline", action="store_true")
+    args = ap.parse_args()
+    if args.impl == "reference":
+        run_reference(args)
+    else:
+        run_ours(args)
+
+
+if __name__ == "__main__":
+    main()

@@ -102,6 +102,14 @@ int stx_modal_info(const stx_modal* sys, int mode, int* nsolve, int* nband);
 int stx_field_solve(stx_modal* sys, const double* d_forcing, double* d_unknown, double tol_rel,
                     int step_max, int* iterations);
 
+/* Field::solve for a DIRECT system with CUDA events recorded on the
+ * context stream between its phases; synchronises and returns the device
+ * milliseconds of [constrain+condense, forward band sweep, backward band
+ * sweep, interior recovery] in phase_ms[4] and the number of kernel launches
+ * in *launches (may be NULL).  Instrumentation for benchmarks. */
+int stx_field_solve_profiled(stx_modal* sys, const double* d_forcing, double* d_unknown,
+                             float* phase_ms, int* launches);
+
 /* AuxField::transform(sign) (src/auxfield.cpp:1157-1194) in place on nz
  * device planes of plane_size doubles. */
 int stx_transform(stx_context* ctx, double* d_data, int sign);
@@ -111,6 +119,9 @@ int stx_transform(stx_context* ctx, double* d_data, int sign);
  * transform, zero Nyquist, solve every mode, inverse transform, copy the
  * physical-space solution out.  Synchronises. */
 int stx_elliptic_solve_host(stx_modal* sys, const double* h_forcing, double* h_solution);
+
+/* The cudaStream_t all of the context's device work runs on. */
+int stx_context_stream(const stx_context* ctx, void** stream);
 
 /* Synchronise the context's stream. */
 int stx_sync(stx_context* ctx);

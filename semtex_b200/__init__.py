@@ -62,6 +62,16 @@ class Context:
     def handle(self):
         return self._h
 
+    @property
+    def stream(self) -> int:
+        """cudaStream_t (as an int) all of this context's device work runs on."""
+        s = C.c_void_p()
+        check(lib().stx_context_stream(self._h, C.byref(s)))
+        return s.value or 0
+
+    def torch_stream(self):
+        return _torch().cuda.ExternalStream(self.stream, device=f"cuda:{self.device}")
+
     def close(self):
         if self._h:
             check(lib().stx_context_destroy(self._h))
@@ -120,6 +130,7 @@ class Field:
         self.ctx, self.name = ctx, name
         self.data = torch.zeros((ctx.nz, ctx.plane_size), dtype=torch.float64,
                                 device=f"cuda:{ctx.device}")
+        torch.cuda.synchronize(self.data.device)
 
     def ptr(self):
         return C.c_void_p(self.data.data_ptr())
@@ -130,6 +141,7 @@ class Field:
         n = self.ctx.nel * self.ctx.np ** 2
         self.data.zero_()
         self.data[:, :n] = torch.from_numpy(np.ascontiguousarray(a).reshape(self.ctx.nz, n)).to(self.data.device)
+        torch.cuda.synchronize(self.data.device)   # library work runs on the context stream
         return self
 
     def to_numpy(self) -> np.ndarray:
@@ -144,7 +156,9 @@ class Field:
 
     def zero_nyquist(self):
         if self.ctx.nz > 1:
+            self.ctx.sync()
             self.data[1].zero_()
+            _torch().cuda.synchronize(self.data.device)
         return self
 
     def solve(self, forcing: "Field", system: "ModalMatrixSys", tol_rel: float | None = None,

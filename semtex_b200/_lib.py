@@ -42,8 +42,10 @@ SIGNATURES = {
     "stx_modal_info": (_i, [_p, _i, _pi, _pi]),
     "stx_field_solve": (_i, [_p, _p, _p, _d, _i, _pi]),
     "stx_transform": (_i, [_p, _p, _i]),
+    "stx_field_solve_profiled": (_i, [_p, _p, _p, C.POINTER(C.c_float), _pi]),
     "stx_elliptic_solve_host": (_i, [_p, _p, _p]),
     "stx_sync": (_i, [_p]),
+    "stx_context_stream": (_i, [_p, C.POINTER(_p)]),
     "stx_context_scratch": (_i, [_p, C.c_ulonglong, C.POINTER(_p)]),
 }
 

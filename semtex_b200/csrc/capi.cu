@@ -456,6 +456,27 @@ int stx_field_solve(stx_modal* sys, const double* d_forcing, double* d_unknown, 
   });
 }
 
+int stx_field_solve_profiled(stx_modal* sys, const double* d_forcing, double* d_unknown,
+                             float* phase_ms, int* launches) {
+  return guarded([&] {
+    if (!sys || !d_forcing || !d_unknown || !phase_ms) throw StxError(STX_EINVAL, "null argument");
+    if (sys->method != STX_DIRECT) throw StxError(STX_EINVAL, "profiled solve is for DIRECT systems");
+    stx_context* ctx = sys->ctx;
+    FieldDev& F = ctx->fields.at(sys->field);
+    cudaSetDevice(ctx->device);
+    cudaEvent_t ev[5];
+    for (auto& e : ev) cuda_check(cudaEventCreate(&e), "event");
+    double* work = ctx->workspace(helmholtz_workspace_doubles(ctx->dg, F.dn));
+    cudaError_t err = helmholtz_direct_solve(ctx->dg, F.dn, sys->store->dm, d_forcing, d_unknown,
+                                             F.d_lines, F.nline, work, ctx->stream, ev);
+    if (err == cudaSuccess) err = cudaEventSynchronize(ev[4]);
+    for (int i = 0; i < 4 && err == cudaSuccess; ++i) err = cudaEventElapsedTime(&phase_ms[i], ev[i], ev[i + 1]);
+    for (auto& e : ev) cudaEventDestroy(e);
+    cuda_check(err, "profiled solve");
+    if (launches) *launches = helmholtz_direct_launches(F.dn, ctx->M.np);
+  });
+}
+
 int stx_transform(stx_context* ctx, double* d_data, int sign) {
   return guarded([&] {
     if (!ctx || !d_data) throw StxError(STX_EINVAL, "null argument");
@@ -499,6 +520,13 @@ int stx_elliptic_solve_host(stx_modal* sys, const double* h_forcing, double* h_s
                                  cudaMemcpyDeviceToHost, ctx->stream),
                  "solution d2h");
     cuda_check(cudaStreamSynchronize(ctx->stream), "sync");
+  });
+}
+
+int stx_context_stream(const stx_context* ctx, void** stream) {
+  return guarded([&] {
+    if (!ctx || !stream) throw StxError(STX_EINVAL, "null argument");
+    *stream = static_cast<void*>(ctx->stream);
   });
 }
 

@@ -457,13 +457,20 @@ size_t helmholtz_workspace_doubles(const DevGeom& g, const DevNumbering& N) {
   return 2 * stride * g.nz;
 }
 
+int helmholtz_direct_launches(const DevNumbering& N, int np) {
+  const bool has_ess = N.nglobal > N.nsolve;
+  const int nedge_nodes = N.nedge * np;
+  return 4 + (has_ess && nedge_nodes ? 1 : 0) + (nedge_nodes ? 1 : 0);
+}
+
 cudaError_t helmholtz_direct_solve(const DevGeom& g, const DevNumbering& N, const DevModal& S,
                                    const double* F, double* U, const double* lines, int nline,
-                                   double* work, cudaStream_t st) {
+                                   double* work, cudaStream_t st, cudaEvent_t* ev) {
   const int rstride = (N.nglobal + 31) / 32 * 32;
   double* R = work;
   double* G = work + static_cast<size_t>(rstride) * g.nz;
   const int nz = g.nz;
+  if (ev) cudaEventRecord(ev[0], st);
   cudaError_t err = cudaMemsetAsync(work, 0, sizeof(double) * 2 * static_cast<size_t>(rstride) * nz, st);
   if (err != cudaSuccess) return err;
   const bool has_ess = N.nglobal > N.nsolve;
@@ -480,10 +487,14 @@ cudaError_t helmholtz_direct_solve(const DevGeom& g, const DevNumbering& N, cons
     dim3 grid((nedge_nodes + 127) / 128, nz);
     k_natural<<<grid, 128, 0, st>>>(g, N, lines, nline, R, rstride, nz);
   }
+  if (ev) cudaEventRecord(ev[1], st);
   k_band_solve<<<S.nmodes, 256, 0, st>>>(S, S.fwd, R, rstride, nz, 0);
+  if (ev) cudaEventRecord(ev[2], st);
   k_band_solve<<<S.nmodes, 256, 0, st>>>(S, S.bwd, R, rstride, nz, 1);
+  if (ev) cudaEventRecord(ev[3], st);
   k_recover<<<egrid, threads, shm + sizeof(double) * g.next, st>>>(g, N, S, F, has_ess ? G : nullptr,
                                                                    rstride, R, rstride, U);
+  if (ev) cudaEventRecord(ev[4], st);
   return cudaGetLastError();
 }
 

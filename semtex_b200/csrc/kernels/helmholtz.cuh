@@ -14,9 +14,15 @@ size_t helmholtz_workspace_doubles(const DevGeom& g, const DevNumbering& N);
 // Field::solve DIRECT over all planes: F (Fourier forcing, reference plane
 // layout) -> U.  `lines` holds the Fourier-space BC values [nz][nline].
 // U's Nyquist plane (k = 1) is left untouched, as in the reference.
+// `phase_events` (optional, 5 events) are recorded on `st` before the
+// condensation, before each banded sweep, before the recovery and at the end.
 cudaError_t helmholtz_direct_solve(const DevGeom& g, const DevNumbering& N, const DevModal& S,
                                    const double* F, double* U, const double* lines, int nline,
-                                   double* work, cudaStream_t st);
+                                   double* work, cudaStream_t st,
+                                   cudaEvent_t* phase_events = nullptr);
+
+// Number of kernel launches one direct solve issues.
+int helmholtz_direct_launches(const DevNumbering& N, int np);
 
 // Field::solve JACPCG over all planes (src/field.cpp:711-805).  U holds the
 // initial guess on entry.  Iterations per plane are written to `iters`
