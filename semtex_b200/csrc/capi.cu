@@ -95,9 +95,50 @@ void host_dft_forward(std::vector<double>& a, int nz, int n) {
   a.swap(out);
 }
 
+// Inverses of the kBandRows x kBandRows diagonal blocks of a lower-triangular
+// band factor stored as rows L[j*nb + t] (column j-kd+t, 1/diagonal at t=kd).
+// Block b covers rows [16b, 16b+16); rows past n are identity.
+void band_block_inverses(const std::vector<double>& L, int n, int nb, double* out) {
+  const int B = kBandRows, kd = nb - 1;
+  for (int j0 = 0, b = 0; j0 < n; j0 += B, ++b) {
+    double T[kBandRows][kBandRows] = {};
+    for (int r = 0; r < B; ++r) {
+      const int j = j0 + r;
+      if (j >= n) {
+        T[r][r] = 1.0;
+        continue;
+      }
+      for (int s2 = 0; s2 < r; ++s2)
+        if (r - s2 <= kd) T[r][s2] = L[static_cast<size_t>(j) * nb + kd - r + s2];
+      T[r][r] = 1.0 / L[static_cast<size_t>(j) * nb + kd];
+    }
+    double* Y = out + static_cast<size_t>(b) * B * B;  // Y = T^{-1}, lower triangular
+    for (int c = 0; c < B; ++c)
+      for (int r = 0; r < B; ++r) {
+        if (r < c) {
+          Y[r * B + c] = 0.0;
+          continue;
+        }
+        double v = (r == c) ? 1.0 : 0.0;
+        for (int s2 = c; s2 < r; ++s2) v -= T[r][s2] * Y[s2 * B + c];
+        Y[r * B + c] = v / T[r][r];
+      }
+  }
+}
+
 }  // namespace stx
 
 using namespace stx;
+
+// Device status word of a DIRECT system: nonzero if a bounded wait inside a
+// banded sweep expired.  Call only after the stream has been synchronised.
+static void check_sweep_status(const stx_modal* sys) {
+  const int* st = sys->store->dm.status;
+  if (!st) return;
+  int v = 0;
+  cuda_check(cudaMemcpy(&v, st, sizeof(int), cudaMemcpyDeviceToHost), "status read");
+  if (v) throw StxError(STX_ECUDA, "banded sweep: bounded wait for a bulk copy expired");
+}
 
 template <class T>
 static T* upload(DeviceArena& A, const std::vector<T>& v) {
@@ -376,22 +417,40 @@ int stx_modal_create(stx_context* ctx, char field, double lambda2, double beta, 
       d.betak2 = upload(st->arena, bk2);
       d.nsolve = upload(st->arena, ns);
       if (method == STX_DIRECT) {
-        std::vector<double> hbi, hii, fwd, bwd;
-        const size_t band = static_cast<size_t>(nsmax) * N.nband;
+        // Device band layout: rows padded to an even stride (16-byte rows for
+        // bulk copies), modes 256-byte aligned, plus the inverse of every
+        // 16x16 diagonal block of each triangular factor.
+        const int nb = N.nband, nbp = (nb + 1) / 2 * 2;
+        const long long mstride = (static_cast<long long>(nsmax) * nbp + 31) / 32 * 32;
+        const int nblk = (nsmax + kBandRows - 1) / kBandRows;
+        const long long dstride = static_cast<long long>(std::max(1, nblk)) * kBandRows * kBandRows;
+        std::vector<double> hbi, hii;
+        std::vector<double> fwd(mstride * num_modes, 0.0), bwd(mstride * num_modes, 0.0);
+        std::vector<double> dfw(dstride * num_modes, 0.0), dbw(dstride * num_modes, 0.0);
         for (int m = 0; m < num_modes; ++m) {
           hbi.insert(hbi.end(), modes[m].hbi.begin(), modes[m].hbi.end());
           hii.insert(hii.end(), modes[m].hii.begin(), modes[m].hii.end());
-          auto f = modes[m].fwd, b = modes[m].bwd;
-          f.resize(band, 0.0);
-          b.resize(band, 0.0);
-          fwd.insert(fwd.end(), f.begin(), f.end());
-          bwd.insert(bwd.end(), b.begin(), b.end());
+          const int n = modes[m].nsolve;
+          for (int j = 0; j < n; ++j)
+            for (int t = 0; t < nb; ++t) {
+              fwd[m * mstride + static_cast<long long>(j) * nbp + t] = modes[m].fwd[static_cast<size_t>(j) * nb + t];
+              bwd[m * mstride + static_cast<long long>(j) * nbp + t] = modes[m].bwd[static_cast<size_t>(j) * nb + t];
+            }
+          band_block_inverses(modes[m].fwd, n, nb, &dfw[m * dstride]);
+          band_block_inverses(modes[m].bwd, n, nb, &dbw[m * dstride]);
           modes[m] = ModeSystem();
         }
+        d.nbp = nbp;
+        d.mode_stride = mstride;
+        d.dinv_stride = dstride;
         d.hbi = upload(st->arena, hbi);
         d.hii = upload(st->arena, hii);
         d.fwd = upload(st->arena, fwd);
         d.bwd = upload(st->arena, bwd);
+        d.dinv_fwd = upload(st->arena, dfw);
+        d.dinv_bwd = upload(st->arena, dbw);
+        d.status = static_cast<int*>(st->arena.alloc(sizeof(int)));
+        cuda_check(cudaMemset(d.status, 0, sizeof(int)), "status");
         d.pc = nullptr;
         d.npts = 0;
       } else {
@@ -399,7 +458,8 @@ int stx_modal_create(stx_context* ctx, char field, double lambda2, double beta, 
         d.npts = N.nglobal + M.nel * M.nint;
         for (int m = 0; m < num_modes; ++m) pc.insert(pc.end(), modes[m].pc.begin(), modes[m].pc.end());
         d.pc = upload(st->arena, pc);
-        d.hbi = d.hii = d.fwd = d.bwd = nullptr;
+        d.hbi = d.hii = d.fwd = d.bwd = d.dinv_fwd = d.dinv_bwd = nullptr;
+        d.status = nullptr;
       }
       sys->store = st;
     }
@@ -473,6 +533,7 @@ int stx_field_solve_profiled(stx_modal* sys, const double* d_forcing, double* d_
     for (int i = 0; i < 4 && err == cudaSuccess; ++i) err = cudaEventElapsedTime(&phase_ms[i], ev[i], ev[i + 1]);
     for (auto& e : ev) cudaEventDestroy(e);
     cuda_check(err, "profiled solve");
+    check_sweep_status(sys);
     if (launches) *launches = helmholtz_direct_launches(F.dn, ctx->M.np);
   });
 }

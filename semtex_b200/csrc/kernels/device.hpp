@@ -42,14 +42,20 @@ struct DevNumbering {
 // A ModalMatrixSys on the device: one MatrixSys per locally held mode.
 struct DevModal {
   int nmodes, method, nfamily;
-  int nband, ns_stride;           // band width, row stride between modes' factors
+  int nband, ns_stride;           // band width, rows reserved per mode
+  int nbp;                        // factor row stride (nband rounded up to even)
+  long long mode_stride;          // doubles between modes' factors (256-byte multiple)
+  long long dinv_stride;          // doubles between modes' inverse diagonal blocks
   const double* lambda2;          // [nmodes]
   const double* betak2;           // [nmodes]
   const int* nsolve;              // [nmodes]
   const double* hbi;              // [nmodes][nfamily][next][nint]
   const double* hii;              // [nmodes][nfamily][nint][nint]
-  const double* fwd;              // [nmodes][ns_stride][nband]
-  const double* bwd;              // [nmodes][ns_stride][nband]
+  const double* fwd;              // [nmodes][mode_stride]: rows of U^T, stride nbp
+  const double* bwd;              // [nmodes][mode_stride]: rows of reversed U
+  const double* dinv_fwd;         // [nmodes][dinv_stride]: 16x16 inverse diagonal blocks
+  const double* dinv_bwd;
+  int* status;                    // device status word (0 = ok)
   const double* pc;               // JACPCG: [nmodes][npts]
   int npts;
 };

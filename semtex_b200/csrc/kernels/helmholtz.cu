@@ -160,7 +160,7 @@ __global__ void k_recover(DevGeom g, DevNumbering N, DevModal S,
 }
 
 // Banded lower-triangular solve L z = c, in place, for the planes of one mode
-// per block.  Row j of L is contiguous: L[j*nband + t] multiplies z[j-kd+t],
+// per block (simple form, used for bands too wide for the pipelined sweep).  Row j of L is contiguous: L[j*nband + t] multiplies z[j-kd+t],
 // t = kd holds 1/L[j][j].  `reversed` addresses vector entry r at n-1-r.
 // Rows are processed in blocks of 32: all warps form the contributions of
 // already-solved columns, then warp 0 finishes the block's 32x32 triangle.
@@ -171,8 +171,8 @@ __global__ void k_band_solve(DevModal S, const double* __restrict__ Lall,
   __shared__ double rdiag[32];
   const int m = blockIdx.x;
   const int n = S.nsolve[m];
-  const int nb = S.nband, kd = nb - 1;
-  const double* L = Lall + static_cast<size_t>(m) * S.ns_stride * nb;
+  const int nb = S.nbp, kd = S.nband - 1;
+  const double* L = Lall + static_cast<size_t>(m) * S.mode_stride;
   const int nr = (nz > 1 && m > 0) ? 2 : 1;
   double* z0 = R + static_cast<size_t>(plane_of(m, 0)) * rstride;
   double* z1 = R + static_cast<size_t>(plane_of(m, 1)) * rstride;
@@ -450,6 +450,202 @@ __global__ void k_pcg_tail(PcgScalars* sc, const double* rho1, const double* r2,
   sc[k].r2 = r2[k];
 }
 
+
+// ---------------------------------------------------------------------------
+// Pipelined banded sweep.  Same contract as k_band_solve.  The factor rows of
+// a 16-row block are contiguous in HBM, so one bulk (TMA) copy per block and
+// one for the block's inverse diagonal move them into a shared-memory ring of
+// `stages` buffers, issued `stages` blocks ahead and completed on an mbarrier
+// per buffer.  The solved entries live in a shared-memory window of W
+// (power of two >= kd + 16) columns per RHS.  Per block: all warps form
+// acc = c - L_far z_far from shared memory, then z_B = T_B^{-1} acc with the
+// precomputed inverse of the block's triangle.  Waits are bounded: on
+// expiry the kernel records an error in S.status and stops.
+// ---------------------------------------------------------------------------
+
+__device__ __forceinline__ uint32_t smem_u32(const void* p) {
+  return static_cast<uint32_t>(__cvta_generic_to_shared(p));
+}
+
+__device__ __forceinline__ void mbar_init(uint64_t* bar, unsigned count) {
+  asm volatile("mbarrier.init.shared::cta.b64 [%0], %1;" ::"r"(smem_u32(bar)), "r"(count));
+}
+
+__device__ __forceinline__ void mbar_expect_tx(uint64_t* bar, unsigned bytes) {
+  asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;" ::"r"(smem_u32(bar)),
+               "r"(bytes)
+               : "memory");
+}
+
+__device__ __forceinline__ void bulk_g2s(void* dst, const void* src, unsigned bytes, uint64_t* bar) {
+  asm volatile(
+      "cp.async.bulk.shared::cluster.global.mbarrier::complete_tx::bytes [%0], [%1], %2, [%3];" ::"r"(
+          smem_u32(dst)),
+      "l"(src), "r"(bytes), "r"(smem_u32(bar))
+      : "memory");
+}
+
+__device__ __forceinline__ unsigned long long global_ns() {
+  unsigned long long t;
+  asm volatile("mov.u64 %0, %%globaltimer;" : "=l"(t));
+  return t;
+}
+
+// Bounded wait (about 2 s of wall time) for phase `parity` of an mbarrier;
+// false if the bound expired.
+__device__ __forceinline__ bool mbar_wait(uint64_t* bar, unsigned parity) {
+  const uint32_t a = smem_u32(bar);
+  const unsigned long long t0 = global_ns();
+  for (;;) {
+    uint32_t done;
+    asm volatile(
+        "{\n .reg .pred p;\n mbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2;\n"
+        " selp.u32 %0, 1, 0, p;\n}\n"
+        : "=r"(done)
+        : "r"(a), "r"(parity)
+        : "memory");
+    if (done) return true;
+    if (global_ns() - t0 > 2000000000ull) return false;
+  }
+}
+
+constexpr int kSweepThreads = 256;
+
+__global__ void __launch_bounds__(kSweepThreads) k_band_sweep(DevModal S, const double* __restrict__ Lall,
+                                                              const double* __restrict__ Dall,
+                                                              double* __restrict__ R, int rstride, int nz,
+                                                              int reversed, int stages, int W) {
+  constexpr int B = kBandRows;
+  extern __shared__ __align__(128) unsigned char smraw[];
+  const int m = blockIdx.x;
+  const int n = S.nsolve[m];
+  const int nbp = S.nbp, kd = S.nband - 1;
+  const size_t stage_doubles = static_cast<size_t>(B) * nbp + B * B;
+  uint64_t* bar = reinterpret_cast<uint64_t*>(smraw);  // [stages], 128-byte slot
+  double* ring = reinterpret_cast<double*>(smraw + 128);
+  double* win0 = ring + stage_doubles * stages;
+  double* win1 = win0 + W;
+  double* acc = win1 + W;  // [B][2]
+  __shared__ int failed;
+  const double* L = Lall + static_cast<size_t>(m) * S.mode_stride;
+  const double* Dv = Dall + static_cast<size_t>(m) * S.dinv_stride;
+  const int nr = (nz > 1 && m > 0) ? 2 : 1;
+  double* z0 = R + static_cast<size_t>(2 * m) * rstride;
+  double* z1 = R + static_cast<size_t>(2 * m + 1) * rstride;
+  const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
+  const int nblk = (n + B - 1) / B;
+  auto at = [&](int r) { return reversed ? n - 1 - r : r; };
+  auto issue = [&](int b) {
+    const int j0 = b * B;
+    const int bn = min(B, n - j0);
+    double* dst = ring + static_cast<size_t>(b % stages) * stage_doubles;
+    const unsigned rows_bytes = static_cast<unsigned>(bn) * nbp * 8u;
+    mbar_expect_tx(&bar[b % stages], rows_bytes + B * B * 8u);
+    bulk_g2s(dst, L + static_cast<size_t>(j0) * nbp, rows_bytes, &bar[b % stages]);
+    bulk_g2s(dst + static_cast<size_t>(B) * nbp, Dv + static_cast<size_t>(b) * B * B, B * B * 8u,
+             &bar[b % stages]);
+  };
+  if (tid == 0) {
+    failed = 0;
+    for (int s = 0; s < stages; ++s) mbar_init(&bar[s], 1);
+    asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
+  }
+  __syncthreads();
+  if (tid == 0)
+    for (int b = 0; b < min(stages, nblk); ++b) issue(b);
+  for (int b = 0; b < nblk; ++b) {
+    const int j0 = b * B;
+    const int bn = min(B, n - j0);
+    const double* Lb = ring + static_cast<size_t>(b % stages) * stage_doubles;
+    const double* Tinv = Lb + static_cast<size_t>(B) * nbp;
+    if (!mbar_wait(&bar[b % stages], (b / stages) & 1)) {
+      if (lane == 0) {
+        failed = 1;
+        atomicExch(S.status, 1);
+      }
+    }
+    __syncthreads();
+    if (failed) break;
+    // -- far contributions: columns < j0, all already in the window
+    for (int rr = warp; rr < bn; rr += kSweepThreads / 32) {
+      const int j = j0 + rr;
+      const double c0 = lane == 0 ? z0[at(j)] : 0.0;
+      const double c1 = (lane == 0 && nr > 1) ? z1[at(j)] : 0.0;
+      const double* Lr = Lb + static_cast<size_t>(rr) * nbp;
+      const int tlo = max(0, kd - j), thi = kd - rr;
+      double s0 = 0.0, s1 = 0.0;
+      if (nr > 1) {
+        for (int t = tlo + lane; t < thi; t += 32) {
+          const int c = (j - kd + t) & (W - 1);
+          const double l = Lr[t];
+          s0 = fma(l, win0[c], s0);
+          s1 = fma(l, win1[c], s1);
+        }
+      } else {
+        for (int t = tlo + lane; t < thi; t += 32) s0 = fma(Lr[t], win0[(j - kd + t) & (W - 1)], s0);
+      }
+      for (int o = 16; o; o >>= 1) {
+        s0 += __shfl_xor_sync(0xffffffffu, s0, o);
+        s1 += __shfl_xor_sync(0xffffffffu, s1, o);
+      }
+      if (lane == 0) {
+        acc[rr * 2] = c0 - s0;
+        acc[rr * 2 + 1] = c1 - s1;
+      }
+    }
+    __syncthreads();
+    // -- the block's triangle through its precomputed inverse
+    if (tid < B * nr) {
+      const int r = tid / B, rr = tid - r * B;
+      if (rr < bn) {
+        double z = 0.0;
+        for (int s2 = 0; s2 <= rr; ++s2) z = fma(Tinv[rr * B + s2], acc[s2 * 2 + r], z);
+        const int c = (j0 + rr) & (W - 1);
+        if (r == 0) {
+          win0[c] = z;
+          z0[at(j0 + rr)] = z;
+        } else {
+          win1[c] = z;
+          z1[at(j0 + rr)] = z;
+        }
+      }
+    }
+    __syncthreads();
+    if (tid == 0 && b + stages < nblk) {
+      asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
+      issue(b + stages);
+    }
+  }
+  // Drain: make sure no bulk copy into this block's shared memory is still
+  // outstanding before the block exits (only reachable after a failed wait).
+  if (failed && tid == 0)
+    for (int s = 0; s < stages; ++s) {
+      mbar_wait(&bar[s], 0);  // bounded
+      mbar_wait(&bar[s], 1);
+    }
+}
+
+// Shared-memory plan of k_band_sweep for a band row stride; 0 stages if the
+// band is too wide for two buffers.
+struct SweepPlan {
+  int stages = 0, W = 0;
+  size_t smem = 0;
+};
+
+SweepPlan sweep_plan(int nbp, int nband) {
+  SweepPlan p;
+  int W = 64;
+  while (W < nband - 1 + kBandRows) W <<= 1;
+  const size_t stage = sizeof(double) * (static_cast<size_t>(kBandRows) * nbp + kBandRows * kBandRows);
+  const size_t fixed = 128 + sizeof(double) * (2 * static_cast<size_t>(W) + 2 * kBandRows);
+  const size_t limit = 220 * 1024;
+  if (fixed + 2 * stage > limit) return p;
+  p.stages = static_cast<int>(std::min<size_t>(4, (limit - fixed) / stage));
+  p.W = W;
+  p.smem = fixed + stage * p.stages;
+  return p;
+}
+
 }  // namespace
 
 size_t helmholtz_workspace_doubles(const DevGeom& g, const DevNumbering& N) {
@@ -488,9 +684,23 @@ cudaError_t helmholtz_direct_solve(const DevGeom& g, const DevNumbering& N, cons
     k_natural<<<grid, 128, 0, st>>>(g, N, lines, nline, R, rstride, nz);
   }
   if (ev) cudaEventRecord(ev[1], st);
-  k_band_solve<<<S.nmodes, 256, 0, st>>>(S, S.fwd, R, rstride, nz, 0);
-  if (ev) cudaEventRecord(ev[2], st);
-  k_band_solve<<<S.nmodes, 256, 0, st>>>(S, S.bwd, R, rstride, nz, 1);
+  const SweepPlan plan = sweep_plan(S.nbp, S.nband);
+  if (plan.stages >= 2) {
+    static int configured = 0;
+    if (!configured) {
+      cudaFuncSetAttribute(k_band_sweep, cudaFuncAttributeMaxDynamicSharedMemorySize, 220 * 1024);
+      configured = 1;
+    }
+    k_band_sweep<<<S.nmodes, kSweepThreads, plan.smem, st>>>(S, S.fwd, S.dinv_fwd, R, rstride, nz, 0,
+                                                             plan.stages, plan.W);
+    if (ev) cudaEventRecord(ev[2], st);
+    k_band_sweep<<<S.nmodes, kSweepThreads, plan.smem, st>>>(S, S.bwd, S.dinv_bwd, R, rstride, nz, 1,
+                                                             plan.stages, plan.W);
+  } else {
+    k_band_solve<<<S.nmodes, 256, 0, st>>>(S, S.fwd, R, rstride, nz, 0);
+    if (ev) cudaEventRecord(ev[2], st);
+    k_band_solve<<<S.nmodes, 256, 0, st>>>(S, S.bwd, R, rstride, nz, 1);
+  }
   if (ev) cudaEventRecord(ev[3], st);
   k_recover<<<egrid, threads, shm + sizeof(double) * g.next, st>>>(g, N, S, F, has_ess ? G : nullptr,
                                                                    rstride, R, rstride, U);

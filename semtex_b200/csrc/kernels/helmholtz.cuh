@@ -7,6 +7,10 @@
 
 namespace stx {
 
+// Rows per block of the pipelined banded sweeps (and of the inverse
+// diagonal blocks the host precomputes for them).
+constexpr int kBandRows = 16;
+
 // Doubles of scratch the direct solve needs: boundary RHS and essential
 // values, one padded globally numbered vector each per plane.
 size_t helmholtz_workspace_doubles(const DevGeom& g, const DevNumbering& N);
