@@ -420,7 +420,7 @@ int stx_modal_create(stx_context* ctx, char field, double lambda2, double beta, 
         // Device band layout: rows padded to an even stride (16-byte rows for
         // bulk copies), modes 256-byte aligned, plus the inverse of every
         // 16x16 diagonal block of each triangular factor.
-        const int nb = N.nband, nbp = (nb + 1) / 2 * 2;
+        const int nb = N.nband, nbp = (nb + 2) / 2 * 2;  // even, >= nb + 1
         const long long mstride = (static_cast<long long>(nsmax) * nbp + 31) / 32 * 32;
         const int nblk = (nsmax + kBandRows - 1) / kBandRows;
         const long long dstride = static_cast<long long>(std::max(1, nblk)) * kBandRows * kBandRows;
@@ -431,11 +431,14 @@ int stx_modal_create(stx_context* ctx, char field, double lambda2, double beta, 
           hbi.insert(hbi.end(), modes[m].hbi.begin(), modes[m].hbi.end());
           hii.insert(hii.end(), modes[m].hii.begin(), modes[m].hii.end());
           const int n = modes[m].nsolve;
-          for (int j = 0; j < n; ++j)
+          // skewed rows: column j-kd+t at position t + ((j-kd) & 1)
+          for (int j = 0; j < n; ++j) {
+            const int off = (j - (nb - 1)) & 1;
             for (int t = 0; t < nb; ++t) {
-              fwd[m * mstride + static_cast<long long>(j) * nbp + t] = modes[m].fwd[static_cast<size_t>(j) * nb + t];
-              bwd[m * mstride + static_cast<long long>(j) * nbp + t] = modes[m].bwd[static_cast<size_t>(j) * nb + t];
+              fwd[m * mstride + static_cast<long long>(j) * nbp + t + off] = modes[m].fwd[static_cast<size_t>(j) * nb + t];
+              bwd[m * mstride + static_cast<long long>(j) * nbp + t + off] = modes[m].bwd[static_cast<size_t>(j) * nb + t];
             }
+          }
           band_block_inverses(modes[m].fwd, n, nb, &dfw[m * dstride]);
           band_block_inverses(modes[m].bwd, n, nb, &dbw[m * dstride]);
           modes[m] = ModeSystem();

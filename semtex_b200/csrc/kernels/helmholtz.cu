@@ -182,7 +182,7 @@ __global__ void k_band_solve(DevModal S, const double* __restrict__ Lall,
     const int bn = min(32, n - j0);
     for (int rr = warp; rr < bn; rr += nwarp) {
       const int j = j0 + rr;
-      const double* Lj = L + static_cast<size_t>(j) * nb;
+      const double* Lj = L + static_cast<size_t>(j) * nb + ((j - kd) & 1);  // skewed row
       const int tlo = max(0, kd - j);
       const int thi = kd - rr;  // columns < j0
       double s0 = 0.0, s1 = 0.0;
@@ -509,29 +509,36 @@ __device__ __forceinline__ bool mbar_wait(uint64_t* bar, unsigned parity) {
   }
 }
 
-constexpr int kSweepThreads = 256;
+constexpr int kSweepWarps = 1 + kBandRows;  // one chain warp + one warp per block row
+constexpr int kSweepThreads = 32 * kSweepWarps;
 
-__global__ void __launch_bounds__(kSweepThreads) k_band_sweep(DevModal S, const double* __restrict__ Lall,
-                                                              const double* __restrict__ Dall,
-                                                              double* __restrict__ R, int rstride, int nz,
-                                                              int reversed, int stages, int W) {
+// Skewed row layout (built on the host): row j holds the coefficients of
+// columns [cs_j, cs_j + nbq) with cs_j = (j - kd) rounded down to even, so
+// that column pairs (2p, 2p+1) are 16-byte aligned in both the factor row
+// and the solution window; entries outside the band are zero.
+__device__ __forceinline__ int skew_start(int j, int kd) {
+  const int c = j - kd;
+  return c - (c & 1);
+}
+
+template <int NR>
+__device__ __forceinline__ void sweep_body(const DevModal& S, const double* __restrict__ Lall,
+                                           const double* __restrict__ Dall, double* __restrict__ R,
+                                           int rstride, int reversed, int stages, int W, int m,
+                                           unsigned char* smraw) {
   constexpr int B = kBandRows;
-  extern __shared__ __align__(128) unsigned char smraw[];
-  const int m = blockIdx.x;
   const int n = S.nsolve[m];
-  const int nbp = S.nbp, kd = S.nband - 1;
-  const size_t stage_doubles = static_cast<size_t>(B) * nbp + B * B;
-  uint64_t* bar = reinterpret_cast<uint64_t*>(smraw);  // [stages], 128-byte slot
+  const int nbq = S.nbp, kd = S.nband - 1;
+  const size_t stage_doubles = static_cast<size_t>(B) * nbq + B * B;
+  uint64_t* bar = reinterpret_cast<uint64_t*>(smraw);  // [stages] in a 128-byte slot
   double* ring = reinterpret_cast<double*>(smraw + 128);
-  double* win0 = ring + stage_doubles * stages;
-  double* win1 = win0 + W;
-  double* acc = win1 + W;  // [B][2]
+  double* win = ring + stage_doubles * stages;  // [NR][W]
+  double* fbuf = win + static_cast<size_t>(NR) * W;  // [2][B][NR] far sums
+  double* cbuf = fbuf + 2 * B * NR;                   // [2][B][NR] right-hand sides
   __shared__ int failed;
   const double* L = Lall + static_cast<size_t>(m) * S.mode_stride;
   const double* Dv = Dall + static_cast<size_t>(m) * S.dinv_stride;
-  const int nr = (nz > 1 && m > 0) ? 2 : 1;
-  double* z0 = R + static_cast<size_t>(2 * m) * rstride;
-  double* z1 = R + static_cast<size_t>(2 * m + 1) * rstride;
+  double* z[2] = {R + static_cast<size_t>(2 * m) * rstride, R + static_cast<size_t>(2 * m + 1) * rstride};
   const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
   const int nblk = (n + B - 1) / B;
   auto at = [&](int r) { return reversed ? n - 1 - r : r; };
@@ -539,90 +546,130 @@ __global__ void __launch_bounds__(kSweepThreads) k_band_sweep(DevModal S, const 
     const int j0 = b * B;
     const int bn = min(B, n - j0);
     double* dst = ring + static_cast<size_t>(b % stages) * stage_doubles;
-    const unsigned rows_bytes = static_cast<unsigned>(bn) * nbp * 8u;
+    const unsigned rows_bytes = static_cast<unsigned>(bn) * nbq * 8u;
     mbar_expect_tx(&bar[b % stages], rows_bytes + B * B * 8u);
-    bulk_g2s(dst, L + static_cast<size_t>(j0) * nbp, rows_bytes, &bar[b % stages]);
-    bulk_g2s(dst + static_cast<size_t>(B) * nbp, Dv + static_cast<size_t>(b) * B * B, B * B * 8u,
+    bulk_g2s(dst, L + static_cast<size_t>(j0) * nbq, rows_bytes, &bar[b % stages]);
+    bulk_g2s(dst + static_cast<size_t>(B) * nbq, Dv + static_cast<size_t>(b) * B * B, B * B * 8u,
              &bar[b % stages]);
   };
+  for (int i = tid; i < NR * W; i += kSweepThreads) win[i] = 0.0;
   if (tid == 0) {
     failed = 0;
-    for (int s = 0; s < stages; ++s) mbar_init(&bar[s], 1);
+    for (int s2 = 0; s2 < stages; ++s2) mbar_init(&bar[s2], 1);
     asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
+  }
+  // block 0: right-hand sides, no far part
+  if (warp >= 1 && lane < NR) {
+    const int rr = warp - 1;
+    cbuf[rr * NR + lane] = rr < min(B, n) ? z[lane][at(rr)] : 0.0;
+    fbuf[rr * NR + lane] = 0.0;
   }
   __syncthreads();
   if (tid == 0)
     for (int b = 0; b < min(stages, nblk); ++b) issue(b);
+  double zprev = 0.0;  // chain warp: z of the previous block, lane = r*16 + rr
   for (int b = 0; b < nblk; ++b) {
     const int j0 = b * B;
-    const int bn = min(B, n - j0);
-    const double* Lb = ring + static_cast<size_t>(b % stages) * stage_doubles;
-    const double* Tinv = Lb + static_cast<size_t>(B) * nbp;
-    if (!mbar_wait(&bar[b % stages], (b / stages) & 1)) {
-      if (lane == 0) {
-        failed = 1;
-        atomicExch(S.status, 1);
+    if (warp == 0) {
+      // ---- chain: z_b = Tinv_b (c_b - far_b - N_b z_{b-1})
+      if (!mbar_wait(&bar[b % stages], (b / stages) & 1)) {
+        if (lane == 0) {
+          failed = 1;
+          atomicExch(S.status, 1);
+        }
+      }
+      __syncwarp();
+      const double* Lb = ring + static_cast<size_t>(b % stages) * stage_doubles;
+      const double* Tinv = Lb + static_cast<size_t>(B) * nbq;
+      const int bn = min(B, n - j0);
+      const int rr = lane & (B - 1), r = lane >> 4;
+      const bool live = rr < bn && r < NR;
+      const int j = j0 + rr;
+      const int cs = skew_start(j, kd);
+      const double* Lr = Lb + static_cast<size_t>(rr) * nbq;
+      double acc = live ? cbuf[(b & 1) * B * NR + rr * NR + r] - fbuf[(b & 1) * B * NR + rr * NR + r] : 0.0;
+      for (int s2 = 0; s2 < B; ++s2) {
+        const double zs = __shfl_sync(0xffffffffu, zprev, (lane & 16) | s2);
+        const int pos = j0 - B + s2 - cs;
+        if (live && pos >= 0) acc = fma(-Lr[pos], zs, acc);
+      }
+      double zb = 0.0;
+      for (int s2 = 0; s2 < B; ++s2) {
+        const double as = __shfl_sync(0xffffffffu, acc, (lane & 16) | s2);
+        if (live && s2 <= rr) zb = fma(Tinv[rr * B + s2], as, zb);
+      }
+      if (live) {
+        win[r * W + ((j0 + rr) & (W - 1))] = zb;
+        z[r][at(j0 + rr)] = zb;
+      }
+      zprev = live ? zb : 0.0;
+    } else if (b + 1 < nblk) {
+      // ---- far part of block b+1: columns < j0(b), rows one per warp
+      const int rr = warp - 1;
+      const int j1 = j0 + B;
+      const int bn1 = min(B, n - j1);
+      if (!mbar_wait(&bar[(b + 1) % stages], ((b + 1) / stages) & 1)) {
+        if (lane == 0) {
+          failed = 1;
+          atomicExch(S.status, 1);
+        }
+      }
+      if (rr < bn1) {
+        const int j = j1 + rr;
+        double c[NR];
+        if (lane == 0)
+          for (int r = 0; r < NR; ++r) c[r] = z[r][at(j)];
+        const double* Lr = ring + static_cast<size_t>((b + 1) % stages) * stage_doubles +
+                           static_cast<size_t>(rr) * nbq;
+        const int cs = skew_start(j, kd);
+        double s0[NR], s1[NR];
+        for (int r = 0; r < NR; ++r) s0[r] = s1[r] = 0.0;
+#pragma unroll 4
+        for (int col = cs + 2 * lane; col < j0; col += 64) {
+          const double2 l = *reinterpret_cast<const double2*>(Lr + (col - cs));
+          const int wi = col & (W - 1);
+          for (int r = 0; r < NR; ++r) {
+            const double2 zz = *reinterpret_cast<const double2*>(win + r * W + wi);
+            s0[r] = fma(l.x, zz.x, s0[r]);
+            s1[r] = fma(l.y, zz.y, s1[r]);
+          }
+        }
+        for (int r = 0; r < NR; ++r) {
+          double v = s0[r] + s1[r];
+          for (int o = 16; o; o >>= 1) v += __shfl_xor_sync(0xffffffffu, v, o);
+          if (lane == 0) {
+            fbuf[((b + 1) & 1) * B * NR + rr * NR + r] = v;
+            cbuf[((b + 1) & 1) * B * NR + rr * NR + r] = c[r];
+          }
+        }
       }
     }
     __syncthreads();
     if (failed) break;
-    // -- far contributions: columns < j0, all already in the window
-    for (int rr = warp; rr < bn; rr += kSweepThreads / 32) {
-      const int j = j0 + rr;
-      const double c0 = lane == 0 ? z0[at(j)] : 0.0;
-      const double c1 = (lane == 0 && nr > 1) ? z1[at(j)] : 0.0;
-      const double* Lr = Lb + static_cast<size_t>(rr) * nbp;
-      const int tlo = max(0, kd - j), thi = kd - rr;
-      double s0 = 0.0, s1 = 0.0;
-      if (nr > 1) {
-        for (int t = tlo + lane; t < thi; t += 32) {
-          const int c = (j - kd + t) & (W - 1);
-          const double l = Lr[t];
-          s0 = fma(l, win0[c], s0);
-          s1 = fma(l, win1[c], s1);
-        }
-      } else {
-        for (int t = tlo + lane; t < thi; t += 32) s0 = fma(Lr[t], win0[(j - kd + t) & (W - 1)], s0);
-      }
-      for (int o = 16; o; o >>= 1) {
-        s0 += __shfl_xor_sync(0xffffffffu, s0, o);
-        s1 += __shfl_xor_sync(0xffffffffu, s1, o);
-      }
-      if (lane == 0) {
-        acc[rr * 2] = c0 - s0;
-        acc[rr * 2 + 1] = c1 - s1;
-      }
-    }
-    __syncthreads();
-    // -- the block's triangle through its precomputed inverse
-    if (tid < B * nr) {
-      const int r = tid / B, rr = tid - r * B;
-      if (rr < bn) {
-        double z = 0.0;
-        for (int s2 = 0; s2 <= rr; ++s2) z = fma(Tinv[rr * B + s2], acc[s2 * 2 + r], z);
-        const int c = (j0 + rr) & (W - 1);
-        if (r == 0) {
-          win0[c] = z;
-          z0[at(j0 + rr)] = z;
-        } else {
-          win1[c] = z;
-          z1[at(j0 + rr)] = z;
-        }
-      }
-    }
-    __syncthreads();
-    if (tid == 0 && b + stages < nblk) {
+    if (tid == 32 && b + stages < nblk) {
       asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
       issue(b + stages);
     }
   }
-  // Drain: make sure no bulk copy into this block's shared memory is still
-  // outstanding before the block exits (only reachable after a failed wait).
   if (failed && tid == 0)
-    for (int s = 0; s < stages; ++s) {
-      mbar_wait(&bar[s], 0);  // bounded
-      mbar_wait(&bar[s], 1);
+    for (int s2 = 0; s2 < stages; ++s2) {
+      mbar_wait(&bar[s2], 0);  // bounded
+      mbar_wait(&bar[s2], 1);
     }
+}
+
+// One block per mode; mode 0 (and every mode when nz == 1) holds one real
+// plane, the others a Re/Im pair that shares each factor read.
+__global__ void __launch_bounds__(kSweepThreads) k_band_sweep(DevModal S, const double* __restrict__ Lall,
+                                                              const double* __restrict__ Dall,
+                                                              double* __restrict__ R, int rstride, int nz,
+                                                              int reversed, int stages, int W) {
+  extern __shared__ __align__(128) unsigned char smraw[];
+  const int m = blockIdx.x;
+  if (nz > 1 && m > 0)
+    sweep_body<2>(S, Lall, Dall, R, rstride, reversed, stages, W, m, smraw);
+  else
+    sweep_body<1>(S, Lall, Dall, R, rstride, reversed, stages, W, m, smraw);
 }
 
 // Shared-memory plan of k_band_sweep for a band row stride; 0 stages if the
@@ -635,9 +682,9 @@ struct SweepPlan {
 SweepPlan sweep_plan(int nbp, int nband) {
   SweepPlan p;
   int W = 64;
-  while (W < nband - 1 + kBandRows) W <<= 1;
+  while (W < nband - 1 + 2 * kBandRows + 2) W <<= 1;
   const size_t stage = sizeof(double) * (static_cast<size_t>(kBandRows) * nbp + kBandRows * kBandRows);
-  const size_t fixed = 128 + sizeof(double) * (2 * static_cast<size_t>(W) + 2 * kBandRows);
+  const size_t fixed = 128 + sizeof(double) * (2 * static_cast<size_t>(W) + 8 * kBandRows);
   const size_t limit = 220 * 1024;
   if (fixed + 2 * stage > limit) return p;
   p.stages = static_cast<int>(std::min<size_t>(4, (limit - fixed) / stage));
