@@ -110,6 +110,22 @@ int stx_field_solve(stx_modal* sys, const double* d_forcing, double* d_unknown, 
 int stx_field_solve_profiled(stx_modal* sys, const double* d_forcing, double* d_unknown,
                              float* phase_ms, int* launches);
 
+/* Field::solve for a DIRECT system that allocates no device memory.
+ * No counterpart in the reference (which has no device memory at all).
+ * For callers that cannot let a library call cudaMalloc after start-up --
+ * hosts whose device memory is owned by their own allocator, or loops that
+ * cannot take the synchronisation an allocation may imply.  The solve
+ * scratch lives in a file-scope device array of 2^20 doubles (8 MiB) that
+ * every GPU loading the library holds until exit; problems needing more
+ * (2 x padded nglobal x nz doubles) are rejected with STX_EINVAL.  The first
+ * call on a device looks up the array's device address (cudaGetSymbolAddress)
+ * and should come before any stream capture.  All calls on a device share
+ * the one array and it keeps the last call's contents (the solve clears what
+ * it accumulates into): calls that overlap on the GPU, e.g. issued on
+ * different streams, race.  Inputs, outputs and BC values are as for
+ * stx_field_solve. */
+int stx_field_solve_noalloc(stx_modal* sys, const double* d_forcing, double* d_unknown);
+
 /* AuxField::transform(sign) (src/auxfield.cpp:1157-1194) in place on nz
  * device planes of plane_size doubles. */
 int stx_transform(stx_context* ctx, double* d_data, int sign);

@@ -43,6 +43,7 @@ SIGNATURES = {
     "stx_field_solve": (_i, [_p, _p, _p, _d, _i, _pi]),
     "stx_transform": (_i, [_p, _p, _i]),
     "stx_field_solve_profiled": (_i, [_p, _p, _p, C.POINTER(C.c_float), _pi]),
+    "stx_field_solve_noalloc": (_i, [_p, _p, _p]),
     "stx_elliptic_solve_host": (_i, [_p, _p, _p]),
     "stx_sync": (_i, [_p]),
     "stx_context_stream": (_i, [_p, C.POINTER(_p)]),

@@ -24,7 +24,7 @@ CXXFLAGS = ["-O3", "-std=c++17", "-fPIC", "-Wall", "-Wno-unused-function"]
 
 def _sources():
     cpp = sorted(glob.glob(os.path.join(CSRC, "host", "*.cpp")))
-    cu = sorted(glob.glob(os.path.join(CSRC, "kernels", "*.cu"))) + [os.path.join(CSRC, "capi.cu")]
+    cu = sorted(glob.glob(os.path.join(CSRC, "kernels", "*.cu"))) + sorted(glob.glob(os.path.join(CSRC, "*.cu")))
     return cpp, cu
 
 

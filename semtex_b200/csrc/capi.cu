@@ -60,6 +60,8 @@ int guarded(F&& f) {
 
 namespace stx {
 
+void set_last_error(const std::string& msg) { g_last_error = msg; }
+
 void* DeviceArena::alloc(size_t bytes) {
   void* p = nullptr;
   if (bytes == 0) bytes = 8;

@@ -40,6 +40,9 @@ struct ModalStore {
 
 void host_dft_forward(std::vector<double>& a, int nz, int n);
 
+// Message returned by stx_last_error() on this thread.
+void set_last_error(const std::string& msg);
+
 }  // namespace stx
 
 struct stx_modal;
