@@ -139,6 +139,30 @@ int stx_elliptic_solve_host(stx_modal* sys, const double* h_forcing, double* h_s
 /* The cudaStream_t all of the context's device work runs on. */
 int stx_context_stream(const stx_context* ctx, void** stream);
 
+/* ---- DNS time stepping: integrate() (dns/integrate.cpp:66-200) ----------
+ * Velocity-correction splitting of order N_TIME with stiffly-stable /
+ * extrapolation coefficients (src/integration.cpp:99-164), Cartesian
+ * coordinates, fields "uvp" (2D) or "uvwp" (N_Z > 1).  advection selects the
+ * nonlinear form as dns -S/-C/-N do (dns/drive.cpp:86-91): 0 skew-symmetric,
+ * 1 alternating skew-symmetric (default), 2 convective, 3 Stokes.  Velocity
+ * Helmholtz systems are DIRECT, with the reference's temporary JACPCG systems
+ * for the first N_TIME-1 steps (dns/integrate.cpp:328-356). */
+int stx_dns_create(stx_context* ctx, int advection, stx_dns** out);
+int stx_dns_destroy(stx_dns* dns);
+/* Domain::restart semantics (src/domain.cpp:123-156): zero the multi-level
+ * storage, step = 0, time = t0, re-evaluate BCs at t0. */
+int stx_dns_restart(stx_dns* dns, double t0);
+/* Set a field from physical-space host data [nz][nel*np*np], forward
+ * transform, zero Nyquist (restart from a .rst file). */
+int stx_dns_set_field(stx_dns* dns, char field, const double* h_phys);
+/* Physical-space copy of a field (Domain::dump's INVERSE transform). */
+int stx_dns_get_field(stx_dns* dns, char field, double* h_phys);
+/* Take nsteps time steps (the while loop of integrate()). */
+int stx_dns_advance(stx_dns* dns, int nsteps);
+int stx_dns_state(const stx_dns* dns, int* step, double* time);
+/* Device pointer of a field's Fourier-space storage (nz x plane_size). */
+int stx_dns_field_ptr(stx_dns* dns, char field, double** d_ptr);
+
 /* Synchronise the context's stream. */
 int stx_sync(stx_context* ctx);
 

@@ -957,7 +957,7 @@ class DNS:
     """
 
     def __init__(self, P: Problem, ic: dict | None = None, t0: float = 0.0,
-                 dealias: bool = False):
+                 dealias: bool = False, advection: int = 1):
         if dealias:
             raise NotImplementedError("3/2-rule products are not in the oracle")
         self.P = P
@@ -987,36 +987,49 @@ class DNS:
         self.Uf = [[np.zeros(shape) for _ in range(self.ncom)] for _ in range(self.nord)]
         self.step, self.time = 0, t0
         self.toggle = 1
+        self.advection = advection          # dns -S/-C/-N (dns/drive.cpp:86-91)
         self.cache = {}
         lam = SS_COEFF[self.nord][0] / (self.dt * self.nu)
         self.vsys = {c: P.modal_systems(c, lam, "DIRECT", self.cache) for c in self.vel}
         self.psys = P.modal_systems(self.pname, 0.0, "DIRECT", self.cache)
 
     def nonlinear(self):
-        """altSkewSymmetric, Cartesian branch (dns/nonlinear.cpp:198-381)."""
+        """Cartesian nonlinear terms (dns/nonlinear.cpp): advection 0 skew-symmetric
+        (:38-190), 1 alternating skew (:198-381), 2 convective (:384-480), 3 Stokes."""
         P = self.P
         U = [self.u[c].copy() for c in self.vel]
         Uphys = [dft_inverse(self.u[c]) for c in self.vel]
+        if self.advection == 1:
+            forms = ("conv",) if self.toggle else ("cons",)
+        elif self.advection == 0:
+            forms = ("conv", "cons")
+        elif self.advection == 2:
+            forms = ("conv",)
+        else:
+            forms = ()
         N = []
         for i in range(self.ncom):
             n = np.zeros_like(U[0])
             for j in range(self.ndim):
-                if self.toggle:
+                if "conv" in forms:
                     if j == 2:
                         tmp = dft_inverse(fourier_grad_z(P, U[i]))
                     else:
                         tmp = grad(P.M, Uphys[i], j)
                     n -= Uphys[j] * tmp
-                else:
+                if "cons" in forms:
                     tmp = Uphys[i] * Uphys[j]
                     if j == 2:
                         tmp = dft_inverse(fourier_grad_z(P, dft_forward(tmp)))
                     else:
                         tmp = grad(P.M, tmp, j)
                     n -= tmp
+            if len(forms) == 2:
+                n *= 0.5
             n = dft_forward(n)
             N.append(smooth(P, self.vel[0], n))
-        self.toggle = 1 - self.toggle
+        if self.advection == 1:
+            self.toggle = 1 - self.toggle
         return U, N
 
     def advance(self, nsteps: int = 1):
@@ -1090,13 +1103,14 @@ def user_functions(S: Session):
     return out
 
 
-def dns_session(path: str, overrides: dict | None = None, nsteps: int | None = None):
+def dns_session(path: str, overrides: dict | None = None, nsteps: int | None = None,
+                advection: int = 1):
     """Run `dns` with the USER solution at t=0 as restart (test/testregress)."""
     S = read_session(path, overrides)
     P = Problem(S)
     funcs = user_functions(S)
     ic = {c: P.evaluate(funcs[c], 0.0) for c in S.fields if c in funcs}
-    D = DNS(P, ic)
+    D = DNS(P, ic, advection=advection)
     D.advance(S.tokens.ivalue("N_STEP") if nsteps is None else nsteps)
     return D
 

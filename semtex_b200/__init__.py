@@ -27,8 +27,8 @@ from .fieldfile import read_field, write_field
 
 DIRECT, JACPCG = STX_DIRECT, STX_JACPCG
 
-__all__ = ["Context", "ModalMatrixSys", "Field", "elliptic", "read_field", "write_field",
-           "FORWARD", "INVERSE", "DIRECT", "JACPCG", "StxError"]
+__all__ = ["Context", "ModalMatrixSys", "Field", "DNS", "elliptic", "dns", "read_field",
+           "write_field", "FORWARD", "INVERSE", "DIRECT", "JACPCG", "StxError"]
 
 
 def _torch():
@@ -264,3 +264,88 @@ def elliptic(session: str, overrides=None, iterative: bool = False, device: int 
     sys_.close()
     ctx.close()
     return u
+
+
+class DNS:
+    """integrate() on the device (dns/integrate.cpp:66-200).
+
+    advection: 0 skew-symmetric, 1 alternating skew-symmetric (default),
+    2 convective, 3 Stokes -- the dns -S / default / -C / -N forms.
+    """
+
+    def __init__(self, ctx: Context, advection: int = 1):
+        self.ctx = ctx
+        self._h = C.c_void_p()
+        check(lib().stx_dns_create(ctx.handle, advection, C.byref(self._h)))
+
+    def close(self):
+        if self._h and self.ctx._h:
+            check(lib().stx_dns_destroy(self._h))
+        self._h = C.c_void_p()
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    def restart(self, fields: dict, t0: float = 0.0):
+        """Set physical-space initial fields {name: [nz, nel, np, np]}."""
+        check(lib().stx_dns_restart(self._h, t0))
+        for c, a in fields.items():
+            a = np.ascontiguousarray(a, dtype=np.float64)
+            check(lib().stx_dns_set_field(self._h, c.encode(), C.c_void_p(a.ctypes.data)))
+
+    def advance(self, nsteps: int):
+        check(lib().stx_dns_advance(self._h, nsteps))
+
+    def field(self, c: str) -> np.ndarray:
+        ctx = self.ctx
+        out = np.empty((ctx.nz, ctx.nel, ctx.np, ctx.np))
+        check(lib().stx_dns_get_field(self._h, c.encode(), C.c_void_p(out.ctypes.data)))
+        return out
+
+    def state(self):
+        s, t = C.c_int(), C.c_double()
+        check(lib().stx_dns_state(self._h, C.byref(s), C.byref(t)))
+        return s.value, t.value
+
+
+def _user_functions(session: str):
+    import re
+    txt = open(session).read()
+    m = re.search(r"<USER>(.*?)</USER>", txt, re.S | re.I)
+    out = {}
+    if m:
+        for ln in m.group(1).splitlines():
+            if "=" in ln:
+                k, v = ln.split("=", 1)
+                out[k.strip()] = v.strip()
+    return out
+
+
+def dns(session: str, overrides=None, nsteps: int | None = None, advection: int = 1, device: int = 0,
+        write: bool = False):
+    """The `dns` driver: restart from ``session.rst`` if present, else from the
+    USER section at t=0 (as `compare` writes it), integrate N_STEP steps and
+    return the physical fields; with ``write`` also write ``session.fld``."""
+    ctx = Context(session, overrides, device)
+    D = DNS(ctx, advection)
+    rst = session + ".rst"
+    t0 = 0.0
+    if os.path.exists(rst):
+        hdr, flds = read_field(rst)
+        t0 = hdr["time"]
+    else:
+        funcs = _user_functions(session)
+        flds = {c: ctx.evaluate(funcs[c], 0.0) for c in ctx.fields if c in funcs}
+    D.restart(flds, t0)
+    D.advance(int(ctx.token("N_STEP")) if nsteps is None else nsteps)
+    out = {c: D.field(c) for c in ctx.fields}
+    step, t = D.state()
+    if write:
+        write_field(session + ".fld", os.path.basename(session), ctx.np, ctx.nz, ctx.nel, step, t,
+                    ctx.token("D_T"), ctx.token("KINVIS"), ctx.token("BETA"), out)
+    D.close()
+    ctx.close()
+    return out, t

@@ -44,6 +44,14 @@ SIGNATURES = {
     "stx_transform": (_i, [_p, _p, _i]),
     "stx_field_solve_profiled": (_i, [_p, _p, _p, C.POINTER(C.c_float), _pi]),
     "stx_field_solve_noalloc": (_i, [_p, _p, _p]),
+    "stx_dns_create": (_i, [_p, _i, C.POINTER(_p)]),
+    "stx_dns_destroy": (_i, [_p]),
+    "stx_dns_restart": (_i, [_p, _d]),
+    "stx_dns_set_field": (_i, [_p, C.c_char, _p]),
+    "stx_dns_get_field": (_i, [_p, C.c_char, _p]),
+    "stx_dns_advance": (_i, [_p, _i]),
+    "stx_dns_state": (_i, [_p, _pi, _pd]),
+    "stx_dns_field_ptr": (_i, [_p, C.c_char, C.POINTER(_p)]),
     "stx_elliptic_solve_host": (_i, [_p, _p, _p]),
     "stx_sync": (_i, [_p]),
     "stx_context_stream": (_i, [_p, C.POINTER(_p)]),

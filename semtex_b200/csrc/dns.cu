@@ -1,0 +1,386 @@
+// DNS velocity-correction time stepping on the device (C ABI stx_dns_*).
+//
+// Host restatement of integrate() (dns/integrate.cpp:66-200): the same
+// multi-level storage Us / Uf rolled by pointer (rollm, src/sem.h:108-122),
+// the same sub-steps in the same order, every field operation a device
+// kernel.  Cartesian coordinates; no body forcing; velocity BCs essential or
+// natural (time-dependent values re-evaluated each step).
+#include <cuda_runtime.h>
+
+#include <algorithm>
+#include <cctype>
+#include <cmath>
+#include <memory>
+#include <cstring>
+#include <map>
+#include <string>
+#include <vector>
+
+#include "../../include/semtex_b200.h"
+#include "kernels/dns_kernels.cuh"
+#include "kernels/helmholtz.cuh"
+#include "stx_internal.hpp"
+
+using namespace stx;
+
+namespace {
+
+const double kSS[4][4] = {{0, 0, 0, 0}, {1.0, -1.0, 0, 0}, {1.5, -2.0, 0.5, 0}, {11.0 / 6.0, -3.0, 1.5, -1.0 / 3.0}};
+const double kEX[4][3] = {{0, 0, 0}, {1.0, 0, 0}, {2.0, -1.0, 0}, {3.0, -3.0, 1.0}};
+
+struct DnsError : std::runtime_error {
+  int code;
+  DnsError(int c, const std::string& m) : std::runtime_error(m), code(c) {}
+};
+
+void ck(cudaError_t e, const char* what) {
+  if (e != cudaSuccess) throw DnsError(STX_ECUDA, std::string(what) + ": " + cudaGetErrorString(e));
+}
+
+void ckstx(int rc) {
+  if (rc != STX_OK) throw DnsError(rc, stx_last_error());
+}
+
+bool depends_on_t(const std::string& expr) {
+  for (size_t i = 0; i < expr.size(); ++i)
+    if (expr[i] == 't' && (i == 0 || !(std::isalnum(static_cast<unsigned char>(expr[i - 1])) || expr[i - 1] == '_')) &&
+        (i + 1 == expr.size() || !(std::isalnum(static_cast<unsigned char>(expr[i + 1])) || expr[i + 1] == '_')))
+      return true;
+  return false;
+}
+
+template <class F>
+int dns_guarded(F&& f) {
+  try {
+    f();
+    set_last_error("");
+    return STX_OK;
+  } catch (const DnsError& e) {
+    set_last_error(e.what());
+    return e.code;
+  } catch (const std::exception& e) {
+    set_last_error(e.what());
+    return STX_ESESSION;
+  }
+}
+
+}  // namespace
+
+struct stx_dns {
+  stx_context* ctx = nullptr;
+  int ncom = 0, ndim = 0, nord = 0, form = 1;
+  double dt = 0, nu = 0, beta = 0, tol = 0;
+  int step_max = 0;
+  int step = 0;
+  double time = 0;
+  int toggle = 1;  // altSkewSymmetric's static switch (dns/nonlinear.cpp:254)
+  std::string names;  // velocity components then pressure
+  DeviceArena arena;
+  size_t fsize = 0;  // doubles per field
+  std::vector<double*> u;                 // [ncom+1] Domain fields (Fourier)
+  std::vector<std::vector<double*>> Us, Uf;  // [nord][ncom]
+  std::vector<double*> Up;                // [ncom] physical velocities
+  double* tmp0 = nullptr;
+  double* tmp1 = nullptr;
+  double* tmp2 = nullptr;
+  double* dsswork = nullptr;
+  std::vector<stx_modal*> vsys;           // DIRECT velocity systems
+  stx_modal* psys = nullptr;
+  std::map<std::pair<char, int>, stx_modal*> pcg;  // temporary JACPCG systems
+  std::vector<char> tdep;                 // per field: BCs depend on t
+  std::vector<int> last_iters;
+};
+
+namespace {
+
+void transform(stx_dns* d, double* f, int sign) {
+  ck(z_transform(f, d->ctx->M.nz, d->ctx->M.plane_size, sign, d->ctx->d_twiddle, nullptr, d->ctx->stream),
+     "transform");
+}
+
+void copy(stx_dns* d, double* dst, const double* src) {
+  ck(cudaMemcpyAsync(dst, src, sizeof(double) * d->fsize, cudaMemcpyDeviceToDevice, d->ctx->stream), "copy");
+}
+
+// Nonlinear terms N(u) into Uf[0], copy of u into Us[0] (dns/nonlinear.cpp).
+void nonlinear(stx_dns* d) {
+  stx_context* ctx = d->ctx;
+  const DevGeom& g = ctx->dg;
+  cudaStream_t st = ctx->stream;
+  const bool z3 = d->ndim == 3;
+  for (int i = 0; i < d->ncom; ++i) {
+    copy(d, d->Us[0][i], d->u[i]);
+    copy(d, d->Up[i], d->u[i]);
+    transform(d, d->Up[i], STX_INVERSE);
+  }
+  int form;  // 0 skew, 1 convective, 2 conservative, -1 Stokes
+  switch (d->form) {
+    case 0: form = 0; break;
+    case 1: form = d->toggle ? 1 : 2; break;
+    case 2: form = 1; break;
+    default: form = -1; break;
+  }
+  const DevNumbering& Nm = ctx->fields.at(d->names[0]).dn;
+  for (int i = 0; i < d->ncom; ++i) {
+    double* N = d->Uf[0][i];
+    if (form < 0) {
+      ck(cudaMemsetAsync(N, 0, sizeof(double) * d->fsize, st), "zero");
+    } else {
+      NonlinearArgs a{};
+      a.U0 = d->Up[0];
+      a.U1 = d->Up[1];
+      a.U2 = z3 ? d->Up[2] : nullptr;
+      a.Ui = d->Up[i];
+      a.N = N;
+      a.form = form;
+      if (z3 && form != 2) {  // u_j grad: w * IFFT(dz U_i)
+        ck(dns_grad_z(g, d->Us[0][i], d->tmp0, d->beta, st), "gradz");
+        transform(d, d->tmp0, STX_INVERSE);
+        a.Tc = d->tmp0;
+      }
+      if (z3 && form != 1) {  // div(uu): IFFT(dz FFT(u_i w))
+        ck(dns_product(g, d->Up[i], d->Up[2], d->tmp2, st), "product");
+        transform(d, d->tmp2, STX_FORWARD);
+        ck(dns_grad_z(g, d->tmp2, d->tmp1, d->beta, st), "gradz");  // not in place
+        transform(d, d->tmp1, STX_INVERSE);
+        a.Tk = d->tmp1;
+      }
+      ck(dns_nonlinear(g, a, st), "nonlinear");
+    }
+    transform(d, N, STX_FORWARD);
+    ck(dns_smooth(g, Nm, N, d->dsswork, st), "smooth");
+  }
+  if (d->form == 1) d->toggle = 1 - d->toggle;
+}
+
+template <class T>
+void rollm(std::vector<std::vector<T>>& u) {
+  if (u.size() < 2) return;
+  std::vector<T> last = u.back();
+  for (size_t i = u.size() - 1; i; --i) u[i] = u[i - 1];
+  u[0] = last;
+}
+
+void solve(stx_dns* d, int idx, double* forcing, stx_modal* sys) {
+  std::vector<int> it(d->ctx->M.nz);
+  int rc = stx_field_solve(sys, forcing, d->u[idx], d->tol, d->step_max, it.data());
+  if (rc == STX_ENOCONV) rc = STX_OK;  // the reference warns and carries on
+  ckstx(rc);
+  if (sys->method == STX_JACPCG) d->last_iters = it;
+}
+
+void advance_one(stx_dns* d) {
+  stx_context* ctx = d->ctx;
+  const DevGeom& g = ctx->dg;
+  cudaStream_t st = ctx->stream;
+  nonlinear(d);
+  d->step += 1;
+  d->time += d->dt;
+  // -- waveProp (dns/integrate.cpp:204-239)
+  const int Je = std::min(d->step, d->nord);
+  for (int i = 0; i < d->ncom; ++i) {
+    CombineArgs a{};
+    a.n = 0;
+    for (int q = 0; q < Je; ++q) {
+      a.c[a.n] = -kSS[Je][q + 1];
+      a.p[a.n++] = d->Us[q][i];
+      a.c[a.n] = kEX[Je][q] * d->dt;
+      a.p[a.n++] = d->Uf[q][i];
+    }
+    a.out = d->u[i];
+    ck(dns_combine(g, a, st), "waveProp");
+  }
+  for (int i = 0; i < d->ncom; ++i) std::swap(d->u[i], d->Us[0][i]);
+  rollm(d->Uf);
+  // -- setPForce: div u^ / dt (dns/integrate.cpp:242-257)
+  ck(dns_divergence(g, d->Us[0][0], d->Us[0][1], d->ndim == 3 ? d->Us[0][2] : nullptr, d->Uf[0][0], d->dt,
+                    d->beta, st),
+     "setPForce");
+  const char pc = d->names[d->ncom];
+  if (d->tdep[d->ncom]) ckstx(stx_field_bc_evaluate(ctx, pc, d->time));
+  solve(d, d->ncom, d->Uf[0][0], d->psys);
+  // -- project (dns/integrate.cpp:260-289)
+  const double alpha = -1.0 / (d->dt * d->nu), bcoef = 1.0 / d->nu;
+  for (int i = 0; i < d->ncom; ++i) {
+    std::swap(d->Us[0][i], d->Uf[0][i]);
+    ck(dns_project(g, d->Uf[0][i], d->u[d->ncom], i < d->ndim ? i : -1, alpha, bcoef, d->beta, st), "project");
+  }
+  for (int i = 0; i < d->ncom; ++i) copy(d, d->Us[0][i], d->u[i]);
+  rollm(d->Us);
+  // -- velocity BCs, viscous substep (dns/integrate.cpp:177-193, 328-356)
+  for (int i = 0; i < d->ncom; ++i)
+    if (d->tdep[i]) ckstx(stx_field_bc_evaluate(ctx, d->names[i], d->time));
+  for (int i = 0; i < d->ncom; ++i) {
+    stx_modal* sys = d->vsys[i];
+    if (d->step < d->nord) {
+      const auto key = std::make_pair(d->names[i], Je);
+      auto itp = d->pcg.find(key);
+      if (itp == d->pcg.end()) {
+        stx_modal* m = nullptr;
+        const double lam = kSS[Je][0] / (d->dt * d->nu);
+        ckstx(stx_modal_create(ctx, d->names[i], lam, d->beta, 0, (ctx->M.nz + 1) / 2, STX_JACPCG, &m));
+        itp = d->pcg.emplace(key, m).first;
+      }
+      sys = itp->second;
+    }
+    solve(d, i, d->Uf[0][i], sys);
+  }
+}
+
+}  // namespace
+
+extern "C" {
+
+int stx_dns_create(stx_context* ctx, int advection, stx_dns** out) {
+  return dns_guarded([&] {
+    if (!ctx || !out) throw DnsError(STX_EINVAL, "null argument");
+    if (advection < 0 || advection > 3) throw DnsError(STX_EINVAL, "advection must be 0..3");
+    *out = nullptr;
+    auto d = new stx_dns();
+    std::unique_ptr<stx_dns> guard(d);
+    d->ctx = ctx;
+    const Session& S = ctx->S;
+    d->names = S.fields;
+    if (d->names.size() < 3) throw DnsError(STX_ESESSION, "dns needs velocity fields and pressure");
+    d->ncom = static_cast<int>(d->names.size()) - 1;
+    d->ndim = ctx->M.nz > 1 ? 3 : 2;
+    if (d->ndim == 3 && d->ncom != 3) throw DnsError(STX_ESESSION, "3D needs fields u v w p");
+    d->nord = S.tokens.ivalue("N_TIME");
+    if (d->nord < 1 || d->nord > 3) throw DnsError(STX_ESESSION, "N_TIME must be 1..3");
+    d->dt = S.tokens.value("D_T");
+    d->nu = S.tokens.value("KINVIS");
+    d->beta = S.tokens.value("BETA");
+    d->tol = S.tokens.value("TOL_REL");
+    d->step_max = S.tokens.ivalue("STEP_MAX");
+    d->form = advection;
+    cudaSetDevice(ctx->device);
+    const DevGeom& g = ctx->dg;
+    d->fsize = static_cast<size_t>(g.nz) * g.plane_size;
+    const int nfield = (d->ncom + 1) + 2 * d->nord * d->ncom + d->ncom + 3;
+    double* base = static_cast<double*>(d->arena.alloc(sizeof(double) * d->fsize * nfield));
+    ck(cudaMemset(base, 0, sizeof(double) * d->fsize * nfield), "memset");
+    int k = 0;
+    for (int i = 0; i <= d->ncom; ++i) d->u.push_back(base + d->fsize * k++);
+    d->Us.assign(d->nord, {});
+    d->Uf.assign(d->nord, {});
+    for (int q = 0; q < d->nord; ++q)
+      for (int i = 0; i < d->ncom; ++i) {
+        d->Us[q].push_back(base + d->fsize * k++);
+        d->Uf[q].push_back(base + d->fsize * k++);
+      }
+    for (int i = 0; i < d->ncom; ++i) d->Up.push_back(base + d->fsize * k++);
+    d->tmp0 = base + d->fsize * k++;
+    d->tmp1 = base + d->fsize * k++;
+    d->tmp2 = base + d->fsize * k++;
+    size_t ws = 0;
+    for (char c : d->names) ws = std::max(ws, dns_smooth_workspace_doubles(g, ctx->fields.at(c).dn));
+    d->dsswork = static_cast<double*>(d->arena.alloc(sizeof(double) * ws));
+    for (char c : d->names) {
+      bool td = false;
+      for (const auto& E : ctx->fields.at(c).N.edges) td = td || depends_on_t(E.expr);
+      d->tdep.push_back(td);
+    }
+    // -- preSolve (dns/integrate.cpp:292-325)
+    const double lam = kSS[d->nord][0] / (d->dt * d->nu);
+    const int nmodes = (ctx->M.nz + 1) / 2;
+    for (int i = 0; i < d->ncom; ++i) {
+      stx_modal* m = nullptr;
+      ckstx(stx_modal_create(ctx, d->names[i], lam, d->beta, 0, nmodes, STX_DIRECT, &m));
+      d->vsys.push_back(m);
+    }
+    ckstx(stx_modal_create(ctx, d->names[d->ncom], 0.0, d->beta, 0, nmodes, STX_DIRECT, &d->psys));
+    *out = guard.release();
+  });
+}
+
+int stx_dns_destroy(stx_dns* d) {
+  return dns_guarded([&] {
+    if (!d) return;
+    cudaSetDevice(d->ctx->device);
+    cudaStreamSynchronize(d->ctx->stream);
+    for (auto* m : d->vsys) stx_modal_destroy(m);
+    if (d->psys) stx_modal_destroy(d->psys);
+    for (auto& kv : d->pcg) stx_modal_destroy(kv.second);
+    delete d;
+  });
+}
+
+int stx_dns_restart(stx_dns* d, double t0) {
+  return dns_guarded([&] {
+    if (!d) throw DnsError(STX_EINVAL, "null argument");
+    cudaSetDevice(d->ctx->device);
+    for (int q = 0; q < d->nord; ++q)
+      for (int i = 0; i < d->ncom; ++i) {
+        ck(cudaMemsetAsync(d->Us[q][i], 0, sizeof(double) * d->fsize, d->ctx->stream), "zero");
+        ck(cudaMemsetAsync(d->Uf[q][i], 0, sizeof(double) * d->fsize, d->ctx->stream), "zero");
+      }
+    d->step = 0;
+    d->time = t0;
+    for (char c : d->names) ckstx(stx_field_bc_evaluate(d->ctx, c, t0));
+  });
+}
+
+int stx_dns_set_field(stx_dns* d, char field, const double* h_phys) {
+  return dns_guarded([&] {
+    if (!d || !h_phys) throw DnsError(STX_EINVAL, "null argument");
+    const size_t idx = d->names.find(field);
+    if (idx == std::string::npos) throw DnsError(STX_EINVAL, std::string("no field ") + field);
+    const Mesh& M = d->ctx->M;
+    cudaSetDevice(d->ctx->device);
+    double* f = d->u[idx];
+    ck(cudaMemsetAsync(f, 0, sizeof(double) * d->fsize, d->ctx->stream), "zero");
+    for (int k = 0; k < M.nz; ++k)
+      ck(cudaMemcpyAsync(f + static_cast<size_t>(k) * M.plane_size, h_phys + static_cast<size_t>(k) * M.nplane,
+                         sizeof(double) * M.nplane, cudaMemcpyHostToDevice, d->ctx->stream),
+         "upload");
+    transform(d, f, STX_FORWARD);
+    if (M.nz > 1) ck(cudaMemsetAsync(f + M.plane_size, 0, sizeof(double) * M.plane_size, d->ctx->stream), "nyq");
+    ck(cudaStreamSynchronize(d->ctx->stream), "sync");
+  });
+}
+
+int stx_dns_get_field(stx_dns* d, char field, double* h_phys) {
+  return dns_guarded([&] {
+    if (!d || !h_phys) throw DnsError(STX_EINVAL, "null argument");
+    const size_t idx = d->names.find(field);
+    if (idx == std::string::npos) throw DnsError(STX_EINVAL, std::string("no field ") + field);
+    const Mesh& M = d->ctx->M;
+    cudaSetDevice(d->ctx->device);
+    copy(d, d->tmp0, d->u[idx]);
+    if (M.nz > 1) ck(cudaMemsetAsync(d->tmp0 + M.plane_size, 0, sizeof(double) * M.plane_size, d->ctx->stream), "nyq");
+    transform(d, d->tmp0, STX_INVERSE);
+    for (int k = 0; k < M.nz; ++k)
+      ck(cudaMemcpyAsync(h_phys + static_cast<size_t>(k) * M.nplane, d->tmp0 + static_cast<size_t>(k) * M.plane_size,
+                         sizeof(double) * M.nplane, cudaMemcpyDeviceToHost, d->ctx->stream),
+         "download");
+    ck(cudaStreamSynchronize(d->ctx->stream), "sync");
+  });
+}
+
+int stx_dns_advance(stx_dns* d, int nsteps) {
+  return dns_guarded([&] {
+    if (!d || nsteps < 0) throw DnsError(STX_EINVAL, "bad argument");
+    cudaSetDevice(d->ctx->device);
+    for (int s = 0; s < nsteps; ++s) advance_one(d);
+    ck(cudaGetLastError(), "advance");
+  });
+}
+
+int stx_dns_state(const stx_dns* d, int* step, double* time) {
+  return dns_guarded([&] {
+    if (!d) throw DnsError(STX_EINVAL, "null argument");
+    if (step) *step = d->step;
+    if (time) *time = d->time;
+  });
+}
+
+int stx_dns_field_ptr(stx_dns* d, char field, double** d_ptr) {
+  return dns_guarded([&] {
+    if (!d || !d_ptr) throw DnsError(STX_EINVAL, "null argument");
+    const size_t idx = d->names.find(field);
+    if (idx == std::string::npos) throw DnsError(STX_EINVAL, std::string("no field ") + field);
+    *d_ptr = d->u[idx];
+  });
+}
+
+}  // extern "C"
