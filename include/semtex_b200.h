@@ -102,6 +102,12 @@ int stx_modal_info(const stx_modal* sys, int mode, int* nsolve, int* nband);
 int stx_field_solve(stx_modal* sys, const double* d_forcing, double* d_unknown, double tol_rel,
                     int step_max, int* iterations);
 
+/* Algorithmic bytes one DIRECT solve of this system must move, per phase of
+ * stx_field_solve_profiled: bytes[4] = [element condensation, skeleton
+ * solve (first half), skeleton solve (second half), element recovery].
+ * Every matrix and field counted once. */
+int stx_modal_bytes(const stx_modal* sys, double* bytes);
+
 /* Field::solve for a DIRECT system with CUDA events recorded on the
  * context stream between its phases; synchronises and returns the device
  * milliseconds of [constrain+condense, forward band sweep, backward band

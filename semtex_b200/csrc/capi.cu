@@ -6,6 +6,7 @@
 // print-and-exit (veclib/util.c:24-46).
 #include <cuda_runtime.h>
 
+#include <algorithm>
 #include <cmath>
 #include <cstring>
 #include <map>
@@ -194,6 +195,32 @@ int stx_context_create(const char* session_path, const char* overrides, int devi
     g.emap = upload(A, M.emap);
     g.pmap = upload(A, M.pmap);
     g.family = upload(A, M.family);
+    {
+      // chunks of up to 32 same-family elements (fewer when the recovery
+      // kernel's shared-memory plan would exceed 200 KB)
+      int cm = 32;
+      auto need = [&](int c) {  // shared memory of the batched recovery kernel
+        return sizeof(double) * (2 * static_cast<size_t>(c) * (M.npnp | 1) + 2 * static_cast<size_t>(c) * (M.next | 1) +
+                                 24 * M.npnp + M.np * M.np);
+      };
+      while (cm > 1 && need(cm) > 200 * 1024) cm /= 2;
+      std::vector<int> sorted(M.nel);
+      for (int e = 0; e < M.nel; ++e) sorted[e] = e;
+      std::stable_sort(sorted.begin(), sorted.end(), [&](int a, int b) { return M.family[a] < M.family[b]; });
+      std::vector<int> cstart, ccount;
+      for (int i = 0; i < M.nel;) {
+        int j = i;
+        while (j < M.nel && j - i < cm && M.family[sorted[j]] == M.family[sorted[i]]) ++j;
+        cstart.push_back(i);
+        ccount.push_back(j - i);
+        i = j;
+      }
+      g.nchunk = static_cast<int>(cstart.size());
+      g.chunk_max = cm;
+      g.chunk_start = upload(A, cstart);
+      g.chunk_count = upload(A, ccount);
+      g.elem_sorted = upload(A, sorted);
+    }
     std::vector<double> tw(2 * std::max(1, M.nz));
     for (int m = 0; m < M.nz; ++m) {
       tw[m] = std::cos(2.0 * M_PI * m / M.nz);
@@ -381,6 +408,8 @@ int stx_modal_create(stx_context* ctx, char field, double lambda2, double beta, 
     if (!sys->store) {
       auto st = std::make_shared<ModalStore>();
       const Mesh& M = ctx->M;
+      const Patching* P = nullptr;
+      if (method == STX_DIRECT) P = ctx->patching(field);
       std::vector<ModeSystem> modes(num_modes);
       std::vector<std::string> errs(num_modes);
       unsigned nth = std::max(1u, std::min<unsigned>(std::thread::hardware_concurrency(), num_modes));
@@ -390,7 +419,7 @@ int stx_modal_create(stx_context* ctx, char field, double lambda2, double beta, 
           for (int m = static_cast<int>(w); m < num_modes; m += nth) {
             try {
               const double bk = beta * (base_mode + m);
-              modes[m] = build_mode_system(M, N, lambda2, bk * bk, method);
+              modes[m] = build_mode_system(M, N, P, lambda2, bk * bk, method);
             } catch (const std::exception& e) {
               errs[m] = e.what();
             }
@@ -410,7 +439,8 @@ int stx_modal_create(stx_context* ctx, char field, double lambda2, double beta, 
       for (int m = 0; m < num_modes; ++m) {
         lam[m] = modes[m].lambda2;
         bk2[m] = modes[m].betak2;
-        ns[m] = modes[m].nsolve;
+        // skeleton unknowns of the mode (the pinned node excluded)
+        ns[m] = P ? (modes[m].singular ? N.nsolve - 1 : N.nsolve) : modes[m].nsolve;
         nsmax = std::max(nsmax, ns[m]);
       }
       st->nsolve = ns;
@@ -418,7 +448,47 @@ int stx_modal_create(stx_context* ctx, char field, double lambda2, double beta, 
       d.lambda2 = upload(st->arena, lam);
       d.betak2 = upload(st->arena, bk2);
       d.nsolve = upload(st->arena, ns);
-      if (method == STX_DIRECT) {
+      d.l2 = 0;
+      if (method == STX_DIRECT && P) {
+        std::vector<double> hbi, hii, sinv, g, gt, ainv;
+        std::vector<int> pin(num_modes, -1);
+        for (int m = 0; m < num_modes; ++m) {
+          hbi.insert(hbi.end(), modes[m].hbi.begin(), modes[m].hbi.end());
+          hii.insert(hii.end(), modes[m].hii.begin(), modes[m].hii.end());
+          sinv.insert(sinv.end(), modes[m].l2_sinv.begin(), modes[m].l2_sinv.end());
+          g.insert(g.end(), modes[m].l2_g.begin(), modes[m].l2_g.end());
+          gt.insert(gt.end(), modes[m].l2_gt.begin(), modes[m].l2_gt.end());
+          ainv.insert(ainv.end(), modes[m].l2_ainv.begin(), modes[m].l2_ainv.end());
+          pin[m] = modes[m].pin_iid;
+          modes[m] = ModeSystem();
+        }
+        d.l2 = 1;
+        d.npatch = P->npatch;
+        d.pfam = P->nfamily;
+        d.nI_max = P->nI_max;
+        d.nB_max = P->nB_max;
+        d.niface = P->niface;
+        d.p_family = upload(st->arena, P->family);
+        d.p_nI = upload(st->arena, P->nI);
+        d.p_nB = upload(st->arena, P->nB);
+        d.p_Igid = upload(st->arena, P->I_gid);
+        d.p_Biid = upload(st->arena, P->B_iid);
+        d.skel_of = upload(st->arena, P->skel_of.empty() ? std::vector<int>{0} : P->skel_of);
+        d.pin = upload(st->arena, pin);
+        d.hbi = upload(st->arena, hbi);
+        d.hii = upload(st->arena, hii);
+        d.l2_sinv = upload(st->arena, sinv);
+        d.l2_g = upload(st->arena, g);
+        d.l2_gt = upload(st->arena, gt);
+        d.l2_ainv = upload(st->arena, ainv.empty() ? std::vector<double>{0.0} : ainv);
+        d.fwd = d.bwd = d.dinv_fwd = d.dinv_bwd = nullptr;
+        d.nbp = 0;
+        d.mode_stride = d.dinv_stride = 0;
+        d.status = static_cast<int*>(st->arena.alloc(sizeof(int)));
+        cuda_check(cudaMemset(d.status, 0, sizeof(int)), "status");
+        d.pc = nullptr;
+        d.npts = 0;
+      } else if (method == STX_DIRECT) {
         // Device band layout: rows padded to an even stride (16-byte rows for
         // bulk copies), modes 256-byte aligned, plus the inverse of every
         // 16x16 diagonal block of each triangular factor.
@@ -504,7 +574,7 @@ int stx_field_solve(stx_modal* sys, const double* d_forcing, double* d_unknown, 
     FieldDev& F = ctx->fields.at(sys->field);
     cudaSetDevice(ctx->device);
     if (sys->method == STX_DIRECT) {
-      double* work = ctx->workspace(helmholtz_workspace_doubles(ctx->dg, F.dn));
+      double* work = ctx->workspace(helmholtz_workspace_doubles(ctx->dg, F.dn, sys->store->dm));
       cuda_check(helmholtz_direct_solve(ctx->dg, F.dn, sys->store->dm, d_forcing, d_unknown,
                                         F.d_lines, F.nline, work, ctx->stream),
                  "direct solve");
@@ -531,7 +601,7 @@ int stx_field_solve_profiled(stx_modal* sys, const double* d_forcing, double* d_
     cudaSetDevice(ctx->device);
     cudaEvent_t ev[5];
     for (auto& e : ev) cuda_check(cudaEventCreate(&e), "event");
-    double* work = ctx->workspace(helmholtz_workspace_doubles(ctx->dg, F.dn));
+    double* work = ctx->workspace(helmholtz_workspace_doubles(ctx->dg, F.dn, sys->store->dm));
     cudaError_t err = helmholtz_direct_solve(ctx->dg, F.dn, sys->store->dm, d_forcing, d_unknown,
                                              F.d_lines, F.nline, work, ctx->stream, ev);
     if (err == cudaSuccess) err = cudaEventSynchronize(ev[4]);
@@ -539,7 +609,42 @@ int stx_field_solve_profiled(stx_modal* sys, const double* d_forcing, double* d_
     for (auto& e : ev) cudaEventDestroy(e);
     cuda_check(err, "profiled solve");
     check_sweep_status(sys);
-    if (launches) *launches = helmholtz_direct_launches(F.dn, ctx->M.np);
+    if (launches) *launches = helmholtz_direct_launches(F.dn, sys->store->dm, ctx->M.np);
+  });
+}
+
+int stx_modal_bytes(const stx_modal* sys, double* bytes) {
+  return guarded([&] {
+    if (!sys || !bytes) throw StxError(STX_EINVAL, "null argument");
+    const stx_context* ctx = sys->ctx;
+    const Mesh& M = ctx->M;
+    const DevModal& d = sys->store->dm;
+    const double w = 8.0;
+    const int nz = M.nz, nm = d.nmodes;
+    const int solved = nz > 1 ? nz - 1 : 1;
+    const double field = w * static_cast<double>(M.nplane) * solved;
+    const double rhs = w * ctx->fields.at(sys->field).N.nglobal * solved;
+    const double fam = w * d.nfamily * nm;
+    // element condensation: forcing in, condensation matrix per family and
+    // mode, skeleton RHS out; recovery: forcing and skeleton values in,
+    // solution out, both condensation matrices
+    bytes[0] = field + fam * M.next * M.nint + rhs;
+    bytes[3] = 2 * field + fam * (M.next * M.nint + static_cast<double>(M.nint) * M.nint) + rhs;
+    if (d.l2) {
+      const Patching* P = ctx->fields.at(sys->field).P.get();
+      double pm = 0;
+      for (int f = 0; f < P->nfamily; ++f) {
+        const int p = P->family_rep[f];
+        pm += static_cast<double>(P->nI[p]) * P->nI[p] + 2.0 * P->nI[p] * P->nB[p];
+      }
+      bytes[1] = w * nm * (pm + static_cast<double>(d.niface) * d.niface) + 4 * rhs;
+      bytes[2] = 0.0;
+    } else {
+      double band = 0;
+      for (int m = 0; m < nm; ++m) band += w * static_cast<double>(sys->store->nsolve[m]) * d.nband;
+      bytes[1] = band + rhs;
+      bytes[2] = band + rhs;
+    }
   });
 }
 

@@ -72,7 +72,96 @@ void element_helmholtz(const Mesh& M, int e, double lambda2, double betak2, doub
     }
 }
 
-ModeSystem build_mode_system(const Mesh& M, const Numbering& N, double lambda2,
+namespace {
+
+// Banded Cholesky A = U^T U in place, A[j*nb + t] = A(j-kd+t, j) (dpbtrf "U"),
+// then the two row layouts the device sweeps read.
+void factor_band(std::vector<double>& A, int ns, int nb, ModeSystem& S) {
+  const int kd = nb - 1;
+  for (int j = 0; j < ns; ++j) {
+    double* cj = &A[static_cast<size_t>(j) * nb];
+    const int i0 = std::max(0, j - kd);
+    for (int i = i0; i < j; ++i) {
+      const double* ci = &A[static_cast<size_t>(i) * nb];
+      double s = cj[kd - (j - i)];
+      const int k0 = std::max(i0, i - kd);
+      for (int k = k0; k < i; ++k) s -= ci[kd - (i - k)] * cj[kd - (j - k)];
+      cj[kd - (j - i)] = s / ci[kd];
+    }
+    double d = cj[kd];
+    for (int k = i0; k < j; ++k) d -= cj[kd - (j - k)] * cj[kd - (j - k)];
+    if (!(d > 0.0))
+      throw std::runtime_error("failed to factor Helmholtz matrix (not positive definite)");
+    cj[kd] = std::sqrt(d);
+  }
+  S.fwd.assign(static_cast<size_t>(ns) * nb, 0.0);
+  S.bwd.assign(static_cast<size_t>(ns) * nb, 0.0);
+  for (int j = 0; j < ns; ++j)
+    for (int t = 0; t < nb; ++t) {
+      double v = A[static_cast<size_t>(j) * nb + t];
+      if (j - kd + t < 0) v = 0.0;
+      S.fwd[static_cast<size_t>(j) * nb + t] = (t == kd) ? 1.0 / v : v;
+    }
+  for (int r = 0; r < ns; ++r) {
+    const int i = ns - 1 - r;
+    for (int t = 0; t < nb; ++t) {
+      const int c = i + kd - t;
+      double v = 0.0;
+      if (c < ns) v = A[static_cast<size_t>(c) * nb + kd - (c - i)];
+      S.bwd[static_cast<size_t>(r) * nb + t] = (t == kd) ? 1.0 / v : v;
+    }
+  }
+}
+
+}  // namespace
+
+void spd_inverse(int n, double* A) {
+  // A = L L^T (lower, in place)
+  for (int j = 0; j < n; ++j) {
+    double* aj = A + static_cast<size_t>(j) * n;
+    double d = aj[j];
+    for (int k = 0; k < j; ++k) d -= aj[k] * aj[k];
+    if (!(d > 0.0)) throw std::runtime_error("failed to factor Helmholtz matrix (not positive definite)");
+    d = std::sqrt(d);
+    aj[j] = d;
+    const double inv = 1.0 / d;
+    for (int i = j + 1; i < n; ++i) {
+      double* ai = A + static_cast<size_t>(i) * n;
+      double s = ai[j];
+      for (int k = 0; k < j; ++k) s -= ai[k] * aj[k];
+      ai[j] = s * inv;
+    }
+  }
+  // W = L^{-1} (lower), stored transposed in the upper triangle as rows of W^T
+  std::vector<double> W(static_cast<size_t>(n) * n, 0.0);  // W[i][j], j <= i
+  for (int i = 0; i < n; ++i) {
+    const double* ai = A + static_cast<size_t>(i) * n;
+    double* wi = &W[static_cast<size_t>(i) * n];
+    wi[i] = 1.0 / ai[i];
+    for (int j = 0; j < i; ++j) {
+      // W[i][j] = -(sum_{k=j}^{i-1} L[i][k] W[k][j]) / L[i][i]
+      double s = 0.0;
+      for (int k = j; k < i; ++k) s += ai[k] * W[static_cast<size_t>(k) * n + j];
+      wi[j] = -s * wi[i];
+    }
+  }
+  // A^{-1} = W^T W : (i,j) = sum_{k >= max(i,j)} W[k][i] W[k][j]
+  std::vector<double> WT(static_cast<size_t>(n) * n, 0.0);  // WT[i][k] = W[k][i]
+  for (int k = 0; k < n; ++k)
+    for (int i = 0; i <= k; ++i) WT[static_cast<size_t>(i) * n + k] = W[static_cast<size_t>(k) * n + i];
+  for (int i = 0; i < n; ++i) {
+    const double* ti = &WT[static_cast<size_t>(i) * n];
+    for (int j = i; j < n; ++j) {
+      const double* tj = &WT[static_cast<size_t>(j) * n];
+      double s = 0.0;
+      for (int k = j; k < n; ++k) s += ti[k] * tj[k];
+      A[static_cast<size_t>(i) * n + j] = s;
+      A[static_cast<size_t>(j) * n + i] = s;
+    }
+  }
+}
+
+ModeSystem build_mode_system(const Mesh& M, const Numbering& N, const Patching* P, double lambda2,
                              double betak2, int method) {
   ModeSystem S;
   S.lambda2 = lambda2;
@@ -138,6 +227,85 @@ ModeSystem build_mode_system(const Mesh& M, const Numbering& N, double lambda2,
     }
   }
 
+  if (P) {
+    // -- second level: per patch family, condense the patch-interior
+    //    skeleton nodes; assemble the interface Schur complements.
+    const int nI_max = std::max(1, P->nI_max), nB_max = std::max(1, P->nB_max);
+    S.l2_sinv.assign(static_cast<size_t>(P->nfamily) * nI_max * nI_max, 0.0);
+    S.l2_g.assign(static_cast<size_t>(P->nfamily) * nI_max * nB_max, 0.0);
+    std::vector<std::vector<double>> T(P->nfamily);
+    for (int f = 0; f < P->nfamily; ++f) {
+      const int p = P->family_rep[f];
+      const int nI = P->nI[p], nB = P->nB[p], nl = nI + nB;
+      std::vector<double> Sp(static_cast<size_t>(nl) * nl, 0.0);
+      const auto& E = P->elems[p];
+      for (size_t k = 0; k < E.size(); ++k) {
+        const double* hbb = &hbb_all[static_cast<size_t>(M.family[E[k]]) * next * next];
+        for (int a = 0; a < next; ++a) {
+          const int la = P->local[p][k * next + a];
+          if (la < 0) continue;
+          for (int b = 0; b < next; ++b) {
+            const int lb = P->local[p][k * next + b];
+            if (lb >= 0) Sp[static_cast<size_t>(la) * nl + lb] += hbb[a * next + b];
+          }
+        }
+      }
+      double* Si = &S.l2_sinv[static_cast<size_t>(f) * nI_max * nI_max];
+      double* G = &S.l2_g[static_cast<size_t>(f) * nI_max * nB_max];
+      std::vector<double> II(static_cast<size_t>(nI) * nI);
+      for (int a = 0; a < nI; ++a)
+        for (int b = 0; b < nI; ++b) II[static_cast<size_t>(a) * nI + b] = Sp[static_cast<size_t>(a) * nl + b];
+      if (nI) invert(nI, II.data());
+      for (int a = 0; a < nI; ++a)
+        for (int b = 0; b < nI; ++b) Si[static_cast<size_t>(a) * nI_max + b] = II[static_cast<size_t>(a) * nI + b];
+      for (int a = 0; a < nI; ++a)
+        for (int b = 0; b < nB; ++b) {
+          double v = 0;
+          for (int c = 0; c < nI; ++c) v += II[static_cast<size_t>(a) * nI + c] * Sp[static_cast<size_t>(c) * nl + nI + b];
+          G[static_cast<size_t>(a) * nB_max + b] = v;
+        }
+      auto& Tf = T[f];
+      Tf.assign(static_cast<size_t>(nB) * nB, 0.0);
+      for (int a = 0; a < nB; ++a)
+        for (int b = 0; b < nB; ++b) {
+          double v = Sp[static_cast<size_t>(nI + a) * nl + nI + b];
+          for (int c = 0; c < nI; ++c)
+            v -= Sp[static_cast<size_t>(nI + a) * nl + c] * G[static_cast<size_t>(c) * nB_max + b];
+          Tf[static_cast<size_t>(a) * nB + b] = v;
+        }
+    }
+    const int ni = P->niface;
+    S.l2_gt.assign(S.l2_g.size(), 0.0);
+    for (int f = 0; f < P->nfamily; ++f)
+      for (int a = 0; a < nI_max; ++a)
+        for (int b = 0; b < nB_max; ++b)
+          S.l2_gt[(static_cast<size_t>(f) * nB_max + b) * nI_max + a] =
+              S.l2_g[(static_cast<size_t>(f) * nI_max + a) * nB_max + b];
+    std::vector<double>& A = S.l2_ainv;
+    A.assign(static_cast<size_t>(ni) * ni, 0.0);
+    for (int p = 0; p < P->npatch; ++p) {
+      const auto& Tf = T[P->family[p]];
+      const int nB = P->nB[p];
+      const int* iid = &P->B_iid[static_cast<size_t>(p) * P->nB_max];
+      for (int a = 0; a < nB; ++a)
+        for (int b = 0; b < nB; ++b) A[static_cast<size_t>(iid[a]) * ni + iid[b]] += Tf[static_cast<size_t>(a) * nB + b];
+    }
+    if (S.singular) {
+      // the pinned node is known (zero): identity row and column
+      const int q = P->pin_iid;
+      for (int t = 0; t < ni; ++t) {
+        A[static_cast<size_t>(q) * ni + t] = 0.0;
+        A[static_cast<size_t>(t) * ni + q] = 0.0;
+      }
+      A[static_cast<size_t>(q) * ni + q] = 1.0;
+      S.pin_iid = q;
+    }
+    if (ni) spd_inverse(ni, A.data());
+    S.nsolve = ni;
+    S.nband = 0;
+    return S;
+  }
+
   // -- banded assembly over the first nsolve global nodes (src/matrix.cpp:218-232)
   const int ns = S.nsolve, nb = S.nband, kd = nb - 1;
   std::vector<double> A(static_cast<size_t>(ns) * nb, 0.0);  // A[j*nb + t] = A(j-kd+t, j)
@@ -155,41 +323,7 @@ ModeSystem build_mode_system(const Mesh& M, const Numbering& N, double lambda2,
       }
     }
   }
-  // -- banded Cholesky A = U^T U, U stored in place as columns (dpbtrf "U")
-  for (int j = 0; j < ns; ++j) {
-    double* cj = &A[static_cast<size_t>(j) * nb];
-    const int i0 = std::max(0, j - kd);
-    for (int i = i0; i < j; ++i) {
-      const double* ci = &A[static_cast<size_t>(i) * nb];
-      double s = cj[kd - (j - i)];
-      const int k0 = std::max(i0, i - kd);
-      for (int k = k0; k < i; ++k) s -= ci[kd - (i - k)] * cj[kd - (j - k)];
-      cj[kd - (j - i)] = s / ci[kd];
-    }
-    double d = cj[kd];
-    for (int k = i0; k < j; ++k) d -= cj[kd - (j - k)] * cj[kd - (j - k)];
-    if (!(d > 0.0))
-      throw std::runtime_error("failed to factor Helmholtz matrix (not positive definite)");
-    cj[kd] = std::sqrt(d);
-  }
-  S.fwd.assign(static_cast<size_t>(ns) * nb, 0.0);
-  S.bwd.assign(static_cast<size_t>(ns) * nb, 0.0);
-  for (int j = 0; j < ns; ++j)
-    for (int t = 0; t < nb; ++t) {
-      double v = A[static_cast<size_t>(j) * nb + t];
-      if (j - kd + t < 0) v = 0.0;
-      S.fwd[static_cast<size_t>(j) * nb + t] = (t == kd) ? 1.0 / v : v;
-    }
-  // bwd row r: entries U[i][i+kd-t] for i = ns-1-r, column c = i+kd-t
-  for (int r = 0; r < ns; ++r) {
-    const int i = ns - 1 - r;
-    for (int t = 0; t < nb; ++t) {
-      const int c = i + kd - t;
-      double v = 0.0;
-      if (c < ns) v = A[static_cast<size_t>(c) * nb + kd - (c - i)];
-      S.bwd[static_cast<size_t>(r) * nb + t] = (t == kd) ? 1.0 / v : v;
-    }
-  }
+  factor_band(A, ns, nb, S);
   return S;
 }
 

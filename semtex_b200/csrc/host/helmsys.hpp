@@ -19,6 +19,7 @@
 #include <vector>
 
 #include "mesh.hpp"
+#include "patch.hpp"
 
 namespace stx {
 
@@ -33,12 +34,23 @@ struct ModeSystem {
   std::vector<double> hii;   // [nfamily][nint][nint]  hii^{-1}
   std::vector<double> fwd, bwd;  // [nsolve][nband]
   std::vector<double> pc;    // JACPCG: [nglobal + nel*nint] inverse diagonal
+  // With a patching (two-level condensation) the patch matrices and the dense
+  // inverse of the patch-interface Schur complement replace the band factor:
+  std::vector<double> l2_sinv;  // [pfamily][nI_max][nI_max]  S_II^{-1}
+  std::vector<double> l2_g;     // [pfamily][nI_max][nB_max]  S_II^{-1} S_IB
+  std::vector<double> l2_gt;    // [pfamily][nB_max][nI_max]  its transpose
+  std::vector<double> l2_ainv;  // [niface][niface] inverse of the interface system
+  int pin_iid = -1;             // interface node fixed to zero (singular mode)
 };
 
 // Full elemental Helmholtz matrix of element e, row-major node order.
 void element_helmholtz(const Mesh& M, int e, double lambda2, double betak2, double* H);
 
-ModeSystem build_mode_system(const Mesh& M, const Numbering& N, double lambda2,
+// `P` (may be null) selects the two-level condensation for DIRECT systems.
+// In-place inverse of a symmetric positive-definite n x n matrix (Cholesky,
+// triangular inverse, product); throws if the matrix is not positive definite.
+void spd_inverse(int n, double* A);
+ModeSystem build_mode_system(const Mesh& M, const Numbering& N, const Patching* P, double lambda2,
                              double betak2, int method);
 
 }  // namespace stx

@@ -278,6 +278,58 @@ int bfs_far(int root, const std::vector<int>& xadj, const std::vector<int>& adj,
 
 }  // namespace
 
+std::vector<int> rcm_order(std::vector<std::vector<int>>& nbr, int rcm_roots) {
+  const int ns = static_cast<int>(nbr.size());
+  std::vector<int> order;
+  if (ns == 0) return order;
+  std::vector<int> xadj(ns + 1, 0), adj, deg(ns);
+  for (int a = 0; a < ns; ++a) {
+    auto& v = nbr[a];
+    std::sort(v.begin(), v.end());
+    v.erase(std::unique(v.begin(), v.end()), v.end());
+    deg[a] = static_cast<int>(v.size());
+    xadj[a + 1] = xadj[a] + deg[a];
+    adj.insert(adj.end(), v.begin(), v.end());
+  }
+  // candidate roots: a pseudo-peripheral node plus a spread of others
+  std::vector<int> cand;
+  {
+    int depth = 0;
+    int r = bfs_far(0, xadj, adj, deg, depth);
+    for (int it = 0; it < 4; ++it) {
+      int d2 = 0;
+      int r2 = bfs_far(r, xadj, adj, deg, d2);
+      if (d2 <= depth) break;
+      depth = d2;
+      r = r2;
+    }
+    cand.push_back(r);
+    for (int k = 1; k < rcm_roots; ++k) cand.push_back(static_cast<int>((static_cast<long>(k) * ns) / rcm_roots));
+  }
+  auto bandwidth = [&](const std::vector<int>& ord) {
+    std::vector<int> pos(ns);
+    for (int k = 0; k < ns; ++k) pos[ord[k]] = k;
+    int bw = 0;
+    for (int a = 0; a < ns; ++a)
+      for (int k = xadj[a]; k < xadj[a + 1]; ++k) bw = std::max(bw, std::abs(pos[a] - pos[adj[k]]));
+    return bw;
+  };
+  int best_bw = -1;
+  for (int root : cand) {
+    std::vector<int> ord;
+    std::vector<char> seen(ns, 0);
+    rcm_from(root, xadj, adj, deg, ord, seen);
+    for (int a = 0; a < ns; ++a)
+      if (!seen[a]) rcm_from(a, xadj, adj, deg, ord, seen);
+    int bw = bandwidth(ord);
+    if (best_bw < 0 || bw < best_bw) {
+      best_bw = bw;
+      order.assign(ord.rbegin(), ord.rend());
+    }
+  }
+  return order;
+}
+
 Numbering build_numbering(const Session& S, const Mesh& M, char field, int rcm_roots) {
   const int n = M.np, nel = M.nel, nm = n - 1, next = M.next;
   Numbering N;
@@ -389,51 +441,7 @@ Numbering build_numbering(const Session& S, const Mesh& M, char field, int rcm_r
         for (int b : v)
           if (a != b) nbr[a].push_back(b);
     }
-    std::vector<int> xadj(ns + 1, 0), adj, deg(ns);
-    for (int a = 0; a < ns; ++a) {
-      auto& v = nbr[a];
-      std::sort(v.begin(), v.end());
-      v.erase(std::unique(v.begin(), v.end()), v.end());
-      deg[a] = static_cast<int>(v.size());
-      xadj[a + 1] = xadj[a] + deg[a];
-      adj.insert(adj.end(), v.begin(), v.end());
-    }
-    // candidate roots: pseudo-peripheral node of each component plus a spread
-    std::vector<int> cand;
-    {
-      int depth = 0;
-      int r = bfs_far(0, xadj, adj, deg, depth);
-      for (int it = 0; it < 4; ++it) {
-        int d2 = 0;
-        int r2 = bfs_far(r, xadj, adj, deg, d2);
-        if (d2 <= depth) break;
-        depth = d2;
-        r = r2;
-      }
-      cand.push_back(r);
-      for (int k = 1; k < rcm_roots; ++k) cand.push_back(static_cast<int>((static_cast<long>(k) * ns) / rcm_roots));
-    }
-    auto bandwidth = [&](const std::vector<int>& ord) {
-      std::vector<int> pos(ns);
-      for (int k = 0; k < ns; ++k) pos[ord[ns - 1 - k]] = k;  // reversed
-      int bw = 0;
-      for (int a = 0; a < ns; ++a)
-        for (int k = xadj[a]; k < xadj[a + 1]; ++k) bw = std::max(bw, std::abs(pos[a] - pos[adj[k]]));
-      return bw;
-    };
-    int best_bw = -1;
-    for (int root : cand) {
-      std::vector<int> ord;
-      std::vector<char> seen(ns, 0);
-      rcm_from(root, xadj, adj, deg, ord, seen);
-      for (int a = 0; a < ns; ++a)
-        if (!seen[a]) rcm_from(a, xadj, adj, deg, ord, seen);
-      int bw = bandwidth(ord);
-      if (best_bw < 0 || bw < best_bw) {
-        best_bw = bw;
-        order.assign(ord.rbegin(), ord.rend());
-      }
-    }
+    order = rcm_order(nbr, rcm_roots);
   } else if (ns == 1) {
     order.push_back(0);
   }

@@ -64,6 +64,10 @@ struct Numbering {
   }
 };
 
+// Reverse Cuthill--McKee order of a graph given as adjacency lists (sorted
+// and deduplicated in place); the best of rcm_roots trial roots by bandwidth.
+std::vector<int> rcm_order(std::vector<std::vector<int>>& nbr, int rcm_roots);
+
 // rcm_roots: number of trial roots for the reverse Cuthill--McKee search
 // (the role of enumerate's optimisation levels, utility/enumerate.cpp:706-832).
 Numbering build_numbering(const Session& S, const Mesh& M, char field, int rcm_roots = 48);

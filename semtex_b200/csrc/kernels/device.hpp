@@ -25,6 +25,12 @@ struct DevGeom {
   const int* emap;      // [npnp] boundary-major traverse
   const int* pmap;      // [npnp] inverse of emap
   const int* family;    // [nel] geometry family
+  // Elements grouped into chunks of one family (for the batched element
+  // kernels): chunk c covers elem_sorted[chunk_start[c] .. + chunk_count[c]).
+  int nchunk, chunk_max;
+  const int* chunk_start;
+  const int* chunk_count;
+  const int* elem_sorted;
 };
 
 struct DevNumbering {
@@ -58,6 +64,21 @@ struct DevModal {
   int* status;                    // device status word (0 = ok)
   const double* pc;               // JACPCG: [nmodes][npts]
   int npts;
+  // Two-level condensation (patches + dense interface inverse); l2 = 0 when
+  // the single banded factor above is used instead.
+  int l2;
+  int npatch, pfam, nI_max, nB_max, niface;
+  const int* p_family;            // [npatch]
+  const int* p_nI;                // [npatch]
+  const int* p_nB;                // [npatch]
+  const int* p_Igid;              // [npatch][nI_max] skeleton ids of interior nodes
+  const int* p_Biid;              // [npatch][nB_max] interface ids of boundary nodes
+  const int* skel_of;             // [niface] skeleton id of each interface unknown
+  const int* pin;                 // [nmodes] pinned interface id or -1
+  const double* l2_sinv;          // [nmodes][pfam][nI_max][nI_max]
+  const double* l2_g;             // [nmodes][pfam][nI_max][nB_max]
+  const double* l2_gt;            // [nmodes][pfam][nB_max][nI_max]
+  const double* l2_ainv;          // [nmodes][niface][niface]
 };
 
 }  // namespace stx

@@ -15,6 +15,7 @@
 //      and imposition of essential values (Field::setEssential,
 //      src/field.cpp:1106-1124).
 #include "helmholtz.cuh"
+#include "twolevel.cuh"
 
 #include <algorithm>
 #include <vector>
@@ -156,6 +157,237 @@ __global__ void k_recover(DevGeom g, DevNumbering N, DevModal S,
     for (int c = 0; c < g.nint; ++c) v += hii[c] * sF[g.next + c];
     for (int a = 0; a < g.next; ++a) v -= hbi[static_cast<size_t>(a) * g.nint + t] * sub[a];
     Up[g.emap[g.next + t]] = v;
+  }
+}
+
+
+// ---------------------------------------------------------------------------
+// Batched element kernels.  One block per (chunk of up to chunk_max elements of
+// one geometry family, Fourier mode): the chunk's constrained forcing for the
+// mode's Re and Im planes forms the columns of a small dense operand in
+// shared memory (column stride padded odd against bank conflicts), and the
+// family's condensation matrices are applied to all columns at once as a
+// register-tiled GEMM (4 rows x 4 columns per thread), each matrix entry read
+// through L1 once per column tile.
+// ---------------------------------------------------------------------------
+
+constexpr int kTile = 4;
+
+// Constrained forcing -(Q4 f + [emask] H g) of the chunk's elements for the
+// planes of mode m into columns of sB (column c = slot*cnt + l, row =
+// boundary-major node, stride ldb).  The lift term H g is formed one column
+// per warp in warp-private scratch (wsc: 3*nn doubles per warp) and skipped
+// where the element's essential values are all zero (H 0 = 0).
+__device__ void chunk_forcing2(const DevGeom& g, const DevNumbering& N, const double* __restrict__ F,
+                               const double* __restrict__ G, int gstride, double hcon, const int* el, int cnt, int m,
+                               int nr, double* sB, int ldb, double* wsc, const double* sD) {
+  const int nn = g.npnp, np = g.np;
+  for (int w = threadIdx.x; w < nr * cnt * nn; w += blockDim.x) {
+    const int c = w / nn, t = w - c * nn;
+    const int slot = c / cnt, l = c - slot * cnt;
+    const int k = 2 * m + slot;
+    const int e = el[l];
+    sB[c * ldb + g.pmap[t]] =
+        -g.Q4[e * nn + t] * F[static_cast<size_t>(k) * g.plane_size + static_cast<size_t>(e) * nn + t];
+  }
+  __syncthreads();
+  if (!G) return;
+  const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31, nwarp = blockDim.x >> 5;
+  double* su = wsc + static_cast<size_t>(warp) * 3 * nn;
+  double* sR = su + nn;
+  double* sS = sR + nn;
+  for (int c = warp; c < nr * cnt; c += nwarp) {
+    const int slot = c / cnt, l = c - slot * cnt;
+    const int k = 2 * m + slot;
+    const int e = el[l];
+    if (!N.emask[e]) continue;  // uniform across the warp
+    const double* Gp = G + static_cast<size_t>(k) * gstride;
+    for (int q = lane; q < nn; q += 32) su[q] = 0.0;
+    __syncwarp();
+    bool nonzero = false;
+    for (int q = lane; q < g.next; q += 32) {
+      const double v = N.bmask[e * g.next + q] ? Gp[N.btog[e * g.next + q]] : 0.0;
+      su[g.emap[q]] = v;
+      nonzero = nonzero || v != 0.0;
+    }
+    if (!__any_sync(0xffffffffu, nonzero)) continue;
+    __syncwarp();
+    for (int q = lane; q < nn; q += 32) {
+      const int i = q / np, j = q - (q / np) * np;
+      double r = 0.0, s2 = 0.0;
+      for (int kk = 0; kk < np; ++kk) {
+        r += su[i * np + kk] * sD[j * np + kk];
+        s2 += sD[i * np + kk] * su[kk * np + j];
+      }
+      const double q1 = g.Q1[e * nn + q], q2 = g.Q2[e * nn + q], q3 = g.Q3[e * nn + q];
+      sR[q] = q1 * r + q3 * s2;
+      sS[q] = q2 * s2 + q3 * r;
+    }
+    __syncwarp();
+    for (int q = lane; q < nn; q += 32) {
+      const int i = q / np, j = q - (q / np) * np;
+      double h = g.Q4[e * nn + q] * su[q] * hcon;
+      for (int kk = 0; kk < np; ++kk) {
+        h += sD[kk * np + i] * sS[kk * np + j];
+        h += sR[i * np + kk] * sD[kk * np + j];
+      }
+      sB[c * ldb + g.pmap[q]] -= h;
+    }
+    __syncwarp();
+  }
+  __syncthreads();
+}
+
+// acc[4][4] += A[r0+ii][k] * B[cb+jj*cs][k], k < K; A row-major (lda) in
+// global memory (rows clamped to M-1), B columns in shared memory (ldb).
+// Threads of a warp share r0 and take consecutive cb: A reads broadcast, B
+// reads hit distinct banks (odd ldb).
+__device__ __forceinline__ void tile_gemm(double (&acc)[kTile][kTile], const double* __restrict__ A, int lda,
+                                          int M, int r0, const double* B, int ldb, int cb, int cs, int ncol, int K,
+                                          int boff) {
+  const double* a[kTile];
+  const double* b[kTile];
+#pragma unroll
+  for (int ii = 0; ii < kTile; ++ii) a[ii] = A + static_cast<size_t>(min(r0 + ii, M - 1)) * lda;
+#pragma unroll
+  for (int jj = 0; jj < kTile; ++jj) b[jj] = B + min(cb + jj * cs, ncol - 1) * ldb + boff;
+  for (int k = 0; k < K; ++k) {
+    double av[kTile], bv[kTile];
+#pragma unroll
+    for (int ii = 0; ii < kTile; ++ii) av[ii] = __ldg(a[ii] + k);
+#pragma unroll
+    for (int jj = 0; jj < kTile; ++jj) bv[jj] = b[jj][k];
+#pragma unroll
+    for (int ii = 0; ii < kTile; ++ii)
+#pragma unroll
+      for (int jj = 0; jj < kTile; ++jj) acc[ii][jj] = fma(av[ii], bv[jj], acc[ii][jj]);
+  }
+}
+
+// Same with A transposed: A^T[r][k] = A[k][r] (A row-major, lda).
+__device__ __forceinline__ void tile_gemm_t(double (&acc)[kTile][kTile], const double* __restrict__ A, int lda,
+                                            int M, int r0, const double* B, int ldb, int cb, int cs, int ncol,
+                                            int K) {
+  const double* b[kTile];
+#pragma unroll
+  for (int jj = 0; jj < kTile; ++jj) b[jj] = B + min(cb + jj * cs, ncol - 1) * ldb;
+  for (int k = 0; k < K; ++k) {
+    double av[kTile], bv[kTile];
+#pragma unroll
+    for (int ii = 0; ii < kTile; ++ii) av[ii] = __ldg(A + static_cast<size_t>(k) * lda + min(r0 + ii, M - 1));
+#pragma unroll
+    for (int jj = 0; jj < kTile; ++jj) bv[jj] = b[jj][k];
+#pragma unroll
+    for (int ii = 0; ii < kTile; ++ii)
+#pragma unroll
+      for (int jj = 0; jj < kTile; ++jj) acc[ii][jj] = fma(av[ii], bv[jj], acc[ii][jj]);
+  }
+}
+
+struct ChunkSmem {
+  int ldb, ldu;
+};
+
+__host__ __device__ inline ChunkSmem chunk_layout(int nn, int next) {
+  ChunkSmem c;
+  c.ldb = nn | 1;      // odd strides: conflict-free column reads
+  c.ldu = next | 1;
+  return c;
+}
+
+__global__ void k_condense_chunk(DevGeom g, DevNumbering N, DevModal S, const double* __restrict__ F,
+                                 const double* __restrict__ G, int gstride, double* __restrict__ R, int rstride) {
+  extern __shared__ double smem[];
+  const int c = blockIdx.x, m = blockIdx.y;
+  const int nz = g.nz;
+  const int nr = (nz > 1 && m > 0) ? 2 : 1;
+  const int nn = g.npnp, next = g.next, nint = g.nint;
+  const int cnt = g.chunk_count[c];
+  const int* el = g.elem_sorted + g.chunk_start[c];
+  const ChunkSmem L = chunk_layout(nn, next);
+  double* sB = smem;                                   // [2*chunk][ldb]
+  double* sD = sB + 2 * g.chunk_max * L.ldb;
+  double* wsc = sD + g.np * g.np;                      // [warps][3*nn]
+  for (int w = threadIdx.x; w < g.np * g.np; w += blockDim.x) sD[w] = g.D[w];
+  __syncthreads();
+  chunk_forcing2(g, N, F, G, gstride, S.lambda2[m] + S.betak2[m], el, cnt, m, nr, sB, L.ldb, wsc, sD);
+  const double* hbi = S.hbi + (static_cast<size_t>(m) * S.nfamily + g.family[el[0]]) * next * nint;
+  const int ncol = nr * cnt;
+  const int rt = (next + kTile - 1) / kTile, cs = (ncol + kTile - 1) / kTile;
+  for (int tile = threadIdx.x; tile < rt * cs; tile += blockDim.x) {
+    const int cb = tile % cs, r0 = (tile / cs) * kTile;
+    double acc[kTile][kTile] = {};
+    if (nint) tile_gemm(acc, hbi, nint, next, r0, sB, L.ldb, cb, cs, ncol, nint, next);
+#pragma unroll
+    for (int ii = 0; ii < kTile; ++ii)
+#pragma unroll
+      for (int jj = 0; jj < kTile; ++jj) {
+        const int a = r0 + ii, col = cb + jj * cs;
+        if (a < next && col < ncol) {
+          const int slot = col / cnt, l = col - slot * cnt;
+          const double v = sB[col * L.ldb + a] - acc[ii][jj];
+          atomicAdd(&R[static_cast<size_t>(2 * m + slot) * rstride + N.btog[el[l] * next + a]], v);
+        }
+      }
+  }
+}
+
+__global__ void k_recover_chunk(DevGeom g, DevNumbering N, DevModal S, const double* __restrict__ F,
+                                const double* __restrict__ G, int gstride, const double* __restrict__ R, int rstride,
+                                double* __restrict__ U) {
+  extern __shared__ double smem[];
+  const int c = blockIdx.x, m = blockIdx.y;
+  const int nz = g.nz;
+  const int nr = (nz > 1 && m > 0) ? 2 : 1;
+  const int nn = g.npnp, next = g.next, nint = g.nint;
+  const int cnt = g.chunk_count[c];
+  const int* el = g.elem_sorted + g.chunk_start[c];
+  const ChunkSmem L = chunk_layout(nn, next);
+  double* sB = smem;                                   // [2*chunk][ldb] forcing columns
+  double* sU = sB + 2 * g.chunk_max * L.ldb;           // [2*chunk][ldu] boundary solution
+  double* sD = sU + 2 * g.chunk_max * L.ldu;
+  double* wsc = sD + g.np * g.np;                      // [warps][3*nn]
+  for (int w = threadIdx.x; w < g.np * g.np; w += blockDim.x) sD[w] = g.D[w];
+  __syncthreads();
+  chunk_forcing2(g, N, F, G, gstride, S.lambda2[m] + S.betak2[m], el, cnt, m, nr, sB, L.ldb, wsc, sD);
+  const int nsolve = S.nsolve[m];
+  const int ncol = nr * cnt;
+  for (int w = threadIdx.x; w < ncol * next; w += blockDim.x) {
+    const int col = w / next, a = w - col * next;
+    const int slot = col / cnt, l = col - slot * cnt;
+    const int k = 2 * m + slot;
+    const int e = el[l];
+    const int gi = N.btog[e * next + a];
+    const double ub = gi < nsolve ? R[static_cast<size_t>(k) * rstride + gi] : 0.0;
+    sU[col * L.ldu + a] = ub;
+    U[static_cast<size_t>(k) * g.plane_size + static_cast<size_t>(e) * nn + g.emap[a]] =
+        (N.bmask[e * next + a] && G) ? G[static_cast<size_t>(k) * gstride + gi] : ub;
+  }
+  __syncthreads();
+  const size_t fm = static_cast<size_t>(m) * S.nfamily + g.family[el[0]];
+  const double* hii = S.hii + fm * nint * nint;
+  const double* hbi = S.hbi + fm * next * nint;
+  const int rt = (nint + kTile - 1) / kTile, cs = (ncol + kTile - 1) / kTile;
+  for (int tile = threadIdx.x; tile < rt * cs; tile += blockDim.x) {
+    const int cb = tile % cs, r0 = (tile / cs) * kTile;
+    double acc[kTile][kTile] = {};
+    tile_gemm(acc, hii, nint, nint, r0, sB, L.ldb, cb, cs, ncol, nint, next);
+#pragma unroll
+    for (int ii = 0; ii < kTile; ++ii)
+#pragma unroll
+      for (int jj = 0; jj < kTile; ++jj) acc[ii][jj] = -acc[ii][jj];
+    tile_gemm_t(acc, hbi, nint, nint, r0, sU, L.ldu, cb, cs, ncol, next);
+#pragma unroll
+    for (int ii = 0; ii < kTile; ++ii)
+#pragma unroll
+      for (int jj = 0; jj < kTile; ++jj) {
+        const int i = r0 + ii, col = cb + jj * cs;
+        if (i < nint && col < ncol) {
+          const int slot = col / cnt, l = col - slot * cnt;
+          U[static_cast<size_t>(2 * m + slot) * g.plane_size + static_cast<size_t>(el[l]) * nn + g.emap[next + i]] =
+              -acc[ii][jj];
+        }
+      }
   }
 }
 
@@ -695,15 +927,15 @@ SweepPlan sweep_plan(int nbp, int nband) {
 
 }  // namespace
 
-size_t helmholtz_workspace_doubles(const DevGeom& g, const DevNumbering& N) {
+size_t helmholtz_workspace_doubles(const DevGeom& g, const DevNumbering& N, const DevModal& S) {
   const size_t stride = (static_cast<size_t>(N.nglobal) + 31) / 32 * 32;
-  return 2 * stride * g.nz;
+  return 2 * stride * g.nz + (S.l2 ? twolevel_workspace_doubles(S, g.nz) : 0);
 }
 
-int helmholtz_direct_launches(const DevNumbering& N, int np) {
+int helmholtz_direct_launches(const DevNumbering& N, const DevModal& S, int np) {
   const bool has_ess = N.nglobal > N.nsolve;
   const int nedge_nodes = N.nedge * np;
-  return 4 + (has_ess && nedge_nodes ? 1 : 0) + (nedge_nodes ? 1 : 0);
+  return 2 + (S.l2 ? twolevel_launches(S) : 2) + (has_ess && nedge_nodes ? 1 : 0) + (nedge_nodes ? 1 : 0);
 }
 
 cudaError_t helmholtz_direct_solve(const DevGeom& g, const DevNumbering& N, const DevModal& S,
@@ -725,14 +957,35 @@ cudaError_t helmholtz_direct_solve(const DevGeom& g, const DevNumbering& N, cons
   const int threads = ((g.npnp + 31) / 32) * 32 < 64 ? 64 : ((g.npnp + 31) / 32) * 32;
   const size_t shm = sizeof(double) * (static_cast<size_t>(g.np) * g.np + 5 * g.npnp);
   dim3 egrid(g.nel, nz);
-  k_condense<<<egrid, threads, shm, st>>>(g, N, S, F, has_ess ? G : nullptr, rstride, R, rstride);
+  const size_t nn = g.npnp, cm = g.chunk_max;
+  const size_t ldb = nn | 1, ldu = g.next | 1;
+  const size_t wsc = 8 * 3 * nn;  // warp scratch of the lift term, 8 warps
+  const size_t shm_cond = sizeof(double) * (2 * cm * ldb + g.np * g.np + wsc);
+  const size_t shm_rec = sizeof(double) * (2 * cm * ldb + 2 * cm * ldu + g.np * g.np + wsc);
+  const bool chunked = g.nchunk > 0 && shm_rec <= 200 * 1024;
+  if (chunked) {
+    static int configured = 0;
+    if (!configured) {
+      cudaFuncSetAttribute(k_condense_chunk, cudaFuncAttributeMaxDynamicSharedMemorySize, 200 * 1024);
+      cudaFuncSetAttribute(k_recover_chunk, cudaFuncAttributeMaxDynamicSharedMemorySize, 200 * 1024);
+      configured = 1;
+    }
+    k_condense_chunk<<<dim3(g.nchunk, S.nmodes), 256, shm_cond, st>>>(g, N, S, F, has_ess ? G : nullptr, rstride,
+                                                                      R, rstride);
+  } else {
+    k_condense<<<egrid, threads, shm, st>>>(g, N, S, F, has_ess ? G : nullptr, rstride, R, rstride);
+  }
   if (nedge_nodes) {
     dim3 grid((nedge_nodes + 127) / 128, nz);
     k_natural<<<grid, 128, 0, st>>>(g, N, lines, nline, R, rstride, nz);
   }
   if (ev) cudaEventRecord(ev[1], st);
-  const SweepPlan plan = sweep_plan(S.nbp, S.nband);
-  if (plan.stages >= 2) {
+  const SweepPlan plan = S.l2 ? SweepPlan() : sweep_plan(S.nbp, S.nband);
+  if (S.l2) {
+    err = twolevel_solve(S, R, rstride, work + 2 * static_cast<size_t>(rstride) * nz, nz, st);
+    if (err != cudaSuccess) return err;
+    if (ev) cudaEventRecord(ev[2], st);
+  } else if (plan.stages >= 2) {
     static int configured = 0;
     if (!configured) {
       cudaFuncSetAttribute(k_band_sweep, cudaFuncAttributeMaxDynamicSharedMemorySize, 220 * 1024);
@@ -749,8 +1002,12 @@ cudaError_t helmholtz_direct_solve(const DevGeom& g, const DevNumbering& N, cons
     k_band_solve<<<S.nmodes, 256, 0, st>>>(S, S.bwd, R, rstride, nz, 1);
   }
   if (ev) cudaEventRecord(ev[3], st);
-  k_recover<<<egrid, threads, shm + sizeof(double) * g.next, st>>>(g, N, S, F, has_ess ? G : nullptr,
-                                                                   rstride, R, rstride, U);
+  if (chunked)
+    k_recover_chunk<<<dim3(g.nchunk, S.nmodes), 256, shm_rec, st>>>(g, N, S, F, has_ess ? G : nullptr, rstride,
+                                                                    R, rstride, U);
+  else
+    k_recover<<<egrid, threads, shm + sizeof(double) * g.next, st>>>(g, N, S, F, has_ess ? G : nullptr,
+                                                                     rstride, R, rstride, U);
   if (ev) cudaEventRecord(ev[4], st);
   return cudaGetLastError();
 }

@@ -13,20 +13,22 @@ constexpr int kBandRows = 16;
 
 // Doubles of scratch the direct solve needs: boundary RHS and essential
 // values, one padded globally numbered vector each per plane.
-size_t helmholtz_workspace_doubles(const DevGeom& g, const DevNumbering& N);
+size_t helmholtz_workspace_doubles(const DevGeom& g, const DevNumbering& N, const DevModal& S);
 
 // Field::solve DIRECT over all planes: F (Fourier forcing, reference plane
 // layout) -> U.  `lines` holds the Fourier-space BC values [nz][nline].
 // U's Nyquist plane (k = 1) is left untouched, as in the reference.
 // `phase_events` (optional, 5 events) are recorded on `st` before the
-// condensation, before each banded sweep, before the recovery and at the end.
+// element condensation, before the skeleton solve (two-level: patch and
+// interface products; otherwise the forward banded sweep), between its two
+// halves, before the element recovery and at the end.
 cudaError_t helmholtz_direct_solve(const DevGeom& g, const DevNumbering& N, const DevModal& S,
                                    const double* F, double* U, const double* lines, int nline,
                                    double* work, cudaStream_t st,
                                    cudaEvent_t* phase_events = nullptr);
 
 // Number of kernel launches one direct solve issues.
-int helmholtz_direct_launches(const DevNumbering& N, int np);
+int helmholtz_direct_launches(const DevNumbering& N, const DevModal& S, int np);
 
 // Field::solve JACPCG over all planes (src/field.cpp:711-805).  U holds the
 // initial guess on entry.  Iterations per plane are written to `iters`

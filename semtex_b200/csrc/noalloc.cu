@@ -47,7 +47,7 @@ extern "C" int stx_field_solve_noalloc(stx_modal* sys, const double* d_forcing, 
   const auto it = ctx->fields.find(sys->field);
   if (it == ctx->fields.end()) return fail(STX_EINVAL, "field not in context");
   const stx::FieldDev& F = it->second;
-  const size_t need = stx::helmholtz_workspace_doubles(ctx->dg, F.dn);
+  const size_t need = stx::helmholtz_workspace_doubles(ctx->dg, F.dn, sys->store->dm);
   if (need > kNoAllocScratchDoubles) {
     return fail(STX_EINVAL, "stx_field_solve_noalloc: this problem needs " + std::to_string(need) +
                                 " doubles of scratch, more than the static maximum of " +

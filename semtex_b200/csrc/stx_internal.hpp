@@ -10,6 +10,7 @@
 #include <vector>
 
 #include "host/mesh.hpp"
+#include "host/patch.hpp"
 #include "host/session.hpp"
 #include "kernels/device.hpp"
 
@@ -27,6 +28,8 @@ struct DeviceArena {
 
 struct FieldDev {
   Numbering N;
+  std::unique_ptr<Patching> P;  // two-level condensation, built on first DIRECT system
+  bool patch_done = false;
   DevNumbering dn{};
   double* d_lines = nullptr;  // [nz][nline] Fourier-space BC values
   int nline = 0;
@@ -59,6 +62,35 @@ struct stx_context {
   double* d_twiddle = nullptr;
   double* d_io = nullptr;
   std::vector<stx_modal*> modals;
+
+  // Patching of a field's numbering for the two-level direct solve, or null
+  // when the single banded factor is used (token STX_TWOLEVEL = 0, or an
+  // interface too large for a dense inverse).  The patch size is the one of
+  // {8, 16, 36, 64} elements that minimises the matrix bytes read per mode.
+  const stx::Patching* patching(char field) {
+    stx::FieldDev& F = fields.at(field);
+    if (!F.patch_done) {
+      F.patch_done = true;
+      const bool want = !S.tokens.has("STX_TWOLEVEL") || S.tokens.ivalue("STX_TWOLEVEL") != 0;
+      if (want) {
+        double best = 0;
+        for (int cap : {8, 16, 36, 64}) {
+          auto P = std::make_unique<stx::Patching>(stx::build_patching(M, F.N, cap));
+          if (P->niface > 6000) continue;
+          double bytes = static_cast<double>(P->niface) * P->niface;
+          for (int f = 0; f < P->nfamily; ++f) {
+            const int p = P->family_rep[f];
+            bytes += static_cast<double>(P->nI[p]) * P->nI[p] + 2.0 * P->nI[p] * P->nB[p];
+          }
+          if (!F.P || bytes < best) {
+            best = bytes;
+            F.P = std::move(P);
+          }
+        }
+      }
+    }
+    return F.P.get();
+  }
 
   // Solver workspace, grown on demand (synchronises before regrowing).
   double* d_work = nullptr;
