@@ -474,6 +474,7 @@ int stx_modal_create(stx_context* ctx, char field, double lambda2, double beta, 
         d.p_Igid = upload(st->arena, P->I_gid);
         d.p_Biid = upload(st->arena, P->B_iid);
         d.skel_of = upload(st->arena, P->skel_of.empty() ? std::vector<int>{0} : P->skel_of);
+
         d.pin = upload(st->arena, pin);
         d.hbi = upload(st->arena, hbi);
         d.hii = upload(st->arena, hii);

@@ -182,6 +182,7 @@ __device__ void chunk_forcing2(const DevGeom& g, const DevNumbering& N, const do
                                const double* __restrict__ G, int gstride, double hcon, const int* el, int cnt, int m,
                                int nr, double* sB, int ldb, double* wsc, const double* sD) {
   const int nn = g.npnp, np = g.np;
+#pragma unroll 8
   for (int w = threadIdx.x; w < nr * cnt * nn; w += blockDim.x) {
     const int c = w / nn, t = w - c * nn;
     const int slot = c / cnt, l = c - slot * cnt;
@@ -251,6 +252,7 @@ __device__ __forceinline__ void tile_gemm(double (&acc)[kTile][kTile], const dou
   for (int ii = 0; ii < kTile; ++ii) a[ii] = A + static_cast<size_t>(min(r0 + ii, M - 1)) * lda;
 #pragma unroll
   for (int jj = 0; jj < kTile; ++jj) b[jj] = B + min(cb + jj * cs, ncol - 1) * ldb + boff;
+#pragma unroll 4
   for (int k = 0; k < K; ++k) {
     double av[kTile], bv[kTile];
 #pragma unroll
@@ -271,6 +273,7 @@ __device__ __forceinline__ void tile_gemm_t(double (&acc)[kTile][kTile], const d
   const double* b[kTile];
 #pragma unroll
   for (int jj = 0; jj < kTile; ++jj) b[jj] = B + min(cb + jj * cs, ncol - 1) * ldb;
+#pragma unroll 4
   for (int k = 0; k < K; ++k) {
     double av[kTile], bv[kTile];
 #pragma unroll
@@ -352,6 +355,7 @@ __global__ void k_recover_chunk(DevGeom g, DevNumbering N, DevModal S, const dou
   chunk_forcing2(g, N, F, G, gstride, S.lambda2[m] + S.betak2[m], el, cnt, m, nr, sB, L.ldb, wsc, sD);
   const int nsolve = S.nsolve[m];
   const int ncol = nr * cnt;
+#pragma unroll 8
   for (int w = threadIdx.x; w < ncol * next; w += blockDim.x) {
     const int col = w / next, a = w - col * next;
     const int slot = col / cnt, l = col - slot * cnt;

@@ -40,8 +40,15 @@ __global__ void k_l2_condense(DevModal S, const double* __restrict__ R, int rstr
   const double* G = S.l2_g + (static_cast<size_t>(m) * S.pfam + f) * S.nI_max * S.nB_max;
   const int pin = S.pin[m];
   for (int b = threadIdx.x; b < nB; b += blockDim.x) {
-    double v = 0.0;
-    for (int i = 0; i < nI; ++i) v = fma(G[static_cast<size_t>(i) * S.nB_max + b], sr[i], v);
+    double v = 0.0, v2 = 0.0;
+    int i = 0;
+#pragma unroll 8
+    for (; i + 1 < nI; i += 2) {
+      v = fma(G[static_cast<size_t>(i) * S.nB_max + b], sr[i], v);
+      v2 = fma(G[static_cast<size_t>(i + 1) * S.nB_max + b], sr[i + 1], v2);
+    }
+    if (i < nI) v = fma(G[static_cast<size_t>(i) * S.nB_max + b], sr[i], v);
+    v += v2;
     const int iid = Bi[b];
     if (iid != pin) atomicAdd(&Ri[static_cast<size_t>(k) * istride + iid], -v);
   }
@@ -70,12 +77,14 @@ __global__ void __launch_bounds__(32 * kRowsPerBlock) k_iface_gemv(DevModal S, c
   const double* A = S.l2_ainv + static_cast<size_t>(m) * n * n + static_cast<size_t>(row) * n;
   double s0 = 0.0, s1 = 0.0;
   if (nr > 1) {
+#pragma unroll 8
     for (int c = lane; c < n; c += 32) {
       const double a = __ldg(A + c);
       s0 = fma(a, sx[c], s0);
       s1 = fma(a, sx[n + c], s1);
     }
   } else {
+#pragma unroll 8
     for (int c = lane; c < n; c += 32) s0 = fma(__ldg(A + c), sx[c], s0);
   }
   for (int o = 16; o; o >>= 1) {
