@@ -321,9 +321,46 @@ def run_ours(args):
         "gpu_launches": int(launches.value) * args.steps,
         "clocks": clocks, "cpu_baseline": cpu,
     }
+    if args.dns_steps > 0 and ws == 1:
+        line["dns"] = run_dns(args.dns_steps, 3, local)
     print(json.dumps(line))
     if ws > 1:
         torch.distributed.destroy_process_group()
+
+
+def run_dns(steps, warmup=3, local=0):
+    """Secondary measurement: DNS steps/s on the 3D Taylor--Green workload
+    (24x24 periodic quads, N_P=9, N_Z=96, Re=1600, D_T=1e-3, N_TIME=3,
+    alternating skew-symmetric advection, plain FP64 direct solves).  The
+    first N_TIME-1 steps use the reference's temporary PCG systems and are
+    excluded; the timed steps are device time (CUDA events on the library
+    stream)."""
+    import torch
+    import semtex_b200 as S
+    from semtex_b200 import sessions
+    d = tempfile.mkdtemp()
+    p = sessions.taylor_green_session(os.path.join(d, "c3"), 24, 9, 96, re=1600.0, dt=1e-3, nstep=200)
+    t0 = time.perf_counter()
+    ctx = S.Context(p, device=local)
+    D = S.DNS(ctx, 1)
+    setup = time.perf_counter() - t0
+    funcs = S._user_functions(p)
+    D.restart({c: ctx.evaluate(funcs[c], 0.0) for c in ctx.fields if c in funcs}, 0.0)
+    D.advance(2 + warmup)
+    stream = ctx.torch_stream()
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    ctx.sync()
+    e0.record(stream)
+    D.advance(steps)
+    e1.record(stream)
+    e1.synchronize()
+    ms = e0.elapsed_time(e1) / steps
+    out = {"metric": "DNS steps/s", "value": 1e3 / ms, "ms_per_step": ms, "steps": steps,
+           "workload": "c3: Taylor-Green 24x24x96, N_P=9, Re=1600, D_T=1e-3, N_TIME=3 (no dealiasing)",
+           "setup_s": setup}
+    D.close()
+    ctx.close()
+    return out
 
 
 def main():
@@ -333,9 +370,17 @@ def main():
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
     ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--dns-steps", type=int, default=20,
+                    help="timed steps of the secondary DNS measurement (0 to skip)")
+    ap.add_argument("--workload", default="c2", choices=["c2", "dns"],
+                    help="dns: run only the DNS measurement (one JSON line)")
     args = ap.parse_args()
     if args.impl == "reference":
         run_reference(args)
+    elif args.workload == "dns":
+        import torch
+        torch.cuda.set_device(0)
+        print(json.dumps(run_dns(max(1, args.dns_steps), args.warmup, 0)))
     else:
         run_ours(args)
 

@@ -65,6 +65,190 @@ __global__ void k_dft(double* __restrict__ data, int nz, int plane_size, int sig
   }
 }
 
+// ---------------------------------------------------------------------------
+// Mixed-radix Stockham FFT (radices 4, 2, 3, 5) of the z-lines of TP
+// consecutive points per block, complex arithmetic in shared memory
+// ([n][p] layout, point index fastest, so global loads and stores of each
+// plane row stay coalesced).  Forward: real lines in, packed spectrum out,
+// scaled by 1/nz; inverse: packed spectrum expanded to its Hermitian form,
+// real lines out.  Twiddles w^m = exp(-2 pi i m / nz) come from the same
+// host-computed table as the DFT's.
+// ---------------------------------------------------------------------------
+
+struct FftPlan {
+  int nf;
+  int radix[16];
+};
+
+__device__ __forceinline__ void cmul(double& ar, double& ai, double br, double bi) {
+  const double r = ar * br - ai * bi;
+  ai = ar * bi + ai * br;
+  ar = r;
+}
+
+// In-place length-R DFT of (vr, vi) with exponent sign s (-1 forward).
+template <int R>
+__device__ __forceinline__ void small_dft(double* vr, double* vi, double s) {
+  if (R == 2) {
+    const double ar = vr[0], ai = vi[0];
+    vr[0] = ar + vr[1];
+    vi[0] = ai + vi[1];
+    vr[1] = ar - vr[1];
+    vi[1] = ai - vi[1];
+  } else if (R == 4) {
+    const double t0r = vr[0] + vr[2], t0i = vi[0] + vi[2];
+    const double t1r = vr[0] - vr[2], t1i = vi[0] - vi[2];
+    const double t2r = vr[1] + vr[3], t2i = vi[1] + vi[3];
+    const double t3r = vr[1] - vr[3], t3i = vi[1] - vi[3];
+    // multiply t3 by s*i: (x + iy) * (s i) = -s y + i s x
+    const double ur = -s * t3i, ui = s * t3r;
+    vr[0] = t0r + t2r;
+    vi[0] = t0i + t2i;
+    vr[2] = t0r - t2r;
+    vi[2] = t0i - t2i;
+    vr[1] = t1r + ur;
+    vi[1] = t1i + ui;
+    vr[3] = t1r - ur;
+    vi[3] = t1i - ui;
+  } else if (R == 3) {
+    const double c = -0.5, sn = s * 0.86602540378443864676;  // sin(2 pi / 3)
+    const double sr = vr[1] + vr[2], si = vi[1] + vi[2];
+    const double dr = vr[1] - vr[2], di = vi[1] - vi[2];
+    const double ar = vr[0] + c * sr, ai = vi[0] + c * si;
+    vr[0] += sr;
+    vi[0] += si;
+    // (dr + i di) * (i sn) = -sn di + i sn dr
+    vr[1] = ar - sn * di;
+    vi[1] = ai + sn * dr;
+    vr[2] = ar + sn * di;
+    vi[2] = ai - sn * dr;
+  } else if (R == 5) {
+    const double c1 = 0.30901699437494742410, c2 = -0.80901699437494742410;   // cos(2pi/5), cos(4pi/5)
+    const double s1 = s * 0.95105651629515357212, s2 = s * 0.58778525229247312917;  // sin(2pi/5), sin(4pi/5)
+    const double a1r = vr[1] + vr[4], a1i = vi[1] + vi[4], b1r = vr[1] - vr[4], b1i = vi[1] - vi[4];
+    const double a2r = vr[2] + vr[3], a2i = vi[2] + vi[3], b2r = vr[2] - vr[3], b2i = vi[2] - vi[3];
+    const double x0r = vr[0], x0i = vi[0];
+    const double p1r = x0r + c1 * a1r + c2 * a2r, p1i = x0i + c1 * a1i + c2 * a2i;
+    const double p2r = x0r + c2 * a1r + c1 * a2r, p2i = x0i + c2 * a1i + c1 * a2i;
+    // q = i * (s1 b1 + s2 b2), r = i * (s2 b1 - s1 b2)
+    const double q1r = -(s1 * b1i + s2 * b2i), q1i = s1 * b1r + s2 * b2r;
+    const double q2r = -(s2 * b1i - s1 * b2i), q2i = s2 * b1r - s1 * b2r;
+    vr[0] = x0r + a1r + a2r;
+    vi[0] = x0i + a1i + a2i;
+    vr[1] = p1r + q1r;
+    vi[1] = p1i + q1i;
+    vr[4] = p1r - q1r;
+    vi[4] = p1i - q1i;
+    vr[2] = p2r + q2r;
+    vi[2] = p2i + q2i;
+    vr[3] = p2r - q2r;
+    vi[3] = p2i - q2i;
+  }
+}
+
+template <int R>
+__device__ __forceinline__ void stockham_stage(const double* xr, const double* xi, double* yr, double* yi, int N,
+                                               int Ns, int tp, const double* tw, double s) {
+  const int nj = N / R;
+  for (int w = threadIdx.x; w < nj * tp; w += blockDim.x) {
+    const int j = w / tp, p = w - j * tp;
+    const int k = j % Ns;
+    double vr[R], vi[R];
+#pragma unroll
+    for (int r = 0; r < R; ++r) {
+      vr[r] = xr[(j + r * nj) * tp + p];
+      vi[r] = xi[(j + r * nj) * tp + p];
+    }
+    // twiddle exp(s 2 pi i r k / (Ns R)) = table entry r*k*N/(Ns R)
+    const int step = N / (Ns * R);
+#pragma unroll
+    for (int r = 1; r < R; ++r) {
+      const int m = (r * k * step) % N;
+      cmul(vr[r], vi[r], tw[m], s * tw[N + m]);  // exp(s i theta) = cos + s i sin
+    }
+    small_dft<R>(vr, vi, s);
+    const int base = (j / Ns) * Ns * R + k;
+#pragma unroll
+    for (int r = 0; r < R; ++r) {
+      yr[(base + r * Ns) * tp + p] = vr[r];
+      yi[(base + r * Ns) * tp + p] = vi[r];
+    }
+  }
+}
+
+__global__ void k_fft(double* __restrict__ data, int nz, int plane_size, int sign, const double* __restrict__ twiddle,
+                      FftPlan plan, int tp) {
+  extern __shared__ double sm[];
+  double* tw = sm;                       // [2][nz]
+  double* ar = tw + 2 * nz;              // four [nz][tp] buffers
+  double* ai = ar + nz * tp;
+  double* br = ai + nz * tp;
+  double* bi = br + nz * tp;
+  const int p0 = blockIdx.x * tp;
+  const int N = nz, half = nz / 2;
+  for (int t = threadIdx.x; t < 2 * nz; t += blockDim.x) tw[t] = twiddle[t];
+  for (int t = threadIdx.x; t < nz * tp; t += blockDim.x) {
+    const int n = t / tp, p = t - n * tp;
+    const double v = (p0 + p < plane_size) ? data[static_cast<size_t>(n) * plane_size + p0 + p] : 0.0;
+    if (sign > 0) {
+      ar[t] = v;
+      ai[t] = 0.0;
+    } else {
+      // packed plane n -> Hermitian spectrum
+      if (n == 0) {
+        ar[p] = v;
+        ai[p] = 0.0;
+      } else if (n == 1) {
+        ar[half * tp + p] = v;
+        ai[half * tp + p] = 0.0;
+      } else {
+        const int kk = n >> 1;
+        if (n & 1) {
+          ai[kk * tp + p] = v;
+          ai[(N - kk) * tp + p] = -v;
+        } else {
+          ar[kk * tp + p] = v;
+          ar[(N - kk) * tp + p] = v;
+        }
+      }
+    }
+  }
+  __syncthreads();
+  const double s = sign > 0 ? -1.0 : 1.0;
+  double *xr = ar, *xi = ai, *yr = br, *yi = bi;
+  int Ns = 1;
+  for (int f = 0; f < plan.nf; ++f) {
+    const int R = plan.radix[f];
+    if (R == 4) stockham_stage<4>(xr, xi, yr, yi, N, Ns, tp, tw, s);
+    else if (R == 2) stockham_stage<2>(xr, xi, yr, yi, N, Ns, tp, tw, s);
+    else if (R == 3) stockham_stage<3>(xr, xi, yr, yi, N, Ns, tp, tw, s);
+    else stockham_stage<5>(xr, xi, yr, yi, N, Ns, tp, tw, s);
+    Ns *= R;
+    double* t0 = xr;
+    xr = yr;
+    yr = t0;
+    t0 = xi;
+    xi = yi;
+    yi = t0;
+    __syncthreads();
+  }
+  const double scale = 1.0 / nz;
+  for (int t = threadIdx.x; t < nz * tp; t += blockDim.x) {
+    const int n = t / tp, p = t - n * tp;
+    if (p0 + p >= plane_size) continue;
+    double v;
+    if (sign > 0) {
+      if (n == 0) v = xr[p] * scale;
+      else if (n == 1) v = xr[half * tp + p] * scale;
+      else if (n & 1) v = xi[(n >> 1) * tp + p] * scale;
+      else v = xr[(n >> 1) * tp + p] * scale;
+    } else {
+      v = xr[t];
+    }
+    data[static_cast<size_t>(n) * plane_size + p0 + p] = v;
+  }
+}
+
 __global__ void k_nz2(double* data, int plane_size, int sign) {
   const int p = blockIdx.x * blockDim.x + threadIdx.x;
   if (p >= plane_size) return;
@@ -80,12 +264,32 @@ cudaError_t z_transform(double* data, int nz, int plane_size, int sign, const do
     k_nz2<<<(plane_size + 255) / 256, 256, 0, st>>>(data, plane_size, sign);
     return cudaGetLastError();
   }
-  const size_t shm = sizeof(double) * (2 * static_cast<size_t>(nz) * kTP + 2 * nz);
+  // Stockham FFT when nz factors into 2, 3, 5 (radix 4 first)
+  FftPlan plan{};
+  {
+    int n = nz;
+    while (n % 4 == 0 && plan.nf < 16) { plan.radix[plan.nf++] = 4; n /= 4; }
+    while (n % 2 == 0 && plan.nf < 16) { plan.radix[plan.nf++] = 2; n /= 2; }
+    while (n % 3 == 0 && plan.nf < 16) { plan.radix[plan.nf++] = 3; n /= 3; }
+    while (n % 5 == 0 && plan.nf < 16) { plan.radix[plan.nf++] = 5; n /= 5; }
+    if (n != 1) plan.nf = 0;
+  }
   static bool attr_set = false;
   if (!attr_set) {
     cudaFuncSetAttribute(k_dft, cudaFuncAttributeMaxDynamicSharedMemorySize, 200 * 1024);
+    cudaFuncSetAttribute(k_fft, cudaFuncAttributeMaxDynamicSharedMemorySize, 200 * 1024);
     attr_set = true;
   }
+  if (plan.nf > 0) {
+    int tp = 32;
+    while (tp > 4 && sizeof(double) * (4 * static_cast<size_t>(nz) * tp + 2 * nz) > 160 * 1024) tp /= 2;
+    const size_t fshm = sizeof(double) * (4 * static_cast<size_t>(nz) * tp + 2 * nz);
+    if (fshm <= 200 * 1024) {
+      k_fft<<<(plane_size + tp - 1) / tp, 256, fshm, st>>>(data, nz, plane_size, sign, twiddle, plan, tp);
+      return cudaGetLastError();
+    }
+  }
+  const size_t shm = sizeof(double) * (2 * static_cast<size_t>(nz) * kTP + 2 * nz);
   k_dft<<<(plane_size + kTP - 1) / kTP, 256, shm, st>>>(data, nz, plane_size, sign, twiddle);
   return cudaGetLastError();
 }

@@ -85,11 +85,13 @@ def test_device_solve_and_transform(tmp_path):
     assert rel_l2(U.to_numpy(), Uo) < TOL
 
 
-def test_transform_roundtrip_odd_factors(tmp_path):
-    p = sessions.helmholtz_session(str(tmp_path / "t"), 2, 5, nz=12)
+@pytest.mark.parametrize("nz", [4, 6, 10, 12, 14, 64, 96])
+def test_transform_roundtrip_odd_factors(tmp_path, nz):
+    # radix 4/2/3/5 FFT paths, and the DFT for a factor outside 2, 3, 5 (14)
+    p = sessions.helmholtz_session(str(tmp_path / "t"), 2, 5, nz=nz)
     ctx = S.Context(p)
-    rng = np.random.default_rng(3)
-    f = rng.standard_normal((12, 4, 5, 5))
+    rng = np.random.default_rng(nz)
+    f = rng.standard_normal((nz, 4, 5, 5))
     F = ctx.new_field().load_physical(f)
     F.transform(S.FORWARD)
     assert rel_l2(F.to_numpy(), O.dft_forward(f)) < 1e-14
