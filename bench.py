@@ -112,11 +112,12 @@ def measured_peaks():
     return 6650.0, "fallback"
 
 
-def load_profile_traffic():
-    """DRAM bytes per launch of the banded sweep from the committed ncu summary."""
-    p = os.path.join(ROOT, "profiles", "band_solve_c2.json")
+def load_profile_traffic(phase):
+    """DRAM bytes (read + write) of one launch of a solve phase, from the
+    committed ncu summary of the same workload (profiles/c2_solve_traffic.json)."""
+    p = os.path.join(ROOT, "profiles", "c2_solve_traffic.json")
     if os.path.exists(p):
-        return json.load(open(p)).get("dram_bytes_per_launch")
+        return json.load(open(p)).get("dram_bytes_per_phase", {}).get(phase)
     return None
 
 
@@ -222,7 +223,7 @@ def run_ours(args):
     d = tempfile.mkdtemp()
     session = make_session(d)
     t0 = time.perf_counter()
-    ctx = S.Context(session, device=local)
+    ctx = S.Context(session, {"STX_TWOLEVEL": 0} if args.solver == "band" else None, device=local)
     x, y = ctx.mesh_coords()
     f, nuniq = forcing_per_unique_node(x, y, ctx.nz, w["seed"])
     sysm = S.ModalMatrixSys(ctx, "c", w["lambda2"], w["beta"])
@@ -294,7 +295,7 @@ def run_ours(args):
     top = int(np.argmax(phase_ms))
     peak, kind = measured_peaks()
     achieved = phase_bytes[top] / (phase_ms[top] / 1e3) / 1e9
-    traffic = load_profile_traffic()
+    traffic = load_profile_traffic(phase_names[top])
     # CPU baseline: the oracle on one core over a bounded sample of planes
     cpu = None
     if not args.no_cpu_baseline:
@@ -372,6 +373,8 @@ def main():
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--dns-steps", type=int, default=20,
                     help="timed steps of the secondary DNS measurement (0 to skip)")
+    ap.add_argument("--solver", default="twolevel", choices=["twolevel", "band"],
+                    help="band: the single banded-Cholesky skeleton solve (for comparison)")
     ap.add_argument("--workload", default="c2", choices=["c2", "dns"],
                     help="dns: run only the DNS measurement (one JSON line)")
     args = ap.parse_args()
