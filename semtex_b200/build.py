@@ -67,7 +67,7 @@ def build(force: bool = False, verbose: bool = False, ptxas_verbose: bool = Fals
             todo.append(s)
     with cf.ThreadPoolExecutor(max_workers=os.cpu_count() or 4) as ex:
         for obj, err in ex.map(lambda s: _compile(s, ptxas_verbose), todo):
-            if verbose and err.strip():
+            if err.strip() and (verbose or "warning" in err):
                 print(err, file=sys.stderr)
     objs = [_obj(s) for s in cpp + cu]
     if todo or not os.path.exists(LIB):

@@ -22,6 +22,7 @@
 #include "host/mesh.hpp"
 #include "host/session.hpp"
 #include "kernels/helmholtz.cuh"
+#include "kernels/element.cuh"
 #include "stx_internal.hpp"
 
 namespace {
@@ -449,6 +450,36 @@ int stx_modal_create(stx_context* ctx, char field, double lambda2, double beta, 
       d.betak2 = upload(st->arena, bk2);
       d.nsolve = upload(st->arena, ns);
       d.l2 = 0;
+      d.ew = d.eb = nullptr;
+      d.ew_ld = d.eb_ld = 0;
+      if (method == STX_DIRECT) {
+        // Element operators for the element kernels, per family and mode,
+        // rows zero-padded to element_ld: the recovery operator row i =
+        // (-hbi[b][i] for the element-boundary nodes b, hii^-1[i][j]), so the
+        // interior solution is one product with the column (u_b, F_i); the
+        // condensation operator row b = hbi[b][.].
+        const int nx = M.next, ni = M.nint, ldw = element_ld(M.npnp), ldc = element_ld(ni);
+        const size_t nf = static_cast<size_t>(num_modes) * M.nfamily;
+        std::vector<double> ew(nf * ni * ldw, 0.0), eb(nf * nx * ldc, 0.0);
+        for (int m = 0; m < num_modes; ++m)
+          for (int f = 0; f < M.nfamily; ++f) {
+            const size_t fm = static_cast<size_t>(m) * M.nfamily + f;
+            const double* hb = modes[m].hbi.data() + static_cast<size_t>(f) * nx * ni;
+            const double* hi = modes[m].hii.data() + static_cast<size_t>(f) * ni * ni;
+            double* w = ew.data() + fm * ni * ldw;
+            for (int i = 0; i < ni; ++i) {
+              for (int b = 0; b < nx; ++b) w[static_cast<size_t>(i) * ldw + b] = -hb[static_cast<size_t>(b) * ni + i];
+              for (int j = 0; j < ni; ++j) w[static_cast<size_t>(i) * ldw + nx + j] = hi[static_cast<size_t>(i) * ni + j];
+            }
+            double* c = eb.data() + fm * nx * ldc;
+            for (int b = 0; b < nx; ++b)
+              for (int j = 0; j < ni; ++j) c[static_cast<size_t>(b) * ldc + j] = hb[static_cast<size_t>(b) * ni + j];
+          }
+        d.ew = upload(st->arena, ew.empty() ? std::vector<double>{0.0, 0.0} : ew);
+        d.eb = upload(st->arena, eb.empty() ? std::vector<double>{0.0, 0.0} : eb);
+        d.ew_ld = ldw;
+        d.eb_ld = ldc;
+      }
       if (method == STX_DIRECT && P) {
         std::vector<double> hbi, hii, sinv, g, gt, ainv;
         std::vector<int> pin(num_modes, -1);

@@ -57,6 +57,11 @@ struct DevModal {
   const int* nsolve;              // [nmodes]
   const double* hbi;              // [nmodes][nfamily][next][nint]
   const double* hii;              // [nmodes][nfamily][nint][nint]
+  // Element operators in the padded layout of the element kernels:
+  const double* ew;               // [nmodes][nfamily][nint][ew_ld]: row i = (-hbi[.][i], hii^-1[i][.], 0...)
+  int ew_ld;
+  const double* eb;               // [nmodes][nfamily][next][eb_ld]: row b = (hbi[b][.], 0...)
+  int eb_ld;
   const double* fwd;              // [nmodes][mode_stride]: rows of U^T, stride nbp
   const double* bwd;              // [nmodes][mode_stride]: rows of reversed U
   const double* dinv_fwd;         // [nmodes][dinv_stride]: 16x16 inverse diagonal blocks

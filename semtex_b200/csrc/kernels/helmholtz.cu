@@ -16,6 +16,8 @@
 //      src/field.cpp:1106-1124).
 #include "helmholtz.cuh"
 #include "twolevel.cuh"
+#include "ptx.cuh"
+#include "element.cuh"
 
 #include <algorithm>
 #include <vector>
@@ -173,6 +175,8 @@ __global__ void k_recover(DevGeom g, DevNumbering N, DevModal S,
 
 constexpr int kTile = 4;
 
+constexpr int kGather = 4;
+
 // Constrained forcing -(Q4 f + [emask] H g) of the chunk's elements for the
 // planes of mode m into columns of sB (column c = slot*cnt + l, row =
 // boundary-major node, stride ldb).  The lift term H g is formed one column
@@ -180,24 +184,41 @@ constexpr int kTile = 4;
 // where the element's essential values are all zero (H 0 = 0).
 __device__ void chunk_forcing2(const DevGeom& g, const DevNumbering& N, const double* __restrict__ F,
                                const double* __restrict__ G, int gstride, double hcon, const int* el, int cnt, int m,
-                               int nr, double* sB, int ldb, double* wsc, const double* sD) {
+                               int nr, double* sB, int ldb, double* wsc, const double* sD, int lift_warps = 8) {
   const int nn = g.npnp, np = g.np;
-#pragma unroll 8
-  for (int w = threadIdx.x; w < nr * cnt * nn; w += blockDim.x) {
-    const int c = w / nn, t = w - c * nn;
-    const int slot = c / cnt, l = c - slot * cnt;
-    const int k = 2 * m + slot;
-    const int e = el[l];
-    sB[c * ldb + g.pmap[t]] =
-        -g.Q4[e * nn + t] * F[static_cast<size_t>(k) * g.plane_size + static_cast<size_t>(e) * nn + t];
+  // One warp per column (nr <= 2, so slot = col >= cnt), lanes over the
+  // element's nodes in natural order: coalesced rows of F and Q4, all loads
+  // of a batch issued before its shared-memory stores.
+  const int wp = threadIdx.x >> 5, ln = threadIdx.x & 31, nwp = blockDim.x >> 5;
+  for (int col = wp; col < nr * cnt; col += nwp) {
+    const int slot = col >= cnt ? 1 : 0, l = col - slot * cnt;
+    const int e = __ldg(el + l);
+    const double* f = F + static_cast<size_t>(2 * m + slot) * g.plane_size + static_cast<size_t>(e) * nn;
+    const double* q = g.Q4 + static_cast<size_t>(e) * nn;
+    double* b = sB + col * ldb;
+    for (int t0 = ln; t0 < nn; t0 += 32 * kGather) {
+      double v[kGather];
+      int d[kGather];
+#pragma unroll
+      for (int u = 0; u < kGather; ++u) {
+        const int t = t0 + 32 * u;
+        d[u] = t < nn ? __ldg(g.pmap + t) : -1;
+        v[u] = t < nn ? -__ldg(q + t) * __ldg(f + t) : 0.0;
+      }
+#pragma unroll
+      for (int u = 0; u < kGather; ++u)
+        if (d[u] >= 0) b[d[u]] = v[u];
+    }
   }
   __syncthreads();
   if (!G) return;
-  const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31, nwarp = blockDim.x >> 5;
+  // warps [0, lift_warps) form the lift, each in its own 3*nn scratch
+  const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31,
+            nwarp = min(lift_warps, static_cast<int>(blockDim.x >> 5));
   double* su = wsc + static_cast<size_t>(warp) * 3 * nn;
   double* sR = su + nn;
   double* sS = sR + nn;
-  for (int c = warp; c < nr * cnt; c += nwarp) {
+  for (int c = warp; warp < nwarp && c < nr * cnt; c += nwarp) {
     const int slot = c / cnt, l = c - slot * cnt;
     const int k = 2 * m + slot;
     const int e = el[l];
@@ -699,51 +720,7 @@ __global__ void k_pcg_tail(PcgScalars* sc, const double* rho1, const double* r2,
 // expiry the kernel records an error in S.status and stops.
 // ---------------------------------------------------------------------------
 
-__device__ __forceinline__ uint32_t smem_u32(const void* p) {
-  return static_cast<uint32_t>(__cvta_generic_to_shared(p));
-}
 
-__device__ __forceinline__ void mbar_init(uint64_t* bar, unsigned count) {
-  asm volatile("mbarrier.init.shared::cta.b64 [%0], %1;" ::"r"(smem_u32(bar)), "r"(count));
-}
-
-__device__ __forceinline__ void mbar_expect_tx(uint64_t* bar, unsigned bytes) {
-  asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;" ::"r"(smem_u32(bar)),
-               "r"(bytes)
-               : "memory");
-}
-
-__device__ __forceinline__ void bulk_g2s(void* dst, const void* src, unsigned bytes, uint64_t* bar) {
-  asm volatile(
-      "cp.async.bulk.shared::cluster.global.mbarrier::complete_tx::bytes [%0], [%1], %2, [%3];" ::"r"(
-          smem_u32(dst)),
-      "l"(src), "r"(bytes), "r"(smem_u32(bar))
-      : "memory");
-}
-
-__device__ __forceinline__ unsigned long long global_ns() {
-  unsigned long long t;
-  asm volatile("mov.u64 %0, %%globaltimer;" : "=l"(t));
-  return t;
-}
-
-// Bounded wait (about 2 s of wall time) for phase `parity` of an mbarrier;
-// false if the bound expired.
-__device__ __forceinline__ bool mbar_wait(uint64_t* bar, unsigned parity) {
-  const uint32_t a = smem_u32(bar);
-  const unsigned long long t0 = global_ns();
-  for (;;) {
-    uint32_t done;
-    asm volatile(
-        "{\n .reg .pred p;\n mbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2;\n"
-        " selp.u32 %0, 1, 0, p;\n}\n"
-        : "=r"(done)
-        : "r"(a), "r"(parity)
-        : "memory");
-    if (done) return true;
-    if (global_ns() - t0 > 2000000000ull) return false;
-  }
-}
 
 constexpr int kSweepWarps = 1 + kBandRows;  // one chain warp + one warp per block row
 constexpr int kSweepThreads = 32 * kSweepWarps;
@@ -967,7 +944,10 @@ cudaError_t helmholtz_direct_solve(const DevGeom& g, const DevNumbering& N, cons
   const size_t shm_cond = sizeof(double) * (2 * cm * ldb + g.np * g.np + wsc);
   const size_t shm_rec = sizeof(double) * (2 * cm * ldb + 2 * cm * ldu + g.np * g.np + wsc);
   const bool chunked = g.nchunk > 0 && shm_rec <= 200 * 1024;
-  if (chunked) {
+  const ElementPlan ep = element_plan(g, S, has_ess);
+  if (ep.ok) {
+    element_condense(ep, g, N, S, F, has_ess ? G : nullptr, rstride, R, rstride, st);
+  } else if (chunked) {
     static int configured = 0;
     if (!configured) {
       cudaFuncSetAttribute(k_condense_chunk, cudaFuncAttributeMaxDynamicSharedMemorySize, 200 * 1024);
@@ -1006,7 +986,9 @@ cudaError_t helmholtz_direct_solve(const DevGeom& g, const DevNumbering& N, cons
     k_band_solve<<<S.nmodes, 256, 0, st>>>(S, S.bwd, R, rstride, nz, 1);
   }
   if (ev) cudaEventRecord(ev[3], st);
-  if (chunked)
+  if (ep.ok)
+    element_recover(ep, g, N, S, F, has_ess ? G : nullptr, rstride, R, rstride, U, st);
+  else if (chunked)
     k_recover_chunk<<<dim3(g.nchunk, S.nmodes), 256, shm_rec, st>>>(g, N, S, F, has_ess ? G : nullptr, rstride,
                                                                     R, rstride, U);
   else
