@@ -23,6 +23,7 @@
 #include "host/session.hpp"
 #include "kernels/helmholtz.cuh"
 #include "kernels/element.cuh"
+#include "kernels/symtile.hpp"
 #include "stx_internal.hpp"
 
 namespace {
@@ -481,18 +482,42 @@ int stx_modal_create(stx_context* ctx, char field, double lambda2, double beta, 
         d.eb_ld = ldc;
       }
       if (method == STX_DIRECT && P) {
-        std::vector<double> hbi, hii, sinv, g, gt, ainv;
+        // Two-level data: the patch-interior inverses S_II^-1 (one per patch
+        // family and mode) and the interface inverse (one per mode), packed
+        // symmetric; the transposed element Schur complements; per element
+        // node its class (essential / patch-interior / interface).
+        const int nx = M.next;
+        std::vector<double> hbi, hii, sct, pack;
+        std::vector<long long> fam_off(static_cast<size_t>(num_modes) * P->nfamily), if_off(num_modes);
         std::vector<int> pin(num_modes, -1);
+        const size_t nI_max = std::max(1, P->nI_max);
         for (int m = 0; m < num_modes; ++m) {
           hbi.insert(hbi.end(), modes[m].hbi.begin(), modes[m].hbi.end());
           hii.insert(hii.end(), modes[m].hii.begin(), modes[m].hii.end());
-          sinv.insert(sinv.end(), modes[m].l2_sinv.begin(), modes[m].l2_sinv.end());
-          g.insert(g.end(), modes[m].l2_g.begin(), modes[m].l2_g.end());
-          gt.insert(gt.end(), modes[m].l2_gt.begin(), modes[m].l2_gt.end());
-          ainv.insert(ainv.end(), modes[m].l2_ainv.begin(), modes[m].l2_ainv.end());
+          for (int f = 0; f < M.nfamily; ++f) {
+            const double* h = modes[m].hsc.data() + static_cast<size_t>(f) * nx * nx;
+            for (int b = 0; b < nx; ++b)
+              for (int a = 0; a < nx; ++a) sct.push_back(h[static_cast<size_t>(a) * nx + b]);
+          }
+          for (int f = 0; f < P->nfamily; ++f) {
+            const int n = P->nI[P->family_rep[f]];
+            fam_off[static_cast<size_t>(m) * P->nfamily + f] = static_cast<long long>(pack.size());
+            pack.resize(pack.size() + sym_size(n), 0.0);
+            sym_pack(n, modes[m].l2_sinv.data() + static_cast<size_t>(f) * nI_max * nI_max, nI_max,
+                     pack.data() + fam_off[static_cast<size_t>(m) * P->nfamily + f]);
+          }
+          if_off[m] = static_cast<long long>(pack.size());
+          pack.resize(pack.size() + sym_size(P->niface), 0.0);
+          sym_pack(P->niface, modes[m].l2_ainv.data(), P->niface, pack.data() + if_off[m]);
           pin[m] = modes[m].pin_iid;
           modes[m] = ModeSystem();
         }
+        std::vector<int> ncls(static_cast<size_t>(M.nel) * nx, 0);
+        for (int e = 0; e < M.nel; ++e)
+          for (int a = 0; a < nx; ++a) {
+            const int gi = N.btog[static_cast<size_t>(e) * nx + a];
+            ncls[static_cast<size_t>(e) * nx + a] = gi >= N.nsolve ? 0 : (P->iface_of[gi] >= 0 ? 2 : 1);
+          }
         d.l2 = 1;
         d.npatch = P->npatch;
         d.pfam = P->nfamily;
@@ -505,14 +530,43 @@ int stx_modal_create(stx_context* ctx, char field, double lambda2, double beta, 
         d.p_Igid = upload(st->arena, P->I_gid);
         d.p_Biid = upload(st->arena, P->B_iid);
         d.skel_of = upload(st->arena, P->skel_of.empty() ? std::vector<int>{0} : P->skel_of);
-
         d.pin = upload(st->arena, pin);
         d.hbi = upload(st->arena, hbi);
         d.hii = upload(st->arena, hii);
-        d.l2_sinv = upload(st->arena, sinv);
-        d.l2_g = upload(st->arena, g);
-        d.l2_gt = upload(st->arena, gt);
-        d.l2_ainv = upload(st->arena, ainv.empty() ? std::vector<double>{0.0} : ainv);
+        d.l2_pack = upload(st->arena, pack.empty() ? std::vector<double>(32, 0.0) : pack);
+        d.l2_sct = upload(st->arena, sct);
+        d.l2_ncls = upload(st->arena, ncls);
+        // work items: the tiles of S_II^-1 per (patch, mode) and of the
+        // interface inverse per mode, in runs
+        std::vector<SymItem> ip, ii;
+        // work items of about 24 tiles (6 per warp): enough items to even
+        // out the waves of resident blocks, few enough x gathers per item
+        auto nparts = [](int nt) { return std::max(1, (nt + 12) / 24); };
+        for (int m = 0; m < num_modes; ++m)
+          for (int p = 0; p < P->npatch; ++p) {
+            const int n = P->nI[p];
+            if (n <= 0) continue;
+            const int nt = sym_ntiles(n), parts = nparts(nt);
+            for (int k = 0; k < parts; ++k)
+              ip.push_back(SymItem{fam_off[static_cast<size_t>(m) * P->nfamily + P->family[p]], n, m,
+                                   static_cast<int>(static_cast<long long>(nt) * k / parts),
+                                   static_cast<int>(static_cast<long long>(nt) * (k + 1) / parts), -1,
+                                   d.p_Igid + static_cast<size_t>(p) * nI_max});
+          }
+        if (P->niface > 0) {
+          const int nt = sym_ntiles(P->niface);
+          const int parts = nparts(nt);
+          for (int m = 0; m < num_modes; ++m)
+            for (int k = 0; k < parts; ++k) {
+              const int q0 = static_cast<int>(static_cast<long long>(nt) * k / parts);
+              const int q1 = static_cast<int>(static_cast<long long>(nt) * (k + 1) / parts);
+              if (q1 > q0) ii.push_back(SymItem{if_off[m], P->niface, m, q0, q1, pin[m], d.skel_of});
+            }
+        }
+        d.items_patch = ip.empty() ? nullptr : upload(st->arena, ip);
+        d.n_items_patch = static_cast<int>(ip.size());
+        d.items_iface = ii.empty() ? nullptr : upload(st->arena, ii);
+        d.n_items_iface = static_cast<int>(ii.size());
         d.fwd = d.bwd = d.dinv_fwd = d.dinv_bwd = nullptr;
         d.nbp = 0;
         d.mode_stride = d.dinv_stride = 0;
@@ -663,14 +717,15 @@ int stx_modal_bytes(const stx_modal* sys, double* bytes) {
     bytes[0] = field + fam * M.next * M.nint + rhs;
     bytes[3] = 2 * field + fam * (M.next * M.nint + static_cast<double>(M.nint) * M.nint) + rhs;
     if (d.l2) {
+      // first half: S_II^-1 products (packed, once per patch family and
+      // mode), element Schur complements, interface products (packed);
+      // second half: the element Schur complements and S_II^-1 again
       const Patching* P = ctx->fields.at(sys->field).P.get();
       double pm = 0;
-      for (int f = 0; f < P->nfamily; ++f) {
-        const int p = P->family_rep[f];
-        pm += static_cast<double>(P->nI[p]) * P->nI[p] + 2.0 * P->nI[p] * P->nB[p];
-      }
-      bytes[1] = w * nm * (pm + static_cast<double>(d.niface) * d.niface) + 4 * rhs;
-      bytes[2] = 0.0;
+      for (int f = 0; f < P->nfamily; ++f) pm += static_cast<double>(sym_size(P->nI[P->family_rep[f]]));
+      const double sc = static_cast<double>(M.nfamily) * M.next * M.next;
+      bytes[1] = w * nm * (pm + sc + static_cast<double>(sym_size(d.niface))) + 4 * rhs;
+      bytes[2] = w * nm * (pm + sc) + 3 * rhs;
     } else {
       double band = 0;
       for (int m = 0; m < nm; ++m) band += w * static_cast<double>(sys->store->nsolve[m]) * d.nband;

@@ -232,7 +232,7 @@ ModeSystem build_mode_system(const Mesh& M, const Numbering& N, const Patching* 
     //    skeleton nodes; assemble the interface Schur complements.
     const int nI_max = std::max(1, P->nI_max), nB_max = std::max(1, P->nB_max);
     S.l2_sinv.assign(static_cast<size_t>(P->nfamily) * nI_max * nI_max, 0.0);
-    S.l2_g.assign(static_cast<size_t>(P->nfamily) * nI_max * nB_max, 0.0);
+    std::vector<double> l2_g(static_cast<size_t>(P->nfamily) * nI_max * nB_max, 0.0);  // S_II^-1 S_IB
     std::vector<std::vector<double>> T(P->nfamily);
     for (int f = 0; f < P->nfamily; ++f) {
       const int p = P->family_rep[f];
@@ -251,7 +251,7 @@ ModeSystem build_mode_system(const Mesh& M, const Numbering& N, const Patching* 
         }
       }
       double* Si = &S.l2_sinv[static_cast<size_t>(f) * nI_max * nI_max];
-      double* G = &S.l2_g[static_cast<size_t>(f) * nI_max * nB_max];
+      double* G = &l2_g[static_cast<size_t>(f) * nI_max * nB_max];
       std::vector<double> II(static_cast<size_t>(nI) * nI);
       for (int a = 0; a < nI; ++a)
         for (int b = 0; b < nI; ++b) II[static_cast<size_t>(a) * nI + b] = Sp[static_cast<size_t>(a) * nl + b];
@@ -275,12 +275,7 @@ ModeSystem build_mode_system(const Mesh& M, const Numbering& N, const Patching* 
         }
     }
     const int ni = P->niface;
-    S.l2_gt.assign(S.l2_g.size(), 0.0);
-    for (int f = 0; f < P->nfamily; ++f)
-      for (int a = 0; a < nI_max; ++a)
-        for (int b = 0; b < nB_max; ++b)
-          S.l2_gt[(static_cast<size_t>(f) * nB_max + b) * nI_max + a] =
-              S.l2_g[(static_cast<size_t>(f) * nI_max + a) * nB_max + b];
+    S.hsc = hbb_all;
     std::vector<double>& A = S.l2_ainv;
     A.assign(static_cast<size_t>(ni) * ni, 0.0);
     for (int p = 0; p < P->npatch; ++p) {

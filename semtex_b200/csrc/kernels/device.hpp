@@ -45,6 +45,16 @@ struct DevNumbering {
   const double* edge_area;  // [nedge*np]
 };
 
+// One packed symmetric product y += A x for the planes of a Fourier mode:
+// tiles [q0, q1) of the matrix at l2_pack + moff (order n); x_i is read and
+// y_i accumulated at position idx[i] of the planes' skeleton vectors
+// (x_pin taken as zero).
+struct SymItem {
+  long long moff;
+  int n, mode, q0, q1, pin;
+  const int* idx;
+};
+
 // A ModalMatrixSys on the device: one MatrixSys per locally held mode.
 struct DevModal {
   int nmodes, method, nfamily;
@@ -69,8 +79,8 @@ struct DevModal {
   int* status;                    // device status word (0 = ok)
   const double* pc;               // JACPCG: [nmodes][npts]
   int npts;
-  // Two-level condensation (patches + dense interface inverse); l2 = 0 when
-  // the single banded factor above is used instead.
+  // Two-level condensation (patches + interface system, both through packed
+  // symmetric inverses); l2 = 0 when the single banded factor above is used.
   int l2;
   int npatch, pfam, nI_max, nB_max, niface;
   const int* p_family;            // [npatch]
@@ -80,10 +90,13 @@ struct DevModal {
   const int* p_Biid;              // [npatch][nB_max] interface ids of boundary nodes
   const int* skel_of;             // [niface] skeleton id of each interface unknown
   const int* pin;                 // [nmodes] pinned interface id or -1
-  const double* l2_sinv;          // [nmodes][pfam][nI_max][nI_max]
-  const double* l2_g;             // [nmodes][pfam][nI_max][nB_max]
-  const double* l2_gt;            // [nmodes][pfam][nB_max][nI_max]
-  const double* l2_ainv;          // [nmodes][niface][niface]
+  const double* l2_pack;          // packed symmetric inverses (symtile.hpp layout)
+  const SymItem* items_patch;     // S_II^-1 products: one per (patch, mode)
+  int n_items_patch;
+  const SymItem* items_iface;     // interface products: (mode, tile range)
+  int n_items_iface;
+  const double* l2_sct;           // [nmodes][nfamily][next][next] element Schur complements, transposed
+  const int* l2_ncls;             // [nel][next]: 0 essential, 1 patch-interior, 2 interface node
 };
 
 }  // namespace stx

@@ -910,7 +910,7 @@ SweepPlan sweep_plan(int nbp, int nband) {
 
 size_t helmholtz_workspace_doubles(const DevGeom& g, const DevNumbering& N, const DevModal& S) {
   const size_t stride = (static_cast<size_t>(N.nglobal) + 31) / 32 * 32;
-  return 2 * stride * g.nz + (S.l2 ? twolevel_workspace_doubles(S, g.nz) : 0);
+  return 2 * stride * g.nz + (S.l2 ? twolevel_workspace_doubles(static_cast<int>(stride), g.nz) : 0);
 }
 
 int helmholtz_direct_launches(const DevNumbering& N, const DevModal& S, int np) {
@@ -965,10 +965,12 @@ cudaError_t helmholtz_direct_solve(const DevGeom& g, const DevNumbering& N, cons
   }
   if (ev) cudaEventRecord(ev[1], st);
   const SweepPlan plan = S.l2 ? SweepPlan() : sweep_plan(S.nbp, S.nband);
+  const double* Rsol = R;  // skeleton solution
   if (S.l2) {
-    err = twolevel_solve(S, R, rstride, work + 2 * static_cast<size_t>(rstride) * nz, nz, st);
+    double* w2 = work + 2 * static_cast<size_t>(rstride) * nz;
+    err = twolevel_solve(S, g, N, R, rstride, w2, nz, st, ev ? ev[2] : nullptr);
     if (err != cudaSuccess) return err;
-    if (ev) cudaEventRecord(ev[2], st);
+    Rsol = twolevel_solution(w2, rstride, nz);
   } else if (plan.stages >= 2) {
     static int configured = 0;
     if (!configured) {
@@ -987,13 +989,13 @@ cudaError_t helmholtz_direct_solve(const DevGeom& g, const DevNumbering& N, cons
   }
   if (ev) cudaEventRecord(ev[3], st);
   if (ep.ok)
-    element_recover(ep, g, N, S, F, has_ess ? G : nullptr, rstride, R, rstride, U, st);
+    element_recover(ep, g, N, S, F, has_ess ? G : nullptr, rstride, Rsol, rstride, U, st);
   else if (chunked)
     k_recover_chunk<<<dim3(g.nchunk, S.nmodes), 256, shm_rec, st>>>(g, N, S, F, has_ess ? G : nullptr, rstride,
-                                                                    R, rstride, U);
+                                                                    Rsol, rstride, U);
   else
     k_recover<<<egrid, threads, shm + sizeof(double) * g.next, st>>>(g, N, S, F, has_ess ? G : nullptr,
-                                                                     rstride, R, rstride, U);
+                                                                     rstride, Rsol, rstride, U);
   if (ev) cudaEventRecord(ev[4], st);
   return cudaGetLastError();
 }

@@ -1,0 +1,71 @@
+// Packed storage of a symmetric n x n matrix for the tiled products of the
+// two-level skeleton solve: the lower triangle of 32 x 32 tiles (I >= J),
+// tile-row-major, the last tile row only as tall as the matrix needs
+// (h = n - 32 (T - 1) rows, stored rounded up to even).  Diagonal tiles hold
+// both triangles; columns past n are zero.  Within a tile, row r occupies 33
+// doubles (entry (r, c) at r*33 + c, the 33rd zero), so that a warp reading
+// a tile row (lanes over c) or a tile column (lanes over r) touches every
+// bank pair once and every address is a constant offset.  Tiles are
+// multiples of 16 bytes and start on 16-byte boundaries: one bulk copy each.
+#pragma once
+
+#include <cstddef>
+
+namespace stx {
+
+constexpr int kSymTile = 32;
+constexpr int kSymLd = kSymTile + 1;
+
+__host__ __device__ inline int sym_tiles(int n) { return (n + kSymTile - 1) / kSymTile; }
+
+__host__ __device__ inline int sym_last_rows(int n) { return n - kSymTile * (sym_tiles(n) - 1); }
+
+// Rows of tile row I, and rows stored for it.
+__host__ __device__ inline int sym_rows(int n, int I) { return I < sym_tiles(n) - 1 ? kSymTile : sym_last_rows(n); }
+__host__ __device__ inline int sym_rows_stored(int n, int I) { return (sym_rows(n, I) + 1) / 2 * 2; }
+
+// Doubles of the packed matrix.
+__host__ __device__ inline long long sym_size(int n) {
+  if (n <= 0) return 0;
+  const long long T = sym_tiles(n), hs = (sym_last_rows(n) + 1) / 2 * 2;
+  return (T - 1) * T / 2 * kSymTile * kSymLd + T * hs * kSymLd;
+}
+
+// Doubles from the matrix start to tile (I, J), J <= I.
+__host__ __device__ inline long long sym_tile_offset(int n, int I, int J) {
+  const int T = sym_tiles(n);
+  const long long full = static_cast<long long>(kSymTile) * kSymLd;
+  if (I < T - 1) return (static_cast<long long>(I) * (I + 1) / 2 + J) * full;
+  return static_cast<long long>(T - 1) * T / 2 * full + static_cast<long long>(J) * sym_rows_stored(n, I) * kSymLd;
+}
+
+// Number of tiles and the tile (I, J) at packed position q (row-major over J <= I).
+__host__ __device__ inline int sym_ntiles(int n) {
+  const int T = sym_tiles(n);
+  return T * (T + 1) / 2;
+}
+
+__host__ __device__ inline void sym_tile_at(int q, int& I, int& J) {
+  int i = 0;
+  while ((i + 1) * (i + 2) / 2 <= q) ++i;
+  I = i;
+  J = q - i * (i + 1) / 2;
+}
+
+// Pack the symmetric matrix A (row-major, leading dimension lda) into out
+// (sym_size(n) doubles, zero-initialised by the caller).
+inline void sym_pack(int n, const double* A, size_t lda, double* out) {
+  const int T = sym_tiles(n);
+  for (int I = 0; I < T; ++I)
+    for (int J = 0; J <= I; ++J) {
+      double* t = out + sym_tile_offset(n, I, J);
+      const int h = sym_rows(n, I);
+      for (int r = 0; r < h; ++r)
+        for (int c = 0; c < kSymTile; ++c) {
+          const int i = kSymTile * I + r, j = kSymTile * J + c;
+          t[r * kSymLd + c] = j < n ? A[static_cast<size_t>(i) * lda + j] : 0.0;
+        }
+    }
+}
+
+}  // namespace stx

@@ -1,19 +1,26 @@
-// Two-level (patch + dense interface) solve of the skeleton system.
+// Two-level (patch + interface) solve of the skeleton system.
 #pragma once
 
-#include <algorithm>
 #include <cstddef>
 
 #include "device.hpp"
 
 namespace stx {
 
-// Doubles of scratch twolevel_solve needs (interface RHS and solution).
-size_t twolevel_workspace_doubles(const DevModal& S, int nz);
+// Doubles of scratch twolevel_solve needs after R: two skeleton vectors per
+// plane (patch-interior products, solution).
+size_t twolevel_workspace_doubles(int rstride, int nz);
 
-// In place on the skeleton vectors R[k][0..nglobal) of every solved plane:
-// on entry the condensed right-hand sides, on exit the skeleton solution.
-cudaError_t twolevel_solve(const DevModal& S, double* R, int rstride, double* work, int nz, cudaStream_t st);
+// Skeleton vectors R[k][0..nglobal) of every solved plane hold the condensed
+// right-hand sides on entry (R is overwritten); the skeleton solution is left
+// in twolevel_solution(work, ...).  `mid` (optional) is recorded after the
+// interface products.
+cudaError_t twolevel_solve(const DevModal& S, const DevGeom& g, const DevNumbering& N, double* R, int rstride,
+                           double* work, int nz, cudaStream_t st, cudaEvent_t mid = nullptr);
+
+inline double* twolevel_solution(double* work, int rstride, int nz) {
+  return work + static_cast<size_t>(rstride) * nz;
+}
 
 int twolevel_launches(const DevModal& S);
 

@@ -13,6 +13,7 @@
 #include "host/patch.hpp"
 #include "host/session.hpp"
 #include "kernels/device.hpp"
+#include "kernels/symtile.hpp"
 
 namespace stx {
 
@@ -64,24 +65,23 @@ struct stx_context {
   std::vector<stx_modal*> modals;
 
   // Patching of a field's numbering for the two-level direct solve, or null
-  // when the single banded factor is used (token STX_TWOLEVEL = 0, or an
-  // interface too large for a dense inverse).  The patch size is the one of
-  // {8, 16, 36, 64} elements that minimises the matrix bytes read per mode.
+  // when the single banded factor is used (token STX_TWOLEVEL = 0, element
+  // boundaries of more than 64 nodes, or an interface too large for a dense
+  // inverse).  The patch size is the one of {8, 16, 36, 64} elements that
+  // minimises the packed matrix bytes read per mode (the interface inverse
+  // once, each patch-interior inverse twice).
   const stx::Patching* patching(char field) {
     stx::FieldDev& F = fields.at(field);
     if (!F.patch_done) {
       F.patch_done = true;
-      const bool want = !S.tokens.has("STX_TWOLEVEL") || S.tokens.ivalue("STX_TWOLEVEL") != 0;
+      const bool want = (!S.tokens.has("STX_TWOLEVEL") || S.tokens.ivalue("STX_TWOLEVEL") != 0) && M.next <= 64;
       if (want) {
         double best = 0;
         for (int cap : {8, 16, 36, 64}) {
           auto P = std::make_unique<stx::Patching>(stx::build_patching(M, F.N, cap));
           if (P->niface > 6000) continue;
-          double bytes = static_cast<double>(P->niface) * P->niface;
-          for (int f = 0; f < P->nfamily; ++f) {
-            const int p = P->family_rep[f];
-            bytes += static_cast<double>(P->nI[p]) * P->nI[p] + 2.0 * P->nI[p] * P->nB[p];
-          }
+          double bytes = static_cast<double>(stx::sym_size(P->niface));
+          for (int f = 0; f < P->nfamily; ++f) bytes += 2.0 * stx::sym_size(P->nI[P->family_rep[f]]);
           if (!F.P || bytes < best) {
             best = bytes;
             F.P = std::move(P);
