@@ -24,6 +24,7 @@
 #include "kernels/helmholtz.cuh"
 #include "kernels/element.cuh"
 #include "kernels/symtile.hpp"
+#include "kernels/twolevel.cuh"
 #include "stx_internal.hpp"
 
 namespace {
@@ -222,6 +223,7 @@ int stx_context_create(const char* session_path, const char* overrides, int devi
       g.chunk_start = upload(A, cstart);
       g.chunk_count = upload(A, ccount);
       g.elem_sorted = upload(A, sorted);
+      ctx->elem_sorted = sorted;
     }
     std::vector<double> tw(2 * std::max(1, M.nz));
     for (int m = 0; m < M.nz; ++m) {
@@ -484,10 +486,12 @@ int stx_modal_create(stx_context* ctx, char field, double lambda2, double beta, 
       if (method == STX_DIRECT && P) {
         // Two-level data: the patch-interior inverses S_II^-1 (one per patch
         // family and mode) and the interface inverse (one per mode), packed
-        // symmetric; the transposed element Schur complements; per element
-        // node its class (essential / patch-interior / interface).
+        // symmetric; the element Schur complements (rows padded to
+        // element_ld); per element node (chunk order) its skeleton id and
+        // class (essential / patch-interior / interface).
         const int nx = M.next;
-        std::vector<double> hbi, hii, sct, pack;
+        std::vector<double> hbi, hii, sc, pack;
+        const int ldsc = element_ld(nx);
         std::vector<long long> fam_off(static_cast<size_t>(num_modes) * P->nfamily), if_off(num_modes);
         std::vector<int> pin(num_modes, -1);
         const size_t nI_max = std::max(1, P->nI_max);
@@ -496,8 +500,8 @@ int stx_modal_create(stx_context* ctx, char field, double lambda2, double beta, 
           hii.insert(hii.end(), modes[m].hii.begin(), modes[m].hii.end());
           for (int f = 0; f < M.nfamily; ++f) {
             const double* h = modes[m].hsc.data() + static_cast<size_t>(f) * nx * nx;
-            for (int b = 0; b < nx; ++b)
-              for (int a = 0; a < nx; ++a) sct.push_back(h[static_cast<size_t>(a) * nx + b]);
+            for (int a = 0; a < nx; ++a)
+              for (int b = 0; b < ldsc; ++b) sc.push_back(b < nx ? h[static_cast<size_t>(a) * nx + b] : 0.0);
           }
           for (int f = 0; f < P->nfamily; ++f) {
             const int n = P->nI[P->family_rep[f]];
@@ -512,12 +516,16 @@ int stx_modal_create(stx_context* ctx, char field, double lambda2, double beta, 
           pin[m] = modes[m].pin_iid;
           modes[m] = ModeSystem();
         }
-        std::vector<int> ncls(static_cast<size_t>(M.nel) * nx, 0);
-        for (int e = 0; e < M.nel; ++e)
+        // per node of the elements in chunk order: skeleton id << 2 | class
+        std::vector<int> ncode(static_cast<size_t>(M.nel) * nx, 0);
+        for (int i = 0; i < M.nel; ++i) {
+          const int e = ctx->elem_sorted[i];
           for (int a = 0; a < nx; ++a) {
             const int gi = N.btog[static_cast<size_t>(e) * nx + a];
-            ncls[static_cast<size_t>(e) * nx + a] = gi >= N.nsolve ? 0 : (P->iface_of[gi] >= 0 ? 2 : 1);
+            const int cls = gi >= N.nsolve ? 0 : (P->iface_of[gi] >= 0 ? 2 : 1);
+            ncode[static_cast<size_t>(i) * nx + a] = gi << 2 | cls;
           }
+        }
         d.l2 = 1;
         d.npatch = P->npatch;
         d.pfam = P->nfamily;
@@ -534,39 +542,26 @@ int stx_modal_create(stx_context* ctx, char field, double lambda2, double beta, 
         d.hbi = upload(st->arena, hbi);
         d.hii = upload(st->arena, hii);
         d.l2_pack = upload(st->arena, pack.empty() ? std::vector<double>(32, 0.0) : pack);
-        d.l2_sct = upload(st->arena, sct);
-        d.l2_ncls = upload(st->arena, ncls);
-        // work items: the tiles of S_II^-1 per (patch, mode) and of the
-        // interface inverse per mode, in runs
-        std::vector<SymItem> ip, ii;
-        // work items of about 24 tiles (6 per warp): enough items to even
-        // out the waves of resident blocks, few enough x gathers per item
-        auto nparts = [](int nt) { return std::max(1, (nt + 12) / 24); };
+        d.l2_sc = upload(st->arena, sc);
+        d.l2_sc_ld = ldsc;
+        d.l2_ncode = upload(st->arena, ncode);
+        // products: S_II^-1 per (patch, mode), the interface inverse per
+        // mode; each streamed by warps in equal runs of tiles
+        std::vector<SymProblem> pp, pi;
         for (int m = 0; m < num_modes; ++m)
-          for (int p = 0; p < P->npatch; ++p) {
-            const int n = P->nI[p];
-            if (n <= 0) continue;
-            const int nt = sym_ntiles(n), parts = nparts(nt);
-            for (int k = 0; k < parts; ++k)
-              ip.push_back(SymItem{fam_off[static_cast<size_t>(m) * P->nfamily + P->family[p]], n, m,
-                                   static_cast<int>(static_cast<long long>(nt) * k / parts),
-                                   static_cast<int>(static_cast<long long>(nt) * (k + 1) / parts), -1,
-                                   d.p_Igid + static_cast<size_t>(p) * nI_max});
-          }
-        if (P->niface > 0) {
-          const int nt = sym_ntiles(P->niface);
-          const int parts = nparts(nt);
-          for (int m = 0; m < num_modes; ++m)
-            for (int k = 0; k < parts; ++k) {
-              const int q0 = static_cast<int>(static_cast<long long>(nt) * k / parts);
-              const int q1 = static_cast<int>(static_cast<long long>(nt) * (k + 1) / parts);
-              if (q1 > q0) ii.push_back(SymItem{if_off[m], P->niface, m, q0, q1, pin[m], d.skel_of});
-            }
-        }
-        d.items_patch = ip.empty() ? nullptr : upload(st->arena, ip);
-        d.n_items_patch = static_cast<int>(ip.size());
-        d.items_iface = ii.empty() ? nullptr : upload(st->arena, ii);
-        d.n_items_iface = static_cast<int>(ii.size());
+          for (int p = 0; p < P->npatch; ++p)
+            if (P->nI[p] > 0)
+              pp.push_back(SymProblem{fam_off[static_cast<size_t>(m) * P->nfamily + P->family[p]], P->nI[p], m, -1,
+                                      d.p_Igid + static_cast<size_t>(p) * nI_max});
+        if (P->niface > 0)
+          for (int m = 0; m < num_modes; ++m) pi.push_back(SymProblem{if_off[m], P->niface, m, pin[m], d.skel_of});
+        const std::vector<SymWarp> wp = sym_schedule(pp, ctx->device), wi = sym_schedule(pi, ctx->device);
+        d.prob_patch = pp.empty() ? nullptr : upload(st->arena, pp);
+        d.warp_patch = wp.empty() ? nullptr : upload(st->arena, wp);
+        d.nwarp_patch = static_cast<int>(wp.size());
+        d.prob_iface = pi.empty() ? nullptr : upload(st->arena, pi);
+        d.warp_iface = wi.empty() ? nullptr : upload(st->arena, wi);
+        d.nwarp_iface = static_cast<int>(wi.size());
         d.fwd = d.bwd = d.dinv_fwd = d.dinv_bwd = nullptr;
         d.nbp = 0;
         d.mode_stride = d.dinv_stride = 0;

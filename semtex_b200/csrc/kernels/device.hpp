@@ -46,13 +46,19 @@ struct DevNumbering {
 };
 
 // One packed symmetric product y += A x for the planes of a Fourier mode:
-// tiles [q0, q1) of the matrix at l2_pack + moff (order n); x_i is read and
-// y_i accumulated at position idx[i] of the planes' skeleton vectors
-// (x_pin taken as zero).
-struct SymItem {
+// the matrix at l2_pack + moff (order n); x_i is read and y_i accumulated at
+// position idx[i] of the planes' skeleton vectors (x_pin taken as zero).
+struct SymProblem {
   long long moff;
-  int n, mode, q0, q1, pin;
+  int n, mode, pin;
   const int* idx;
+};
+
+// The tiles one warp of a packed product streams: `count` tiles in packed
+// order from tile q of problem `prob`, continuing into the following
+// problems.
+struct SymWarp {
+  int prob, q, count;
 };
 
 // A ModalMatrixSys on the device: one MatrixSys per locally held mode.
@@ -91,12 +97,16 @@ struct DevModal {
   const int* skel_of;             // [niface] skeleton id of each interface unknown
   const int* pin;                 // [nmodes] pinned interface id or -1
   const double* l2_pack;          // packed symmetric inverses (symtile.hpp layout)
-  const SymItem* items_patch;     // S_II^-1 products: one per (patch, mode)
-  int n_items_patch;
-  const SymItem* items_iface;     // interface products: (mode, tile range)
-  int n_items_iface;
-  const double* l2_sct;           // [nmodes][nfamily][next][next] element Schur complements, transposed
-  const int* l2_ncls;             // [nel][next]: 0 essential, 1 patch-interior, 2 interface node
+  const SymProblem* prob_patch;   // S_II^-1 products: one per (patch, mode)
+  const SymWarp* warp_patch;
+  int nwarp_patch;
+  const SymProblem* prob_iface;   // interface products: one per mode
+  const SymWarp* warp_iface;
+  int nwarp_iface;
+  const double* l2_sc;            // [nmodes][nfamily][next][l2_sc_ld] element Schur complements
+  int l2_sc_ld;
+  const int* l2_ncode;            // [nel][next], elements in chunk order: skeleton id << 2 | class
+                                  // (0 essential, 1 patch-interior, 2 interface node)
 };
 
 }  // namespace stx

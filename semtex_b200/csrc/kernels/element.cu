@@ -427,6 +427,78 @@ __global__ void __launch_bounds__(32 * kMaxWarps, 1)
   }
 }
 
+
+// Element Schur complement products: one block per (chunk, mode).  The
+// family-mode matrix S_e (rows padded) and the chunk's input columns (the
+// source values at the element nodes of the taken class, zero elsewhere)
+// in shared memory; out = S_e x on the tensor cores; the rows of the put
+// class are subtracted from dst.
+__global__ void __launch_bounds__(256)
+    k_elem_schur(int dir, DevGeom g, DevNumbering N, DevModal S, const double* __restrict__ src,
+                 double* __restrict__ dst, int rstride) {
+  extern __shared__ __align__(16) unsigned char sraw[];
+  const int c = blockIdx.x, m = blockIdx.y;
+  const int nr = (g.nz > 1 && m > 0) ? 2 : 1;
+  const int next = g.next, cnt = g.chunk_count[c], ncol = nr * cnt;
+  const int* el = g.elem_sorted + g.chunk_start[c];
+  const int lda = S.l2_sc_ld, ldb = element_ld(next);
+  double* sA = reinterpret_cast<double*>(sraw);               // [next][lda]
+  double* sB = sA + next * lda;                               // [2 cm][ldb]
+  int* sN = reinterpret_cast<int*>(sB + 2 * g.chunk_max * ldb);  // [cm][next] skeleton id << 2 | class
+  const int take = dir == 0 ? 1 : 2, put = dir == 0 ? 2 : 1;
+  const double* A = S.l2_sc + (static_cast<size_t>(m) * S.nfamily + g.family[el[0]]) * next * lda;
+  for (int i = threadIdx.x; i < next * lda; i += blockDim.x) sA[i] = __ldg(A + i);
+  const int wp = threadIdx.x >> 5, ln = threadIdx.x & 31, nwp = blockDim.x >> 5;
+  const int* code = S.l2_ncode + static_cast<size_t>(g.chunk_start[c]) * next;
+  for (int i = threadIdx.x; i < cnt * next; i += blockDim.x) sN[i] = __ldg(code + i);
+  __syncthreads();
+  // input columns, loads of kColBatch columns per warp in flight together
+  for (int c0 = wp; c0 < ncol; c0 += nwp * kColBatch) {
+    double v[kColBatch][2];
+#pragma unroll
+    for (int j = 0; j < kColBatch; ++j) {
+      const int col = c0 + j * nwp;
+      int slot, l;
+      col_slot(min(col, ncol - 1), cnt, slot, l);
+      const double* sp = src + static_cast<size_t>(2 * m + slot) * rstride;
+#pragma unroll
+      for (int h = 0; h < 2; ++h) {
+        const int a = ln + 32 * h;
+        const int cd = (col < ncol && a < next) ? sN[l * next + a] : 0;
+        v[j][h] = (cd & 3) == take ? sp[cd >> 2] : 0.0;
+      }
+    }
+#pragma unroll
+    for (int j = 0; j < kColBatch; ++j) {
+      const int col = c0 + j * nwp;
+      if (col >= ncol) continue;
+#pragma unroll
+      for (int h = 0; h < 2; ++h)
+        if (ln + 32 * h < next) sB[col * ldb + ln + 32 * h] = v[j][h];
+    }
+  }
+  __syncthreads();
+  const int ntile = (ncol + 7) / 8, strips = (next + 7) / 8;
+  const int ncg = (ntile + kUnitTiles - 1) / kUnitTiles;
+  for (int unit = wp; unit < strips * ncg; unit += nwp) {
+    const int strip = unit / ncg, j0 = (unit - strip * ncg) * kUnitTiles;
+    double acc[kUnitTiles][2];
+    unit_product(acc, sA, lda, next, strip, sB, ldb, ncol, j0, ntile, 0, next);
+    const int row = strip * 8 + (ln >> 2);
+#pragma unroll
+    for (int j = 0; j < kUnitTiles; ++j)
+#pragma unroll
+      for (int i = 0; i < 2; ++i) {
+        const int col = (j0 + j) * 8 + 2 * (ln & 3) + i;
+        if (j0 + j < ntile && row < next && col < ncol) {
+          int slot, l;
+          col_slot(col, cnt, slot, l);
+          const int cd = sN[l * next + row];
+          if ((cd & 3) == put) atomicAdd(&dst[static_cast<size_t>(2 * m + slot) * rstride + (cd >> 2)], -acc[j][i]);
+        }
+      }
+  }
+}
 }  // namespace
 
 ElementPlan element_plan(const DevGeom& g, const DevModal& S, bool lift) {
@@ -474,6 +546,19 @@ void element_recover(const ElementPlan& P, const DevGeom& g, const DevNumbering&
   }
   k_elem_recover<<<dim3(g.nchunk, S.nmodes, P.rec_rb), P.rec_threads, P.rec_smem, st>>>(g, N, S, F, G, gstride, R,
                                                                                         rstride, U, P.rec_rows);
+}
+
+void element_schur_apply(int dir, const DevGeom& g, const DevNumbering& N, const DevModal& S, const double* src,
+                         double* dst, int rstride, cudaStream_t st) {
+  const size_t smem = sizeof(double) * (static_cast<size_t>(g.next) * S.l2_sc_ld +
+                                        2 * static_cast<size_t>(g.chunk_max) * element_ld(g.next)) +
+                      sizeof(int) * static_cast<size_t>(g.chunk_max) * g.next;
+  static size_t configured = 0;
+  if (smem > 48 * 1024 && smem > configured) {
+    cudaFuncSetAttribute(k_elem_schur, cudaFuncAttributeMaxDynamicSharedMemorySize, static_cast<int>(smem));
+    configured = smem;
+  }
+  k_elem_schur<<<dim3(g.nchunk, S.nmodes), 256, smem, st>>>(dir, g, N, S, src, dst, rstride);
 }
 
 }  // namespace stx

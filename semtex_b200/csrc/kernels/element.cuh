@@ -45,4 +45,11 @@ void element_recover(const ElementPlan& P, const DevGeom& g, const DevNumbering&
                      const double* F, const double* G, int gstride, const double* R, int rstride, double* U,
                      cudaStream_t st);
 
+// Skeleton couplings through the element Schur complements S_e (two-level
+// solve), for every element and solved plane, with I / B the element nodes
+// that are patch-interior / patch-interface skeleton unknowns:
+//   dir 0:  dst[B] -= S_BI src[I]        dir 1:  dst[I] -= S_IB src[B]
+void element_schur_apply(int dir, const DevGeom& g, const DevNumbering& N, const DevModal& S, const double* src,
+                         double* dst, int rstride, cudaStream_t st);
+
 }  // namespace stx

@@ -63,6 +63,13 @@ __device__ __forceinline__ void cp_async8(void* dst, const void* src) {
 
 __device__ __forceinline__ void cp_async_wait_all() { asm volatile("cp.async.wait_all;" ::: "memory"); }
 
+// Arrive on `bar` once all of this thread's earlier cp.async copies have
+// landed (the arrival is not added to the expected count: the barrier's
+// initial count must include it).
+__device__ __forceinline__ void cp_async_arrive_noinc(uint64_t* bar) {
+  asm volatile("cp.async.mbarrier.arrive.noinc.shared.b64 [%0];" ::"r"(smem_u32(bar)) : "memory");
+}
+
 // D(8x8) += A(8x4) B(4x8) in FP64.  Lane l = 4 g + t holds A[g][t], B[t][g]
 // and D[g][2t], D[g][2t+1].
 __device__ __forceinline__ void dmma_8x8x4(double& d0, double& d1, double a, double b) {

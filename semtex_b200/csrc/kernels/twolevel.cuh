@@ -2,6 +2,7 @@
 #pragma once
 
 #include <cstddef>
+#include <vector>
 
 #include "device.hpp"
 
@@ -23,5 +24,9 @@ inline double* twolevel_solution(double* work, int rstride, int nz) {
 }
 
 int twolevel_launches(const DevModal& S);
+
+// Split the tiles of `probs` (in order) into equal runs, one per warp of a
+// grid that fills `device` once at the product kernel's occupancy.
+std::vector<SymWarp> sym_schedule(const std::vector<SymProblem>& probs, int device);
 
 }  // namespace stx

@@ -60,6 +60,7 @@ struct stx_context {
   std::map<char, stx::FieldDev> fields;
   stx::DeviceArena arena;
   stx::DevGeom dg{};
+  std::vector<int> elem_sorted;  // host copy of dg.elem_sorted
   double* d_twiddle = nullptr;
   double* d_io = nullptr;
   std::vector<stx_modal*> modals;
