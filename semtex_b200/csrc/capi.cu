@@ -224,6 +224,10 @@ int stx_context_create(const char* session_path, const char* overrides, int devi
       g.chunk_count = upload(A, ccount);
       g.elem_sorted = upload(A, sorted);
       ctx->elem_sorted = sorted;
+      std::vector<int4> desc(cstart.size());
+      for (size_t k = 0; k < cstart.size(); ++k)
+        desc[k] = make_int4(cstart[k], ccount[k], M.family[sorted[cstart[k]]], 0);
+      g.chunk_desc = upload(A, desc);
     }
     std::vector<double> tw(2 * std::max(1, M.nz));
     for (int m = 0; m < M.nz; ++m) {
@@ -456,12 +460,15 @@ int stx_modal_create(stx_context* ctx, char field, double lambda2, double beta, 
       d.ew = d.eb = nullptr;
       d.ew_ld = d.eb_ld = 0;
       if (method == STX_DIRECT) {
-        // Element operators for the element kernels, per family and mode,
-        // rows zero-padded to element_ld: the recovery operator row i =
-        // (-hbi[b][i] for the element-boundary nodes b, hii^-1[i][j]), so the
-        // interior solution is one product with the column (u_b, F_i); the
-        // condensation operator row b = hbi[b][.].
-        const int nx = M.next, ni = M.nint, ldw = element_ld(M.npnp), ldc = element_ld(ni);
+        // Element operators for the element kernels, per family and mode
+        // (rows zero-padded to element_ld): the recovery operator row i, with
+        // columns in the natural node order of the recovery's columns,
+        // = (-hbi[b][i] at the element-boundary nodes, hii^-1[i][j] at the
+        // interior nodes), so the interior solution is one product with the
+        // column (u_b at the boundary nodes, F_i at the interior nodes); the
+        // condensation operator row b = hbi[b][.] (interior nodes in
+        // boundary-major order, as the condensation's columns).
+        const int nx = M.next, ni = M.nint, nn = M.npnp, ldw = element_ld(nn), ldc = element_ld(ni);
         const size_t nf = static_cast<size_t>(num_modes) * M.nfamily;
         std::vector<double> ew(nf * ni * ldw, 0.0), eb(nf * nx * ldc, 0.0);
         for (int m = 0; m < num_modes; ++m)
@@ -470,11 +477,13 @@ int stx_modal_create(stx_context* ctx, char field, double lambda2, double beta, 
             const double* hb = modes[m].hbi.data() + static_cast<size_t>(f) * nx * ni;
             const double* hi = modes[m].hii.data() + static_cast<size_t>(f) * ni * ni;
             double* w = ew.data() + fm * ni * ldw;
-            for (int i = 0; i < ni; ++i) {
-              for (int b = 0; b < nx; ++b) w[static_cast<size_t>(i) * ldw + b] = -hb[static_cast<size_t>(b) * ni + i];
-              for (int j = 0; j < ni; ++j) w[static_cast<size_t>(i) * ldw + nx + j] = hi[static_cast<size_t>(i) * ni + j];
-            }
             double* c = eb.data() + fm * nx * ldc;
+            for (int t = 0; t < nn; ++t) {
+              const int p = M.pmap[t];
+              for (int i = 0; i < ni; ++i)
+                w[static_cast<size_t>(i) * ldw + t] =
+                    p < nx ? -hb[static_cast<size_t>(p) * ni + i] : hi[static_cast<size_t>(i) * ni + p - nx];
+            }
             for (int b = 0; b < nx; ++b)
               for (int j = 0; j < ni; ++j) c[static_cast<size_t>(b) * ldc + j] = hb[static_cast<size_t>(b) * ni + j];
           }

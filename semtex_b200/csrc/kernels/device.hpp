@@ -31,6 +31,7 @@ struct DevGeom {
   const int* chunk_start;
   const int* chunk_count;
   const int* elem_sorted;
+  const int4* chunk_desc;  // [nchunk] (chunk_start, chunk_count, family, 0): one load per block
 };
 
 struct DevNumbering {
@@ -73,10 +74,13 @@ struct DevModal {
   const int* nsolve;              // [nmodes]
   const double* hbi;              // [nmodes][nfamily][next][nint]
   const double* hii;              // [nmodes][nfamily][nint][nint]
-  // Element operators in the padded layout of the element kernels:
-  const double* ew;               // [nmodes][nfamily][nint][ew_ld]: row i = (-hbi[.][i], hii^-1[i][.], 0...)
+  // Element operators of the element kernels, rows padded: recovery row i
+  // (columns in natural node order) = -hbi[b][i] at boundary node b,
+  // hii^-1[i][j] at interior node j; condensation row b = hbi[b][.] over the
+  // interior nodes in boundary-major order.
+  const double* ew;               // [nmodes][nfamily][nint][ew_ld]
   int ew_ld;
-  const double* eb;               // [nmodes][nfamily][next][eb_ld]: row b = (hbi[b][.], 0...)
+  const double* eb;               // [nmodes][nfamily][next][eb_ld]
   int eb_ld;
   const double* fwd;              // [nmodes][mode_stride]: rows of U^T, stride nbp
   const double* bwd;              // [nmodes][mode_stride]: rows of reversed U

@@ -1,9 +1,10 @@
 // Element kernels: one block per (chunk of up to chunk_max same-family
 // elements, Fourier mode, row block of the family operator).  The forcing
-// columns of the chunk (Re and Im planes of the mode, boundary-major node
-// order) are assembled in shared memory; the family-mode operator slice is
-// bulk-copied alongside; the product runs on the FP64 tensor cores
-// (m8n8k4), one warp per 8-row strip against all columns.
+// columns of the chunk (Re and Im planes of the mode; boundary-major node
+// order for the condensation, natural order for the recovery, whose operator
+// columns are permuted to match on the host) are assembled in shared memory;
+// the family-mode operator slice is bulk-copied alongside; the product runs
+// on the FP64 tensor cores (m8n8k4), one warp per 8-row by 32-column unit.
 //
 // Latency, not bandwidth, bounds this work (a few MB per launch), so every
 // global -> shared transfer is asynchronous (8-byte cp.async, one bulk copy
@@ -66,6 +67,12 @@ __device__ __forceinline__ ElemIdx load_idx(const DevGeom& g, unsigned char* sra
   return ElemIdx{sp, se, sl};
 }
 
+// Row of node t of a column: natural node order or boundary-major order.
+template <bool kNatural>
+__device__ __forceinline__ int node_row(const ElemIdx& X, int t) {
+  return kNatural ? t : X.pmap[t];
+}
+
 __device__ __forceinline__ void col_slot(int col, int cnt, int& slot, int& l) {
   slot = col >= cnt ? 1 : 0;  // at most two planes (Re, Im) per mode
   l = col - slot * cnt;
@@ -95,9 +102,11 @@ __device__ __forceinline__ bool rows_ready(uint64_t* bar, int* status) {
   return ok;
 }
 
-// Issue the asynchronous copies of the forcing columns (f at the nodes whose
-// boundary-major position p satisfies p >= pmin) and of the elements' Q4 at
-// the same nodes; zero the padding rows [nn, ldb) of every column.
+// Issue the asynchronous copies of the forcing columns, natural node order
+// (f at the nodes whose boundary-major position p satisfies p >= pmin), and
+// of the elements' Q4 at the same nodes; zero the padding rows [nn, ldb) of
+// every column.  A warp's copies of a column are contiguous in both memories.
+template <bool kNatural>
 __device__ __forceinline__ void issue_forcing(const DevGeom& g, const double* __restrict__ F, const ElemIdx& X,
                                               int cnt, int m, int ncol, double* sB, int ldb, double* sQ, int pmin) {
   const int nn = g.npnp;
@@ -110,9 +119,8 @@ __device__ __forceinline__ void issue_forcing(const DevGeom& g, const double* __
     const double* q4 = g.Q4 + static_cast<size_t>(e) * nn;
     double* b = sB + col * ldb;
     for (int t = ln; t < nn; t += 32) {
-      const int p = X.pmap[t];
-      if (p < pmin) continue;
-      cp_async8(b + p, f + t);
+      if (X.pmap[t] < pmin) continue;
+      cp_async8(b + node_row<kNatural>(X, t), f + t);
       if (slot == 0) cp_async8(sQ + l * nn + t, q4 + t);
     }
     for (int r = nn + ln; r < ldb; r += 32) b[r] = 0.0;
@@ -120,6 +128,7 @@ __device__ __forceinline__ void issue_forcing(const DevGeom& g, const double* __
 }
 
 // After the copies: forcing column entries become -Q4 f.
+template <bool kNatural>
 __device__ __forceinline__ void scale_forcing(const DevGeom& g, const ElemIdx& X, int cnt, int ncol, double* sB,
                                               int ldb, const double* sQ, int pmin) {
   const int nn = g.npnp;
@@ -128,10 +137,8 @@ __device__ __forceinline__ void scale_forcing(const DevGeom& g, const ElemIdx& X
     int slot, l;
     col_slot(col, cnt, slot, l);
     double* b = sB + col * ldb;
-    for (int t = ln; t < nn; t += 32) {
-      const int p = X.pmap[t];
-      if (p >= pmin) b[p] *= -sQ[l * nn + t];
-    }
+    for (int t = ln; t < nn; t += 32)
+      if (X.pmap[t] >= pmin) b[node_row<kNatural>(X, t)] *= -sQ[l * nn + t];
   }
 }
 
@@ -180,8 +187,9 @@ __device__ void scan_boundary(const DevGeom& g, const DevNumbering& N, const dou
           gv[j][h] = bm[j][h] ? G[static_cast<size_t>(k) * gstride + gi[j][h]] : 0.0;
           if (kGather && gi[j][h] >= 0) {
             const int a = a0 + 32 * h + ln;
-            if (gi[j][h] < nsolve) cp_async8(sB + col * ldb + a, R + static_cast<size_t>(k) * rstride + gi[j][h]);
-            else sB[col * ldb + a] = 0.0;
+            const int t = X.emap[a];
+            if (gi[j][h] < nsolve) cp_async8(sB + col * ldb + t, R + static_cast<size_t>(k) * rstride + gi[j][h]);
+            else sB[col * ldb + t] = 0.0;
           }
         }
       }
@@ -219,6 +227,7 @@ __device__ void scan_boundary(const DevGeom& g, const DevNumbering& N, const dou
 // Lift term H g of the flagged columns, subtracted from their forcing (at
 // all nodes, or only interior ones): one column per warp among the first 8
 // warps, each with 3*nn doubles of scratch in wsc.
+template <bool kNatural>
 __device__ void lift_columns(const DevGeom& g, const DevNumbering& N, const double* __restrict__ G, int gstride,
                              double hcon, const ElemIdx& X, int cnt, int m, int ncol, double* sB, int ldb,
                              double* wsc, const double* sD, const int* sFlag, int pmin) {
@@ -253,15 +262,14 @@ __device__ void lift_columns(const DevGeom& g, const DevNumbering& N, const doub
     }
     __syncwarp();
     for (int q = lane; q < nn; q += 32) {
-      const int p = X.pmap[q];
-      if (p < pmin) continue;
+      if (X.pmap[q] < pmin) continue;
       const int i = q / np, j = q - (q / np) * np;
       double h = g.Q4[e * nn + q] * su[q] * hcon;
       for (int kk = 0; kk < np; ++kk) {
         h += sD[kk * np + i] * sS[kk * np + j];
         h += sR[i * np + kk] * sD[kk * np + j];
       }
-      sB[col * ldb + p] -= h;
+      sB[col * ldb + node_row<kNatural>(X, q)] -= h;
     }
     __syncwarp();
   }
@@ -295,10 +303,11 @@ __global__ void __launch_bounds__(32 * kMaxWarps, 1)
   extern __shared__ __align__(16) unsigned char sraw[];
   const int c = blockIdx.x, m = blockIdx.y;
   const int nr = (g.nz > 1 && m > 0) ? 2 : 1;
-  const int nn = g.npnp, next = g.next, nint = g.nint;
-  const int cnt = g.chunk_count[c];
+  const int nn = g.npnp, next = g.next;
+  const int4 cd = __ldg(g.chunk_desc + c);  // start, count, family
+  const int cnt = cd.y;
   const int ncol = nr * cnt;
-  const int* el = g.elem_sorted + g.chunk_start[c];
+  const int* el = g.elem_sorted + cd.x;
   const int ldb = element_ld(nn), lda = S.eb_ld;
   const int r_lo = blockIdx.z * rb_rows, rows = min(rb_rows, next - r_lo);
   const ElemSmem L = elem_layout(rb_rows * lda, g.chunk_max, ldb, g.np, nn, next, G != nullptr);
@@ -308,27 +317,28 @@ __global__ void __launch_bounds__(32 * kMaxWarps, 1)
   double* sD = reinterpret_cast<double*>(sraw + L.d);
   double* sQ = reinterpret_cast<double*>(sraw + L.q);
   int* sFlag = reinterpret_cast<int*>(sraw + L.flag);
-  const size_t fm = static_cast<size_t>(m) * S.nfamily + g.family[el[0]];
+  const size_t fm = static_cast<size_t>(m) * S.nfamily + cd.z;
   stage_rows(bar, sA, S.eb + (fm * next + r_lo) * lda, static_cast<unsigned>(sizeof(double) * rows * lda));
   const ElemIdx X = load_idx(g, sraw, L, el, cnt);
   for (int w = threadIdx.x; w < g.np * g.np; w += blockDim.x) sD[w] = g.D[w];
   __syncthreads();
-  issue_forcing(g, F, X, cnt, m, ncol, sB, ldb, sQ, 0);
+  // boundary-major columns: the product takes the interior rows, F_b stays
+  issue_forcing<false>(g, F, X, cnt, m, ncol, sB, ldb, sQ, 0);
   if (G)
     scan_boundary<false>(g, N, G, gstride, nullptr, 0, nullptr, 0, X, cnt, m, ncol, sB, ldb, sFlag, nullptr);
   cp_async_wait_all();
   __syncthreads();
-  scale_forcing(g, X, cnt, ncol, sB, ldb, sQ, 0);
+  scale_forcing<false>(g, X, cnt, ncol, sB, ldb, sQ, 0);
   __syncthreads();
   if (G) {
-    lift_columns(g, N, G, gstride, S.lambda2[m] + S.betak2[m], X, cnt, m, ncol, sB, ldb, sQ, sD, sFlag, 0);
+    lift_columns<false>(g, N, G, gstride, S.lambda2[m] + S.betak2[m], X, cnt, m, ncol, sB, ldb, sQ, sD, sFlag, 0);
     __syncthreads();
   }
   if (!rows_ready(bar, S.status)) return;
   const int wp = threadIdx.x >> 5, ln = threadIdx.x & 31;
   const int ntile = (ncol + 7) / 8, strips = (rows + 7) / 8;
   const int ncg = (ntile + kUnitTiles - 1) / kUnitTiles;
-  const int K = (nint + 3) / 4 * 4;
+  const int K = (g.nint + 3) / 4 * 4;
   for (int unit = wp; unit < strips * ncg; unit += blockDim.x >> 5) {
     const int strip = unit / ncg, j0 = (unit - strip * ncg) * kUnitTiles;
     double acc[kUnitTiles][2];
@@ -357,9 +367,10 @@ __global__ void __launch_bounds__(32 * kMaxWarps, 1)
   const int c = blockIdx.x, m = blockIdx.y;
   const int nr = (g.nz > 1 && m > 0) ? 2 : 1;
   const int nn = g.npnp, next = g.next, nint = g.nint;
-  const int cnt = g.chunk_count[c];
+  const int4 cd = __ldg(g.chunk_desc + c);  // start, count, family
+  const int cnt = cd.y;
   const int ncol = nr * cnt;
-  const int* el = g.elem_sorted + g.chunk_start[c];
+  const int* el = g.elem_sorted + cd.x;
   const int ldb = element_ld(nn), lda = S.ew_ld;
   const int r_lo = blockIdx.z * rb_rows, rows = min(rb_rows, nint - r_lo);
   const ElemSmem L = elem_layout(rb_rows * lda, g.chunk_max, ldb, g.np, nn, next, G != nullptr);
@@ -371,13 +382,13 @@ __global__ void __launch_bounds__(32 * kMaxWarps, 1)
   int* sFlag = reinterpret_cast<int*>(sraw + L.flag);
   unsigned* sBits = reinterpret_cast<unsigned*>(sraw + L.bits);
   const int nwords = (next + 31) / 32;
-  const size_t fm = static_cast<size_t>(m) * S.nfamily + g.family[el[0]];
+  const size_t fm = static_cast<size_t>(m) * S.nfamily + cd.z;
   stage_rows(bar, sA, S.ew + (fm * nint + r_lo) * lda, static_cast<unsigned>(sizeof(double) * rows * lda));
   const ElemIdx X = load_idx(g, sraw, L, el, cnt);
   for (int w = threadIdx.x; w < g.np * g.np; w += blockDim.x) sD[w] = g.D[w];
   __syncthreads();
   // interior forcing only: the boundary rows carry u_b
-  issue_forcing(g, F, X, cnt, m, ncol, sB, ldb, sQ, next);
+  issue_forcing<true>(g, F, X, cnt, m, ncol, sB, ldb, sQ, next);
   const int nsolve = S.nsolve[m];
   // every row block gathers u_b (it enters every row's product); only row
   // block 0 writes the essential values
@@ -385,10 +396,10 @@ __global__ void __launch_bounds__(32 * kMaxWarps, 1)
                       ldb, sFlag, sBits);
   cp_async_wait_all();
   __syncthreads();
-  scale_forcing(g, X, cnt, ncol, sB, ldb, sQ, next);
+  scale_forcing<true>(g, X, cnt, ncol, sB, ldb, sQ, next);
   __syncthreads();
   if (G) {
-    lift_columns(g, N, G, gstride, S.lambda2[m] + S.betak2[m], X, cnt, m, ncol, sB, ldb, sQ, sD, sFlag, next);
+    lift_columns<true>(g, N, G, gstride, S.lambda2[m] + S.betak2[m], X, cnt, m, ncol, sB, ldb, sQ, sD, sFlag, next);
     __syncthreads();
   }
   if (!rows_ready(bar, S.status)) return;
@@ -408,7 +419,7 @@ __global__ void __launch_bounds__(32 * kMaxWarps, 1)
 #pragma unroll
       for (int i = 0; i < 2; ++i) {
         const int col = (j0 + j) * 8 + 2 * (ln & 3) + i;
-        if (j0 + j < ntile && row < rows && col < ncol) sB[col * ldb + next + r_lo + row] = acc[j][i];
+        if (j0 + j < ntile && row < rows && col < ncol) sB[col * ldb + X.emap[next + r_lo + row]] = acc[j][i];
       }
   }
   __syncthreads();
@@ -422,7 +433,7 @@ __global__ void __launch_bounds__(32 * kMaxWarps, 1)
       const int p = X.pmap[t];
       const bool w = p >= next ? (p - next >= r_lo && p - next < r_lo + rows)
                                : (blockIdx.z == 0 && !((bits[p >> 5] >> (p & 31)) & 1u));
-      if (w) u_e[t] = b[p];
+      if (w) u_e[t] = b[t];
     }
   }
 }
@@ -439,17 +450,19 @@ __global__ void __launch_bounds__(256)
   extern __shared__ __align__(16) unsigned char sraw[];
   const int c = blockIdx.x, m = blockIdx.y;
   const int nr = (g.nz > 1 && m > 0) ? 2 : 1;
-  const int next = g.next, cnt = g.chunk_count[c], ncol = nr * cnt;
-  const int* el = g.elem_sorted + g.chunk_start[c];
+  // this block's part of the chunk: elements [e0, e0 + cnt)
+  const int4 cd = __ldg(g.chunk_desc + c);  // start, count, family
+  const int e0 = cd.y * blockIdx.z / gridDim.z, cnt = cd.y * (blockIdx.z + 1) / gridDim.z - e0;
+  const int next = g.next, ncol = nr * cnt;
   const int lda = S.l2_sc_ld, ldb = element_ld(next);
   double* sA = reinterpret_cast<double*>(sraw);               // [next][lda]
   double* sB = sA + next * lda;                               // [2 cm][ldb]
   int* sN = reinterpret_cast<int*>(sB + 2 * g.chunk_max * ldb);  // [cm][next] skeleton id << 2 | class
   const int take = dir == 0 ? 1 : 2, put = dir == 0 ? 2 : 1;
-  const double* A = S.l2_sc + (static_cast<size_t>(m) * S.nfamily + g.family[el[0]]) * next * lda;
+  const double* A = S.l2_sc + (static_cast<size_t>(m) * S.nfamily + cd.z) * next * lda;
   for (int i = threadIdx.x; i < next * lda; i += blockDim.x) sA[i] = __ldg(A + i);
   const int wp = threadIdx.x >> 5, ln = threadIdx.x & 31, nwp = blockDim.x >> 5;
-  const int* code = S.l2_ncode + static_cast<size_t>(g.chunk_start[c]) * next;
+  const int* code = S.l2_ncode + static_cast<size_t>(cd.x + e0) * next;
   for (int i = threadIdx.x; i < cnt * next; i += blockDim.x) sN[i] = __ldg(code + i);
   __syncthreads();
   // input columns, loads of kColBatch columns per warp in flight together
@@ -464,8 +477,8 @@ __global__ void __launch_bounds__(256)
 #pragma unroll
       for (int h = 0; h < 2; ++h) {
         const int a = ln + 32 * h;
-        const int cd = (col < ncol && a < next) ? sN[l * next + a] : 0;
-        v[j][h] = (cd & 3) == take ? sp[cd >> 2] : 0.0;
+        const int code_v = (col < ncol && a < next) ? sN[l * next + a] : 0;
+        v[j][h] = (code_v & 3) == take ? sp[code_v >> 2] : 0.0;
       }
     }
 #pragma unroll
@@ -493,8 +506,9 @@ __global__ void __launch_bounds__(256)
         if (j0 + j < ntile && row < next && col < ncol) {
           int slot, l;
           col_slot(col, cnt, slot, l);
-          const int cd = sN[l * next + row];
-          if ((cd & 3) == put) atomicAdd(&dst[static_cast<size_t>(2 * m + slot) * rstride + (cd >> 2)], -acc[j][i]);
+          const int code_v = sN[l * next + row];
+          if ((code_v & 3) == put)
+            atomicAdd(&dst[static_cast<size_t>(2 * m + slot) * rstride + (code_v >> 2)], -acc[j][i]);
         }
       }
   }
@@ -504,11 +518,14 @@ __global__ void __launch_bounds__(256)
 ElementPlan element_plan(const DevGeom& g, const DevModal& S, bool lift) {
   ElementPlan P;
   if (g.nchunk <= 0 || !S.ew || !S.eb || S.ew_ld <= 0 || S.eb_ld <= 0 || g.nint <= 0) return P;
-  const size_t cap = 227 * 1024;
   const int ldb = element_ld(g.npnp);
   const int ncg = ((2 * g.chunk_max + 7) / 8 + kUnitTiles - 1) / kUnitTiles;
-  auto fit = [&](int nrow, int ld, int& rows, int& nrb, int& threads, size_t& smem) {
-    rows = std::min(nrow, 8 * (kMaxWarps / ncg));  // one warp per product unit
+  // Two blocks of 16 warps per SM (<= 113 KB each), so that one block's
+  // gathers overlap the other's product, when the whole operator fits;
+  // otherwise one block of 32 warps per SM, operator rows split into
+  // balanced row blocks where needed.
+  auto fit = [&](int nrow, int ld, int warps, size_t cap, int& rows, int& nrb, int& threads, size_t& smem) {
+    rows = std::min(nrow, 8 * (warps / ncg));  // one warp per product unit
     if (rows < nrow) rows -= rows % 8;
     for (;;) {
       smem = elem_layout(rows * ld, g.chunk_max, ldb, g.np, g.npnp, g.next, lift).bytes;
@@ -517,11 +534,21 @@ ElementPlan element_plan(const DevGeom& g, const DevModal& S, bool lift) {
       if (rows < 8) return false;
     }
     nrb = (nrow + rows - 1) / rows;
-    threads = 32 * kMaxWarps;
-    return (rows + 7) / 8 * ncg <= kMaxWarps;
+    if (nrb > 1) {  // balance: equal row blocks, multiples of 8
+      rows = ((nrow + nrb - 1) / nrb + 7) / 8 * 8;
+      nrb = (nrow + rows - 1) / rows;
+      smem = elem_layout(rows * ld, g.chunk_max, ldb, g.np, g.npnp, g.next, lift).bytes;
+    }
+    threads = 32 * warps;
+    return (rows + 7) / 8 * ncg <= warps && smem <= cap;
   };
-  P.ok = fit(g.next, S.eb_ld, P.cond_rows, P.cond_rb, P.cond_threads, P.cond_smem) &&
-         fit(g.nint, S.ew_ld, P.rec_rows, P.rec_rb, P.rec_threads, P.rec_smem);
+  // per kernel: the two-block tier only when it needs no row split
+  auto choose = [&](int nrow, int ld, int& rows, int& nrb, int& threads, size_t& smem) {
+    if (fit(nrow, ld, kMaxWarps / 2, 113 * 1024, rows, nrb, threads, smem) && nrb == 1) return true;
+    return fit(nrow, ld, kMaxWarps, 227 * 1024, rows, nrb, threads, smem);
+  };
+  P.ok = choose(g.next, S.eb_ld, P.cond_rows, P.cond_rb, P.cond_threads, P.cond_smem) &&
+         choose(g.nint, S.ew_ld, P.rec_rows, P.rec_rb, P.rec_threads, P.rec_smem);
   return P;
 }
 
@@ -558,7 +585,8 @@ void element_schur_apply(int dir, const DevGeom& g, const DevNumbering& N, const
     cudaFuncSetAttribute(k_elem_schur, cudaFuncAttributeMaxDynamicSharedMemorySize, static_cast<int>(smem));
     configured = smem;
   }
-  k_elem_schur<<<dim3(g.nchunk, S.nmodes), 256, smem, st>>>(dir, g, N, S, src, dst, rstride);
+  // two blocks per chunk and mode: the work is latency-bound
+  k_elem_schur<<<dim3(g.nchunk, S.nmodes, 2), 256, smem, st>>>(dir, g, N, S, src, dst, rstride);
 }
 
 }  // namespace stx
