@@ -763,24 +763,25 @@ int stx_elliptic_solve_host(stx_modal* sys, const double* h_forcing, double* h_s
     }
     double* dF = ctx->d_io;
     double* dU = ctx->d_io + ps * nz;
-    for (size_t k = 0; k < nz; ++k)
-      cuda_check(cudaMemcpyAsync(dF + k * ps, h_forcing + k * nplane, sizeof(double) * nplane,
-                                 cudaMemcpyHostToDevice, ctx->stream),
-                 "forcing h2d");
+    // one pitched copy per direction: host planes are nplane doubles apart,
+    // device planes plane_size
+    cuda_check(cudaMemcpy2DAsync(dF, sizeof(double) * ps, h_forcing, sizeof(double) * nplane,
+                                 sizeof(double) * nplane, nz, cudaMemcpyHostToDevice, ctx->stream),
+               "forcing h2d");
     cuda_check(z_transform(dF, M.nz, M.plane_size, STX_FORWARD, ctx->d_twiddle, nullptr, ctx->stream),
                "forward transform");
     if (nz > 1) cuda_check(cudaMemsetAsync(dF + ps, 0, sizeof(double) * ps, ctx->stream), "nyquist");
-    cuda_check(cudaMemsetAsync(dU, 0, sizeof(double) * ps * nz, ctx->stream), "zero solution");
+    // the solve writes every plane but the Nyquist one
+    if (nz > 1) cuda_check(cudaMemsetAsync(dU + ps, 0, sizeof(double) * ps, ctx->stream), "zero nyquist");
     const double tol = ctx->S.tokens.value("TOL_REL");
     const int smax = ctx->S.tokens.ivalue("STEP_MAX");
     int rc = stx_field_solve(sys, dF, dU, tol, smax, nullptr);
     if (rc != STX_OK) throw StxError(rc, g_last_error);
     cuda_check(z_transform(dU, M.nz, M.plane_size, STX_INVERSE, ctx->d_twiddle, nullptr, ctx->stream),
                "inverse transform");
-    for (size_t k = 0; k < nz; ++k)
-      cuda_check(cudaMemcpyAsync(h_solution + k * nplane, dU + k * ps, sizeof(double) * nplane,
-                                 cudaMemcpyDeviceToHost, ctx->stream),
-                 "solution d2h");
+    cuda_check(cudaMemcpy2DAsync(h_solution, sizeof(double) * nplane, dU, sizeof(double) * ps,
+                                 sizeof(double) * nplane, nz, cudaMemcpyDeviceToHost, ctx->stream),
+               "solution d2h");
     cuda_check(cudaStreamSynchronize(ctx->stream), "sync");
   });
 }

@@ -329,10 +329,9 @@ int stx_dns_set_field(stx_dns* d, char field, const double* h_phys) {
     cudaSetDevice(d->ctx->device);
     double* f = d->u[idx];
     ck(cudaMemsetAsync(f, 0, sizeof(double) * d->fsize, d->ctx->stream), "zero");
-    for (int k = 0; k < M.nz; ++k)
-      ck(cudaMemcpyAsync(f + static_cast<size_t>(k) * M.plane_size, h_phys + static_cast<size_t>(k) * M.nplane,
-                         sizeof(double) * M.nplane, cudaMemcpyHostToDevice, d->ctx->stream),
-         "upload");
+    ck(cudaMemcpy2DAsync(f, sizeof(double) * M.plane_size, h_phys, sizeof(double) * M.nplane,
+                         sizeof(double) * M.nplane, M.nz, cudaMemcpyHostToDevice, d->ctx->stream),
+       "upload");
     transform(d, f, STX_FORWARD);
     if (M.nz > 1) ck(cudaMemsetAsync(f + M.plane_size, 0, sizeof(double) * M.plane_size, d->ctx->stream), "nyq");
     ck(cudaStreamSynchronize(d->ctx->stream), "sync");
@@ -349,10 +348,9 @@ int stx_dns_get_field(stx_dns* d, char field, double* h_phys) {
     copy(d, d->tmp0, d->u[idx]);
     if (M.nz > 1) ck(cudaMemsetAsync(d->tmp0 + M.plane_size, 0, sizeof(double) * M.plane_size, d->ctx->stream), "nyq");
     transform(d, d->tmp0, STX_INVERSE);
-    for (int k = 0; k < M.nz; ++k)
-      ck(cudaMemcpyAsync(h_phys + static_cast<size_t>(k) * M.nplane, d->tmp0 + static_cast<size_t>(k) * M.plane_size,
-                         sizeof(double) * M.nplane, cudaMemcpyDeviceToHost, d->ctx->stream),
-         "download");
+    ck(cudaMemcpy2DAsync(h_phys, sizeof(double) * M.nplane, d->tmp0, sizeof(double) * M.plane_size,
+                         sizeof(double) * M.nplane, M.nz, cudaMemcpyDeviceToHost, d->ctx->stream),
+       "download");
     ck(cudaStreamSynchronize(d->ctx->stream), "sync");
   });
 }
