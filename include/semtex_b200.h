@@ -108,6 +108,12 @@ int stx_field_solve(stx_modal* sys, const double* d_forcing, double* d_unknown, 
  * Every matrix and field counted once. */
 int stx_modal_bytes(const stx_modal* sys, double* bytes);
 
+/* Kernel launches one stx_field_solve of a DIRECT system issues (two-level
+ * systems split their modes into groups that run on parallel streams, each
+ * group launching the whole sequence).  Instrumentation for benchmarks; no
+ * counterpart in the reference. */
+int stx_modal_launches(const stx_modal* sys, int* launches);
+
 /* Field::solve for a DIRECT system with CUDA events recorded on the
  * context stream between its phases; synchronises and returns the device
  * milliseconds of [constrain+condense, forward band sweep, backward band

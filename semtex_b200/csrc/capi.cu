@@ -571,6 +571,32 @@ int stx_modal_create(stx_context* ctx, char field, double lambda2, double beta, 
         d.prob_iface = pi.empty() ? nullptr : upload(st->arena, pi);
         d.warp_iface = wi.empty() ? nullptr : upload(st->arena, wi);
         d.nwarp_iface = static_cast<int>(wi.size());
+        // mode groups (token STX_MODE_GROUPS, default 2): contiguous modes,
+        // their own product schedules over their slice of the problems
+        const int ng = std::min(num_modes, std::max(1, ctx->S.tokens.has("STX_MODE_GROUPS")
+                                                           ? ctx->S.tokens.ivalue("STX_MODE_GROUPS")
+                                                           : 2));
+        if (ng > 1 && element_plan(ctx->dg, d, N.nglobal > N.nsolve).ok) {
+          size_t ppos = 0, ipos = 0;
+          for (int k = 0; k < ng; ++k) {
+            const int m0 = num_modes * k / ng, m1 = num_modes * (k + 1) / ng;
+            DevModal v = d;
+            v.mode0 = m0;
+            v.nmodes = m1 - m0;
+            std::vector<SymProblem> gp, gi;
+            const size_t p0 = ppos, i0 = ipos;
+            while (ppos < pp.size() && pp[ppos].mode < m1) gp.push_back(pp[ppos++]);
+            while (ipos < pi.size() && pi[ipos].mode < m1) gi.push_back(pi[ipos++]);
+            const std::vector<SymWarp> gwp = sym_schedule(gp, ctx->device), gwi = sym_schedule(gi, ctx->device);
+            v.prob_patch = gp.empty() ? nullptr : d.prob_patch + p0;
+            v.warp_patch = gwp.empty() ? nullptr : upload(st->arena, gwp);
+            v.nwarp_patch = static_cast<int>(gwp.size());
+            v.prob_iface = gi.empty() ? nullptr : d.prob_iface + i0;
+            v.warp_iface = gwi.empty() ? nullptr : upload(st->arena, gwi);
+            v.nwarp_iface = static_cast<int>(gwi.size());
+            st->groups.push_back(v);
+          }
+        }
         d.fwd = d.bwd = d.dinv_fwd = d.dinv_bwd = nullptr;
         d.nbp = 0;
         d.mode_stride = d.dinv_stride = 0;
@@ -578,6 +604,12 @@ int stx_modal_create(stx_context* ctx, char field, double lambda2, double beta, 
         cuda_check(cudaMemset(d.status, 0, sizeof(int)), "status");
         d.pc = nullptr;
         d.npts = 0;
+        for (auto& v : st->groups) {
+          v.status = d.status;
+          v.pc = nullptr;
+          v.npts = 0;
+          v.fwd = v.bwd = v.dinv_fwd = v.dinv_bwd = nullptr;
+        }
       } else if (method == STX_DIRECT) {
         // Device band layout: rows padded to an even stride (16-byte rows for
         // bulk copies), modes 256-byte aligned, plus the inverse of every
@@ -665,9 +697,27 @@ int stx_field_solve(stx_modal* sys, const double* d_forcing, double* d_unknown, 
     cudaSetDevice(ctx->device);
     if (sys->method == STX_DIRECT) {
       double* work = ctx->workspace(helmholtz_workspace_doubles(ctx->dg, F.dn, sys->store->dm));
-      cuda_check(helmholtz_direct_solve(ctx->dg, F.dn, sys->store->dm, d_forcing, d_unknown,
-                                        F.d_lines, F.nline, work, ctx->stream),
-                 "direct solve");
+      const auto& groups = sys->store->groups;
+      if (groups.size() > 1) {
+        // mode groups on parallel streams, forked from and joined back into
+        // the context stream
+        ctx->ensure_aux(groups.size() - 1);
+        cuda_check(cudaEventRecord(ctx->aux_ev[0], ctx->stream), "fork");
+        for (size_t k = 1; k < groups.size(); ++k)
+          cuda_check(cudaStreamWaitEvent(ctx->aux[k - 1], ctx->aux_ev[0], 0), "fork wait");
+        for (size_t k = 0; k < groups.size(); ++k)
+          cuda_check(helmholtz_direct_solve(ctx->dg, F.dn, groups[k], d_forcing, d_unknown, F.d_lines, F.nline,
+                                            work, k ? ctx->aux[k - 1] : ctx->stream),
+                     "direct solve");
+        for (size_t k = 1; k < groups.size(); ++k) {
+          cuda_check(cudaEventRecord(ctx->aux_ev[k], ctx->aux[k - 1]), "join");
+          cuda_check(cudaStreamWaitEvent(ctx->stream, ctx->aux_ev[k], 0), "join wait");
+        }
+      } else {
+        cuda_check(helmholtz_direct_solve(ctx->dg, F.dn, sys->store->dm, d_forcing, d_unknown,
+                                          F.d_lines, F.nline, work, ctx->stream),
+                   "direct solve");
+      }
     } else {
       double* work = ctx->workspace(jacpcg_workspace_doubles(ctx->dg, F.dn));
       std::vector<int> it(ctx->M.nz, -1);
@@ -700,6 +750,17 @@ int stx_field_solve_profiled(stx_modal* sys, const double* d_forcing, double* d_
     cuda_check(err, "profiled solve");
     check_sweep_status(sys);
     if (launches) *launches = helmholtz_direct_launches(F.dn, sys->store->dm, ctx->M.np);
+  });
+}
+
+int stx_modal_launches(const stx_modal* sys, int* launches) {
+  return guarded([&] {
+    if (!sys || !launches) throw StxError(STX_EINVAL, "null argument");
+    if (sys->method != STX_DIRECT) throw StxError(STX_EINVAL, "launch count is for DIRECT systems");
+    const stx_context* ctx = sys->ctx;
+    const auto& groups = sys->store->groups;
+    const int per = helmholtz_direct_launches(ctx->fields.at(sys->field).dn, sys->store->dm, ctx->M.np);
+    *launches = per * std::max<int>(1, static_cast<int>(groups.size()));
   });
 }
 

@@ -65,6 +65,7 @@ struct SymWarp {
 // A ModalMatrixSys on the device: one MatrixSys per locally held mode.
 struct DevModal {
   int nmodes, method, nfamily;
+  int mode0;                      // mode of blockIdx.y = 0: a launch covers modes [mode0, mode0 + nmodes)
   int nband, ns_stride;           // band width, rows reserved per mode
   int nbp;                        // factor row stride (nband rounded up to even)
   long long mode_stride;          // doubles between modes' factors (256-byte multiple)

@@ -301,7 +301,7 @@ __global__ void __launch_bounds__(32 * kMaxWarps, 1)
     k_elem_condense(DevGeom g, DevNumbering N, DevModal S, const double* __restrict__ F, const double* __restrict__ G,
                     int gstride, double* __restrict__ R, int rstride, int rb_rows) {
   extern __shared__ __align__(16) unsigned char sraw[];
-  const int c = blockIdx.x, m = blockIdx.y;
+  const int c = blockIdx.x, m = S.mode0 + blockIdx.y;
   const int nr = (g.nz > 1 && m > 0) ? 2 : 1;
   const int nn = g.npnp, next = g.next;
   const int4 cd = __ldg(g.chunk_desc + c);  // start, count, family
@@ -364,7 +364,7 @@ __global__ void __launch_bounds__(32 * kMaxWarps, 1)
     k_elem_recover(DevGeom g, DevNumbering N, DevModal S, const double* __restrict__ F, const double* __restrict__ G,
                    int gstride, const double* __restrict__ R, int rstride, double* __restrict__ U, int rb_rows) {
   extern __shared__ __align__(16) unsigned char sraw[];
-  const int c = blockIdx.x, m = blockIdx.y;
+  const int c = blockIdx.x, m = S.mode0 + blockIdx.y;
   const int nr = (g.nz > 1 && m > 0) ? 2 : 1;
   const int nn = g.npnp, next = g.next, nint = g.nint;
   const int4 cd = __ldg(g.chunk_desc + c);  // start, count, family
@@ -448,7 +448,7 @@ __global__ void __launch_bounds__(256)
     k_elem_schur(int dir, DevGeom g, DevNumbering N, DevModal S, const double* __restrict__ src,
                  double* __restrict__ dst, int rstride) {
   extern __shared__ __align__(16) unsigned char sraw[];
-  const int c = blockIdx.x, m = blockIdx.y;
+  const int c = blockIdx.x, m = S.mode0 + blockIdx.y;
   const int nr = (g.nz > 1 && m > 0) ? 2 : 1;
   // this block's part of the chunk: elements [e0, e0 + cnt)
   const int4 cd = __ldg(g.chunk_desc + c);  // start, count, family

@@ -70,9 +70,9 @@ __device__ void constrained_forcing(const DevGeom& g, const DevNumbering& N,
 }
 
 __global__ void k_essential(DevGeom g, DevNumbering N, const double* __restrict__ lines,
-                            int nline, double* __restrict__ G, int gstride, int nz) {
+                            int nline, double* __restrict__ G, int gstride, int nz, int k0) {
   const int idx = blockIdx.x * blockDim.x + threadIdx.x;
-  const int k = blockIdx.y;
+  const int k = k0 + blockIdx.y;
   if (k >= nz || idx >= N.nedge * g.np) return;
   const int b = idx / g.np;
   if (N.edge_kind[b] != 'D') return;
@@ -80,9 +80,9 @@ __global__ void k_essential(DevGeom g, DevNumbering N, const double* __restrict_
 }
 
 __global__ void k_natural(DevGeom g, DevNumbering N, const double* __restrict__ lines,
-                          int nline, double* __restrict__ R, int rstride, int nz) {
+                          int nline, double* __restrict__ R, int rstride, int nz, int k0) {
   const int idx = blockIdx.x * blockDim.x + threadIdx.x;
-  const int k = blockIdx.y;
+  const int k = k0 + blockIdx.y;
   if (k >= nz || (nz > 1 && k == 1) || idx >= N.nedge * g.np) return;
   const int b = idx / g.np;
   if (N.edge_kind[b] != 'N') return;
@@ -926,14 +926,18 @@ cudaError_t helmholtz_direct_solve(const DevGeom& g, const DevNumbering& N, cons
   double* R = work;
   double* G = work + static_cast<size_t>(rstride) * g.nz;
   const int nz = g.nz;
+  // planes of the launch's modes [mode0, mode0 + nmodes): [k0, k1)
+  const int k0 = nz > 1 ? 2 * S.mode0 : 0, k1 = nz > 1 ? std::min(nz, 2 * (S.mode0 + S.nmodes)) : 1;
+  const size_t pz = static_cast<size_t>(rstride) * (k1 - k0);
   if (ev) cudaEventRecord(ev[0], st);
-  cudaError_t err = cudaMemsetAsync(work, 0, sizeof(double) * 2 * static_cast<size_t>(rstride) * nz, st);
+  cudaError_t err = cudaMemsetAsync(R + static_cast<size_t>(rstride) * k0, 0, sizeof(double) * pz, st);
+  if (err == cudaSuccess) err = cudaMemsetAsync(G + static_cast<size_t>(rstride) * k0, 0, sizeof(double) * pz, st);
   if (err != cudaSuccess) return err;
   const bool has_ess = N.nglobal > N.nsolve;
   const int nedge_nodes = N.nedge * g.np;
   if (has_ess && nedge_nodes) {
-    dim3 grid((nedge_nodes + 127) / 128, nz);
-    k_essential<<<grid, 128, 0, st>>>(g, N, lines, nline, G, rstride, nz);
+    dim3 grid((nedge_nodes + 127) / 128, k1 - k0);
+    k_essential<<<grid, 128, 0, st>>>(g, N, lines, nline, G, rstride, nz, k0);
   }
   const int threads = ((g.npnp + 31) / 32) * 32 < 64 ? 64 : ((g.npnp + 31) / 32) * 32;
   const size_t shm = sizeof(double) * (static_cast<size_t>(g.np) * g.np + 5 * g.npnp);
@@ -960,8 +964,8 @@ cudaError_t helmholtz_direct_solve(const DevGeom& g, const DevNumbering& N, cons
     k_condense<<<egrid, threads, shm, st>>>(g, N, S, F, has_ess ? G : nullptr, rstride, R, rstride);
   }
   if (nedge_nodes) {
-    dim3 grid((nedge_nodes + 127) / 128, nz);
-    k_natural<<<grid, 128, 0, st>>>(g, N, lines, nline, R, rstride, nz);
+    dim3 grid((nedge_nodes + 127) / 128, k1 - k0);
+    k_natural<<<grid, 128, 0, st>>>(g, N, lines, nline, R, rstride, nz, k0);
   }
   if (ev) cudaEventRecord(ev[1], st);
   const SweepPlan plan = S.l2 ? SweepPlan() : sweep_plan(S.nbp, S.nband);
@@ -1044,7 +1048,7 @@ cudaError_t helmholtz_jacpcg_solve(const DevGeom& g, const DevNumbering& N, cons
   const int nedge_nodes = N.nedge * g.np;
   if (has_ess && nedge_nodes) {
     dim3 grid((nedge_nodes + 127) / 128, nz);
-    k_essential<<<grid, 128, 0, st>>>(g, N, lines, nline, G, gs, nz);
+    k_essential<<<grid, 128, 0, st>>>(g, N, lines, nline, G, gs, nz, 0);
   }
   const int threads = ((g.npnp + 31) / 32) * 32 < 64 ? 64 : ((g.npnp + 31) / 32) * 32;
   const size_t shm = sizeof(double) * (static_cast<size_t>(g.np) * g.np + 5 * g.npnp);
@@ -1052,7 +1056,7 @@ cudaError_t helmholtz_jacpcg_solve(const DevGeom& g, const DevNumbering& N, cons
   k_pcg_rhs<<<egrid, threads, shm, st>>>(g, N, S, F, has_ess ? G : nullptr, gs, r, vs);
   if (nedge_nodes) {
     dim3 grid((nedge_nodes + 127) / 128, nz);
-    k_natural<<<grid, 128, 0, st>>>(g, N, lines, nline, r, vs, nz);
+    k_natural<<<grid, 128, 0, st>>>(g, N, lines, nline, r, vs, nz, 0);
   }
   const dim3 vgrid(std::min(1024, (npts + 255) / 256), nz);
   const dim3 zgrid(std::max(1, std::min(64, (N.nglobal + 255) / 256)), nz);

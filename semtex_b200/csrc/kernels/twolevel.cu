@@ -218,7 +218,11 @@ cudaError_t twolevel_solve(const DevModal& S, const DevGeom& g, const DevNumberi
                            double* work, int nz, cudaStream_t st, cudaEvent_t mid) {
   double* Yv = work;
   double* Z = twolevel_solution(work, rstride, nz);
-  cudaError_t err = cudaMemsetAsync(work, 0, sizeof(double) * twolevel_workspace_doubles(rstride, nz), st);
+  // planes of the launch's modes
+  const int k0 = nz > 1 ? 2 * S.mode0 : 0, k1 = nz > 1 ? std::min(nz, 2 * (S.mode0 + S.nmodes)) : 1;
+  const size_t off = static_cast<size_t>(rstride) * k0, len = sizeof(double) * rstride * (k1 - k0);
+  cudaError_t err = cudaMemsetAsync(Yv + off, 0, len, st);
+  if (err == cudaSuccess) err = cudaMemsetAsync(Z + off, 0, len, st);
   if (err != cudaSuccess) return err;
 
   // y_I = S_II^-1 R_I; r_B = R_B - S_BI y_I

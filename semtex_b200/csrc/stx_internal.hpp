@@ -40,6 +40,11 @@ struct ModalStore {
   DeviceArena arena;
   DevModal dm{};
   std::vector<int> nsolve;
+  // Two-level DIRECT systems: views of dm over contiguous mode groups, each
+  // with its own product schedules.  The groups of a solve run on parallel
+  // streams (the modes are independent), so the phases of one group overlap
+  // those of another.
+  std::vector<DevModal> groups;
 };
 
 void host_dft_forward(std::vector<double>& a, int nz, int n);
@@ -120,7 +125,29 @@ struct stx_context {
     }
     return d_scratch;
   }
+  // Streams of mode groups 1.. (group 0 runs on `stream`) and the events
+  // that fork them from `stream` and join them back.
+  std::vector<cudaStream_t> aux;
+  std::vector<cudaEvent_t> aux_ev;  // [0] fork, [i] join of aux[i - 1]
+  void ensure_aux(size_t n) {
+    if (aux_ev.empty()) {
+      aux_ev.resize(1);
+      if (cudaEventCreateWithFlags(&aux_ev[0], cudaEventDisableTiming) != cudaSuccess)
+        throw std::runtime_error("event creation failed");
+    }
+    while (aux.size() < n) {
+      cudaStream_t s;
+      cudaEvent_t e;
+      if (cudaStreamCreateWithFlags(&s, cudaStreamNonBlocking) != cudaSuccess ||
+          cudaEventCreateWithFlags(&e, cudaEventDisableTiming) != cudaSuccess)
+        throw std::runtime_error("stream creation failed");
+      aux.push_back(s);
+      aux_ev.push_back(e);
+    }
+  }
   ~stx_context() {
+    for (auto s : aux) cudaStreamDestroy(s);
+    for (auto e : aux_ev) cudaEventDestroy(e);
     if (d_work) cudaFree(d_work);
     if (d_scratch) cudaFree(d_scratch);
   }
