@@ -11,6 +11,7 @@
 // owns 32 consecutive points of every plane: loads and stores of each plane
 // row are coalesced, and the transform runs out of shared memory.
 #include "helmholtz.cuh"
+#include "ptx.cuh"
 
 namespace stx {
 
@@ -75,9 +76,12 @@ __global__ void k_dft(double* __restrict__ data, int nz, int plane_size, int sig
 // host-computed table as the DFT's.
 // ---------------------------------------------------------------------------
 
+// Radices of the stages, 4 bits each from the lowest (read with shifts: a
+// kernel parameter indexed at run time would be copied to local memory).
 struct FftPlan {
   int nf;
-  int radix[16];
+  unsigned long long radices;
+  __device__ int dradix(int f) const { return static_cast<int>((radices >> (4 * f)) & 15u); }
 };
 
 __device__ __forceinline__ void cmul(double& ar, double& ai, double br, double bi) {
@@ -146,9 +150,10 @@ __device__ __forceinline__ void small_dft(double* vr, double* vi, double s) {
   }
 }
 
-template <int R>
+template <int R, int TP>
 __device__ __forceinline__ void stockham_stage(const double* xr, const double* xi, double* yr, double* yi, int N,
-                                               int Ns, int tp, const double* tw, double s) {
+                                               int Ns, const double* tw, double s) {
+  constexpr int tp = TP;
   const int nj = N / R;
   for (int w = threadIdx.x; w < nj * tp; w += blockDim.x) {
     const int j = w / tp, p = w - j * tp;
@@ -159,11 +164,11 @@ __device__ __forceinline__ void stockham_stage(const double* xr, const double* x
       vr[r] = xr[(j + r * nj) * tp + p];
       vi[r] = xi[(j + r * nj) * tp + p];
     }
-    // twiddle exp(s 2 pi i r k / (Ns R)) = table entry r*k*N/(Ns R)
+    // twiddle exp(s 2 pi i r k / (Ns R)) = table entry r*k*N/(Ns R) (< N)
     const int step = N / (Ns * R);
 #pragma unroll
     for (int r = 1; r < R; ++r) {
-      const int m = (r * k * step) % N;
+      const int m = r * k * step;
       cmul(vr[r], vi[r], tw[m], s * tw[N + m]);  // exp(s i theta) = cos + s i sin
     }
     small_dft<R>(vr, vi, s);
@@ -176,40 +181,81 @@ __device__ __forceinline__ void stockham_stage(const double* xr, const double* x
   }
 }
 
+// Set when a bounded wait of k_fft for its bulk copies expired (the block
+// then leaves its lines untransformed).
+__device__ int g_fft_timeout = 0;
+
+// bulk != 0: the block's plane rows (tp contiguous points each, 16-byte
+// aligned) arrive by bulk copies issued by one warp, all on one mbarrier, so
+// the whole load is one memory round trip.
+template <int TP>
 __global__ void k_fft(double* __restrict__ data, int nz, int plane_size, int sign, const double* __restrict__ twiddle,
-                      FftPlan plan, int tp) {
-  extern __shared__ double sm[];
-  double* tw = sm;                       // [2][nz]
+                      FftPlan plan, int bulk) {
+  constexpr int tp = TP;
+  extern __shared__ __align__(16) double sm[];
+  uint64_t* bar = reinterpret_cast<uint64_t*>(sm);
+  double* tw = sm + 2;                   // [2][nz]
   double* ar = tw + 2 * nz;              // four [nz][tp] buffers
   double* ai = ar + nz * tp;
   double* br = ai + nz * tp;
   double* bi = br + nz * tp;
   const int p0 = blockIdx.x * tp;
+  const int cnt = min(tp, plane_size - p0);
   const int N = nz, half = nz / 2;
+  double* land = sign > 0 ? ar : br;     // plane rows as stored: real lines, or the packed spectrum
+  if (bulk) {
+    if (threadIdx.x == 0) {
+      mbar_init(bar, 1);
+      asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
+      mbar_expect_tx(bar, static_cast<unsigned>(sizeof(double) * nz * cnt));
+    }
+    __syncthreads();  // armed before any copy can complete
+    if (threadIdx.x < 32)
+      for (int n = threadIdx.x; n < nz; n += 32)
+        bulk_g2s(land + n * tp, data + static_cast<size_t>(n) * plane_size + p0,
+                 static_cast<unsigned>(sizeof(double) * cnt), bar);
+  }
   for (int t = threadIdx.x; t < 2 * nz; t += blockDim.x) tw[t] = twiddle[t];
+  if (bulk) {
+    if (cnt < tp)
+      for (int t = threadIdx.x; t < nz * tp; t += blockDim.x)
+        if (t % tp >= cnt) land[t] = 0.0;  // columns no copy writes
+    const bool ok = __syncthreads_and(mbar_wait(bar, 0));
+    if (!ok) {
+      if (threadIdx.x == 0) atomicExch(&g_fft_timeout, 1);
+      mbar_wait(bar, 0);
+      return;
+    }
+  } else {
+    for (int t = threadIdx.x; t < nz * tp; t += blockDim.x) {
+      const int n = t / tp, p = t - n * tp;
+      land[t] = (p < cnt) ? data[static_cast<size_t>(n) * plane_size + p0 + p] : 0.0;
+    }
+    __syncthreads();
+  }
+  // complex lines: real input, or the packed spectrum expanded to its
+  // Hermitian form
   for (int t = threadIdx.x; t < nz * tp; t += blockDim.x) {
-    const int n = t / tp, p = t - n * tp;
-    const double v = (p0 + p < plane_size) ? data[static_cast<size_t>(n) * plane_size + p0 + p] : 0.0;
     if (sign > 0) {
-      ar[t] = v;
       ai[t] = 0.0;
+      continue;
+    }
+    const int n = t / tp, p = t - n * tp;
+    const double v = br[t];
+    if (n == 0) {
+      ar[p] = v;
+      ai[p] = 0.0;
+    } else if (n == 1) {
+      ar[half * tp + p] = v;
+      ai[half * tp + p] = 0.0;
     } else {
-      // packed plane n -> Hermitian spectrum
-      if (n == 0) {
-        ar[p] = v;
-        ai[p] = 0.0;
-      } else if (n == 1) {
-        ar[half * tp + p] = v;
-        ai[half * tp + p] = 0.0;
+      const int kk = n >> 1;
+      if (n & 1) {
+        ai[kk * tp + p] = v;
+        ai[(N - kk) * tp + p] = -v;
       } else {
-        const int kk = n >> 1;
-        if (n & 1) {
-          ai[kk * tp + p] = v;
-          ai[(N - kk) * tp + p] = -v;
-        } else {
-          ar[kk * tp + p] = v;
-          ar[(N - kk) * tp + p] = v;
-        }
+        ar[kk * tp + p] = v;
+        ar[(N - kk) * tp + p] = v;
       }
     }
   }
@@ -218,11 +264,11 @@ __global__ void k_fft(double* __restrict__ data, int nz, int plane_size, int sig
   double *xr = ar, *xi = ai, *yr = br, *yi = bi;
   int Ns = 1;
   for (int f = 0; f < plan.nf; ++f) {
-    const int R = plan.radix[f];
-    if (R == 4) stockham_stage<4>(xr, xi, yr, yi, N, Ns, tp, tw, s);
-    else if (R == 2) stockham_stage<2>(xr, xi, yr, yi, N, Ns, tp, tw, s);
-    else if (R == 3) stockham_stage<3>(xr, xi, yr, yi, N, Ns, tp, tw, s);
-    else stockham_stage<5>(xr, xi, yr, yi, N, Ns, tp, tw, s);
+    const int R = plan.dradix(f);
+    if (R == 4) stockham_stage<4, TP>(xr, xi, yr, yi, N, Ns, tw, s);
+    else if (R == 2) stockham_stage<2, TP>(xr, xi, yr, yi, N, Ns, tw, s);
+    else if (R == 3) stockham_stage<3, TP>(xr, xi, yr, yi, N, Ns, tw, s);
+    else stockham_stage<5, TP>(xr, xi, yr, yi, N, Ns, tw, s);
     Ns *= R;
     double* t0 = xr;
     xr = yr;
@@ -268,24 +314,35 @@ cudaError_t z_transform(double* data, int nz, int plane_size, int sign, const do
   FftPlan plan{};
   {
     int n = nz;
-    while (n % 4 == 0 && plan.nf < 16) { plan.radix[plan.nf++] = 4; n /= 4; }
-    while (n % 2 == 0 && plan.nf < 16) { plan.radix[plan.nf++] = 2; n /= 2; }
-    while (n % 3 == 0 && plan.nf < 16) { plan.radix[plan.nf++] = 3; n /= 3; }
-    while (n % 5 == 0 && plan.nf < 16) { plan.radix[plan.nf++] = 5; n /= 5; }
+    auto add = [&](unsigned long long r) { plan.radices |= r << (4 * plan.nf++); };
+    while (n % 4 == 0 && plan.nf < 16) { add(4); n /= 4; }
+    while (n % 2 == 0 && plan.nf < 16) { add(2); n /= 2; }
+    while (n % 3 == 0 && plan.nf < 16) { add(3); n /= 3; }
+    while (n % 5 == 0 && plan.nf < 16) { add(5); n /= 5; }
     if (n != 1) plan.nf = 0;
   }
   static bool attr_set = false;
   if (!attr_set) {
     cudaFuncSetAttribute(k_dft, cudaFuncAttributeMaxDynamicSharedMemorySize, 200 * 1024);
-    cudaFuncSetAttribute(k_fft, cudaFuncAttributeMaxDynamicSharedMemorySize, 200 * 1024);
+    cudaFuncSetAttribute(k_fft<32>, cudaFuncAttributeMaxDynamicSharedMemorySize, 200 * 1024);
+    cudaFuncSetAttribute(k_fft<16>, cudaFuncAttributeMaxDynamicSharedMemorySize, 200 * 1024);
+    cudaFuncSetAttribute(k_fft<8>, cudaFuncAttributeMaxDynamicSharedMemorySize, 200 * 1024);
+    cudaFuncSetAttribute(k_fft<4>, cudaFuncAttributeMaxDynamicSharedMemorySize, 200 * 1024);
     attr_set = true;
   }
   if (plan.nf > 0) {
     int tp = 32;
-    while (tp > 4 && sizeof(double) * (4 * static_cast<size_t>(nz) * tp + 2 * nz) > 160 * 1024) tp /= 2;
-    const size_t fshm = sizeof(double) * (4 * static_cast<size_t>(nz) * tp + 2 * nz);
+    while (tp > 4 && sizeof(double) * (4 * static_cast<size_t>(nz) * tp + 2 * nz + 2) > 160 * 1024) tp /= 2;
+    const size_t fshm = sizeof(double) * (4 * static_cast<size_t>(nz) * tp + 2 * nz + 2);
+    // bulk row copies need 16-byte aligned rows: an aligned base and an even
+    // plane size (tp is even)
+    const int bulk = (reinterpret_cast<uintptr_t>(data) % 16 == 0 && plane_size % 2 == 0 && tp % 2 == 0) ? 1 : 0;
     if (fshm <= 200 * 1024) {
-      k_fft<<<(plane_size + tp - 1) / tp, 256, fshm, st>>>(data, nz, plane_size, sign, twiddle, plan, tp);
+      const int nb = (plane_size + tp - 1) / tp;
+      if (tp == 32) k_fft<32><<<nb, 256, fshm, st>>>(data, nz, plane_size, sign, twiddle, plan, bulk);
+      else if (tp == 16) k_fft<16><<<nb, 256, fshm, st>>>(data, nz, plane_size, sign, twiddle, plan, bulk);
+      else if (tp == 8) k_fft<8><<<nb, 256, fshm, st>>>(data, nz, plane_size, sign, twiddle, plan, bulk);
+      else k_fft<4><<<nb, 256, fshm, st>>>(data, nz, plane_size, sign, twiddle, plan, bulk);
       return cudaGetLastError();
     }
   }
