@@ -53,15 +53,33 @@ def forcing_per_unique_node(x, y, nz, seed):
     return vals[:, inv].reshape((nz,) + x.shape), len(uniq)
 
 
-def dist_init():
+def dist_init(backend="nccl"):
+    """One process per GPU (torchrun env); a short timeout so that ranks
+    waiting on a lost peer end with an error."""
     ws = int(os.environ.get("WORLD_SIZE", "1"))
     rank = int(os.environ.get("RANK", "0"))
     local = int(os.environ.get("LOCAL_RANK", "0"))
     if ws > 1:
         import torch.distributed as dist
         import datetime
-        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=120))
+        dist.init_process_group(backend, timeout=datetime.timedelta(seconds=120))
     return ws, rank, local
+
+
+def max_over_ranks(value, ws, device):
+    """The largest of the ranks' values (the job's time is its slowest rank's)."""
+    if ws <= 1:
+        return value
+    import torch
+    t = torch.tensor([value], dtype=torch.float64, device=device)
+    torch.distributed.all_reduce(t, op=torch.distributed.ReduceOp.MAX)
+    return t.item()
+
+
+def job_rate(units_per_rank, ws, seconds):
+    """Whole-job throughput of ws replicas that each processed
+    units_per_rank in at most `seconds` (weak scaling)."""
+    return units_per_rank * ws / seconds
 
 
 def clocks_start():
@@ -271,11 +289,9 @@ def run_ours(args):
             flush.fill_(1.0)
         phases.append(solve_profiled())
     torch.cuda.synchronize()
+    t_total = max_over_ranks(t_total, ws, f"cuda:{local}")
     if ws > 1:
-        t = torch.tensor([t_total], device=f"cuda:{local}")
-        torch.distributed.all_reduce(t, op=torch.distributed.ReduceOp.MAX)
         torch.distributed.barrier()
-        t_total = t.item()
     # -- end to end through the host-buffer call
     fh = torch.from_numpy(np.ascontiguousarray(f)).pin_memory()
     uh = torch.empty_like(fh).pin_memory()
@@ -289,10 +305,7 @@ def run_ours(args):
         _lib.check(_lib.lib().stx_elliptic_solve_host(sysm.handle, C.c_void_p(fh.data_ptr()),
                                                       C.c_void_p(uh.data_ptr())))
     e_total = time.perf_counter() - e0
-    if ws > 1:
-        t = torch.tensor([e_total], device=f"cuda:{local}")
-        torch.distributed.all_reduce(t, op=torch.distributed.ReduceOp.MAX)
-        e_total = t.item()
+    e_total = max_over_ranks(e_total, ws, f"cuda:{local}")
     clocks = clocks_stop(clk_p, clk_f, local)
     if rank != 0:
         if ws > 1:
@@ -320,11 +333,11 @@ def run_ours(args):
                "sample": f"{len(planes)} of {w['nz'] - 1} solved planes (modes 0,1,10,31), "
                          "oracle restatement: per-element condensation + LAPACK dpbtrs, 1 thread"}
     line = {
-        "metric": METRIC, "value": dof * args.steps * ws / t_total, "unit": UNIT, "n_gpus": ws,
+        "metric": METRIC, "value": job_rate(dof * args.steps, ws, t_total), "unit": UNIT, "n_gpus": ws,
         "steps": args.steps, "warmup": args.warmup, "ms_per_step": 1e3 * t_total / args.steps,
         "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f64",
         "data": "synthetic", "config": config_block(),
-        "e2e": {"value": dof * args.steps * ws / e_total, "unit": UNIT,
+        "e2e": {"value": job_rate(dof * args.steps, ws, e_total), "unit": UNIT,
                 "h2d_bytes_per_step": int(fh.numel() * 8), "d2h_bytes_per_step": int(uh.numel() * 8)},
         "roofline": {"bound": "hbm", "kernel": phase_names[top], "achieved": achieved, "peak": peak,
                      "unit": "GB/s", "frac": achieved / peak, "peak_kind": kind, "traffic": traffic,
