@@ -502,6 +502,8 @@ int stx_modal_create(stx_context* ctx, char field, double lambda2, double beta, 
         std::vector<double> hbi, hii, sc, pack;
         const int ldsc = element_ld(nx);
         std::vector<long long> fam_off(static_cast<size_t>(num_modes) * P->nfamily), if_off(num_modes);
+        std::vector<long long> g_off(static_cast<size_t>(num_modes) * P->nfamily);
+        const size_t nB_max = std::max(1, P->nB_max);
         std::vector<int> pin(num_modes, -1);
         const size_t nI_max = std::max(1, P->nI_max);
         for (int m = 0; m < num_modes; ++m) {
@@ -518,6 +520,13 @@ int stx_modal_create(stx_context* ctx, char field, double lambda2, double beta, 
             pack.resize(pack.size() + sym_size(n), 0.0);
             sym_pack(n, modes[m].l2_sinv.data() + static_cast<size_t>(f) * nI_max * nI_max, nI_max,
                      pack.data() + fam_off[static_cast<size_t>(m) * P->nfamily + f]);
+          }
+          for (int f = 0; f < P->nfamily; ++f) {
+            const int rep = P->family_rep[f], nI = P->nI[rep], nB = P->nB[rep];
+            g_off[static_cast<size_t>(m) * P->nfamily + f] = static_cast<long long>(pack.size());
+            pack.resize(pack.size() + gen_size(nI, nB), 0.0);
+            gen_pack(nI, nB, modes[m].l2_g.data() + static_cast<size_t>(f) * nI_max * nB_max, nB_max,
+                     pack.data() + g_off[static_cast<size_t>(m) * P->nfamily + f]);
           }
           if_off[m] = static_cast<long long>(pack.size());
           pack.resize(pack.size() + sym_size(P->niface), 0.0);
@@ -547,6 +556,10 @@ int stx_modal_create(stx_context* ctx, char field, double lambda2, double beta, 
         d.p_Igid = upload(st->arena, P->I_gid);
         d.p_Biid = upload(st->arena, P->B_iid);
         d.skel_of = upload(st->arena, P->skel_of.empty() ? std::vector<int>{0} : P->skel_of);
+        // skeleton ids of each patch's interface nodes (columns of its G)
+        std::vector<int> bgid(P->B_iid.size(), 0);
+        for (size_t k = 0; k < bgid.size(); ++k) bgid[k] = P->B_iid[k] >= 0 ? P->skel_of[P->B_iid[k]] : 0;
+        const int* d_bgid = upload(st->arena, bgid.empty() ? std::vector<int>{0} : bgid);
         d.pin = upload(st->arena, pin);
         d.hbi = upload(st->arena, hbi);
         d.hii = upload(st->arena, hii);
@@ -554,17 +567,27 @@ int stx_modal_create(stx_context* ctx, char field, double lambda2, double beta, 
         d.l2_sc = upload(st->arena, sc);
         d.l2_sc_ld = ldsc;
         d.l2_ncode = upload(st->arena, ncode);
-        // products: S_II^-1 per (patch, mode), the interface inverse per
-        // mode; each streamed by warps in equal runs of tiles
-        std::vector<SymProblem> pp, pi;
+        // products: S_II^-1 and -G per (patch, mode), the interface inverse
+        // per mode; each streamed by warps in equal runs of tiles
+        std::vector<SymProblem> pp, pi, pg;
         for (int m = 0; m < num_modes; ++m)
-          for (int p = 0; p < P->npatch; ++p)
-            if (P->nI[p] > 0)
-              pp.push_back(SymProblem{fam_off[static_cast<size_t>(m) * P->nfamily + P->family[p]], P->nI[p], m, -1,
-                                      d.p_Igid + static_cast<size_t>(p) * nI_max});
+          for (int p = 0; p < P->npatch; ++p) {
+            if (P->nI[p] <= 0) continue;
+            const size_t fm = static_cast<size_t>(m) * P->nfamily + P->family[p];
+            const int* rows = d.p_Igid + static_cast<size_t>(p) * nI_max;
+            pp.push_back(SymProblem{fam_off[fm], P->nI[p], m, -1, rows, 0, nullptr, 1.0});
+            if (P->nB[p] > 0)
+              pg.push_back(SymProblem{g_off[fm], P->nI[p], m, -1, rows, P->nB[p], d_bgid + static_cast<size_t>(p) * nB_max,
+                                      -1.0});
+          }
         if (P->niface > 0)
-          for (int m = 0; m < num_modes; ++m) pi.push_back(SymProblem{if_off[m], P->niface, m, pin[m], d.skel_of});
-        const std::vector<SymWarp> wp = sym_schedule(pp, ctx->device), wi = sym_schedule(pi, ctx->device);
+          for (int m = 0; m < num_modes; ++m)
+            pi.push_back(SymProblem{if_off[m], P->niface, m, pin[m], d.skel_of, 0, nullptr, 1.0});
+        const std::vector<SymWarp> wp = sym_schedule(pp, ctx->device), wi = sym_schedule(pi, ctx->device),
+                                   wg = sym_schedule(pg, ctx->device);
+        d.prob_gen = pg.empty() ? nullptr : upload(st->arena, pg);
+        d.warp_gen = wg.empty() ? nullptr : upload(st->arena, wg);
+        d.nwarp_gen = static_cast<int>(wg.size());
         d.prob_patch = pp.empty() ? nullptr : upload(st->arena, pp);
         d.warp_patch = wp.empty() ? nullptr : upload(st->arena, wp);
         d.nwarp_patch = static_cast<int>(wp.size());
@@ -577,17 +600,22 @@ int stx_modal_create(stx_context* ctx, char field, double lambda2, double beta, 
                                                            ? ctx->S.tokens.ivalue("STX_MODE_GROUPS")
                                                            : 2));
         if (ng > 1 && element_plan(ctx->dg, d, N.nglobal > N.nsolve).ok) {
-          size_t ppos = 0, ipos = 0;
+          size_t ppos = 0, ipos = 0, gpos = 0;
           for (int k = 0; k < ng; ++k) {
             const int m0 = num_modes * k / ng, m1 = num_modes * (k + 1) / ng;
             DevModal v = d;
             v.mode0 = m0;
             v.nmodes = m1 - m0;
-            std::vector<SymProblem> gp, gi;
-            const size_t p0 = ppos, i0 = ipos;
+            std::vector<SymProblem> gp, gi, gg;
+            const size_t p0 = ppos, i0 = ipos, q0 = gpos;
             while (ppos < pp.size() && pp[ppos].mode < m1) gp.push_back(pp[ppos++]);
             while (ipos < pi.size() && pi[ipos].mode < m1) gi.push_back(pi[ipos++]);
-            const std::vector<SymWarp> gwp = sym_schedule(gp, ctx->device), gwi = sym_schedule(gi, ctx->device);
+            while (gpos < pg.size() && pg[gpos].mode < m1) gg.push_back(pg[gpos++]);
+            const std::vector<SymWarp> gwp = sym_schedule(gp, ctx->device), gwi = sym_schedule(gi, ctx->device),
+                                       gwg = sym_schedule(gg, ctx->device);
+            v.prob_gen = gg.empty() ? nullptr : d.prob_gen + q0;
+            v.warp_gen = gwg.empty() ? nullptr : upload(st->arena, gwg);
+            v.nwarp_gen = static_cast<int>(gwg.size());
             v.prob_patch = gp.empty() ? nullptr : d.prob_patch + p0;
             v.warp_patch = gwp.empty() ? nullptr : upload(st->arena, gwp);
             v.nwarp_patch = static_cast<int>(gwp.size());
@@ -784,13 +812,19 @@ int stx_modal_bytes(const stx_modal* sys, double* bytes) {
     if (d.l2) {
       // first half: S_II^-1 products (packed, once per patch family and
       // mode), element Schur complements, interface products (packed);
-      // second half: the element Schur complements and S_II^-1 again
+      // second half: the G = S_II^-1 S_IB products (tiles, once per patch
+      // family and mode)
       const Patching* P = ctx->fields.at(sys->field).P.get();
       double pm = 0;
       for (int f = 0; f < P->nfamily; ++f) pm += static_cast<double>(sym_size(P->nI[P->family_rep[f]]));
       const double sc = static_cast<double>(M.nfamily) * M.next * M.next;
+      double gm = 0;
+      for (int f = 0; f < P->nfamily; ++f) {
+        const int rep = P->family_rep[f];
+        gm += static_cast<double>(gen_size(P->nI[rep], P->nB[rep]));
+      }
       bytes[1] = w * nm * (pm + sc + static_cast<double>(sym_size(d.niface))) + 4 * rhs;
-      bytes[2] = w * nm * (pm + sc) + 3 * rhs;
+      bytes[2] = w * nm * gm + 2 * rhs;
     } else {
       double band = 0;
       for (int m = 0; m < nm; ++m) band += w * static_cast<double>(sys->store->nsolve[m]) * d.nband;

@@ -232,7 +232,7 @@ ModeSystem build_mode_system(const Mesh& M, const Numbering& N, const Patching* 
     //    skeleton nodes; assemble the interface Schur complements.
     const int nI_max = std::max(1, P->nI_max), nB_max = std::max(1, P->nB_max);
     S.l2_sinv.assign(static_cast<size_t>(P->nfamily) * nI_max * nI_max, 0.0);
-    std::vector<double> l2_g(static_cast<size_t>(P->nfamily) * nI_max * nB_max, 0.0);  // S_II^-1 S_IB
+    S.l2_g.assign(static_cast<size_t>(P->nfamily) * nI_max * nB_max, 0.0);
     std::vector<std::vector<double>> T(P->nfamily);
     for (int f = 0; f < P->nfamily; ++f) {
       const int p = P->family_rep[f];
@@ -251,7 +251,7 @@ ModeSystem build_mode_system(const Mesh& M, const Numbering& N, const Patching* 
         }
       }
       double* Si = &S.l2_sinv[static_cast<size_t>(f) * nI_max * nI_max];
-      double* G = &l2_g[static_cast<size_t>(f) * nI_max * nB_max];
+      double* G = &S.l2_g[static_cast<size_t>(f) * nI_max * nB_max];
       std::vector<double> II(static_cast<size_t>(nI) * nI);
       for (int a = 0; a < nI; ++a)
         for (int b = 0; b < nI; ++b) II[static_cast<size_t>(a) * nI + b] = Sp[static_cast<size_t>(a) * nl + b];

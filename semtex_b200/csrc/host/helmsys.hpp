@@ -37,6 +37,7 @@ struct ModeSystem {
   // With a patching (two-level condensation) the patch matrices and the dense
   // inverse of the patch-interface Schur complement replace the band factor:
   std::vector<double> l2_sinv;  // [pfamily][nI_max][nI_max]  S_II^{-1}
+  std::vector<double> l2_g;     // [pfamily][nI_max][nB_max]  S_II^{-1} S_IB
   std::vector<double> l2_ainv;  // [niface][niface] inverse of the interface system
   std::vector<double> hsc;      // [nfamily][next][next] element Schur complements h_bb - h_bi h_ii^-1 h_ib
   int pin_iid = -1;             // interface node fixed to zero (singular mode)

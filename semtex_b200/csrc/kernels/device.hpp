@@ -46,13 +46,18 @@ struct DevNumbering {
   const double* edge_area;  // [nedge*np]
 };
 
-// One packed symmetric product y += A x for the planes of a Fourier mode:
-// the matrix at l2_pack + moff (order n); x_i is read and y_i accumulated at
-// position idx[i] of the planes' skeleton vectors (x_pin taken as zero).
+// One tiled product y += scale A x for the planes of a Fourier mode, the
+// matrix at l2_pack + moff: symmetric packed (ncol = 0, order n; x_i read
+// and y_i accumulated at position idx[i] of the planes' skeleton vectors,
+// x_pin taken as zero) or general n x ncol (y_i at idx[i], x_j read at
+// idx_col[j]).
 struct SymProblem {
   long long moff;
   int n, mode, pin;
   const int* idx;
+  int ncol;
+  const int* idx_col;
+  double scale;
 };
 
 // The tiles one warp of a packed product streams: `count` tiles in packed
@@ -108,6 +113,9 @@ struct DevModal {
   const SymProblem* prob_iface;   // interface products: one per mode
   const SymWarp* warp_iface;
   int nwarp_iface;
+  const SymProblem* prob_gen;     // recovery products -G x_B: one per (patch, mode)
+  const SymWarp* warp_gen;
+  int nwarp_gen;
   const double* l2_sc;            // [nmodes][nfamily][next][l2_sc_ld] element Schur complements
   int l2_sc_ld;
   const int* l2_ncode;            // [nel][next], elements in chunk order: skeleton id << 2 | class

@@ -68,4 +68,36 @@ inline void sym_pack(int n, const double* A, size_t lda, double* out) {
     }
 }
 
+// General (rectangular) nr x nc matrices in the same tile format: all
+// T_r x T_c tiles, tile-row-major, last tile row stored as tall as needed
+// (rounded up to even), columns past nc zero.
+__host__ __device__ inline int gen_ntiles(int nr, int nc) { return sym_tiles(nr) * sym_tiles(nc); }
+
+__host__ __device__ inline long long gen_size(int nr, int nc) {
+  if (nr <= 0 || nc <= 0) return 0;
+  const long long Tr = sym_tiles(nr), Tc = sym_tiles(nc), hs = (sym_last_rows(nr) + 1) / 2 * 2;
+  return (Tr - 1) * Tc * kSymTile * kSymLd + Tc * hs * kSymLd;
+}
+
+__host__ __device__ inline long long gen_tile_offset(int nr, int nc, int I, int J) {
+  const int Tr = sym_tiles(nr), Tc = sym_tiles(nc);
+  const long long full = static_cast<long long>(kSymTile) * kSymLd;
+  if (I < Tr - 1) return (static_cast<long long>(I) * Tc + J) * full;
+  return static_cast<long long>(Tr - 1) * Tc * full + static_cast<long long>(J) * sym_rows_stored(nr, I) * kSymLd;
+}
+
+inline void gen_pack(int nr, int nc, const double* A, size_t lda, double* out) {
+  const int Tr = sym_tiles(nr), Tc = sym_tiles(nc);
+  for (int I = 0; I < Tr; ++I)
+    for (int J = 0; J < Tc; ++J) {
+      double* t = out + gen_tile_offset(nr, nc, I, J);
+      const int h = sym_rows(nr, I);
+      for (int r = 0; r < h; ++r)
+        for (int c = 0; c < kSymTile; ++c) {
+          const int i = kSymTile * I + r, j = kSymTile * J + c;
+          t[r * kSymLd + c] = j < nc ? A[static_cast<size_t>(i) * lda + j] : 0.0;
+        }
+    }
+}
+
 }  // namespace stx

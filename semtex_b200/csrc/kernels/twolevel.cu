@@ -10,10 +10,11 @@
 //   r_B = R_B - S_BI y_I                 (per element: S is assembled from
 //                                         the element Schur complements)
 //   x_B = A^-1 r_B                       (A = S_BB - S_BI S_II^-1 S_IB)
-//   x_I = S_II^-1 (R_I - S_IB x_B)       (per element, then per patch)
-// S_II^-1 and A^-1 are symmetric and stored packed (symtile.hpp); each
-// product streams its tiles with bulk copies, the Re and Im planes of a mode
-// sharing every tile read, each tile applied as itself and as its transpose.
+//   x_I = y_I - G x_B                    (per patch, G = S_II^-1 S_IB)
+// S_II^-1 and A^-1 are symmetric and stored packed, G in tiles
+// (symtile.hpp); each product streams its tiles with bulk copies, the Re and
+// Im planes of a mode sharing every tile read, a symmetric tile applied as
+// itself and as its transpose.
 #include "twolevel.cuh"
 
 #include <algorithm>
@@ -39,21 +40,33 @@ struct SymWarpSmem {
 };
 constexpr size_t kSymSmem = kSymWarps * sizeof(SymWarpSmem);
 
-// Position of a warp in the packed tiles of its problems.
+// Position of a warp in the tiles of its problems.
 struct SymCursor {
-  int p, q, I, J, nt;
+  int p, q, I, J, nt, tc;
   SymProblem P;
   __device__ void load(const SymProblem* probs, int prob, int tile) {
     p = prob;
     q = tile;
     P = probs[p];
-    nt = sym_ntiles(P.n);
-    sym_tile_at(q, I, J);
+    if (P.ncol) {
+      tc = sym_tiles(P.ncol);
+      nt = sym_tiles(P.n) * tc;
+      I = q / tc;
+      J = q - I * tc;
+    } else {
+      tc = 0;
+      nt = sym_ntiles(P.n);
+      sym_tile_at(q, I, J);
+    }
+  }
+  __device__ bool row_last() const { return P.ncol ? J == tc - 1 : J == I; }
+  __device__ long long offset() const {
+    return P.ncol ? gen_tile_offset(P.n, P.ncol, I, J) : sym_tile_offset(P.n, I, J);
   }
   __device__ void next(const SymProblem* probs, bool more) {
     if (++q == nt) {
       if (more) load(probs, p + 1, 0);
-    } else if (J == I) {
+    } else if (row_last()) {
       ++I;
       J = 0;
     } else {
@@ -62,7 +75,7 @@ struct SymCursor {
   }
 };
 
-// y[idx] += A x[idx] for every problem: each warp streams its run of tiles
+// y[idx] += scale A x[idx] for every problem: each warp streams its run of tiles
 // (SymWarp) through a two-buffer ring.  For a tile, lane 0 bulk-copies the
 // tile and every lane copies (cp.async) the x entries of the tile's column
 // and row blocks, all completing on the buffer's mbarrier (count 1 + 32).
@@ -93,10 +106,14 @@ __global__ void __launch_bounds__(32 * kSymWarps)
   // issue (column block, row block), loaded one issue ahead
   int pf[2];
   auto prefetch = [&]() {
-#pragma unroll
-    for (int h = 0; h < 2; ++h) {
-      const int i = kSymTile * (h ? ic.I : ic.J) + ln;
-      pf[h] = (i < ic.P.n && i != ic.P.pin) ? __ldg(ic.P.idx + i) : -1;
+    const int i = kSymTile * ic.J + ln;  // column block
+    if (ic.P.ncol) {
+      pf[0] = i < ic.P.ncol ? __ldg(ic.P.idx_col + i) : -1;
+      pf[1] = -1;  // general products have no transposed part
+    } else {
+      pf[0] = (i < ic.P.n && i != ic.P.pin) ? __ldg(ic.P.idx + i) : -1;
+      const int r = kSymTile * ic.I + ln;  // row block
+      pf[1] = (r < ic.P.n && r != ic.P.pin) ? __ldg(ic.P.idx + r) : -1;
     }
   };
   prefetch();
@@ -106,7 +123,7 @@ __global__ void __launch_bounds__(32 * kSymWarps)
     if (ln == 0) {
       const unsigned bytes = static_cast<unsigned>(sizeof(double) * kSymLd * sym_rows_stored(n, ic.I));
       mbar_expect_tx(&sm.bar[s], bytes);
-      bulk_g2s(sm.tile[s], pack + ic.P.moff + sym_tile_offset(n, ic.I, ic.J), bytes, &sm.bar[s]);
+      bulk_g2s(sm.tile[s], pack + ic.P.moff + ic.offset(), bytes, &sm.bar[s]);
     }
     const double* X0 = X + static_cast<size_t>(2 * m) * rstride;
     const double* X1 = X0 + rstride;
@@ -137,14 +154,15 @@ __global__ void __launch_bounds__(32 * kSymWarps)
       break;
     }
     const int n = cc.P.n, m = cc.P.mode, I = cc.I, J = cc.J;
-    const bool two = nz > 1 && m > 0;
+    const bool two = nz > 1 && m > 0, sym = cc.P.ncol == 0;
+    const double scale = cc.P.scale;
     const double* A = sm.tile[s];
     const double2* xs = sm.x[s];
     const int h = sym_rows(n, I);
     // output positions (column block for the transposed part, row block at a
     // row's end), loaded before the products to overlap their latency
-    const bool row_end = J == I || done + 1 == W.count;
-    const int g_col = J < I ? __ldg(cc.P.idx + kSymTile * J + ln) : 0;  // J < T - 1: a full tile column
+    const bool row_end = cc.row_last() || done + 1 == W.count;
+    const int g_col = (sym && J < I) ? __ldg(cc.P.idx + kSymTile * J + ln) : 0;  // J < T - 1: a full tile column
     const int g_row = (row_end && ln < h) ? __ldg(cc.P.idx + kSymTile * I + ln) : 0;
     if (ln < h) {
       const double* Ar = A + ln * kSymLd;
@@ -161,7 +179,7 @@ __global__ void __launch_bounds__(32 * kSymWarps)
     }
     double* Y0 = Y + static_cast<size_t>(2 * m) * rstride;
     double* Y1 = Y0 + rstride;
-    if (J < I) {
+    if (sym && J < I) {
       double p0[4] = {0.0, 0.0, 0.0, 0.0}, p1[4] = {0.0, 0.0, 0.0, 0.0};
       if (h == kSymTile) {
 #pragma unroll
@@ -179,13 +197,13 @@ __global__ void __launch_bounds__(32 * kSymWarps)
           p1[0] = fma(a, x.y, p1[0]);
         }
       }
-      atomicAdd(&Y0[g_col], (p0[0] + p0[1]) + (p0[2] + p0[3]));
-      if (two) atomicAdd(&Y1[g_col], (p1[0] + p1[1]) + (p1[2] + p1[3]));
+      atomicAdd(&Y0[g_col], scale * ((p0[0] + p0[1]) + (p0[2] + p0[3])));
+      if (two) atomicAdd(&Y1[g_col], scale * ((p1[0] + p1[1]) + (p1[2] + p1[3])));
     }
     if (row_end) {
       if (ln < h) {
-        atomicAdd(&Y0[g_row], d0);
-        if (two) atomicAdd(&Y1[g_row], d1);
+        atomicAdd(&Y0[g_row], scale * d0);
+        if (two) atomicAdd(&Y1[g_row], scale * d1);
       }
       d0 = d1 = 0.0;
     }
@@ -212,42 +230,40 @@ cudaError_t launch_psymv(const DevModal& S, const SymProblem* probs, const SymWa
 
 }  // namespace
 
-size_t twolevel_workspace_doubles(int rstride, int nz) { return 2 * static_cast<size_t>(rstride) * nz; }
+size_t twolevel_workspace_doubles(int rstride, int nz) { return static_cast<size_t>(rstride) * nz; }
 
 cudaError_t twolevel_solve(const DevModal& S, const DevGeom& g, const DevNumbering& N, double* R, int rstride,
                            double* work, int nz, cudaStream_t st, cudaEvent_t mid) {
-  double* Yv = work;
-  double* Z = twolevel_solution(work, rstride, nz);
+  double* Yv = twolevel_solution(work, rstride, nz);  // y_I, then the whole skeleton solution
   // planes of the launch's modes
   const int k0 = nz > 1 ? 2 * S.mode0 : 0, k1 = nz > 1 ? std::min(nz, 2 * (S.mode0 + S.nmodes)) : 1;
-  const size_t off = static_cast<size_t>(rstride) * k0, len = sizeof(double) * rstride * (k1 - k0);
-  cudaError_t err = cudaMemsetAsync(Yv + off, 0, len, st);
-  if (err == cudaSuccess) err = cudaMemsetAsync(Z + off, 0, len, st);
+  cudaError_t err = cudaMemsetAsync(Yv + static_cast<size_t>(rstride) * k0, 0,
+                                    sizeof(double) * rstride * (k1 - k0), st);
   if (err != cudaSuccess) return err;
-
   // y_I = S_II^-1 R_I; r_B = R_B - S_BI y_I
   err = launch_psymv(S, S.prob_patch, S.warp_patch, S.nwarp_patch, R, Yv, rstride, nz, st);
   if (err != cudaSuccess) return err;
   element_schur_apply(0, g, N, S, Yv, R, rstride, st);
-  // x_B = A^-1 r_B
-  err = launch_psymv(S, S.prob_iface, S.warp_iface, S.nwarp_iface, R, Z, rstride, nz, st);
+  // x_B = A^-1 r_B (into the interface positions of Y)
+  err = launch_psymv(S, S.prob_iface, S.warp_iface, S.nwarp_iface, R, Yv, rstride, nz, st);
   if (err != cudaSuccess) return err;
   if (mid) cudaEventRecord(mid, st);
-  // R_I -= S_IB x_B; x_I = S_II^-1 R_I
-  element_schur_apply(1, g, N, S, Z, R, rstride, st);
-  err = launch_psymv(S, S.prob_patch, S.warp_patch, S.nwarp_patch, R, Z, rstride, nz, st);
+  // x_I = y_I - G x_B, G = S_II^-1 S_IB
+  err = launch_psymv(S, S.prob_gen, S.warp_gen, S.nwarp_gen, Yv, Yv, rstride, nz, st);
   if (err != cudaSuccess) return err;
   return cudaGetLastError();
 }
 
 int twolevel_launches(const DevModal& S) {
-  return (S.nwarp_patch > 0 ? 2 : 0) + (S.nwarp_iface > 0 ? 1 : 0) + 2;
+  return (S.nwarp_patch > 0 ? 1 : 0) + (S.nwarp_iface > 0 ? 1 : 0) + (S.nwarp_gen > 0 ? 1 : 0) + 1;
 }
+
+static int prob_ntiles(const SymProblem& P) { return P.ncol ? gen_ntiles(P.n, P.ncol) : sym_ntiles(P.n); }
 
 std::vector<SymWarp> sym_schedule(const std::vector<SymProblem>& probs, int device) {
   std::vector<SymWarp> out;
   long long total = 0;
-  for (const auto& P : probs) total += sym_ntiles(P.n);
+  for (const auto& P : probs) total += prob_ntiles(P);
   if (total == 0) return out;
   int sms = 148, per_sm = 1;
   cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, device);
@@ -260,7 +276,7 @@ std::vector<SymWarp> sym_schedule(const std::vector<SymProblem>& probs, int devi
   long long before = 0;  // tiles of problems [0, p)
   for (long long w = 0; w < nw; ++w) {
     const long long t0 = total * w / nw, t1 = total * (w + 1) / nw;
-    while (before + sym_ntiles(probs[p].n) <= t0) before += sym_ntiles(probs[p++].n);
+    while (before + prob_ntiles(probs[p]) <= t0) before += prob_ntiles(probs[p++]);
     out.push_back(SymWarp{static_cast<int>(p), static_cast<int>(t0 - before), static_cast<int>(t1 - t0)});
   }
   return out;

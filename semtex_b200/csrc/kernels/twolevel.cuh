@@ -8,8 +8,8 @@
 
 namespace stx {
 
-// Doubles of scratch twolevel_solve needs after R: two skeleton vectors per
-// plane (patch-interior products, solution).
+// Doubles of scratch twolevel_solve needs after R: one skeleton vector per
+// plane (patch-interior products, then the solution).
 size_t twolevel_workspace_doubles(int rstride, int nz);
 
 // Skeleton vectors R[k][0..nglobal) of every solved plane hold the condensed
@@ -19,9 +19,7 @@ size_t twolevel_workspace_doubles(int rstride, int nz);
 cudaError_t twolevel_solve(const DevModal& S, const DevGeom& g, const DevNumbering& N, double* R, int rstride,
                            double* work, int nz, cudaStream_t st, cudaEvent_t mid = nullptr);
 
-inline double* twolevel_solution(double* work, int rstride, int nz) {
-  return work + static_cast<size_t>(rstride) * nz;
-}
+inline double* twolevel_solution(double* work, int /*rstride*/, int /*nz*/) { return work; }
 
 int twolevel_launches(const DevModal& S);
 

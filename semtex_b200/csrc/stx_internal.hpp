@@ -74,8 +74,8 @@ struct stx_context {
   // when the single banded factor is used (token STX_TWOLEVEL = 0, element
   // boundaries of more than 64 nodes, or an interface too large for a dense
   // inverse).  The patch size is the one of {8, 16, 36, 64} elements that
-  // minimises the packed matrix bytes read per mode (the interface inverse
-  // once, each patch-interior inverse twice).
+  // minimises the matrix bytes read per mode (the interface inverse and,
+  // per patch family, S_II^-1 and G = S_II^-1 S_IB once each).
   const stx::Patching* patching(char field) {
     stx::FieldDev& F = fields.at(field);
     if (!F.patch_done) {
@@ -87,7 +87,10 @@ struct stx_context {
           auto P = std::make_unique<stx::Patching>(stx::build_patching(M, F.N, cap));
           if (P->niface > 6000) continue;
           double bytes = static_cast<double>(stx::sym_size(P->niface));
-          for (int f = 0; f < P->nfamily; ++f) bytes += 2.0 * stx::sym_size(P->nI[P->family_rep[f]]);
+          for (int f = 0; f < P->nfamily; ++f) {
+            const int rep = P->family_rep[f];
+            bytes += static_cast<double>(stx::sym_size(P->nI[rep]) + stx::gen_size(P->nI[rep], P->nB[rep]));
+          }
           if (!F.P || bytes < best) {
             best = bytes;
             F.P = std::move(P);
