@@ -150,7 +150,8 @@ __device__ __forceinline__ void small_dft(double* vr, double* vi, double s) {
   }
 }
 
-template <int R, int TP>
+// One radix-R stage over TP complex lines whose rows are LD doubles apart.
+template <int R, int TP, int LD>
 __device__ __forceinline__ void stockham_stage(const double* xr, const double* xi, double* yr, double* yi, int N,
                                                int Ns, const double* tw, double s) {
   constexpr int tp = TP;
@@ -161,8 +162,8 @@ __device__ __forceinline__ void stockham_stage(const double* xr, const double* x
     double vr[R], vi[R];
 #pragma unroll
     for (int r = 0; r < R; ++r) {
-      vr[r] = xr[(j + r * nj) * tp + p];
-      vi[r] = xi[(j + r * nj) * tp + p];
+      vr[r] = xr[(j + r * nj) * LD + p];
+      vi[r] = xi[(j + r * nj) * LD + p];
     }
     // twiddle exp(s 2 pi i r k / (Ns R)) = table entry r*k*N/(Ns R) (< N)
     const int step = N / (Ns * R);
@@ -175,8 +176,8 @@ __device__ __forceinline__ void stockham_stage(const double* xr, const double* x
     const int base = (j / Ns) * Ns * R + k;
 #pragma unroll
     for (int r = 0; r < R; ++r) {
-      yr[(base + r * Ns) * tp + p] = vr[r];
-      yi[(base + r * Ns) * tp + p] = vi[r];
+      yr[(base + r * Ns) * LD + p] = vr[r];
+      yi[(base + r * Ns) * LD + p] = vi[r];
     }
   }
 }
@@ -185,24 +186,25 @@ __device__ __forceinline__ void stockham_stage(const double* xr, const double* x
 // then leaves its lines untransformed).
 __device__ int g_fft_timeout = 0;
 
-// bulk != 0: the block's plane rows (tp contiguous points each, 16-byte
-// aligned) arrive by bulk copies issued by one warp, all on one mbarrier, so
-// the whole load is one memory round trip.
-template <int TP>
+// Real transforms of TPL z-lines per block as TPL/2 complex transforms: the
+// block's rows [n][TPL] are read as complex lines z = x_p + i x_{p+TPL/2}
+// (real part columns 0..TPL/2-1, imaginary part the rest); the two real
+// spectra are separated afterwards through Hermitian symmetry (forward), or
+// combined before the transform (inverse).  bulk != 0: the rows (16-byte
+// aligned) arrive by bulk copies issued by one warp on one mbarrier.
+template <int TPL>
 __global__ void k_fft(double* __restrict__ data, int nz, int plane_size, int sign, const double* __restrict__ twiddle,
                       FftPlan plan, int bulk) {
-  constexpr int tp = TP;
+  constexpr int TPC = TPL / 2, LD = TPL;
   extern __shared__ __align__(16) double sm[];
   uint64_t* bar = reinterpret_cast<uint64_t*>(sm);
   double* tw = sm + 2;                   // [2][nz]
-  double* ar = tw + 2 * nz;              // four [nz][tp] buffers
-  double* ai = ar + nz * tp;
-  double* br = ai + nz * tp;
-  double* bi = br + nz * tp;
-  const int p0 = blockIdx.x * tp;
-  const int cnt = min(tp, plane_size - p0);
+  double* A = tw + 2 * nz;               // two [nz][LD] buffers
+  double* B = A + nz * LD;
+  const int p0 = blockIdx.x * TPL;
+  const int cnt = min(TPL, plane_size - p0);
   const int N = nz, half = nz / 2;
-  double* land = sign > 0 ? ar : br;     // plane rows as stored: real lines, or the packed spectrum
+  double* land = sign > 0 ? A : B;       // plane rows as stored: real lines, or the packed spectra
   if (bulk) {
     if (threadIdx.x == 0) {
       mbar_init(bar, 1);
@@ -212,14 +214,14 @@ __global__ void k_fft(double* __restrict__ data, int nz, int plane_size, int sig
     __syncthreads();  // armed before any copy can complete
     if (threadIdx.x < 32)
       for (int n = threadIdx.x; n < nz; n += 32)
-        bulk_g2s(land + n * tp, data + static_cast<size_t>(n) * plane_size + p0,
+        bulk_g2s(land + n * LD, data + static_cast<size_t>(n) * plane_size + p0,
                  static_cast<unsigned>(sizeof(double) * cnt), bar);
   }
   for (int t = threadIdx.x; t < 2 * nz; t += blockDim.x) tw[t] = twiddle[t];
   if (bulk) {
-    if (cnt < tp)
-      for (int t = threadIdx.x; t < nz * tp; t += blockDim.x)
-        if (t % tp >= cnt) land[t] = 0.0;  // columns no copy writes
+    if (cnt < TPL)
+      for (int t = threadIdx.x; t < nz * LD; t += blockDim.x)
+        if (t % LD >= cnt) land[t] = 0.0;  // columns no copy writes
     const bool ok = __syncthreads_and(mbar_wait(bar, 0));
     if (!ok) {
       if (threadIdx.x == 0) atomicExch(&g_fft_timeout, 1);
@@ -227,71 +229,77 @@ __global__ void k_fft(double* __restrict__ data, int nz, int plane_size, int sig
       return;
     }
   } else {
-    for (int t = threadIdx.x; t < nz * tp; t += blockDim.x) {
-      const int n = t / tp, p = t - n * tp;
-      land[t] = (p < cnt) ? data[static_cast<size_t>(n) * plane_size + p0 + p] : 0.0;
+    for (int t = threadIdx.x; t < nz * LD; t += blockDim.x) {
+      const int n = t / LD, c = t - n * LD;
+      land[t] = (c < cnt) ? data[static_cast<size_t>(n) * plane_size + p0 + c] : 0.0;
     }
     __syncthreads();
   }
-  // complex lines: real input, or the packed spectrum expanded to its
-  // Hermitian form
-  for (int t = threadIdx.x; t < nz * tp; t += blockDim.x) {
-    if (sign > 0) {
-      ai[t] = 0.0;
-      continue;
-    }
-    const int n = t / tp, p = t - n * tp;
-    const double v = br[t];
-    if (n == 0) {
-      ar[p] = v;
-      ai[p] = 0.0;
-    } else if (n == 1) {
-      ar[half * tp + p] = v;
-      ai[half * tp + p] = 0.0;
-    } else {
-      const int kk = n >> 1;
-      if (n & 1) {
-        ai[kk * tp + p] = v;
-        ai[(N - kk) * tp + p] = -v;
-      } else {
-        ar[kk * tp + p] = v;
-        ar[(N - kk) * tp + p] = v;
+  if (sign < 0) {
+    // Z_k = X_k + i X'_k from the packed spectra of lines q and q + TPC
+    // (B: plane 0 = Re X_0, 1 = Re X_{N/2}, 2k / 2k+1 = Re / Im X_k)
+    for (int t = threadIdx.x; t < N * TPC; t += blockDim.x) {
+      const int k = t / TPC, q = t - k * TPC;
+      double xr[2], xi[2];
+#pragma unroll
+      for (int h = 0; h < 2; ++h) {
+        const int c = q + h * TPC;
+        if (k == 0) {
+          xr[h] = B[c];
+          xi[h] = 0.0;
+        } else if (k == half) {
+          xr[h] = B[LD + c];
+          xi[h] = 0.0;
+        } else if (k < half) {
+          xr[h] = B[(2 * k) * LD + c];
+          xi[h] = B[(2 * k + 1) * LD + c];
+        } else {
+          xr[h] = B[(2 * (N - k)) * LD + c];
+          xi[h] = -B[(2 * (N - k) + 1) * LD + c];
+        }
       }
+      A[k * LD + q] = xr[0] - xi[1];
+      A[k * LD + q + TPC] = xi[0] + xr[1];
     }
   }
   __syncthreads();
   const double s = sign > 0 ? -1.0 : 1.0;
-  double *xr = ar, *xi = ai, *yr = br, *yi = bi;
+  double *xb = A, *yb = B;
   int Ns = 1;
   for (int f = 0; f < plan.nf; ++f) {
     const int R = plan.dradix(f);
-    if (R == 4) stockham_stage<4, TP>(xr, xi, yr, yi, N, Ns, tw, s);
-    else if (R == 2) stockham_stage<2, TP>(xr, xi, yr, yi, N, Ns, tw, s);
-    else if (R == 3) stockham_stage<3, TP>(xr, xi, yr, yi, N, Ns, tw, s);
-    else stockham_stage<5, TP>(xr, xi, yr, yi, N, Ns, tw, s);
+    if (R == 4) stockham_stage<4, TPC, LD>(xb, xb + TPC, yb, yb + TPC, N, Ns, tw, s);
+    else if (R == 2) stockham_stage<2, TPC, LD>(xb, xb + TPC, yb, yb + TPC, N, Ns, tw, s);
+    else if (R == 3) stockham_stage<3, TPC, LD>(xb, xb + TPC, yb, yb + TPC, N, Ns, tw, s);
+    else stockham_stage<5, TPC, LD>(xb, xb + TPC, yb, yb + TPC, N, Ns, tw, s);
     Ns *= R;
-    double* t0 = xr;
-    xr = yr;
-    yr = t0;
-    t0 = xi;
-    xi = yi;
-    yi = t0;
+    double* t0 = xb;
+    xb = yb;
+    yb = t0;
     __syncthreads();
   }
-  const double scale = 1.0 / nz;
-  for (int t = threadIdx.x; t < nz * tp; t += blockDim.x) {
-    const int n = t / tp, p = t - n * tp;
-    if (p0 + p >= plane_size) continue;
-    double v;
-    if (sign > 0) {
-      if (n == 0) v = xr[p] * scale;
-      else if (n == 1) v = xr[half * tp + p] * scale;
-      else if (n & 1) v = xi[(n >> 1) * tp + p] * scale;
-      else v = xr[(n >> 1) * tp + p] * scale;
-    } else {
-      v = xr[t];
+  if (sign < 0) {
+    // z_n = x_n + i x'_n: the rows are the real lines again
+    for (int t = threadIdx.x; t < nz * LD; t += blockDim.x) {
+      const int n = t / LD, c = t - n * LD;
+      if (c < cnt) data[static_cast<size_t>(n) * plane_size + p0 + c] = xb[t];
     }
-    data[static_cast<size_t>(n) * plane_size + p0 + p] = v;
+    return;
+  }
+  // X_k = (Z_k + conj Z_{N-k}) / 2, X'_k = (Z_k - conj Z_{N-k}) / 2i, packed and scaled
+  const double scale = 0.5 / nz;
+  for (int t = threadIdx.x; t < nz * TPC; t += blockDim.x) {
+    const int n = t / TPC, q = t - n * TPC;
+    const int k = n == 0 ? 0 : (n == 1 ? half : n >> 1);
+    const bool im = n >= 2 && (n & 1);
+    const int kn = k == 0 ? 0 : N - k;
+    const double zr = xb[k * LD + q], zi = xb[k * LD + q + TPC];
+    const double wr = xb[kn * LD + q], wi = xb[kn * LD + q + TPC];
+    const double v0 = im ? (zi - wi) : (zr + wr);   // line q
+    const double v1 = im ? (wr - zr) : (zi + wi);   // line q + TPC
+    const size_t row = static_cast<size_t>(n) * plane_size + p0;
+    if (q < cnt) data[row + q] = v0 * scale;
+    if (q + TPC < cnt) data[row + q + TPC] = v1 * scale;
   }
 }
 
@@ -332,8 +340,8 @@ cudaError_t z_transform(double* data, int nz, int plane_size, int sign, const do
   }
   if (plan.nf > 0) {
     int tp = 32;
-    while (tp > 4 && sizeof(double) * (4 * static_cast<size_t>(nz) * tp + 2 * nz + 2) > 160 * 1024) tp /= 2;
-    const size_t fshm = sizeof(double) * (4 * static_cast<size_t>(nz) * tp + 2 * nz + 2);
+    while (tp > 4 && sizeof(double) * (2 * static_cast<size_t>(nz) * tp + 2 * nz + 2) > 160 * 1024) tp /= 2;
+    const size_t fshm = sizeof(double) * (2 * static_cast<size_t>(nz) * tp + 2 * nz + 2);
     // bulk row copies need 16-byte aligned rows: an aligned base and an even
     // plane size (tp is even)
     const int bulk = (reinterpret_cast<uintptr_t>(data) % 16 == 0 && plane_size % 2 == 0 && tp % 2 == 0) ? 1 : 0;
