@@ -8,9 +8,10 @@
 //   waveProp              dns/integrate.cpp:204-239
 //   setPForce, project    dns/integrate.cpp:242-289
 //
-// Element kernels run one block per (element, plane) with a thread per node;
-// the element's plane data, D and the inverse mapping partials are read once
-// and the node results are produced in a single pass over the element.
+// Element kernels run one warp per (element, plane), kEpPlanes planes of one
+// element per block: D is staged once per block, each warp holds its plane's
+// element data in its own shared memory (lanes over nodes, a few nodes per
+// lane loaded together) and synchronises only with itself.
 #include "dns_kernels.cuh"
 
 namespace stx {
@@ -39,16 +40,47 @@ __device__ __forceinline__ double zderiv(const double* a, int k, size_t x, int p
   return -beta * m * a[static_cast<size_t>(k + 1) * plane_size + x];
 }
 
+constexpr int kEpPlanes = 8;  // planes (warps) per block of the element kernels
+constexpr int kEpNodes = 8;   // nodes per lane loaded together (np <= 16)
+
+// Block (element, planes [kEpPlanes y, +kEpPlanes)): stage D, return this
+// warp's plane (or -1 past the last plane) and its shared-memory area of
+// `fields` element planes.
+__device__ __forceinline__ int ep_setup(const DevGeom& g, double* sm, int fields, double*& ws) {
+  for (int q = threadIdx.x; q < g.np * g.np; q += blockDim.x) sm[q] = g.D[q];
+  __syncthreads();
+  const int w = threadIdx.x >> 5;
+  ws = sm + g.np * g.np + static_cast<size_t>(w) * fields * g.npnp;
+  const int k = blockIdx.y * kEpPlanes + w;
+  return k < g.nz ? k : -1;
+}
+
+// dst[t] = src[t] for the element's nodes (lanes over nodes, loads first).
+__device__ __forceinline__ void ep_load(const double* __restrict__ src, double* dst, int npnp) {
+  const int ln = threadIdx.x & 31;
+  double v[kEpNodes];
+#pragma unroll
+  for (int u = 0; u < kEpNodes; ++u) {
+    const int t = ln + 32 * u;
+    v[u] = t < npnp ? src[t] : 0.0;
+  }
+#pragma unroll
+  for (int u = 0; u < kEpNodes; ++u) {
+    const int t = ln + 32 * u;
+    if (t < npnp) dst[t] = v[u];
+  }
+}
+
 __global__ void k_grad_xy(DevGeom g, const double* __restrict__ in, double* __restrict__ out, int dir) {
   extern __shared__ double sm[];
-  double* sD = sm;
-  double* su = sD + g.np * g.np;
-  const int e = blockIdx.x, k = blockIdx.y, t = threadIdx.x;
+  double* su;
+  const int k = ep_setup(g, sm, 1, su);
+  if (k < 0) return;
+  const int e = blockIdx.x, ln = threadIdx.x & 31;
   const size_t base = static_cast<size_t>(k) * g.plane_size + static_cast<size_t>(e) * g.npnp;
-  for (int q = t; q < g.np * g.np; q += blockDim.x) sD[q] = g.D[q];
-  if (t < g.npnp) su[t] = in[base + t];
-  __syncthreads();
-  if (t < g.npnp) out[base + t] = elem_deriv(g, su, sD, e, t, dir);
+  ep_load(in + base, su, g.npnp);
+  __syncwarp();
+  for (int t = ln; t < g.npnp; t += 32) out[base + t] = elem_deriv(g, su, sm, e, t, dir);
 }
 
 __global__ void k_grad_z(const double* __restrict__ in, double* __restrict__ out, int nz, int plane_size,
@@ -71,57 +103,77 @@ __global__ void k_product(const double* __restrict__ a, const double* __restrict
 // N = sc * [ conv: -(U0 dUi/dx + U1 dUi/dy + U2 Tc)
 //            cons: -(d(Ui U0)/dx + d(Ui U1)/dy + Tk) ] , form 0 skew (sc=1/2,
 // both), 1 convective, 2 conservative.  Tc / Tk / U2 may be null (2D).
-__global__ void k_nonlinear(DevGeom g, NonlinearArgs a) {
+__global__ void __launch_bounds__(32 * kEpPlanes, 3) k_nonlinear(DevGeom g, NonlinearArgs a) {
   extern __shared__ double sm[];
-  const int npnp = g.npnp;
-  double* sD = sm;
-  double* sUi = sD + g.np * g.np;
+  double* ws;
+  const int k = ep_setup(g, sm, 5, ws);
+  if (k < 0) return;
+  const int np = g.np, npnp = g.npnp, e = blockIdx.x, ln = threadIdx.x & 31;
+  double* sUi = ws;
   double* sP0 = sUi + npnp;
   double* sP1 = sP0 + npnp;
-  const int e = blockIdx.x, k = blockIdx.y, t = threadIdx.x;
+  double* sU0 = sP1 + npnp;
+  double* sU1 = sU0 + npnp;
   const size_t base = static_cast<size_t>(k) * g.plane_size + static_cast<size_t>(e) * npnp;
-  for (int q = t; q < g.np * g.np; q += blockDim.x) sD[q] = g.D[q];
-  double u0 = 0.0, u1 = 0.0, ui = 0.0;
-  if (t < npnp) {
-    u0 = a.U0[base + t];
-    u1 = a.U1[base + t];
-    ui = a.Ui[base + t];
-    sUi[t] = ui;
-    sP0[t] = ui * u0;
-    sP1[t] = ui * u1;
+  ep_load(a.U0 + base, sU0, npnp);
+  ep_load(a.U1 + base, sU1, npnp);
+  ep_load(a.Ui + base, sUi, npnp);
+  __syncwarp();
+  for (int t = ln; t < npnp; t += 32) {
+    sP0[t] = sUi[t] * sU0[t];
+    sP1[t] = sUi[t] * sU1[t];
   }
-  __syncthreads();
-  if (t >= npnp) return;
-  double conv = 0.0, cons = 0.0;
-  if (a.form != 2) {
-    conv = -(u0 * elem_deriv(g, sUi, sD, e, t, 0) + u1 * elem_deriv(g, sUi, sD, e, t, 1));
-    if (a.U2 && a.Tc) conv -= a.U2[base + t] * a.Tc[base + t];
+  __syncwarp();
+  const bool conv_on = a.form != 2, cons_on = a.form != 1;
+  for (int t = ln; t < npnp; t += 32) {
+    const int i = t / np, j = t - i * np;
+    // reference (r, s) derivatives of Ui, Ui U0, Ui U1 in one pass
+    double ur = 0.0, us = 0.0, p0r = 0.0, p0s = 0.0, p1r = 0.0, p1s = 0.0;
+    for (int kk = 0; kk < np; ++kk) {
+      const double dj = sm[j * np + kk], di = sm[i * np + kk];
+      const int row = i * np + kk, col = kk * np + j;
+      ur = fma(sUi[row], dj, ur);
+      us = fma(di, sUi[col], us);
+      p0r = fma(sP0[row], dj, p0r);
+      p0s = fma(di, sP0[col], p0s);
+      p1r = fma(sP1[row], dj, p1r);
+      p1s = fma(di, sP1[col], p1s);
+    }
+    const int q = e * npnp + t;
+    const double rx = g.drdx[q], ry = g.drdy[q], sx = g.dsdx[q], sy = g.dsdy[q];
+    double conv = 0.0, cons = 0.0;
+    if (conv_on) {
+      conv = -(sU0[t] * (ur * rx + us * sx) + sU1[t] * (ur * ry + us * sy));
+      if (a.U2 && a.Tc) conv -= a.U2[base + t] * a.Tc[base + t];
+    }
+    if (cons_on) {
+      cons = -((p0r * rx + p0s * sx) + (p1r * ry + p1s * sy));
+      if (a.Tk) cons -= a.Tk[base + t];
+    }
+    a.N[base + t] = a.form == 0 ? 0.5 * (conv + cons) : (a.form == 1 ? conv : cons);
   }
-  if (a.form != 1) {
-    cons = -(elem_deriv(g, sP0, sD, e, t, 0) + elem_deriv(g, sP1, sD, e, t, 1));
-    if (a.Tk) cons -= a.Tk[base + t];
-  }
-  double v = a.form == 0 ? 0.5 * (conv + cons) : (a.form == 1 ? conv : cons);
-  a.N[base + t] = v;
 }
 
 __global__ void k_dss_accum(DevGeom g, DevNumbering N, const double* __restrict__ in, double* __restrict__ ds,
                             int gstride) {
-  const int e = blockIdx.x, k = blockIdx.y, t = threadIdx.x;
-  if (t >= g.next) return;
-  const int node = g.emap[t];
-  const double v = g.Q4[e * g.npnp + node] *
-                   in[static_cast<size_t>(k) * g.plane_size + static_cast<size_t>(e) * g.npnp + node];
-  atomicAdd(&ds[static_cast<size_t>(k) * gstride + N.btog[e * g.next + t]], v);
+  const int e = blockIdx.x, k = blockIdx.y * kEpPlanes + (threadIdx.x >> 5), ln = threadIdx.x & 31;
+  if (k >= g.nz) return;
+  const double* src = in + static_cast<size_t>(k) * g.plane_size + static_cast<size_t>(e) * g.npnp;
+  for (int t = ln; t < g.next; t += 32) {
+    const int node = g.emap[t];
+    atomicAdd(&ds[static_cast<size_t>(k) * gstride + N.btog[e * g.next + t]], g.Q4[e * g.npnp + node] * src[node]);
+  }
 }
 
 __global__ void k_dss_insert(DevGeom g, DevNumbering N, double* __restrict__ io, const double* __restrict__ ds,
                              int gstride) {
-  const int e = blockIdx.x, k = blockIdx.y, t = threadIdx.x;
-  if (t >= g.next) return;
-  const int gi = N.btog[e * g.next + t];
-  io[static_cast<size_t>(k) * g.plane_size + static_cast<size_t>(e) * g.npnp + g.emap[t]] =
-      ds[static_cast<size_t>(k) * gstride + gi] * N.imass[gi];
+  const int e = blockIdx.x, k = blockIdx.y * kEpPlanes + (threadIdx.x >> 5), ln = threadIdx.x & 31;
+  if (k >= g.nz) return;
+  double* dst = io + static_cast<size_t>(k) * g.plane_size + static_cast<size_t>(e) * g.npnp;
+  for (int t = ln; t < g.next; t += 32) {
+    const int gi = N.btog[e * g.next + t];
+    dst[g.emap[t]] = ds[static_cast<size_t>(k) * gstride + gi] * N.imass[gi];
+  }
 }
 
 __global__ void k_combine(CombineArgs a, size_t n) {
@@ -138,44 +190,50 @@ __global__ void k_divergence(DevGeom g, const double* __restrict__ a0, const dou
                              const double* __restrict__ a2, double* __restrict__ out, double inv_dt,
                              double beta) {
   extern __shared__ double sm[];
-  double* sD = sm;
-  double* s0 = sD + g.np * g.np;
-  double* s1 = s0 + g.npnp;
-  const int e = blockIdx.x, k = blockIdx.y, t = threadIdx.x;
+  double* ws;
+  const int k = ep_setup(g, sm, 2, ws);
+  if (k < 0) return;
+  const int e = blockIdx.x, ln = threadIdx.x & 31;
+  double* s0 = ws;
+  double* s1 = ws + g.npnp;
   const size_t base = static_cast<size_t>(k) * g.plane_size + static_cast<size_t>(e) * g.npnp;
-  for (int q = t; q < g.np * g.np; q += blockDim.x) sD[q] = g.D[q];
-  if (t < g.npnp) {
-    s0[t] = a0[base + t];
-    s1[t] = a1[base + t];
+  ep_load(a0 + base, s0, g.npnp);
+  ep_load(a1 + base, s1, g.npnp);
+  __syncwarp();
+  for (int t = ln; t < g.npnp; t += 32) {
+    double v = elem_deriv(g, s0, sm, e, t, 0) + elem_deriv(g, s1, sm, e, t, 1);
+    if (a2) v += zderiv(a2, k, base + t - static_cast<size_t>(k) * g.plane_size, g.plane_size, beta);
+    out[base + t] = v * inv_dt;
   }
-  __syncthreads();
-  if (t >= g.npnp) return;
-  double v = elem_deriv(g, s0, sD, e, t, 0) + elem_deriv(g, s1, sD, e, t, 1);
-  if (a2) v += zderiv(a2, k, base + t - static_cast<size_t>(k) * g.plane_size, g.plane_size, beta);
-  out[base + t] = v * inv_dt;
 }
 
 // io = alpha * io + b * d p / dx_dir  (dir 0, 1 element; 2 Fourier z; -1 none)
 __global__ void k_project(DevGeom g, double* __restrict__ io, const double* __restrict__ p, int dir,
                           double alpha, double b, double beta) {
   extern __shared__ double sm[];
-  double* sD = sm;
-  double* sp = sD + g.np * g.np;
-  const int e = blockIdx.x, k = blockIdx.y, t = threadIdx.x;
+  double* sp;
+  const int k = ep_setup(g, sm, 1, sp);
+  if (k < 0) return;
+  const int e = blockIdx.x, ln = threadIdx.x & 31;
   const size_t base = static_cast<size_t>(k) * g.plane_size + static_cast<size_t>(e) * g.npnp;
-  for (int q = t; q < g.np * g.np; q += blockDim.x) sD[q] = g.D[q];
-  if (t < g.npnp) sp[t] = p[base + t];
-  __syncthreads();
-  if (t >= g.npnp) return;
-  double v = alpha * io[base + t];
-  if (dir == 0 || dir == 1) v += b * elem_deriv(g, sp, sD, e, t, dir);
-  if (dir == 2) v += b * zderiv(p, k, base + t - static_cast<size_t>(k) * g.plane_size, g.plane_size, beta);
-  io[base + t] = v;
+  if (dir == 0 || dir == 1) {
+    ep_load(p + base, sp, g.npnp);
+    __syncwarp();
+  }
+  for (int t = ln; t < g.npnp; t += 32) {
+    double v = alpha * io[base + t];
+    if (dir == 0 || dir == 1) v += b * elem_deriv(g, sp, sm, e, t, dir);
+    if (dir == 2) v += b * zderiv(p, k, base + t - static_cast<size_t>(k) * g.plane_size, g.plane_size, beta);
+    io[base + t] = v;
+  }
 }
 
-inline int elem_threads(const DevGeom& g) {
-  const int t = (g.npnp + 31) / 32 * 32;
-  return t < 64 ? 64 : t;
+inline dim3 ep_grid(const DevGeom& g) { return dim3(g.nel, (g.nz + kEpPlanes - 1) / kEpPlanes); }
+// the warp-per-plane kernels hold up to 32 * kEpNodes nodes per element
+inline bool ep_fits(const DevGeom& g) { return g.npnp <= 32 * kEpNodes; }
+constexpr int kEpThreads = 32 * kEpPlanes;
+inline size_t ep_smem(const DevGeom& g, int fields) {
+  return sizeof(double) * (static_cast<size_t>(g.np) * g.np + static_cast<size_t>(kEpPlanes) * fields * g.npnp);
 }
 
 inline unsigned stream_blocks(size_t n) {
@@ -186,8 +244,8 @@ inline unsigned stream_blocks(size_t n) {
 }  // namespace
 
 cudaError_t dns_grad_xy(const DevGeom& g, const double* in, double* out, int dir, cudaStream_t st) {
-  const size_t shm = sizeof(double) * (g.np * g.np + g.npnp);
-  k_grad_xy<<<dim3(g.nel, g.nz), elem_threads(g), shm, st>>>(g, in, out, dir);
+  if (!ep_fits(g)) return cudaErrorInvalidValue;
+  k_grad_xy<<<ep_grid(g), kEpThreads, ep_smem(g, 1), st>>>(g, in, out, dir);
   return cudaGetLastError();
 }
 
@@ -204,8 +262,8 @@ cudaError_t dns_product(const DevGeom& g, const double* a, const double* b, doub
 }
 
 cudaError_t dns_nonlinear(const DevGeom& g, const NonlinearArgs& a, cudaStream_t st) {
-  const size_t shm = sizeof(double) * (g.np * g.np + 3 * g.npnp);
-  k_nonlinear<<<dim3(g.nel, g.nz), elem_threads(g), shm, st>>>(g, a);
+  if (!ep_fits(g)) return cudaErrorInvalidValue;
+  k_nonlinear<<<ep_grid(g), kEpThreads, ep_smem(g, 5), st>>>(g, a);
   return cudaGetLastError();
 }
 
@@ -213,9 +271,8 @@ cudaError_t dns_smooth(const DevGeom& g, const DevNumbering& N, double* io, doub
   const int gstride = (N.nglobal + 31) / 32 * 32;
   cudaError_t e = cudaMemsetAsync(work, 0, sizeof(double) * gstride * static_cast<size_t>(g.nz), st);
   if (e != cudaSuccess) return e;
-  const int th = (g.next + 31) / 32 * 32;
-  k_dss_accum<<<dim3(g.nel, g.nz), th, 0, st>>>(g, N, io, work, gstride);
-  k_dss_insert<<<dim3(g.nel, g.nz), th, 0, st>>>(g, N, io, work, gstride);
+  k_dss_accum<<<ep_grid(g), kEpThreads, 0, st>>>(g, N, io, work, gstride);
+  k_dss_insert<<<ep_grid(g), kEpThreads, 0, st>>>(g, N, io, work, gstride);
   return cudaGetLastError();
 }
 
@@ -231,15 +288,15 @@ cudaError_t dns_combine(const DevGeom& g, const CombineArgs& a, cudaStream_t st)
 
 cudaError_t dns_divergence(const DevGeom& g, const double* a0, const double* a1, const double* a2, double* out,
                            double dt, double beta, cudaStream_t st) {
-  const size_t shm = sizeof(double) * (g.np * g.np + 2 * g.npnp);
-  k_divergence<<<dim3(g.nel, g.nz), elem_threads(g), shm, st>>>(g, a0, a1, a2, out, 1.0 / dt, beta);
+  if (!ep_fits(g)) return cudaErrorInvalidValue;
+  k_divergence<<<ep_grid(g), kEpThreads, ep_smem(g, 2), st>>>(g, a0, a1, a2, out, 1.0 / dt, beta);
   return cudaGetLastError();
 }
 
 cudaError_t dns_project(const DevGeom& g, double* io, const double* p, int dir, double alpha, double b,
                         double beta, cudaStream_t st) {
-  const size_t shm = sizeof(double) * (g.np * g.np + g.npnp);
-  k_project<<<dim3(g.nel, g.nz), elem_threads(g), shm, st>>>(g, io, p, dir, alpha, b, beta);
+  if (!ep_fits(g)) return cudaErrorInvalidValue;
+  k_project<<<ep_grid(g), kEpThreads, ep_smem(g, 1), st>>>(g, io, p, dir, alpha, b, beta);
   return cudaGetLastError();
 }
 
