@@ -66,6 +66,16 @@ int stx_context_fields(const stx_context* ctx, char* buf, int len);
 int stx_token(const stx_context* ctx, const char* expr, double* value);
 /* NumberSys sizes for a field (src/numbersys.h:44-46). */
 int stx_numbering(const stx_context* ctx, char field, int* nglobal, int* nsolve, int* nband);
+/* The `enumerate` utility (utility/enumerate.cpp:110-199) without a GPU:
+ * reads the session and returns one field's numbering; nel and next =
+ * 4*(np-1) give the sizes; h_btog / h_bmask (nel*next ints each,
+ * boundary-major per element, or NULL) receive the
+ * global numbers and the essential mask (the `.num` file's contents,
+ * src/bcmgr.cpp:645-826).  Fields without essential nodes are numbered as
+ * `enumerate -O3` numbers them (their singular k=0 system pins the highest
+ * number); others by this library's reverse Cuthill--McKee. */
+int stx_numbering_host(const char* session_path, const char* overrides, char field, int* nel,
+                       int* next, int* nglobal, int* nsolve, int* nband, int* h_btog, int* h_bmask);
 /* Element node locations, host buffers of nel*np*np (Element::_xmesh). */
 int stx_mesh_coords(const stx_context* ctx, double* h_x, double* h_y);
 /* Number of geometry families (elements sharing condensed matrices). */

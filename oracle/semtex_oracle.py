@@ -21,11 +21,15 @@ CUDA library accelerates:
 The banded factorisation and solve call LAPACK dpbtrf/dpbtrs through scipy,
 the same routines the reference calls (src/matrix.cpp:252, src/field.cpp:693).
 
-Node numbering is this module's own (connectivity + reverse Cuthill--McKee).
-It differs from the reference `enumerate` output, which changes nothing but
-round-off, except for the singular k=0 pressure problem, whose pinned node
-(src/matrix.cpp:160-162) is the highest-numbered solve node: the pressure is
-then determined up to a constant that depends on the numbering.
+Node numbering is this module's own (connectivity + reverse Cuthill--McKee)
+where a field has essential nodes: it differs from the reference `enumerate`
+output only in round-off.  A field without essential nodes has a singular k=0
+system whose pinned node (src/matrix.cpp:160-162) is the highest-numbered
+solve node; where the discrete Neumann data are not compatible (high-order
+pressure BCs) the pin changes the whole solution, not only a constant.  Such
+fields take the reference's own `enumerate -O3` numbering (`reference_map`,
+`enumerate_o3`), which reproduces the regress goldens of the kovas sessions
+in every field.
 """
 
 from __future__ import annotations
@@ -445,6 +449,11 @@ class Numbering:
         newid[order] = np.arange(nsolve)
         newid[ess_nodes] = nsolve + np.arange(len(ess_nodes))
         self.btog = newid[gid]
+        if rcm and not len(ess_nodes):
+            # no essential nodes: the k=0 system of this field is singular and
+            # its pinned node (the highest number) decides the solution, so
+            # the reference's own numbering is used
+            self.btog = enumerate_o3(reference_map(M))
         self.bmask = ess[gid].astype(int)
         self.emask = self.bmask.any(axis=1).astype(int)
         self.nglobal, self.nsolve = nglobal, nsolve
@@ -459,6 +468,154 @@ class Numbering:
         for e in range(nel):
             np.add.at(mass, self.btog[e], M.Q4[e].ravel()[em[:next_]])
         self.imass = 1.0 / mass
+
+
+def _choose_node(per, n1, n2):
+    """Mesh::chooseNode (src/mesh.cpp:479-531): periodic representative of a
+    vertex pair, the lower node id among the alternatives (fixPeriodic,
+    :538-554, changes nothing)."""
+    p1, p2 = per[n1], per[n2]
+    if p1 is None:
+        if p2 is None:
+            pn = min(n1, n2)
+            per[n1] = per[n2] = pn
+        elif p2 != n2:
+            pn = n1 if n1 < p2 else p2
+            per[n1] = per[n2] = pn
+            per[p2] = pn
+        else:
+            pn = min(n1, n2)
+            per[n1] = per[n2] = pn
+    elif p1 != n1:
+        if p2 is None:
+            pn = p1 if p1 < n2 else n2
+            per[n2] = per[n1] = pn
+            per[p1] = pn
+        elif p2 != n2:
+            pn = p1 if p1 < p2 else p2
+            per[n1] = per[n2] = pn
+            per[p1] = pn
+            per[p2] = pn
+        else:
+            pn = p1 if p1 < n2 else n2
+            per[n2] = per[n1] = pn
+            per[p1] = pn
+    else:
+        if p2 is None:
+            pn = min(n1, n2)
+            per[n1] = per[n2] = pn
+        elif p2 != n2:
+            pn = n1 if n1 < p2 else n2
+            per[n2] = per[n1] = pn
+            per[p1] = pn
+        else:
+            pn = min(n1, n2)
+            per[n1] = per[n2] = pn
+
+
+def reference_map(M: "Mesh"):
+    """Mesh::buildMap (src/mesh.cpp:884-990, Side::connect :994-1030): the
+    reference's initial global numbers of element-boundary nodes, [nel, next]
+    in boundary-major order (side s, knot t at s*(np-1) + t)."""
+    S, n, nel = M.S, M.np, M.nel
+    nm, ni = n - 1, n - 2
+    per = [None] * len(S.nodes)
+    for (e, s, kind, val) in S.surfaces:
+        if kind == "P":
+            me, ms = val
+            _choose_node(per, S.elements[e][s], S.elements[me][(ms + 1) % 4])
+            _choose_node(per, S.elements[e][(s + 1) % 4], S.elements[me][ms])
+    vg = [-1] * len(S.nodes)
+    sg = {}
+    nxt = 0
+
+    def vertex(v):
+        nonlocal nxt
+        p = per[v]
+        if p is not None:
+            if vg[p] < 0:
+                vg[p] = nxt
+                nxt += 1
+            if vg[v] < 0:
+                vg[v] = vg[p]
+        if vg[v] < 0:
+            vg[v] = nxt
+            nxt += 1
+
+    for e in range(nel):
+        for s in range(4):
+            vertex(S.elements[e][s])
+            if ni:
+                m = M.mate.get((e, s))
+                if m is not None and m in sg:
+                    sg[(e, s)] = sg[m][::-1]
+                else:
+                    sg[(e, s)] = list(range(nxt, nxt + ni))
+                    nxt += ni
+            vertex(S.elements[e][(s + 1) % 4])
+    out = np.empty((nel, 4 * nm), int)
+    for e in range(nel):
+        for s in range(4):
+            out[e, s * nm] = vg[S.elements[e][s]]
+            out[e, s * nm + 1: s * nm + nm] = sg.get((e, s), [])
+    return out
+
+
+def _sparspak_rcm(root, adj, deg):
+    """RCM of the component of root (George & Liu, SPARSPAK RCM/DEGREE as in
+    femlib/netlib.f:1678-1890): breadth-first levels, each node's new
+    neighbours in adjacency order, stably sorted by degree; reversed."""
+    mask = np.ones(len(adj), bool)
+    mask[root] = False
+    perm = [root]
+    lvlend = 0
+    while True:
+        lbegin, lvlend = lvlend, len(perm)
+        for i in range(lbegin, lvlend):
+            fnbr = len(perm)
+            for nb in adj[perm[i]]:
+                if mask[nb]:
+                    mask[nb] = False
+                    perm.append(nb)
+            if len(perm) - fnbr > 1:
+                perm[fnbr:] = sorted(perm[fnbr:], key=lambda v: deg[v])
+        if len(perm) <= lvlend:
+            break
+    return perm[::-1]
+
+
+def enumerate_o3(bmap):
+    """`enumerate -O3` of a field without essential nodes (utility/
+    enumerate.cpp:694-831, connectivSC :883-920, globalBandwidth :923-964):
+    every node in turn as the RCM root, the first with the least global
+    bandwidth kept.  bmap [nel, next] holds Mesh::buildMap numbers; returns
+    the renumbered map (the chosen root becomes the highest number)."""
+    nel, nxt = bmap.shape
+    nsolve = int(bmap.max()) + 1
+    adj = [[] for _ in range(nsolve)]
+    for e in range(nel):
+        row = [int(v) for v in bmap[e]]
+        for i in range(nxt):
+            a = adj[row[i]]
+            for j in range(nxt):
+                if i != j and row[j] not in a:
+                    a.append(row[j])
+    deg = [len(a) for a in adj]
+    lo_hi = [(sorted(set(int(v) for v in bmap[e]))) for e in range(nel)]
+    best, best_root = None, 0
+    for root in range(nsolve):
+        perm = _sparspak_rcm(root, adj, deg)
+        if len(perm) != nsolve:
+            raise ValueError("numbering graph is not connected")
+        inv = np.empty(nsolve, int)
+        inv[perm] = np.arange(nsolve)
+        bw = max(int(inv[g].max() - inv[g].min()) for g in lo_hi) + 1
+        if best is None or bw < best:
+            best, best_root = bw, root
+    perm = _sparspak_rcm(best_root, adj, deg)
+    inv = np.empty(nsolve, int)
+    inv[perm] = np.arange(nsolve)
+    return inv[bmap]
 
 
 # ---------------------------------------------------------------------------
@@ -553,7 +710,7 @@ class BoundarySystem:
         """Natural::sum (src/condition.cpp:192-219): <h, w> into tgt."""
         nm = self.M.np - 1
         for b, (e, s, kind, _) in enumerate(self.edges):
-            if kind == "N":
+            if kind in ("N", "H"):   # NaturalCBCp::sum (src/condition.cpp:470-495) is the same sum
                 g = [self.N.btog[e, (s * nm + t) % (4 * nm)] for t in range(nm + 1)]
                 np.add.at(tgt, g, line[b] * self.area[b])
 
@@ -970,8 +1127,6 @@ class DNS:
         self.nu = tok["KINVIS"]
         self.vel = S.fields[:self.ncom]
         self.pname = S.fields[self.ncom]
-        if any(kind == "H" for g in S.bcs.values() for (kind, _) in g.values()):
-            raise NotImplementedError("high-order pressure BCs are not in the oracle")
         shape = (P.nz, P.nel, P.np, P.np)
         self.u = {}
         for c in S.fields:
@@ -992,6 +1147,103 @@ class DNS:
         lam = SS_COEFF[self.nord][0] / (self.dt * self.nu)
         self.vsys = {c: P.modal_systems(c, lam, "DIRECT", self.cache) for c in self.vel}
         self.psys = P.modal_systems(self.pname, 0.0, "DIRECT", self.cache)
+        self._hopbc_setup()
+
+    # -- High-order pressure BCs (BCmgr::buildComputedBCs / maintainFourier /
+    #    evaluateCNBCp, src/bcmgr.cpp:937-996, 1036-1296, 1299-1331;
+    #    Edge::curlCurl, src/edge.cpp:110-256).
+    def _hopbc_setup(self):
+        P, M = self.P, self.P.M
+        B = P.B[self.pname]
+        self.hedges = [b for b, (_, _, kind, _) in enumerate(B.edges) if kind == "H"]
+        nedge = len(B.edges)
+        self.eidx, self.nx, self.ny = [], np.zeros((nedge, P.np)), np.zeros((nedge, P.np))
+        for b, (e, s, _, _) in enumerate(B.edges):
+            idx = M.side_nodes(s)
+            self.eidx.append((e, idx))
+            # Element::sideGeom (src/element.cpp:1625-1747): outward normal
+            # from the mapping partials at the side's nodes, normalised
+            sgn, (a, c) = {0: (-1, ("dsdx", "dsdy")), 1: (1, ("drdx", "drdy")),
+                           2: (1, ("dsdx", "dsdy")), 3: (-1, ("drdx", "drdy"))}[s]
+            nx = sgn * getattr(M, a)[e].ravel()[idx]
+            ny = sgn * getattr(M, c)[e].ravel()[idx]
+            ln = np.hypot(nx, ny)
+            self.nx[b], self.ny[b] = nx / ln, ny / ln
+        shape = (P.nz, nedge, P.np)
+        self.un = [np.zeros(shape) for _ in range(self.nord)]
+        self.hop = [np.zeros(shape) for _ in range(self.nord)]
+
+    def _edges(self, f):
+        """Values of plane data f [nel, np, np] along every boundary edge."""
+        return np.stack([f[e].ravel()[idx] for (e, idx) in self.eidx])
+
+    def _maintain_fourier(self, U, N):
+        """BCmgr::maintainFourier (src/bcmgr.cpp:1036-1296), the terms the
+        high-order pressure BC uses: -d(u.n)/dt, n.N and -nu n.curlcurl u."""
+        if not self.hedges:
+            return
+        P, M = self.P, self.P.M
+        nz = P.nz
+        Je = min(self.step - 1, self.nord)
+        invdt = 1.0 / self.dt
+        self.hop = [np.zeros_like(self.hop[0])] + self.hop[:-1]
+        h = self.hop[0]
+        un = np.zeros_like(h)
+        for k in range(nz):
+            if k == 1:
+                continue
+            un[k] = self._edges(U[0][k]) * self.nx + self._edges(U[1][k]) * self.ny
+            if Je:
+                a = SS_COEFF[Je]
+                w = a[0] * un[k]
+                for q in range(Je):
+                    w = w + a[q + 1] * self.un[q][k]
+                h[k] = -invdt * w
+            h[k] += self._edges(N[0][k]) * self.nx + self._edges(N[1][k]) * self.ny
+        self.un = [un] + self.un[:-1]
+        beta = P.S.tokens["BETA"]
+        nu = self.nu
+
+        def curl_terms(Ur, Vr):
+            w = grad(M, Vr, 0) - grad(M, Ur, 1)
+            return self._edges(grad(M, w, 1)), -self._edges(grad(M, w, 0))
+
+        xr, yr = curl_terms(U[0][0], U[1][0])
+        h[0] += -nu * xr * self.nx
+        h[0] += -nu * yr * self.ny
+        for m in range(1, nz // 2):
+            bk = m * beta
+            kr, ki = 2 * m, 2 * m + 1
+            xr, yr = curl_terms(U[0][kr], U[1][kr])
+            xi, yi = curl_terms(U[0][ki], U[1][ki])
+            xi = xi + bk * self._edges(grad(M, U[2][kr], 0))
+            yi = yi + bk * self._edges(grad(M, U[2][kr], 1))
+            xr = xr - bk * self._edges(grad(M, U[2][ki], 0))
+            yr = yr - bk * self._edges(grad(M, U[2][ki], 1))
+            xr = xr + bk * bk * self._edges(U[0][kr])
+            xi = xi + bk * bk * self._edges(U[0][ki])
+            yr = yr + bk * bk * self._edges(U[1][kr])
+            yi = yi + bk * bk * self._edges(U[1][ki])
+            h[kr] += -nu * xr * self.nx
+            h[ki] += -nu * xi * self.nx
+            h[kr] += -nu * yr * self.ny
+            h[ki] += -nu * yi * self.ny
+
+    def _hopbc_lines(self, lines):
+        """BCmgr::evaluateCNBCp (src/bcmgr.cpp:1299-1331): extrapolated
+        dp/dn on the high-order pressure edges of the Fourier BC lines."""
+        if not self.hedges:
+            return lines
+        Je = min(self.step, self.nord)
+        b = EX_COEFF[Je]
+        for k in range(self.P.nz):
+            for e in self.hedges:
+                v = np.zeros(self.P.np)
+                if k != 1:
+                    for q in range(Je):
+                        v = v + b[q] * self.hop[q][k, e]
+                lines[k, e] = v
+        return lines
 
     def nonlinear(self):
         """Cartesian nonlinear terms (dns/nonlinear.cpp): advection 0 skew-symmetric
@@ -1041,6 +1293,7 @@ class DNS:
             self.Uf[0] = N
             self.step += 1
             self.time += self.dt
+            self._maintain_fourier(U, N)
             # -- waveProp (dns/integrate.cpp:204-239)
             Je = min(self.step, self.nord)
             alpha = SS_COEFF[Je]
@@ -1060,7 +1313,7 @@ class DNS:
             div /= self.dt
             pc = self.pname
             self.u[pc] = P.solve(pc, div, self.u[pc], self.psys,
-                                 P.bc_lines(pc, self.time), tok["TOL_REL"])
+                                 self._hopbc_lines(P.bc_lines(pc, self.time)), tok["TOL_REL"])
             # -- project (dns/integrate.cpp:260-289)
             a = -1.0 / (self.dt * self.nu)
             b = 1.0 / self.nu

@@ -226,6 +226,24 @@ class ModalMatrixSys:
         return out
 
 
+def numbering(session: str, field: str, overrides=None):
+    """The `enumerate` utility (utility/enumerate.cpp:110-199) on the host, no
+    GPU needed: one field's global numbering as a dict of nglobal, nsolve,
+    nband and the per-element boundary-major arrays btog / bmask."""
+    if isinstance(overrides, dict):
+        overrides = ";".join(f"{k}={v}" for k, v in overrides.items())
+    ov = overrides.encode() if overrides else None
+    v = [C.c_int() for _ in range(5)]
+    check(lib().stx_numbering_host(session.encode(), ov, field.encode(), *[C.byref(x) for x in v],
+                                   None, None))
+    nel, next_, nglobal, nsolve, nband = (x.value for x in v)
+    btog = np.zeros((nel, next_), np.int32)
+    bmask = np.zeros((nel, next_), np.int32)
+    check(lib().stx_numbering_host(session.encode(), ov, field.encode(), None, None, None, None, None,
+                                   C.c_void_p(btog.ctypes.data), C.c_void_p(bmask.ctypes.data)))
+    return {"nglobal": nglobal, "nsolve": nsolve, "nband": nband, "btog": btog, "bmask": bmask}
+
+
 def _user_value(session: str, key: str):
     txt = open(session).read()
     import re

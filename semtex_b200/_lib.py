@@ -33,6 +33,7 @@ SIGNATURES = {
     "stx_context_fields": (_i, [_p, _s, _i]),
     "stx_token": (_i, [_p, _s, _pd]),
     "stx_numbering": (_i, [_p, C.c_char, _pi, _pi, _pi]),
+    "stx_numbering_host": (_i, [_s, _s, C.c_char, _pi, _pi, _pi, _pi, _pi, _p, _p]),
     "stx_mesh_coords": (_i, [_p, _p, _p]),
     "stx_mesh_families": (_i, [_p, _pi]),
     "stx_field_evaluate": (_i, [_p, _s, _d, _p]),

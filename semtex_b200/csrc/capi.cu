@@ -255,7 +255,7 @@ int stx_context_create(const char* session_path, const char* overrides, int devi
           gid.push_back(N.btog[E.elmt * M.next + (E.side * (M.np - 1) + t) % M.next]);
           area.push_back(E.area[t]);
         }
-        kind.push_back(E.kind);
+        kind.push_back(E.kind == 'H' ? 'N' : E.kind);  // NaturalCBCp::sum is Natural::sum (src/condition.cpp:470-495)
       }
       d.edge_gid = upload(A, gid);
       d.edge_kind = upload(A, kind);
@@ -322,6 +322,24 @@ int stx_numbering(const stx_context* ctx, char field, int* nglobal, int* nsolve,
   });
 }
 
+int stx_numbering_host(const char* session_path, const char* overrides, char field, int* nel, int* next,
+                       int* nglobal, int* nsolve, int* nband, int* h_btog, int* h_bmask) {
+  return guarded([&] {
+    if (!session_path) throw StxError(STX_EINVAL, "null argument");
+    const Session S = read_session(session_path, overrides ? overrides : "");
+    if (S.fields.find(field) == std::string::npos) throw StxError(STX_EINVAL, std::string("no field ") + field);
+    const Mesh M = build_mesh(S);
+    const Numbering N = build_numbering(S, M, field);
+    if (nel) *nel = M.nel;
+    if (next) *next = M.next;
+    if (nglobal) *nglobal = N.nglobal;
+    if (nsolve) *nsolve = N.nsolve;
+    if (nband) *nband = N.nband;
+    if (h_btog) std::memcpy(h_btog, N.btog.data(), sizeof(int) * N.btog.size());
+    if (h_bmask) std::memcpy(h_bmask, N.bmask.data(), sizeof(int) * N.bmask.size());
+  });
+}
+
 int stx_mesh_coords(const stx_context* ctx, double* h_x, double* h_y) {
   return guarded([&] {
     if (!ctx) throw StxError(STX_EINVAL, "null context");
@@ -375,7 +393,9 @@ int stx_field_bc_evaluate(stx_context* ctx, char field, double t) {
         for (int q = 0; q < np; ++q) {
           vars["x"] = E.x[q];
           vars["y"] = E.y[q];
-          line[static_cast<size_t>(k) * F.nline + b * np + q] = ctx->S.tokens.eval(E.expr, &vars);
+          // high-order pressure values are computed on the device each step
+          line[static_cast<size_t>(k) * F.nline + b * np + q] =
+              E.kind == 'H' ? 0.0 : ctx->S.tokens.eval(E.expr, &vars);
         }
       }
     }

@@ -4,7 +4,9 @@
 // multi-level storage Us / Uf rolled by pointer (rollm, src/sem.h:108-122),
 // the same sub-steps in the same order, every field operation a device
 // kernel.  Cartesian coordinates; no body forcing; velocity BCs essential or
-// natural (time-dependent values re-evaluated each step).
+// natural (time-dependent values re-evaluated each step); pressure BCs
+// essential, natural or high-order (<H>, BCmgr::maintainFourier /
+// evaluateCNBCp, src/bcmgr.cpp:1036-1331, computed on the device each step).
 #include <cuda_runtime.h>
 
 #include <algorithm>
@@ -89,6 +91,17 @@ struct stx_dns {
   std::map<std::pair<char, int>, stx_modal*> pcg;  // temporary JACPCG systems
   std::vector<char> tdep;                 // per field: BCs depend on t
   std::vector<int> last_iters;
+  // High-order pressure BCs: edge tables and the multi-level storage of u.n
+  // and of the BC terms (BCmgr::_un / _hopbc), levels newest first and
+  // rolled by pointer like rollv (src/sem.h:98-106).
+  int nh = 0;
+  const int* h_elmt = nullptr;
+  const int* h_side = nullptr;
+  const int* h_line = nullptr;
+  const double* h_nx = nullptr;
+  const double* h_ny = nullptr;
+  std::vector<double*> un_lvl, hop_lvl;
+  size_t hsize = 0;  // doubles per level
 };
 
 namespace {
@@ -153,6 +166,12 @@ void nonlinear(stx_dns* d) {
   if (d->form == 1) d->toggle = 1 - d->toggle;
 }
 
+// rollv (src/sem.h:98-106): the last level moves to the front.
+void rollm_levels(std::vector<double*>& v) {
+  if (v.size() < 2) return;
+  std::rotate(v.rbegin(), v.rbegin() + 1, v.rend());
+}
+
 template <class T>
 void rollm(std::vector<std::vector<T>>& u) {
   if (u.size() < 2) return;
@@ -169,6 +188,42 @@ void solve(stx_dns* d, int idx, double* forcing, stx_modal* sys) {
   if (sys->method == STX_JACPCG) d->last_iters = it;
 }
 
+// BCmgr::maintainFourier + Pressure->evaluateBoundaries (dns/integrate.cpp:
+// 153-156) for the high-order pressure edges, from Us[0] and Uf[0].
+void hopbc(stx_dns* d) {
+  stx_context* ctx = d->ctx;
+  const int Je = std::min(d->step - 1, d->nord), Jx = std::min(d->step, d->nord);
+  rollm_levels(d->hop_lvl);
+  HopbcArgs a{};
+  a.U = d->Us[0][0];
+  a.V = d->Us[0][1];
+  a.W = d->ndim == 3 ? d->Us[0][2] : nullptr;
+  a.Nx = d->Uf[0][0];
+  a.Ny = d->Uf[0][1];
+  a.nh = d->nh;
+  a.elmt = d->h_elmt;
+  a.side = d->h_side;
+  a.line = d->h_line;
+  a.nx = d->h_nx;
+  a.ny = d->h_ny;
+  for (int q = 0; q < Je; ++q) a.un_old[q] = d->un_lvl[q];
+  a.un_new = d->un_lvl[d->nord - 1];
+  a.hop_new = d->hop_lvl[0];
+  for (int q = 0; q + 1 < Jx; ++q) a.hop_old[q] = d->hop_lvl[q + 1];
+  const FieldDev& P = ctx->fields.at(d->names[d->ncom]);
+  a.lines = P.d_lines;
+  a.nline = P.nline;
+  a.Je = Je;
+  for (int q = 0; q <= Je; ++q) a.alpha[q] = kSS[Je][q];
+  a.invdt = 1.0 / d->dt;
+  a.nu = d->nu;
+  a.beta = d->beta;
+  a.Jx = Jx;
+  for (int q = 0; q < Jx; ++q) a.ex[q] = kEX[Jx][q];
+  ck(dns_hopbc(ctx->dg, a, ctx->stream), "hopbc");
+  rollm_levels(d->un_lvl);
+}
+
 void advance_one(stx_dns* d) {
   stx_context* ctx = d->ctx;
   const DevGeom& g = ctx->dg;
@@ -176,6 +231,9 @@ void advance_one(stx_dns* d) {
   nonlinear(d);
   d->step += 1;
   d->time += d->dt;
+  const char pc = d->names[d->ncom];
+  if (d->tdep[d->ncom]) ckstx(stx_field_bc_evaluate(ctx, pc, d->time));
+  if (d->nh) hopbc(d);
   // -- waveProp (dns/integrate.cpp:204-239)
   const int Je = std::min(d->step, d->nord);
   for (int i = 0; i < d->ncom; ++i) {
@@ -196,8 +254,6 @@ void advance_one(stx_dns* d) {
   ck(dns_divergence(g, d->Us[0][0], d->Us[0][1], d->ndim == 3 ? d->Us[0][2] : nullptr, d->Uf[0][0], d->dt,
                     d->beta, st),
      "setPForce");
-  const char pc = d->names[d->ncom];
-  if (d->tdep[d->ncom]) ckstx(stx_field_bc_evaluate(ctx, pc, d->time));
   solve(d, d->ncom, d->Uf[0][0], d->psys);
   // -- project (dns/integrate.cpp:260-289)
   const double alpha = -1.0 / (d->dt * d->nu), bcoef = 1.0 / d->nu;
@@ -280,6 +336,43 @@ int stx_dns_create(stx_context* ctx, int advection, stx_dns** out) {
       for (const auto& E : ctx->fields.at(c).N.edges) td = td || depends_on_t(E.expr);
       d->tdep.push_back(td);
     }
+    // -- high-order pressure BC edges and storage (BCmgr::buildComputedBCs,
+    //    src/bcmgr.cpp:937-996)
+    {
+      const FieldDev& P = ctx->fields.at(d->names[d->ncom]);
+      std::vector<int> el, sd, ln;
+      std::vector<double> nx, ny;
+      for (size_t b = 0; b < P.N.edges.size(); ++b) {
+        const BoundaryEdge& E = P.N.edges[b];
+        if (E.kind != 'H') continue;
+        el.push_back(E.elmt);
+        sd.push_back(E.side);
+        ln.push_back(static_cast<int>(b));
+        nx.insert(nx.end(), E.nx.begin(), E.nx.end());
+        ny.insert(ny.end(), E.ny.begin(), E.ny.end());
+      }
+      d->nh = static_cast<int>(el.size());
+      if (d->nh) {
+        auto up = [&](const auto& v) {
+          using T = typename std::decay_t<decltype(v)>::value_type;
+          T* p = static_cast<T*>(d->arena.alloc(sizeof(T) * v.size()));
+          ck(cudaMemcpy(p, v.data(), sizeof(T) * v.size(), cudaMemcpyHostToDevice), "upload");
+          return p;
+        };
+        d->h_elmt = up(el);
+        d->h_side = up(sd);
+        d->h_line = up(ln);
+        d->h_nx = up(nx);
+        d->h_ny = up(ny);
+        d->hsize = static_cast<size_t>(g.nz) * d->nh * g.np;
+        double* hb = static_cast<double*>(d->arena.alloc(sizeof(double) * d->hsize * 2 * d->nord));
+        ck(cudaMemset(hb, 0, sizeof(double) * d->hsize * 2 * d->nord), "memset");
+        for (int q = 0; q < d->nord; ++q) {
+          d->un_lvl.push_back(hb + d->hsize * q);
+          d->hop_lvl.push_back(hb + d->hsize * (d->nord + q));
+        }
+      }
+    }
     // -- preSolve (dns/integrate.cpp:292-325)
     const double lam = kSS[d->nord][0] / (d->dt * d->nu);
     const int nmodes = (ctx->M.nz + 1) / 2;
@@ -314,6 +407,8 @@ int stx_dns_restart(stx_dns* d, double t0) {
         ck(cudaMemsetAsync(d->Us[q][i], 0, sizeof(double) * d->fsize, d->ctx->stream), "zero");
         ck(cudaMemsetAsync(d->Uf[q][i], 0, sizeof(double) * d->fsize, d->ctx->stream), "zero");
       }
+    for (double* p : d->un_lvl) ck(cudaMemsetAsync(p, 0, sizeof(double) * d->hsize, d->ctx->stream), "zero");
+    for (double* p : d->hop_lvl) ck(cudaMemsetAsync(p, 0, sizeof(double) * d->hsize, d->ctx->stream), "zero");
     d->step = 0;
     d->time = t0;
     for (char c : d->names) ckstx(stx_field_bc_evaluate(d->ctx, c, t0));

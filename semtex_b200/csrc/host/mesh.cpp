@@ -5,7 +5,10 @@
 #include <map>
 #include <numeric>
 #include <queue>
+#include <atomic>
+#include <limits>
 #include <stdexcept>
+#include <thread>
 
 namespace stx {
 
@@ -330,6 +333,227 @@ std::vector<int> rcm_order(std::vector<std::vector<int>>& nbr, int rcm_roots) {
   return order;
 }
 
+namespace {
+
+// Mesh::chooseNode (src/mesh.cpp:479-531): the periodic representative of a
+// vertex pair is the lower node id among the alternatives; per[v] = -1 when
+// unset.  (fixPeriodic, :538-554, changes nothing.)
+void choose_node(std::vector<int>& per, int n1, int n2) {
+  const int p1 = per[n1], p2 = per[n2];
+  int pn;
+  if (p1 < 0) {
+    if (p2 < 0) {
+      pn = std::min(n1, n2);
+      per[n1] = per[n2] = pn;
+    } else if (p2 != n2) {
+      pn = n1 < p2 ? n1 : p2;
+      per[n1] = per[n2] = pn;
+      per[p2] = pn;
+    } else {
+      pn = std::min(n1, n2);
+      per[n1] = per[n2] = pn;
+    }
+  } else if (p1 != n1) {
+    if (p2 < 0) {
+      pn = p1 < n2 ? p1 : n2;
+      per[n2] = per[n1] = pn;
+      per[p1] = pn;
+    } else if (p2 != n2) {
+      pn = p1 < p2 ? p1 : p2;
+      per[n1] = per[n2] = pn;
+      per[p1] = pn;
+      per[p2] = pn;
+    } else {
+      pn = p1 < n2 ? p1 : n2;
+      per[n2] = per[n1] = pn;
+      per[p1] = pn;
+    }
+  } else {
+    if (p2 < 0) {
+      pn = std::min(n1, n2);
+      per[n1] = per[n2] = pn;
+    } else if (p2 != n2) {
+      pn = n1 < p2 ? n1 : n2;
+      per[n2] = per[n1] = pn;
+      per[p1] = pn;
+    } else {
+      pn = std::min(n1, n2);
+      per[n1] = per[n2] = pn;
+    }
+  }
+}
+
+// One SPARSPAK RCM ordering (George & Liu; RCM and DEGREE as in
+// femlib/netlib.f:1678-1890) of a connected graph from `root`, in Cuthill--
+// McKee order (not yet reversed): breadth-first levels, each node's
+// unnumbered neighbours in adjacency order, stably sorted by degree.  While
+// numbering, the element spans (positions max - min over an element's
+// nodes) are tracked; the walk stops early, returning -1, once a span
+// exceeds `limit`.  Otherwise returns the largest span.
+int cm_walk(int root, const std::vector<int>& xadj, const std::vector<int>& adj, const std::vector<int>& deg,
+            const std::vector<int>& xel, const std::vector<int>& nel_of, int limit,
+            std::vector<int>& perm, std::vector<int>& pos, std::vector<int>& first) {
+  const int n = static_cast<int>(xadj.size()) - 1;
+  perm.clear();
+  std::fill(pos.begin(), pos.end(), -1);
+  std::fill(first.begin(), first.end(), -1);
+  int span = 0;
+  auto place = [&](int v) {
+    const int p = static_cast<int>(perm.size());
+    pos[v] = p;
+    perm.push_back(v);
+    for (int k = xel[v]; k < xel[v + 1]; ++k) {
+      const int e = nel_of[k];
+      if (first[e] < 0) first[e] = p;
+      span = std::max(span, p - first[e]);
+    }
+  };
+  place(root);
+  int lvlend = 0;
+  while (true) {
+    const int lbegin = lvlend;
+    lvlend = static_cast<int>(perm.size());
+    for (int i = lbegin; i < lvlend; ++i) {
+      const int node = perm[i];
+      const size_t fnbr = perm.size();
+      for (int k = xadj[node]; k < xadj[node + 1]; ++k) {
+        const int nb = adj[k];
+        if (pos[nb] < 0) {
+          pos[nb] = -2;  // taken; position assigned after the sort
+          perm.push_back(nb);
+        }
+      }
+      if (perm.size() - fnbr > 1)
+        std::stable_sort(perm.begin() + fnbr, perm.end(), [&](int a, int b) { return deg[a] < deg[b]; });
+      const std::vector<int> fresh(perm.begin() + fnbr, perm.end());
+      perm.resize(fnbr);
+      for (int v : fresh) place(v);
+      if (span > limit) return -1;
+    }
+    if (static_cast<int>(perm.size()) <= lvlend) break;
+  }
+  if (static_cast<int>(perm.size()) != n) throw std::runtime_error("numbering graph is not connected");
+  return span;
+}
+
+}  // namespace
+
+std::vector<int> reference_map(const Session& S, const Mesh& M) {
+  const int n = M.np, nel = M.nel, nm = n - 1, ni = n - 2, next = M.next;
+  std::vector<int> per(S.nodes.size(), -1);
+  for (const Surface& f : S.surfaces)
+    if (f.kind == 'P') {
+      choose_node(per, S.elements[f.elmt][f.side], S.elements[f.mate_elmt][(f.mate_side + 1) % 4]);
+      choose_node(per, S.elements[f.elmt][(f.side + 1) % 4], S.elements[f.mate_elmt][f.mate_side]);
+    }
+  std::vector<int> vg(S.nodes.size(), -1);
+  std::vector<std::vector<int>> sg(nel * 4);
+  int nxt = 0;
+  auto vertex = [&](int v) {
+    const int p = per[v];
+    if (p >= 0) {
+      if (vg[p] < 0) vg[p] = nxt++;
+      if (vg[v] < 0) vg[v] = vg[p];
+    }
+    if (vg[v] < 0) vg[v] = nxt++;
+  };
+  for (int e = 0; e < nel; ++e)
+    for (int s = 0; s < 4; ++s) {
+      vertex(S.elements[e][s]);
+      if (ni) {
+        const auto m = M.mate[e * 4 + s];
+        std::vector<int>& g = sg[e * 4 + s];
+        if (m[0] >= 0 && !sg[m[0] * 4 + m[1]].empty()) {
+          const std::vector<int>& o = sg[m[0] * 4 + m[1]];
+          g.assign(o.rbegin(), o.rend());
+        } else {
+          for (int t = 0; t < ni; ++t) g.push_back(nxt++);
+        }
+      }
+      vertex(S.elements[e][(s + 1) % 4]);
+    }
+  std::vector<int> map(nel * next);
+  for (int e = 0; e < nel; ++e)
+    for (int s = 0; s < 4; ++s) {
+      map[e * next + s * nm] = vg[S.elements[e][s]];
+      for (int t = 0; t < ni; ++t) map[e * next + s * nm + 1 + t] = sg[e * 4 + s][t];
+    }
+  return map;
+}
+
+std::vector<int> enumerate_o3(const std::vector<int>& bmap, int nel, int next) {
+  const int n = *std::max_element(bmap.begin(), bmap.end()) + 1;
+  // -- Nsys::buildAdjncy / connectivSC (utility/enumerate.cpp:832-920):
+  //    neighbours in order of first appearance, element by element
+  std::vector<std::vector<int>> lists(n);
+  for (int e = 0; e < nel; ++e) {
+    const int* row = &bmap[e * next];
+    for (int i = 0; i < next; ++i) {
+      std::vector<int>& a = lists[row[i]];
+      for (int j = 0; j < next; ++j)
+        if (i != j && std::find(a.begin(), a.end(), row[j]) == a.end()) a.push_back(row[j]);
+    }
+  }
+  std::vector<int> xadj(n + 1, 0), adj, deg(n);
+  for (int v = 0; v < n; ++v) {
+    deg[v] = static_cast<int>(lists[v].size());
+    xadj[v + 1] = xadj[v] + deg[v];
+    adj.insert(adj.end(), lists[v].begin(), lists[v].end());
+  }
+  // elements of each node (distinct), for the span bookkeeping
+  std::vector<int> xel(n + 1, 0), nel_of;
+  {
+    std::vector<std::vector<int>> els(n);
+    for (int e = 0; e < nel; ++e)
+      for (int i = 0; i < next; ++i) {
+        std::vector<int>& l = els[bmap[e * next + i]];
+        if (l.empty() || l.back() != e) l.push_back(e);
+      }
+    for (int v = 0; v < n; ++v) {
+      xel[v + 1] = xel[v] + static_cast<int>(els[v].size());
+      nel_of.insert(nel_of.end(), els[v].begin(), els[v].end());
+    }
+  }
+  // -- Nsys::renumber level 3 (utility/enumerate.cpp:694-831): every node
+  //    as the root, the first of least global bandwidth (max element span
+  //    + 1, globalBandwidth :923-964) wins.  Spans of reversed and forward
+  //    orders are equal.  Roots are shared among threads; a walk stops once
+  //    its span exceeds the best found so far (ties run to completion, so
+  //    the lowest root among equals is kept).
+  std::vector<int> span(n, -1);
+  std::atomic<int> best{std::numeric_limits<int>::max()};
+  std::atomic<int> next_root{0};
+  const int nthr = std::max(1, std::min(16, static_cast<int>(std::thread::hardware_concurrency())));
+  auto work = [&] {
+    std::vector<int> perm, pos(n), first(nel);
+    perm.reserve(n);
+    for (int r; (r = next_root.fetch_add(1)) < n;) {
+      const int sp = cm_walk(r, xadj, adj, deg, xel, nel_of, best.load(), perm, pos, first);
+      span[r] = sp;
+      if (sp >= 0) {
+        int b = best.load();
+        while (sp < b && !best.compare_exchange_weak(b, sp)) {
+        }
+      }
+    }
+  };
+  std::vector<std::thread> pool;
+  for (int t = 1; t < nthr; ++t) pool.emplace_back(work);
+  work();
+  for (auto& t : pool) t.join();
+  int root = -1;
+  for (int r = 0; r < n; ++r)
+    if (span[r] >= 0 && (root < 0 || span[r] < span[root])) root = r;
+  std::vector<int> perm, pos(n), first(nel);
+  cm_walk(root, xadj, adj, deg, xel, nel_of, std::numeric_limits<int>::max(), perm, pos, first);
+  // reversed: CM position p -> number n - 1 - p (the root gets n - 1)
+  std::vector<int> inv(n);
+  for (int p = 0; p < n; ++p) inv[perm[p]] = n - 1 - p;
+  std::vector<int> out(bmap.size());
+  for (size_t k = 0; k < bmap.size(); ++k) out[k] = inv[bmap[k]];
+  return out;
+}
+
 Numbering build_numbering(const Session& S, const Mesh& M, char field, int rcm_roots) {
   const int n = M.np, nel = M.nel, nm = n - 1, next = M.next;
   Numbering N;
@@ -398,6 +622,9 @@ Numbering build_numbering(const Session& S, const Mesh& M, char field, int rcm_r
       const BCSpec& bc = bi->second;
       if (bc.kind == 'D') {
         for (int t = 0; t <= nm; ++t) ess[gid[e * next + (s * nm + t) % next]] = 1;
+      } else if (bc.kind == 'H') {
+        if (field != 'p')
+          throw std::runtime_error(std::string("high-order BC <H> given for field ") + field + ", not pressure");
       } else if (bc.kind != 'N') {
         throw std::runtime_error(std::string("boundary condition kind <") + bc.kind +
                                  "> is not supported");
@@ -414,6 +641,23 @@ Numbering build_numbering(const Session& S, const Mesh& M, char field, int rcm_r
       for (int t = 0; t < n; ++t) {
         E.x[t] = M.x[e * M.npnp + idx[t]];
         E.y[t] = M.y[e * M.npnp + idx[t]];
+      }
+      // unit outward normal from the mapping partials at the side's nodes
+      // (Element::sideGeom, src/element.cpp:1625-1747)
+      E.nx.resize(n);
+      E.ny.resize(n);
+      for (int t = 0; t < n; ++t) {
+        const int k = e * M.npnp + idx[t];
+        double ax, ay;
+        switch (s) {
+          case 0: ax = -M.dsdx[k]; ay = -M.dsdy[k]; break;
+          case 1: ax = M.drdx[k]; ay = M.drdy[k]; break;
+          case 2: ax = M.dsdx[k]; ay = M.dsdy[k]; break;
+          default: ax = -M.drdx[k]; ay = -M.drdy[k]; break;
+        }
+        const double len = std::hypot(ax, ay);
+        E.nx[t] = ax / len;
+        E.ny[t] = ay / len;
       }
       const double L = std::hypot(E.x[n - 1] - E.x[0], E.y[n - 1] - E.y[0]);
       E.area.resize(n);
@@ -459,6 +703,13 @@ Numbering build_numbering(const Session& S, const Mesh& M, char field, int rcm_r
     N.btog[k] = newid[gid[k]];
     N.bmask[k] = ess[gid[k]];
     if (N.bmask[k]) N.emask[k / next] = 1;
+  }
+  if (ns == nglobal && ns > 1) {
+    // No essential nodes: the k=0 system is singular and its pinned node, the
+    // highest number, decides the solution (with high-order pressure BCs
+    // the discrete Neumann data are not compatible, so more than a constant).
+    // Such fields take the reference's own `enumerate -O3` numbering.
+    N.btog = enumerate_o3(reference_map(S, M), nel, next);
   }
   int bw = 0;
   for (int e = 0; e < nel; ++e) {

@@ -7,7 +7,9 @@
 // femlib/mapping.c:46-132.  Numbering plays the role of the `.num`
 // NumberSys (src/numbersys.h, src/bcmgr.cpp:586-826): btog, bmask, emask,
 // nglobal / nsolve / nband and the inverse boundary mass (imass).  The
-// ordering is this library's own reverse Cuthill--McKee.
+// ordering is this library's own reverse Cuthill--McKee, except for fields
+// without essential nodes, which take the reference's `enumerate -O3`
+// numbering (their singular k=0 system pins the highest-numbered node).
 #pragma once
 
 #include <array>
@@ -46,10 +48,11 @@ Mesh build_mesh(const Session& S);
 
 struct BoundaryEdge {
   int elmt = 0, side = 0;
-  char kind = 0;              // 'D' or 'N' (others rejected)
+  char kind = 0;              // 'D', 'N' or 'H' (pressure only; others rejected)
   std::string expr;
   std::vector<double> area;   // np quadrature-weighted side lengths
   std::vector<double> x, y;   // np node locations along the side
+  std::vector<double> nx, ny; // np unit outward normal components
 };
 
 struct Numbering {
@@ -63,6 +66,17 @@ struct Numbering {
     return nglobal == o.nglobal && nsolve == o.nsolve && btog == o.btog;
   }
 };
+
+// Mesh::buildMap (src/mesh.cpp:884-1030): the reference's initial global
+// numbers of element-boundary nodes, [nel*next] in boundary-major order,
+// with periodic vertices identified as Mesh::chooseNode does.
+std::vector<int> reference_map(const Session& S, const Mesh& M);
+
+// `enumerate -O3` (utility/enumerate.cpp:694-964) of a numbering without
+// essential nodes: each node in turn as the SPARSPAK RCM root, the first of
+// least global bandwidth kept; returns the renumbered map (the chosen root
+// gets the highest number).
+std::vector<int> enumerate_o3(const std::vector<int>& bmap, int nel, int next);
 
 // Reverse Cuthill--McKee order of a graph given as adjacency lists (sorted
 // and deduplicated in place); the best of rcm_roots trial roots by bandwidth.

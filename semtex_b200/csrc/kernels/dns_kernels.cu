@@ -7,6 +7,8 @@
 //   DSS smoothing         Field::smooth        src/field.cpp:282-327
 //   waveProp              dns/integrate.cpp:204-239
 //   setPForce, project    dns/integrate.cpp:242-289
+//   high-order pressure   BCmgr::maintainFourier / evaluateCNBCp
+//   BCs                   src/bcmgr.cpp:1036-1331, src/edge.cpp:110-256
 //
 // Element kernels run one warp per (element, plane), kEpPlanes planes of one
 // element per block: D is staged once per block, each warp holds its plane's
@@ -81,6 +83,89 @@ __global__ void k_grad_xy(DevGeom g, const double* __restrict__ in, double* __re
   ep_load(in + base, su, g.npnp);
   __syncwarp();
   for (int t = ln; t < g.npnp; t += 32) out[base + t] = elem_deriv(g, su, sm, e, t, dir);
+}
+
+// One block per (high-order edge h, Fourier mode m): planes 0 (m = 0) or
+// 2m, 2m+1.  The element's U, V (W) planes and the vorticity dV/dx - dU/dy
+// are staged in shared memory; one thread per (plane, edge knot) forms
+//   curl curl u . n   (x = dw/dy, y = -dw/dx, plus the beta k terms of W and
+//                      beta^2 k^2 U, V in 3D, Edge::curlCurl),
+//   -d(u.n)/dt        (stiffly stable difference of the stored u.n),
+//   n . N,
+// the new level  hop = -d(u.n)/dt + n.N - nu curlcurl(u).n  and the
+// extrapolated pressure BC value  sum_q ex[q] hop_q.  The Nyquist plane is
+// never touched (its lines stay zero).
+__global__ void k_hopbc(DevGeom g, HopbcArgs a) {
+  extern __shared__ double sm[];
+  const int np = g.np, nn = g.npnp;
+  const int h = blockIdx.x, m = blockIdx.y;
+  const int e = a.elmt[h], side = a.side[h];
+  const int nplane = m ? 2 : 1;
+  const bool z3 = a.W != nullptr && m > 0;
+  double* sD = sm;
+  double* f = sm + np * np;  // plane p: U at f + 4 nn p, V +nn, W +2nn, vorticity +3nn
+  for (int q = threadIdx.x; q < np * np; q += blockDim.x) sD[q] = g.D[q];
+  for (int q = threadIdx.x; q < nplane * nn; q += blockDim.x) {
+    const int p = q / nn, t = q - p * nn;
+    const int k = m ? 2 * m + p : 0;
+    const size_t x = static_cast<size_t>(k) * g.plane_size + static_cast<size_t>(e) * nn + t;
+    double* fp = f + 4 * nn * p;
+    fp[t] = a.U[x];
+    fp[nn + t] = a.V[x];
+    if (z3) fp[2 * nn + t] = a.W[x];
+  }
+  __syncthreads();
+  for (int q = threadIdx.x; q < nplane * nn; q += blockDim.x) {
+    const int p = q / nn, t = q - p * nn;
+    double* fp = f + 4 * nn * p;
+    fp[3 * nn + t] = elem_deriv(g, fp + nn, sD, e, t, 0) - elem_deriv(g, fp, sD, e, t, 1);
+  }
+  __syncthreads();
+  if (threadIdx.x >= nplane * np) return;
+  const int p = threadIdx.x / np, r = threadIdx.x - p * np;
+  int i, j;  // knot r of the side in CCW traverse (row i = s, column j = r)
+  switch (side) {
+    case 0: i = 0; j = r; break;
+    case 1: i = r; j = np - 1; break;
+    case 2: i = np - 1; j = np - 1 - r; break;
+    default: i = np - 1 - r; j = 0; break;
+  }
+  const int t = i * np + j;
+  const double* fp = f + 4 * nn * p;
+  double cx = elem_deriv(g, fp + 3 * nn, sD, e, t, 1);
+  double cy = -elem_deriv(g, fp + 3 * nn, sD, e, t, 0);
+  if (z3) {
+    const double bk = m * a.beta;
+    const double* Wo = f + 4 * nn * (1 - p) + 2 * nn;  // W of the other plane of the mode
+    if (p == 0) {  // real part: -beta k d(W_im)
+      cx -= bk * elem_deriv(g, Wo, sD, e, t, 0);
+      cy -= bk * elem_deriv(g, Wo, sD, e, t, 1);
+    } else {       // imaginary part: +beta k d(W_re)
+      cx += bk * elem_deriv(g, Wo, sD, e, t, 0);
+      cy += bk * elem_deriv(g, Wo, sD, e, t, 1);
+    }
+    cx += bk * bk * fp[t];
+    cy += bk * bk * fp[nn + t];
+  }
+  const int k = m ? 2 * m + p : 0;
+  const double nxv = a.nx[h * np + r], nyv = a.ny[h * np + r];
+  const size_t pos = static_cast<size_t>(k) * a.nh * np + static_cast<size_t>(h) * np + r;
+  const double un = fp[t] * nxv + fp[nn + t] * nyv;
+  double hv = 0.0;
+  if (a.Je) {
+    double w = a.alpha[0] * un;
+    for (int q = 0; q < a.Je; ++q) w += a.alpha[q + 1] * a.un_old[q][pos];
+    hv = -a.invdt * w;
+  }
+  const size_t x = static_cast<size_t>(k) * g.plane_size + static_cast<size_t>(e) * nn + t;
+  hv += a.Nx[x] * nxv + a.Ny[x] * nyv;
+  hv += -a.nu * cx * nxv;
+  hv += -a.nu * cy * nyv;
+  a.un_new[pos] = un;
+  a.hop_new[pos] = hv;
+  double v = a.ex[0] * hv;
+  for (int q = 0; q + 1 < a.Jx; ++q) v += a.ex[q + 1] * a.hop_old[q][pos];
+  a.lines[static_cast<size_t>(k) * a.nline + static_cast<size_t>(a.line[h]) * np + r] = v;
 }
 
 __global__ void k_grad_z(const double* __restrict__ in, double* __restrict__ out, int nz, int plane_size,
@@ -278,6 +363,16 @@ cudaError_t dns_smooth(const DevGeom& g, const DevNumbering& N, double* io, doub
 
 size_t dns_smooth_workspace_doubles(const DevGeom& g, const DevNumbering& N) {
   return static_cast<size_t>((N.nglobal + 31) / 32 * 32) * g.nz;
+}
+
+size_t dns_hopbc_smem(const DevGeom& g) { return sizeof(double) * (g.np * g.np + 8 * g.npnp); }
+
+cudaError_t dns_hopbc(const DevGeom& g, const HopbcArgs& a, cudaStream_t st) {
+  if (a.nh == 0) return cudaSuccess;
+  if (2 * g.np > 128 || a.Je < 0 || a.Je > 3 || a.Jx < 1 || a.Jx > 3) return cudaErrorInvalidValue;
+  const dim3 grid(a.nh, g.nz > 1 ? g.nz / 2 : 1);
+  k_hopbc<<<grid, 128, dns_hopbc_smem(g), st>>>(g, a);
+  return cudaGetLastError();
 }
 
 cudaError_t dns_combine(const DevGeom& g, const CombineArgs& a, cudaStream_t st) {

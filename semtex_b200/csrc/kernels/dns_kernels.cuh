@@ -26,6 +26,39 @@ struct CombineArgs {
   double* out;
 };
 
+// High-order pressure BC terms of one step (BCmgr::maintainFourier,
+// src/bcmgr.cpp:1036-1296; Edge::curlCurl, src/edge.cpp:110-256) and their
+// extrapolation into the pressure BC lines (BCmgr::evaluateCNBCp,
+// :1299-1331).  Edge storage is [nz][nh*np], edge h at h*np, knots in the
+// CCW side traverse.
+struct HopbcArgs {
+  const double* U;            // Fourier velocity components (current level)
+  const double* V;
+  const double* W;            // null in 2D
+  const double* Nx;           // Fourier nonlinear terms of the same level
+  const double* Ny;
+  int nh;                     // high-order pressure edges
+  const int* elmt;            // [nh] element, side and BC line edge number
+  const int* side;
+  const int* line;
+  const double* nx;           // [nh*np] unit outward normal
+  const double* ny;
+  const double* un_old[3];    // u.n of the previous steps, newest first
+  double* un_new;             // u.n of this step (may be un_old[Je-1]: each entry is read first)
+  const double* hop_old[2];   // earlier pressure BC levels, newest first
+  double* hop_new;
+  double* lines;              // pressure BC lines [nz][nline]
+  int nline;
+  int Je;                     // time-derivative order (0: no -d(u.n)/dt term)
+  double alpha[4];            // stiffly stable coefficients of order Je
+  double invdt, nu, beta;
+  int Jx;                     // extrapolation order
+  double ex[3];               // extrapolation coefficients of order Jx
+};
+
+size_t dns_hopbc_smem(const DevGeom& g);
+cudaError_t dns_hopbc(const DevGeom& g, const HopbcArgs& a, cudaStream_t st);
+
 cudaError_t dns_grad_xy(const DevGeom& g, const double* in, double* out, int dir, cudaStream_t st);
 cudaError_t dns_grad_z(const DevGeom& g, const double* in, double* out, double beta, cudaStream_t st);
 cudaError_t dns_product(const DevGeom& g, const double* a, const double* b, double* out, cudaStream_t st);

@@ -1,10 +1,12 @@
 """GPU parity of the DNS step (dns/integrate.cpp) against the oracle, and
 against the reference's regression goldens (regress/*.ok) through the GPU path.
 
-Velocities: relative L2 <= 1e-10 vs the oracle.  Pressure: the k=0 pressure
-problem of a periodic domain is singular and pinned at the highest-numbered
-solve node (src/matrix.cpp:160-162); the two codes number nodes differently,
-so pressure is compared after removing its mean.
+Velocities: relative L2 <= 1e-10 vs the oracle.  Pressure: relative L2 <=
+1e-9; a pressure field without essential nodes has a singular k=0 problem
+pinned at its highest-numbered node (src/matrix.cpp:160-162), whose solution
+carries round-off amplified by that pinned system's condition number.  Both
+codes number such fields as the reference's `enumerate -O3` does, so they pin
+the same node and the pressures are compared as they are, constant included.
 """
 import json
 import os
@@ -26,15 +28,25 @@ def rel_l2(a, b):
     return np.linalg.norm(a - b) / max(np.linalg.norm(b), 1e-300)
 
 
-def _compare(path, gpu, D, tol=1e-10):
+def _compare(path, gpu, D, tol=1e-10, ptol=1e-9):
     phys = D.physical()
     scale = max(np.linalg.norm(phys[c]) for c in D.vel)   # components may be identically zero
     for c in D.vel:
         err = np.linalg.norm(gpu[c] - phys[c]) / scale
         assert err < tol, (c, err)
     pc = D.pname
-    pg, po = gpu[pc], D.physical()[pc]
-    assert rel_l2(pg - pg.mean(), po - po.mean()) < 1e-9
+    assert rel_l2(gpu[pc], phys[pc]) < ptol, (pc, rel_l2(gpu[pc], phys[pc]))
+
+
+def _goldens(name, gpu, t, D, fields):
+    """The reference's own regression numbers (`compare -n`), from GPU fields."""
+    funcs = O.user_functions(D.P.S)
+    tt = float(f"{t:.6g}")
+    for c in fields:
+        ex = D.P.evaluate(funcs[c], tt)
+        err = np.abs(ex - gpu[c]).max()
+        got = "noise-level" if err < 1e-12 else f"{err:.4e}"
+        assert got == GOLD[name][c], (name, c, got)
 
 
 @pytest.mark.parametrize("name", ["taylor2", "taylor3", "taylor4", "taylor5"])
@@ -43,14 +55,17 @@ def test_regress_sessions_gpu(name):
     gpu, t = S.dns(path)
     D = O.dns_session(path)
     _compare(path, gpu, D)
-    # the reference's own regression numbers, from the GPU fields
-    funcs = O.user_functions(D.P.S)
-    tt = float(f"{t:.6g}")
-    for c in D.vel:
-        ex = D.P.evaluate(funcs[c], tt)
-        err = np.abs(ex - gpu[c]).max()
-        got = "noise-level" if err < 1e-12 else f"{err:.4e}"
-        assert got == GOLD[name][c], (name, c, got)
+    _goldens(name, gpu, t, D, D.vel + D.pname)
+
+
+@pytest.mark.parametrize("name", ["kovas1", "kovas2", "kovas3", "kovas4", "kovas5"])
+def test_high_order_pressure_bc_sessions_gpu(name):
+    """Kovasznay flow with high-order pressure BCs <H> (src/bcmgr.cpp:1036-1331)."""
+    path = os.path.join(SESSIONS, name)
+    gpu, t = S.dns(path)
+    D = O.dns_session(path)
+    _compare(path, gpu, D)
+    _goldens(name, gpu, t, D, D.vel + D.pname)
 
 
 @pytest.mark.parametrize("advection", [0, 1, 2, 3])
@@ -75,6 +90,27 @@ def test_dirichlet_channel_2d(tmp_path, ntime):
                               fields="uvp", periodic_x=True,
                               bcs={"w": {"u": "<D> 0", "v": "<D> 0", "p": "<D> 0"}},
                               user=["u = 1-y*y+0.1*sin(PI*x)*(1-y*y)", "v = 0.05*(1-y*y)", "p = 0"])
+    gpu, t = S.dns(p)
+    D = O.dns_session(p)
+    _compare(p, gpu, D)
+
+
+@pytest.mark.parametrize("nz,ntime", [(1, 2), (8, 3)])
+def test_channel_high_order_pressure_walls(tmp_path, nz, ntime):
+    # Periodic-in-x channel, Dirichlet velocity walls, high-order pressure
+    # walls (the BCs of the wall-bounded configurations); in 3D with z-varying
+    # initial data so that every Fourier term of curl curl u is exercised.
+    fields = "uvwp" if nz > 1 else "uvp"
+    bcs = {"u": "<D> 0", "v": "<D> 0", "p": "<H> 0"}
+    user = ["u = 1-y*y+0.1*sin(PI*x)*(1-y*y)", "v = 0.05*(1-y*y)*cos(PI*x)", "p = 0"]
+    if nz > 1:
+        bcs["w"] = "<D> 0"
+        user = ["u = 1-y*y+0.1*sin(PI*x)*(1-y*y)*cos(z)", "v = 0.05*(1-y*y)*sin(z)",
+                "w = 0.03*(1-y*y)*sin(PI*x)*cos(2*z)", "p = 0"]
+    p = sessions.rect_session(str(tmp_path / "chh"), 4, 3, x=(0.0, 2.0), y=(-1.0, 1.0),
+                              tokens={"N_P": 6, "N_Z": nz, "N_TIME": ntime, "D_T": 0.01, "KINVIS": 0.1,
+                                      "N_STEP": 6, "TOL_REL": 1e-14},
+                              fields=fields, periodic_x=True, bcs={"w": bcs}, user=user)
     gpu, t = S.dns(p)
     D = O.dns_session(p)
     _compare(p, gpu, D)

@@ -18,20 +18,47 @@ GOLD = json.load(open(os.path.join(GOLDEN, "regress_ok.json")))["goldens"]
 
 
 @pytest.mark.parametrize("name,fields", [
-    ("taylor2", "uv"), ("taylor3", "uvw"), ("taylor4", "uvw"), ("taylor5", "uvwp"),
+    ("taylor2", "uvp"), ("taylor3", "uvwp"), ("taylor4", "uvwp"), ("taylor5", "uvwp"),
+    # high-order pressure BCs <H> (src/bcmgr.cpp:1036-1331) on Dirichlet-velocity walls
+    ("kovas1", "uvp"), ("kovas2", "uvwp"), ("kovas3", "uvwp"), ("kovas4", "uvwp"), ("kovas5", "uvwp"),
 ])
 def test_dns_regress_goldens(name, fields):
     D = O.dns_session(os.path.join(SESSIONS, name))
     got = O.compare_errors(D)
     for c in fields:
         assert got[c] == GOLD[name][c], (name, c, got[c], GOLD[name][c])
+        if "MPI/" + name in GOLD:
+            assert got[c] == GOLD["MPI/" + name][c]
 
 
-def test_taylor3_mpi_golden_velocity():
-    D = O.dns_session(os.path.join(SESSIONS, "taylor3"))
-    got = O.compare_errors(D)
-    for c in "uvw":
-        assert got[c] == GOLD["MPI/taylor3"][c]
+def test_enumerate_o3_pin_is_best_root():
+    """The pinned (highest) number of an enumerate -O3 numbering goes to the
+    first root, in Mesh::buildMap order, of least RCM bandwidth."""
+    S = O.read_session(os.path.join(SESSIONS, "kovas3"))
+    bmap = O.reference_map(O.Mesh(S, 5))
+    nsolve = bmap.max() + 1
+    assert sorted(set(bmap.ravel())) == list(range(nsolve))
+    new = O.enumerate_o3(bmap)
+    assert sorted(set(new.ravel())) == list(range(nsolve))
+
+    def bandwidth(m):
+        return max(int(r.max() - r.min()) for r in m) + 1
+
+    adj = [[] for _ in range(nsolve)]
+    for row in bmap:
+        for i, a in enumerate(row):
+            for j, b in enumerate(row):
+                if i != j and b not in adj[a]:
+                    adj[a].append(int(b))
+    deg = [len(a) for a in adj]
+    bws = []
+    for root in range(nsolve):
+        inv = np.empty(nsolve, int)
+        inv[O._sparspak_rcm(root, adj, deg)] = np.arange(nsolve)
+        bws.append(bandwidth(inv[bmap]))
+    pin_root = int(bmap.ravel()[np.argmax(new.ravel())])
+    assert pin_root == int(np.argmin(bws))
+    assert bandwidth(new) == min(bws)
 
 
 @pytest.mark.parametrize("name,tol", [
