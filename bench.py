@@ -354,30 +354,49 @@ def run_ours(args):
         "clocks": clocks, "cpu_baseline": cpu,
     }
     if args.dns_steps > 0 and ws == 1:
-        line["dns"] = run_dns(args.dns_steps, 3, local)
+        line["dns"] = run_dns(args.dns_steps, 3, local, "c3")
+        line["dns_c5"] = run_dns(args.dns_steps, 3, local, "c5")
     print(json.dumps(line))
     if ws > 1:
         torch.distributed.destroy_process_group()
 
 
-def run_dns(steps, warmup=3, local=0):
-    """Secondary measurement: DNS steps/s on the 3D Taylor--Green workload
-    (24x24 periodic quads, N_P=9, N_Z=96, Re=1600, D_T=1e-3, N_TIME=3,
-    alternating skew-symmetric advection, plain FP64 direct solves).  The
-    first N_TIME-1 steps use the reference's temporary PCG systems and are
-    excluded; the timed steps are device time (CUDA events on the library
-    stream)."""
+DNS_WORKLOADS = {
+    "c3": "c3: Taylor-Green 24x24x96, N_P=9, Re=1600, D_T=1e-3, N_TIME=3 (no dealiasing)",
+    "c5": "c5: channel [0,2pi]x[-1,1]x[0,2pi) 16x8x32, N_P=9, Re=500, D_T=5e-3, N_TIME=3, "
+          "no-slip walls with high-order pressure BCs, u=1-y^2 + seeded 1e-3 perturbation",
+}
+
+
+def run_dns(steps, warmup=3, local=0, workload="c3"):
+    """Secondary measurement: DNS steps/s, plain FP64 direct solves,
+    alternating skew-symmetric advection.  c3: 3D Taylor--Green (24x24
+    periodic quads, N_P=9, N_Z=96, Re=1600, D_T=1e-3, N_TIME=3).  c5: plane
+    channel (16x8 quads periodic in x, N_P=9, N_Z=32, Re=500, D_T=5e-3,
+    N_TIME=3, walls <D> u=v=w=0 / <H> p, base flow plus a seeded stream-
+    function perturbation).  The first N_TIME-1 steps use the reference's
+    temporary PCG systems and are excluded; the timed steps are device time
+    (CUDA events on the library stream)."""
     import torch
     import semtex_b200 as S
     from semtex_b200 import sessions
     d = tempfile.mkdtemp()
-    p = sessions.taylor_green_session(os.path.join(d, "c3"), 24, 9, 96, re=1600.0, dt=1e-3, nstep=200)
+    if workload == "c3":
+        p = sessions.taylor_green_session(os.path.join(d, "c3"), 24, 9, 96, re=1600.0, dt=1e-3, nstep=200)
+    else:
+        p = sessions.channel_session(os.path.join(d, "c5"), 16, 8, 9, 32, re=500.0, dt=5e-3, nstep=100)
     t0 = time.perf_counter()
     ctx = S.Context(p, device=local)
     D = S.DNS(ctx, 1)
     setup = time.perf_counter() - t0
-    funcs = S._user_functions(p)
-    D.restart({c: ctx.evaluate(funcs[c], 0.0) for c in ctx.fields if c in funcs}, 0.0)
+    if workload == "c3":
+        funcs = S._user_functions(p)
+        ic = {c: ctx.evaluate(funcs[c], 0.0) for c in ctx.fields if c in funcs}
+    else:
+        x, y = ctx.mesh_coords()
+        z = np.arange(ctx.nz) * 2 * np.pi / ctx.nz
+        ic = sessions.channel_initial(x, y, z)
+    D.restart(ic, 0.0)
     D.advance(2 + warmup)
     stream = ctx.torch_stream()
     e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
@@ -388,8 +407,7 @@ def run_dns(steps, warmup=3, local=0):
     e1.synchronize()
     ms = e0.elapsed_time(e1) / steps
     out = {"metric": "DNS steps/s", "value": 1e3 / ms, "ms_per_step": ms, "steps": steps,
-           "workload": "c3: Taylor-Green 24x24x96, N_P=9, Re=1600, D_T=1e-3, N_TIME=3 (no dealiasing)",
-           "setup_s": setup}
+           "workload": DNS_WORKLOADS[workload], "setup_s": setup}
     D.close()
     ctx.close()
     return out
@@ -408,15 +426,16 @@ def main():
                     help="Fourier-mode groups solved on parallel streams (0: library default)")
     ap.add_argument("--solver", default="twolevel", choices=["twolevel", "band"],
                     help="band: the single banded-Cholesky skeleton solve (for comparison)")
-    ap.add_argument("--workload", default="c2", choices=["c2", "dns"],
-                    help="dns: run only the DNS measurement (one JSON line)")
+    ap.add_argument("--workload", default="c2", choices=["c2", "dns", "dns_c5"],
+                    help="dns / dns_c5: run only the c3 / c5 DNS measurement (one JSON line)")
     args = ap.parse_args()
     if args.impl == "reference":
         run_reference(args)
-    elif args.workload == "dns":
+    elif args.workload in ("dns", "dns_c5"):
         import torch
         torch.cuda.set_device(0)
-        print(json.dumps(run_dns(max(1, args.dns_steps), args.warmup, 0)))
+        print(json.dumps(run_dns(max(1, args.dns_steps), args.warmup, 0,
+                                 "c3" if args.workload == "dns" else "c5")))
     else:
         run_ours(args)
 

@@ -105,3 +105,44 @@ def taylor_green_session(path, n, np_, nz, re=1600.0, dt=1e-3, nstep=200, extra=
     user = ["u = sin(x)*cos(y)*cos(z)", "v = -cos(x)*sin(y)*cos(z)", "w = 0", "p = 0"]
     return rect_session(path, n, n, x=(0.0, 2 * np.pi), y=(0.0, 2 * np.pi), tokens=tok,
                         fields="uvwp", periodic_x=True, periodic_y=True, user=user)
+
+
+def channel_session(path, nx=16, ny=8, np_=9, nz=32, re=500.0, dt=5e-3, nstep=100, ntime=3, extra=None):
+    """Plane channel [0, 2 pi] x [-1, 1] x [0, 2 pi), periodic in x and z,
+    no-slip walls at y = +-1 with high-order pressure BCs (config c5)."""
+    tok = {"N_P": np_, "N_Z": nz, "BETA": 1, "KINVIS": f"1.0/{re}", "D_T": dt, "N_TIME": ntime,
+           "N_STEP": nstep, "TOL_REL": 1e-13}
+    tok.update(extra or {})
+    fields = "uvwp" if nz > 1 else "uvp"
+    bc = {"u": "<D> 0", "v": "<D> 0", "p": "<H> 0"}
+    if nz > 1:
+        bc["w"] = "<D> 0"
+    return rect_session(path, nx, ny, x=(0.0, 2 * np.pi), y=(-1.0, 1.0), tokens=tok, fields=fields,
+                        periodic_x=True, bcs={"w": bc})
+
+
+def channel_initial(x, y, z, seed=20261203, amplitude=1e-3, modes=3):
+    """Base flow u = 1 - y^2 plus a divergence-free perturbation from a seeded
+    random stream function psi(x, y; z) = (1 - y^2)^2 sum a cos(kx x + b)
+    cos(kz z + c):  u' = dpsi/dy, v' = -dpsi/dx, w' = 0, all zero at the
+    walls; scaled so that max |u'| = amplitude.  x, y are node coordinates
+    [nel, np, np]; z the plane positions.  Returns {u, v, w, p} arrays
+    [nz, nel, np, np]."""
+    rng = np.random.default_rng(seed)
+    X = x[None]
+    Y = y[None]
+    Z = np.asarray(z, float)[:, None, None, None]
+    g = (1 - Y * Y) ** 2
+    dg = -4 * Y * (1 - Y * Y)
+    up = np.zeros(Z.shape[:1] + x.shape)
+    vp = np.zeros_like(up)
+    for kx in range(1, modes + 1):
+        for kz in range(0, modes if len(z) > 1 else 1):
+            a, b, c = rng.uniform(-1, 1), rng.uniform(0, 2 * np.pi), rng.uniform(0, 2 * np.pi)
+            cx, sx = np.cos(kx * X + b), np.sin(kx * X + b)
+            cz = np.cos(kz * Z + c)
+            up += a * dg * cx * cz
+            vp += a * kx * g * sx * cz
+    s = amplitude / max(np.abs(up).max(), 1e-300)
+    base = np.broadcast_to(1 - Y * Y, up.shape)
+    return {"u": base + s * up, "v": s * vp, "w": np.zeros_like(up), "p": np.zeros_like(up)}

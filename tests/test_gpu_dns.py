@@ -1,12 +1,15 @@
 """GPU parity of the DNS step (dns/integrate.cpp) against the oracle, and
 against the reference's regression goldens (regress/*.ok) through the GPU path.
 
-Velocities: relative L2 <= 1e-10 vs the oracle.  Pressure: relative L2 <=
-1e-9; a pressure field without essential nodes has a singular k=0 problem
-pinned at its highest-numbered node (src/matrix.cpp:160-162), whose solution
-carries round-off amplified by that pinned system's condition number.  Both
-codes number such fields as the reference's `enumerate -O3` does, so they pin
-the same node and the pressures are compared as they are, constant included.
+Velocities: L2 error <= 1e-10 relative to the largest velocity component.
+Pressure: L2 error <= 1e-9 relative to the larger of its own norm and the
+dynamic-pressure scale (the norm of |u|^2), since a flow whose pressure is far
+below |u|^2 carries velocity-scale round-off in it; a pressure field without
+essential nodes also has a singular k=0 problem pinned at its highest-
+numbered node (src/matrix.cpp:160-162), whose solution carries round-off
+amplified by that pinned system's condition number.  Both codes number such
+fields as the reference's `enumerate -O3` does, so they pin the same node and
+the pressures are compared as they are, constant included.
 """
 import json
 import os
@@ -35,7 +38,9 @@ def _compare(path, gpu, D, tol=1e-10, ptol=1e-9):
         err = np.linalg.norm(gpu[c] - phys[c]) / scale
         assert err < tol, (c, err)
     pc = D.pname
-    assert rel_l2(gpu[pc], phys[pc]) < ptol, (pc, rel_l2(gpu[pc], phys[pc]))
+    pscale = max(np.linalg.norm(phys[pc]), np.linalg.norm(sum(phys[c] ** 2 for c in D.vel)))
+    perr = np.linalg.norm(gpu[pc] - phys[pc]) / pscale
+    assert perr < ptol, (pc, perr)
 
 
 def _goldens(name, gpu, t, D, fields):
@@ -114,3 +119,22 @@ def test_channel_high_order_pressure_walls(tmp_path, nz, ntime):
     gpu, t = S.dns(p)
     D = O.dns_session(p)
     _compare(p, gpu, D)
+
+
+def test_channel_c5_builder(tmp_path):
+    # The c5 channel (walls <D> / <H>) at reduced size, from the bench's own
+    # session builder and seeded initial perturbation.
+    p = sessions.channel_session(str(tmp_path / "c5"), 4, 2, 6, 8, nstep=6, extra={"TOL_REL": 1e-14})
+    ctx = S.Context(p)
+    x, y = ctx.mesh_coords()
+    ic = sessions.channel_initial(x, y, np.arange(ctx.nz) * 2 * np.pi / ctx.nz)
+    D = S.DNS(ctx, 1)
+    D.restart(ic, 0.0)
+    D.advance(6)
+    gpu = {c: D.field(c) for c in ctx.fields}
+    D.close()
+    ctx.close()
+    P = O.Problem(O.read_session(p))
+    Do = O.DNS(P, ic)
+    Do.advance(6)
+    _compare(p, gpu, Do)
