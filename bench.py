@@ -45,12 +45,8 @@ def make_session(d):
 
 
 def forcing_per_unique_node(x, y, nz, seed):
-    """U[-1,1] per unique (x, y, z) node, identical on coincident element copies."""
-    key = np.round(x * 1e9).astype(np.int64) * 4000000007 + np.round(y * 1e9).astype(np.int64)
-    uniq, inv = np.unique(key.ravel(), return_inverse=True)
-    rng = np.random.default_rng(seed)
-    vals = rng.uniform(-1.0, 1.0, (nz, len(uniq)))
-    return vals[:, inv].reshape((nz,) + x.shape), len(uniq)
+    from semtex_b200 import sessions
+    return sessions.forcing_per_unique_node(x, y, nz, seed)
 
 
 def dist_init(backend="nccl"):
@@ -356,6 +352,7 @@ def run_ours(args):
     if args.dns_steps > 0 and ws == 1:
         line["dns"] = run_dns(args.dns_steps, 3, local, "c3")
         line["dns_c5"] = run_dns(args.dns_steps, 3, local, "c5")
+        line["batch_c4"] = run_batch(args.dns_steps, 3, local)
     print(json.dumps(line))
     if ws > 1:
         torch.distributed.destroy_process_group()
@@ -413,6 +410,87 @@ def run_dns(steps, warmup=3, local=0, workload="c3"):
     return out
 
 
+def run_batch(steps, warmup=3, local=0):
+    """Secondary measurement: the uneven batch (64 independent 2D Helmholtz
+    problems, n x n quads with n uniform in 4..32, order N uniform in 6..12,
+    lambda^2 log-uniform in [0.1, 100], Dirichlet zero, U[-1,1] forcing per
+    unique node, seeded).  Helmholtz DOF/s of the whole batch, device time
+    (CUDA events), L2 flushed between steps, for (a) one replay of the
+    captured CUDA graph (stx_batch_launch) and (b) the same 64 DIRECT solves
+    issued one stx_field_solve call at a time from the host."""
+    import ctypes as C
+    import torch
+    import semtex_b200 as S
+    from semtex_b200 import sessions
+    from semtex_b200._lib import lib
+    d = tempfile.mkdtemp()
+    specs = sessions.uneven_batch()
+    t0 = time.perf_counter()
+    items, ctxs, dof = [], [], 0
+    for i, sp in enumerate(specs):
+        path = sessions.helmholtz_session(os.path.join(d, f"p{i}"), sp["n"], sp["np"], lambda2=sp["lambda2"])
+        ctx = S.Context(path, device=local)
+        x, y = ctx.mesh_coords()
+        f, nu = sessions.forcing_per_unique_node(x, y, 1, sp["seed"])
+        dof += nu
+        sys_ = S.ModalMatrixSys(ctx, "c", sp["lambda2"])
+        items.append((sys_, ctx.new_field("f").load_physical(f), ctx.new_field("u")))
+        ctxs.append(ctx)
+    B = S.Batch(items)
+    setup = time.perf_counter() - t0
+    dev = f"cuda:{local}"
+    main = torch.cuda.ExternalStream(B.stream, device=dev)
+    side = [torch.cuda.ExternalStream(c.stream, device=dev) for c in ctxs]
+    flush = torch.empty(256 * 1024 * 1024 // 4, dtype=torch.float32, device=dev)
+    calls = [(s.handle, fF.ptr(), fU.ptr()) for s, fF, fU in items]
+    solve = lib().stx_field_solve
+
+    def one_loop():
+        ev0 = torch.cuda.Event()
+        ev0.record(main)
+        for st in side:
+            st.wait_event(ev0)
+        for h, pf, pu in calls:
+            rc = solve(h, pf, pu, 0.0, 0, None)
+            if rc:
+                raise RuntimeError(f"stx_field_solve failed ({rc})")
+        for st in side:
+            ev = torch.cuda.Event()
+            ev.record(st)
+            main.wait_event(ev)
+
+    def timed(fn):
+        ms = []
+        for k in range(warmup + steps):
+            with torch.cuda.stream(main):
+                flush.fill_(1.0)
+            e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+            e0.record(main)
+            fn()
+            e1.record(main)
+            e1.synchronize()
+            if k >= warmup:
+                ms.append(e0.elapsed_time(e1))
+        return statistics.mean(ms)
+
+    ms_graph = timed(B.launch)
+    ms_loop = timed(one_loop)
+    out = {"metric": "Helmholtz DOF/s (uneven batch, one CUDA graph)", "value": dof / (ms_graph * 1e-3),
+           "unit": "DOF/s", "ms_per_step": ms_graph, "steps": steps,
+           "per_problem_calls": {"value": dof / (ms_loop * 1e-3), "ms_per_step": ms_loop},
+           "problems": len(specs), "dof": dof, "elements": sum(sp["n"] ** 2 for sp in specs),
+           "kernel_nodes": B.kernel_nodes,
+           "workload": "c4: 64 Dirichlet Helmholtz problems on [0,1]^2, n in 4..32, N in 6..12, "
+                       "lambda^2 log-uniform [0.1,100], seed 20261203",
+           "setup_s": setup}
+    B.close()
+    for sys_, _, _ in items:
+        sys_.close()
+    for c in ctxs:
+        c.close()
+    return out
+
+
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
@@ -426,8 +504,8 @@ def main():
                     help="Fourier-mode groups solved on parallel streams (0: library default)")
     ap.add_argument("--solver", default="twolevel", choices=["twolevel", "band"],
                     help="band: the single banded-Cholesky skeleton solve (for comparison)")
-    ap.add_argument("--workload", default="c2", choices=["c2", "dns", "dns_c5"],
-                    help="dns / dns_c5: run only the c3 / c5 DNS measurement (one JSON line)")
+    ap.add_argument("--workload", default="c2", choices=["c2", "dns", "dns_c5", "batch_c4"],
+                    help="dns / dns_c5 / batch_c4: run only that secondary measurement (one JSON line)")
     args = ap.parse_args()
     if args.impl == "reference":
         run_reference(args)
@@ -436,6 +514,10 @@ def main():
         torch.cuda.set_device(0)
         print(json.dumps(run_dns(max(1, args.dns_steps), args.warmup, 0,
                                  "c3" if args.workload == "dns" else "c5")))
+    elif args.workload == "batch_c4":
+        import torch
+        torch.cuda.set_device(0)
+        print(json.dumps(run_batch(max(1, args.dns_steps), args.warmup, 0)))
     else:
         run_ours(args)
 

@@ -43,6 +43,7 @@ extern "C" {
 typedef struct stx_context stx_context;
 typedef struct stx_modal stx_modal;
 typedef struct stx_dns stx_dns;
+typedef struct stx_batch stx_batch;
 
 /* Message of the last failed call on this thread ("" if none). */
 const char* stx_last_error(void);
@@ -184,6 +185,24 @@ int stx_dns_advance(stx_dns* dns, int nsteps);
 int stx_dns_state(const stx_dns* dns, int* step, double* time);
 /* Device pointer of a field's Fourier-space storage (nz x plane_size). */
 int stx_dns_field_ptr(stx_dns* dns, char field, double** d_ptr);
+
+/* ---- Batches of independent solves --------------------------------------
+ * The reference solves one problem per `elliptic` run (elliptic/drive.cpp:
+ * 61-96: one Field::solve).  stx_batch_create captures n DIRECT solves --
+ * stx_field_solve(systems[i], d_forcing[i], d_unknown[i]) each on its own
+ * context's stream -- as one CUDA graph whose independent problems are
+ * parallel branches; it runs every solve once first, outside the capture
+ * (the d_unknown buffers are written).  The device buffers are fixed in the
+ * graph.  stx_batch_launch replays all n solves with one graph launch on
+ * `stream` (NULL: a stream the batch creates; stx_batch_info returns it).
+ * Systems may come from different contexts (different meshes and orders) on
+ * one device; the systems and buffers must outlive the batch. */
+int stx_batch_create(stx_modal* const* systems, const double* const* d_forcing, double* const* d_unknown,
+                     int n, void* stream, stx_batch** out);
+int stx_batch_launch(stx_batch* batch);
+/* Number of systems, kernel launches per replay and the replay stream. */
+int stx_batch_info(const stx_batch* batch, int* nsystems, int* kernel_nodes, void** stream);
+int stx_batch_destroy(stx_batch* batch);
 
 /* Synchronise the context's stream. */
 int stx_sync(stx_context* ctx);

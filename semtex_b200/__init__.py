@@ -27,7 +27,7 @@ from .fieldfile import read_field, write_field
 
 DIRECT, JACPCG = STX_DIRECT, STX_JACPCG
 
-__all__ = ["Context", "ModalMatrixSys", "Field", "DNS", "elliptic", "dns", "read_field",
+__all__ = ["Context", "ModalMatrixSys", "Field", "DNS", "Batch", "numbering", "elliptic", "dns", "read_field",
            "write_field", "FORWARD", "INVERSE", "DIRECT", "JACPCG", "StxError"]
 
 
@@ -224,6 +224,41 @@ class ModalMatrixSys:
         check(lib().stx_elliptic_solve_host(self._h, C.c_void_p(f.ctypes.data),
                                             C.c_void_p(out.ctypes.data)))
         return out
+
+
+class Batch:
+    """Independent DIRECT solves replayed as one CUDA graph (stx_batch_*).
+
+    ``items`` is a list of (ModalMatrixSys, forcing Field, solution Field);
+    the fields' device storage is fixed in the graph.  ``launch()`` replays
+    every solve with one graph launch on ``stream``."""
+
+    def __init__(self, items, stream: int | None = None):
+        n = len(items)
+        self.items = list(items)   # keep systems and buffers alive
+        sys_ = (C.c_void_p * n)(*[s.handle.value for s, _, _ in items])
+        frc = (C.c_void_p * n)(*[f.ptr().value for _, f, _ in items])
+        unk = (C.c_void_p * n)(*[u.ptr().value for _, _, u in items])
+        self._h = C.c_void_p()
+        check(lib().stx_batch_create(sys_, frc, unk, n, C.c_void_p(stream) if stream else None,
+                                     C.byref(self._h)))
+        a, b, st = C.c_int(), C.c_int(), C.c_void_p()
+        check(lib().stx_batch_info(self._h, C.byref(a), C.byref(b), C.byref(st)))
+        self.nsystems, self.kernel_nodes, self.stream = a.value, b.value, st.value
+
+    def launch(self):
+        check(lib().stx_batch_launch(self._h))
+
+    def close(self):
+        if self._h:
+            check(lib().stx_batch_destroy(self._h))
+        self._h = C.c_void_p()
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
 
 
 def numbering(session: str, field: str, overrides=None):

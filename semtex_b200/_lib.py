@@ -59,6 +59,10 @@ SIGNATURES = {
     "stx_sync": (_i, [_p]),
     "stx_context_stream": (_i, [_p, C.POINTER(_p)]),
     "stx_context_scratch": (_i, [_p, C.c_ulonglong, C.POINTER(_p)]),
+    "stx_batch_create": (_i, [_p, _p, _p, _i, _p, C.POINTER(_p)]),
+    "stx_batch_launch": (_i, [_p]),
+    "stx_batch_info": (_i, [_p, _pi, _pi, C.POINTER(_p)]),
+    "stx_batch_destroy": (_i, [_p]),
 }
 
 

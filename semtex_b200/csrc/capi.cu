@@ -440,14 +440,16 @@ int stx_modal_create(stx_context* ctx, char field, double lambda2, double beta, 
       if (method == STX_DIRECT) P = ctx->patching(field);
       std::vector<ModeSystem> modes(num_modes);
       std::vector<std::string> errs(num_modes);
-      unsigned nth = std::max(1u, std::min<unsigned>(std::thread::hardware_concurrency(), num_modes));
+      const unsigned hw = std::max(1u, std::thread::hardware_concurrency());
+      unsigned nth = std::max(1u, std::min<unsigned>(hw, num_modes));
+      const int inner = static_cast<int>(std::max(1u, hw / nth));  // threads of each mode's dense inverses
       std::vector<std::thread> pool;
       for (unsigned w = 0; w < nth; ++w)
         pool.emplace_back([&, w] {
           for (int m = static_cast<int>(w); m < num_modes; m += nth) {
             try {
               const double bk = beta * (base_mode + m);
-              modes[m] = build_mode_system(M, N, P, lambda2, bk * bk, method);
+              modes[m] = build_mode_system(M, N, P, lambda2, bk * bk, method, inner);
             } catch (const std::exception& e) {
               errs[m] = e.what();
             }

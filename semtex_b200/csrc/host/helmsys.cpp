@@ -1,8 +1,10 @@
 #include "helmsys.hpp"
 
+#include <algorithm>
 #include <cmath>
 #include <stdexcept>
 #include <string>
+#include <thread>
 
 namespace stx {
 
@@ -37,6 +39,38 @@ void invert(int n, double* A) {
   }
   for (int i = 0; i < n; ++i)
     for (int j = 0; j < n; ++j) A[i * n + j] = B[i * 2 * n + n + j];
+}
+// f(lo, hi) over [0, n) split into contiguous ranges on `nthreads` threads.
+template <class F>
+void parallel_ranges(int n, int nthreads, F&& f) {
+  const int t = std::max(1, std::min(nthreads, n / 16));
+  if (t <= 1) {
+    f(0, n);
+    return;
+  }
+  std::vector<std::thread> pool;
+  for (int w = 0; w < t; ++w) {
+    const int lo = static_cast<int>(static_cast<long long>(n) * w / t);
+    const int hi = static_cast<int>(static_cast<long long>(n) * (w + 1) / t);
+    pool.emplace_back([&f, lo, hi] { f(lo, hi); });
+  }
+  for (auto& th : pool) th.join();
+}
+
+// Same, with rows interleaved (for triangular work whose cost grows with the row).
+template <class F>
+void parallel_rows(int n, int nthreads, F&& f) {
+  const int t = std::max(1, std::min(nthreads, n / 16));
+  if (t <= 1) {
+    for (int i = 0; i < n; ++i) f(i);
+    return;
+  }
+  std::vector<std::thread> pool;
+  for (int w = 0; w < t; ++w)
+    pool.emplace_back([&f, w, t, n] {
+      for (int i = w; i < n; i += t) f(i);
+    });
+  for (auto& th : pool) th.join();
 }
 }  // namespace
 
@@ -115,54 +149,67 @@ void factor_band(std::vector<double>& A, int ns, int nb, ModeSystem& S) {
 
 }  // namespace
 
-void spd_inverse(int n, double* A) {
-  // A = L L^T (lower, in place)
-  for (int j = 0; j < n; ++j) {
-    double* aj = A + static_cast<size_t>(j) * n;
-    double d = aj[j];
-    for (int k = 0; k < j; ++k) d -= aj[k] * aj[k];
-    if (!(d > 0.0)) throw std::runtime_error("failed to factor Helmholtz matrix (not positive definite)");
-    d = std::sqrt(d);
-    aj[j] = d;
-    const double inv = 1.0 / d;
-    for (int i = j + 1; i < n; ++i) {
-      double* ai = A + static_cast<size_t>(i) * n;
-      double s = ai[j];
-      for (int k = 0; k < j; ++k) s -= ai[k] * aj[k];
-      ai[j] = s * inv;
+void spd_inverse(int n, double* A, int nthreads) {
+  // A = L L^T, lower triangle in place, in column blocks of kb: the diagonal
+  // block serially, then the rows below it in parallel (row i of the block
+  // needs only its own earlier columns and the block's rows).
+  constexpr int kb = 48;
+  for (int j0 = 0; j0 < n; j0 += kb) {
+    const int j1 = std::min(n, j0 + kb);
+    for (int j = j0; j < j1; ++j) {
+      double* aj = A + static_cast<size_t>(j) * n;
+      double d = aj[j];
+      for (int k = 0; k < j; ++k) d -= aj[k] * aj[k];
+      if (!(d > 0.0)) throw std::runtime_error("failed to factor Helmholtz matrix (not positive definite)");
+      aj[j] = std::sqrt(d);
+      for (int i = j + 1; i < j1; ++i) {
+        double* ai = A + static_cast<size_t>(i) * n;
+        double v = ai[j];
+        for (int k = 0; k < j; ++k) v -= ai[k] * aj[k];
+        ai[j] = v / aj[j];
+      }
     }
+    parallel_ranges(n - j1, nthreads, [&](int lo, int hi) {
+      for (int i = j1 + lo; i < j1 + hi; ++i) {
+        double* ai = A + static_cast<size_t>(i) * n;
+        for (int j = j0; j < j1; ++j) {
+          const double* aj = A + static_cast<size_t>(j) * n;
+          double v = ai[j];
+          for (int k = 0; k < j; ++k) v -= ai[k] * aj[k];
+          ai[j] = v / aj[j];
+        }
+      }
+    });
   }
-  // W = L^{-1} (lower), stored transposed in the upper triangle as rows of W^T
-  std::vector<double> W(static_cast<size_t>(n) * n, 0.0);  // W[i][j], j <= i
-  for (int i = 0; i < n; ++i) {
-    const double* ai = A + static_cast<size_t>(i) * n;
-    double* wi = &W[static_cast<size_t>(i) * n];
-    wi[i] = 1.0 / ai[i];
-    for (int j = 0; j < i; ++j) {
-      // W[i][j] = -(sum_{k=j}^{i-1} L[i][k] W[k][j]) / L[i][i]
-      double s = 0.0;
-      for (int k = j; k < i; ++k) s += ai[k] * W[static_cast<size_t>(k) * n + j];
-      wi[j] = -s * wi[i];
+  // W = L^{-1}: column c of W solves L w = e_c (forward substitution over
+  // rows i >= c); stored as row c of WT (WT[c][i] = W[i][c]).
+  std::vector<double> WT(static_cast<size_t>(n) * n, 0.0);
+  parallel_rows(n, nthreads, [&](int c) {
+    double* w = &WT[static_cast<size_t>(c) * n];
+    w[c] = 1.0 / A[static_cast<size_t>(c) * n + c];
+    for (int i = c + 1; i < n; ++i) {
+      const double* ai = A + static_cast<size_t>(i) * n;
+      double v = 0.0;
+      for (int k = c; k < i; ++k) v -= ai[k] * w[k];
+      w[i] = v / ai[i];
     }
-  }
-  // A^{-1} = W^T W : (i,j) = sum_{k >= max(i,j)} W[k][i] W[k][j]
-  std::vector<double> WT(static_cast<size_t>(n) * n, 0.0);  // WT[i][k] = W[k][i]
-  for (int k = 0; k < n; ++k)
-    for (int i = 0; i <= k; ++i) WT[static_cast<size_t>(i) * n + k] = W[static_cast<size_t>(k) * n + i];
-  for (int i = 0; i < n; ++i) {
+  });
+  // A^{-1} = W^T W: (i, j) = sum_{k >= max(i, j)} WT[i][k] WT[j][k]
+  parallel_rows(n, nthreads, [&](int i) {
     const double* ti = &WT[static_cast<size_t>(i) * n];
     for (int j = i; j < n; ++j) {
       const double* tj = &WT[static_cast<size_t>(j) * n];
-      double s = 0.0;
-      for (int k = j; k < n; ++k) s += ti[k] * tj[k];
-      A[static_cast<size_t>(i) * n + j] = s;
-      A[static_cast<size_t>(j) * n + i] = s;
+      double v = 0.0;
+      for (int k = j; k < n; ++k) v += ti[k] * tj[k];
+      A[static_cast<size_t>(i) * n + j] = v;
     }
-  }
+  });
+  for (int i = 0; i < n; ++i)
+    for (int j = 0; j < i; ++j) A[static_cast<size_t>(i) * n + j] = A[static_cast<size_t>(j) * n + i];
 }
 
 ModeSystem build_mode_system(const Mesh& M, const Numbering& N, const Patching* P, double lambda2,
-                             double betak2, int method) {
+                             double betak2, int method, int nthreads) {
   ModeSystem S;
   S.lambda2 = lambda2;
   S.betak2 = betak2;
@@ -255,24 +302,40 @@ ModeSystem build_mode_system(const Mesh& M, const Numbering& N, const Patching* 
       std::vector<double> II(static_cast<size_t>(nI) * nI);
       for (int a = 0; a < nI; ++a)
         for (int b = 0; b < nI; ++b) II[static_cast<size_t>(a) * nI + b] = Sp[static_cast<size_t>(a) * nl + b];
-      if (nI) invert(nI, II.data());
+      if (nI) spd_inverse(nI, II.data(), nthreads);  // S_II is symmetric positive definite
       for (int a = 0; a < nI; ++a)
         for (int b = 0; b < nI; ++b) Si[static_cast<size_t>(a) * nI_max + b] = II[static_cast<size_t>(a) * nI + b];
-      for (int a = 0; a < nI; ++a)
-        for (int b = 0; b < nB; ++b) {
-          double v = 0;
-          for (int c = 0; c < nI; ++c) v += II[static_cast<size_t>(a) * nI + c] * Sp[static_cast<size_t>(c) * nl + nI + b];
-          G[static_cast<size_t>(a) * nB_max + b] = v;
+      // S_BI rows (= S_IB columns, contiguous): SB[b][c] = Sp[nI + b][c]
+      std::vector<double> SB(static_cast<size_t>(nB) * std::max(nI, 1));
+      for (int b = 0; b < nB; ++b)
+        for (int c = 0; c < nI; ++c) SB[static_cast<size_t>(b) * nI + c] = Sp[static_cast<size_t>(nI + b) * nl + c];
+      // G = S_II^-1 S_IB, GT[b][a] = G[a][b] kept for the Schur update
+      std::vector<double> GT(static_cast<size_t>(nB) * std::max(nI, 1));
+      parallel_ranges(nI, nthreads, [&](int lo, int hi) {
+        for (int a = lo; a < hi; ++a) {
+          const double* ia = &II[static_cast<size_t>(a) * nI];
+          for (int b = 0; b < nB; ++b) {
+            const double* sb = &SB[static_cast<size_t>(b) * nI];
+            double v = 0;
+            for (int c = 0; c < nI; ++c) v += ia[c] * sb[c];
+            G[static_cast<size_t>(a) * nB_max + b] = v;
+            GT[static_cast<size_t>(b) * nI + a] = v;
+          }
         }
+      });
       auto& Tf = T[f];
       Tf.assign(static_cast<size_t>(nB) * nB, 0.0);
-      for (int a = 0; a < nB; ++a)
-        for (int b = 0; b < nB; ++b) {
-          double v = Sp[static_cast<size_t>(nI + a) * nl + nI + b];
-          for (int c = 0; c < nI; ++c)
-            v -= Sp[static_cast<size_t>(nI + a) * nl + c] * G[static_cast<size_t>(c) * nB_max + b];
-          Tf[static_cast<size_t>(a) * nB + b] = v;
+      parallel_ranges(nB, nthreads, [&](int lo, int hi) {
+        for (int a = lo; a < hi; ++a) {
+          const double* sa = &SB[static_cast<size_t>(a) * nI];
+          for (int b = 0; b < nB; ++b) {
+            const double* gb = &GT[static_cast<size_t>(b) * nI];
+            double v = Sp[static_cast<size_t>(nI + a) * nl + nI + b];
+            for (int c = 0; c < nI; ++c) v -= sa[c] * gb[c];
+            Tf[static_cast<size_t>(a) * nB + b] = v;
+          }
         }
+      });
     }
     const int ni = P->niface;
     S.hsc = hbb_all;
@@ -295,7 +358,7 @@ ModeSystem build_mode_system(const Mesh& M, const Numbering& N, const Patching* 
       A[static_cast<size_t>(q) * ni + q] = 1.0;
       S.pin_iid = q;
     }
-    if (ni) spd_inverse(ni, A.data());
+    if (ni) spd_inverse(ni, A.data(), nthreads);
     S.nsolve = ni;
     S.nband = 0;
     return S;

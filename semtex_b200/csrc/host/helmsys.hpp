@@ -48,9 +48,10 @@ void element_helmholtz(const Mesh& M, int e, double lambda2, double betak2, doub
 
 // `P` (may be null) selects the two-level condensation for DIRECT systems.
 // In-place inverse of a symmetric positive-definite n x n matrix (Cholesky,
-// triangular inverse, product); throws if the matrix is not positive definite.
-void spd_inverse(int n, double* A);
+// triangular inverse, product) on `nthreads` host threads; throws if the
+// matrix is not positive definite.
+void spd_inverse(int n, double* A, int nthreads = 1);
 ModeSystem build_mode_system(const Mesh& M, const Numbering& N, const Patching* P, double lambda2,
-                             double betak2, int method);
+                             double betak2, int method, int nthreads = 1);
 
 }  // namespace stx

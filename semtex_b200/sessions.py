@@ -146,3 +146,30 @@ def channel_initial(x, y, z, seed=20261203, amplitude=1e-3, modes=3):
     s = amplitude / max(np.abs(up).max(), 1e-300)
     base = np.broadcast_to(1 - Y * Y, up.shape)
     return {"u": base + s * up, "v": s * vp, "w": np.zeros_like(up), "p": np.zeros_like(up)}
+
+
+def forcing_per_unique_node(x, y, nz, seed):
+    """U[-1,1] per unique (x, y, z) node, identical on coincident element
+    copies.  x, y are node coordinates [nel, np, np]; returns the forcing
+    [nz, nel, np, np] and the number of unique nodes per plane."""
+    key = np.round(x * 1e9).astype(np.int64) * 4000000007 + np.round(y * 1e9).astype(np.int64)
+    uniq, inv = np.unique(key.ravel(), return_inverse=True)
+    rng = np.random.default_rng(seed)
+    vals = rng.uniform(-1.0, 1.0, (nz, len(uniq)))
+    return vals[:, inv].reshape((nz,) + x.shape), len(uniq)
+
+
+def uneven_batch(count=64, seed=20261203, n_range=(4, 32), order_range=(6, 12), lambda2_range=(0.1, 100.0)):
+    """The uneven batch of independent 2D Helmholtz problems (config c4):
+    n x n quads on [0,1]^2 with n uniform in n_range, polynomial order N
+    uniform in order_range (N_P = N + 1), lambda^2 log-uniform in
+    lambda2_range, Dirichlet zero; forcing seeds follow.  Returns a list of
+    dicts (n, np, lambda2, seed)."""
+    rng = np.random.default_rng(seed)
+    out = []
+    for i in range(count):
+        n = int(rng.integers(n_range[0], n_range[1] + 1))
+        order = int(rng.integers(order_range[0], order_range[1] + 1))
+        lam = float(np.exp(rng.uniform(np.log(lambda2_range[0]), np.log(lambda2_range[1]))))
+        out.append({"n": n, "np": order + 1, "lambda2": lam, "seed": seed + 1 + i})
+    return out
