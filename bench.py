@@ -351,6 +351,7 @@ def run_ours(args):
     }
     if args.dns_steps > 0 and ws == 1:
         line["dns"] = run_dns(args.dns_steps, 3, local, "c3")
+        line["dns_c3_dealiased"] = run_dns(args.dns_steps, 3, local, "c3d")
         line["dns_c5"] = run_dns(args.dns_steps, 3, local, "c5")
         line["batch_c4"] = run_batch(args.dns_steps, 3, local)
     print(json.dumps(line))
@@ -360,6 +361,7 @@ def run_ours(args):
 
 DNS_WORKLOADS = {
     "c3": "c3: Taylor-Green 24x24x96, N_P=9, Re=1600, D_T=1e-3, N_TIME=3 (no dealiasing)",
+    "c3d": "c3: Taylor-Green 24x24x96, N_P=9, Re=1600, D_T=1e-3, N_TIME=3, 3/2-rule dealiased products",
     "c5": "c5: channel [0,2pi]x[-1,1]x[0,2pi) 16x8x32, N_P=9, Re=500, D_T=5e-3, N_TIME=3, "
           "no-slip walls with high-order pressure BCs, u=1-y^2 + seeded 1e-3 perturbation",
 }
@@ -378,15 +380,16 @@ def run_dns(steps, warmup=3, local=0, workload="c3"):
     import semtex_b200 as S
     from semtex_b200 import sessions
     d = tempfile.mkdtemp()
-    if workload == "c3":
-        p = sessions.taylor_green_session(os.path.join(d, "c3"), 24, 9, 96, re=1600.0, dt=1e-3, nstep=200)
+    if workload in ("c3", "c3d"):
+        p = sessions.taylor_green_session(os.path.join(d, "c3"), 24, 9, 96, re=1600.0, dt=1e-3, nstep=200,
+                                          extra={"DEALIAS": 1} if workload == "c3d" else None)
     else:
         p = sessions.channel_session(os.path.join(d, "c5"), 16, 8, 9, 32, re=500.0, dt=5e-3, nstep=100)
     t0 = time.perf_counter()
     ctx = S.Context(p, device=local)
     D = S.DNS(ctx, 1)
     setup = time.perf_counter() - t0
-    if workload == "c3":
+    if workload in ("c3", "c3d"):
         funcs = S._user_functions(p)
         ic = {c: ctx.evaluate(funcs[c], 0.0) for c in ctx.fields if c in funcs}
     else:

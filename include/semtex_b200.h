@@ -169,7 +169,13 @@ int stx_context_stream(const stx_context* ctx, void** stream);
  * nonlinear form as dns -S/-C/-N do (dns/drive.cpp:86-91): 0 skew-symmetric,
  * 1 alternating skew-symmetric (default), 2 convective, 3 Stokes.  Velocity
  * Helmholtz systems are DIRECT, with the reference's temporary JACPCG systems
- * for the first N_TIME-1 steps (dns/integrate.cpp:328-356). */
+ * for the first N_TIME-1 steps (dns/integrate.cpp:328-356).  Pressure BCs
+ * may be <H> (high-order, computed each step: src/bcmgr.cpp:1036-1331).
+ * Session token DEALIAS > 0 (with N_Z > 2) forms every nonlinear product on
+ * the 3/2-padded z grid with AuxField::transform32's semantics
+ * (src/auxfield.cpp:1197-1258), the reference's compile-time DEALIAS build
+ * as a run-time token; by default products are not dealiased, as in the
+ * reference's dns. */
 int stx_dns_create(stx_context* ctx, int advection, stx_dns** out);
 int stx_dns_destroy(stx_dns* dns);
 /* Domain::restart semantics (src/domain.cpp:123-156): zero the multi-level

@@ -1114,9 +1114,10 @@ class DNS:
     """
 
     def __init__(self, P: Problem, ic: dict | None = None, t0: float = 0.0,
-                 dealias: bool = False, advection: int = 1):
-        if dealias:
-            raise NotImplementedError("3/2-rule products are not in the oracle")
+                 dealias: bool | None = None, advection: int = 1):
+        if dealias is None:   # the session token (the reference's build-time DEALIAS)
+            dealias = float(P.S.tokens.get("DEALIAS", 0)) > 0
+        self.dealias = bool(dealias) and P.nz > 2
         self.P = P
         S = P.S
         tok = S.tokens
@@ -1245,12 +1246,30 @@ class DNS:
                 lines[k, e] = v
         return lines
 
+    # -- 3/2-rule transforms (AuxField::transform32, src/auxfield.cpp:1197-1258,
+    #    as compiled with DEALIAS): the nz Fourier planes zero-padded to
+    #    3 nz / 2 planes before the inverse transform; the first nz planes of
+    #    the 3 nz / 2 forward transform kept.
+    def _inverse32(self, F):
+        nz = self.P.nz
+        if not self.dealias:
+            return dft_inverse(F)
+        pad = np.zeros((3 * nz // 2,) + F.shape[1:])
+        pad[:nz] = F
+        return dft_inverse(pad)
+
+    def _forward32(self, phys):
+        if not self.dealias:
+            return dft_forward(phys)
+        return dft_forward(phys)[:self.P.nz]
+
     def nonlinear(self):
         """Cartesian nonlinear terms (dns/nonlinear.cpp): advection 0 skew-symmetric
-        (:38-190), 1 alternating skew (:198-381), 2 convective (:384-480), 3 Stokes."""
+        (:38-190), 1 alternating skew (:198-381), 2 convective (:384-480), 3 Stokes.
+        With dealias, every product is formed on the 3/2-padded z grid."""
         P = self.P
         U = [self.u[c].copy() for c in self.vel]
-        Uphys = [dft_inverse(self.u[c]) for c in self.vel]
+        Uphys = [self._inverse32(self.u[c]) for c in self.vel]
         if self.advection == 1:
             forms = ("conv",) if self.toggle else ("cons",)
         elif self.advection == 0:
@@ -1261,24 +1280,24 @@ class DNS:
             forms = ()
         N = []
         for i in range(self.ncom):
-            n = np.zeros_like(U[0])
+            n = np.zeros_like(Uphys[0])
             for j in range(self.ndim):
                 if "conv" in forms:
                     if j == 2:
-                        tmp = dft_inverse(fourier_grad_z(P, U[i]))
+                        tmp = self._inverse32(fourier_grad_z(P, U[i]))
                     else:
                         tmp = grad(P.M, Uphys[i], j)
                     n -= Uphys[j] * tmp
                 if "cons" in forms:
                     tmp = Uphys[i] * Uphys[j]
                     if j == 2:
-                        tmp = dft_inverse(fourier_grad_z(P, dft_forward(tmp)))
+                        tmp = self._inverse32(fourier_grad_z(P, self._forward32(tmp)))
                     else:
                         tmp = grad(P.M, tmp, j)
                     n -= tmp
             if len(forms) == 2:
                 n *= 0.5
-            n = dft_forward(n)
+            n = self._forward32(n)
             N.append(smooth(P, self.vel[0], n))
         if self.advection == 1:
             self.toggle = 1 - self.toggle

@@ -102,6 +102,14 @@ struct stx_dns {
   const double* h_ny = nullptr;
   std::vector<double*> un_lvl, hop_lvl;
   size_t hsize = 0;  // doubles per level
+  // 3/2-rule products (token DEALIAS, N_Z > 2): physical fields on nz32 =
+  // 3 N_Z / 2 planes (AuxField::transform32, src/auxfield.cpp:1197-1258).
+  int nz32 = 0;
+  double* twiddle32 = nullptr;
+  std::vector<double*> Up32;               // [ncom] padded physical velocities
+  double* A32 = nullptr;                   // padded nonlinear terms
+  double* B32 = nullptr;                   // padded z-derivative term (convective)
+  double* C32 = nullptr;                   // padded product / z-derivative term (conservative)
 };
 
 namespace {
@@ -115,23 +123,89 @@ void copy(stx_dns* d, double* dst, const double* src) {
   ck(cudaMemcpyAsync(dst, src, sizeof(double) * d->fsize, cudaMemcpyDeviceToDevice, d->ctx->stream), "copy");
 }
 
+// AuxField::transform32 INVERSE: Fourier f (N_Z planes) zero-padded to nz32
+// planes, inverse transform of length nz32, into out.
+void inverse32(stx_dns* d, const double* f, double* out) {
+  stx_context* ctx = d->ctx;
+  const size_t ps = ctx->M.plane_size, nz = ctx->M.nz;
+  ck(cudaMemcpyAsync(out, f, sizeof(double) * nz * ps, cudaMemcpyDeviceToDevice, ctx->stream), "pad");
+  ck(cudaMemsetAsync(out + nz * ps, 0, sizeof(double) * (d->nz32 - nz) * ps, ctx->stream), "pad");
+  ck(z_transform(out, d->nz32, ctx->M.plane_size, STX_INVERSE, d->twiddle32, nullptr, ctx->stream), "transform32");
+}
+
+// AuxField::transform32 FORWARD: transform of length nz32 in place, the first
+// N_Z planes copied to out (or left in place when out is null).
+void forward32(stx_dns* d, double* io, double* out) {
+  stx_context* ctx = d->ctx;
+  const size_t ps = ctx->M.plane_size, nz = ctx->M.nz;
+  ck(z_transform(io, d->nz32, ctx->M.plane_size, STX_FORWARD, d->twiddle32, nullptr, ctx->stream), "transform32");
+  if (out) ck(cudaMemcpyAsync(out, io, sizeof(double) * nz * ps, cudaMemcpyDeviceToDevice, ctx->stream), "truncate");
+}
+
+// The same nonlinear terms with every product on the 3/2-padded z grid.
+void nonlinear32(stx_dns* d, int form) {
+  stx_context* ctx = d->ctx;
+  DevGeom g32 = ctx->dg;
+  g32.nz = d->nz32;
+  cudaStream_t st = ctx->stream;
+  for (int i = 0; i < d->ncom; ++i) {
+    copy(d, d->Us[0][i], d->u[i]);
+    inverse32(d, d->u[i], d->Up32[i]);
+  }
+  const DevNumbering& Nm = ctx->fields.at(d->names[0]).dn;
+  for (int i = 0; i < d->ncom; ++i) {
+    double* N = d->Uf[0][i];
+    if (form < 0) {
+      ck(cudaMemsetAsync(N, 0, sizeof(double) * d->fsize, st), "zero");
+    } else {
+      NonlinearArgs a{};
+      a.U0 = d->Up32[0];
+      a.U1 = d->Up32[1];
+      a.U2 = d->Up32[2];
+      a.Ui = d->Up32[i];
+      a.N = d->A32;
+      a.form = form;
+      if (form != 2) {  // u_j grad: w * IFFT32(dz U_i)
+        ck(dns_grad_z(ctx->dg, d->Us[0][i], d->tmp0, d->beta, st), "gradz");
+        inverse32(d, d->tmp0, d->B32);
+        a.Tc = d->B32;
+      }
+      if (form != 1) {  // div(uu): IFFT32(dz FFT32(u_i w))
+        ck(dns_product(g32, d->Up32[i], d->Up32[2], d->C32, st), "product");
+        forward32(d, d->C32, nullptr);
+        ck(dns_grad_z(ctx->dg, d->C32, d->tmp1, d->beta, st), "gradz");
+        inverse32(d, d->tmp1, d->C32);
+        a.Tk = d->C32;
+      }
+      ck(dns_nonlinear(g32, a, st), "nonlinear");
+      forward32(d, d->A32, N);
+    }
+    ck(dns_smooth(ctx->dg, Nm, N, d->dsswork, st), "smooth");
+  }
+}
+
 // Nonlinear terms N(u) into Uf[0], copy of u into Us[0] (dns/nonlinear.cpp).
 void nonlinear(stx_dns* d) {
   stx_context* ctx = d->ctx;
   const DevGeom& g = ctx->dg;
   cudaStream_t st = ctx->stream;
   const bool z3 = d->ndim == 3;
-  for (int i = 0; i < d->ncom; ++i) {
-    copy(d, d->Us[0][i], d->u[i]);
-    copy(d, d->Up[i], d->u[i]);
-    transform(d, d->Up[i], STX_INVERSE);
-  }
   int form;  // 0 skew, 1 convective, 2 conservative, -1 Stokes
   switch (d->form) {
     case 0: form = 0; break;
     case 1: form = d->toggle ? 1 : 2; break;
     case 2: form = 1; break;
     default: form = -1; break;
+  }
+  if (d->nz32) {
+    nonlinear32(d, form);
+    if (d->form == 1) d->toggle = 1 - d->toggle;
+    return;
+  }
+  for (int i = 0; i < d->ncom; ++i) {
+    copy(d, d->Us[0][i], d->u[i]);
+    copy(d, d->Up[i], d->u[i]);
+    transform(d, d->Up[i], STX_INVERSE);
   }
   const DevNumbering& Nm = ctx->fields.at(d->names[0]).dn;
   for (int i = 0; i < d->ncom; ++i) {
@@ -335,6 +409,23 @@ int stx_dns_create(stx_context* ctx, int advection, stx_dns** out) {
       bool td = false;
       for (const auto& E : ctx->fields.at(c).N.edges) td = td || depends_on_t(E.expr);
       d->tdep.push_back(td);
+    }
+    // -- 3/2-rule products: padded buffers and the length-nz32 twiddles
+    if (S.tokens.has("DEALIAS") && S.tokens.ivalue("DEALIAS") > 0 && g.nz > 2) {
+      d->nz32 = 3 * g.nz / 2;
+      const size_t n32 = static_cast<size_t>(d->nz32) * g.plane_size;
+      double* pb = static_cast<double*>(d->arena.alloc(sizeof(double) * n32 * (d->ncom + 3)));
+      for (int i = 0; i < d->ncom; ++i) d->Up32.push_back(pb + n32 * i);
+      d->A32 = pb + n32 * d->ncom;
+      d->B32 = d->A32 + n32;
+      d->C32 = d->B32 + n32;
+      std::vector<double> tw(2 * d->nz32);
+      for (int m = 0; m < d->nz32; ++m) {
+        tw[m] = std::cos(2.0 * M_PI * m / d->nz32);
+        tw[d->nz32 + m] = std::sin(2.0 * M_PI * m / d->nz32);
+      }
+      d->twiddle32 = static_cast<double*>(d->arena.alloc(sizeof(double) * tw.size()));
+      ck(cudaMemcpy(d->twiddle32, tw.data(), sizeof(double) * tw.size(), cudaMemcpyHostToDevice), "twiddle");
     }
     // -- high-order pressure BC edges and storage (BCmgr::buildComputedBCs,
     //    src/bcmgr.cpp:937-996)

@@ -138,3 +138,36 @@ def test_channel_c5_builder(tmp_path):
     Do = O.DNS(P, ic)
     Do.advance(6)
     _compare(p, gpu, Do)
+
+
+@pytest.mark.parametrize("advection", [0, 1, 2])
+def test_dealiased_products(tmp_path, advection):
+    # Token DEALIAS: every nonlinear product on the 3/2-padded z grid
+    # (AuxField::transform32 semantics, src/auxfield.cpp:1197-1258), against
+    # the oracle's restatement of the same rule.
+    p = sessions.taylor_green_session(str(tmp_path / "tgd"), 3, 6, 8, re=100.0, dt=2e-3, nstep=6,
+                                      extra={"TOL_REL": 1e-14, "DEALIAS": 1})
+    gpu, t = S.dns(p, advection=advection)
+    D = O.dns_session(p, advection=advection)
+    assert D.dealias
+    _compare(p, gpu, D)
+    plain = O.dns_session(p, {"DEALIAS": 0}, advection=advection).physical()
+    assert max(np.abs(plain[c] - gpu[c]).max() for c in "uvw") > 1e-12   # the rule changed the result
+
+
+def test_dealiased_channel_high_order_pressure(tmp_path):
+    p = sessions.channel_session(str(tmp_path / "c5d"), 4, 2, 6, 8, nstep=6,
+                                 extra={"TOL_REL": 1e-14, "DEALIAS": 1})
+    ctx = S.Context(p)
+    x, y = ctx.mesh_coords()
+    ic = sessions.channel_initial(x, y, np.arange(ctx.nz) * 2 * np.pi / ctx.nz, amplitude=0.1)
+    D = S.DNS(ctx, 1)
+    D.restart(ic, 0.0)
+    D.advance(6)
+    gpu = {c: D.field(c) for c in ctx.fields}
+    D.close()
+    ctx.close()
+    Do = O.DNS(O.Problem(O.read_session(p)), ic)
+    assert Do.dealias
+    Do.advance(6)
+    _compare(p, gpu, Do)

@@ -97,3 +97,19 @@ def test_gll_operators():
     assert abs(w.sum() - 2) < 1e-14
     for p in range(8):
         assert np.abs(D @ z ** p - (p * z ** (p - 1) if p else 0 * z)).max() < 1e-12
+
+
+def test_three_halves_rule_removes_aliases():
+    """transform32 semantics (src/auxfield.cpp:1197-1258): cos 3z cos 2z on 8
+    planes aliases its mode-5 half onto mode 3; on the padded grid it does not."""
+    S = O.read_session(os.path.join(SESSIONS, "taylor3"), {"N_Z": 8})
+    P = O.Problem(S)
+    D = O.DNS(P, dealias=True)
+    z = np.arange(8) * 2 * np.pi / 8
+    shape = (1, P.nel, P.np, P.np)
+    F = O.dft_forward(np.cos(3 * z)[:, None, None, None] * np.ones(shape))
+    G = O.dft_forward(np.cos(2 * z)[:, None, None, None] * np.ones(shape))
+    prod = D._forward32(D._inverse32(F) * D._inverse32(G))
+    plain = O.dft_forward(O.dft_inverse(F) * O.dft_inverse(G))
+    assert abs(prod[2] - 0.25).max() < 1e-15 and abs(prod[6]).max() < 1e-15
+    assert abs(plain[6] - 0.25).max() < 1e-15
