@@ -350,6 +350,7 @@ def run_ours(args):
         "clocks": clocks, "cpu_baseline": cpu,
     }
     if args.dns_steps > 0 and ws == 1:
+        line["mixed"] = run_mixed(ctx, sysm, F, args, flush, stream, dof)
         line["dns"] = run_dns(args.dns_steps, 3, local, "c3")
         line["dns_c3_dealiased"] = run_dns(args.dns_steps, 3, local, "c3d")
         line["dns_c5"] = run_dns(args.dns_steps, 3, local, "c5")
@@ -357,6 +358,49 @@ def run_ours(args):
     print(json.dumps(line))
     if ws > 1:
         torch.distributed.destroy_process_group()
+
+
+def run_mixed(ctx, sysm, F, args, flush, stream, dof):
+    """The same c2 solve with STX_MIXED: the skeleton solve's packed inverses
+    in FP32 (sums in FP64) and two FP64 iterative refinements of the skeleton
+    solution.  Same timing rules as the FP64 line; the error is the relative
+    L2 difference from the FP64 solution of the same forcing (which matches
+    the oracle to 1e-10)."""
+    import ctypes as C
+    import torch
+    import semtex_b200 as S
+    from semtex_b200 import _lib
+    L = _lib.lib()
+    w = WORKLOAD
+    sysx = S.ModalMatrixSys(ctx, "c", w["lambda2"], w["beta"], method=S.MIXED)
+    U64, U32 = ctx.new_field("u64"), ctx.new_field("u32")
+    _lib.check(L.stx_field_solve(sysm.handle, F.ptr(), U64.ptr(), C.c_double(1e-12), 1000, None))
+
+    def solve():
+        _lib.check(L.stx_field_solve(sysx.handle, F.ptr(), U32.ptr(), C.c_double(1e-12), 1000, None))
+
+    for _ in range(args.warmup):
+        solve()
+    torch.cuda.synchronize()
+    ev = [(torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)) for _ in range(args.steps)]
+    for e0, e1 in ev:
+        with torch.cuda.stream(stream):
+            flush.fill_(1.0)
+        e0.record(stream)
+        solve()
+        e1.record(stream)
+    torch.cuda.synchronize()
+    t = sum(e0.elapsed_time(e1) for e0, e1 in ev) / 1e3
+    err = float(torch.linalg.norm(U32.data - U64.data) / torch.linalg.norm(U64.data))
+    launches = C.c_int()
+    _lib.check(L.stx_modal_launches(sysx.handle, C.byref(launches)))
+    out = {"metric": METRIC.replace("plain FP64 direct", "FP32 skeleton inverses + FP64 refinement"),
+           "value": dof * args.steps / t, "unit": UNIT, "ms_per_step": 1e3 * t / args.steps,
+           "refinements": 2,
+           "rel_l2_vs_fp64": err, "dtype": "f32 matrices, f64 sums / residuals / refinement",
+           "gpu_launches": int(launches.value) * args.steps}
+    sysx.close()
+    return out
 
 
 DNS_WORKLOADS = {
@@ -502,7 +546,8 @@ def main():
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--dns-steps", type=int, default=20,
-                    help="timed steps of the secondary DNS measurement (0 to skip)")
+                    help="timed steps of the secondary measurements (mixed-precision c2, DNS c3 / c5, "
+                         "batch c4); 0 skips them")
     ap.add_argument("--mode-groups", type=int, default=0,
                     help="Fourier-mode groups solved on parallel streams (0: library default)")
     ap.add_argument("--solver", default="twolevel", choices=["twolevel", "band"],

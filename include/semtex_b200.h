@@ -36,6 +36,12 @@ extern "C" {
 
 #define STX_DIRECT 0 /* SolverKind DIRECT  (src/matrix.h:6-9) */
 #define STX_JACPCG 1 /* SolverKind JACPCG                     */
+/* DIRECT with the skeleton solve's packed inverses held in FP32 (sums in
+ * FP64) and STX_REFINE (token, default 2; 0 = none, for error studies) FP64
+ * iterative refinements of the skeleton solution, residuals from the FP64
+ * element Schur complements.  Needs the two-level skeleton solve and a
+ * non-singular system. */
+#define STX_MIXED 2
 
 #define STX_FORWARD 1  /* femlib/cfemdef.h FORWARD */
 #define STX_INVERSE -1 /* femlib/cfemdef.h INVERSE */
@@ -194,7 +200,8 @@ int stx_dns_field_ptr(stx_dns* dns, char field, double** d_ptr);
 
 /* ---- Batches of independent solves --------------------------------------
  * The reference solves one problem per `elliptic` run (elliptic/drive.cpp:
- * 61-96: one Field::solve).  stx_batch_create captures n DIRECT solves --
+ * 61-96: one Field::solve).  stx_batch_create captures n DIRECT (or MIXED)
+ * solves --
  * stx_field_solve(systems[i], d_forcing[i], d_unknown[i]) each on its own
  * context's stream -- as one CUDA graph whose independent problems are
  * parallel branches; it runs every solve once first, outside the capture

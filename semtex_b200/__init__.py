@@ -22,13 +22,13 @@ import os
 import numpy as np
 
 from . import _lib
-from ._lib import FORWARD, INVERSE, STX_DIRECT, STX_JACPCG, StxError, check, lib
+from ._lib import FORWARD, INVERSE, STX_DIRECT, STX_JACPCG, STX_MIXED, StxError, check, lib
 from .fieldfile import read_field, write_field
 
-DIRECT, JACPCG = STX_DIRECT, STX_JACPCG
+DIRECT, JACPCG, MIXED = STX_DIRECT, STX_JACPCG, STX_MIXED
 
 __all__ = ["Context", "ModalMatrixSys", "Field", "DNS", "Batch", "numbering", "elliptic", "dns", "read_field",
-           "write_field", "FORWARD", "INVERSE", "DIRECT", "JACPCG", "StxError"]
+           "write_field", "FORWARD", "INVERSE", "DIRECT", "JACPCG", "MIXED", "StxError"]
 
 
 def _torch():

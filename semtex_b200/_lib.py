@@ -15,7 +15,7 @@ LIB_PATH = os.path.join(HERE, "libsemtex_b200.so")
 HEADER = os.path.join(HERE, "..", "include", "semtex_b200.h")
 
 STX_OK, STX_EINVAL, STX_ESESSION, STX_ENUMERIC, STX_ECUDA, STX_ENOCONV, STX_EUNSUPPORTED = range(7)
-STX_DIRECT, STX_JACPCG = 0, 1
+STX_DIRECT, STX_JACPCG, STX_MIXED = 0, 1, 2
 FORWARD, INVERSE = 1, -1
 
 _p = C.c_void_p

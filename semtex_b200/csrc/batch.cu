@@ -78,7 +78,7 @@ int stx_batch_create(stx_modal* const* systems, const double* const* d_forcing, 
     const int device = systems[0] ? systems[0]->ctx->device : 0;
     for (int i = 0; i < n; ++i) {
       if (!systems[i] || !d_forcing[i] || !d_unknown[i]) throw BatchError(STX_EINVAL, "null system or buffer");
-      if (systems[i]->method != STX_DIRECT) throw BatchError(STX_EINVAL, "batched solves are DIRECT");
+      if (systems[i]->method == STX_JACPCG) throw BatchError(STX_EINVAL, "batched solves are DIRECT or MIXED");
       if (systems[i]->ctx->device != device) throw BatchError(STX_EINVAL, "systems on different devices");
     }
     ck(cudaSetDevice(device), "cudaSetDevice");

@@ -414,7 +414,9 @@ int stx_modal_create(stx_context* ctx, char field, double lambda2, double beta, 
     *out = nullptr;
     auto it = ctx->fields.find(field);
     if (it == ctx->fields.end()) throw StxError(STX_EINVAL, std::string("no field ") + field);
-    if (method != STX_DIRECT && method != STX_JACPCG) throw StxError(STX_EINVAL, "unknown method");
+    if (method != STX_DIRECT && method != STX_JACPCG && method != STX_MIXED)
+      throw StxError(STX_EINVAL, "unknown method");
+    const bool direct = method != STX_JACPCG;  // DIRECT, or DIRECT with FP32 skeleton matrices
     const int nmode_total = (ctx->M.nz + 1) / 2;
     if (base_mode != 0 || num_modes != nmode_total)
       throw StxError(STX_EINVAL, "a single-device context holds all modes: base 0, nz/2 modes");
@@ -437,7 +439,7 @@ int stx_modal_create(stx_context* ctx, char field, double lambda2, double beta, 
       auto st = std::make_shared<ModalStore>();
       const Mesh& M = ctx->M;
       const Patching* P = nullptr;
-      if (method == STX_DIRECT) P = ctx->patching(field);
+      if (direct) P = ctx->patching(field);
       std::vector<ModeSystem> modes(num_modes);
       std::vector<std::string> errs(num_modes);
       const unsigned hw = std::max(1u, std::thread::hardware_concurrency());
@@ -481,7 +483,7 @@ int stx_modal_create(stx_context* ctx, char field, double lambda2, double beta, 
       d.l2 = 0;
       d.ew = d.eb = nullptr;
       d.ew_ld = d.eb_ld = 0;
-      if (method == STX_DIRECT) {
+      if (direct) {
         // Element operators for the element kernels, per family and mode
         // (rows zero-padded to element_ld): the recovery operator row i, with
         // columns in the natural node order of the recovery's columns,
@@ -514,7 +516,7 @@ int stx_modal_create(stx_context* ctx, char field, double lambda2, double beta, 
         d.ew_ld = ldw;
         d.eb_ld = ldc;
       }
-      if (method == STX_DIRECT && P) {
+      if (direct && P) {
         // Two-level data: the patch-interior inverses S_II^-1 (one per patch
         // family and mode) and the interface inverse (one per mode), packed
         // symmetric; the element Schur complements (rows padded to
@@ -585,7 +587,20 @@ int stx_modal_create(stx_context* ctx, char field, double lambda2, double beta, 
         d.pin = upload(st->arena, pin);
         d.hbi = upload(st->arena, hbi);
         d.hii = upload(st->arena, hii);
-        d.l2_pack = upload(st->arena, pack.empty() ? std::vector<double>(32, 0.0) : pack);
+        if (method == STX_MIXED) {
+          // FP32 copies of the packed matrices (same entry offsets) and the
+          // number of FP64 refinement steps (token STX_REFINE, default 2)
+          for (int m = 0; m < num_modes; ++m)
+            if (pin[m] >= 0) throw StxError(STX_EUNSUPPORTED, "mixed precision needs a non-singular system");
+          std::vector<float> p32(pack.begin(), pack.end());
+          if (p32.empty()) p32.assign(32, 0.0f);
+          d.l2_pack32 = upload(st->arena, p32);
+          d.l2_pack = nullptr;
+          d.refine = ctx->S.tokens.has("STX_REFINE") ? ctx->S.tokens.ivalue("STX_REFINE") : 2;
+          if (d.refine < 0) throw StxError(STX_EINVAL, "STX_REFINE must be at least 0");
+        } else {
+          d.l2_pack = upload(st->arena, pack.empty() ? std::vector<double>(32, 0.0) : pack);
+        }
         d.l2_sc = upload(st->arena, sc);
         d.l2_sc_ld = ldsc;
         d.l2_ncode = upload(st->arena, ncode);
@@ -660,7 +675,7 @@ int stx_modal_create(stx_context* ctx, char field, double lambda2, double beta, 
           v.npts = 0;
           v.fwd = v.bwd = v.dinv_fwd = v.dinv_bwd = nullptr;
         }
-      } else if (method == STX_DIRECT) {
+      } else if (direct) {
         // Device band layout: rows padded to an even stride (16-byte rows for
         // bulk copies), modes 256-byte aligned, plus the inverse of every
         // 16x16 diagonal block of each triangular factor.
@@ -745,7 +760,7 @@ int stx_field_solve(stx_modal* sys, const double* d_forcing, double* d_unknown, 
     stx_context* ctx = sys->ctx;
     FieldDev& F = ctx->fields.at(sys->field);
     cudaSetDevice(ctx->device);
-    if (sys->method == STX_DIRECT) {
+    if (sys->method != STX_JACPCG) {
       double* work = ctx->workspace(helmholtz_workspace_doubles(ctx->dg, F.dn, sys->store->dm));
       const auto& groups = sys->store->groups;
       if (groups.size() > 1) {
@@ -785,7 +800,7 @@ int stx_field_solve_profiled(stx_modal* sys, const double* d_forcing, double* d_
                              float* phase_ms, int* launches) {
   return guarded([&] {
     if (!sys || !d_forcing || !d_unknown || !phase_ms) throw StxError(STX_EINVAL, "null argument");
-    if (sys->method != STX_DIRECT) throw StxError(STX_EINVAL, "profiled solve is for DIRECT systems");
+    if (sys->method == STX_JACPCG) throw StxError(STX_EINVAL, "profiled solve is for DIRECT systems");
     stx_context* ctx = sys->ctx;
     FieldDev& F = ctx->fields.at(sys->field);
     cudaSetDevice(ctx->device);
@@ -806,7 +821,7 @@ int stx_field_solve_profiled(stx_modal* sys, const double* d_forcing, double* d_
 int stx_modal_launches(const stx_modal* sys, int* launches) {
   return guarded([&] {
     if (!sys || !launches) throw StxError(STX_EINVAL, "null argument");
-    if (sys->method != STX_DIRECT) throw StxError(STX_EINVAL, "launch count is for DIRECT systems");
+    if (sys->method == STX_JACPCG) throw StxError(STX_EINVAL, "launch count is for DIRECT systems");
     const stx_context* ctx = sys->ctx;
     const auto& groups = sys->store->groups;
     const int per = helmholtz_direct_launches(ctx->fields.at(sys->field).dn, sys->store->dm, ctx->M.np);

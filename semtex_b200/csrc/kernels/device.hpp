@@ -120,6 +120,11 @@ struct DevModal {
   int l2_sc_ld;
   const int* l2_ncode;            // [nel][next], elements in chunk order: skeleton id << 2 | class
                                   // (0 essential, 1 patch-interior, 2 interface node)
+  // Mixed precision (l2_pack32 set): the packed matrices of l2_pack held in
+  // FP32 at the same entry offsets, and `refine` FP64 residual corrections
+  // of the skeleton solution.
+  const float* l2_pack32;
+  int refine;
 };
 
 }  // namespace stx

@@ -443,7 +443,9 @@ __global__ void __launch_bounds__(32 * kMaxWarps, 1)
 // family-mode matrix S_e (rows padded) and the chunk's input columns (the
 // source values at the element nodes of the taken class, zero elsewhere)
 // in shared memory; out = S_e x on the tensor cores; the rows of the put
-// class are subtracted from dst.
+// class are subtracted from dst.  dir 0: patch-interior -> interface,
+// 1: interface -> patch-interior, 2: every non-essential node both ways
+// (dst -= S x, the skeleton residual).
 __global__ void __launch_bounds__(256)
     k_elem_schur(int dir, DevGeom g, DevNumbering N, DevModal S, const double* __restrict__ src,
                  double* __restrict__ dst, int rstride) {
@@ -459,6 +461,7 @@ __global__ void __launch_bounds__(256)
   double* sB = sA + next * lda;                               // [2 cm][ldb]
   int* sN = reinterpret_cast<int*>(sB + 2 * g.chunk_max * ldb);  // [cm][next] skeleton id << 2 | class
   const int take = dir == 0 ? 1 : 2, put = dir == 0 ? 2 : 1;
+  const bool every = dir == 2;
   const double* A = S.l2_sc + (static_cast<size_t>(m) * S.nfamily + cd.z) * next * lda;
   for (int i = threadIdx.x; i < next * lda; i += blockDim.x) sA[i] = __ldg(A + i);
   const int wp = threadIdx.x >> 5, ln = threadIdx.x & 31, nwp = blockDim.x >> 5;
@@ -478,7 +481,7 @@ __global__ void __launch_bounds__(256)
       for (int h = 0; h < 2; ++h) {
         const int a = ln + 32 * h;
         const int code_v = (col < ncol && a < next) ? sN[l * next + a] : 0;
-        v[j][h] = (code_v & 3) == take ? sp[code_v >> 2] : 0.0;
+        v[j][h] = (every ? (code_v & 3) != 0 : (code_v & 3) == take) ? sp[code_v >> 2] : 0.0;
       }
     }
 #pragma unroll
@@ -507,7 +510,7 @@ __global__ void __launch_bounds__(256)
           int slot, l;
           col_slot(col, cnt, slot, l);
           const int code_v = sN[l * next + row];
-          if ((code_v & 3) == put)
+          if (every ? (code_v & 3) != 0 : (code_v & 3) == put)
             atomicAdd(&dst[static_cast<size_t>(2 * m + slot) * rstride + (code_v >> 2)], -acc[j][i]);
         }
       }

@@ -79,6 +79,13 @@ __global__ void k_essential(DevGeom g, DevNumbering N, const double* __restrict_
   G[static_cast<size_t>(k) * gstride + N.edge_gid[idx]] = lines[static_cast<size_t>(k) * nline + idx];
 }
 
+// y += x over n entries.
+__global__ void k_add(double* __restrict__ y, const double* __restrict__ x, size_t n) {
+  for (size_t i = blockIdx.x * static_cast<size_t>(blockDim.x) + threadIdx.x; i < n;
+       i += static_cast<size_t>(gridDim.x) * blockDim.x)
+    y[i] += x[i];
+}
+
 __global__ void k_natural(DevGeom g, DevNumbering N, const double* __restrict__ lines,
                           int nline, double* __restrict__ R, int rstride, int nz, int k0) {
   const int idx = blockIdx.x * blockDim.x + threadIdx.x;
@@ -910,13 +917,21 @@ SweepPlan sweep_plan(int nbp, int nband) {
 
 size_t helmholtz_workspace_doubles(const DevGeom& g, const DevNumbering& N, const DevModal& S) {
   const size_t stride = (static_cast<size_t>(N.nglobal) + 31) / 32 * 32;
-  return 2 * stride * g.nz + (S.l2 ? twolevel_workspace_doubles(static_cast<int>(stride), g.nz) : 0);
+  size_t n = 2 * stride * g.nz;
+  if (S.l2) {
+    n += twolevel_workspace_doubles(static_cast<int>(stride), g.nz);
+    // mixed precision: the condensed right-hand side, the residual and the
+    // correction's solve
+    if (S.refine > 0) n += 2 * stride * g.nz + twolevel_workspace_doubles(static_cast<int>(stride), g.nz);
+  }
+  return n;
 }
 
 int helmholtz_direct_launches(const DevNumbering& N, const DevModal& S, int np) {
   const bool has_ess = N.nglobal > N.nsolve;
   const int nedge_nodes = N.nedge * np;
-  return 2 + (S.l2 ? twolevel_launches(S) : 2) + (has_ess && nedge_nodes ? 1 : 0) + (nedge_nodes ? 1 : 0);
+  const int refine = S.l2 ? S.refine * (twolevel_launches(S) + 2) : 0;
+  return 2 + (S.l2 ? twolevel_launches(S) : 2) + (has_ess && nedge_nodes ? 1 : 0) + (nedge_nodes ? 1 : 0) + refine;
 }
 
 cudaError_t helmholtz_direct_solve(const DevGeom& g, const DevNumbering& N, const DevModal& S,
@@ -972,9 +987,29 @@ cudaError_t helmholtz_direct_solve(const DevGeom& g, const DevNumbering& N, cons
   const double* Rsol = R;  // skeleton solution
   if (S.l2) {
     double* w2 = work + 2 * static_cast<size_t>(rstride) * nz;
-    err = twolevel_solve(S, g, N, R, rstride, w2, nz, st, ev ? ev[2] : nullptr);
+    // mixed precision: skeleton products with FP32 matrices, then `refine`
+    // corrections  Y += S^-1_32 (R - S Y)  whose residual uses the FP64
+    // element Schur complements (the operator the FP64 inverses invert)
+    const bool mixed = S.l2_pack32 != nullptr;
+    const size_t off = static_cast<size_t>(rstride) * k0;
+    double* R0 = w2 + twolevel_workspace_doubles(rstride, nz);
+    double* rr = R0 + static_cast<size_t>(rstride) * nz;
+    double* w3 = rr + static_cast<size_t>(rstride) * nz;
+    if (mixed && S.refine > 0)
+      err = cudaMemcpyAsync(R0 + off, R + off, sizeof(double) * pz, cudaMemcpyDeviceToDevice, st);
+    if (err == cudaSuccess) err = twolevel_solve(S, g, N, R, rstride, w2, nz, st, ev ? ev[2] : nullptr, mixed);
     if (err != cudaSuccess) return err;
-    Rsol = twolevel_solution(w2, rstride, nz);
+    double* Y = twolevel_solution(w2, rstride, nz);
+    for (int it = 0; it < S.refine; ++it) {
+      err = cudaMemcpyAsync(rr + off, R0 + off, sizeof(double) * pz, cudaMemcpyDeviceToDevice, st);
+      if (err != cudaSuccess) return err;
+      element_schur_apply(2, g, N, S, Y, rr, rstride, st);
+      err = twolevel_solve(S, g, N, rr, rstride, w3, nz, st, nullptr, true);
+      if (err != cudaSuccess) return err;
+      const double* D = twolevel_solution(w3, rstride, nz);
+      k_add<<<(static_cast<unsigned>(pz) + 255) / 256, 256, 0, st>>>(Y + off, D + off, pz);
+    }
+    Rsol = Y;
   } else if (plan.stages >= 2) {
     static int configured = 0;
     if (!configured) {

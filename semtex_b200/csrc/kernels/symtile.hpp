@@ -1,12 +1,13 @@
 // Packed storage of a symmetric n x n matrix for the tiled products of the
 // two-level skeleton solve: the lower triangle of 32 x 32 tiles (I >= J),
 // tile-row-major, the last tile row only as tall as the matrix needs
-// (h = n - 32 (T - 1) rows, stored rounded up to even).  Diagonal tiles hold
-// both triangles; columns past n are zero.  Within a tile, row r occupies 33
-// doubles (entry (r, c) at r*33 + c, the 33rd zero), so that a warp reading
-// a tile row (lanes over c) or a tile column (lanes over r) touches every
-// bank pair once and every address is a constant offset.  Tiles are
-// multiples of 16 bytes and start on 16-byte boundaries: one bulk copy each.
+// (h = n - 32 (T - 1) rows, stored rounded up to a multiple of 4).  Diagonal
+// tiles hold both triangles; columns past n are zero.  Within a tile, row r
+// occupies 33 entries (entry (r, c) at r*33 + c, the 33rd zero), so that a
+// warp reading a tile row (lanes over c) or a tile column (lanes over r)
+// touches every bank once and every address is a constant offset.  Offsets
+// and sizes count entries; with doubles or floats alike every tile is a
+// multiple of 16 bytes and starts on a 16-byte boundary: one bulk copy each.
 #pragma once
 
 #include <cstddef>
@@ -22,12 +23,12 @@ __host__ __device__ inline int sym_last_rows(int n) { return n - kSymTile * (sym
 
 // Rows of tile row I, and rows stored for it.
 __host__ __device__ inline int sym_rows(int n, int I) { return I < sym_tiles(n) - 1 ? kSymTile : sym_last_rows(n); }
-__host__ __device__ inline int sym_rows_stored(int n, int I) { return (sym_rows(n, I) + 1) / 2 * 2; }
+__host__ __device__ inline int sym_rows_stored(int n, int I) { return (sym_rows(n, I) + 3) / 4 * 4; }
 
 // Doubles of the packed matrix.
 __host__ __device__ inline long long sym_size(int n) {
   if (n <= 0) return 0;
-  const long long T = sym_tiles(n), hs = (sym_last_rows(n) + 1) / 2 * 2;
+  const long long T = sym_tiles(n), hs = (sym_last_rows(n) + 3) / 4 * 4;
   return (T - 1) * T / 2 * kSymTile * kSymLd + T * hs * kSymLd;
 }
 
@@ -70,12 +71,12 @@ inline void sym_pack(int n, const double* A, size_t lda, double* out) {
 
 // General (rectangular) nr x nc matrices in the same tile format: all
 // T_r x T_c tiles, tile-row-major, last tile row stored as tall as needed
-// (rounded up to even), columns past nc zero.
+// (rounded up to a multiple of 4), columns past nc zero.
 __host__ __device__ inline int gen_ntiles(int nr, int nc) { return sym_tiles(nr) * sym_tiles(nc); }
 
 __host__ __device__ inline long long gen_size(int nr, int nc) {
   if (nr <= 0 || nc <= 0) return 0;
-  const long long Tr = sym_tiles(nr), Tc = sym_tiles(nc), hs = (sym_last_rows(nr) + 1) / 2 * 2;
+  const long long Tr = sym_tiles(nr), Tc = sym_tiles(nc), hs = (sym_last_rows(nr) + 3) / 4 * 4;
   return (Tr - 1) * Tc * kSymTile * kSymLd + Tc * hs * kSymLd;
 }
 

@@ -14,7 +14,8 @@
 // S_II^-1 and A^-1 are symmetric and stored packed, G in tiles
 // (symtile.hpp); each product streams its tiles with bulk copies, the Re and
 // Im planes of a mode sharing every tile read, a symmetric tile applied as
-// itself and as its transpose.
+// itself and as its transpose.  Tiles are read as doubles, or as floats for
+// the mixed-precision solve (the same layout; sums in FP64 either way).
 #include "twolevel.cuh"
 
 #include <algorithm>
@@ -84,8 +85,9 @@ struct SymCursor {
 // independent partial sums per plane; y_I is accumulated along the row and
 // added at its end.  Waits are bounded; on expiry `status` is set and the
 // warp stops.
+template <class T>
 __global__ void __launch_bounds__(32 * kSymWarps)
-    k_psymv(const double* __restrict__ pack, const SymProblem* __restrict__ probs, const SymWarp* __restrict__ warps,
+    k_psymv(const T* __restrict__ pack, const SymProblem* __restrict__ probs, const SymWarp* __restrict__ warps,
             int nwarps, const double* __restrict__ X, double* __restrict__ Y, int rstride, int nz, int* status) {
   extern __shared__ __align__(16) unsigned char sraw[];
   const int wp = threadIdx.x >> 5, ln = threadIdx.x & 31;
@@ -121,7 +123,7 @@ __global__ void __launch_bounds__(32 * kSymWarps)
     const int n = ic.P.n, m = ic.P.mode;
     const bool two = nz > 1 && m > 0;
     if (ln == 0) {
-      const unsigned bytes = static_cast<unsigned>(sizeof(double) * kSymLd * sym_rows_stored(n, ic.I));
+      const unsigned bytes = static_cast<unsigned>(sizeof(T) * kSymLd * sym_rows_stored(n, ic.I));
       mbar_expect_tx(&sm.bar[s], bytes);
       bulk_g2s(sm.tile[s], pack + ic.P.moff + ic.offset(), bytes, &sm.bar[s]);
     }
@@ -156,7 +158,7 @@ __global__ void __launch_bounds__(32 * kSymWarps)
     const int n = cc.P.n, m = cc.P.mode, I = cc.I, J = cc.J;
     const bool two = nz > 1 && m > 0, sym = cc.P.ncol == 0;
     const double scale = cc.P.scale;
-    const double* A = sm.tile[s];
+    const T* A = reinterpret_cast<const T*>(sm.tile[s]);
     const double2* xs = sm.x[s];
     const int h = sym_rows(n, I);
     // output positions (column block for the transposed part, row block at a
@@ -165,11 +167,11 @@ __global__ void __launch_bounds__(32 * kSymWarps)
     const int g_col = (sym && J < I) ? __ldg(cc.P.idx + kSymTile * J + ln) : 0;  // J < T - 1: a full tile column
     const int g_row = (row_end && ln < h) ? __ldg(cc.P.idx + kSymTile * I + ln) : 0;
     if (ln < h) {
-      const double* Ar = A + ln * kSymLd;
+      const T* Ar = A + ln * kSymLd;
       double p0[4] = {0.0, 0.0, 0.0, 0.0}, p1[4] = {0.0, 0.0, 0.0, 0.0};
 #pragma unroll
       for (int c = 0; c < kSymTile; ++c) {
-        const double a = Ar[c];
+        const double a = static_cast<double>(Ar[c]);
         const double2 x = xs[c];
         p0[c & 3] = fma(a, x.x, p0[c & 3]);
         p1[c & 3] = fma(a, x.y, p1[c & 3]);
@@ -184,14 +186,14 @@ __global__ void __launch_bounds__(32 * kSymWarps)
       if (h == kSymTile) {
 #pragma unroll
         for (int r = 0; r < kSymTile; ++r) {
-          const double a = A[r * kSymLd + ln];
+          const double a = static_cast<double>(A[r * kSymLd + ln]);
           const double2 x = xs[kSymTile + r];
           p0[r & 3] = fma(a, x.x, p0[r & 3]);
           p1[r & 3] = fma(a, x.y, p1[r & 3]);
         }
       } else {
         for (int r = 0; r < h; ++r) {
-          const double a = A[r * kSymLd + ln];
+          const double a = static_cast<double>(A[r * kSymLd + ln]);
           const double2 x = xs[kSymTile + r];
           p0[0] = fma(a, x.x, p0[0]);
           p1[0] = fma(a, x.y, p1[0]);
@@ -215,16 +217,26 @@ __global__ void __launch_bounds__(32 * kSymWarps)
   for (int k = done; k < issued; ++k) mbar_wait(&sm.bar[k % kSymStages], (k / kSymStages) & 1);
 }
 
-cudaError_t launch_psymv(const DevModal& S, const SymProblem* probs, const SymWarp* warps, int nwarps,
-                         const double* X, double* Y, int rstride, int nz, cudaStream_t st) {
-  if (nwarps <= 0) return cudaSuccess;
+void configure_psymv() {
   static bool configured = false;
   if (!configured) {
-    cudaFuncSetAttribute(k_psymv, cudaFuncAttributeMaxDynamicSharedMemorySize, static_cast<int>(kSymSmem));
+    cudaFuncSetAttribute(k_psymv<double>, cudaFuncAttributeMaxDynamicSharedMemorySize, static_cast<int>(kSymSmem));
+    cudaFuncSetAttribute(k_psymv<float>, cudaFuncAttributeMaxDynamicSharedMemorySize, static_cast<int>(kSymSmem));
     configured = true;
   }
-  k_psymv<<<(nwarps + kSymWarps - 1) / kSymWarps, 32 * kSymWarps, kSymSmem, st>>>(S.l2_pack, probs, warps, nwarps,
-                                                                                   X, Y, rstride, nz, S.status);
+}
+
+cudaError_t launch_psymv(const DevModal& S, const SymProblem* probs, const SymWarp* warps, int nwarps,
+                         const double* X, double* Y, int rstride, int nz, bool fp32, cudaStream_t st) {
+  if (nwarps <= 0) return cudaSuccess;
+  configure_psymv();
+  const int blocks = (nwarps + kSymWarps - 1) / kSymWarps;
+  if (fp32)
+    k_psymv<float><<<blocks, 32 * kSymWarps, kSymSmem, st>>>(S.l2_pack32, probs, warps, nwarps, X, Y, rstride, nz,
+                                                             S.status);
+  else
+    k_psymv<double><<<blocks, 32 * kSymWarps, kSymSmem, st>>>(S.l2_pack, probs, warps, nwarps, X, Y, rstride, nz,
+                                                              S.status);
   return cudaGetLastError();
 }
 
@@ -233,7 +245,7 @@ cudaError_t launch_psymv(const DevModal& S, const SymProblem* probs, const SymWa
 size_t twolevel_workspace_doubles(int rstride, int nz) { return static_cast<size_t>(rstride) * nz; }
 
 cudaError_t twolevel_solve(const DevModal& S, const DevGeom& g, const DevNumbering& N, double* R, int rstride,
-                           double* work, int nz, cudaStream_t st, cudaEvent_t mid) {
+                           double* work, int nz, cudaStream_t st, cudaEvent_t mid, bool fp32) {
   double* Yv = twolevel_solution(work, rstride, nz);  // y_I, then the whole skeleton solution
   // planes of the launch's modes
   const int k0 = nz > 1 ? 2 * S.mode0 : 0, k1 = nz > 1 ? std::min(nz, 2 * (S.mode0 + S.nmodes)) : 1;
@@ -241,15 +253,15 @@ cudaError_t twolevel_solve(const DevModal& S, const DevGeom& g, const DevNumberi
                                     sizeof(double) * rstride * (k1 - k0), st);
   if (err != cudaSuccess) return err;
   // y_I = S_II^-1 R_I; r_B = R_B - S_BI y_I
-  err = launch_psymv(S, S.prob_patch, S.warp_patch, S.nwarp_patch, R, Yv, rstride, nz, st);
+  err = launch_psymv(S, S.prob_patch, S.warp_patch, S.nwarp_patch, R, Yv, rstride, nz, fp32, st);
   if (err != cudaSuccess) return err;
   element_schur_apply(0, g, N, S, Yv, R, rstride, st);
   // x_B = A^-1 r_B (into the interface positions of Y)
-  err = launch_psymv(S, S.prob_iface, S.warp_iface, S.nwarp_iface, R, Yv, rstride, nz, st);
+  err = launch_psymv(S, S.prob_iface, S.warp_iface, S.nwarp_iface, R, Yv, rstride, nz, fp32, st);
   if (err != cudaSuccess) return err;
   if (mid) cudaEventRecord(mid, st);
   // x_I = y_I - G x_B, G = S_II^-1 S_IB
-  err = launch_psymv(S, S.prob_gen, S.warp_gen, S.nwarp_gen, Yv, Yv, rstride, nz, st);
+  err = launch_psymv(S, S.prob_gen, S.warp_gen, S.nwarp_gen, Yv, Yv, rstride, nz, fp32, st);
   if (err != cudaSuccess) return err;
   return cudaGetLastError();
 }
@@ -267,8 +279,8 @@ std::vector<SymWarp> sym_schedule(const std::vector<SymProblem>& probs, int devi
   if (total == 0) return out;
   int sms = 148, per_sm = 1;
   cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, device);
-  cudaFuncSetAttribute(k_psymv, cudaFuncAttributeMaxDynamicSharedMemorySize, static_cast<int>(kSymSmem));
-  if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_psymv, 32 * kSymWarps, kSymSmem) != cudaSuccess ||
+  configure_psymv();
+  if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_psymv<double>, 32 * kSymWarps, kSymSmem) != cudaSuccess ||
       per_sm < 1)
     per_sm = 1;
   const long long nw = std::min<long long>(total, static_cast<long long>(sms) * per_sm * kSymWarps);

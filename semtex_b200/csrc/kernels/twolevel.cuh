@@ -15,9 +15,9 @@ size_t twolevel_workspace_doubles(int rstride, int nz);
 // Skeleton vectors R[k][0..nglobal) of every solved plane hold the condensed
 // right-hand sides on entry (R is overwritten); the skeleton solution is left
 // in twolevel_solution(work, ...).  `mid` (optional) is recorded after the
-// interface products.
+// interface products.  fp32: the matrices are read from S.l2_pack32.
 cudaError_t twolevel_solve(const DevModal& S, const DevGeom& g, const DevNumbering& N, double* R, int rstride,
-                           double* work, int nz, cudaStream_t st, cudaEvent_t mid = nullptr);
+                           double* work, int nz, cudaStream_t st, cudaEvent_t mid = nullptr, bool fp32 = false);
 
 inline double* twolevel_solution(double* work, int /*rstride*/, int /*nz*/) { return work; }
 

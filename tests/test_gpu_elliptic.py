@@ -97,3 +97,26 @@ def test_transform_roundtrip_odd_factors(tmp_path, nz):
     assert rel_l2(F.to_numpy(), O.dft_forward(f)) < 1e-14
     F.transform(S.INVERSE)
     assert rel_l2(F.to_numpy(), f) < 1e-14
+
+
+@pytest.mark.parametrize("n,np_,nz,perturb", [(8, 9, 8, 0.0), (8, 7, 6, 0.3)])
+def test_mixed_precision_refined(tmp_path, n, np_, nz, perturb):
+    """STX_MIXED: FP32 skeleton matrices (FP64 sums) with FP64 iterative
+    refinement on the skeleton system reaches the FP64 oracle to 1e-10 (the
+    default two refinements); without refinement (STX_REFINE = 0) the FP32
+    matrices alone leave an error above 1e-9, so the refinement does the work."""
+    p, ctx, f = _random_case(tmp_path, n, np_, nz, seed=n * 10 + np_, perturb=perturb)
+    plain = S.ModalMatrixSys(ctx, "c", 1.0).solve_host(f)
+    mixed = S.ModalMatrixSys(ctx, "c", 1.0, method=S.MIXED).solve_host(f)
+    P, U = O.elliptic(p, forcing_phys=f)
+    assert rel_l2(plain, U) < TOL
+    assert rel_l2(mixed, U) < TOL, rel_l2(mixed, U)
+    ctx0 = S.Context(p, overrides={"STX_REFINE": 0})
+    none = S.ModalMatrixSys(ctx0, "c", 1.0, method=S.MIXED).solve_host(f)
+    assert rel_l2(none, U) > 1e-9, rel_l2(none, U)
+
+
+def test_mixed_precision_rejects_singular_systems():
+    ctx = S.Context(os.path.join(SESSIONS, "taylor2"))
+    with pytest.raises(S.StxError):
+        S.ModalMatrixSys(ctx, "p", 0.0, method=S.MIXED)
