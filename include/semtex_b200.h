@@ -155,6 +155,16 @@ int stx_field_solve_profiled(stx_modal* sys, const double* d_forcing, double* d_
  * stx_field_solve. */
 int stx_field_solve_noalloc(stx_modal* sys, const double* d_forcing, double* d_unknown);
 
+/* Field::solve for n fields at once, e.g. the velocity components of a
+ * viscous substep (dns/integrate.cpp:186-193): solution i of systems[i] with
+ * forcing d_forcing[i] (each field its own BC lines).  When the systems
+ * share their matrices (equal constants and numbering: stx_modal_create
+ * shares the storage) and n <= 3, one skeleton solve reads every matrix
+ * tile once for all of them; otherwise the solves run one after another.
+ * DIRECT (or MIXED, solved one by one) systems of one context. */
+int stx_field_solve_multi(stx_modal* const* systems, int n, const double* const* d_forcing,
+                          double* const* d_unknown);
+
 /* AuxField::transform(sign) (src/auxfield.cpp:1157-1194) in place on nz
  * device planes of plane_size doubles. */
 int stx_transform(stx_context* ctx, double* d_data, int sign);

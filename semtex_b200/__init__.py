@@ -27,7 +27,7 @@ from .fieldfile import read_field, write_field
 
 DIRECT, JACPCG, MIXED = STX_DIRECT, STX_JACPCG, STX_MIXED
 
-__all__ = ["Context", "ModalMatrixSys", "Field", "DNS", "Batch", "numbering", "elliptic", "dns", "read_field",
+__all__ = ["Context", "ModalMatrixSys", "Field", "DNS", "Batch", "numbering", "solve_multi", "elliptic", "dns", "read_field",
            "write_field", "FORWARD", "INVERSE", "DIRECT", "JACPCG", "MIXED", "StxError"]
 
 
@@ -224,6 +224,16 @@ class ModalMatrixSys:
         check(lib().stx_elliptic_solve_host(self._h, C.c_void_p(f.ctypes.data),
                                             C.c_void_p(out.ctypes.data)))
         return out
+
+
+def solve_multi(systems, forcings, unknowns):
+    """Field::solve of several fields at once (stx_field_solve_multi): systems
+    sharing their matrices read every skeleton matrix tile once for all."""
+    n = len(systems)
+    sy = (C.c_void_p * n)(*[s.handle.value for s in systems])
+    fr = (C.c_void_p * n)(*[f.ptr().value for f in forcings])
+    un = (C.c_void_p * n)(*[u.ptr().value for u in unknowns])
+    check(lib().stx_field_solve_multi(sy, n, fr, un))
 
 
 class Batch:

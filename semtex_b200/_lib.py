@@ -45,6 +45,7 @@ SIGNATURES = {
     "stx_transform": (_i, [_p, _p, _i]),
     "stx_field_solve_profiled": (_i, [_p, _p, _p, C.POINTER(C.c_float), _pi]),
     "stx_field_solve_noalloc": (_i, [_p, _p, _p]),
+    "stx_field_solve_multi": (_i, [_p, _i, _p, _p]),
     "stx_modal_bytes": (_i, [_p, _pd]),
     "stx_modal_launches": (_i, [_p, _pi]),
     "stx_dns_create": (_i, [_p, _i, C.POINTER(_p)]),

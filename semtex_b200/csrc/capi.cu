@@ -796,6 +796,60 @@ int stx_field_solve(stx_modal* sys, const double* d_forcing, double* d_unknown, 
   });
 }
 
+int stx_field_solve_multi(stx_modal* const* systems, int n, const double* const* d_forcing,
+                          double* const* d_unknown) {
+  return guarded([&] {
+    if (!systems || !d_forcing || !d_unknown || n < 1) throw StxError(STX_EINVAL, "bad argument");
+    for (int f = 0; f < n; ++f)
+      if (!systems[f] || !d_forcing[f] || !d_unknown[f]) throw StxError(STX_EINVAL, "null system or buffer");
+    stx_context* ctx = systems[0]->ctx;
+    bool shared = n <= 3;
+    for (int f = 0; f < n; ++f) {
+      if (systems[f]->ctx != ctx) throw StxError(STX_EINVAL, "systems of different contexts");
+      if (systems[f]->method == STX_JACPCG) throw StxError(STX_EINVAL, "multi-field solves are DIRECT");
+      shared = shared && systems[f]->store == systems[0]->store;
+    }
+    cudaSetDevice(ctx->device);
+    std::vector<const DevNumbering*> N(n);
+    std::vector<const double*> lines(n);
+    std::vector<int> nline(n);
+    for (int f = 0; f < n; ++f) {
+      const FieldDev& F = ctx->fields.at(systems[f]->field);
+      N[f] = &F.dn;
+      lines[f] = F.d_lines;
+      nline[f] = F.nline;
+    }
+    const ModalStore& st = *systems[0]->store;
+    if (n == 1 || !shared || !helmholtz_fields_supported(ctx->dg, *N[0], st.dm)) {
+      for (int f = 0; f < n; ++f) {
+        const int rc = stx_field_solve(systems[f], d_forcing[f], d_unknown[f], 0.0, 0, nullptr);
+        if (rc != STX_OK) throw StxError(rc, stx_last_error());
+      }
+      return;
+    }
+    double* work = ctx->workspace(helmholtz_fields_workspace_doubles(ctx->dg, *N[0], n));
+    const auto& groups = st.groups;
+    if (groups.size() > 1) {
+      ctx->ensure_aux(groups.size() - 1);
+      cuda_check(cudaEventRecord(ctx->aux_ev[0], ctx->stream), "fork");
+      for (size_t k = 1; k < groups.size(); ++k)
+        cuda_check(cudaStreamWaitEvent(ctx->aux[k - 1], ctx->aux_ev[0], 0), "fork wait");
+      for (size_t k = 0; k < groups.size(); ++k)
+        cuda_check(helmholtz_direct_solve_fields(ctx->dg, N.data(), groups[k], d_forcing, d_unknown, lines.data(),
+                                                 nline.data(), n, work, k ? ctx->aux[k - 1] : ctx->stream),
+                   "multi-field solve");
+      for (size_t k = 1; k < groups.size(); ++k) {
+        cuda_check(cudaEventRecord(ctx->aux_ev[k], ctx->aux[k - 1]), "join");
+        cuda_check(cudaStreamWaitEvent(ctx->stream, ctx->aux_ev[k], 0), "join wait");
+      }
+    } else {
+      cuda_check(helmholtz_direct_solve_fields(ctx->dg, N.data(), st.dm, d_forcing, d_unknown, lines.data(),
+                                               nline.data(), n, work, ctx->stream),
+                 "multi-field solve");
+    }
+  });
+}
+
 int stx_field_solve_profiled(stx_modal* sys, const double* d_forcing, double* d_unknown,
                              float* phase_ms, int* launches) {
   return guarded([&] {

@@ -340,6 +340,20 @@ void advance_one(stx_dns* d) {
   // -- velocity BCs, viscous substep (dns/integrate.cpp:177-193, 328-356)
   for (int i = 0; i < d->ncom; ++i)
     if (d->tdep[i]) ckstx(stx_field_bc_evaluate(ctx, d->names[i], d->time));
+  // direct systems sharing their matrices: one skeleton solve for all
+  // components (every matrix tile read once)
+  bool shared = d->step >= d->nord && d->ncom <= 3;
+  for (int i = 1; i < d->ncom; ++i) shared = shared && d->vsys[i]->store == d->vsys[0]->store;
+  if (shared) {
+    const double* F[3];
+    double* U[3];
+    for (int i = 0; i < d->ncom; ++i) {
+      F[i] = d->Uf[0][i];
+      U[i] = d->u[i];
+    }
+    ckstx(stx_field_solve_multi(d->vsys.data(), d->ncom, F, U));
+    return;
+  }
   for (int i = 0; i < d->ncom; ++i) {
     stx_modal* sys = d->vsys[i];
     if (d->step < d->nord) {

@@ -1039,6 +1039,54 @@ cudaError_t helmholtz_direct_solve(const DevGeom& g, const DevNumbering& N, cons
   return cudaGetLastError();
 }
 
+bool helmholtz_fields_supported(const DevGeom& g, const DevNumbering& N, const DevModal& S) {
+  return S.l2 && !S.l2_pack32 && S.refine == 0 && element_plan(g, S, N.nglobal > N.nsolve).ok;
+}
+
+size_t helmholtz_fields_workspace_doubles(const DevGeom& g, const DevNumbering& N, int nf) {
+  const size_t stride = (static_cast<size_t>(N.nglobal) + 31) / 32 * 32;
+  return 3 * stride * g.nz * nf;
+}
+
+cudaError_t helmholtz_direct_solve_fields(const DevGeom& g, const DevNumbering* const* N, const DevModal& S,
+                                          const double* const* F, double* const* U, const double* const* lines,
+                                          const int* nline, int nf, double* work, cudaStream_t st) {
+  if (nf < 1 || nf > 3 || !helmholtz_fields_supported(g, *N[0], S)) return cudaErrorInvalidValue;
+  const int rstride = (N[0]->nglobal + 31) / 32 * 32;
+  const int nz = g.nz;
+  const size_t fs = static_cast<size_t>(rstride) * nz;  // field stride of each region
+  double* R = work;             // [nf] skeleton right-hand sides
+  double* G = R + nf * fs;      // [nf] essential values
+  double* Y = G + nf * fs;      // [nf] skeleton solutions
+  const int k0 = nz > 1 ? 2 * S.mode0 : 0, k1 = nz > 1 ? std::min(nz, 2 * (S.mode0 + S.nmodes)) : 1;
+  const size_t pz = static_cast<size_t>(rstride) * (k1 - k0), off = static_cast<size_t>(rstride) * k0;
+  const bool has_ess = N[0]->nglobal > N[0]->nsolve;
+  const ElementPlan ep = element_plan(g, S, has_ess);
+  cudaError_t err = cudaSuccess;
+  for (int f = 0; f < nf; ++f) {
+    double* Rf = R + f * fs;
+    double* Gf = G + f * fs;
+    err = cudaMemsetAsync(Rf + off, 0, sizeof(double) * pz, st);
+    if (err == cudaSuccess) err = cudaMemsetAsync(Gf + off, 0, sizeof(double) * pz, st);
+    if (err != cudaSuccess) return err;
+    const int nedge_nodes = N[f]->nedge * g.np;
+    if (has_ess && nedge_nodes) {
+      dim3 grid((nedge_nodes + 127) / 128, k1 - k0);
+      k_essential<<<grid, 128, 0, st>>>(g, *N[f], lines[f], nline[f], Gf, rstride, nz, k0);
+    }
+    element_condense(ep, g, *N[f], S, F[f], has_ess ? Gf : nullptr, rstride, Rf, rstride, st);
+    if (nedge_nodes) {
+      dim3 grid((nedge_nodes + 127) / 128, k1 - k0);
+      k_natural<<<grid, 128, 0, st>>>(g, *N[f], lines[f], nline[f], Rf, rstride, nz, k0);
+    }
+  }
+  err = twolevel_solve_fields(S, g, *N[0], R, Y, fs, nf, rstride, nz, st);
+  if (err != cudaSuccess) return err;
+  for (int f = 0; f < nf; ++f)
+    element_recover(ep, g, *N[f], S, F[f], has_ess ? G + f * fs : nullptr, rstride, Y + f * fs, rstride, U[f], st);
+  return cudaGetLastError();
+}
+
 }  // namespace stx
 
 namespace stx {

@@ -27,6 +27,18 @@ cudaError_t helmholtz_direct_solve(const DevGeom& g, const DevNumbering& N, cons
                                    double* work, cudaStream_t st,
                                    cudaEvent_t* phase_events = nullptr);
 
+// The direct solve of nf (1..3) fields whose systems share S (the same
+// matrices: equal constants and numbering; each field its own forcing, BC
+// lines and DevNumbering): per-field condensation and recovery, one skeleton
+// solve reading every matrix tile once for all fields.  Needs the two-level
+// path with the element kernels and FP64 matrices
+// (helmholtz_fields_supported); scratch helmholtz_fields_workspace_doubles.
+bool helmholtz_fields_supported(const DevGeom& g, const DevNumbering& N, const DevModal& S);
+size_t helmholtz_fields_workspace_doubles(const DevGeom& g, const DevNumbering& N, int nf);
+cudaError_t helmholtz_direct_solve_fields(const DevGeom& g, const DevNumbering* const* N, const DevModal& S,
+                                          const double* const* F, double* const* U, const double* const* lines,
+                                          const int* nline, int nf, double* work, cudaStream_t st);
+
 // Number of kernel launches one direct solve issues.
 int helmholtz_direct_launches(const DevNumbering& N, const DevModal& S, int np);
 

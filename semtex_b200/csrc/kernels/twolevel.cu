@@ -33,13 +33,17 @@ constexpr int kSymStages = 2;  // tile buffers per warp
 constexpr int kTileDoubles = kSymTile * kSymLd;
 
 // Shared memory per warp: barriers, tile ring, x entries of each buffered
-// tile (32 of its column block, 32 of its row block, both planes).
+// tile (32 of its column block, 32 of its row block, both planes of each of
+// NF fields that share the matrices).
+template <int NF>
 struct SymWarpSmem {
   uint64_t bar[kSymStages];
-  double2 x[kSymStages][2 * kSymTile];
+  double2 x[kSymStages][2 * kSymTile * NF];
   double tile[kSymStages][kTileDoubles];
 };
-constexpr size_t kSymSmem = kSymWarps * sizeof(SymWarpSmem);
+template <int NF>
+constexpr size_t sym_smem() { return kSymWarps * sizeof(SymWarpSmem<NF>); }
+constexpr size_t kSymSmem = sym_smem<1>();
 
 // Position of a warp in the tiles of its problems.
 struct SymCursor {
@@ -76,7 +80,8 @@ struct SymCursor {
   }
 };
 
-// y[idx] += scale A x[idx] for every problem: each warp streams its run of tiles
+// y[idx] += scale A x[idx] for every problem (and each of NF fields whose
+// vectors are fstride doubles apart): each warp streams its run of tiles
 // (SymWarp) through a two-buffer ring.  For a tile, lane 0 bulk-copies the
 // tile and every lane copies (cp.async) the x entries of the tile's column
 // and row blocks, all completing on the buffer's mbarrier (count 1 + 32).
@@ -85,15 +90,16 @@ struct SymCursor {
 // independent partial sums per plane; y_I is accumulated along the row and
 // added at its end.  Waits are bounded; on expiry `status` is set and the
 // warp stops.
-template <class T>
+template <class T, int NF>
 __global__ void __launch_bounds__(32 * kSymWarps)
     k_psymv(const T* __restrict__ pack, const SymProblem* __restrict__ probs, const SymWarp* __restrict__ warps,
-            int nwarps, const double* __restrict__ X, double* __restrict__ Y, int rstride, int nz, int* status) {
+            int nwarps, const double* __restrict__ X, double* __restrict__ Y, int rstride, size_t fstride, int nz,
+            int* status) {
   extern __shared__ __align__(16) unsigned char sraw[];
   const int wp = threadIdx.x >> 5, ln = threadIdx.x & 31;
   const int gw = blockIdx.x * kSymWarps + wp;
   if (gw >= nwarps) return;  // the warps of a block never synchronise with each other
-  SymWarpSmem& sm = reinterpret_cast<SymWarpSmem*>(sraw)[wp];
+  SymWarpSmem<NF>& sm = reinterpret_cast<SymWarpSmem<NF>*>(sraw)[wp];
   const SymWarp W = warps[gw];
   SymCursor ic, cc;  // issue and consume cursors
   ic.load(probs, W.prob, W.q);
@@ -132,13 +138,16 @@ __global__ void __launch_bounds__(32 * kSymWarps)
 #pragma unroll
     for (int h = 0; h < 2; ++h) {
       const int gi = pf[h];
-      double2* d = &sm.x[s][kSymTile * h + ln];
-      if (gi >= 0) {
-        cp_async8(&d->x, X0 + gi);
-        if (two) cp_async8(&d->y, X1 + gi);
-        else d->y = 0.0;
-      } else {
-        *d = make_double2(0.0, 0.0);
+#pragma unroll
+      for (int f = 0; f < NF; ++f) {
+        double2* d = &sm.x[s][(kSymTile * h + ln) * NF + f];
+        if (gi >= 0) {
+          cp_async8(&d->x, X0 + f * fstride + gi);
+          if (two) cp_async8(&d->y, X1 + f * fstride + gi);
+          else d->y = 0.0;
+        } else {
+          *d = make_double2(0.0, 0.0);
+        }
       }
     }
     cp_async_arrive_noinc(&sm.bar[s]);
@@ -147,7 +156,9 @@ __global__ void __launch_bounds__(32 * kSymWarps)
     if (issued < W.count) prefetch();
   };
   for (int s = 0; s < kSymStages && s < W.count; ++s) issue(s);
-  double d0 = 0.0, d1 = 0.0;  // direct part of row 32 I + ln
+  double d0[NF], d1[NF];  // direct part of row 32 I + ln
+#pragma unroll
+  for (int f = 0; f < NF; ++f) d0[f] = d1[f] = 0.0;
   int done = 0;
   for (; done < W.count; ++done) {
     const int s = done % kSymStages;
@@ -168,46 +179,73 @@ __global__ void __launch_bounds__(32 * kSymWarps)
     const int g_row = (row_end && ln < h) ? __ldg(cc.P.idx + kSymTile * I + ln) : 0;
     if (ln < h) {
       const T* Ar = A + ln * kSymLd;
-      double p0[4] = {0.0, 0.0, 0.0, 0.0}, p1[4] = {0.0, 0.0, 0.0, 0.0};
+      double p0[NF][4], p1[NF][4];
+#pragma unroll
+      for (int f = 0; f < NF; ++f)
+#pragma unroll
+        for (int u = 0; u < 4; ++u) p0[f][u] = p1[f][u] = 0.0;
 #pragma unroll
       for (int c = 0; c < kSymTile; ++c) {
         const double a = static_cast<double>(Ar[c]);
-        const double2 x = xs[c];
-        p0[c & 3] = fma(a, x.x, p0[c & 3]);
-        p1[c & 3] = fma(a, x.y, p1[c & 3]);
+#pragma unroll
+        for (int f = 0; f < NF; ++f) {
+          const double2 x = xs[c * NF + f];
+          p0[f][c & 3] = fma(a, x.x, p0[f][c & 3]);
+          p1[f][c & 3] = fma(a, x.y, p1[f][c & 3]);
+        }
       }
-      d0 += (p0[0] + p0[1]) + (p0[2] + p0[3]);
-      d1 += (p1[0] + p1[1]) + (p1[2] + p1[3]);
+#pragma unroll
+      for (int f = 0; f < NF; ++f) {
+        d0[f] += (p0[f][0] + p0[f][1]) + (p0[f][2] + p0[f][3]);
+        d1[f] += (p1[f][0] + p1[f][1]) + (p1[f][2] + p1[f][3]);
+      }
     }
     double* Y0 = Y + static_cast<size_t>(2 * m) * rstride;
     double* Y1 = Y0 + rstride;
     if (sym && J < I) {
-      double p0[4] = {0.0, 0.0, 0.0, 0.0}, p1[4] = {0.0, 0.0, 0.0, 0.0};
+      double p0[NF][4], p1[NF][4];
+#pragma unroll
+      for (int f = 0; f < NF; ++f)
+#pragma unroll
+        for (int u = 0; u < 4; ++u) p0[f][u] = p1[f][u] = 0.0;
       if (h == kSymTile) {
 #pragma unroll
         for (int r = 0; r < kSymTile; ++r) {
           const double a = static_cast<double>(A[r * kSymLd + ln]);
-          const double2 x = xs[kSymTile + r];
-          p0[r & 3] = fma(a, x.x, p0[r & 3]);
-          p1[r & 3] = fma(a, x.y, p1[r & 3]);
+#pragma unroll
+          for (int f = 0; f < NF; ++f) {
+            const double2 x = xs[(kSymTile + r) * NF + f];
+            p0[f][r & 3] = fma(a, x.x, p0[f][r & 3]);
+            p1[f][r & 3] = fma(a, x.y, p1[f][r & 3]);
+          }
         }
       } else {
         for (int r = 0; r < h; ++r) {
           const double a = static_cast<double>(A[r * kSymLd + ln]);
-          const double2 x = xs[kSymTile + r];
-          p0[0] = fma(a, x.x, p0[0]);
-          p1[0] = fma(a, x.y, p1[0]);
+#pragma unroll
+          for (int f = 0; f < NF; ++f) {
+            const double2 x = xs[(kSymTile + r) * NF + f];
+            p0[f][0] = fma(a, x.x, p0[f][0]);
+            p1[f][0] = fma(a, x.y, p1[f][0]);
+          }
         }
       }
-      atomicAdd(&Y0[g_col], scale * ((p0[0] + p0[1]) + (p0[2] + p0[3])));
-      if (two) atomicAdd(&Y1[g_col], scale * ((p1[0] + p1[1]) + (p1[2] + p1[3])));
+#pragma unroll
+      for (int f = 0; f < NF; ++f) {
+        atomicAdd(&Y0[f * fstride + g_col], scale * ((p0[f][0] + p0[f][1]) + (p0[f][2] + p0[f][3])));
+        if (two) atomicAdd(&Y1[f * fstride + g_col], scale * ((p1[f][0] + p1[f][1]) + (p1[f][2] + p1[f][3])));
+      }
     }
     if (row_end) {
       if (ln < h) {
-        atomicAdd(&Y0[g_row], scale * d0);
-        if (two) atomicAdd(&Y1[g_row], scale * d1);
+#pragma unroll
+        for (int f = 0; f < NF; ++f) {
+          atomicAdd(&Y0[f * fstride + g_row], scale * d0[f]);
+          if (two) atomicAdd(&Y1[f * fstride + g_row], scale * d1[f]);
+        }
       }
-      d0 = d1 = 0.0;
+#pragma unroll
+      for (int f = 0; f < NF; ++f) d0[f] = d1[f] = 0.0;
     }
     __syncwarp();
     if (issued < W.count) issue(s);  // the buffer's reads are complete (syncwarp)
@@ -220,23 +258,36 @@ __global__ void __launch_bounds__(32 * kSymWarps)
 void configure_psymv() {
   static bool configured = false;
   if (!configured) {
-    cudaFuncSetAttribute(k_psymv<double>, cudaFuncAttributeMaxDynamicSharedMemorySize, static_cast<int>(kSymSmem));
-    cudaFuncSetAttribute(k_psymv<float>, cudaFuncAttributeMaxDynamicSharedMemorySize, static_cast<int>(kSymSmem));
+    cudaFuncSetAttribute(k_psymv<double, 1>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                         static_cast<int>(sym_smem<1>()));
+    cudaFuncSetAttribute(k_psymv<float, 1>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                         static_cast<int>(sym_smem<1>()));
+    cudaFuncSetAttribute(k_psymv<double, 2>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                         static_cast<int>(sym_smem<2>()));
+    cudaFuncSetAttribute(k_psymv<double, 3>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                         static_cast<int>(sym_smem<3>()));
     configured = true;
   }
 }
 
 cudaError_t launch_psymv(const DevModal& S, const SymProblem* probs, const SymWarp* warps, int nwarps,
-                         const double* X, double* Y, int rstride, int nz, bool fp32, cudaStream_t st) {
+                         const double* X, double* Y, int rstride, int nz, bool fp32, cudaStream_t st, int nf = 1,
+                         size_t fstride = 0) {
   if (nwarps <= 0) return cudaSuccess;
   configure_psymv();
-  const int blocks = (nwarps + kSymWarps - 1) / kSymWarps;
+  const int blocks = (nwarps + kSymWarps - 1) / kSymWarps, th = 32 * kSymWarps;
   if (fp32)
-    k_psymv<float><<<blocks, 32 * kSymWarps, kSymSmem, st>>>(S.l2_pack32, probs, warps, nwarps, X, Y, rstride, nz,
-                                                             S.status);
+    k_psymv<float, 1><<<blocks, th, sym_smem<1>(), st>>>(S.l2_pack32, probs, warps, nwarps, X, Y, rstride, 0, nz,
+                                                         S.status);
+  else if (nf == 3)
+    k_psymv<double, 3><<<blocks, th, sym_smem<3>(), st>>>(S.l2_pack, probs, warps, nwarps, X, Y, rstride, fstride,
+                                                          nz, S.status);
+  else if (nf == 2)
+    k_psymv<double, 2><<<blocks, th, sym_smem<2>(), st>>>(S.l2_pack, probs, warps, nwarps, X, Y, rstride, fstride,
+                                                          nz, S.status);
   else
-    k_psymv<double><<<blocks, 32 * kSymWarps, kSymSmem, st>>>(S.l2_pack, probs, warps, nwarps, X, Y, rstride, nz,
-                                                              S.status);
+    k_psymv<double, 1><<<blocks, th, sym_smem<1>(), st>>>(S.l2_pack, probs, warps, nwarps, X, Y, rstride, 0, nz,
+                                                          S.status);
   return cudaGetLastError();
 }
 
@@ -266,6 +317,25 @@ cudaError_t twolevel_solve(const DevModal& S, const DevGeom& g, const DevNumberi
   return cudaGetLastError();
 }
 
+cudaError_t twolevel_solve_fields(const DevModal& S, const DevGeom& g, const DevNumbering& N, double* R,
+                                  double* Y, size_t fstride, int nf, int rstride, int nz, cudaStream_t st) {
+  if (nf < 1 || nf > 3 || S.refine > 0 || S.l2_pack32) return cudaErrorInvalidValue;
+  const int k0 = nz > 1 ? 2 * S.mode0 : 0, k1 = nz > 1 ? std::min(nz, 2 * (S.mode0 + S.nmodes)) : 1;
+  cudaError_t err = cudaSuccess;
+  for (int f = 0; f < nf && err == cudaSuccess; ++f)
+    err = cudaMemsetAsync(Y + f * fstride + static_cast<size_t>(rstride) * k0, 0,
+                          sizeof(double) * rstride * (k1 - k0), st);
+  if (err != cudaSuccess) return err;
+  err = launch_psymv(S, S.prob_patch, S.warp_patch, S.nwarp_patch, R, Y, rstride, nz, false, st, nf, fstride);
+  if (err != cudaSuccess) return err;
+  for (int f = 0; f < nf; ++f) element_schur_apply(0, g, N, S, Y + f * fstride, R + f * fstride, rstride, st);
+  err = launch_psymv(S, S.prob_iface, S.warp_iface, S.nwarp_iface, R, Y, rstride, nz, false, st, nf, fstride);
+  if (err != cudaSuccess) return err;
+  err = launch_psymv(S, S.prob_gen, S.warp_gen, S.nwarp_gen, Y, Y, rstride, nz, false, st, nf, fstride);
+  if (err != cudaSuccess) return err;
+  return cudaGetLastError();
+}
+
 int twolevel_launches(const DevModal& S) {
   return (S.nwarp_patch > 0 ? 1 : 0) + (S.nwarp_iface > 0 ? 1 : 0) + (S.nwarp_gen > 0 ? 1 : 0) + 1;
 }
@@ -280,7 +350,8 @@ std::vector<SymWarp> sym_schedule(const std::vector<SymProblem>& probs, int devi
   int sms = 148, per_sm = 1;
   cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, device);
   configure_psymv();
-  if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_psymv<double>, 32 * kSymWarps, kSymSmem) != cudaSuccess ||
+  if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_psymv<double, 1>, 32 * kSymWarps, kSymSmem) !=
+          cudaSuccess ||
       per_sm < 1)
     per_sm = 1;
   const long long nw = std::min<long long>(total, static_cast<long long>(sms) * per_sm * kSymWarps);

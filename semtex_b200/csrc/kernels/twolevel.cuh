@@ -21,6 +21,12 @@ cudaError_t twolevel_solve(const DevModal& S, const DevGeom& g, const DevNumberi
 
 inline double* twolevel_solution(double* work, int /*rstride*/, int /*nz*/) { return work; }
 
+// The same solve for nf (1..3) fields that share the matrices (FP64 only):
+// field f's right-hand sides at R + f fstride, its solution written to
+// Y + f fstride; every tile is read once for all fields.
+cudaError_t twolevel_solve_fields(const DevModal& S, const DevGeom& g, const DevNumbering& N, double* R,
+                                  double* Y, size_t fstride, int nf, int rstride, int nz, cudaStream_t st);
+
 int twolevel_launches(const DevModal& S);
 
 // Split the tiles of `probs` (in order) into equal runs, one per warp of a

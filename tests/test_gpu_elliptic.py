@@ -120,3 +120,38 @@ def test_mixed_precision_rejects_singular_systems():
     ctx = S.Context(os.path.join(SESSIONS, "taylor2"))
     with pytest.raises(S.StxError):
         S.ModalMatrixSys(ctx, "p", 0.0, method=S.MIXED)
+
+
+@pytest.mark.parametrize("nf", [3, 2])
+def test_multi_field_solve_matches_single(tmp_path, nf):
+    """stx_field_solve_multi: velocity systems that share their matrices are
+    solved with one skeleton pass for all fields; the results equal the
+    one-by-one solves (round-off) and the oracle (1e-10)."""
+    p = sessions.channel_session(str(tmp_path / "mf"), 4, 3, 7, 8, extra={"TOL_REL": 1e-14})
+    ctx = S.Context(p)
+    lam = 3.7
+    names = "uvw"[:nf]
+    systems = [S.ModalMatrixSys(ctx, c, lam) for c in names]
+    rng = np.random.default_rng(nf)
+    fs, single, multi, phys = [], [], [], []
+    for c in names:
+        f = rng.uniform(-1, 1, (ctx.nz, ctx.nel, ctx.np, ctx.np))
+        phys.append(f)
+        fs.append(ctx.new_field("f" + c).load_physical(f).transform(S.FORWARD).zero_nyquist())
+        single.append(ctx.new_field("s" + c))
+        multi.append(ctx.new_field("m" + c))
+    for sys_, F, U in zip(systems, fs, single):
+        U.solve(F, sys_)
+    S.solve_multi(systems, fs, multi)
+    P = O.Problem(O.read_session(p))
+    for i, c in enumerate(names):
+        a, b = multi[i].to_numpy(), single[i].to_numpy()
+        assert rel_l2(a, b) < 1e-13, (c, rel_l2(a, b))
+        F = O.dft_forward(phys[i])
+        F[1] = 0.0
+        Uo = P.solve(c, F, np.zeros_like(F), P.modal_systems(c, lam), P.bc_lines(c))
+        Uo[1] = 0.0
+        assert rel_l2(a, Uo) < TOL, (c, rel_l2(a, Uo))
+    for sys_ in systems:
+        sys_.close()
+    ctx.close()
