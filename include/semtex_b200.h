@@ -205,6 +205,15 @@ int stx_dns_get_field(stx_dns* dns, char field, double* h_phys);
 /* Take nsteps time steps (the while loop of integrate()). */
 int stx_dns_advance(stx_dns* dns, int nsteps);
 int stx_dns_state(const stx_dns* dns, int* step, double* time);
+/* Analyser (src/analysis.cpp:329-443), computed on the device from the
+ * current (Fourier) velocity: modal energies per unit area
+ * sum_i AuxField::mode_L2(m) over the DIM components (h_ek: (N_Z+1)/2
+ * values); the divergence energy sum_m mode_L2(m) of div u, divided by
+ * 2 pi / BETA; the CFL inverse time scale max(u.CFL(0), v.CFL(1)[, w.CFL(2)])
+ * of Analyser::estimateCFL (CFL number = inv_dt * D_T). */
+int stx_dns_modal_energy(stx_dns* dns, double* h_ek);
+int stx_dns_divergence_energy(stx_dns* dns, double* value);
+int stx_dns_cfl(stx_dns* dns, double* inv_dt);
 /* Device pointer of a field's Fourier-space storage (nz x plane_size). */
 int stx_dns_field_ptr(stx_dns* dns, char field, double** d_ptr);
 

@@ -1355,6 +1355,41 @@ class DNS:
                                     P.bc_lines(c, self.time), tok["TOL_REL"],
                                     tok.ivalue("STEP_MAX"))
 
+    # -- Analyser (src/analysis.cpp:329-443)
+    def _mode_l2(self, F, m):
+        """AuxField::mode_L2 (src/auxfield.cpp:919-947): sum over elements of
+        Q4-weighted Re^2 + Im^2 of mode m, over twice the area."""
+        Q4 = self.P.M.Q4
+        re = F[2 * m] if self.P.nz > 1 else F[0]
+        ek = (Q4 * re * re).sum()
+        if self.P.nz > 1:
+            ek += (Q4 * F[2 * m + 1] ** 2).sum()
+        return ek / (2.0 * Q4.sum())
+
+    def modal_energy(self):
+        nm = (self.P.nz + 1) // 2
+        return np.array([sum(self._mode_l2(self.u[c], m) for c in self.vel[:self.ndim]) for m in range(nm)])
+
+    def divergence_energy(self):
+        P = self.P
+        div = sum(plane_grad(P, self.u[c], i) for i, c in enumerate(self.vel[:self.ndim]))
+        L2 = sum(self._mode_l2(div, m) for m in range((P.nz + 1) // 2))
+        return L2 / (2 * math.pi / P.S.tokens["BETA"])
+
+    def cfl(self):
+        """Analyser::estimateCFL's inverse time scale (Element::CFL,
+        src/element.cpp:1207-1250; AuxField::CFL, src/auxfield.cpp:1719-1762)."""
+        M, P = self.P.M, self.P
+        d = M.z[1] - M.z[0]
+        out = 0.0
+        for i, (a, b) in enumerate((("drdx", "dsdx"), ("drdy", "dsdy"))):
+            u = self.u[self.vel[i]][0]
+            w = d * np.abs(getattr(M, a)) + d * np.abs(getattr(M, b))
+            out = max(out, np.abs(u / w).max())
+        if self.ncom == 3:
+            out = max(out, np.abs(self.u[self.vel[2]][0]).max() / (2 * math.pi / P.S.tokens["BETA"] / P.nz))
+        return out
+
     def physical(self):
         out = {}
         for c, v in self.u.items():

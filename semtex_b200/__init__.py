@@ -373,6 +373,23 @@ class DNS:
         check(lib().stx_dns_state(self._h, C.byref(s), C.byref(t)))
         return s.value, t.value
 
+    # -- Analyser (src/analysis.cpp:329-443) on the device
+    def modal_energy(self) -> np.ndarray:
+        out = np.zeros((self.ctx.nz + 1) // 2)
+        check(lib().stx_dns_modal_energy(self._h, C.c_void_p(out.ctypes.data)))
+        return out
+
+    def divergence_energy(self) -> float:
+        v = C.c_double()
+        check(lib().stx_dns_divergence_energy(self._h, C.byref(v)))
+        return v.value
+
+    def cfl(self) -> float:
+        """Inverse CFL time scale (Analyser::estimateCFL); CFL number = cfl() * D_T."""
+        v = C.c_double()
+        check(lib().stx_dns_cfl(self._h, C.byref(v)))
+        return v.value
+
 
 def _user_functions(session: str):
     import re

@@ -110,6 +110,7 @@ struct stx_dns {
   double* A32 = nullptr;                   // padded nonlinear terms
   double* B32 = nullptr;                   // padded z-derivative term (convective)
   double* C32 = nullptr;                   // padded product / z-derivative term (conservative)
+  double* part = nullptr;                  // analysis partials: blocks x max(modes, 3)
 };
 
 namespace {
@@ -416,6 +417,8 @@ int stx_dns_create(stx_context* ctx, int advection, stx_dns** out) {
     d->tmp0 = base + d->fsize * k++;
     d->tmp1 = base + d->fsize * k++;
     d->tmp2 = base + d->fsize * k++;
+    d->part = static_cast<double*>(
+        d->arena.alloc(sizeof(double) * dns_analysis_blocks() * std::max((g.nz + 1) / 2, 3)));
     size_t ws = 0;
     for (char c : d->names) ws = std::max(ws, dns_smooth_workspace_doubles(g, ctx->fields.at(c).dn));
     d->dsswork = static_cast<double*>(d->arena.alloc(sizeof(double) * ws));
@@ -569,6 +572,86 @@ int stx_dns_state(const stx_dns* d, int* step, double* time) {
     if (!d) throw DnsError(STX_EINVAL, "null argument");
     if (step) *step = d->step;
     if (time) *time = d->time;
+  });
+}
+
+namespace {
+
+// Q4-weighted energies of every mode of Fourier field f, summed in order.
+std::vector<double> mode_energies(stx_dns* d, const double* f) {
+  stx_context* ctx = d->ctx;
+  const int nb = dns_analysis_blocks(), nm = (ctx->M.nz + 1) / 2;
+  double* part = d->part;
+  ck(dns_mode_energy_partials(ctx->dg, f, part, ctx->stream), "mode energy");
+  std::vector<double> h(static_cast<size_t>(nb) * nm), out(nm, 0.0);
+  ck(cudaMemcpyAsync(h.data(), part, sizeof(double) * h.size(), cudaMemcpyDeviceToHost, ctx->stream), "download");
+  ck(cudaStreamSynchronize(ctx->stream), "sync");
+  for (int m = 0; m < nm; ++m)
+    for (int b = 0; b < nb; ++b) out[m] += h[static_cast<size_t>(m) * nb + b];
+  return out;
+}
+
+double mesh_area(const stx_context* ctx) {
+  double a = 0.0;
+  for (double q : ctx->M.Q4) a += q;
+  return a;
+}
+
+}  // namespace
+
+int stx_dns_modal_energy(stx_dns* d, double* h_ek) {
+  return dns_guarded([&] {
+    if (!d || !h_ek) throw DnsError(STX_EINVAL, "null argument");
+    cudaSetDevice(d->ctx->device);
+    const int nm = (d->ctx->M.nz + 1) / 2;
+    const double area = mesh_area(d->ctx);
+    for (int m = 0; m < nm; ++m) h_ek[m] = 0.0;
+    for (int i = 0; i < d->ndim; ++i) {
+      const std::vector<double> e = mode_energies(d, d->u[i]);
+      for (int m = 0; m < nm; ++m) h_ek[m] += e[m] / (2.0 * area);
+    }
+  });
+}
+
+int stx_dns_divergence_energy(stx_dns* d, double* value) {
+  return dns_guarded([&] {
+    if (!d || !value) throw DnsError(STX_EINVAL, "null argument");
+    stx_context* ctx = d->ctx;
+    cudaSetDevice(ctx->device);
+    ck(dns_divergence(ctx->dg, d->u[0], d->u[1], d->ndim == 3 ? d->u[2] : nullptr, d->tmp1, 1.0, d->beta,
+                      ctx->stream),
+       "divergence");
+    const std::vector<double> e = mode_energies(d, d->tmp1);
+    const double area = mesh_area(ctx);
+    double L2 = 0.0;
+    for (double v : e) L2 += v / (2.0 * area);
+    *value = L2 / (2.0 * M_PI / d->beta);
+  });
+}
+
+int stx_dns_cfl(stx_dns* d, double* inv_dt) {
+  return dns_guarded([&] {
+    if (!d || !inv_dt) throw DnsError(STX_EINVAL, "null argument");
+    stx_context* ctx = d->ctx;
+    cudaSetDevice(ctx->device);
+    const int nb = dns_analysis_blocks();
+    const double dxy = ctx->M.q.z[1] - ctx->M.q.z[0];
+    const int ndir = d->ncom == 3 ? 3 : 2;
+    std::vector<double> h(static_cast<size_t>(nb) * ndir);
+    for (int dir = 0; dir < ndir; ++dir)
+      ck(dns_cfl_partials(ctx->dg, d->u[dir], dir, dxy, d->part + static_cast<size_t>(nb) * dir, ctx->stream),
+         "cfl");
+    ck(cudaMemcpyAsync(h.data(), d->part, sizeof(double) * h.size(), cudaMemcpyDeviceToHost, ctx->stream),
+       "download");
+    ck(cudaStreamSynchronize(ctx->stream), "sync");
+    double c = 0.0;
+    for (int dir = 0; dir < ndir; ++dir) {
+      double m = 0.0;
+      for (int b = 0; b < nb; ++b) m = std::max(m, h[static_cast<size_t>(nb) * dir + b]);
+      if (dir == 2) m /= 2.0 * M_PI / d->beta / ctx->M.nz;
+      c = std::max(c, m);
+    }
+    *inv_dt = c;
   });
 }
 

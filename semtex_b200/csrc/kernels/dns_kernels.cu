@@ -9,6 +9,8 @@
 //   setPForce, project    dns/integrate.cpp:242-289
 //   high-order pressure   BCmgr::maintainFourier / evaluateCNBCp
 //   BCs                   src/bcmgr.cpp:1036-1331, src/edge.cpp:110-256
+//   modal energy, CFL     AuxField::mode_L2 / CFL, Element::CFL
+//                         src/auxfield.cpp:919-947, 1719-1762, src/element.cpp:1207-1250
 //
 // Element kernels run one warp per (element, plane), kEpPlanes planes of one
 // element per block: D is staged once per block, each warp holds its plane's
@@ -166,6 +168,61 @@ __global__ void k_hopbc(DevGeom g, HopbcArgs a) {
   double v = a.ex[0] * hv;
   for (int q = 0; q + 1 < a.Jx; ++q) v += a.ex[q + 1] * a.hop_old[q][pos];
   a.lines[static_cast<size_t>(k) * a.nline + static_cast<size_t>(a.line[h]) * np + r] = v;
+}
+
+// Block sum (kAnaThreads threads) of v into part[slot].
+constexpr int kAnaThreads = 256;
+__device__ __forceinline__ void block_store(double v, double* part, int slot, bool use_max) {
+  __shared__ double red[kAnaThreads / 32];
+  for (int o = 16; o; o >>= 1) {
+    const double w = __shfl_xor_sync(0xffffffffu, v, o);
+    v = use_max ? fmax(v, w) : v + w;
+  }
+  if ((threadIdx.x & 31) == 0) red[threadIdx.x >> 5] = v;
+  __syncthreads();
+  if (threadIdx.x == 0) {
+    double t = red[0];
+    for (int w = 1; w < kAnaThreads / 32; ++w) t = use_max ? fmax(t, red[w]) : t + red[w];
+    part[slot] = t;
+  }
+}
+
+// Per (block, mode m): sum of Q4 (Re^2 + Im^2) over the block's share of the
+// element nodes of mode m (planes 2m, 2m+1; plane 0 alone when nz == 1).
+__global__ void __launch_bounds__(kAnaThreads) k_mode_energy(DevGeom g, const double* __restrict__ f,
+                                                             double* __restrict__ part) {
+  const int m = blockIdx.y;
+  const size_t n = static_cast<size_t>(g.nel) * g.npnp;
+  const double* re = f + static_cast<size_t>(g.nz > 1 ? 2 * m : 0) * g.plane_size;
+  const double* im = g.nz > 1 ? re + g.plane_size : nullptr;
+  double s = 0.0;
+  for (size_t i = blockIdx.x * static_cast<size_t>(blockDim.x) + threadIdx.x; i < n;
+       i += static_cast<size_t>(gridDim.x) * blockDim.x) {
+    const double q = g.Q4[i];
+    s += q * re[i] * re[i];
+    if (im) s += q * im[i] * im[i];
+  }
+  block_store(s, part, m * gridDim.x + blockIdx.x, false);
+}
+
+// Per block: max over plane 0 (the zeroth mode) of |u| / (d (|dr/dx_dir| +
+// |ds/dx_dir|)) for dir 0, 1 (Element::CFL), or of |u| for dir 2.
+__global__ void __launch_bounds__(kAnaThreads) k_cfl(DevGeom g, const double* __restrict__ u, int dir, double d,
+                                                     double* __restrict__ part) {
+  const size_t n = static_cast<size_t>(g.nel) * g.npnp;
+  double s = 0.0;
+  for (size_t i = blockIdx.x * static_cast<size_t>(blockDim.x) + threadIdx.x; i < n;
+       i += static_cast<size_t>(gridDim.x) * blockDim.x) {
+    double v;
+    if (dir == 2) {
+      v = fabs(u[i]);
+    } else {
+      const double w = dir == 0 ? d * fabs(g.drdx[i]) + d * fabs(g.dsdx[i]) : d * fabs(g.drdy[i]) + d * fabs(g.dsdy[i]);
+      v = fabs(u[i] / w);
+    }
+    s = fmax(s, v);
+  }
+  block_store(s, part, blockIdx.x, true);
 }
 
 __global__ void k_grad_z(const double* __restrict__ in, double* __restrict__ out, int nz, int plane_size,
@@ -363,6 +420,19 @@ cudaError_t dns_smooth(const DevGeom& g, const DevNumbering& N, double* io, doub
 
 size_t dns_smooth_workspace_doubles(const DevGeom& g, const DevNumbering& N) {
   return static_cast<size_t>((N.nglobal + 31) / 32 * 32) * g.nz;
+}
+
+int dns_analysis_blocks() { return 64; }
+
+cudaError_t dns_mode_energy_partials(const DevGeom& g, const double* f, double* part, cudaStream_t st) {
+  const int nmodes = (g.nz + 1) / 2;
+  k_mode_energy<<<dim3(dns_analysis_blocks(), nmodes), kAnaThreads, 0, st>>>(g, f, part);
+  return cudaGetLastError();
+}
+
+cudaError_t dns_cfl_partials(const DevGeom& g, const double* u, int dir, double d, double* part, cudaStream_t st) {
+  k_cfl<<<dns_analysis_blocks(), kAnaThreads, 0, st>>>(g, u, dir, d, part);
+  return cudaGetLastError();
 }
 
 size_t dns_hopbc_smem(const DevGeom& g) { return sizeof(double) * (g.np * g.np + 8 * g.npnp); }

@@ -59,6 +59,13 @@ struct HopbcArgs {
 size_t dns_hopbc_smem(const DevGeom& g);
 cudaError_t dns_hopbc(const DevGeom& g, const HopbcArgs& a, cudaStream_t st);
 
+// Analysis reductions, as per-block partials (dns_analysis_blocks() per
+// mode) that the host sums in a fixed order: Q4-weighted energy of every
+// mode of a Fourier field (part[m * blocks + b]); the CFL maxima of plane 0.
+int dns_analysis_blocks();
+cudaError_t dns_mode_energy_partials(const DevGeom& g, const double* f, double* part, cudaStream_t st);
+cudaError_t dns_cfl_partials(const DevGeom& g, const double* u, int dir, double d, double* part, cudaStream_t st);
+
 cudaError_t dns_grad_xy(const DevGeom& g, const double* in, double* out, int dir, cudaStream_t st);
 cudaError_t dns_grad_z(const DevGeom& g, const double* in, double* out, double beta, cudaStream_t st);
 cudaError_t dns_product(const DevGeom& g, const double* a, const double* b, double* out, cudaStream_t st);

@@ -171,3 +171,34 @@ def test_dealiased_channel_high_order_pressure(tmp_path):
     assert Do.dealias
     Do.advance(6)
     _compare(p, gpu, Do)
+
+
+@pytest.mark.parametrize("case", ["tg", "channel2d"])
+def test_analysis_reductions(tmp_path, case):
+    # Analyser::modalEnergy / divergence / estimateCFL on the device against
+    # the oracle's restatement, after a few steps.
+    if case == "tg":
+        p = sessions.taylor_green_session(str(tmp_path / "tga"), 3, 6, 8, re=100.0, dt=2e-3, nstep=4,
+                                          extra={"TOL_REL": 1e-14})
+        ctx = S.Context(p)
+        funcs = S._user_functions(p)
+        ic = {c: ctx.evaluate(funcs[c], 0.0) for c in ctx.fields if c in funcs}
+    else:
+        p = sessions.channel_session(str(tmp_path / "cha"), 4, 2, 6, 1, nstep=4, extra={"TOL_REL": 1e-14})
+        ctx = S.Context(p)
+        x, y = ctx.mesh_coords()
+        ic = sessions.channel_initial(x, y, [0.0], amplitude=0.05)
+        ic = {c: v for c, v in ic.items() if c in ctx.fields}
+    D = S.DNS(ctx, 1)
+    D.restart(ic, 0.0)
+    D.advance(4)
+    ek, div, cfl = D.modal_energy(), D.divergence_energy(), D.cfl()
+    D.close()
+    ctx.close()
+    Do = O.DNS(O.Problem(O.read_session(p)), ic)
+    Do.advance(4)
+    ek_o = Do.modal_energy()
+    assert ek.shape == ek_o.shape
+    assert np.abs(ek - ek_o).max() <= 1e-10 * np.abs(ek_o).max()
+    assert abs(div - Do.divergence_energy()) <= 1e-9 * max(abs(Do.divergence_energy()), 1e-30) + 1e-20
+    assert abs(cfl - Do.cfl()) <= 1e-10 * Do.cfl()
