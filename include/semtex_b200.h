@@ -202,8 +202,15 @@ int stx_dns_restart(stx_dns* dns, double t0);
 int stx_dns_set_field(stx_dns* dns, char field, const double* h_phys);
 /* Physical-space copy of a field (Domain::dump's INVERSE transform). */
 int stx_dns_get_field(stx_dns* dns, char field, double* h_phys);
-/* Take nsteps time steps (the while loop of integrate()). */
+/* Take nsteps time steps (the while loop of integrate()).  Steady steps
+ * (past the start-up orders, no time-dependent BCs) are captured once as a
+ * CUDA graph of one cycle of steps -- from a storage-rotation and
+ * alternating-form state back to it -- and replayed (token STX_DNS_GRAPH,
+ * default 1; capture needs 12 steps left in the call). */
 int stx_dns_advance(stx_dns* dns, int nsteps);
+/* Length of the captured step cycle (0: none) and the number of graph
+ * launches so far. */
+int stx_dns_graph_info(const stx_dns* dns, int* period, long long* launches);
 int stx_dns_state(const stx_dns* dns, int* step, double* time);
 /* Analyser (src/analysis.cpp:329-443), computed on the device from the
  * current (Fourier) velocity: modal energies per unit area

@@ -373,6 +373,12 @@ class DNS:
         check(lib().stx_dns_state(self._h, C.byref(s), C.byref(t)))
         return s.value, t.value
 
+    def graph_info(self):
+        """(cycle length of the captured step graph, graph launches so far)."""
+        a, b = C.c_int(), C.c_longlong()
+        check(lib().stx_dns_graph_info(self._h, C.byref(a), C.byref(b)))
+        return a.value, b.value
+
     # -- Analyser (src/analysis.cpp:329-443) on the device
     def modal_energy(self) -> np.ndarray:
         out = np.zeros((self.ctx.nz + 1) // 2)

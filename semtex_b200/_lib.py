@@ -59,6 +59,7 @@ SIGNATURES = {
     "stx_dns_modal_energy": (_i, [_p, _p]),
     "stx_dns_divergence_energy": (_i, [_p, _pd]),
     "stx_dns_cfl": (_i, [_p, _pd]),
+    "stx_dns_graph_info": (_i, [_p, _pi, C.POINTER(C.c_longlong)]),
     "stx_elliptic_solve_host": (_i, [_p, _p, _p]),
     "stx_sync": (_i, [_p]),
     "stx_context_stream": (_i, [_p, C.POINTER(_p)]),

@@ -111,6 +111,16 @@ struct stx_dns {
   double* B32 = nullptr;                   // padded z-derivative term (convective)
   double* C32 = nullptr;                   // padded product / z-derivative term (conservative)
   double* part = nullptr;                  // analysis partials: blocks x max(modes, 3)
+  // Steady steps replayed as a CUDA graph (token STX_DNS_GRAPH, default 1):
+  // the steps from one pointer state back to the same state (the multi-level
+  // storage rolls by pointer, the alternating form toggles) captured once.
+  bool use_graph = true;
+  cudaGraphExec_t gexec = nullptr;
+  int gperiod = 0;
+  std::vector<double*> gkey;  // pointer state the captured steps start from and return to
+  int gtoggle = 0;
+  int eager_steady = 0;       // steady steps run directly since the last restart
+  long long graph_launches = 0;
 };
 
 namespace {
@@ -374,6 +384,90 @@ void advance_one(stx_dns* d) {
 
 }  // namespace
 
+namespace {
+
+constexpr int kMaxCycle = 42;
+
+// Buffers whose roles rotate from step to step (by pointer), in a fixed order.
+std::vector<double*> pointer_state(const stx_dns* d) {
+  std::vector<double*> k(d->u.begin(), d->u.end());
+  for (const auto& v : d->Us) k.insert(k.end(), v.begin(), v.end());
+  for (const auto& v : d->Uf) k.insert(k.end(), v.begin(), v.end());
+  k.insert(k.end(), d->un_lvl.begin(), d->un_lvl.end());
+  k.insert(k.end(), d->hop_lvl.begin(), d->hop_lvl.end());
+  return k;
+}
+
+// A step is steady (its kernels and coefficients repeat) once the start-up
+// orders are past, and no BC is re-evaluated on the host.
+bool steady(const stx_dns* d) {
+  if (d->step < d->nord) return false;
+  for (char t : d->tdep)
+    if (t) return false;
+  return true;
+}
+
+void drop_graph(stx_dns* d) {
+  if (d->gexec) cudaGraphExecDestroy(d->gexec);
+  d->gexec = nullptr;
+  d->gperiod = 0;
+  d->gkey.clear();
+}
+
+// Capture the steps from the current pointer state back to it (at most
+// kMaxCycle: the velocity storage of N_TIME = 3 rotates through a 7-cycle,
+// the alternating form through 2 and the pressure BC levels through 3).
+// The host state moves on during the capture without the work running; on
+// success the graph is launched once to run those steps, on failure the
+// host state is put back and false returned.
+bool capture_steps(stx_dns* d) {
+  stx_context* ctx = d->ctx;
+  const auto u = d->u;
+  const auto Us = d->Us, Uf = d->Uf;
+  const auto un = d->un_lvl, hop = d->hop_lvl;
+  const int step = d->step, toggle = d->toggle;
+  const double time = d->time;
+  const std::vector<double*> key = pointer_state(d);
+  if (cudaStreamBeginCapture(ctx->stream, cudaStreamCaptureModeThreadLocal) != cudaSuccess) return false;
+  int period = 0;
+  bool ok = true;
+  try {
+    do {
+      advance_one(d);
+      ++period;
+    } while (period < kMaxCycle && !(pointer_state(d) == key && d->toggle == toggle));
+  } catch (const std::exception&) {
+    ok = false;
+  }
+  cudaGraph_t graph = nullptr;
+  const cudaError_t e = cudaStreamEndCapture(ctx->stream, &graph);
+  ok = ok && e == cudaSuccess && graph && pointer_state(d) == key && d->toggle == toggle;
+  cudaGraphExec_t exec = nullptr;
+  if (ok) ok = cudaGraphInstantiate(&exec, graph, 0) == cudaSuccess;
+  if (graph) cudaGraphDestroy(graph);
+  cudaGetLastError();  // clear a capture error, the steps run directly instead
+  if (!ok) {
+    d->u = u;
+    d->Us = Us;
+    d->Uf = Uf;
+    d->un_lvl = un;
+    d->hop_lvl = hop;
+    d->step = step;
+    d->toggle = toggle;
+    d->time = time;
+    return false;
+  }
+  d->gexec = exec;
+  d->gperiod = period;
+  d->gkey = key;
+  d->gtoggle = toggle;
+  ck(cudaGraphLaunch(d->gexec, ctx->stream), "graph launch");
+  ++d->graph_launches;
+  return true;
+}
+
+}  // namespace
+
 extern "C" {
 
 int stx_dns_create(stx_context* ctx, int advection, stx_dns** out) {
@@ -398,6 +492,7 @@ int stx_dns_create(stx_context* ctx, int advection, stx_dns** out) {
     d->tol = S.tokens.value("TOL_REL");
     d->step_max = S.tokens.ivalue("STEP_MAX");
     d->form = advection;
+    d->use_graph = !S.tokens.has("STX_DNS_GRAPH") || S.tokens.ivalue("STX_DNS_GRAPH") != 0;
     cudaSetDevice(ctx->device);
     const DevGeom& g = ctx->dg;
     d->fsize = static_cast<size_t>(g.nz) * g.plane_size;
@@ -499,6 +594,7 @@ int stx_dns_destroy(stx_dns* d) {
     if (!d) return;
     cudaSetDevice(d->ctx->device);
     cudaStreamSynchronize(d->ctx->stream);
+    drop_graph(d);
     for (auto* m : d->vsys) stx_modal_destroy(m);
     if (d->psys) stx_modal_destroy(d->psys);
     for (auto& kv : d->pcg) stx_modal_destroy(kv.second);
@@ -517,6 +613,9 @@ int stx_dns_restart(stx_dns* d, double t0) {
       }
     for (double* p : d->un_lvl) ck(cudaMemsetAsync(p, 0, sizeof(double) * d->hsize, d->ctx->stream), "zero");
     for (double* p : d->hop_lvl) ck(cudaMemsetAsync(p, 0, sizeof(double) * d->hsize, d->ctx->stream), "zero");
+    ck(cudaStreamSynchronize(d->ctx->stream), "sync");
+    drop_graph(d);
+    d->eager_steady = 0;
     d->step = 0;
     d->time = t0;
     for (char c : d->names) ckstx(stx_field_bc_evaluate(d->ctx, c, t0));
@@ -558,11 +657,35 @@ int stx_dns_get_field(stx_dns* d, char field, double* h_phys) {
   });
 }
 
+
 int stx_dns_advance(stx_dns* d, int nsteps) {
   return dns_guarded([&] {
     if (!d || nsteps < 0) throw DnsError(STX_EINVAL, "bad argument");
     cudaSetDevice(d->ctx->device);
-    for (int s = 0; s < nsteps; ++s) advance_one(d);
+    int left = nsteps;
+    while (left > 0) {
+      const bool st = steady(d);
+      if (d->use_graph && st && d->eager_steady > 0) {
+        if (d->gexec && pointer_state(d) == d->gkey && d->toggle == d->gtoggle && left >= d->gperiod) {
+          ck(cudaGraphLaunch(d->gexec, d->ctx->stream), "graph launch");
+          ++d->graph_launches;
+          d->step += d->gperiod;
+          for (int k = 0; k < d->gperiod; ++k) d->time += d->dt;
+          left -= d->gperiod;
+          continue;
+        }
+        if (!d->gexec && left >= kMaxCycle) {  // never run past nsteps
+          if (capture_steps(d)) {
+            left -= d->gperiod;
+            continue;
+          }
+          d->use_graph = false;  // not capturable here: run every step directly
+        }
+      }
+      advance_one(d);
+      if (st) ++d->eager_steady;
+      --left;
+    }
     ck(cudaGetLastError(), "advance");
   });
 }
@@ -652,6 +775,14 @@ int stx_dns_cfl(stx_dns* d, double* inv_dt) {
       c = std::max(c, m);
     }
     *inv_dt = c;
+  });
+}
+
+int stx_dns_graph_info(const stx_dns* d, int* period, long long* launches) {
+  return dns_guarded([&] {
+    if (!d) throw DnsError(STX_EINVAL, "null argument");
+    if (period) *period = d->gperiod;
+    if (launches) *launches = d->graph_launches;
   });
 }
 
