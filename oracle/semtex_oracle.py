@@ -686,12 +686,29 @@ class BoundarySystem:
             L = math.hypot(xs[-1] - xs[0], ys[-1] - ys[0])
             self.area.append(0.5 * L * M.w)
         self.nline = len(self.edges) * n
+        # Mixed BCs dc/dn + K (c - C) = 0, "K;C" (Mixed::Mixed, src/condition.cpp:295-312):
+        # K C <1, w> in the RHS on every plane (Mixed::sum :315-343) and K <c, w>
+        # on the diagonal of the boundary system (augmentSC/Op/Dg :345-435)
+        self.mix = {}
+        self.mixdiag = None
+        nm = n - 1
+        for b, (e, s, kind, expr) in enumerate(self.edges):
+            if kind != "M":
+                continue
+            k_s, c_s = re.split(r"[;,]", expr, maxsplit=1)
+            K = float(M.S.tokens.evaluate(k_s))
+            C = float(M.S.tokens.evaluate(c_s))
+            self.mix[b] = (K, C)
+            if self.mixdiag is None:
+                self.mixdiag = np.zeros(N.nglobal)
+            g = [N.btog[e, (s * nm + t) % (4 * nm)] for t in range(n)]
+            np.add.at(self.mixdiag, g, K * self.area[b])
 
     def evaluate_physical(self, tok: Tokens, z: float, t: float):
         """BC line (values along each edge) in physical space at plane z."""
         out = np.zeros((len(self.edges), self.M.np))
         for b, (e, s, kind, expr) in enumerate(self.edges):
-            if kind in ("D", "N"):
+            if kind in ("D", "N"):       # ('M' lines are not used; 'H' computed)
                 idx = self.M.side_nodes(s)
                 xs, ys = self.M.x[e].ravel()[idx], self.M.y[e].ravel()[idx]
                 val = tok.evaluate(expr, x=xs, y=ys, z=z, t=t)
@@ -713,6 +730,10 @@ class BoundarySystem:
             if kind in ("N", "H"):   # NaturalCBCp::sum (src/condition.cpp:470-495) is the same sum
                 g = [self.N.btog[e, (s * nm + t) % (4 * nm)] for t in range(nm + 1)]
                 np.add.at(tgt, g, line[b] * self.area[b])
+            elif kind == "M":
+                K, C = self.mix[b]
+                g = [self.N.btog[e, (s * nm + t) % (4 * nm)] for t in range(nm + 1)]
+                np.add.at(tgt, g, K * C * self.area[b])
 
 
 # ---------------------------------------------------------------------------
@@ -723,9 +744,11 @@ class MatrixSys:
     """Statically condensed, banded-Cholesky Helmholtz system of one mode."""
 
     def __init__(self, M: Mesh, N: Numbering, lambda2: float, betak2: float,
-                 method: str = "DIRECT", mixed_bc: bool = False):
+                 method: str = "DIRECT", mixdiag=None):
         self.M, self.N = M, N
         self.lambda2, self.betak2, self.method = lambda2, betak2, method
+        self.mixdiag = mixdiag
+        mixed_bc = mixdiag is not None
         n = M.np
         next_ = 4 * (n - 1)
         em = M.emap()
@@ -760,6 +783,8 @@ class MatrixSys:
                         nn = g[k]
                         if nn < ns and nn >= m:
                             AB[kd + m - nn, nn] += hbb[i, k]
+            if mixdiag is not None:
+                AB[kd, :ns] += mixdiag[:ns]
             self.factor = sla.cholesky_banded(AB, lower=False) if ns else AB
         else:
             npts = N.nglobal + nel * (n - 2) ** 2
@@ -769,6 +794,8 @@ class MatrixSys:
                 dg = np.diag(H)[em]
                 np.add.at(pc, N.btog[e], dg[:next_])
                 pc[N.nglobal + e * (n - 2) ** 2: N.nglobal + (e + 1) * (n - 2) ** 2] = dg[next_:]
+            if mixdiag is not None:
+                pc[:N.nglobal] += mixdiag
             self.PC = 1.0 / pc
             self.npts = npts
 
@@ -835,6 +862,8 @@ def _global_op(M, N, MS, xg):
     y = np.zeros_like(xg)
     np.add.at(y, N.btog, HP[:, em[:next_]])
     y[N.nglobal:] = HP[:, em[next_:]].ravel()
+    if MS.mixdiag is not None:
+        y[:N.nglobal] += MS.mixdiag * xg[:N.nglobal]
     return y
 
 
@@ -1010,7 +1039,7 @@ class Problem:
             if cache is not None and key in cache:
                 out.append(cache[key])
                 continue
-            ms = MatrixSys(self.M, self.N[c], lambda2, bk2, method)
+            ms = MatrixSys(self.M, self.N[c], lambda2, bk2, method, self.B[c].mixdiag)
             if cache is not None:
                 cache[key] = ms
             out.append(ms)

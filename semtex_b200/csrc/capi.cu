@@ -255,10 +255,13 @@ int stx_context_create(const char* session_path, const char* overrides, int devi
           gid.push_back(N.btog[E.elmt * M.next + (E.side * (M.np - 1) + t) % M.next]);
           area.push_back(E.area[t]);
         }
-        kind.push_back(E.kind == 'H' ? 'N' : E.kind);  // NaturalCBCp::sum is Natural::sum (src/condition.cpp:470-495)
+        // NaturalCBCp::sum is Natural::sum (src/condition.cpp:470-495); Mixed::sum
+        // adds K C w, the line value of an 'M' edge (:315-343)
+        kind.push_back(E.kind == 'H' || E.kind == 'M' ? 'N' : E.kind);
       }
       d.edge_gid = upload(A, gid);
       d.edge_kind = upload(A, kind);
+      d.mixdiag = F.N.mixdiag.empty() ? nullptr : upload(A, F.N.mixdiag);
       d.edge_area = upload(A, area);
       F.nline = d.nedge * M.np;
       F.d_lines = static_cast<double*>(A.alloc(sizeof(double) * std::max(1, F.nline) * M.nz));
@@ -395,11 +398,18 @@ int stx_field_bc_evaluate(stx_context* ctx, char field, double t) {
           vars["y"] = E.y[q];
           // high-order pressure values are computed on the device each step
           line[static_cast<size_t>(k) * F.nline + b * np + q] =
-              E.kind == 'H' ? 0.0 : ctx->S.tokens.eval(E.expr, &vars);
+              E.kind == 'H' || E.kind == 'M' ? 0.0 : ctx->S.tokens.eval(E.expr, &vars);
         }
       }
     }
     host_dft_forward(line, nz, F.nline);
+    // Mixed::sum adds K C <1, w> on every plane (src/condition.cpp:315-343)
+    for (size_t b = 0; b < F.N.edges.size(); ++b) {
+      const BoundaryEdge& E = F.N.edges[b];
+      if (E.kind != 'M') continue;
+      for (int k = 0; k < nz; ++k)
+        for (int q = 0; q < np; ++q) line[static_cast<size_t>(k) * F.nline + b * np + q] = E.mix_K * E.mix_C;
+    }
     cuda_check(cudaMemcpyAsync(F.d_lines, line.data(), sizeof(double) * line.size(),
                                cudaMemcpyHostToDevice, ctx->stream),
                "bc upload");
@@ -440,6 +450,8 @@ int stx_modal_create(stx_context* ctx, char field, double lambda2, double beta, 
       const Mesh& M = ctx->M;
       const Patching* P = nullptr;
       if (direct) P = ctx->patching(field);
+      if (method == STX_MIXED && !P)
+        throw StxError(STX_EUNSUPPORTED, "mixed precision needs the two-level skeleton solve");
       std::vector<ModeSystem> modes(num_modes);
       std::vector<std::string> errs(num_modes);
       const unsigned hw = std::max(1u, std::thread::hardware_concurrency());
@@ -592,6 +604,7 @@ int stx_modal_create(stx_context* ctx, char field, double lambda2, double beta, 
           // number of FP64 refinement steps (token STX_REFINE, default 2)
           for (int m = 0; m < num_modes; ++m)
             if (pin[m] >= 0) throw StxError(STX_EUNSUPPORTED, "mixed precision needs a non-singular system");
+          if (!N.mixdiag.empty()) throw StxError(STX_EUNSUPPORTED, "mixed precision with mixed (Robin) BCs");
           std::vector<float> p32(pack.begin(), pack.end());
           if (p32.empty()) p32.assign(32, 0.0f);
           d.l2_pack32 = upload(st->arena, p32);

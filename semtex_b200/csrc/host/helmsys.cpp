@@ -215,7 +215,7 @@ ModeSystem build_mode_system(const Mesh& M, const Numbering& N, const Patching* 
   S.betak2 = betak2;
   S.method = method;
   S.nglobal = N.nglobal;
-  S.singular = (lambda2 + betak2) < kEpsSP && N.nglobal == N.nsolve;
+  S.singular = (lambda2 + betak2) < kEpsSP && N.nglobal == N.nsolve && N.mixdiag.empty();
   S.nsolve = S.singular ? N.nsolve - 1 : N.nsolve;
   S.nband = N.nband;
   const int nn = M.npnp, next = M.next, nint = M.nint, nel = M.nel;
@@ -232,6 +232,7 @@ ModeSystem build_mode_system(const Mesh& M, const Numbering& N, const Patching* 
         S.pc[N.nglobal + static_cast<size_t>(e) * nint + i] = H[static_cast<size_t>(r) * nn + r];
       }
     }
+    for (size_t g = 0; g < N.mixdiag.size(); ++g) S.pc[g] += N.mixdiag[g];  // Mixed::augmentDg
     for (auto& v : S.pc) v = 1.0 / v;
     return S;
   }
@@ -302,6 +303,11 @@ ModeSystem build_mode_system(const Mesh& M, const Numbering& N, const Patching* 
       std::vector<double> II(static_cast<size_t>(nI) * nI);
       for (int a = 0; a < nI; ++a)
         for (int b = 0; b < nI; ++b) II[static_cast<size_t>(a) * nI + b] = Sp[static_cast<size_t>(a) * nl + b];
+      // mixed-BC diagonal of the patch-interior nodes (the family's patches
+      // agree on it: it is part of the family signature)
+      if (!N.mixdiag.empty())
+        for (int a = 0; a < nI; ++a)
+          II[static_cast<size_t>(a) * nI + a] += N.mixdiag[P->I_gid[static_cast<size_t>(p) * P->nI_max + a]];
       if (nI) spd_inverse(nI, II.data(), nthreads);  // S_II is symmetric positive definite
       for (int a = 0; a < nI; ++a)
         for (int b = 0; b < nI; ++b) Si[static_cast<size_t>(a) * nI_max + b] = II[static_cast<size_t>(a) * nI + b];
@@ -348,6 +354,9 @@ ModeSystem build_mode_system(const Mesh& M, const Numbering& N, const Patching* 
       for (int a = 0; a < nB; ++a)
         for (int b = 0; b < nB; ++b) A[static_cast<size_t>(iid[a]) * ni + iid[b]] += Tf[static_cast<size_t>(a) * nB + b];
     }
+    // mixed-BC diagonal of the interface nodes (Mixed::augmentSC)
+    if (!N.mixdiag.empty())
+      for (int q = 0; q < ni; ++q) A[static_cast<size_t>(q) * ni + q] += N.mixdiag[P->skel_of[q]];
     if (S.singular) {
       // the pinned node is known (zero): identity row and column
       const int q = P->pin_iid;
@@ -381,6 +390,8 @@ ModeSystem build_mode_system(const Mesh& M, const Numbering& N, const Patching* 
       }
     }
   }
+  for (int j = 0; j < ns && j < static_cast<int>(N.mixdiag.size()); ++j)  // Mixed::augmentSC
+    A[static_cast<size_t>(j) * nb + kd] += N.mixdiag[j];
   factor_band(A, ns, nb, S);
   return S;
 }

@@ -625,7 +625,7 @@ Numbering build_numbering(const Session& S, const Mesh& M, char field, int rcm_r
       } else if (bc.kind == 'H') {
         if (field != 'p')
           throw std::runtime_error(std::string("high-order BC <H> given for field ") + field + ", not pressure");
-      } else if (bc.kind != 'N') {
+      } else if (bc.kind != 'N' && bc.kind != 'M') {
         throw std::runtime_error(std::string("boundary condition kind <") + bc.kind +
                                  "> is not supported");
       }
@@ -634,6 +634,13 @@ Numbering build_numbering(const Session& S, const Mesh& M, char field, int rcm_r
       E.side = s;
       E.kind = bc.kind;
       E.expr = bc.expr;
+      if (bc.kind == 'M') {  // "K;C" or "K,C" (Mixed::Mixed, src/condition.cpp:295-312)
+        const size_t cut = bc.expr.find_first_of(";,");
+        if (cut == std::string::npos)
+          throw std::runtime_error("mixed BC needs two values separated by ';' or ','");
+        E.mix_K = S.tokens.eval(bc.expr.substr(0, cut), nullptr);
+        E.mix_C = S.tokens.eval(bc.expr.substr(cut + 1), nullptr);
+      }
       std::vector<int> idx(n);
       M.side_nodes(s, idx.data());
       E.x.resize(n);
@@ -711,6 +718,12 @@ Numbering build_numbering(const Session& S, const Mesh& M, char field, int rcm_r
     // Such fields take the reference's own `enumerate -O3` numbering.
     N.btog = enumerate_o3(reference_map(S, M), nel, next);
   }
+  for (const BoundaryEdge& E : N.edges)
+    if (E.kind == 'M') {
+      if (N.mixdiag.empty()) N.mixdiag.assign(nglobal, 0.0);
+      for (int t = 0; t < n; ++t)
+        N.mixdiag[N.btog[E.elmt * next + (E.side * nm + t) % next]] += E.mix_K * E.area[t];
+    }
   int bw = 0;
   for (int e = 0; e < nel; ++e) {
     int lo = nglobal, hi = -1;

@@ -48,8 +48,9 @@ Mesh build_mesh(const Session& S);
 
 struct BoundaryEdge {
   int elmt = 0, side = 0;
-  char kind = 0;              // 'D', 'N' or 'H' (pressure only; others rejected)
+  char kind = 0;              // 'D', 'N', 'M' (mixed) or 'H' (pressure only); others rejected
   std::string expr;
+  double mix_K = 0.0, mix_C = 0.0;  // 'M': dc/dn + K (c - C) = 0
   std::vector<double> area;   // np quadrature-weighted side lengths
   std::vector<double> x, y;   // np node locations along the side
   std::vector<double> nx, ny; // np unit outward normal components
@@ -62,8 +63,12 @@ struct Numbering {
   std::vector<int> emask;        // [nel]
   std::vector<double> imass;     // [nglobal]
   std::vector<BoundaryEdge> edges;
+  // Mixed BCs: K * (quadrature-weighted side length) summed into the
+  // diagonal of the assembled boundary system at each edge node
+  // (Mixed::augmentSC, src/condition.cpp:345-376); empty without <M> edges.
+  std::vector<double> mixdiag;   // [nglobal]
   bool same_as(const Numbering& o) const {
-    return nglobal == o.nglobal && nsolve == o.nsolve && btog == o.btog;
+    return nglobal == o.nglobal && nsolve == o.nsolve && btog == o.btog && mixdiag == o.mixdiag;
   }
 };
 

@@ -1,5 +1,7 @@
 #include "patch.hpp"
 
+#include <cstring>
+
 #include <algorithm>
 #include <cmath>
 #include <map>
@@ -154,6 +156,14 @@ Patching build_patching(const Mesh& M, const Numbering& N, int max_patch_elems, 
         sig.push_back(l);
       }
     }
+    // mixed-BC diagonal entries of the interior nodes (bit patterns): patches
+    // sharing matrices must agree on them
+    if (!N.mixdiag.empty())
+      for (int g : Ilist) {
+        long long bits;
+        std::memcpy(&bits, &N.mixdiag[g], sizeof(bits));
+        sig.push_back(bits);
+      }
     auto it = fam_of.find(sig);
     if (it == fam_of.end()) {
       it = fam_of.emplace(sig, P.nfamily++).first;

@@ -44,6 +44,7 @@ struct DevNumbering {
   const int* edge_gid;  // [nedge*np] global id of each edge node
   const int* edge_kind; // [nedge]  'D' or 'N'
   const double* edge_area;  // [nedge*np]
+  const double* mixdiag;    // [nglobal] mixed-BC diagonal (K x side weights), or null
 };
 
 // One tiled product y += scale A x for the planes of a Fourier mode, the

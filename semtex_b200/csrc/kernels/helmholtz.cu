@@ -520,6 +520,8 @@ __global__ void k_global_op(DevGeom g, DevNumbering N, DevModal S, const double*
   const double hcon = S.lambda2[m] + S.betak2[m];
   const double* x = X + static_cast<size_t>(k) * vstride;
   double* y = Y + static_cast<size_t>(k) * vstride;
+  if (N.mixdiag && e == 0)  // <K x, w> on mixed-BC edges (Mixed::augmentOp, src/condition.cpp:379-407)
+    for (int q = t; q < N.nglobal; q += blockDim.x) atomicAdd(&y[q], N.mixdiag[q] * x[q]);
   for (int q = t; q < np * np; q += blockDim.x) sD[q] = g.D[q];
   if (t < g.next) su[g.emap[t]] = x[N.btog[e * g.next + t]];
   if (t < g.nint) su[g.emap[g.next + t]] = x[N.nglobal + static_cast<size_t>(e) * g.nint + t];

@@ -23,7 +23,7 @@ def rel_l2(a, b):
     return np.linalg.norm(a - b) / max(np.linalg.norm(b), 1e-300)
 
 
-@pytest.mark.parametrize("name", ["helmholtz1", "poisson1", "laplace1", "laplace4", "laplace3"])
+@pytest.mark.parametrize("name", ["helmholtz1", "poisson1", "laplace1", "laplace4", "laplace3", "mixed1"])
 @pytest.mark.parametrize("iterative", [False, True])
 def test_reference_sessions(name, iterative):
     path = os.path.join(SESSIONS, name)
@@ -154,4 +154,42 @@ def test_multi_field_solve_matches_single(tmp_path, nf):
         assert rel_l2(a, Uo) < TOL, (c, rel_l2(a, Uo))
     for sys_ in systems:
         sys_.close()
+    ctx.close()
+
+
+
+def _robin_session(path, nx, ny, np_, nz, K, C):
+    """Periodic in x, Dirichlet 0 at y = 0, mixed dc/dn + K (c - C) = 0 at y = 1."""
+    p = sessions.rect_session(path, nx, ny, tokens={"N_P": np_, "N_Z": nz, "BETA": 1.0, "LAMBDA2": 1.0,
+                                                     "TOL_REL": 1e-14},
+                              periodic_x=True, bcs={"w": {"c": f"<M> {K};{C}"}})
+    txt = open(p).read()
+    txt = txt.replace("<GROUPS NUMBER=1>", "<GROUPS NUMBER=2>\n\t2\tz\tclamp")
+    txt = txt.replace("<BCS NUMBER=1>", "<BCS NUMBER=2>\n\t2\tz\t1\n\t\t<D>\tc = 0\t</D>")
+    out = []
+    for ln in txt.splitlines():
+        parts = ln.split("\t")
+        if len(parts) >= 4 and parts[3] == "1" and "<B>" in ln:   # side 1: bottom
+            ln = ln.replace("<B>\tw\t</B>", "<B>\tz\t</B>")
+        out.append(ln)
+    open(p, "w").write("\n".join(out) + "\n")
+    return p
+
+
+@pytest.mark.parametrize("solver", ["twolevel", "band", "pcg"])
+def test_mixed_bc_fourier(tmp_path, solver):
+    """Mixed (Robin) BCs (src/condition.cpp:295-435) in 3D, against the oracle:
+    K C <1, w> on every plane, K <c, w> on the boundary-system diagonal."""
+    p = _robin_session(str(tmp_path / "rb"), 8, 6, 7, 8, 2.5, 0.3)
+    ov = {"STX_TWOLEVEL": 0} if solver == "band" else ({"ITERATIVE": 1} if solver == "pcg" else None)
+    ctx = S.Context(p, ov)
+    rng = np.random.default_rng(5)
+    f = rng.uniform(-1, 1, (ctx.nz, ctx.nel, ctx.np, ctx.np))
+    sysm = S.ModalMatrixSys(ctx, "c", 1.0, method=S.JACPCG if solver == "pcg" else S.DIRECT)
+    u = sysm.solve_host(f)
+    P, U = O.elliptic(p, {"ITERATIVE": 1} if solver == "pcg" else None, forcing_phys=f)
+    assert rel_l2(u, U) < (1e-9 if solver == "pcg" else TOL), rel_l2(u, U)
+    with pytest.raises(S.StxError):
+        S.ModalMatrixSys(ctx, "c", 1.0, method=S.MIXED)
+    sysm.close()
     ctx.close()

@@ -63,6 +63,7 @@ def test_enumerate_o3_pin_is_best_root():
 
 @pytest.mark.parametrize("name,tol", [
     ("helmholtz1", 1e-13), ("poisson1", 1e-13), ("laplace4", 1e-13), ("laplace1", 2e-10),
+    ("mixed1", 1e-12),   # mixed (Robin) BC dc/dn + 3 (c - 7) = 0, quadratic exact solution
 ])
 def test_elliptic_exact(name, tol):
     P, U = O.elliptic(os.path.join(SESSIONS, name))
