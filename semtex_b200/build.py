@@ -17,6 +17,7 @@ HERE = os.path.dirname(os.path.abspath(__file__))
 CSRC = os.path.join(HERE, "csrc")
 BUILD = os.path.join(HERE, "_build")
 LIB = os.path.join(HERE, "libsemtex_b200.so")
+BIN = os.path.join(HERE, "bin")
 NVCC = os.environ.get("NVCC", "/usr/local/cuda/bin/nvcc")
 ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]
 CXXFLAGS = ["-O3", "-std=c++17", "-fPIC", "-Wall", "-Wno-unused-function"]
@@ -70,11 +71,25 @@ def build(force: bool = False, verbose: bool = False, ptxas_verbose: bool = Fals
             if err.strip() and (verbose or "warning" in err):
                 print(err, file=sys.stderr)
     objs = [_obj(s) for s in cpp + cu]
+    relinked = False
     if todo or not os.path.exists(LIB):
         cmd = [NVCC, *ARCH, "-shared", "-o", LIB, *objs, "-lpthread"]
         r = subprocess.run(cmd, capture_output=True, text=True)
         if r.returncode != 0:
             raise RuntimeError(f"link failed: {' '.join(cmd)}\n{r.stdout}\n{r.stderr}")
+        relinked = True
+    # the `elliptic` and `dns` programs over the library (semtex_b200/bin)
+    os.makedirs(BIN, exist_ok=True)
+    for src in sorted(glob.glob(os.path.join(CSRC, "cli", "*.cpp"))):
+        exe = os.path.join(BIN, os.path.splitext(os.path.basename(src))[0])
+        if force or relinked or not os.path.exists(exe) or os.path.getmtime(exe) < max(os.path.getmtime(src), hdr):
+            cmd = ["g++", *CXXFLAGS, "-I", CSRC, src, "-o", exe, "-L", HERE, "-lsemtex_b200",
+                   "-Wl,-rpath,$ORIGIN/.."]
+            r = subprocess.run(cmd, capture_output=True, text=True)
+            if r.returncode != 0:
+                raise RuntimeError(f"program build failed: {' '.join(cmd)}\n{r.stdout}\n{r.stderr}")
+            if r.stderr.strip() and "warning" in r.stderr:
+                print(r.stderr, file=sys.stderr)
     return LIB
 
 

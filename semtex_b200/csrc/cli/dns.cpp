@@ -1,0 +1,166 @@
+// dns [-h] [-S|-C|-N] [-chk] [-v] session
+//
+// The `dns` program (dns/drive.cpp:56-160) on the device: the session's
+// fields start from session.rst if present, else zero (Domain::restart,
+// src/domain.cpp:123-156); N_STEP velocity-correction steps of integrate()
+// (dns/integrate.cpp:66-200) with the advection form of -S (skew-symmetric),
+// default (alternating skew-symmetric), -C (convective) or -N (Stokes).
+// Field dumps follow Domain::dump (src/domain.cpp:158-215): every IO_FLD
+// steps and at the end, to session.chk (previous one kept as .chk.bak) with
+// the final dump to session.fld, or with -chk all appended to session.fld.
+// Every IO_CFL steps the CFL estimate and divergence energy are printed
+// (Analyser::estimateCFL / divergence, src/analysis.cpp:382-443).
+#include <cmath>
+#include <cstdio>
+#include <cstring>
+#include <fstream>
+#include <string>
+#include <vector>
+
+#include "../../../include/semtex_b200.h"
+#include "host/fieldfile.hpp"
+
+namespace {
+
+[[noreturn]] void fail(const std::string& what) {
+  std::fprintf(stderr, "dns: %s\n", what.c_str());
+  std::exit(EXIT_FAILURE);
+}
+
+void check(int rc, const char* what) {
+  if (rc != STX_OK) fail(std::string(what) + ": " + stx_last_error());
+}
+
+const char* kUsage =
+    "Usage: dns [options] session-file\n"
+    "  [options]:\n"
+    "  -h       ... print this message\n"
+    "  -v[v...] ... increase verbosity level\n"
+    "  -chk     ... turn off checkpoint field dumps [default: selected]\n"
+    "  -S|C|N   ... regular skew-symm || convective || Stokes advection\n";
+
+double token(const stx_context* ctx, const char* name) {
+  double v = 0.0;
+  check(stx_token(ctx, name, &v), name);
+  return v;
+}
+
+}  // namespace
+
+int main(int argc, char** argv) {
+  int advection = 1, verbose = 0;
+  bool no_chk = false;
+  int a = 1;
+  for (; a < argc && argv[a][0] == '-'; ++a) {
+    const std::string o = argv[a];
+    if (o == "-h") {
+      std::fputs(kUsage, stdout);
+      return EXIT_SUCCESS;
+    } else if (o == "-S") {
+      advection = 0;
+    } else if (o == "-C") {
+      advection = 2;
+    } else if (o == "-N") {
+      advection = 3;
+    } else if (o == "-chk") {
+      no_chk = true;
+    } else if (o[1] == 'v') {
+      verbose += static_cast<int>(o.size()) - 1;
+    } else {
+      std::fputs(kUsage, stderr);
+      return EXIT_FAILURE;
+    }
+  }
+  if (a != argc - 1) fail("no session definition file");
+  const std::string session = argv[a];
+  stx_context* ctx = nullptr;
+  check(stx_context_create(session.c_str(), nullptr, 0, nullptr, &ctx), "session");
+  int np = 0, nz = 0, nel = 0, ps = 0;
+  check(stx_context_geometry(ctx, &np, &nz, &nel, &ps), "geometry");
+  char fbuf[64];
+  check(stx_context_fields(ctx, fbuf, sizeof(fbuf)), "fields");
+  const std::string fields = fbuf;
+  const size_t n = static_cast<size_t>(nz) * nel * np * np;
+  stx_dns* dns = nullptr;
+  check(stx_dns_create(ctx, advection, &dns), "integrate");
+  // -- Domain::restart
+  double t0 = 0.0;
+  stx::FieldFile rst;
+  const bool have_rst = static_cast<bool>(std::ifstream(session + ".rst"));
+  if (have_rst) {
+    rst = stx::read_field(session + ".rst");
+    t0 = rst.time;
+  }
+  check(stx_dns_restart(dns, t0), "restart");
+  std::vector<double> zero(n, 0.0);
+  for (char c : fields) {
+    const size_t k = have_rst ? rst.names.find(c) : std::string::npos;
+    if (k != std::string::npos && rst.data[k].size() != n) fail(session + ".rst does not match the session");
+    check(stx_dns_set_field(dns, c, k != std::string::npos ? rst.data[k].data() : zero.data()), "restart");
+  }
+  std::printf("-- Initial condition       : %s\n", have_rst ? ("read from file " + session + ".rst").c_str()
+                                                             : "set to zero");
+  const int nstep = static_cast<int>(std::lround(token(ctx, "N_STEP")));
+  const int io_fld = std::max(1, static_cast<int>(std::lround(token(ctx, "IO_FLD"))));
+  const int io_cfl = static_cast<int>(std::lround(token(ctx, "IO_CFL")));
+  const double dt = token(ctx, "D_T");
+  const bool chkpoint = !no_chk && token(ctx, "CHKPOINT") != 0.0;
+  stx::FieldFile out;
+  const size_t slash = session.find_last_of('/');
+  out.session = slash == std::string::npos ? session : session.substr(slash + 1);
+  out.np = np;
+  out.nz = nz;
+  out.nel = nel;
+  out.dt = dt;
+  out.kinvis = token(ctx, "KINVIS");
+  out.beta = token(ctx, "BETA");
+  out.names = fields;
+  out.data.assign(fields.size(), std::vector<double>(n));
+  int step = 0;
+  while (step < nstep) {
+    int next = std::min(nstep, (step / io_fld + 1) * io_fld);
+    if (io_cfl > 0) next = std::min(next, (step / io_cfl + 1) * io_cfl);
+    if (verbose) {  // the step line of DNSAnalyser::analyse, one step at a time
+      for (; step < next; ++step) {
+        check(stx_dns_advance(dns, 1), "integrate");
+        double t;
+        check(stx_dns_state(dns, nullptr, &t), "state");
+        std::printf("Step: %d  Time: %g\n", step + 1, t);
+      }
+    } else {
+      check(stx_dns_advance(dns, next - step), "integrate");
+      step = next;
+    }
+    double time;
+    check(stx_dns_state(dns, nullptr, &time), "state");
+    if (io_cfl > 0 && step % io_cfl == 0) {
+      double inv = 0.0, div = 0.0;
+      check(stx_dns_cfl(dns, &inv), "CFL");
+      check(stx_dns_divergence_energy(dns, &div), "divergence");
+      const double dt_max = 0.9 * 0.7 / inv;
+      std::printf("-- CFL: %g, dt (max): %g, dt (set): %g (%d%%)\n", inv * dt, dt_max, dt,
+                  static_cast<int>(100.0 * dt / dt_max));
+      std::printf("------- Divergence Energy: %g\n", div);
+    }
+    const bool periodic = step % io_fld == 0, initial = step == io_fld, final = step == nstep;
+    if (periodic || final) {
+      for (size_t k = 0; k < fields.size(); ++k)
+        check(stx_dns_get_field(dns, fields[k], out.data[k].data()), "dump");
+      out.step = step;
+      out.time = time;
+      if (chkpoint) {
+        if (final) {
+          stx::write_field(session + ".fld", out);
+        } else {
+          if (!initial) std::rename((session + ".chk").c_str(), (session + ".chk.bak").c_str());
+          stx::write_field(session + ".chk", out);
+        }
+      } else {
+        stx::write_field(session + ".fld", out, !initial);
+      }
+    }
+  }
+  stx_dns_destroy(dns);
+  stx_context_destroy(ctx);
+  return EXIT_SUCCESS;
+}

@@ -1,0 +1,65 @@
+"""The `elliptic` and `dns` programs (semtex_b200/bin), built over the C ABI.
+
+CPU: they exist and print their usage.  GPU: the reference's own regression
+workflow (test/testregress:14-30) -- a restart file holding the USER-section
+solution at t = 0, `dns -chk session`, then the errors of session.fld -- and
+`elliptic` on the test sessions, against the oracle.
+"""
+import json
+import os
+import shutil
+import subprocess
+
+import numpy as np
+import pytest
+
+import semtex_oracle as O
+from semtex_b200.fieldfile import read_field, write_field
+
+from conftest import GOLDEN, SESSIONS
+
+ROOT = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
+BIN = os.path.join(ROOT, "semtex_b200", "bin")
+GOLD = json.load(open(os.path.join(GOLDEN, "regress_ok.json")))["goldens"]
+
+
+@pytest.mark.parametrize("prog", ["dns", "elliptic"])
+def test_programs_print_usage(prog):
+    r = subprocess.run([os.path.join(BIN, prog), "-h"], capture_output=True, text=True, timeout=60)
+    assert r.returncode == 0 and "Usage" in r.stdout
+
+
+@pytest.mark.gpu
+@pytest.mark.parametrize("name", ["helmholtz1", "mixed1"])
+def test_elliptic_program(tmp_path, name):
+    path = str(tmp_path / name)
+    shutil.copy(os.path.join(SESSIONS, name), path)
+    r = subprocess.run([os.path.join(BIN, "elliptic"), path], capture_output=True, text=True, timeout=600)
+    assert r.returncode == 0, r.stderr
+    hdr, flds = read_field(path + ".fld")
+    P, U = O.elliptic(path)
+    u = flds[P.S.fields[0]]
+    assert np.linalg.norm(u - U) / np.linalg.norm(U) < 1e-10
+    assert "norm_inf" in r.stdout
+
+
+@pytest.mark.gpu
+@pytest.mark.parametrize("name", ["kovas1", "taylor2"])
+def test_dns_program_regression_workflow(tmp_path, name):
+    path = str(tmp_path / name)
+    shutil.copy(os.path.join(SESSIONS, name), path)
+    S = O.read_session(path)
+    P = O.Problem(S)
+    funcs = O.user_functions(S)
+    ic = {c: P.evaluate(funcs[c], 0.0) for c in S.fields if c in funcs}   # what `compare` writes
+    write_field(path + ".rst", name, P.np, P.nz, P.nel, 0, 0.0, S.tokens["D_T"], S.tokens["KINVIS"],
+                S.tokens["BETA"], ic)
+    r = subprocess.run([os.path.join(BIN, "dns"), "-chk", path], capture_output=True, text=True, timeout=600)
+    assert r.returncode == 0, r.stderr
+    hdr, flds = read_field(path + ".fld")
+    assert hdr["step"] == S.tokens.ivalue("N_STEP")
+    t = float(f"{hdr['time']:.6g}")
+    for c in S.fields:
+        err = np.abs(P.evaluate(funcs[c], t) - flds[c]).max()
+        got = "noise-level" if err < 1e-12 else f"{err:.4e}"
+        assert got == GOLD[name][c], (name, c, got)
