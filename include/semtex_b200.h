@@ -85,6 +85,9 @@ int stx_numbering_host(const char* session_path, const char* overrides, char fie
                        int* next, int* nglobal, int* nsolve, int* nband, int* h_btog, int* h_bmask);
 /* Element node locations, host buffers of nel*np*np (Element::_xmesh). */
 int stx_mesh_coords(const stx_context* ctx, double* h_x, double* h_y);
+/* Element mass weights (quadrature weight x Jacobian, Element::_Q4), host
+ * buffer of nel*np*np. */
+int stx_mesh_mass(const stx_context* ctx, double* h_q4);
 /* Number of geometry families (elements sharing condensed matrices). */
 int stx_mesh_families(const stx_context* ctx, int* nfamily);
 

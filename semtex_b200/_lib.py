@@ -36,6 +36,7 @@ SIGNATURES = {
     "stx_numbering_host": (_i, [_s, _s, C.c_char, _pi, _pi, _pi, _pi, _pi, _p, _p]),
     "stx_mesh_coords": (_i, [_p, _p, _p]),
     "stx_mesh_families": (_i, [_p, _pi]),
+    "stx_mesh_mass": (_i, [_p, _p]),
     "stx_field_evaluate": (_i, [_p, _s, _d, _p]),
     "stx_field_bc_evaluate": (_i, [_p, C.c_char, _d]),
     "stx_modal_create": (_i, [_p, C.c_char, _d, _d, _i, _i, _i, C.POINTER(_p)]),

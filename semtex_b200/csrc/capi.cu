@@ -351,6 +351,13 @@ int stx_mesh_coords(const stx_context* ctx, double* h_x, double* h_y) {
   });
 }
 
+int stx_mesh_mass(const stx_context* ctx, double* h_q4) {
+  return guarded([&] {
+    if (!ctx || !h_q4) throw StxError(STX_EINVAL, "null argument");
+    std::memcpy(h_q4, ctx->M.Q4.data(), sizeof(double) * ctx->M.Q4.size());
+  });
+}
+
 int stx_mesh_families(const stx_context* ctx, int* nfamily) {
   return guarded([&] {
     if (!ctx || !nfamily) throw StxError(STX_EINVAL, "null argument");
