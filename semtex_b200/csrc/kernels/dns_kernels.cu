@@ -17,6 +17,7 @@
 // element data in its own shared memory (lanes over nodes, a few nodes per
 // lane loaded together) and synchronises only with itself.
 #include "dns_kernels.cuh"
+#include "launch.hpp"
 
 namespace stx {
 
@@ -387,6 +388,7 @@ inline unsigned stream_blocks(size_t n) {
 
 cudaError_t dns_grad_xy(const DevGeom& g, const double* in, double* out, int dir, cudaStream_t st) {
   if (!ep_fits(g)) return cudaErrorInvalidValue;
+  raise_smem_limit(reinterpret_cast<const void*>(k_grad_xy), ep_smem(g, 1));
   k_grad_xy<<<ep_grid(g), kEpThreads, ep_smem(g, 1), st>>>(g, in, out, dir);
   return cudaGetLastError();
 }
@@ -405,6 +407,7 @@ cudaError_t dns_product(const DevGeom& g, const double* a, const double* b, doub
 
 cudaError_t dns_nonlinear(const DevGeom& g, const NonlinearArgs& a, cudaStream_t st) {
   if (!ep_fits(g)) return cudaErrorInvalidValue;
+  raise_smem_limit(reinterpret_cast<const void*>(k_nonlinear), ep_smem(g, 5));
   k_nonlinear<<<ep_grid(g), kEpThreads, ep_smem(g, 5), st>>>(g, a);
   return cudaGetLastError();
 }
@@ -454,6 +457,7 @@ cudaError_t dns_combine(const DevGeom& g, const CombineArgs& a, cudaStream_t st)
 cudaError_t dns_divergence(const DevGeom& g, const double* a0, const double* a1, const double* a2, double* out,
                            double dt, double beta, cudaStream_t st) {
   if (!ep_fits(g)) return cudaErrorInvalidValue;
+  raise_smem_limit(reinterpret_cast<const void*>(k_divergence), ep_smem(g, 2));
   k_divergence<<<ep_grid(g), kEpThreads, ep_smem(g, 2), st>>>(g, a0, a1, a2, out, 1.0 / dt, beta);
   return cudaGetLastError();
 }
@@ -461,6 +465,7 @@ cudaError_t dns_divergence(const DevGeom& g, const double* a0, const double* a1,
 cudaError_t dns_project(const DevGeom& g, double* io, const double* p, int dir, double alpha, double b,
                         double beta, cudaStream_t st) {
   if (!ep_fits(g)) return cudaErrorInvalidValue;
+  raise_smem_limit(reinterpret_cast<const void*>(k_project), ep_smem(g, 1));
   k_project<<<ep_grid(g), kEpThreads, ep_smem(g, 1), st>>>(g, io, p, dir, alpha, b, beta);
   return cudaGetLastError();
 }

@@ -14,6 +14,7 @@
 
 #include <algorithm>
 
+#include "launch.hpp"
 #include "ptx.cuh"
 
 namespace stx {
@@ -557,11 +558,7 @@ ElementPlan element_plan(const DevGeom& g, const DevModal& S, bool lift) {
 
 void element_condense(const ElementPlan& P, const DevGeom& g, const DevNumbering& N, const DevModal& S,
                       const double* F, const double* G, int gstride, double* R, int rstride, cudaStream_t st) {
-  static size_t configured = 0;
-  if (P.cond_smem > configured) {
-    cudaFuncSetAttribute(k_elem_condense, cudaFuncAttributeMaxDynamicSharedMemorySize, static_cast<int>(P.cond_smem));
-    configured = P.cond_smem;
-  }
+  raise_smem_limit(reinterpret_cast<const void*>(k_elem_condense), P.cond_smem);
   k_elem_condense<<<dim3(g.nchunk, S.nmodes, P.cond_rb), P.cond_threads, P.cond_smem, st>>>(g, N, S, F, G, gstride,
                                                                                             R, rstride, P.cond_rows);
 }
@@ -569,11 +566,7 @@ void element_condense(const ElementPlan& P, const DevGeom& g, const DevNumbering
 void element_recover(const ElementPlan& P, const DevGeom& g, const DevNumbering& N, const DevModal& S,
                      const double* F, const double* G, int gstride, const double* R, int rstride, double* U,
                      cudaStream_t st) {
-  static size_t configured = 0;
-  if (P.rec_smem > configured) {
-    cudaFuncSetAttribute(k_elem_recover, cudaFuncAttributeMaxDynamicSharedMemorySize, static_cast<int>(P.rec_smem));
-    configured = P.rec_smem;
-  }
+  raise_smem_limit(reinterpret_cast<const void*>(k_elem_recover), P.rec_smem);
   k_elem_recover<<<dim3(g.nchunk, S.nmodes, P.rec_rb), P.rec_threads, P.rec_smem, st>>>(g, N, S, F, G, gstride, R,
                                                                                         rstride, U, P.rec_rows);
 }
@@ -583,11 +576,7 @@ void element_schur_apply(int dir, const DevGeom& g, const DevNumbering& N, const
   const size_t smem = sizeof(double) * (static_cast<size_t>(g.next) * S.l2_sc_ld +
                                         2 * static_cast<size_t>(g.chunk_max) * element_ld(g.next)) +
                       sizeof(int) * static_cast<size_t>(g.chunk_max) * g.next;
-  static size_t configured = 0;
-  if (smem > 48 * 1024 && smem > configured) {
-    cudaFuncSetAttribute(k_elem_schur, cudaFuncAttributeMaxDynamicSharedMemorySize, static_cast<int>(smem));
-    configured = smem;
-  }
+  raise_smem_limit(reinterpret_cast<const void*>(k_elem_schur), smem);
   // two blocks per chunk and mode: the work is latency-bound
   k_elem_schur<<<dim3(g.nchunk, S.nmodes, 2), 256, smem, st>>>(dir, g, N, S, src, dst, rstride);
 }

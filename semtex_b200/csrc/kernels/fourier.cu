@@ -11,6 +11,7 @@
 // owns 32 consecutive points of every plane: loads and stores of each plane
 // row are coalesced, and the transform runs out of shared memory.
 #include "helmholtz.cuh"
+#include "launch.hpp"
 #include "ptx.cuh"
 
 namespace stx {
@@ -329,15 +330,11 @@ cudaError_t z_transform(double* data, int nz, int plane_size, int sign, const do
     while (n % 5 == 0 && plan.nf < 16) { add(5); n /= 5; }
     if (n != 1) plan.nf = 0;
   }
-  static bool attr_set = false;
-  if (!attr_set) {
-    cudaFuncSetAttribute(k_dft, cudaFuncAttributeMaxDynamicSharedMemorySize, 200 * 1024);
-    cudaFuncSetAttribute(k_fft<32>, cudaFuncAttributeMaxDynamicSharedMemorySize, 200 * 1024);
-    cudaFuncSetAttribute(k_fft<16>, cudaFuncAttributeMaxDynamicSharedMemorySize, 200 * 1024);
-    cudaFuncSetAttribute(k_fft<8>, cudaFuncAttributeMaxDynamicSharedMemorySize, 200 * 1024);
-    cudaFuncSetAttribute(k_fft<4>, cudaFuncAttributeMaxDynamicSharedMemorySize, 200 * 1024);
-    attr_set = true;
-  }
+  raise_smem_limit(reinterpret_cast<const void*>(k_dft), 200 * 1024);
+  raise_smem_limit(reinterpret_cast<const void*>(k_fft<32>), 200 * 1024);
+  raise_smem_limit(reinterpret_cast<const void*>(k_fft<16>), 200 * 1024);
+  raise_smem_limit(reinterpret_cast<const void*>(k_fft<8>), 200 * 1024);
+  raise_smem_limit(reinterpret_cast<const void*>(k_fft<4>), 200 * 1024);
   if (plan.nf > 0) {
     int tp = 32;
     while (tp > 4 && sizeof(double) * (2 * static_cast<size_t>(nz) * tp + 2 * nz + 2) > 160 * 1024) tp /= 2;

@@ -18,6 +18,7 @@
 #include "twolevel.cuh"
 #include "ptx.cuh"
 #include "element.cuh"
+#include "launch.hpp"
 
 #include <algorithm>
 #include <vector>
@@ -969,12 +970,8 @@ cudaError_t helmholtz_direct_solve(const DevGeom& g, const DevNumbering& N, cons
   if (ep.ok) {
     element_condense(ep, g, N, S, F, has_ess ? G : nullptr, rstride, R, rstride, st);
   } else if (chunked) {
-    static int configured = 0;
-    if (!configured) {
-      cudaFuncSetAttribute(k_condense_chunk, cudaFuncAttributeMaxDynamicSharedMemorySize, 200 * 1024);
-      cudaFuncSetAttribute(k_recover_chunk, cudaFuncAttributeMaxDynamicSharedMemorySize, 200 * 1024);
-      configured = 1;
-    }
+    raise_smem_limit(reinterpret_cast<const void*>(k_condense_chunk), 200 * 1024);
+    raise_smem_limit(reinterpret_cast<const void*>(k_recover_chunk), 200 * 1024);
     k_condense_chunk<<<dim3(g.nchunk, S.nmodes), 256, shm_cond, st>>>(g, N, S, F, has_ess ? G : nullptr, rstride,
                                                                       R, rstride);
   } else {
@@ -1013,11 +1010,7 @@ cudaError_t helmholtz_direct_solve(const DevGeom& g, const DevNumbering& N, cons
     }
     Rsol = Y;
   } else if (plan.stages >= 2) {
-    static int configured = 0;
-    if (!configured) {
-      cudaFuncSetAttribute(k_band_sweep, cudaFuncAttributeMaxDynamicSharedMemorySize, 220 * 1024);
-      configured = 1;
-    }
+    raise_smem_limit(reinterpret_cast<const void*>(k_band_sweep), 220 * 1024);
     k_band_sweep<<<S.nmodes, kSweepThreads, plan.smem, st>>>(S, S.fwd, S.dinv_fwd, R, rstride, nz, 0,
                                                              plan.stages, plan.W);
     if (ev) cudaEventRecord(ev[2], st);

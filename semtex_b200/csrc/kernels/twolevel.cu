@@ -21,6 +21,7 @@
 #include <algorithm>
 
 #include "element.cuh"
+#include "launch.hpp"
 #include "ptx.cuh"
 #include "symtile.hpp"
 
@@ -256,18 +257,10 @@ __global__ void __launch_bounds__(32 * kSymWarps)
 }
 
 void configure_psymv() {
-  static bool configured = false;
-  if (!configured) {
-    cudaFuncSetAttribute(k_psymv<double, 1>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                         static_cast<int>(sym_smem<1>()));
-    cudaFuncSetAttribute(k_psymv<float, 1>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                         static_cast<int>(sym_smem<1>()));
-    cudaFuncSetAttribute(k_psymv<double, 2>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                         static_cast<int>(sym_smem<2>()));
-    cudaFuncSetAttribute(k_psymv<double, 3>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                         static_cast<int>(sym_smem<3>()));
-    configured = true;
-  }
+  raise_smem_limit(reinterpret_cast<const void*>(k_psymv<double, 1>), sym_smem<1>());
+  raise_smem_limit(reinterpret_cast<const void*>(k_psymv<float, 1>), sym_smem<1>());
+  raise_smem_limit(reinterpret_cast<const void*>(k_psymv<double, 2>), sym_smem<2>());
+  raise_smem_limit(reinterpret_cast<const void*>(k_psymv<double, 3>), sym_smem<3>());
 }
 
 cudaError_t launch_psymv(const DevModal& S, const SymProblem* probs, const SymWarp* warps, int nwarps,

@@ -256,3 +256,13 @@ def test_graph_replay_matches_direct_steps(tmp_path, case):
         for a, b in ((g1, d1), (g2, d2)):
             err = np.linalg.norm(a[c] - b[c]) / max(np.linalg.norm(b[c]), 1e-300)
             assert err < tol, (c, err)
+
+
+def test_high_order_elements(tmp_path):
+    # N_P = 13: the element kernels' shared memory exceeds the 48 KB default
+    # (the limit is raised per kernel and device).
+    p = sessions.taylor_green_session(str(tmp_path / "tg13"), 2, 13, 4, re=100.0, dt=2e-3, nstep=4,
+                                      extra={"TOL_REL": 1e-14})
+    gpu, t = S.dns(p)
+    D = O.dns_session(p)
+    _compare(p, gpu, D)
