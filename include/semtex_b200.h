@@ -158,6 +158,12 @@ int stx_field_solve_profiled(stx_modal* sys, const double* d_forcing, double* d_
  * stx_field_solve. */
 int stx_field_solve_noalloc(stx_modal* sys, const double* d_forcing, double* d_unknown);
 
+/* Synchronise and read the system's device status word: 0 when every
+ * bounded wait of its solves met its copy; otherwise the solutions since the
+ * word was set are not valid (1 banded sweep, 3 element kernels, 4 packed
+ * skeleton products, 5 z-FFT).  Host-buffer solves check it themselves. */
+int stx_modal_status(stx_modal* sys, int* status);
+
 /* Field::solve for n fields at once, e.g. the velocity components of a
  * viscous substep (dns/integrate.cpp:186-193): solution i of systems[i] with
  * forcing d_forcing[i] (each field its own BC lines).  When the systems
@@ -211,6 +217,8 @@ int stx_dns_get_field(stx_dns* dns, char field, double* h_phys);
  * alternating-form state back to it -- and replayed (token STX_DNS_GRAPH,
  * default 1; capture needs 12 steps left in the call). */
 int stx_dns_advance(stx_dns* dns, int nsteps);
+/* stx_modal_status over every system of the time stepping (0: all valid). */
+int stx_dns_status(stx_dns* dns, int* status);
 /* Length of the captured step cycle (0: none) and the number of graph
  * launches so far. */
 int stx_dns_graph_info(const stx_dns* dns, int* period, long long* launches);

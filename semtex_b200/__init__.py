@@ -196,6 +196,12 @@ class ModalMatrixSys:
     def handle(self):
         return self._h
 
+    def status(self) -> int:
+        """Device status word (stx_modal_status): 0 when every bounded wait met its copy."""
+        v = C.c_int()
+        check(lib().stx_modal_status(self._h, C.byref(v)))
+        return v.value
+
     def info(self, mode: int):
         a, b = C.c_int(), C.c_int()
         check(lib().stx_modal_info(self._h, mode, C.byref(a), C.byref(b)))
@@ -372,6 +378,12 @@ class DNS:
         s, t = C.c_int(), C.c_double()
         check(lib().stx_dns_state(self._h, C.byref(s), C.byref(t)))
         return s.value, t.value
+
+    def status(self) -> int:
+        """Device status of every system (0: every bounded wait met its copy)."""
+        v = C.c_int()
+        check(lib().stx_dns_status(self._h, C.byref(v)))
+        return v.value
 
     def graph_info(self):
         """(cycle length of the captured step graph, graph launches so far)."""

@@ -49,6 +49,7 @@ SIGNATURES = {
     "stx_field_solve_multi": (_i, [_p, _i, _p, _p]),
     "stx_modal_bytes": (_i, [_p, _pd]),
     "stx_modal_launches": (_i, [_p, _pi]),
+    "stx_modal_status": (_i, [_p, _pi]),
     "stx_dns_create": (_i, [_p, _i, C.POINTER(_p)]),
     "stx_dns_destroy": (_i, [_p]),
     "stx_dns_restart": (_i, [_p, _d]),
@@ -61,6 +62,7 @@ SIGNATURES = {
     "stx_dns_divergence_energy": (_i, [_p, _pd]),
     "stx_dns_cfl": (_i, [_p, _pd]),
     "stx_dns_graph_info": (_i, [_p, _pi, C.POINTER(C.c_longlong)]),
+    "stx_dns_status": (_i, [_p, _pi]),
     "stx_elliptic_solve_host": (_i, [_p, _p, _p]),
     "stx_sync": (_i, [_p]),
     "stx_context_stream": (_i, [_p, C.POINTER(_p)]),

@@ -136,14 +136,23 @@ void band_block_inverses(const std::vector<double>& L, int n, int nb, double* ou
 
 using namespace stx;
 
-// Device status word of a DIRECT system: nonzero if a bounded wait inside a
-// banded sweep expired.  Call only after the stream has been synchronised.
-static void check_sweep_status(const stx_modal* sys) {
-  const int* st = sys->store->dm.status;
-  if (!st) return;
+// Device status word of a DIRECT system: nonzero if a bounded wait for a
+// copy expired (1 banded sweep, 3 element kernels, 4 packed skeleton
+// products); every wait is bounded, so the kernels return and the context
+// stays usable, but the solution is not valid.  Read after synchronising.
+static int status_word(const stx_modal* sys) {
+  const int* st = sys->store ? sys->store->dm.status : nullptr;
+  if (!st) return 0;
   int v = 0;
   cuda_check(cudaMemcpy(&v, st, sizeof(int), cudaMemcpyDeviceToHost), "status read");
-  if (v) throw StxError(STX_ECUDA, "banded sweep: bounded wait for a bulk copy expired");
+  return v;
+}
+
+static void check_sweep_status(const stx_modal* sys) {
+  const int v = status_word(sys);
+  if (!v) return;
+  const char* where = v == 1 ? "banded sweep" : v == 3 ? "element kernel" : v == 4 ? "packed skeleton product" : "solve";
+  throw StxError(STX_ECUDA, std::string(where) + ": a bounded wait for a bulk copy expired");
 }
 
 template <class T>
@@ -892,6 +901,16 @@ int stx_field_solve_profiled(stx_modal* sys, const double* d_forcing, double* d_
   });
 }
 
+int stx_modal_status(stx_modal* sys, int* status) {
+  return guarded([&] {
+    if (!sys || !status) throw StxError(STX_EINVAL, "null argument");
+    cudaSetDevice(sys->ctx->device);
+    cuda_check(cudaStreamSynchronize(sys->ctx->stream), "sync");
+    *status = status_word(sys);
+    if (*status == 0 && fft_timeout_flag() > 0) *status = 5;
+  });
+}
+
 int stx_modal_launches(const stx_modal* sys, int* launches) {
   return guarded([&] {
     if (!sys || !launches) throw StxError(STX_EINVAL, "null argument");
@@ -988,7 +1007,20 @@ int stx_elliptic_solve_host(stx_modal* sys, const double* h_forcing, double* h_s
     cuda_check(cudaMemcpy2DAsync(h_solution, sizeof(double) * nplane, dU, sizeof(double) * ps,
                                  sizeof(double) * nplane, nz, cudaMemcpyDeviceToHost, ctx->stream),
                "solution d2h");
+    // the status words travel with the solution (no extra synchronisation)
+    int* fl = ctx->flags();
+    fl[0] = fl[1] = 0;
+    if (sys->store->dm.status)
+      cuda_check(cudaMemcpyAsync(&fl[0], sys->store->dm.status, sizeof(int), cudaMemcpyDeviceToHost, ctx->stream),
+                 "status d2h");
+    if (const int* ft = fft_timeout_address())
+      cuda_check(cudaMemcpyAsync(&fl[1], ft, sizeof(int), cudaMemcpyDeviceToHost, ctx->stream), "status d2h");
     cuda_check(cudaStreamSynchronize(ctx->stream), "sync");
+    if (fl[0]) {
+      const char* where = fl[0] == 1 ? "banded sweep" : fl[0] == 3 ? "element kernel" : "packed skeleton product";
+      throw StxError(STX_ECUDA, std::string(where) + ": a bounded wait for a bulk copy expired");
+    }
+    if (fl[1]) throw StxError(STX_ECUDA, "z-FFT: a bounded wait for a bulk copy expired");
   });
 }
 

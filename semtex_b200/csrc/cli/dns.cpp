@@ -160,6 +160,9 @@ int main(int argc, char** argv) {
       }
     }
   }
+  int status = 0;
+  check(stx_dns_status(dns, &status), "status");
+  if (status) fail("a bounded wait on the device expired: the fields are not valid");
   stx_dns_destroy(dns);
   stx_context_destroy(ctx);
   return EXIT_SUCCESS;

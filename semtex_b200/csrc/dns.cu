@@ -778,6 +778,21 @@ int stx_dns_cfl(stx_dns* d, double* inv_dt) {
   });
 }
 
+int stx_dns_status(stx_dns* d, int* status) {
+  return dns_guarded([&] {
+    if (!d || !status) throw DnsError(STX_EINVAL, "null argument");
+    *status = 0;
+    std::vector<stx_modal*> all(d->vsys.begin(), d->vsys.end());
+    all.push_back(d->psys);
+    for (auto& kv : d->pcg) all.push_back(kv.second);
+    for (stx_modal* m : all) {
+      int v = 0;
+      ckstx(stx_modal_status(m, &v));
+      if (v && !*status) *status = v;
+    }
+  });
+}
+
 int stx_dns_graph_info(const stx_dns* d, int* period, long long* launches) {
   return dns_guarded([&] {
     if (!d) throw DnsError(STX_EINVAL, "null argument");

@@ -187,6 +187,22 @@ __device__ __forceinline__ void stockham_stage(const double* xr, const double* x
 // then leaves its lines untransformed).
 __device__ int g_fft_timeout = 0;
 
+}  // namespace
+
+int fft_timeout_flag() {
+  int v = 0;
+  if (cudaMemcpyFromSymbol(&v, g_fft_timeout, sizeof(int)) != cudaSuccess) return -1;
+  return v;
+}
+
+const int* fft_timeout_address() {
+  void* p = nullptr;
+  if (cudaGetSymbolAddress(&p, g_fft_timeout) != cudaSuccess) return nullptr;
+  return static_cast<const int*>(p);
+}
+
+namespace {
+
 // Real transforms of TPL z-lines per block as TPL/2 complex transforms: the
 // block's rows [n][TPL] are read as complex lines z = x_p + i x_{p+TPL/2}
 // (real part columns 0..TPL/2-1, imaginary part the rest); the two real

@@ -52,6 +52,12 @@ cudaError_t helmholtz_jacpcg_solve(const DevGeom& g, const DevNumbering& N, cons
                                    double tol_rel, int step_max, double* work, int* iters,
                                    cudaStream_t st);
 
+// Nonzero once a bounded wait in the z-FFT expired on the current device
+// (read after the work has been synchronised; -1 if it cannot be read).
+int fft_timeout_flag();
+// Device address of that flag on the current device (null if unavailable).
+const int* fft_timeout_address();
+
 // AuxField::transform (src/auxfield.cpp:1157-1194, femlib/fourier.c:40-165)
 // of nz planes in place: sign +1 forward (scaled by 1/nz), -1 inverse.
 // `twiddle` holds cos/sin(2 pi m / nz), m < nz, as [2][nz].

@@ -148,11 +148,20 @@ struct stx_context {
       aux_ev.push_back(e);
     }
   }
+  // Pinned host words the status flags of a synchronising call are copied
+  // into on the stream (no extra synchronisation): [0] system, [1] z-FFT.
+  int* h_flags = nullptr;
+  int* flags() {
+    if (!h_flags && cudaMallocHost(&h_flags, 2 * sizeof(int)) != cudaSuccess)
+      throw std::runtime_error("cudaMallocHost of the status words failed");
+    return h_flags;
+  }
   ~stx_context() {
     for (auto s : aux) cudaStreamDestroy(s);
     for (auto e : aux_ev) cudaEventDestroy(e);
     if (d_work) cudaFree(d_work);
     if (d_scratch) cudaFree(d_scratch);
+    if (h_flags) cudaFreeHost(h_flags);
   }
 };
 

@@ -66,6 +66,7 @@ def test_two_calls_in_a_row_identical(tmp_path):
     u1 = sysm.solve_host(f).copy()
     u2 = sysm.solve_host(f)
     assert rel_l2(u1, u2) < 1e-14
+    assert sysm.status() == 0   # every bounded wait met its copy
 
 
 def test_device_solve_and_transform(tmp_path):
