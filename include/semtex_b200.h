@@ -217,6 +217,17 @@ int stx_dns_get_field(stx_dns* dns, char field, double* h_phys);
  * alternating-form state back to it -- and replayed (token STX_DNS_GRAPH,
  * default 1; capture needs 12 steps left in the call). */
 int stx_dns_advance(stx_dns* dns, int nsteps);
+/* Running averages (Statistics, src/statistics.cpp; session token AVERAGE
+ * 1: the raw fields, 2: also the velocity products A=uu B=uv C=vv D=uw E=vw
+ * F=ww).  stx_dns_stats_update is Statistics::update (the caller chooses
+ * when: the dns program every IO_HIS steps).  stx_dns_stats_info returns the
+ * averages' names in file order (NUL terminated) and the number of updates,
+ * and sets that number when set_navg >= 0; get / set move one average in
+ * physical space (set: Statistics::initialise from a .avg file). */
+int stx_dns_stats_update(stx_dns* dns);
+int stx_dns_stats_info(stx_dns* dns, char* names, int len, int* navg, int set_navg);
+int stx_dns_stats_get(stx_dns* dns, char name, double* h_phys);
+int stx_dns_stats_set(stx_dns* dns, char name, const double* h_phys);
 /* stx_modal_status over every system of the time stepping (0: all valid). */
 int stx_dns_status(stx_dns* dns, int* status);
 /* Length of the captured step cycle (0: none) and the number of graph

@@ -1384,6 +1384,47 @@ class DNS:
                                     P.bc_lines(c, self.time), tok["TOL_REL"],
                                     tok.ivalue("STEP_MAX"))
 
+    # -- Statistics (src/statistics.cpp:94-405), AVERAGE 1 or 2
+    def stats_init(self, level):
+        names = list(self.P.S.fields)
+        if level > 1:
+            names += [chr(ord("A") + i) for i in range(self.ncom * (self.ncom + 1) // 2)]
+        shape = (self.P.nz, self.P.nel, self.P.np, self.P.np)
+        self.avg = {c: np.zeros(shape) for c in sorted(names)}
+        self.avg_level, self.navg = level, 0
+
+    def stats_update(self):
+        """Statistics::update: weight, add the raw fields (Fourier) and the
+        velocity products (physical), smooth with the first field's
+        numbering, normalise."""
+        n = self.navg
+        for c in self.avg:
+            self.avg[c] = self.avg[c] * n
+        for c in self.P.S.fields:
+            self.avg[c] = self.avg[c] + self.u[c]
+        if self.avg_level > 1:
+            ph = [dft_inverse(self.u[c]) for c in self.vel]
+            pairs = [(0, 0), (0, 1), (1, 1), (0, 2), (1, 2), (2, 2)]
+            for k in range(self.ncom * (self.ncom + 1) // 2):
+                i, j = pairs[k]
+                c = chr(ord("A") + k)
+                self.avg[c] = self.avg[c] + ph[i] * ph[j]
+        for c in self.avg:
+            self.avg[c] = smooth(self.P, self.vel[0], self.avg[c]) / (n + 1)
+        self.navg += 1
+
+    def stats_physical(self):
+        out = {}
+        for c, v in self.avg.items():
+            if c in self.P.S.fields:
+                f = v.copy()
+                if self.P.nz > 1:
+                    f[1] = 0.0
+                out[c] = dft_inverse(f)
+            else:
+                out[c] = v.copy()
+        return out
+
     # -- Analyser (src/analysis.cpp:329-443)
     def _mode_l2(self, F, m):
         """AuxField::mode_L2 (src/auxfield.cpp:919-947): sum over elements of

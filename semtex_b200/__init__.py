@@ -385,6 +385,23 @@ class DNS:
         check(lib().stx_dns_status(self._h, C.byref(v)))
         return v.value
 
+    # -- Statistics (src/statistics.cpp), token AVERAGE 1 or 2
+    def stats_update(self):
+        check(lib().stx_dns_stats_update(self._h))
+
+    def stats(self):
+        """(number of updates, {name: physical average [nz, nel, np, np]})."""
+        buf = C.create_string_buffer(64)
+        n = C.c_int()
+        check(lib().stx_dns_stats_info(self._h, buf, 64, C.byref(n), -1))
+        ctx = self.ctx
+        out = {}
+        for c in buf.value.decode():
+            a = np.empty((ctx.nz, ctx.nel, ctx.np, ctx.np))
+            check(lib().stx_dns_stats_get(self._h, c.encode(), C.c_void_p(a.ctypes.data)))
+            out[c] = a
+        return n.value, out
+
     def graph_info(self):
         """(cycle length of the captured step graph, graph launches so far)."""
         a, b = C.c_int(), C.c_longlong()

@@ -63,6 +63,10 @@ SIGNATURES = {
     "stx_dns_cfl": (_i, [_p, _pd]),
     "stx_dns_graph_info": (_i, [_p, _pi, C.POINTER(C.c_longlong)]),
     "stx_dns_status": (_i, [_p, _pi]),
+    "stx_dns_stats_update": (_i, [_p]),
+    "stx_dns_stats_info": (_i, [_p, _s, _i, _pi, _i]),
+    "stx_dns_stats_get": (_i, [_p, C.c_char, _p]),
+    "stx_dns_stats_set": (_i, [_p, C.c_char, _p]),
     "stx_elliptic_solve_host": (_i, [_p, _p, _p]),
     "stx_sync": (_i, [_p]),
     "stx_context_stream": (_i, [_p, C.POINTER(_p)]),

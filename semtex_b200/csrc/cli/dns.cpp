@@ -9,7 +9,9 @@
 // steps and at the end, to session.chk (previous one kept as .chk.bak) with
 // the final dump to session.fld, or with -chk all appended to session.fld.
 // Every IO_CFL steps the CFL estimate and divergence energy are printed
-// (Analyser::estimateCFL / divergence, src/analysis.cpp:382-443).
+// (Analyser::estimateCFL / divergence, src/analysis.cpp:382-443); with
+// AVERAGE > 0 running averages are updated every IO_HIS steps and written
+// to session.avg with each dump (Statistics, src/statistics.cpp).
 #include <cmath>
 #include <cstdio>
 #include <cstring>
@@ -103,6 +105,23 @@ int main(int argc, char** argv) {
   const int nstep = static_cast<int>(std::lround(token(ctx, "N_STEP")));
   const int io_fld = std::max(1, static_cast<int>(std::lround(token(ctx, "IO_FLD"))));
   const int io_cfl = static_cast<int>(std::lround(token(ctx, "IO_CFL")));
+  const int io_his = std::max(1, static_cast<int>(std::lround(token(ctx, "IO_HIS"))));
+  const bool averaging = token(ctx, "AVERAGE") > 0.0;
+  std::string avg_names;
+  if (averaging) {  // Statistics::initialise: from session.avg, else zero
+    char nb[64];
+    check(stx_dns_stats_info(dns, nb, sizeof(nb), nullptr, -1), "statistics");
+    avg_names = nb;
+    if (std::ifstream(session + ".avg")) {
+      const stx::FieldFile A = stx::read_field(session + ".avg");
+      if (A.names != avg_names) fail(session + ".avg holds other averages than AVERAGE asks for");
+      for (size_t k = 0; k < avg_names.size(); ++k) {
+        if (A.data[k].size() != n) fail(session + ".avg does not match the session");
+        check(stx_dns_stats_set(dns, avg_names[k], A.data[k].data()), "statistics");
+      }
+      check(stx_dns_stats_info(dns, nullptr, 0, nullptr, A.step), "statistics");
+    }
+  }
   const double dt = token(ctx, "D_T");
   const bool chkpoint = !no_chk && token(ctx, "CHKPOINT") != 0.0;
   stx::FieldFile out;
@@ -120,6 +139,7 @@ int main(int argc, char** argv) {
   while (step < nstep) {
     int next = std::min(nstep, (step / io_fld + 1) * io_fld);
     if (io_cfl > 0) next = std::min(next, (step / io_cfl + 1) * io_cfl);
+    if (averaging) next = std::min(next, (step / io_his + 1) * io_his);
     if (verbose) {  // the step line of DNSAnalyser::analyse, one step at a time
       for (; step < next; ++step) {
         check(stx_dns_advance(dns, 1), "integrate");
@@ -142,6 +162,7 @@ int main(int argc, char** argv) {
                   static_cast<int>(100.0 * dt / dt_max));
       std::printf("------- Divergence Energy: %g\n", div);
     }
+    if (averaging && step % io_his == 0) check(stx_dns_stats_update(dns), "statistics");
     const bool periodic = step % io_fld == 0, initial = step == io_fld, final = step == nstep;
     if (periodic || final) {
       for (size_t k = 0; k < fields.size(); ++k)
@@ -157,6 +178,17 @@ int main(int argc, char** argv) {
         }
       } else {
         stx::write_field(session + ".fld", out, !initial);
+      }
+      if (averaging) {  // Statistics::dump: the averages, step = number of updates
+        stx::FieldFile A = out;
+        A.names = avg_names;
+        A.data.assign(avg_names.size(), std::vector<double>(n));
+        int navg = 0;
+        check(stx_dns_stats_info(dns, nullptr, 0, &navg, -1), "statistics");
+        A.step = navg;
+        for (size_t k = 0; k < avg_names.size(); ++k)
+          check(stx_dns_stats_get(dns, avg_names[k], A.data[k].data()), "statistics");
+        stx::write_field(session + ".avg", A);
       }
     }
   }

@@ -121,6 +121,15 @@ struct stx_dns {
   int gtoggle = 0;
   int eager_steady = 0;       // steady steps run directly since the last restart
   long long graph_launches = 0;
+  // Running averages (Statistics, src/statistics.cpp:94-466; token AVERAGE
+  // 1 or 2): buffers named as the reference names them, in its order (the
+  // sorted keys of its map): the raw fields held in Fourier space and, for
+  // AVERAGE 2, the velocity products A = uu, B = uv, C = vv, D = uw, E = vw,
+  // F = ww held in physical space.
+  int avg_level = 0;
+  int navg = 0;
+  std::string avg_names;
+  std::vector<double*> avg_buf;
 };
 
 namespace {
@@ -522,6 +531,20 @@ int stx_dns_create(stx_context* ctx, int advection, stx_dns** out) {
       for (const auto& E : ctx->fields.at(c).N.edges) td = td || depends_on_t(E.expr);
       d->tdep.push_back(td);
     }
+    // -- running averages (Statistics::Statistics)
+    d->avg_level = S.tokens.has("AVERAGE") ? S.tokens.ivalue("AVERAGE") : 0;
+    if (d->avg_level < 0 || d->avg_level > 2)
+      throw DnsError(STX_EUNSUPPORTED, "AVERAGE must be 0, 1 or 2 (energy-equation correlations are not built)");
+    if (d->avg_level > 0) {
+      std::string names = d->names;
+      if (d->avg_level > 1)
+        for (int i = 0; i < d->ncom * (d->ncom + 1) / 2; ++i) names.push_back(static_cast<char>('A' + i));
+      std::sort(names.begin(), names.end());
+      d->avg_names = names;
+      double* ab = static_cast<double*>(d->arena.alloc(sizeof(double) * d->fsize * names.size()));
+      ck(cudaMemset(ab, 0, sizeof(double) * d->fsize * names.size()), "memset");
+      for (size_t k = 0; k < names.size(); ++k) d->avg_buf.push_back(ab + d->fsize * k);
+    }
     // -- 3/2-rule products: padded buffers and the length-nz32 twiddles
     if (S.tokens.has("DEALIAS") && S.tokens.ivalue("DEALIAS") > 0 && g.nz > 2) {
       d->nz32 = 3 * g.nz / 2;
@@ -790,6 +813,115 @@ int stx_dns_status(stx_dns* d, int* status) {
       ckstx(stx_modal_status(m, &v));
       if (v && !*status) *status = v;
     }
+  });
+}
+
+namespace {
+
+void combine2(stx_dns* d, double* out, double a, const double* x, double b, const double* y) {
+  CombineArgs c{};
+  c.n = 0;
+  c.c[c.n] = a;
+  c.p[c.n++] = x;
+  if (y) {
+    c.c[c.n] = b;
+    c.p[c.n++] = y;
+  }
+  c.out = out;
+  ck(dns_combine(d->ctx->dg, c, d->ctx->stream), "combine");
+}
+
+double* avg_buffer(stx_dns* d, char name) {
+  const size_t k = d->avg_names.find(name);
+  if (k == std::string::npos) throw DnsError(STX_EINVAL, std::string("no average ") + name);
+  return d->avg_buf[k];
+}
+
+}  // namespace
+
+int stx_dns_stats_update(stx_dns* d) {
+  return dns_guarded([&] {
+    if (!d) throw DnsError(STX_EINVAL, "null argument");
+    if (!d->avg_level) throw DnsError(STX_EINVAL, "no averaging (token AVERAGE)");
+    stx_context* ctx = d->ctx;
+    cudaSetDevice(ctx->device);
+    const double n = d->navg;
+    // Statistics::update (src/statistics.cpp:206-405): weight the old
+    // averages, add the raw fields and the velocity products, smooth,
+    // normalise.
+    for (double* b : d->avg_buf) combine2(d, b, n, b, 0.0, nullptr);
+    for (size_t i = 0; i < d->names.size(); ++i) {
+      double* b = avg_buffer(d, d->names[i]);
+      combine2(d, b, 1.0, b, 1.0, d->u[i]);
+    }
+    if (d->avg_level > 1) {
+      for (int i = 0; i < d->ncom; ++i) {
+        copy(d, d->Up[i], d->u[i]);
+        transform(d, d->Up[i], STX_INVERSE);
+      }
+      const int pi[6] = {0, 0, 1, 0, 1, 2}, pj[6] = {0, 1, 1, 2, 2, 2};
+      for (int k = 0; k < d->ncom * (d->ncom + 1) / 2; ++k) {
+        ck(dns_product(ctx->dg, d->Up[pi[k]], d->Up[pj[k]], d->tmp0, ctx->stream), "product");
+        double* b = avg_buffer(d, static_cast<char>('A' + k));
+        combine2(d, b, 1.0, b, 1.0, d->tmp0);
+      }
+    }
+    const DevNumbering& Nm = ctx->fields.at(d->names[0]).dn;
+    for (double* b : d->avg_buf) {
+      ck(dns_smooth(ctx->dg, Nm, b, d->dsswork, ctx->stream), "smooth");
+      combine2(d, b, 1.0 / (n + 1.0), b, 0.0, nullptr);
+    }
+    ++d->navg;
+    ck(cudaGetLastError(), "stats");
+  });
+}
+
+int stx_dns_stats_info(stx_dns* d, char* names, int len, int* navg, int set_navg) {
+  return dns_guarded([&] {
+    if (!d) throw DnsError(STX_EINVAL, "null argument");
+    if (set_navg >= 0) d->navg = set_navg;
+    if (navg) *navg = d->navg;
+    if (names) {
+      if (len < static_cast<int>(d->avg_names.size()) + 1) throw DnsError(STX_EINVAL, "name buffer too short");
+      std::memcpy(names, d->avg_names.c_str(), d->avg_names.size() + 1);
+    }
+  });
+}
+
+int stx_dns_stats_get(stx_dns* d, char name, double* h_phys) {
+  return dns_guarded([&] {
+    if (!d || !h_phys) throw DnsError(STX_EINVAL, "null argument");
+    const Mesh& M = d->ctx->M;
+    cudaSetDevice(d->ctx->device);
+    double* b = avg_buffer(d, name);
+    copy(d, d->tmp0, b);
+    if (d->names.find(name) != std::string::npos) {  // raw averages are held in Fourier space
+      if (M.nz > 1)
+        ck(cudaMemsetAsync(d->tmp0 + M.plane_size, 0, sizeof(double) * M.plane_size, d->ctx->stream), "nyq");
+      transform(d, d->tmp0, STX_INVERSE);
+    }
+    ck(cudaMemcpy2DAsync(h_phys, sizeof(double) * M.nplane, d->tmp0, sizeof(double) * M.plane_size,
+                         sizeof(double) * M.nplane, M.nz, cudaMemcpyDeviceToHost, d->ctx->stream),
+       "download");
+    ck(cudaStreamSynchronize(d->ctx->stream), "sync");
+  });
+}
+
+int stx_dns_stats_set(stx_dns* d, char name, const double* h_phys) {
+  return dns_guarded([&] {
+    if (!d || !h_phys) throw DnsError(STX_EINVAL, "null argument");
+    const Mesh& M = d->ctx->M;
+    cudaSetDevice(d->ctx->device);
+    double* b = avg_buffer(d, name);
+    ck(cudaMemsetAsync(b, 0, sizeof(double) * d->fsize, d->ctx->stream), "zero");
+    ck(cudaMemcpy2DAsync(b, sizeof(double) * M.plane_size, h_phys, sizeof(double) * M.nplane,
+                         sizeof(double) * M.nplane, M.nz, cudaMemcpyHostToDevice, d->ctx->stream),
+       "upload");
+    if (d->names.find(name) != std::string::npos) {  // Statistics::initialise: raw data to Fourier space
+      transform(d, b, STX_FORWARD);
+      if (M.nz > 1) ck(cudaMemsetAsync(b + M.plane_size, 0, sizeof(double) * M.plane_size, d->ctx->stream), "nyq");
+    }
+    ck(cudaStreamSynchronize(d->ctx->stream), "sync");
   });
 }
 

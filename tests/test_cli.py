@@ -63,3 +63,28 @@ def test_dns_program_regression_workflow(tmp_path, name):
         err = np.abs(P.evaluate(funcs[c], t) - flds[c]).max()
         got = "noise-level" if err < 1e-12 else f"{err:.4e}"
         assert got == GOLD[name][c], (name, c, got)
+
+
+@pytest.mark.gpu
+def test_dns_program_writes_averages(tmp_path):
+    # AVERAGE = 2: running averages updated every IO_HIS steps, written to
+    # session.avg with the dumps (step = number of updates), names in the
+    # reference's order.
+    from semtex_b200 import sessions
+    path = sessions.taylor_green_session(str(tmp_path / "tgavg"), 3, 6, 8, re=100.0, dt=2e-3, nstep=12,
+                                         extra={"TOL_REL": 1e-14, "AVERAGE": 2, "IO_HIS": 3, "IO_FLD": 6})
+    S = O.read_session(path)
+    P = O.Problem(S)
+    funcs = O.user_functions(S)
+    ic = {c: P.evaluate(funcs[c], 0.0) for c in S.fields if c in funcs}
+    write_field(path + ".rst", "tgavg", P.np, P.nz, P.nel, 0, 0.0, S.tokens["D_T"], S.tokens["KINVIS"],
+                S.tokens["BETA"], ic)
+    r = subprocess.run([os.path.join(BIN, "dns"), path], capture_output=True, text=True, timeout=600)
+    assert r.returncode == 0, r.stderr
+    hdr, avg = read_field(path + ".avg")
+    assert hdr["fields"] == "ABCDEFpuvw" and hdr["step"] == 4
+    hdr, chk = read_field(path + ".chk")
+    assert hdr["step"] == 6
+    hdr, fld = read_field(path + ".fld")
+    assert hdr["step"] == 12
+    assert np.all(np.isfinite(avg["A"])) and np.abs(avg["A"]).max() > 0.1

@@ -266,3 +266,40 @@ def test_high_order_elements(tmp_path):
     gpu, t = S.dns(p)
     D = O.dns_session(p)
     _compare(p, gpu, D)
+
+
+@pytest.mark.parametrize("nz", [8, 1])
+def test_running_statistics(tmp_path, nz):
+    # Statistics (token AVERAGE = 2): running averages of u, v, (w,) p and
+    # the velocity products, updated every 3 steps, against the oracle.
+    if nz > 1:
+        p = sessions.taylor_green_session(str(tmp_path / "tgs"), 3, 6, nz, re=100.0, dt=2e-3, nstep=12,
+                                          extra={"TOL_REL": 1e-14, "AVERAGE": 2})
+    else:
+        p = sessions.channel_session(str(tmp_path / "chs"), 4, 2, 6, 1, nstep=12,
+                                     extra={"TOL_REL": 1e-14, "AVERAGE": 2})
+    ctx = S.Context(p)
+    x, y = ctx.mesh_coords()
+    if nz > 1:
+        funcs = S._user_functions(p)
+        ic = {c: ctx.evaluate(funcs[c], 0.0) for c in ctx.fields if c in funcs}
+    else:
+        ic = {c: v for c, v in sessions.channel_initial(x, y, [0.0], amplitude=0.05).items() if c in ctx.fields}
+    D = S.DNS(ctx, 1)
+    D.restart(ic, 0.0)
+    Do = O.DNS(O.Problem(O.read_session(p)), ic)
+    Do.stats_init(2)
+    for _ in range(4):
+        D.advance(3)
+        D.stats_update()
+        Do.advance(3)
+        Do.stats_update()
+    n, avg = D.stats()
+    D.close()
+    ctx.close()
+    ref = Do.stats_physical()
+    assert n == 4 and sorted(avg) == sorted(ref)
+    for c in ref:
+        scale = max(np.linalg.norm(ref[c]), 1e-300)
+        tol = 1e-9 if c == "p" else 1e-10
+        assert np.linalg.norm(avg[c] - ref[c]) / scale < tol, (c, np.linalg.norm(avg[c] - ref[c]) / scale)
