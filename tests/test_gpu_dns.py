@@ -303,3 +303,21 @@ def test_running_statistics(tmp_path, nz):
         scale = max(np.linalg.norm(ref[c]), 1e-300)
         tol = 1e-9 if c == "p" else 1e-10
         assert np.linalg.norm(avg[c] - ref[c]) / scale < tol, (c, np.linalg.norm(avg[c] - ref[c]) / scale)
+
+
+@pytest.mark.parametrize("nz", [1, 4])
+def test_low_order_dns(tmp_path, nz):
+    p = sessions.channel_session(str(tmp_path / "lo"), 3, 2, 3, nz, nstep=5, extra={"TOL_REL": 1e-14})
+    ctx = S.Context(p)
+    x, y = ctx.mesh_coords()
+    ic = {c: v for c, v in sessions.channel_initial(x, y, np.arange(ctx.nz) * 2 * np.pi / ctx.nz,
+                                                      amplitude=0.05).items() if c in ctx.fields}
+    D = S.DNS(ctx, 1)
+    D.restart(ic, 0.0)
+    D.advance(5)
+    gpu = {c: D.field(c) for c in ctx.fields}
+    D.close()
+    ctx.close()
+    Do = O.DNS(O.Problem(O.read_session(p)), ic)
+    Do.advance(5)
+    _compare(p, gpu, Do)

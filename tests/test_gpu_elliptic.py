@@ -194,3 +194,16 @@ def test_mixed_bc_fourier(tmp_path, solver):
         S.ModalMatrixSys(ctx, "c", 1.0, method=S.MIXED)
     sysm.close()
     ctx.close()
+
+
+@pytest.mark.parametrize("n,np_,nz", [(4, 2, 4), (3, 3, 8), (5, 4, 2), (1, 5, 4), (2, 2, 1)])
+def test_edge_sizes(tmp_path, n, np_, nz):
+    """Linear elements (N_P = 2: no interior nodes), quadratics, N_Z = 2 (mean
+    and Nyquist planes only), a single element; direct and PCG."""
+    p, ctx, f = _random_case(tmp_path, n, np_, nz, seed=n * 1000 + np_ * 10 + nz)
+    P, U = O.elliptic(p, forcing_phys=f)
+    u = S.ModalMatrixSys(ctx, "c", 1.0).solve_host(f)
+    assert rel_l2(u, U) < TOL, rel_l2(u, U)
+    ctx2 = S.Context(p, {"ITERATIVE": 1, "TOL_REL": 1e-14})
+    ui = S.ModalMatrixSys(ctx2, "c", 1.0, method=S.JACPCG).solve_host(f)
+    assert rel_l2(ui, U) < 1e-9, rel_l2(ui, U)
