@@ -85,9 +85,9 @@ struct SymCursor {
 
 // y[idx] += scale A x[idx] for every problem (and each of NF fields whose
 // vectors are fstride doubles apart): each warp streams its run of tiles
-// (SymWarp) through a two-buffer ring.  For a tile, lane 0 bulk-copies the
-// tile and every lane copies (cp.async) the x entries of the tile's column
-// and row blocks, all completing on the buffer's mbarrier (count 1 + 32).
+// (SymWarp) through a ring of kSymStages buffers.  For a tile, lane 0
+// bulk-copies the tile and every lane copies (cp.async) the x entries of the
+// tile's column and row blocks, all completing on the buffer's mbarrier (count 1 + 32).
 // Per tile (I, J): direct part y_I += A_IJ x_J (lane = tile row), and for
 // J < I the transposed part y_J += A_IJ^T x_I (lane = tile column), four
 // independent partial sums per plane; y_I is accumulated along the row and
