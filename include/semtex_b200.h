@@ -96,6 +96,16 @@ int stx_mesh_families(const stx_context* ctx, int* nfamily);
  * h_out[nz*nel*np*np] (physical space, unpadded planes). */
 int stx_field_evaluate(const stx_context* ctx, const char* expr, double t, double* h_out);
 
+/* The expression evaluator on its own, host only (no device, no context):
+ * `expr` of x, y, z, t evaluated at n points, with the default token table
+ * (femlib/defaults.h:10-96) plus `assignments` ("NAME = expr" separated by
+ * ';', or null).  compiled = 0: the interpreter (femlib/initial.y:138-249
+ * restated); 1: the postfix program the device runs for forcing fields and
+ * spatio-temporal forcing (dns/fieldforce.cpp:463-514), on the host.  *nops
+ * (if not null) receives the program length after constant folding. */
+int stx_expression_eval(const char* expr, const char* assignments, int compiled, int n, const double* x,
+                        const double* y, const double* z, double t, double* out, int* nops);
+
 /* Evaluate a field's boundary values at time t in physical space on every
  * plane and Fourier-transform them (Field::evaluateBoundaries +
  * Field::bTransform, src/field.cpp:160-243).  Synchronises. */

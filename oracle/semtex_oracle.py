@@ -118,6 +118,7 @@ class Session:
     elements: np.ndarray         # [nel, 4] zero-based node ids (CCW)
     surfaces: list               # (elmt, side, 'B', group) | (elmt, side, 'P', (me, ms))
     user: list = dfield(default_factory=list)
+    force: list | None = None    # raw lines of the FORCE section, None if absent
 
 
 def _section(text: str, name: str):
@@ -199,9 +200,34 @@ def read_session(path: str, overrides: dict | None = None) -> Session:
         raise NotImplementedError("curved sides are outside the oracle's scope")
     _, body = _section(text, "USER")
     user = _lines(body) if body else []
+    _, body = _section(text, "FORCE")
+    force = None if body is None else [ln.rstrip("\r") for ln in body.split("\n")[1:]]
     name = os.path.basename(path)
     return Session(name, tok, fields, groups, bcs, nodes, np.array(elems, int),
-                   surfaces, user)
+                   surfaces, user, force)
+
+
+def force_value(S: Session, token: str):
+    """FEML::valueFromSection on the FORCE section (src/feml.cpp:519-560):
+    the first line whose first word (words end at tab, '=' or space) is
+    `token` gives the text after it up to the next '='.  A '#' line is read
+    together with the line after it and both are skipped.  None if absent."""
+    lines = S.force or []
+    k = 0
+    while k < len(lines):
+        s = lines[k]
+        k += 1
+        if s.startswith("#"):
+            k += 1
+            continue
+        m = re.match(r"[\t= ]*([^\t= ]+)", s)
+        if not m or m.group(1) != token:
+            continue
+        rest = s[m.end(1) + 1:] if m.end(1) < len(s) else ""
+        rest = rest.lstrip("=")
+        val = rest.split("=", 1)[0]
+        return val if val else None
+    return None
 
 
 # ---------------------------------------------------------------------------
@@ -1178,6 +1204,162 @@ class DNS:
         self.vsys = {c: P.modal_systems(c, lam, "DIRECT", self.cache) for c in self.vel}
         self.psys = P.modal_systems(self.pname, 0.0, "DIRECT", self.cache)
         self._hopbc_setup()
+        self._force_setup()
+
+    # -- Body forcing (FieldForce, dns/fieldforce.cpp:31-137, and the
+    #    VirtualForce classes :240-822), on the grid of the products.
+    def _force_grid(self, expr, t):
+        P, M = self.P, self.P.M
+        nzl = 3 * P.nz // 2 if self.dealias else P.nz
+        dz = 2 * math.pi / P.S.tokens["BETA"] / nzl
+        out = np.empty((nzl,) + M.x.shape)
+        for k in range(nzl):
+            val = P.S.tokens.evaluate(expr, x=M.x, y=M.y, z=k * dz, t=t)
+            out[k] = np.broadcast_to(np.asarray(val, float), M.x.shape)
+        return out
+
+    def _force_file(self, fname):
+        hdr, flds = read_field(fname.strip())
+        P = self.P
+        shape = (P.nz, P.nel, P.np, P.np)
+        return [np.asarray(flds[c], float).reshape(shape) if c in flds else np.zeros(shape)
+                for c in "uvw"[:self.ncom]]
+
+    def _force_setup(self):
+        S, tok = self.P.S, self.P.S.tokens
+        self.force = None
+        if S.force is None:
+            return
+        t0 = tok["t"]
+        xyz = "XYZ"
+
+        def val(name):
+            v = force_value(S, name)
+            return None if v is None else float(tok.evaluate(v))
+
+        F = {"const": [val("CONST_" + xyz[i]) or 0.0 for i in range(self.ncom)]}
+        for i in range(self.ncom):
+            if abs(val("WHITE_EPS_" + xyz[i]) or 0.0) > EPSDP:
+                raise NotImplementedError("white-noise forcing")
+        fname = force_value(S, "STEADY_FILE")
+        if fname is not None:
+            F["steady"] = self._force_file(fname)
+        else:
+            F["steady"] = [None if force_value(S, "STEADY_" + xyz[i]) is None
+                           else self._force_grid(force_value(S, "STEADY_" + xyz[i]), t0)
+                           for i in range(self.ncom)]
+        alpha = [force_value(S, "MOD_ALPHA_" + xyz[i]) for i in range(self.ncom)]
+        F["alpha"] = [a if a is not None else "0" for a in alpha]
+        F["moda"] = [None] * self.ncom
+        if any(a is not None for a in alpha):
+            fname = force_value(S, "MOD_A_FILE")
+            if fname is not None:
+                F["moda"] = self._force_file(fname)
+            else:
+                F["moda"] = [None if force_value(S, "MOD_A_" + xyz[i]) is None
+                             else self._force_grid(force_value(S, "MOD_A_" + xyz[i]), t0)
+                             for i in range(self.ncom)]
+        F["st"] = [force_value(S, "SPATIOTEMP_ALPHA_" + xyz[i]) for i in range(self.ncom)]
+        F["mask"] = None
+        m = force_value(S, "SPONGE_M")
+        if m is not None:
+            F["mask"] = self._force_grid(m, t0)
+            F["mask_expr"] = m
+            upd = force_value(S, "SPONGE_UPDATE")
+            F["update"] = 0 if upd is None else int(round(float(tok.evaluate(upd))))
+            F["uref"] = [self._force_grid(force_value(S, "SPONGE_" + "UVW"[i]) or "0", t0)
+                         for i in range(self.ncom)]
+        d = force_value(S, "DRAG_M")
+        F["drag"] = None if d is None else self._force_grid(d, t0)
+        uns = force_value(S, "CORIOLIS_UNSTEADY")
+        uns = 0 if uns is None else int(round(float(tok.evaluate(uns))))
+        omega, domega, on = ["0"] * 3, ["0"] * 3, False
+        for i in range(3):
+            if self.ncom == 3 or i == 2:
+                v = force_value(S, "CORIOLIS_OMEGA_" + xyz[i])
+                if v is not None:
+                    omega[i], on = v, True
+                v = force_value(S, f"CORIOLIS_DOMEGA_{xyz[i]}_DT")
+                if uns and v is not None:
+                    domega[i] = v
+        F["coriolis"] = (2 if uns else 1) if on else 0
+        F["omega"], F["domega"] = omega, domega
+        F["m2o"] = [-2.0 * float(tok.evaluate(o)) for o in omega]
+        F["o"], F["mo"], F["dodt"] = [0.0] * 3, [0.0] * 3, [0.0] * 3
+        dl, ch = val("SFD_DELTA"), val("SFD_CHI")
+        F["qbar"] = None
+        if dl is not None or ch is not None:
+            if dl is None or ch is None:
+                raise ValueError("SFD_DELTA and SFD_CHI must be paired.")
+            F["chi"], F["rate"] = ch, self.dt / dl
+            F["qbar"] = [None] * self.ncom
+        self.force = F
+
+    def _force_physical(self, i, n, Uphys):
+        """FieldForce::addPhysical (dns/fieldforce.cpp:75-107) for component i."""
+        F = self.force
+        if F is None:
+            return n
+        P, M, tok = self.P, self.P.M, self.P.S.tokens
+        t = self.time
+        nzl = n.shape[0]
+        dz = 2 * math.pi / tok["BETA"] / nzl
+        X, Y = M.x[None], M.y[None]
+        Z = (np.arange(nzl) * dz)[:, None, None, None]
+        f = np.zeros_like(n)
+        if F["mask"] is not None:                        # SpongeForce (:563-578)
+            if F["update"] and self.step % F["update"] == 0:
+                F["mask"] = self._force_grid(F["mask_expr"], t)
+            f = (F["uref"][i] - Uphys[i]) * F["mask"]
+        if F["coriolis"]:                                # CoriolisForce (:726-756)
+            def cross_x(c, a):                           # (a x X)_c, src/element.cpp:1752-1785
+                if c == 0:
+                    return a[1] * Z - a[2] * Y
+                if c == 1:
+                    return a[2] * X - a[0] * Z
+                return a[0] * Y - a[1] * X
+
+            def cross(c, a, b):                          # src/auxfield.cpp:325-383
+                if self.ncom == 2:
+                    return -2.0 * a[2] * b[1] if c == 0 else 2.0 * a[2] * b[0]
+                c0, c1 = (1, 2, 0)[c], (2, 0, 1)[c]
+                return a[c0] * b[c1] - a[c1] * b[c0]
+
+            if F["coriolis"] == 2:
+                if i == 0:
+                    for c in ((2,) if self.ncom == 2 else range(3)):
+                        F["o"][c] = float(tok.evaluate(F["omega"][c], t=t))
+                        F["mo"][c] = -F["o"][c]
+                        F["m2o"][c] = -2.0 * F["o"][c]
+                        F["dodt"][c] = -float(tok.evaluate(F["domega"][c], t=t))
+                f = f + cross_x(i, F["dodt"])
+                w = [cross_x(c, F["mo"]) for c in range(self.ncom)]
+                f = f + cross(i, F["o"], w)
+            f = f + cross(i, F["m2o"], Uphys)
+        if F["steady"][i] is not None:                   # SteadyForce (:335-344)
+            f = f + F["steady"][i]
+        if F["moda"][i] is not None:                     # ModulatedForce (:449-460)
+            alpha = float(tok.evaluate(F["alpha"][i], t=t))
+            if abs(alpha) > EPSDP:
+                f = f + alpha * F["moda"][i]
+        if F["st"][i] is not None:                       # SpatioTemporalForce (:499-514)
+            f = f + self._force_grid(F["st"][i], t)
+        if F["drag"] is not None:                        # DragForce (:614-628)
+            mag = np.sqrt(sum(u * u for u in Uphys))
+            f = f - mag * F["drag"] * Uphys[i]
+        if F["qbar"] is not None:                        # SFDForce (:792-822)
+            if F["qbar"][i] is None:
+                F["qbar"][i] = Uphys[i].copy()
+            q = F["qbar"][i]
+            f = f - F["chi"] * Uphys[i] + F["chi"] * q
+            F["qbar"][i] = q * (1.0 - F["rate"]) + F["rate"] * Uphys[i]
+        return n + f
+
+    def _force_fourier(self, i, N):
+        """FieldForce::addFourier (dns/fieldforce.cpp:110-137): ConstForce."""
+        if self.force is not None and abs(self.force["const"][i]) > EPSDP:
+            N[0] += self.force["const"][i]
+        return N
 
     # -- High-order pressure BCs (BCmgr::buildComputedBCs / maintainFourier /
     #    evaluateCNBCp, src/bcmgr.cpp:937-996, 1036-1296, 1299-1331;
@@ -1326,7 +1508,9 @@ class DNS:
                     n -= tmp
             if len(forms) == 2:
                 n *= 0.5
+            n = self._force_physical(i, n, Uphys)
             n = self._forward32(n)
+            n = self._force_fourier(i, n)
             N.append(smooth(P, self.vel[0], n))
         if self.advection == 1:
             self.toggle = 1 - self.toggle

@@ -27,7 +27,7 @@ from .fieldfile import read_field, write_field
 
 DIRECT, JACPCG, MIXED = STX_DIRECT, STX_JACPCG, STX_MIXED
 
-__all__ = ["Context", "ModalMatrixSys", "Field", "DNS", "Batch", "numbering", "solve_multi", "elliptic", "dns", "read_field",
+__all__ = ["Context", "ModalMatrixSys", "Field", "DNS", "Batch", "expression", "numbering", "solve_multi", "elliptic", "dns", "read_field",
            "write_field", "FORWARD", "INVERSE", "DIRECT", "JACPCG", "MIXED", "StxError"]
 
 
@@ -275,6 +275,21 @@ class Batch:
             self.close()
         except Exception:
             pass
+
+
+def expression(expr: str, x, y, z, t: float = 0.0, assignments: str | None = None, compiled: bool = True):
+    """The session-expression evaluator on the host (no device): `expr` at the
+    points (x, y, z) and time t.  compiled=True runs the postfix program the
+    device runs for forcing fields; False the interpreter.  Returns (values,
+    program length)."""
+    x, y, z = (np.ascontiguousarray(np.broadcast_to(np.asarray(v, float), np.broadcast(x, y, z).shape)).ravel()
+               for v in (x, y, z))
+    out = np.empty_like(x)
+    nops = C.c_int(0)
+    check(lib().stx_expression_eval(expr.encode(), assignments.encode() if assignments else None, int(compiled),
+                                     x.size, x.ctypes.data, y.ctypes.data, z.ctypes.data, float(t),
+                                     out.ctypes.data, C.byref(nops)))
+    return out, nops.value
 
 
 def numbering(session: str, field: str, overrides=None):

@@ -392,6 +392,39 @@ int stx_field_evaluate(const stx_context* ctx, const char* expr, double t, doubl
   });
 }
 
+int stx_expression_eval(const char* expr, const char* assignments, int compiled, int n, const double* x,
+                        const double* y, const double* z, double t, double* out, int* nops) {
+  return guarded([&] {
+    if (!expr || n < 0 || (n > 0 && (!x || !y || !z || !out))) throw StxError(STX_EINVAL, "bad argument");
+    TokenTable T;
+    if (assignments) {
+      std::string all(assignments), item;
+      for (size_t a = 0; a <= all.size();) {
+        size_t b = all.find(';', a);
+        if (b == std::string::npos) b = all.size();
+        item = all.substr(a, b - a);
+        if (item.find_first_not_of(" \t") != std::string::npos) T.assign(item);
+        a = b + 1;
+      }
+    }
+    if (compiled) {
+      const ExprProgram P = T.compile(expr);
+      if (nops) *nops = static_cast<int>(P.ops.size());
+      for (int i = 0; i < n; ++i) out[i] = P.run(x[i], y[i], z[i], t);
+    } else {
+      if (nops) *nops = 0;
+      std::map<std::string, double> vars;
+      vars["t"] = t;
+      for (int i = 0; i < n; ++i) {
+        vars["x"] = x[i];
+        vars["y"] = y[i];
+        vars["z"] = z[i];
+        out[i] = T.eval(expr, &vars);
+      }
+    }
+  });
+}
+
 int stx_field_bc_evaluate(stx_context* ctx, char field, double t) {
   return guarded([&] {
     if (!ctx) throw StxError(STX_EINVAL, "null context");

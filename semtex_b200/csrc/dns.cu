@@ -3,7 +3,8 @@
 // Host restatement of integrate() (dns/integrate.cpp:66-200): the same
 // multi-level storage Us / Uf rolled by pointer (rollm, src/sem.h:108-122),
 // the same sub-steps in the same order, every field operation a device
-// kernel.  Cartesian coordinates; no body forcing; velocity BCs essential or
+// kernel.  Cartesian coordinates; body forcing from the <FORCE> section
+// (FieldForce, dns/fieldforce.cpp) except white noise; velocity BCs essential or
 // natural (time-dependent values re-evaluated each step); pressure BCs
 // essential, natural or high-order (<H>, BCmgr::maintainFourier /
 // evaluateCNBCp, src/bcmgr.cpp:1036-1331, computed on the device each step).
@@ -19,7 +20,9 @@
 #include <vector>
 
 #include "../../include/semtex_b200.h"
+#include "host/fieldfile.hpp"
 #include "kernels/dns_kernels.cuh"
+#include "kernels/force.cuh"
 #include "kernels/helmholtz.cuh"
 #include "stx_internal.hpp"
 
@@ -130,6 +133,38 @@ struct stx_dns {
   int navg = 0;
   std::string avg_names;
   std::vector<double*> avg_buf;
+  // Body forcing (<FORCE>; FieldForce and its classes, dns/fieldforce.cpp),
+  // on the grid of the nonlinear products (nzl planes: N_Z, or 3 N_Z / 2
+  // with DEALIAS).  Fields are device arrays of nzl planes, null when a term
+  // is absent; time-dependent scalars are evaluated on the host each step.
+  struct Force {
+    bool on = false;        // FORCE section present
+    bool physical = false;  // some physical-space term present
+    bool tdep = false;      // some term changes from step to step
+    double cst[3] = {0.0, 0.0, 0.0};  // ConstForce
+    int nzl = 0;
+    double dz = 0.0;
+    double* x = nullptr;  // node coordinates [nplane]
+    double* y = nullptr;
+    double* mask = nullptr;  // SpongeForce
+    double* uref[3] = {nullptr, nullptr, nullptr};
+    int sponge_update = 0;
+    ExprOp* mask_prog = nullptr;
+    int nmask = 0;
+    int coriolis = 0;  // CoriolisForce: 0 off, 1 steady, 2 unsteady
+    std::string omega[3], domega[3];
+    double m2o[3] = {0.0, 0.0, 0.0}, o[3] = {0.0, 0.0, 0.0}, mo[3] = {0.0, 0.0, 0.0},
+           dodt[3] = {0.0, 0.0, 0.0};
+    double* steady[3] = {nullptr, nullptr, nullptr};  // SteadyForce
+    std::string alpha[3];                              // ModulatedForce
+    double* moda[3] = {nullptr, nullptr, nullptr};
+    ExprOp* st[3] = {nullptr, nullptr, nullptr};  // SpatioTemporalForce
+    int nst[3] = {0, 0, 0};
+    double* drag = nullptr;  // DragForce
+    double* qbar[3] = {nullptr, nullptr, nullptr};  // SFDForce
+    double chi = 0.0, rate = 0.0;
+    bool sfd_started = false;
+  } force;
 };
 
 namespace {
@@ -162,6 +197,258 @@ void forward32(stx_dns* d, double* io, double* out) {
   if (out) ck(cudaMemcpyAsync(out, io, sizeof(double) * nz * ps, cudaMemcpyDeviceToDevice, ctx->stream), "truncate");
 }
 
+// -- body forcing (dns/fieldforce.cpp) ------------------------------------
+
+constexpr double kEpsDp = 6.0e-14;  // EPSDP, veclib/cveclib.h:58
+
+ExprOp* upload_program(stx_dns* d, const ExprProgram& P) {
+  auto* p = static_cast<ExprOp*>(d->arena.alloc(sizeof(ExprOp) * std::max<size_t>(P.ops.size(), 1)));
+  if (!P.ops.empty())
+    ck(cudaMemcpy(p, P.ops.data(), sizeof(ExprOp) * P.ops.size(), cudaMemcpyHostToDevice), "program upload");
+  return p;
+}
+
+// A forcing field: the expression at every node of the forcing grid (the
+// reference's AuxField = "expr"), evaluated on the device.
+double* force_field(stx_dns* d, const std::string& expr) {
+  auto& F = d->force;
+  const Mesh& M = d->ctx->M;
+  const size_t n = static_cast<size_t>(F.nzl) * M.plane_size;
+  auto* f = static_cast<double*>(d->arena.alloc(sizeof(double) * n));
+  ck(cudaMemset(f, 0, sizeof(double) * n), "memset");
+  const ExprProgram P = d->ctx->S.tokens.compile(expr);
+  ExprOp* ops = upload_program(d, P);
+  ck(eval_program_field(ops, static_cast<int>(P.ops.size()), f, F.nzl, M.plane_size, M.nplane, F.x, F.y, F.dz,
+                        d->ctx->S.tokens.value("t"), d->ctx->stream),
+     "force field");
+  ck(cudaStreamSynchronize(d->ctx->stream), "force field");
+  return f;
+}
+
+// Velocity-component forcing fields read from a field file (VirtualForce::
+// readSteadyFromFile, dns/fieldforce.cpp:217-233, readField, src/misc.cpp:
+// 182-222): fields named u, v, w; one named in no dump stays zero.
+void force_from_file(stx_dns* d, std::string fname, double** out) {
+  const size_t a = fname.find_first_not_of(" \t"), b = fname.find_last_not_of(" \t");
+  fname = a == std::string::npos ? "" : fname.substr(a, b - a + 1);
+  auto& F = d->force;
+  const Mesh& M = d->ctx->M;
+  if (d->nz32) throw DnsError(STX_EUNSUPPORTED, "forcing from a file with DEALIAS: the file holds N_Z planes");
+  FieldFile ff;
+  try {
+    ff = read_field(fname);
+  } catch (const std::exception& e) {
+    throw DnsError(STX_ESESSION, std::string("can't open '") + fname + "' file: " + e.what());
+  }
+  if (ff.np != M.np || ff.nz != M.nz || ff.nel != M.nel)
+    throw DnsError(STX_ESESSION, "forcing file '" + fname + "': sizes differ from the session");
+  const size_t n = static_cast<size_t>(F.nzl) * M.plane_size;
+  for (int i = 0; i < d->ncom; ++i) {
+    out[i] = static_cast<double*>(d->arena.alloc(sizeof(double) * n));
+    ck(cudaMemset(out[i], 0, sizeof(double) * n), "memset");
+    const size_t k = ff.names.find(static_cast<char>('u' + i));
+    if (k == std::string::npos) continue;
+    ck(cudaMemcpy2D(out[i], sizeof(double) * M.plane_size, ff.data[k].data(), sizeof(double) * M.nplane,
+                    sizeof(double) * M.nplane, M.nz, cudaMemcpyHostToDevice),
+       "forcing upload");
+  }
+}
+
+// FieldForce::FieldForce and the class constructors (dns/fieldforce.cpp:
+// 31-73, 240-822): which terms the FORCE section switches on.
+void force_setup(stx_dns* d) {
+  const Session& S = d->ctx->S;
+  const TokenTable& T = S.tokens;
+  auto& F = d->force;
+  if (!S.has_force) return;
+  F.on = true;
+  const Mesh& M = d->ctx->M;
+  F.nzl = d->nz32 ? d->nz32 : M.nz;
+  F.dz = 2.0 * M_PI / d->beta / F.nzl;
+  F.x = static_cast<double*>(d->arena.alloc(sizeof(double) * M.nplane));
+  F.y = static_cast<double*>(d->arena.alloc(sizeof(double) * M.nplane));
+  ck(cudaMemcpy(F.x, M.x.data(), sizeof(double) * M.nplane, cudaMemcpyHostToDevice), "x");
+  ck(cudaMemcpy(F.y, M.y.data(), sizeof(double) * M.nplane, cudaMemcpyHostToDevice), "y");
+  const char xyz[3] = {'X', 'Y', 'Z'};
+  auto str = [&](const std::string& tok, std::string& v) { return S.force_value(tok, v); };
+  auto num = [&](const std::string& tok, double& v) {
+    std::string s;
+    if (!str(tok, s)) return false;
+    v = T.eval(s);
+    return true;
+  };
+  auto tok = [&](const char* stem, int i) { return std::string(stem) + xyz[i]; };
+  std::string s;
+  // ConstForce (:240-270)
+  for (int i = 0; i < d->ncom; ++i) num(tok("CONST_", i), F.cst[i]);
+  // WhiteNoiseForce (:347-384): a random stream of the reference's own
+  for (int i = 0; i < d->ncom; ++i) {
+    double eps = 0.0;
+    if (num(tok("WHITE_EPS_", i), eps) && std::fabs(eps) > kEpsDp)
+      throw DnsError(STX_EUNSUPPORTED, "WHITE_EPS_* (white-noise forcing) is not supported");
+  }
+  // SteadyForce (:273-332)
+  if (str("STEADY_FILE", s)) {
+    force_from_file(d, s, F.steady);
+  } else {
+    for (int i = 0; i < d->ncom; ++i)
+      if (str(tok("STEADY_", i), s)) F.steady[i] = force_field(d, s);
+  }
+  // ModulatedForce (:387-446)
+  bool alpha_found = false;
+  for (int i = 0; i < d->ncom; ++i) {
+    F.alpha[i] = "0";
+    if (str(tok("MOD_ALPHA_", i), F.alpha[i])) alpha_found = true;
+  }
+  if (alpha_found) {
+    if (str("MOD_A_FILE", s)) {
+      force_from_file(d, s, F.moda);
+    } else {
+      for (int i = 0; i < d->ncom; ++i)
+        if (str(tok("MOD_A_", i), s)) F.moda[i] = force_field(d, s);
+    }
+    for (int i = 0; i < d->ncom; ++i) F.tdep = F.tdep || (F.moda[i] && depends_on_t(F.alpha[i]));
+  }
+  // SpatioTemporalForce (:463-496)
+  for (int i = 0; i < d->ncom; ++i)
+    if (str(tok("SPATIOTEMP_ALPHA_", i), s)) {
+      const ExprProgram P = T.compile(s);
+      F.st[i] = upload_program(d, P);
+      F.nst[i] = static_cast<int>(P.ops.size());
+      F.tdep = true;
+    }
+  // SpongeForce (:516-560).  A mask re-evaluated every SPONGE_UPDATE steps is
+  // also evaluated here, so that it holds values before its first update.
+  if (str("SPONGE_M", s)) {
+    F.mask = force_field(d, s);
+    std::string u;
+    if (str("SPONGE_UPDATE", u)) {
+      F.sponge_update = static_cast<int>(std::lround(T.eval(u)));
+      const ExprProgram P = T.compile(s);
+      F.mask_prog = upload_program(d, P);
+      F.nmask = static_cast<int>(P.ops.size());
+      F.tdep = F.tdep || F.sponge_update != 0;
+    }
+    const char* ref[3] = {"SPONGE_U", "SPONGE_V", "SPONGE_W"};
+    for (int i = 0; i < d->ncom; ++i) {
+      std::string r = "0";
+      str(ref[i], r);
+      F.uref[i] = force_field(d, r);
+    }
+  }
+  // DragForce (:581-611)
+  if (str("DRAG_M", s)) F.drag = force_field(d, s);
+  // CoriolisForce (:631-723): in 2-D only the z components are read
+  {
+    std::string u;
+    const int unsteady = str("CORIOLIS_UNSTEADY", u) ? static_cast<int>(std::lround(T.eval(u))) : 0;
+    bool enabled = false;
+    for (int i = 0; i < 3; ++i) {
+      F.omega[i] = "0";
+      F.domega[i] = "0";
+      if (d->ncom == 3 || i == 2) {
+        if (str(tok("CORIOLIS_OMEGA_", i), F.omega[i])) enabled = true;
+        if (unsteady) str(tok("CORIOLIS_DOMEGA_", i) + "_DT", F.domega[i]);
+      }
+    }
+    if (enabled) {
+      F.coriolis = unsteady ? 2 : 1;
+      if (!unsteady)
+        for (int i = 0; i < 3; ++i) F.m2o[i] = -2.0 * T.eval(F.omega[i]);
+      F.tdep = F.tdep || unsteady;
+    }
+  }
+  // SFDForce (:759-789)
+  {
+    double delta = 0.0, chi = 0.0;
+    const bool hd = num("SFD_DELTA", delta), hc = num("SFD_CHI", chi);
+    if (hd || hc) {
+      if (!(hd && hc)) throw DnsError(STX_ESESSION, "SFD_DELTA and SFD_CHI must be paired.");
+      F.chi = chi;
+      F.rate = d->dt / delta;
+      const size_t n = static_cast<size_t>(F.nzl) * M.plane_size;
+      for (int i = 0; i < d->ncom; ++i) {
+        F.qbar[i] = static_cast<double*>(d->arena.alloc(sizeof(double) * n));
+        ck(cudaMemset(F.qbar[i], 0, sizeof(double) * n), "memset");
+      }
+    }
+  }
+  for (int i = 0; i < d->ncom; ++i)
+    F.physical = F.physical || F.steady[i] || F.moda[i] || F.st[i] || F.qbar[i];
+  F.physical = F.physical || F.mask || F.drag || F.coriolis;
+}
+
+// FieldForce::addPhysical (dns/fieldforce.cpp:75-107) for component i: the
+// force added to N, physical values on the forcing grid; Up the physical
+// velocities on the same grid.
+void force_physical(stx_dns* d, int i, double* N, const std::vector<double*>& Up) {
+  auto& F = d->force;
+  if (!F.physical) return;
+  const Mesh& M = d->ctx->M;
+  const TokenTable& T = d->ctx->S.tokens;
+  cudaStream_t st = d->ctx->stream;
+  std::map<std::string, double> vars{{"t", d->time}};
+  ForceArgs a{};
+  a.N = N;
+  for (int c = 0; c < d->ncom; ++c) a.U[c] = Up[c];
+  a.ncom = d->ncom;
+  a.com = i;
+  a.nzl = F.nzl;
+  a.plane_size = M.plane_size;
+  a.nplane = M.nplane;
+  a.dz = F.dz;
+  a.t = F.tdep ? d->time : 0.0;
+  a.x = F.x;
+  a.y = F.y;
+  if (F.mask) {
+    if (i == 0 && F.sponge_update && d->step % F.sponge_update == 0)
+      ck(eval_program_field(F.mask_prog, F.nmask, F.mask, F.nzl, M.plane_size, M.nplane, F.x, F.y, F.dz, d->time,
+                            st),
+         "sponge mask");
+    a.mask = F.mask;
+    a.uref = F.uref[i];
+  }
+  if (F.coriolis) {
+    if (F.coriolis == 2 && i == 0)
+      for (int c = d->ncom == 2 ? 2 : 0; c < 3; ++c) {
+        F.o[c] = T.eval(F.omega[c], &vars);
+        F.mo[c] = -F.o[c];
+        F.m2o[c] = -2.0 * F.o[c];
+        F.dodt[c] = -T.eval(F.domega[c], &vars);
+      }
+    a.coriolis = F.coriolis;
+    for (int c = 0; c < 3; ++c) {
+      a.m2o[c] = F.m2o[c];
+      a.o[c] = F.o[c];
+      a.mo[c] = F.mo[c];
+      a.dodt[c] = F.dodt[c];
+    }
+  }
+  a.steady = F.steady[i];
+  if (F.moda[i]) {
+    a.alpha = T.eval(F.alpha[i], &vars);
+    if (std::fabs(a.alpha) > kEpsDp) a.moda = F.moda[i];
+  }
+  a.st = F.st[i];
+  a.nst = F.nst[i];
+  a.drag = F.drag;
+  if (F.qbar[i]) {
+    a.qbar = F.qbar[i];
+    a.chi = F.chi;
+    a.rate = F.rate;
+    a.sfd_init = F.sfd_started ? 0 : 1;
+    if (i == d->ncom - 1) F.sfd_started = true;
+  }
+  ck(dns_force_physical(a, st), "force");
+}
+
+// FieldForce::addFourier (dns/fieldforce.cpp:110-137): ConstForce on mode 0.
+void force_fourier(stx_dns* d, int i, double* N) {
+  const auto& F = d->force;
+  if (F.on && std::fabs(F.cst[i]) > kEpsDp)
+    ck(dns_force_const(N, d->ctx->M.nplane, F.cst[i], d->ctx->stream), "const force");
+}
+
 // The same nonlinear terms with every product on the 3/2-padded z grid.
 void nonlinear32(stx_dns* d, int form) {
   stx_context* ctx = d->ctx;
@@ -176,7 +463,13 @@ void nonlinear32(stx_dns* d, int form) {
   for (int i = 0; i < d->ncom; ++i) {
     double* N = d->Uf[0][i];
     if (form < 0) {
-      ck(cudaMemsetAsync(N, 0, sizeof(double) * d->fsize, st), "zero");
+      if (d->force.physical) {  // the force alone, on the padded grid
+        ck(cudaMemsetAsync(d->A32, 0, sizeof(double) * d->nz32 * ctx->M.plane_size, st), "zero");
+        force_physical(d, i, d->A32, d->Up32);
+        forward32(d, d->A32, N);
+      } else {
+        ck(cudaMemsetAsync(N, 0, sizeof(double) * d->fsize, st), "zero");
+      }
     } else {
       NonlinearArgs a{};
       a.U0 = d->Up32[0];
@@ -198,8 +491,10 @@ void nonlinear32(stx_dns* d, int form) {
         a.Tk = d->C32;
       }
       ck(dns_nonlinear(g32, a, st), "nonlinear");
+      force_physical(d, i, d->A32, d->Up32);
       forward32(d, d->A32, N);
     }
+    force_fourier(d, i, N);
     ck(dns_smooth(ctx->dg, Nm, N, d->dsswork, st), "smooth");
   }
 }
@@ -254,7 +549,9 @@ void nonlinear(stx_dns* d) {
       }
       ck(dns_nonlinear(g, a, st), "nonlinear");
     }
+    force_physical(d, i, N, d->Up);
     transform(d, N, STX_FORWARD);
+    force_fourier(d, i, N);
     ck(dns_smooth(g, Nm, N, d->dsswork, st), "smooth");
   }
   if (d->form == 1) d->toggle = 1 - d->toggle;
@@ -408,9 +705,10 @@ std::vector<double*> pointer_state(const stx_dns* d) {
 }
 
 // A step is steady (its kernels and coefficients repeat) once the start-up
-// orders are past, and no BC is re-evaluated on the host.
+// orders are past, no BC is re-evaluated on the host and no forcing term
+// changes with time.
 bool steady(const stx_dns* d) {
-  if (d->step < d->nord) return false;
+  if (d->step < d->nord || d->force.tdep) return false;
   for (char t : d->tdep)
     if (t) return false;
   return true;
@@ -562,6 +860,8 @@ int stx_dns_create(stx_context* ctx, int advection, stx_dns** out) {
       d->twiddle32 = static_cast<double*>(d->arena.alloc(sizeof(double) * tw.size()));
       ck(cudaMemcpy(d->twiddle32, tw.data(), sizeof(double) * tw.size(), cudaMemcpyHostToDevice), "twiddle");
     }
+    // -- body forcing (FieldForce::FieldForce)
+    force_setup(d);
     // -- high-order pressure BC edges and storage (BCmgr::buildComputedBCs,
     //    src/bcmgr.cpp:937-996)
     {
@@ -641,6 +941,7 @@ int stx_dns_restart(stx_dns* d, double t0) {
     d->eager_steady = 0;
     d->step = 0;
     d->time = t0;
+    d->force.sfd_started = false;  // SFD's filtered field restarts from u
     for (char c : d->names) ckstx(stx_field_bc_evaluate(d->ctx, c, t0));
   });
 }

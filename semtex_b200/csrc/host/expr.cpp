@@ -1,5 +1,6 @@
 #include "expr.hpp"
 
+#include <algorithm>
 #include <cctype>
 #include <cmath>
 #include <cstdio>
@@ -207,7 +208,216 @@ struct Parser {
   }
 };
 
+// The same grammar as Parser, emitting a postfix program instead of a
+// value.  Operations whose operands are all constants are folded.
+struct Compiler {
+  const std::string& s;
+  size_t i = 0;
+  const std::map<std::string, double>& tab;
+  ExprProgram prog;
+  int sp = 0;
+
+  Compiler(const std::string& src, const std::map<std::string, double>& t) : s(src), tab(t) {}
+
+  void ws() {
+    while (i < s.size() && std::isspace(static_cast<unsigned char>(s[i]))) ++i;
+  }
+  bool eat(char c) {
+    ws();
+    if (i < s.size() && s[i] == c) {
+      ++i;
+      return true;
+    }
+    return false;
+  }
+  [[noreturn]] void fail(const char* what) const {
+    throw std::runtime_error(std::string("expression error (") + what + ") in: " + s);
+  }
+  bool last_const(int k) const {  // the k-th op from the end is a constant
+    const int n = static_cast<int>(prog.ops.size());
+    return n >= k && prog.ops[n - k].code == kExConst;
+  }
+  void push(int code, int fn = 0, double val = 0.0) {
+    if (static_cast<int>(prog.ops.size()) >= kExprMaxOps) fail("program too long");
+    prog.ops.push_back(ExprOp{code, fn, val});
+  }
+  void value(int code, double val = 0.0) {
+    push(code, 0, val);
+    if (++sp > kExprStack) fail("expression nested too deeply");
+    prog.depth = std::max(prog.depth, sp);
+  }
+  void binary(int code) {
+    if (last_const(1) && last_const(2)) {
+      const double b = prog.ops.back().val;
+      prog.ops.pop_back();
+      prog.ops.back().val = expr_binary(code, prog.ops.back().val, b);
+    } else {
+      push(code);
+    }
+    --sp;
+  }
+  void fn2(int fn) {
+    if (last_const(1) && last_const(2)) {
+      const double b = prog.ops.back().val;
+      prog.ops.pop_back();
+      prog.ops.back().val = expr_fn2(fn, prog.ops.back().val, b);
+    } else {
+      push(kExFn2, fn);
+    }
+    --sp;
+  }
+  void fn1(int fn) {
+    if (last_const(1)) prog.ops.back().val = expr_fn1(fn, prog.ops.back().val);
+    else push(kExFn1, fn);
+  }
+  void negate() {
+    if (last_const(1)) prog.ops.back().val = -prog.ops.back().val;
+    else push(kExNeg);
+  }
+
+  void expr() {
+    term();
+    for (;;) {
+      if (eat('+')) {
+        term();
+        binary(kExAdd);
+      } else if (eat('-')) {
+        term();
+        binary(kExSub);
+      } else {
+        return;
+      }
+    }
+  }
+  void term() {
+    unary();
+    for (;;) {
+      if (eat('*')) {
+        unary();
+        binary(kExMul);
+      } else if (eat('/')) {
+        unary();
+        binary(kExDiv);
+      } else if (eat('%')) {
+        unary();
+        binary(kExMod);
+      } else {
+        return;
+      }
+    }
+  }
+  void unary() {
+    if (eat('-')) {
+      unary();
+      negate();
+      return;
+    }
+    if (eat('+')) {
+      unary();
+      return;
+    }
+    power();
+  }
+  void power() {
+    atom();
+    ws();
+    if (i < s.size() && (s[i] == '^' || s[i] == '&' || s[i] == '~')) {
+      const char op = s[i++];
+      unary();  // right-associative
+      binary(op == '^' ? kExPow : op == '&' ? kExHypot : kExAtan2);
+    }
+  }
+  void call(const std::string& name, int nargs) {
+    static const std::map<std::string, int> one = {
+        {"cos", kFnCos},     {"sin", kFnSin},     {"tan", kFnTan},     {"exp", kFnExp},
+        {"sinh", kFnSinh},   {"cosh", kFnCosh},   {"tanh", kFnTanh},   {"erf", kFnErf},
+        {"erfc", kFnErfc},   {"int", kFnInt},     {"abs", kFnAbs},     {"floor", kFnFloor},
+        {"ceil", kFnCeil},   {"acos", kFnAcos},   {"asin", kFnAsin},   {"atan", kFnAtan},
+        {"acosh", kFnAcosh}, {"asinh", kFnAsinh}, {"atanh", kFnAtanh}, {"log", kFnLog},
+        {"log10", kFnLog10}, {"sqrt", kFnSqrt},   {"heav", kFnHeav},   {"sgn", kFnSgn},
+        {"j0", kFnJ0},       {"j1", kFnJ1},       {"y0", kFnY0},       {"y1", kFnY1},
+        {"gamma", kFnGamma}, {"lgamma", kFnLgamma}};
+    static const std::map<std::string, int> two = {
+        {"jn", kFnJn}, {"yn", kFnYn}, {"rad", kFnRad}, {"ang", kFnAng}, {"step", kFnStep}};
+    auto a = one.find(name);
+    if (a != one.end()) {
+      if (nargs != 1) fail("wrong number of arguments");
+      fn1(a->second);
+      return;
+    }
+    auto b = two.find(name);
+    if (b != two.end()) {
+      if (nargs != 2) fail("wrong number of arguments");
+      fn2(b->second);
+      return;
+    }
+    fail(("unknown function " + name).c_str());
+  }
+  void atom() {
+    ws();
+    if (i >= s.size()) fail("unexpected end");
+    const char c = s[i];
+    if (c == '(') {
+      ++i;
+      expr();
+      if (!eat(')')) fail("missing )");
+      return;
+    }
+    if (std::isdigit(static_cast<unsigned char>(c)) || c == '.') {
+      size_t used = 0;
+      const double v = std::stod(s.substr(i), &used);
+      i += used;
+      value(kExConst, v);
+      return;
+    }
+    if (std::isalpha(static_cast<unsigned char>(c)) || c == '_') {
+      size_t j = i;
+      while (j < s.size() && (std::isalnum(static_cast<unsigned char>(s[j])) || s[j] == '_')) ++j;
+      const std::string name = s.substr(i, j - i);
+      i = j;
+      ws();
+      if (i < s.size() && s[i] == '(') {
+        ++i;
+        int nargs = 0;
+        if (!eat(')')) {
+          do {
+            expr();
+            ++nargs;
+          } while (eat(','));
+          if (!eat(')')) fail("missing ) after arguments");
+        }
+        call(name, nargs);
+        return;
+      }
+      if (i < s.size() && s[i] == '=' && (i + 1 >= s.size() || s[i + 1] != '='))
+        fail("assignment inside a compiled expression");
+      if (name == "x" || name == "y" || name == "z") {
+        prog.uses_xyz = true;
+        value(name == "x" ? kExX : name == "y" ? kExY : kExZ);
+      } else if (name == "t") {
+        prog.uses_t = true;
+        value(kExT);
+      } else {
+        auto it = tab.find(name);
+        if (it == tab.end()) std::fprintf(stderr, "yyparse: undefined variable %s\n", name.c_str());
+        value(kExConst, it == tab.end() ? 0.0 : it->second);
+      }
+      return;
+    }
+    fail("unexpected character");
+  }
+};
+
 }  // namespace
+
+ExprProgram TokenTable::compile(const std::string& e) const {
+  Compiler c(e, table_);
+  c.expr();
+  c.ws();
+  if (c.i != e.size()) c.fail("trailing characters");
+  if (c.sp != 1) c.fail("malformed expression");
+  return c.prog;
+}
 
 TokenTable::TokenTable() {
   for (const auto& d : kDefaults) table_[d.name] = d.value;

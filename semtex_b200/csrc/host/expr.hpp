@@ -19,7 +19,22 @@
 #include <string>
 #include <vector>
 
+#include "../kernels/exprprog.hpp"
+
 namespace stx {
+
+// A compiled expression (see exprprog.hpp): the postfix program, the
+// deepest operand stack it needs and which of x, y, z, t it reads.
+struct ExprProgram {
+  std::vector<ExprOp> ops;
+  int depth = 0;
+  bool uses_xyz = false;
+  bool uses_t = false;
+  bool constant() const { return !uses_xyz && !uses_t; }
+  double run(double x, double y, double z, double t) const {
+    return expr_run(ops.data(), static_cast<int>(ops.size()), x, y, z, t);
+  }
+};
 
 class TokenTable {
  public:
@@ -27,6 +42,11 @@ class TokenTable {
   // Evaluate an expression; `vars` overrides table entries (x, y, z, t ...).
   double eval(const std::string& expr,
               const std::map<std::string, double>* vars = nullptr) const;
+  // The expression as a program of the free variables x, y, z, t; other
+  // names take their current table values.  Assignments inside the
+  // expression are not accepted, nor programs longer than kExprMaxOps or
+  // deeper than kExprStack (std::runtime_error).
+  ExprProgram compile(const std::string& expr) const;
   // "NAME = expr" assignment (FEML <TOKENS> line).
   void assign(const std::string& line);
   double value(const std::string& name) const;

@@ -208,7 +208,42 @@ Session read_session(const std::string& path, const std::string& overrides) {
   }
   if (section(text, "CURVES", body)) S.has_curves = !lines(body).empty();
   if (section(text, "USER", body)) S.user = lines(body);
+  if (section(text, "FORCE", body)) {
+    S.has_force = true;
+    std::istringstream is(body);
+    std::string ln;
+    std::getline(is, ln);  // the rest of the opening tag's line
+    while (std::getline(is, ln)) {
+      if (!ln.empty() && ln.back() == '\r') ln.pop_back();
+      S.force.push_back(ln);
+    }
+  }
   return S;
+}
+
+bool Session::force_value(const std::string& token, std::string& value) const {
+  for (size_t k = 0; k < force.size(); ++k) {
+    const std::string& s = force[k];
+    if (!s.empty() && s[0] == '#') {
+      ++k;  // the reference reads past the comment line and the one after it
+      continue;
+    }
+    auto delim = [](char c) { return c == '\t' || c == '=' || c == ' '; };
+    size_t a = 0;
+    while (a < s.size() && delim(s[a])) ++a;
+    if (a == s.size()) continue;
+    size_t b = a;
+    while (b < s.size() && !delim(s[b])) ++b;
+    if (s.compare(a, b - a, token) != 0 || b - a != token.size()) continue;
+    size_t c = b < s.size() ? b + 1 : b;  // the delimiter that ended the word
+    while (c < s.size() && s[c] == '=') ++c;
+    size_t d = c;
+    while (d < s.size() && s[d] != '=') ++d;
+    if (c == d) return false;
+    value = s.substr(c, d - c);
+    return true;
+  }
+  return false;
 }
 
 }  // namespace stx

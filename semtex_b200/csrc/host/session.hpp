@@ -3,8 +3,9 @@
 // Reads the sections the reference reads for the dns / elliptic hot path
 // (src/feml.cpp:64-330, src/mesh.cpp:129-470, src/bcmgr.cpp:100-110):
 // TOKENS, FIELDS, GROUPS, BCS, NODES, ELEMENTS (<Q> quads), SURFACES
-// (<B> boundary group or <P> periodic mate), USER.  CURVES are recorded as
-// present and rejected by the mesh builder (straight sides only).
+// (<B> boundary group or <P> periodic mate), USER, FORCE (dns/fieldforce.cpp:
+// 31-73).  CURVES are recorded as present and rejected by the mesh builder
+// (straight sides only).
 #pragma once
 
 #include <array>
@@ -39,6 +40,15 @@ struct Session {
   std::vector<Surface> surfaces;
   std::vector<std::string> user;                     // USER section lines
   bool has_curves = false;
+  bool has_force = false;                            // <FORCE> section present
+  std::vector<std::string> force;                    // its raw lines
+
+  // FEML::valueFromSection (src/feml.cpp:430-560) on the FORCE section: the
+  // text after `token` on the first line whose first word is `token` (words
+  // end at tab, '=' or space; the value is what follows up to the next '=').
+  // A line starting with '#' is skipped together with the line after it, as
+  // the reference skips them.  False if absent.
+  bool force_value(const std::string& token, std::string& value) const;
 
   // USER line "key value" (elliptic forcing/exact) or "name = expr".
   std::string user_value(const std::string& key) const;

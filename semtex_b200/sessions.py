@@ -12,12 +12,13 @@ import numpy as np
 
 def rect_session(path, nx, ny, x=(0.0, 1.0), y=(0.0, 1.0), tokens=None, fields="c",
                  periodic_x=False, periodic_y=False, bcs=None, user=None, xs=None, ys=None,
-                 wall_group="w"):
+                 wall_group="w", force=None):
     """Write a session file.
 
     bcs: {group_char: {field: "<D> value" | "<N> value" | "<H>"}} applied to
     every non-periodic boundary side (group `wall_group`), or None for no BCs.
     xs / ys: explicit node coordinates along x / y (length nx+1 / ny+1).
+    force: lines of a <FORCE> section ("CONST_X = 0.1", ...), or None.
     """
     xs = np.linspace(x[0], x[1], nx + 1) if xs is None else np.asarray(xs, float)
     ys = np.linspace(y[0], y[1], ny + 1) if ys is None else np.asarray(ys, float)
@@ -33,6 +34,10 @@ def rect_session(path, nx, ny, x=(0.0, 1.0), y=(0.0, 1.0), tokens=None, fields="
     for k, v in (tokens or {}).items():
         lines.append(f"\t{k} = {v}")
     lines.append("</TOKENS>\n")
+    if force is not None:
+        lines.append("<FORCE>")
+        lines += [f"\t{f}" for f in force]
+        lines.append("</FORCE>\n")
     if bcs:
         lines.append(f"<GROUPS NUMBER={len(bcs)}>")
         for i, g in enumerate(bcs):
@@ -97,17 +102,18 @@ def helmholtz_session(path, n, np_, nz=1, lambda2=1.0, beta=1.0, extra=None, use
                         user=user, xs=xs, ys=ys)
 
 
-def taylor_green_session(path, n, np_, nz, re=1600.0, dt=1e-3, nstep=200, extra=None):
+def taylor_green_session(path, n, np_, nz, re=1600.0, dt=1e-3, nstep=200, extra=None, force=None):
     """3D-periodic Taylor--Green vortex on [0, 2 pi]^3 (config c3)."""
     tok = {"N_P": np_, "N_Z": nz, "BETA": 1, "KINVIS": f"1.0/{re}", "D_T": dt, "N_TIME": 3,
            "N_STEP": nstep, "TOL_REL": 1e-13}
     tok.update(extra or {})
     user = ["u = sin(x)*cos(y)*cos(z)", "v = -cos(x)*sin(y)*cos(z)", "w = 0", "p = 0"]
     return rect_session(path, n, n, x=(0.0, 2 * np.pi), y=(0.0, 2 * np.pi), tokens=tok,
-                        fields="uvwp", periodic_x=True, periodic_y=True, user=user)
+                        fields="uvwp", periodic_x=True, periodic_y=True, user=user, force=force)
 
 
-def channel_session(path, nx=16, ny=8, np_=9, nz=32, re=500.0, dt=5e-3, nstep=100, ntime=3, extra=None):
+def channel_session(path, nx=16, ny=8, np_=9, nz=32, re=500.0, dt=5e-3, nstep=100, ntime=3, extra=None,
+                    force=None):
     """Plane channel [0, 2 pi] x [-1, 1] x [0, 2 pi), periodic in x and z,
     no-slip walls at y = +-1 with high-order pressure BCs (config c5)."""
     tok = {"N_P": np_, "N_Z": nz, "BETA": 1, "KINVIS": f"1.0/{re}", "D_T": dt, "N_TIME": ntime,
@@ -118,7 +124,7 @@ def channel_session(path, nx=16, ny=8, np_=9, nz=32, re=500.0, dt=5e-3, nstep=10
     if nz > 1:
         bc["w"] = "<D> 0"
     return rect_session(path, nx, ny, x=(0.0, 2 * np.pi), y=(-1.0, 1.0), tokens=tok, fields=fields,
-                        periodic_x=True, bcs={"w": bc})
+                        periodic_x=True, bcs={"w": bc}, force=force)
 
 
 def channel_initial(x, y, z, seed=20261203, amplitude=1e-3, modes=3):
