@@ -106,6 +106,15 @@ int stx_field_evaluate(const stx_context* ctx, const char* expr, double t, doubl
 int stx_expression_eval(const char* expr, const char* assignments, int compiled, int n, const double* x,
                         const double* y, const double* z, double t, double* out, int* nops);
 
+/* Spectral vanishing viscosity operators, host only (SVV::operators and
+ * SVV::coeffs / coeffs_z, src/svv.cpp:20-185): d_matrix[np*np] receives the
+ * derivative matrix the viscous (lambda2 > 0) systems use -- the SVV one for
+ * tokens SVV_EPSN = eps_n, SVV_MN = m_n, or the plain GLL derivative when SVV
+ * is off -- and z_factors[(nz+1)/2] the factors of beta^2 k^2 of their Fourier
+ * modes (SVV_EPSZ = eps_z, SVV_MZ = m_z); either pointer may be null. */
+int stx_svv(int np, double eps_n, int m_n, int nz, double eps_z, int m_z, double kinvis, double* d_matrix,
+            double* z_factors);
+
 /* Evaluate a field's boundary values at time t in physical space on every
  * plane and Fourier-transform them (Field::evaluateBoundaries +
  * Field::bTransform, src/field.cpp:160-243).  Synchronises. */

@@ -275,6 +275,40 @@ def gll(np_: int):
     return z, w, D
 
 
+def svv_derivative(z, w, D, eps, mN, nu):
+    """SVV-modified derivative MI diag(sqrt S) MF D (SVV::operators,
+    src/svv.cpp:126-185): MF, MI the GLL Legendre transform pair
+    (femlib/operators.c:317-490, C_k = 1/gamma_k of the discrete norms),
+    S_k = 1 + eps/nu exp(-((N-k)/(mN-k))^2) for k > mN (SVV::coeffs,
+    :20-52).  None when SVV is off."""
+    np_ = len(z)
+    N = np_ - 1
+    if not (0 <= mN < N and eps > EPSDP):
+        return None
+    S = np.zeros(np_)
+    for k in range(mN + 1, np_):
+        S[k] = math.exp(-((N - k) / (1.0 * mN - k)) ** 2)
+    S = 1.0 + eps / nu * S
+    L = np.array([_legendre(k, z) for k in range(np_)])        # L[k, j] = P_k(z_j)
+    C = np.array([0.5 * (2 * k + 1) if k < N else 0.5 * N for k in range(np_)])
+    MF = C[:, None] * w[None, :] * L
+    MI = L.T
+    return MI @ (np.sqrt(S)[:, None] * MF) @ D
+
+
+def svv_z(nz, num_modes, eps, mN, nu):
+    """SVV::coeffs_z (src/svv.cpp:55-90): factors of beta^2 k^2 for the
+    viscous systems' modes, N = nMode - 1."""
+    N = (nz + 1) // 2 - 1
+    S = np.zeros(num_modes)
+    if 0 <= mN < N and eps > EPSDP:
+        for i in range(num_modes):
+            if i > mN:
+                S[i] = math.exp(-((N - i) / (1.0 * mN - i)) ** 2)
+        return 1.0 + eps / nu * S
+    return np.ones(num_modes)
+
+
 # ---------------------------------------------------------------------------
 # Mesh and element geometry
 # ---------------------------------------------------------------------------
@@ -288,6 +322,14 @@ class Mesh:
         self.z, self.w, self.D = gll(np_)
         nel, z = self.nel, self.z
         tok = S.tokens
+        # viscous operators take the SVV-stabilised derivative (src/element.cpp:1454-1455)
+        self.Dv = self.D
+        if tok["SVV_EPSN"] > EPSDP:
+            if tok["SVV_MN"] > np_:
+                raise ValueError("SVV_MN exceeds N_P")      # dns/drive.cpp:244-245
+            Dv = svv_derivative(self.z, self.w, self.D, tok["SVV_EPSN"], int(tok["SVV_MN"]), tok["KINVIS"])
+            if Dv is not None:
+                self.Dv = Dv
         x = np.zeros((nel, np_, np_))
         y = np.zeros((nel, np_, np_))
         for e in range(nel):
@@ -656,7 +698,7 @@ def helmholtz_matrix(M: Mesh, e: int, lambda2: float, betak2: float):
                    + Q3[i,n] D[n,j] D[i,m] + Q3[m,j] D[j,n] D[m,i]
                    + d_im d_jn Q4[i,j] (lambda2 + betak2)
     """
-    n, D = M.np, M.D
+    n, D = M.np, (M.Dv if lambda2 > EPSDP else M.D)
     Q1, Q2, Q3, Q4 = M.Q1[e], M.Q2[e], M.Q3[e], M.Q4[e]
     I = np.eye(n)
     T1 = np.einsum("im,iq,qj,qn->ijmn", I, Q1, D, D)
@@ -668,7 +710,7 @@ def helmholtz_matrix(M: Mesh, e: int, lambda2: float, betak2: float):
 
 def helmholtz_op(M: Mesh, u, lambda2, betak2):
     """Batched Element::HelmholtzOp over all elements; u: [nel, np, np]."""
-    D = M.D
+    D = M.Dv if lambda2 > EPSDP else M.D
     R = u @ D.T
     S = D @ u
     R2 = M.Q1 * R + M.Q3 * S
@@ -1056,11 +1098,15 @@ class Problem:
 
     def modal_systems(self, c, lambda2, method="DIRECT", cache=None):
         """ModalMatrixSys (src/matrix.cpp:33-105): one MatrixSys per mode."""
-        beta = self.S.tokens["BETA"]
+        tok = self.S.tokens
+        beta = tok["BETA"]
         nmodes = (self.nz + 1) // 2
+        # viscous systems: beta^2 k^2 times the SVV factor (src/matrix.cpp:78-83)
+        sz = (svv_z(self.nz, nmodes, tok["SVV_EPSZ"], int(tok["SVV_MZ"]), tok["KINVIS"])
+              if lambda2 > EPSDP else np.ones(nmodes))
         out = []
         for m in range(nmodes):
-            bk2 = (beta * m) ** 2
+            bk2 = (beta * m) ** 2 * sz[m]
             key = (c, round(lambda2, 14), round(bk2, 14), method)
             if cache is not None and key in cache:
                 out.append(cache[key])

@@ -27,7 +27,7 @@ from .fieldfile import read_field, write_field
 
 DIRECT, JACPCG, MIXED = STX_DIRECT, STX_JACPCG, STX_MIXED
 
-__all__ = ["Context", "ModalMatrixSys", "Field", "DNS", "Batch", "expression", "numbering", "solve_multi", "elliptic", "dns", "read_field",
+__all__ = ["Context", "ModalMatrixSys", "Field", "DNS", "Batch", "expression", "svv", "numbering", "solve_multi", "elliptic", "dns", "read_field",
            "write_field", "FORWARD", "INVERSE", "DIRECT", "JACPCG", "MIXED", "StxError"]
 
 
@@ -290,6 +290,17 @@ def expression(expr: str, x, y, z, t: float = 0.0, assignments: str | None = Non
                                      x.size, x.ctypes.data, y.ctypes.data, z.ctypes.data, float(t),
                                      out.ctypes.data, C.byref(nops)))
     return out, nops.value
+
+
+def svv(np_: int, eps_n: float, m_n: int, nz: int = 1, eps_z: float = 0.0, m_z: int = -1, kinvis: float = 1.0):
+    """Spectral vanishing viscosity operators (host): the derivative matrix of
+    the viscous systems [np, np] and the factors of beta^2 k^2 of their
+    (nz+1)/2 Fourier modes."""
+    D = np.empty((np_, np_))
+    Z = np.empty((nz + 1) // 2)
+    check(lib().stx_svv(int(np_), float(eps_n), int(m_n), int(nz), float(eps_z), int(m_z), float(kinvis),
+                        D.ctypes.data, Z.ctypes.data))
+    return D, Z
 
 
 def numbering(session: str, field: str, overrides=None):

@@ -425,6 +425,23 @@ int stx_expression_eval(const char* expr, const char* assignments, int compiled,
   });
 }
 
+int stx_svv(int np, double eps_n, int m_n, int nz, double eps_z, int m_z, double kinvis, double* d_matrix,
+            double* z_factors) {
+  return guarded([&] {
+    if (np < 2 || nz < 1 || !(kinvis > 0.0)) throw StxError(STX_EINVAL, "bad argument");
+    if (d_matrix) {
+      const Quadrature q = gll(np);
+      std::vector<double> D = svv_derivative(q, eps_n, m_n, kinvis);
+      if (D.empty()) D = q.D;
+      std::copy(D.begin(), D.end(), d_matrix);
+    }
+    if (z_factors) {
+      const std::vector<double> S = svv_z(nz, (nz + 1) / 2, eps_z, m_z, kinvis);
+      std::copy(S.begin(), S.end(), z_factors);
+    }
+  });
+}
+
 int stx_field_bc_evaluate(stx_context* ctx, char field, double t) {
   return guarded([&] {
     if (!ctx) throw StxError(STX_EINVAL, "null context");
@@ -503,6 +520,13 @@ int stx_modal_create(stx_context* ctx, char field, double lambda2, double beta, 
         throw StxError(STX_EUNSUPPORTED, "mixed precision needs the two-level skeleton solve");
       std::vector<ModeSystem> modes(num_modes);
       std::vector<std::string> errs(num_modes);
+      // viscous systems: beta^2 k^2 scaled by the SVV factors of the modes
+      // (src/matrix.cpp:78-83)
+      const TokenTable& T = ctx->S.tokens;
+      const std::vector<double> svz =
+          lambda2 > 6.0e-14 ? svv_z(M.nz, num_modes, T.value("SVV_EPSZ"), static_cast<int>(T.value("SVV_MZ")),
+                                    T.value("KINVIS"))
+                            : std::vector<double>(num_modes, 1.0);
       const unsigned hw = std::max(1u, std::thread::hardware_concurrency());
       unsigned nth = std::max(1u, std::min<unsigned>(hw, num_modes));
       const int inner = static_cast<int>(std::max(1u, hw / nth));  // threads of each mode's dense inverses
@@ -512,7 +536,7 @@ int stx_modal_create(stx_context* ctx, char field, double lambda2, double beta, 
           for (int m = static_cast<int>(w); m < num_modes; m += nth) {
             try {
               const double bk = beta * (base_mode + m);
-              modes[m] = build_mode_system(M, N, P, lambda2, bk * bk, method, inner);
+              modes[m] = build_mode_system(M, N, P, lambda2, bk * bk * svz[m], method, inner);
             } catch (const std::exception& e) {
               errs[m] = e.what();
             }
@@ -540,6 +564,7 @@ int stx_modal_create(stx_context* ctx, char field, double lambda2, double beta, 
       d.ns_stride = nsmax;
       d.lambda2 = upload(st->arena, lam);
       d.betak2 = upload(st->arena, bk2);
+      d.D = lambda2 > 6.0e-14 && !M.svv_D.empty() ? upload(st->arena, M.svv_D) : ctx->dg.D;
       d.nsolve = upload(st->arena, ns);
       d.l2 = 0;
       d.ew = d.eb = nullptr;

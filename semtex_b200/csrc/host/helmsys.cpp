@@ -76,7 +76,8 @@ void parallel_rows(int n, int nthreads, F&& f) {
 
 void element_helmholtz(const Mesh& M, int e, double lambda2, double betak2, double* H) {
   const int n = M.np, nn = M.npnp;
-  const double* D = M.q.D.data();
+  // viscous systems take the SVV-stabilised derivative (src/element.cpp:1454-1455)
+  const double* D = lambda2 > 6.0e-14 && !M.svv_D.empty() ? M.svv_D.data() : M.q.D.data();
   const double* Q1 = &M.Q1[e * nn];
   const double* Q2 = &M.Q2[e * nn];
   const double* Q3 = &M.Q3[e * nn];

@@ -70,6 +70,70 @@ Quadrature gll(int np) {
   return Q;
 }
 
+namespace {
+constexpr double kEpsDp = 6.0e-14;  // EPSDP, veclib/cveclib.h:58
+}
+
+std::vector<double> svv_derivative(const Quadrature& q, double eps, int mN, double nu) {
+  const int np = q.np, N = np - 1;
+  if (!(mN >= 0 && mN < N && eps > kEpsDp)) return {};
+  std::vector<double> S(np, 0.0), L(static_cast<size_t>(np) * np);
+  for (int k = mN + 1; k < np; ++k) {
+    const double r = (N - k) / (1.0 * mN - k);
+    S[k] = std::exp(-r * r);
+  }
+  for (int k = 0; k < np; ++k) S[k] = 1.0 + eps / nu * S[k];
+  // L[k][j] = P_k(z_j); forward transform MF[k][j] = C_k w_j L[k][j] with
+  // C_k = 1/gamma_k of the discrete GLL norms; inverse MI[j][k] = L[k][j]
+  for (int j = 0; j < np; ++j) {
+    double p0 = 1.0, p1 = q.z[j];
+    L[j] = 1.0;
+    if (np > 1) L[np + j] = p1;
+    for (int k = 2; k < np; ++k) {
+      const double p2 = ((2 * k - 1) * q.z[j] * p1 - (k - 1) * p0) / k;
+      L[static_cast<size_t>(k) * np + j] = p2;
+      p0 = p1;
+      p1 = p2;
+    }
+  }
+  std::vector<double> dv(static_cast<size_t>(np) * np), dt(static_cast<size_t>(np) * np),
+      out(static_cast<size_t>(np) * np, 0.0);
+  for (int k = 0; k < np; ++k) {
+    const double ck = k < N ? 0.5 * (k + k + 1) : 0.5 * N;
+    const double sk = std::sqrt(S[k]);
+    for (int j = 0; j < np; ++j) dv[k * np + j] = sk * (ck * q.w[j] * L[k * np + j]);
+  }
+  for (int i = 0; i < np; ++i)  // dt = MI dv
+    for (int j = 0; j < np; ++j) {
+      double v = 0.0;
+      for (int k = 0; k < np; ++k) v += L[k * np + i] * dv[k * np + j];
+      dt[i * np + j] = v;
+    }
+  for (int i = 0; i < np; ++i)  // out = dt D
+    for (int j = 0; j < np; ++j) {
+      double v = 0.0;
+      for (int k = 0; k < np; ++k) v += dt[i * np + k] * q.D[k * np + j];
+      out[i * np + j] = v;
+    }
+  return out;
+}
+
+std::vector<double> svv_z(int nz, int num_modes, double eps, int mN, double nu) {
+  std::vector<double> S(num_modes, 0.0);
+  const int N = (nz + 1) / 2 - 1;
+  if (mN >= 0 && mN < N && eps > kEpsDp) {
+    for (int i = 0; i < num_modes; ++i)
+      if (i > mN) {
+        const double r = (N - i) / (1.0 * mN - i);
+        S[i] = std::exp(-r * r);
+      }
+    for (auto& v : S) v = 1.0 + eps / nu * v;
+  } else {
+    for (auto& v : S) v = 1.0;
+  }
+  return S;
+}
+
 void Mesh::side_nodes(int s, int* idx) const {
   const int n = np;
   for (int t = 0; t < n; ++t) {
@@ -97,6 +161,12 @@ Mesh build_mesh(const Session& S) {
   M.nplane = nel * M.npnp;
   M.plane_size = M.nplane + (M.nplane % 2);  // src/geometry.cpp:105-108
   M.q = gll(n);
+  if (S.tokens.value("SVV_EPSN") > kEpsDp) {
+    if (S.tokens.value("SVV_MN") > n)  // dns/drive.cpp:244-245
+      throw std::runtime_error("SVV_MN exceeds N_P");
+    M.svv_D = svv_derivative(M.q, S.tokens.value("SVV_EPSN"), static_cast<int>(S.tokens.value("SVV_MN")),
+                             S.tokens.value("KINVIS"));
+  }
   const auto& z = M.q.z;
   const auto& w = M.q.w;
   const auto& D = M.q.D;

@@ -26,6 +26,16 @@ struct Quadrature {
 };
 Quadrature gll(int np);
 
+// Spectral vanishing viscosity (src/svv.cpp).  svv_derivative: the
+// SVV-modified derivative matrix MI diag(sqrt S) MF D (SVV::operators,
+// :126-185; MF, MI the GLL Legendre transform pair of femlib/operators.c:
+// 317-490), S_k = 1 + eps/nu exp(-((N-k)/(mN-k))^2) for k > mN (SVV::coeffs,
+// :20-52); empty when SVV is off (mN outside [0, N) or eps <= EPSDP).
+// svv_z: the factors of beta^2 k^2 for the viscous systems' num_modes
+// Fourier modes (SVV::coeffs_z, :55-90; N = nMode - 1).
+std::vector<double> svv_derivative(const Quadrature& q, double eps, int mN, double nu);
+std::vector<double> svv_z(int nz, int num_modes, double eps, int mN, double nu);
+
 struct Mesh {
   int np = 0, nel = 0, nz = 1;
   int npnp = 0, next = 0, nint = 0;
@@ -39,6 +49,7 @@ struct Mesh {
   std::vector<int> family;               // element -> geometry family
   std::vector<int> family_rep;           // family -> representative element
   int nfamily = 0;
+  std::vector<double> svv_D;             // SVV derivative of the viscous operators, or empty
 
   // Row-major node indices of side s in CCW traverse (src/element.h:162-170).
   void side_nodes(int s, int* idx) const;

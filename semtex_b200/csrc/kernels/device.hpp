@@ -76,6 +76,8 @@ struct DevModal {
   int nbp;                        // factor row stride (nband rounded up to even)
   long long mode_stride;          // doubles between modes' factors (256-byte multiple)
   long long dinv_stride;          // doubles between modes' inverse diagonal blocks
+  const double* D;                // [np*np] derivative matrix of the operators: the
+                                  // SVV-stabilised one for viscous systems with SVV
   const double* lambda2;          // [nmodes]
   const double* betak2;           // [nmodes]
   const int* nsolve;              // [nmodes]

@@ -321,7 +321,7 @@ __global__ void __launch_bounds__(32 * kMaxWarps, 1)
   const size_t fm = static_cast<size_t>(m) * S.nfamily + cd.z;
   stage_rows(bar, sA, S.eb + (fm * next + r_lo) * lda, static_cast<unsigned>(sizeof(double) * rows * lda));
   const ElemIdx X = load_idx(g, sraw, L, el, cnt);
-  for (int w = threadIdx.x; w < g.np * g.np; w += blockDim.x) sD[w] = g.D[w];
+  for (int w = threadIdx.x; w < g.np * g.np; w += blockDim.x) sD[w] = S.D[w];
   __syncthreads();
   // boundary-major columns: the product takes the interior rows, F_b stays
   issue_forcing<false>(g, F, X, cnt, m, ncol, sB, ldb, sQ, 0);
@@ -386,7 +386,7 @@ __global__ void __launch_bounds__(32 * kMaxWarps, 1)
   const size_t fm = static_cast<size_t>(m) * S.nfamily + cd.z;
   stage_rows(bar, sA, S.ew + (fm * nint + r_lo) * lda, static_cast<unsigned>(sizeof(double) * rows * lda));
   const ElemIdx X = load_idx(g, sraw, L, el, cnt);
-  for (int w = threadIdx.x; w < g.np * g.np; w += blockDim.x) sD[w] = g.D[w];
+  for (int w = threadIdx.x; w < g.np * g.np; w += blockDim.x) sD[w] = S.D[w];
   __syncthreads();
   // interior forcing only: the boundary rows carry u_b
   issue_forcing<true>(g, F, X, cnt, m, ncol, sB, ldb, sQ, next);

@@ -112,7 +112,7 @@ __global__ void k_condense(DevGeom g, DevNumbering N, DevModal S,
   const int k = blockIdx.y;
   if (g.nz > 1 && k == 1) return;  // Nyquist plane is never solved
   const int m = k >> 1;
-  for (int t = threadIdx.x; t < g.np * g.np; t += blockDim.x) sD[t] = g.D[t];
+  for (int t = threadIdx.x; t < g.np * g.np; t += blockDim.x) sD[t] = S.D[t];
   __syncthreads();
   constrained_forcing(g, N, F + static_cast<size_t>(k) * g.plane_size,
                       G ? G + static_cast<size_t>(k) * gstride : nullptr,
@@ -143,7 +143,7 @@ __global__ void k_recover(DevGeom g, DevNumbering N, DevModal S,
   const int k = blockIdx.y;
   if (g.nz > 1 && k == 1) return;
   const int m = k >> 1;
-  for (int t = threadIdx.x; t < g.np * g.np; t += blockDim.x) sD[t] = g.D[t];
+  for (int t = threadIdx.x; t < g.np * g.np; t += blockDim.x) sD[t] = S.D[t];
   __syncthreads();
   const double* Gp = G ? G + static_cast<size_t>(k) * gstride : nullptr;
   constrained_forcing(g, N, F + static_cast<size_t>(k) * g.plane_size, Gp,
@@ -340,7 +340,7 @@ __global__ void k_condense_chunk(DevGeom g, DevNumbering N, DevModal S, const do
   double* sB = smem;                                   // [2*chunk][ldb]
   double* sD = sB + 2 * g.chunk_max * L.ldb;
   double* wsc = sD + g.np * g.np;                      // [warps][3*nn]
-  for (int w = threadIdx.x; w < g.np * g.np; w += blockDim.x) sD[w] = g.D[w];
+  for (int w = threadIdx.x; w < g.np * g.np; w += blockDim.x) sD[w] = S.D[w];
   __syncthreads();
   chunk_forcing2(g, N, F, G, gstride, S.lambda2[m] + S.betak2[m], el, cnt, m, nr, sB, L.ldb, wsc, sD);
   const double* hbi = S.hbi + (static_cast<size_t>(m) * S.nfamily + g.family[el[0]]) * next * nint;
@@ -379,7 +379,7 @@ __global__ void k_recover_chunk(DevGeom g, DevNumbering N, DevModal S, const dou
   double* sU = sB + 2 * g.chunk_max * L.ldb;           // [2*chunk][ldu] boundary solution
   double* sD = sU + 2 * g.chunk_max * L.ldu;
   double* wsc = sD + g.np * g.np;                      // [warps][3*nn]
-  for (int w = threadIdx.x; w < g.np * g.np; w += blockDim.x) sD[w] = g.D[w];
+  for (int w = threadIdx.x; w < g.np * g.np; w += blockDim.x) sD[w] = S.D[w];
   __syncthreads();
   chunk_forcing2(g, N, F, G, gstride, S.lambda2[m] + S.betak2[m], el, cnt, m, nr, sB, L.ldb, wsc, sD);
   const int nsolve = S.nsolve[m];
@@ -523,7 +523,7 @@ __global__ void k_global_op(DevGeom g, DevNumbering N, DevModal S, const double*
   double* y = Y + static_cast<size_t>(k) * vstride;
   if (N.mixdiag && e == 0)  // <K x, w> on mixed-BC edges (Mixed::augmentOp, src/condition.cpp:379-407)
     for (int q = t; q < N.nglobal; q += blockDim.x) atomicAdd(&y[q], N.mixdiag[q] * x[q]);
-  for (int q = t; q < np * np; q += blockDim.x) sD[q] = g.D[q];
+  for (int q = t; q < np * np; q += blockDim.x) sD[q] = S.D[q];
   if (t < g.next) su[g.emap[t]] = x[N.btog[e * g.next + t]];
   if (t < g.nint) su[g.emap[g.next + t]] = x[N.nglobal + static_cast<size_t>(e) * g.nint + t];
   __syncthreads();
@@ -567,7 +567,7 @@ __global__ void k_pcg_rhs(DevGeom g, DevNumbering N, DevModal S, const double* _
   const int e = blockIdx.x, k = blockIdx.y;
   if (g.nz > 1 && k == 1) return;
   const int m = k >> 1;
-  for (int t = threadIdx.x; t < g.np * g.np; t += blockDim.x) sD[t] = g.D[t];
+  for (int t = threadIdx.x; t < g.np * g.np; t += blockDim.x) sD[t] = S.D[t];
   __syncthreads();
   constrained_forcing(g, N, F + static_cast<size_t>(k) * g.plane_size,
                       G ? G + static_cast<size_t>(k) * gstride : nullptr,
