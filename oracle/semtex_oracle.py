@@ -1247,7 +1247,9 @@ class DNS:
         self.advection = advection          # dns -S/-C/-N (dns/drive.cpp:86-91)
         self.cache = {}
         lam = SS_COEFF[self.nord][0] / (self.dt * self.nu)
-        self.vsys = {c: P.modal_systems(c, lam, "DIRECT", self.cache) for c in self.vel}
+        # preSolve (dns/integrate.cpp:292-325): ITERATIVE selects Jacobi-PCG velocity systems
+        vmethod = "JACPCG" if tok.ivalue("ITERATIVE") else "DIRECT"
+        self.vsys = {c: P.modal_systems(c, lam, vmethod, self.cache) for c in self.vel}
         self.psys = P.modal_systems(self.pname, 0.0, "DIRECT", self.cache)
         self._hopbc_setup()
         self._force_setup()

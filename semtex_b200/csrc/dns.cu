@@ -76,6 +76,7 @@ struct stx_dns {
   int ncom = 0, ndim = 0, nord = 0, form = 1;
   double dt = 0, nu = 0, beta = 0, tol = 0;
   int step_max = 0;
+  bool iterative = false;  // ITERATIVE: Jacobi-PCG velocity systems at every step
   int step = 0;
   double time = 0;
   int toggle = 1;  // altSkewSymmetric's static switch (dns/nonlinear.cpp:254)
@@ -659,7 +660,7 @@ void advance_one(stx_dns* d) {
     if (d->tdep[i]) ckstx(stx_field_bc_evaluate(ctx, d->names[i], d->time));
   // direct systems sharing their matrices: one skeleton solve for all
   // components (every matrix tile read once)
-  bool shared = d->step >= d->nord && d->ncom <= 3;
+  bool shared = d->step >= d->nord && d->ncom <= 3 && !d->iterative;
   for (int i = 1; i < d->ncom; ++i) shared = shared && d->vsys[i]->store == d->vsys[0]->store;
   if (shared) {
     const double* F[3];
@@ -705,10 +706,11 @@ std::vector<double*> pointer_state(const stx_dns* d) {
 }
 
 // A step is steady (its kernels and coefficients repeat) once the start-up
-// orders are past, no BC is re-evaluated on the host and no forcing term
-// changes with time.
+// orders are past, no BC is re-evaluated on the host, no forcing term
+// changes with time and the velocity solves are direct (a Jacobi-PCG solve
+// reads its iteration counts back).
 bool steady(const stx_dns* d) {
-  if (d->step < d->nord || d->force.tdep) return false;
+  if (d->step < d->nord || d->force.tdep || d->iterative) return false;
   for (char t : d->tdep)
     if (t) return false;
   return true;
@@ -899,12 +901,15 @@ int stx_dns_create(stx_context* ctx, int advection, stx_dns** out) {
         }
       }
     }
-    // -- preSolve (dns/integrate.cpp:292-325)
+    // -- preSolve (dns/integrate.cpp:292-325): ITERATIVE = 1 selects
+    //    Jacobi-PCG velocity systems; the pressure system is always direct
     const double lam = kSS[d->nord][0] / (d->dt * d->nu);
     const int nmodes = (ctx->M.nz + 1) / 2;
+    d->iterative = S.tokens.ivalue("ITERATIVE") != 0;
     for (int i = 0; i < d->ncom; ++i) {
       stx_modal* m = nullptr;
-      ckstx(stx_modal_create(ctx, d->names[i], lam, d->beta, 0, nmodes, STX_DIRECT, &m));
+      ckstx(stx_modal_create(ctx, d->names[i], lam, d->beta, 0, nmodes, d->iterative ? STX_JACPCG : STX_DIRECT,
+                             &m));
       d->vsys.push_back(m);
     }
     ckstx(stx_modal_create(ctx, d->names[d->ncom], 0.0, d->beta, 0, nmodes, STX_DIRECT, &d->psys));
