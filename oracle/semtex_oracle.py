@@ -16,7 +16,10 @@ CUDA library accelerates:
 * Field::solve DIRECT / JACPCG                 (src/field.cpp:598-809)
 * z-direction real DFT, packed Re0,Nyq,Re1,Im1 (femlib/fourier.c:40-165)
 * the DNS velocity-correction step             (dns/integrate.cpp:66-289,
-  dns/nonlinear.cpp:198-381)
+  dns/nonlinear.cpp:38-530)
+* body forcing, SVV                            (dns/fieldforce.cpp, src/svv.cpp)
+* cylindrical coordinates with axis BCs        (src/element.cpp:1389-1399,
+  src/field.cpp:1127-1227, src/bcmgr.cpp:153-180, src/edge.cpp:98-256)
 
 The banded factorisation and solve call LAPACK dpbtrf/dpbtrs through scipy,
 the same routines the reference calls (src/matrix.cpp:252, src/field.cpp:693).
@@ -351,6 +354,14 @@ class Mesh:
             y *= tok["Y_SCALE"]
         self.x, self.y = x, y
         self._factors()
+        # Cylindrical coordinates (x axial, y radial, z azimuthal): the
+        # quadrature of Q1-Q4 premultiplied by r = y; Q8 keeps the plain
+        # mass, which weights forcing (src/element.cpp:1389-1399, 800-806)
+        self.cyl = tok.ivalue("CYLINDRICAL") > 0
+        self.Q8 = self.Q4.copy()
+        if self.cyl:
+            for nm in ("Q1", "Q2", "Q3", "Q4"):
+                setattr(self, nm, getattr(self, nm) * self.y)
         self._connect()
 
     # -- src/element.cpp:1253-1408 (Element::mapping)
@@ -445,7 +456,7 @@ class Numbering:
     bmask (1 = essential), solve nodes numbered first, RCM-ordered.
     """
 
-    def __init__(self, M: Mesh, fld: str, rcm: bool = True):
+    def __init__(self, M: Mesh, fld: str, rcm: bool = True, mclass: int = 0):
         S, n, nel = M.S, M.np, M.nel
         nm = n - 1
         next_ = 4 * nm
@@ -491,7 +502,7 @@ class Numbering:
             if (e, s) in M.mate:
                 continue
             bc = S.bcs.get(g, {}).get(fld)
-            if bc and bc[0] == "D":
+            if bc and axis_kind(bc[0], fld, mclass) == "D":
                 for t in range(n):
                     ess[gid[e, (s * nm + t) % next_]] = True
         solve_nodes = np.where(~ess)[0]
@@ -534,7 +545,7 @@ class Numbering:
         em = M.emap()
         mass = np.zeros(nglobal)
         for e in range(nel):
-            np.add.at(mass, self.btog[e], M.Q4[e].ravel()[em[:next_]])
+            np.add.at(mass, self.btog[e], _dssum_weight(M, e)[em[:next_]])
         self.imass = 1.0 / mass
 
 
@@ -704,8 +715,39 @@ def helmholtz_matrix(M: Mesh, e: int, lambda2: float, betak2: float):
     T1 = np.einsum("im,iq,qj,qn->ijmn", I, Q1, D, D)
     T2 = np.einsum("jn,pj,pi,pm->ijmn", I, Q2, D, D)
     T3 = np.einsum("in,nj,im->ijmn", Q3, D, D) + np.einsum("mj,jn,mi->ijmn", Q3, D, D)
-    T4 = np.einsum("im,jn,ij->ijmn", I, I, Q4) * (lambda2 + betak2)
+    T4 = np.einsum("im,jn,ij->ijmn", I, I, Q4 * _hcon(M, e, lambda2, betak2))
     return (T1 + T2 + T3 + T4).reshape(n * n, n * n)
+
+
+def mode_constant(M: Mesh, name: str, mode: int, beta: float):
+    """Field::modeConstant (src/field.cpp:1204-1227): beta k, except in
+    cylindrical coordinates for the coupled v~ (beta k + 1) and w~ (beta k -
+    1) fields, whose uncoupled zeroth mode takes 1."""
+    if not M.cyl or name in "cpu":
+        return beta * mode
+    if name == "v":
+        return 1.0 if mode == 0 else beta * mode + 1.0
+    if name == "w":
+        return 1.0 if mode == 0 else beta * mode - 1.0
+    raise ValueError(f"unrecognised field name {name}")
+
+
+def _hcon(M: Mesh, e, lambda2, betak2):
+    """Helmholtz constant at the nodes: lambda2 + betak2, or in cylindrical
+    coordinates betak2 / r^2 + lambda2 (zero where r^2 <= EPSDP), as
+    Element::HelmholtzRow / HelmholtzKern form it (src/element.cpp:1450,
+    1554-1575)."""
+    if not M.cyl:
+        return lambda2 + betak2
+    r2 = (M.y if e is None else M.y[e]) ** 2
+    return np.where(r2 > EPSDP, betak2 / np.where(r2 > EPSDP, r2, 1.0) + lambda2, 0.0)
+
+
+def _dssum_weight(M: Mesh, e):
+    """Element::bndryDsSum weights (src/element.cpp:433-463): the mass, or
+    in cylindrical coordinates the r-weighted mass, 1 where it vanishes."""
+    w = M.Q4[e].ravel()
+    return np.where(w > EPSDP, w, 1.0) if M.cyl else w
 
 
 def helmholtz_op(M: Mesh, u, lambda2, betak2):
@@ -715,7 +757,7 @@ def helmholtz_op(M: Mesh, u, lambda2, betak2):
     S = D @ u
     R2 = M.Q1 * R + M.Q3 * S
     S2 = M.Q2 * S + M.Q3 * R
-    return M.Q4 * u * (lambda2 + betak2) + D.T @ S2 + R2 @ D
+    return M.Q4 * u * _hcon(M, None, lambda2, betak2) + D.T @ S2 + R2 @ D
 
 
 def grad(M: Mesh, u, direction):
@@ -731,10 +773,27 @@ def grad(M: Mesh, u, direction):
 # Boundary conditions (src/condition.cpp, src/boundary.cpp, src/field.cpp)
 # ---------------------------------------------------------------------------
 
+def axis_kind(kind: str, fld: str, mclass: int) -> str:
+    """An axis BC <A> (cylindrical coordinates) as the homogeneous essential
+    ('D') or natural ('N') condition of its field and Fourier mode class
+    (0, 1, 2 = modes 2 and up), as src/bcmgr.cpp:153-180 tabulates: u, p, c
+    natural in mode 0, essential above; v~ essential; w~ essential except
+    natural in mode 1.  Other kinds are returned unchanged."""
+    if kind != "A":
+        return kind
+    if fld in "upc":
+        return "N" if mclass == 0 else "D"
+    if fld == "v":
+        return "D"
+    if fld == "w":
+        return "N" if mclass == 1 else "D"
+    raise ValueError(f"axis BC for unknown field {fld}")
+
+
 class BoundarySystem:
     """Boundary edges (BCtriples) of one field with their kinds."""
 
-    def __init__(self, M: Mesh, N: Numbering, fld: str):
+    def __init__(self, M: Mesh, N: Numbering, fld: str, mclass: int = 0):
         self.M, self.N, self.fld = M, N, fld
         S = M.S
         self.edges = []      # (e, s, kind, expr)
@@ -744,7 +803,8 @@ class BoundarySystem:
             bc = S.bcs.get(g, {}).get(fld)
             if bc is None:
                 raise ValueError(f"no BC for field {fld} in group {g}")
-            self.edges.append((e, s, bc[0], bc[1]))
+            kind = axis_kind(bc[0], fld, mclass)
+            self.edges.append((e, s, kind, "0.0" if bc[0] == "A" else bc[1]))
         n = M.np
         self.area = []
         for (e, s, _, _) in self.edges:
@@ -752,7 +812,8 @@ class BoundarySystem:
             xs, ys = M.x[e].ravel()[idx], M.y[e].ravel()[idx]
             # straight side: |dx/dl| along the side times the GLL weight
             L = math.hypot(xs[-1] - xs[0], ys[-1] - ys[0])
-            self.area.append(0.5 * L * M.w)
+            # times r in cylindrical coordinates (src/edge.cpp:75)
+            self.area.append(0.5 * L * M.w * (ys if M.cyl else 1.0))
         self.nline = len(self.edges) * n
         # Mixed BCs dc/dn + K (c - C) = 0, "K;C" (Mixed::Mixed, src/condition.cpp:295-312):
         # K C <1, w> in the RHS on every plane (Mixed::sum :315-343) and K <c, w>
@@ -882,7 +943,7 @@ def solve_plane(M: Mesh, N: Numbering, B: BoundarySystem, MS: MatrixSys,
     # -- constrain: f <- -(M f + H g)              (src/field.cpp:812-852)
     gvec = np.zeros(nglobal)
     B.get_essential(bcline, gvec)
-    F = M.Q4 * forcing
+    F = M.Q8 * forcing
     if N.emask.any():
         u = np.zeros_like(F)
         flat = u.reshape(nel, -1)
@@ -1078,7 +1139,23 @@ class Problem:
         for c in S.fields:
             self.N[c] = Numbering(self.M, c, rcm)
             self.B[c] = BoundarySystem(self.M, self.N[c], c)
+        # cylindrical 3D with axis BCs: numbering and BCs per Fourier mode
+        # class 0, 1, 2+ (BCmgr::getNumberSys, src/bcmgr.cpp:550-583)
+        self.axis = self.M.cyl and self.nz > 1 and any(
+            bc[0] == "A" for g in S.bcs.values() for bc in g.values())
+        self.NB = {}
+        for c in S.fields:
+            for mc in range(3):
+                if self.axis and mc > 0:
+                    N = Numbering(self.M, c, rcm, mc)
+                    self.NB[(c, mc)] = (N, BoundarySystem(self.M, N, c, mc))
+                else:
+                    self.NB[(c, mc)] = (self.N[c], self.B[c])
         self.dz = 2 * math.pi / tok["BETA"] / self.nz
+
+    def nb(self, c, mode):
+        """(Numbering, BoundarySystem) of field c for Fourier mode `mode`."""
+        return self.NB[(c, min(mode, 2))]
 
     def evaluate(self, expr, t=0.0):
         """AuxField = function, physical space (src/auxfield.cpp:198-220)."""
@@ -1106,12 +1183,13 @@ class Problem:
               if lambda2 > EPSDP else np.ones(nmodes))
         out = []
         for m in range(nmodes):
-            bk2 = (beta * m) ** 2 * sz[m]
-            key = (c, round(lambda2, 14), round(bk2, 14), method)
+            bk2 = mode_constant(self.M, c, m, beta) ** 2 * sz[m]
+            key = (c, round(lambda2, 14), round(bk2, 14), method, min(m, 2) if self.axis else 0)
             if cache is not None and key in cache:
                 out.append(cache[key])
                 continue
-            ms = MatrixSys(self.M, self.N[c], lambda2, bk2, method, self.B[c].mixdiag)
+            N, B = self.nb(c, m)
+            ms = MatrixSys(self.M, N, lambda2, bk2, method, B.mixdiag)
             if cache is not None:
                 cache[key] = ms
             out.append(ms)
@@ -1123,7 +1201,8 @@ class Problem:
         for k in range(self.nz):
             if k == 1:
                 continue
-            out[k] = solve_plane(self.M, self.N[c], self.B[c], systems[k >> 1],
+            N, B = self.nb(c, k >> 1)
+            out[k] = solve_plane(self.M, N, B, systems[k >> 1],
                                  forcing[k], unknown[k], bclines[k], tol_rel, step_max)
         return out
 
@@ -1197,7 +1276,7 @@ def smooth(P: Problem, c: str, u):
     next_ = 4 * (P.np - 1)
     em = M.emap()[:next_]
     out = u.copy()
-    wq = M.Q4.reshape(P.nel, -1)[:, em]
+    wq = np.stack([_dssum_weight(M, e) for e in range(P.nel)])[:, em]
     for k in range(u.shape[0]):
         flat = out[k].reshape(P.nel, -1)
         ds = np.zeros(N.nglobal)
@@ -1429,6 +1508,8 @@ class DNS:
             ny = sgn * getattr(M, c)[e].ravel()[idx]
             ln = np.hypot(nx, ny)
             self.nx[b], self.ny[b] = nx / ln, ny / ln
+        ey = np.stack([M.y[e].ravel()[idx] for (e, idx) in self.eidx]) if self.eidx else np.zeros((0, P.np))
+        self._edge_divy = np.where(ey > EPSDP, 1.0 / np.where(ey > EPSDP, ey, 1.0), 0.0)
         shape = (P.nz, nedge, P.np)
         self.un = [np.zeros(shape) for _ in range(self.nord)]
         self.hop = [np.zeros(shape) for _ in range(self.nord)]
@@ -1459,14 +1540,23 @@ class DNS:
                 for q in range(Je):
                     w = w + a[q + 1] * self.un[q][k]
                 h[k] = -invdt * w
-            h[k] += self._edges(N[0][k]) * self.nx + self._edges(N[1][k]) * self.ny
+            nN = self._edges(N[0][k]) * self.nx + self._edges(N[1][k]) * self.ny
+            if M.cyl:        # N_x, N_y are radius-premultiplied (src/bcmgr.cpp:1141-1143)
+                nN = nN * self._edge_divy
+            h[k] += nN
         self.un = [un] + self.un[:-1]
         beta = P.S.tokens["BETA"]
         nu = self.nu
 
+        dy = self._edge_divy if M.cyl else 1.0       # Element::sideDivY (src/element.cpp:965-1010)
+        dy2 = dy * dy if M.cyl else 1.0
+
         def curl_terms(Ur, Vr):
             w = grad(M, Vr, 0) - grad(M, Ur, 1)
-            return self._edges(grad(M, w, 1)), -self._edges(grad(M, w, 0))
+            x = self._edges(grad(M, w, 1))
+            if M.cyl:                                  # + w / r (src/edge.cpp:160-167)
+                x = x + self._edges(w) * dy
+            return x, -self._edges(grad(M, w, 0))
 
         xr, yr = curl_terms(U[0][0], U[1][0])
         h[0] += -nu * xr * self.nx
@@ -1476,14 +1566,17 @@ class DNS:
             kr, ki = 2 * m, 2 * m + 1
             xr, yr = curl_terms(U[0][kr], U[1][kr])
             xi, yi = curl_terms(U[0][ki], U[1][ki])
-            xi = xi + bk * self._edges(grad(M, U[2][kr], 0))
-            yi = yi + bk * self._edges(grad(M, U[2][kr], 1))
-            xr = xr - bk * self._edges(grad(M, U[2][ki], 0))
-            yr = yr - bk * self._edges(grad(M, U[2][ki], 1))
-            xr = xr + bk * bk * self._edges(U[0][kr])
-            xi = xi + bk * bk * self._edges(U[0][ki])
-            yr = yr + bk * bk * self._edges(U[1][kr])
-            yi = yi + bk * bk * self._edges(U[1][ki])
+            xi = xi + bk * self._edges(grad(M, U[2][kr], 0)) * dy
+            yi = yi + bk * self._edges(grad(M, U[2][kr], 1)) * dy
+            xr = xr - bk * self._edges(grad(M, U[2][ki], 0)) * dy
+            yr = yr - bk * self._edges(grad(M, U[2][ki], 1)) * dy
+            if M.cyl:                                  # src/edge.cpp:203-204, 221-222
+                yi = yi + bk * self._edges(U[2][kr]) * dy2
+                yr = yr - bk * self._edges(U[2][ki]) * dy2
+            xr = xr + bk * bk * self._edges(U[0][kr]) * dy2
+            xi = xi + bk * bk * self._edges(U[0][ki]) * dy2
+            yr = yr + bk * bk * self._edges(U[1][kr]) * dy2
+            yi = yi + bk * bk * self._edges(U[1][ki]) * dy2
             h[kr] += -nu * xr * self.nx
             h[ki] += -nu * xi * self.nx
             h[kr] += -nu * yr * self.ny
@@ -1538,6 +1631,8 @@ class DNS:
         else:
             forms = ()
         N = []
+        if P.M.cyl:
+            return self._nonlinear_cyl(U, Uphys, forms)
         for i in range(self.ncom):
             n = np.zeros_like(Uphys[0])
             for j in range(self.ndim):
@@ -1564,6 +1659,89 @@ class DNS:
             self.toggle = 1 - self.toggle
         return U, N
 
+    def _nonlinear_cyl(self, U, Uphys, forms):
+        """Cylindrical nonlinear terms (dns/nonlinear.cpp:97-160, 258-334,
+        398-440): radius-premultiplied x and r components, frame terms of
+        the azimuthal velocity, z the azimuthal Fourier direction."""
+        P = self.P
+        y = P.M.y[None]
+        nz3 = P.nz > 2
+        divy = np.where(y > EPSDP, 1.0 / np.where(y > EPSDP, y, 1.0), 0.0)
+        N = []
+        for i in range(self.ncom):
+            n = np.zeros_like(Uphys[0])
+            if forms == ("conv", "cons"):                 # skewSymmetric (:97-160)
+                if i == 0:
+                    n -= Uphys[0] * Uphys[1]
+                if i == 1:
+                    n -= Uphys[1] * Uphys[1]
+                if self.ncom == 3:
+                    if i == 1:
+                        n += 2.0 * (Uphys[2] * Uphys[2])
+                    if i == 2:
+                        n += -3.0 * (Uphys[2] * Uphys[1])
+                    if nz3:
+                        n -= Uphys[2] * self._inverse32(fourier_grad_z(P, U[i]))
+                        n -= self._inverse32(fourier_grad_z(P, self._forward32(Uphys[i] * Uphys[2])))
+            elif forms == ("conv",):                       # u.grad(u) (:264-292, 398-430)
+                if self.ncom == 3:
+                    if i == 1:
+                        n = Uphys[2] * Uphys[2]
+                    if i == 2:
+                        n = -(Uphys[2] * Uphys[1])
+                    if nz3:
+                        n -= Uphys[2] * self._inverse32(fourier_grad_z(P, U[i]))
+            elif forms == ("cons",):                       # div(uu) (:298-334)
+                if i == 0:
+                    n -= Uphys[0] * Uphys[1]
+                if i == 1:
+                    n -= Uphys[1] * Uphys[1]
+                if self.ncom == 3:
+                    if i == 1:
+                        n += Uphys[2] * Uphys[2]
+                    if i == 2:
+                        n += -2.0 * (Uphys[2] * Uphys[1])
+                    if nz3:
+                        n -= self._inverse32(fourier_grad_z(P, self._forward32(Uphys[i] * Uphys[2])))
+            if forms and i == 2:
+                n = n * divy
+            if "conv" in forms:
+                for j in range(2):
+                    tmp = grad(P.M, Uphys[i], j)
+                    if i < 2:
+                        tmp = tmp * y
+                    n -= Uphys[j] * tmp
+            if "cons" in forms:
+                for j in range(2):
+                    tmp = grad(P.M, Uphys[j] * Uphys[i], j)
+                    if i < 2:
+                        tmp = tmp * y
+                    n -= tmp
+            if len(forms) == 2:
+                n *= 0.5
+            n = self._force_physical(i, n, Uphys)
+            n = self._forward32(n)
+            n = self._force_fourier(i, n)
+            N.append(smooth(P, self.vel[0], n))
+        if self.advection == 1:
+            self.toggle = 1 - self.toggle
+        return U, N
+
+    def _couple(self, v, w, sign):
+        """AuxField::couple (src/auxfield.cpp:1376-1451) on modes k >= 1:
+        forward v~ = v + i w, w~ = v - i w; inverse back."""
+        v, w = v.copy(), w.copy()
+        for m in range(1, (self.P.nz + 1) // 2):
+            kr, ki = 2 * m, 2 * m + 1
+            Vr, Vi, Wr, Wi = v[kr].copy(), v[ki].copy(), w[kr].copy(), w[ki].copy()
+            if sign > 0:
+                v[kr], v[ki] = Vr - Wi, Vi + Wr
+                w[kr], w[ki] = Vr + Wi, Vi - Wr
+            else:
+                v[kr], v[ki] = 0.5 * (Vr + Wr), 0.5 * (Vi + Wi)
+                w[kr], w[ki] = 0.5 * (Vi - Wi), 0.5 * (Wr - Vr)
+        return v, w
+
     def advance(self, nsteps: int = 1):
         P = self.P
         tok = P.S.tokens
@@ -1574,6 +1752,11 @@ class DNS:
             self.step += 1
             self.time += self.dt
             self._maintain_fourier(U, N)
+            cyl = P.M.cyl
+            if cyl:                                   # dns/integrate.cpp:160
+                y = P.M.y[None]
+                U[0], U[1] = U[0] * y, U[1] * y
+                self.Us[0] = U
             # -- waveProp (dns/integrate.cpp:204-239)
             Je = min(self.step, self.nord)
             alpha = SS_COEFF[Je]
@@ -1599,13 +1782,25 @@ class DNS:
             b = 1.0 / self.nu
             forc = []
             for i in range(self.ncom):
-                f = a * uhat[i]
+                f = a * (uhat[i] * y if cyl and i == 2 else uhat[i])
                 if i < self.ndim:
-                    f = f + b * plane_grad(P, self.u[pc], i)
+                    g = plane_grad(P, self.u[pc], i)
+                    f = f + b * (g * y if cyl and i < 2 else g)
                 forc.append(f)
-            self.Us[0] = [self.u[c] for c in self.vel]
+            # the velocity level stored is the step's old velocity as the
+            # nonlinear step copied it (radius-weighted in cylindrical
+            # coordinates: D->u holds it after waveProp's swap)
+            self.Us[0] = U
             self.Us = [self.Us[-1]] + self.Us[:-1]          # rollm(Us)
-            # -- viscous substep (dns/integrate.cpp:186-193, 328-356)
+            # -- viscous substep (dns/integrate.cpp:177-193, 328-356); in
+            #    cylindrical 3D v and w are solved coupled as v~, w~
+            c3d = cyl and self.ncom == 3
+            lines = {c: P.bc_lines(c, self.time) for c in self.vel}
+            if c3d:
+                forc[1], forc[2] = self._couple(forc[1], forc[2], 1)
+                self.u[self.vel[1]], self.u[self.vel[2]] = self._couple(self.u[self.vel[1]],
+                                                                        self.u[self.vel[2]], 1)
+                lines[self.vel[1]], lines[self.vel[2]] = self._couple(lines[self.vel[1]], lines[self.vel[2]], 1)
             for i, c in enumerate(self.vel):
                 if self.step < self.nord:
                     lam = SS_COEFF[Je][0] / (self.dt * self.nu)
@@ -1613,8 +1808,11 @@ class DNS:
                 else:
                     sysi = self.vsys[c]
                 self.u[c] = P.solve(c, forc[i], self.u[c], sysi,
-                                    P.bc_lines(c, self.time), tok["TOL_REL"],
+                                    lines[c], tok["TOL_REL"],
                                     tok.ivalue("STEP_MAX"))
+            if c3d:
+                self.u[self.vel[1]], self.u[self.vel[2]] = self._couple(self.u[self.vel[1]],
+                                                                        self.u[self.vel[2]], -1)
 
     # -- Statistics (src/statistics.cpp:94-405), AVERAGE 1 or 2
     def stats_init(self, level):

@@ -31,6 +31,20 @@ def test_dns_regress_goldens(name, fields):
             assert got[c] == GOLD["MPI/" + name][c]
 
 
+@pytest.mark.parametrize("name,fields", [
+    ("sbr", "uvwp"), ("tc1", "uvwp"), ("tube1", "uvp"), ("tube2", "uvwp"), ("tube3", "uvwp"), ("cylkov2", "uvwp"),
+])
+def test_cylindrical_regress_goldens(name, fields):
+    # cylindrical coordinates (x axial, y radial, z azimuthal): radius-weighted
+    # quadrature, mode constants and coupling of v and w, axis BCs per Fourier
+    # mode class, radius-premultiplied nonlinear terms (src/element.cpp:1389-
+    # 1399, src/field.cpp:1127-1227, src/bcmgr.cpp:153-180, dns/nonlinear.cpp)
+    D = O.dns_session(os.path.join(SESSIONS, name))
+    got = O.compare_errors(D)
+    for c in fields:
+        assert got[c] == GOLD[name][c], (name, c, got[c], GOLD[name][c])
+
+
 def test_dns_iterative_velocity_goldens():
     # ITERATIVE = 1: Jacobi-PCG velocity systems at every step (preSolve,
     # dns/integrate.cpp:292-325) leave the 5-digit goldens unchanged
