@@ -20,7 +20,7 @@ import sys
 HERE = os.path.dirname(os.path.abspath(__file__))
 SESSIONS = ["taylor2", "taylor3", "taylor4", "taylor5", "kovas1", "kovas2", "kovas3", "kovas4", "kovas5",
             "helmholtz1", "laplace1",
-            "laplace3", "laplace4", "poisson1", "tgreen", "mixed1", "tgreen100", "sbr", "tc1", "tube1", "tube2", "tube3", "cylkov2"]
+            "laplace3", "laplace4", "poisson1", "tgreen", "mixed1", "tgreen100", "sbr", "tc1", "tube1", "tube2", "tube3", "cylkov2", "laplace8", "laplace9"]
 
 
 def main(ref):

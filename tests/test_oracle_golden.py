@@ -158,3 +158,12 @@ def test_three_halves_rule_removes_aliases():
     plain = O.dft_forward(O.dft_inverse(F) * O.dft_inverse(G))
     assert abs(prod[2] - 0.25).max() < 1e-15 and abs(prod[6]).max() < 1e-15
     assert abs(plain[6] - 0.25).max() < 1e-15
+
+
+@pytest.mark.parametrize("name", ["laplace8", "laplace9"])
+def test_cylindrical_laplace_analytic(name):
+    # elliptic/testsuite cylindrical Laplace problems with analytic solutions
+    # (laplace8 reaches the axis: axis BCs by Fourier mode class)
+    P, U = O.elliptic(os.path.join(SESSIONS, name))
+    exact = P.evaluate(O.user_functions(P.S)["c"])
+    assert np.abs(U - exact).max() < 1e-8 * np.abs(exact).max()
