@@ -83,6 +83,19 @@ int stx_numbering(const stx_context* ctx, char field, int* nglobal, int* nsolve,
  * number); others by this library's reverse Cuthill--McKee. */
 int stx_numbering_host(const char* session_path, const char* overrides, char field, int* nel,
                        int* next, int* nglobal, int* nsolve, int* nband, int* h_btog, int* h_bmask);
+/* As stx_numbering_host, for Fourier mode `mode`: in cylindrical 3D sessions
+ * with axis BCs <A> the numbering of modes 0, 1 and 2+ differ
+ * (BCmgr::getNumberSys, src/bcmgr.cpp:550-583: the `.num` schemes u/U,
+ * w/W, p/P, c/C); otherwise every mode takes the mode-0 numbering. */
+int stx_numbering_host_mode(const char* session_path, const char* overrides, char field, int mode, int* nel,
+                            int* next, int* nglobal, int* nsolve, int* nband, int* h_btog, int* h_bmask);
+/* Elemental Helmholtz matrix of element `elmt` on the host, np^2 x np^2
+ * row-major over the element's row-major nodes (Element::HelmholtzRow,
+ * src/element.cpp:1411-1481; in cylindrical coordinates r-weighted, with
+ * betak2 / r^2 + lambda2 as the Helmholtz constant).  *np (if not null)
+ * receives N_P; h_matrix may be null. */
+int stx_element_matrix_host(const char* session_path, const char* overrides, int elmt, double lambda2,
+                            double betak2, int* np, double* h_matrix);
 /* Element node locations, host buffers of nel*np*np (Element::_xmesh). */
 int stx_mesh_coords(const stx_context* ctx, double* h_x, double* h_y);
 /* Element mass weights (quadrature weight x Jacobian, Element::_Q4), host

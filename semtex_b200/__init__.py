@@ -27,7 +27,7 @@ from .fieldfile import read_field, write_field
 
 DIRECT, JACPCG, MIXED = STX_DIRECT, STX_JACPCG, STX_MIXED
 
-__all__ = ["Context", "ModalMatrixSys", "Field", "DNS", "Batch", "expression", "svv", "numbering", "solve_multi", "elliptic", "dns", "read_field",
+__all__ = ["Context", "ModalMatrixSys", "Field", "DNS", "Batch", "expression", "svv", "numbering", "element_matrix", "solve_multi", "elliptic", "dns", "read_field",
            "write_field", "FORWARD", "INVERSE", "DIRECT", "JACPCG", "MIXED", "StxError"]
 
 
@@ -303,22 +303,37 @@ def svv(np_: int, eps_n: float, m_n: int, nz: int = 1, eps_z: float = 0.0, m_z: 
     return D, Z
 
 
-def numbering(session: str, field: str, overrides=None):
+def numbering(session: str, field: str, overrides=None, mode: int = 0):
     """The `enumerate` utility (utility/enumerate.cpp:110-199) on the host, no
-    GPU needed: one field's global numbering as a dict of nglobal, nsolve,
-    nband and the per-element boundary-major arrays btog / bmask."""
+    GPU needed: one field's global numbering for Fourier mode `mode` (they
+    differ only in cylindrical sessions with axis BCs) as a dict of nglobal,
+    nsolve, nband and the per-element boundary-major arrays btog / bmask."""
     if isinstance(overrides, dict):
         overrides = ";".join(f"{k}={v}" for k, v in overrides.items())
     ov = overrides.encode() if overrides else None
     v = [C.c_int() for _ in range(5)]
-    check(lib().stx_numbering_host(session.encode(), ov, field.encode(), *[C.byref(x) for x in v],
-                                   None, None))
+    check(lib().stx_numbering_host_mode(session.encode(), ov, field.encode(), int(mode),
+                                        *[C.byref(x) for x in v], None, None))
     nel, next_, nglobal, nsolve, nband = (x.value for x in v)
     btog = np.zeros((nel, next_), np.int32)
     bmask = np.zeros((nel, next_), np.int32)
-    check(lib().stx_numbering_host(session.encode(), ov, field.encode(), None, None, None, None, None,
-                                   C.c_void_p(btog.ctypes.data), C.c_void_p(bmask.ctypes.data)))
+    check(lib().stx_numbering_host_mode(session.encode(), ov, field.encode(), int(mode), None, None, None, None,
+                                        None, C.c_void_p(btog.ctypes.data), C.c_void_p(bmask.ctypes.data)))
     return {"nglobal": nglobal, "nsolve": nsolve, "nband": nband, "btog": btog, "bmask": bmask}
+
+
+def element_matrix(session: str, elmt: int, lambda2: float, betak2: float, overrides=None):
+    """Elemental Helmholtz matrix (np^2 x np^2, row-major nodes) on the host."""
+    if isinstance(overrides, dict):
+        overrides = ";".join(f"{k}={v}" for k, v in overrides.items())
+    ov = overrides.encode() if overrides else None
+    n = C.c_int()
+    check(lib().stx_element_matrix_host(session.encode(), ov, int(elmt), float(lambda2), float(betak2),
+                                        C.byref(n), None))
+    H = np.empty((n.value ** 2, n.value ** 2))
+    check(lib().stx_element_matrix_host(session.encode(), ov, int(elmt), float(lambda2), float(betak2), None,
+                                        H.ctypes.data))
+    return H
 
 
 def _user_value(session: str, key: str):

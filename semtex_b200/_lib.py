@@ -34,6 +34,8 @@ SIGNATURES = {
     "stx_token": (_i, [_p, _s, _pd]),
     "stx_numbering": (_i, [_p, C.c_char, _pi, _pi, _pi]),
     "stx_numbering_host": (_i, [_s, _s, C.c_char, _pi, _pi, _pi, _pi, _pi, _p, _p]),
+    "stx_numbering_host_mode": (_i, [_s, _s, C.c_char, _i, _pi, _pi, _pi, _pi, _pi, _p, _p]),
+    "stx_element_matrix_host": (_i, [_s, _s, _i, _d, _d, _pi, _p]),
     "stx_mesh_coords": (_i, [_p, _p, _p]),
     "stx_mesh_families": (_i, [_p, _pi]),
     "stx_mesh_mass": (_i, [_p, _p]),

@@ -336,12 +336,22 @@ int stx_numbering(const stx_context* ctx, char field, int* nglobal, int* nsolve,
 
 int stx_numbering_host(const char* session_path, const char* overrides, char field, int* nel, int* next,
                        int* nglobal, int* nsolve, int* nband, int* h_btog, int* h_bmask) {
+  return stx_numbering_host_mode(session_path, overrides, field, 0, nel, next, nglobal, nsolve, nband, h_btog,
+                                 h_bmask);
+}
+
+int stx_numbering_host_mode(const char* session_path, const char* overrides, char field, int mode, int* nel,
+                            int* next, int* nglobal, int* nsolve, int* nband, int* h_btog, int* h_bmask) {
   return guarded([&] {
-    if (!session_path) throw StxError(STX_EINVAL, "null argument");
+    if (!session_path || mode < 0) throw StxError(STX_EINVAL, "bad argument");
     const Session S = read_session(session_path, overrides ? overrides : "");
     if (S.fields.find(field) == std::string::npos) throw StxError(STX_EINVAL, std::string("no field ") + field);
     const Mesh M = build_mesh(S);
-    const Numbering N = build_numbering(S, M, field);
+    bool axis = false;
+    for (const auto& g : S.bcs)
+      for (const auto& f : g.second) axis = axis || f.second.kind == 'A';
+    const int mclass = M.cyl && M.nz > 1 && axis ? std::min(mode, 2) : 0;
+    const Numbering N = build_numbering(S, M, field, 48, mclass);
     if (nel) *nel = M.nel;
     if (next) *next = M.next;
     if (nglobal) *nglobal = N.nglobal;
@@ -349,6 +359,18 @@ int stx_numbering_host(const char* session_path, const char* overrides, char fie
     if (nband) *nband = N.nband;
     if (h_btog) std::memcpy(h_btog, N.btog.data(), sizeof(int) * N.btog.size());
     if (h_bmask) std::memcpy(h_bmask, N.bmask.data(), sizeof(int) * N.bmask.size());
+  });
+}
+
+int stx_element_matrix_host(const char* session_path, const char* overrides, int elmt, double lambda2,
+                            double betak2, int* np, double* h_matrix) {
+  return guarded([&] {
+    if (!session_path) throw StxError(STX_EINVAL, "null argument");
+    const Session S = read_session(session_path, overrides ? overrides : "");
+    const Mesh M = build_mesh(S);
+    if (elmt < 0 || elmt >= M.nel) throw StxError(STX_EINVAL, "element out of range");
+    if (np) *np = M.np;
+    if (h_matrix) element_helmholtz(M, elmt, lambda2, betak2, h_matrix);
   });
 }
 

@@ -103,7 +103,9 @@ void element_helmholtz(const Mesh& M, int e, double lambda2, double betak2, doub
           row[m * n + c] += Q3[i * n + c] * D[c * n + j] * D[i * n + m];
           row[m * n + c] += Q3[m * n + j] * D[j * n + c] * D[m * n + i];
         }
-      row[i * n + j] += Q4[i * n + j] * hcon;
+      // cylindrical: betak2 / r^2 + lambda2, zero on the axis (src/element.cpp:1450)
+      const double r2 = M.cyl ? M.y[e * nn + i * n + j] * M.y[e * nn + i * n + j] : 1.0;
+      row[i * n + j] += Q4[i * n + j] * (M.cyl ? (r2 > 6.0e-14 ? betak2 / r2 + lambda2 : 0.0) : hcon);
     }
 }
 

@@ -216,7 +216,8 @@ Mesh build_mesh(const Session& S) {
   }
 
   // -- geometric factors (src/element.cpp:1307-1407)
-  for (auto* v : {&M.Q1, &M.Q2, &M.Q3, &M.Q4, &M.drdx, &M.drdy, &M.dsdx, &M.dsdy})
+  M.cyl = S.tokens.ivalue("CYLINDRICAL") != 0;
+  for (auto* v : {&M.Q1, &M.Q2, &M.Q3, &M.Q4, &M.Q8, &M.drdx, &M.drdy, &M.dsdx, &M.dsdy})
     v->assign(M.nplane, 0.0);
   for (int e = 0; e < nel; ++e) {
     const double* X = &M.x[e * M.npnp];
@@ -243,6 +244,15 @@ Mesh build_mesh(const Session& S) {
         M.drdy[ij] = -xs_ / jac;
         M.dsdx[ij] = -yr / jac;
         M.dsdy[ij] = xr / jac;
+      }
+    // the plain mass, then r premultiplied into the quadrature
+    for (int k = 0; k < M.npnp; ++k) M.Q8[e * M.npnp + k] = M.Q4[e * M.npnp + k];
+    if (M.cyl)
+      for (int k = e * M.npnp; k < (e + 1) * M.npnp; ++k) {
+        M.Q1[k] *= M.y[k];
+        M.Q2[k] *= M.y[k];
+        M.Q3[k] *= M.y[k];
+        M.Q4[k] *= M.y[k];
       }
     // null-mapping: vectors below 4*EPSDP in 2-norm are exactly zero
     for (auto* v : {&M.drdx, &M.drdy, &M.dsdx, &M.dsdy, &M.Q3}) {
@@ -624,7 +634,15 @@ std::vector<int> enumerate_o3(const std::vector<int>& bmap, int nel, int next) {
   return out;
 }
 
-Numbering build_numbering(const Session& S, const Mesh& M, char field, int rcm_roots) {
+char axis_kind(char kind, char field, int mclass) {
+  if (kind != 'A') return kind;
+  if (field == 'u' || field == 'p' || field == 'c') return mclass == 0 ? 'N' : 'D';
+  if (field == 'v') return 'D';
+  if (field == 'w') return mclass == 1 ? 'N' : 'D';
+  throw std::runtime_error(std::string("axis BC for unknown field ") + field);
+}
+
+Numbering build_numbering(const Session& S, const Mesh& M, char field, int rcm_roots, int mclass) {
   const int n = M.np, nel = M.nel, nm = n - 1, next = M.next;
   Numbering N;
   N.field = field;
@@ -689,7 +707,17 @@ Numbering build_numbering(const Session& S, const Mesh& M, char field, int rcm_r
       auto bi = gi->second.find(field);
       if (bi == gi->second.end())
         throw std::runtime_error(std::string("no BC for field ") + field + " in group " + g);
-      const BCSpec& bc = bi->second;
+      BCSpec bc = bi->second;
+      if (bc.kind == 'A') {  // axis: on y = 0, cylindrical only (BCmgr::buildsurf, src/bcmgr.cpp:872-890)
+        if (!M.cyl) throw std::runtime_error("axis BCs disallowed in Cartesian coords");
+        std::vector<int> idx(n);
+        M.side_nodes(s, idx.data());
+        for (int t = 0; t < n; ++t)
+          if (std::fabs(M.y[e * M.npnp + idx[t]]) > kEpsDP)
+            throw std::runtime_error("y value too large on axis BC");
+        bc.kind = axis_kind('A', field, mclass);
+        bc.expr = "0.0";
+      }
       if (bc.kind == 'D') {
         for (int t = 0; t <= nm; ++t) ess[gid[e * next + (s * nm + t) % next]] = 1;
       } else if (bc.kind == 'H') {
@@ -811,7 +839,12 @@ Numbering build_numbering(const Session& S, const Mesh& M, char field, int rcm_r
   N.imass.assign(nglobal, 0.0);
   for (int e = 0; e < nel; ++e)
     for (int i = 0; i < next; ++i)
-      N.imass[N.btog[e * next + i]] += M.Q4[e * M.npnp + M.emap[i]];
+    {
+      // Element::bndryDsSum weights (src/element.cpp:433-463): in cylindrical
+      // coordinates 1 where the r-weighted mass vanishes (on the axis)
+      const double w = M.Q4[e * M.npnp + M.emap[i]];
+      N.imass[N.btog[e * next + i]] += M.cyl && !(w > kEpsDP) ? 1.0 : w;
+    }
   for (auto& v : N.imass) v = 1.0 / v;
   return N;
 }

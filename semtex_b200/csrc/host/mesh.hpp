@@ -50,6 +50,11 @@ struct Mesh {
   std::vector<int> family_rep;           // family -> representative element
   int nfamily = 0;
   std::vector<double> svv_D;             // SVV derivative of the viscous operators, or empty
+  // Cylindrical coordinates (token CYLINDRICAL; x axial, y radial, z
+  // azimuthal): Q1-Q4 carry the radius r = y in their quadrature, Q8 the
+  // plain mass that weights forcing (src/element.cpp:1389-1399, 800-806).
+  bool cyl = false;
+  std::vector<double> Q8;                // [nel*npnp]
 
   // Row-major node indices of side s in CCW traverse (src/element.h:162-170).
   void side_nodes(int s, int* idx) const;
@@ -100,6 +105,15 @@ std::vector<int> rcm_order(std::vector<std::vector<int>>& nbr, int rcm_roots);
 
 // rcm_roots: number of trial roots for the reverse Cuthill--McKee search
 // (the role of enumerate's optimisation levels, utility/enumerate.cpp:706-832).
-Numbering build_numbering(const Session& S, const Mesh& M, char field, int rcm_roots = 48);
+// mclass: the Fourier mode class (0, 1, 2 = modes 2 and up) whose axis BCs
+// apply (cylindrical coordinates, axis_kind); 0 when there is no axis.
+Numbering build_numbering(const Session& S, const Mesh& M, char field, int rcm_roots = 48, int mclass = 0);
+
+// An axis BC <A> as the homogeneous essential ('D') or natural ('N')
+// condition of field `field` in Fourier mode class `mclass` (0, 1, 2+),
+// as src/bcmgr.cpp:153-180 tabulates: u, p, c natural in mode 0 and
+// essential above; v~ essential; w~ essential except natural in mode 1.
+// Other kinds are returned unchanged.
+char axis_kind(char kind, char field, int mclass);
 
 }  // namespace stx
