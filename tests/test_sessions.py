@@ -1,4 +1,4 @@
-"""Session writer produces the BASELINE shapes (CPU, oracle numbering)."""
+"""Session writer produces the benchmark workloads' shapes (CPU, oracle numbering)."""
 import numpy as np
 
 import semtex_oracle as O
