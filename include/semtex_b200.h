@@ -119,6 +119,12 @@ int stx_field_evaluate(const stx_context* ctx, const char* expr, double t, doubl
 int stx_expression_eval(const char* expr, const char* assignments, int compiled, int n, const double* x,
                         const double* y, const double* z, double t, double* out, int* nops);
 
+/* FORCE-section token lookup, host only (FEML::valueFromSection on
+ * <FORCE>, src/feml.cpp:519-560): the text after `token` on its line, up to
+ * the next '=', into buf (len bytes, NUL-terminated).  *found = 0 when the
+ * section or the token is absent. */
+int stx_session_force_value(const char* session_path, const char* token, char* buf, int len, int* found);
+
 /* Spectral vanishing viscosity operators, host only (SVV::operators and
  * SVV::coeffs / coeffs_z, src/svv.cpp:20-185): d_matrix[np*np] receives the
  * derivative matrix the viscous (lambda2 > 0) systems use -- the SVV one for

@@ -42,6 +42,7 @@ SIGNATURES = {
     "stx_field_evaluate": (_i, [_p, _s, _d, _p]),
     "stx_expression_eval": (_i, [_s, _s, _i, _i, _p, _p, _p, _d, _p, _pi]),
     "stx_svv": (_i, [_i, _d, _i, _i, _d, _i, _d, _p, _p]),
+    "stx_session_force_value": (_i, [_s, _s, _p, _i, _pi]),
     "stx_field_bc_evaluate": (_i, [_p, C.c_char, _d]),
     "stx_modal_create": (_i, [_p, C.c_char, _d, _d, _i, _i, _i, C.POINTER(_p)]),
     "stx_modal_destroy": (_i, [_p]),

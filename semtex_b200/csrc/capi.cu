@@ -447,6 +447,18 @@ int stx_expression_eval(const char* expr, const char* assignments, int compiled,
   });
 }
 
+int stx_session_force_value(const char* session_path, const char* token, char* buf, int len, int* found) {
+  return guarded([&] {
+    if (!session_path || !token || !buf || len < 1 || !found) throw StxError(STX_EINVAL, "bad argument");
+    const Session S = read_session(session_path, "");
+    std::string v;
+    *found = S.force_value(token, v) ? 1 : 0;
+    if (!*found) v.clear();
+    if (static_cast<int>(v.size()) >= len) throw StxError(STX_EINVAL, "buffer too short");
+    std::memcpy(buf, v.c_str(), v.size() + 1);
+  });
+}
+
 int stx_svv(int np, double eps_n, int m_n, int nz, double eps_z, int m_z, double kinvis, double* d_matrix,
             double* z_factors) {
   return guarded([&] {

@@ -76,3 +76,25 @@ def test_oracle_poiseuille_stays_steady(tmp_path):
     D0.force = None
     D0.advance(5)
     assert np.abs(D0.physical()["u"] - ph["u"]).max() > 1e-3
+
+
+def test_force_section_lookup_matches_oracle(tmp_path):
+    # the library's FORCE-section reader (host, no device) against the
+    # oracle's restatement of FEML::valueFromSection, quirks included
+    import ctypes as C
+    from semtex_b200._lib import lib
+    lines = ["CONST_X = 1.5", "# a comment hides the next line", "CONST_Y = 2", "\tSPONGE_M=0.5*x",
+             "A =x= 3", "MOD_ALPHA_X", "STEADY_FILE =forcing.fld", "  SFD_CHI  =  0.25  "]
+    p = sessions.rect_session(str(tmp_path / "fs"), 2, 2, tokens={"N_P": 3}, fields="uvp", force=lines)
+    txt = open(p).read().replace("\t# a comment", "# a comment")   # a '#' in the first column
+    open(p, "w").write(txt)
+    S_ = O.read_session(p)
+    assert O.force_value(S_, "CONST_Y") is None
+    for tok in ("CONST_X", "CONST_Y", "SPONGE_M", "A", "MOD_ALPHA_X", "STEADY_FILE", "SFD_CHI", "CONST",
+                "NOT_THERE"):
+        buf = C.create_string_buffer(256)
+        found = C.c_int()
+        assert lib().stx_session_force_value(p.encode(), tok.encode(), buf, 256, C.byref(found)) == 0
+        want = O.force_value(S_, tok)
+        got = buf.value.decode() if found.value else None
+        assert got == want, (tok, got, want)
