@@ -20,6 +20,8 @@ CUDA library accelerates:
 * body forcing, SVV                            (dns/fieldforce.cpp, src/svv.cpp)
 * cylindrical coordinates with axis BCs        (src/element.cpp:1389-1399,
   src/field.cpp:1127-1227, src/bcmgr.cpp:153-180, src/edge.cpp:98-256)
+* computed outflow BCs                         (src/bcmgr.cpp:998-1633;
+  parity unpinned: the reference has no golden for them)
 
 The banded factorisation and solve call LAPACK dpbtrf/dpbtrs through scipy,
 the same routines the reference calls (src/matrix.cpp:252, src/field.cpp:693).
@@ -502,7 +504,7 @@ class Numbering:
             if (e, s) in M.mate:
                 continue
             bc = S.bcs.get(g, {}).get(fld)
-            if bc and axis_kind(bc[0], fld, mclass) == "D":
+            if bc and (axis_kind(bc[0], fld, mclass) == "D" or (bc[0] == "O" and fld == "p")):
                 for t in range(n):
                     ess[gid[e, (s * nm + t) % next_]] = True
         solve_nodes = np.where(~ess)[0]
@@ -804,7 +806,9 @@ class BoundarySystem:
             if bc is None:
                 raise ValueError(f"no BC for field {fld} in group {g}")
             kind = axis_kind(bc[0], fld, mclass)
-            self.edges.append((e, s, kind, "0.0" if bc[0] == "A" else bc[1]))
+            if kind == "O":      # computed outflow BCs (src/bcmgr.cpp:416-431)
+                kind = {"u": "OU", "v": "OV", "p": "OP"}.get(fld, "N")
+            self.edges.append((e, s, kind, "0.0" if bc[0] in "AO" else bc[1]))
         n = M.np
         self.area = []
         for (e, s, _, _) in self.edges:
@@ -848,7 +852,7 @@ class BoundarySystem:
         """Field::getEssential -> Essential::set (src/condition.cpp:80-101)."""
         nm = self.M.np - 1
         for b, (e, s, kind, _) in enumerate(self.edges):
-            if kind == "D":
+            if kind in ("D", "OP"):
                 g = [self.N.btog[e, (s * nm + t) % (4 * nm)] for t in range(nm + 1)]
                 tgt[g] = line[b]
 
@@ -856,7 +860,7 @@ class BoundarySystem:
         """Natural::sum (src/condition.cpp:192-219): <h, w> into tgt."""
         nm = self.M.np - 1
         for b, (e, s, kind, _) in enumerate(self.edges):
-            if kind in ("N", "H"):   # NaturalCBCp::sum (src/condition.cpp:470-495) is the same sum
+            if kind in ("N", "H", "OU", "OV"):   # the computed natural BCs sum the same way (src/condition.cpp:470-495, 573-660)
                 g = [self.N.btog[e, (s * nm + t) % (4 * nm)] for t in range(nm + 1)]
                 np.add.at(tgt, g, line[b] * self.area[b])
             elif kind == "M":
@@ -1513,6 +1517,14 @@ class DNS:
         shape = (P.nz, nedge, P.np)
         self.un = [np.zeros(shape) for _ in range(self.nord)]
         self.hop = [np.zeros(shape) for _ in range(self.nord)]
+        # computed outflow BCs (BCmgr::buildComputedBCs, src/bcmgr.cpp:937-996):
+        # edge velocities in physical space, div u and n.grad(u).n per level
+        self.oedges = [b for b, (_, _, kind, _) in enumerate(B.edges) if kind == "OP"]
+        self.ouvw = [[np.zeros(shape) for _ in range(3)] for _ in range(self.nord)]
+        self.odivu = [np.zeros(shape) for _ in range(self.nord)]
+        self.ogradu = [np.zeros(shape) for _ in range(self.nord)]
+        self.otoggle = False
+        self.ofbuf = np.zeros(shape)
 
     def _edges(self, f):
         """Values of plane data f [nel, np, np] along every boundary edge."""
@@ -1520,7 +1532,10 @@ class DNS:
 
     def _maintain_fourier(self, U, N):
         """BCmgr::maintainFourier (src/bcmgr.cpp:1036-1296), the terms the
-        high-order pressure BC uses: -d(u.n)/dt, n.N and -nu n.curlcurl u."""
+        high-order pressure BC uses: -d(u.n)/dt, n.N and -nu n.curlcurl u,
+        and the gradient terms of the computed outflow BCs."""
+        if self.oedges:
+            self._outflow_fourier(U)
         if not self.hedges:
             return
         P, M = self.P, self.P.M
@@ -1582,6 +1597,100 @@ class DNS:
             h[kr] += -nu * yr * self.ny
             h[ki] += -nu * yi * self.ny
 
+    # -- Computed outflow BCs (Dong, Karniadakis & Chryssostomidis 2014;
+    #    BCmgr::maintainFourier :1203-1293, evaluateCEBCp :1361-1465,
+    #    evaluateCNBCu :1516-1633)
+    def _outflow_fourier(self, U):
+        """nu div u and nu n.grad(u).n along every edge, newest level first."""
+        P, M = self.P, self.P.M
+        nu, beta = self.nu, P.S.tokens["BETA"]
+        self.odivu = [np.zeros_like(self.odivu[0])] + self.odivu[:-1]
+        self.ogradu = [np.zeros_like(self.ogradu[0])] + self.ogradu[:-1]
+        dv, gr = self.odivu[0], self.ogradu[0]
+        dy = self._edge_divy
+
+        def side_grad(f):
+            return self._edges(grad(M, f, 0)), self._edges(grad(M, f, 1))
+
+        # The reference's loop over the higher modes (src/bcmgr.cpp:1231-1238)
+        # never sets UxIm: its imaginary planes take du/dx from the plane the
+        # curl curl loop before it left there, the highest mode's imaginary
+        # plane; restated as computed.
+        last_im = 2 * (P.nz // 2 - 1) + 1
+
+        def planes(k, kz, sgn):
+            xr, yr = side_grad(U[0][last_im if k > 1 and k % 2 else k])
+            dv[k] += xr
+            gr[k] += (xr * self.nx + yr * self.ny) * self.nx
+            xr, yr = side_grad(U[1][k])
+            dv[k] += yr
+            gr[k] += (xr * self.nx + yr * self.ny) * self.ny
+            if M.cyl:
+                dv[k] += self._edges(U[1][k]) * dy
+            if kz is not None:
+                wz = self._edges(U[2][kz])
+                dv[k] += sgn * (wz * dy if M.cyl else wz)
+
+        planes(0, None, 0.0)
+        for m in range(1, P.nz // 2):
+            bk = m * beta
+            planes(2 * m, 2 * m + 1, -bk)
+            planes(2 * m + 1, 2 * m, bk)
+        dv *= nu
+        gr *= nu
+
+    def _outflow_p_lines(self, lines):
+        """Essential outflow pressure: extrapolated nu n.grad(u).n minus the
+        transform of KE* S0, KE* = |u*|^2 / 2 and S0 = (1 - tanh(u*.n /
+        U0Delta)) / 2 from the extrapolated edge velocities."""
+        if not self.oedges:
+            return lines
+        P, tok = self.P, self.P.S.tokens
+        Je = min(self.step, self.nord)
+        b = EX_COEFF[Je]
+        if self.otoggle:
+            u, v, w = (sum(b[q] * self.ouvw[q][c] for q in range(Je)) for c in range(3))
+            unp = self.nx * u + self.ny * v
+            ke = 0.5 * (w * w + (v * v + u * u))
+            with np.errstate(divide="ignore"):
+                iuzd = 1.0 / float(tok.get("U0Delta", 0.0))
+            s0 = 0.5 * (1.0 - np.tanh(unp * iuzd))
+            fb = ke * s0
+            if P.nz > 2:
+                fb = dft_forward(fb)
+            elif P.nz == 2:
+                fb = fb.copy()
+                fb[1] = 0.0
+            self.ofbuf = fb
+            self.otoggle = False
+        for k in range(P.nz):
+            for e in self.oedges:
+                if P.nz > 1 and k == 1:
+                    lines[k, e] = 0.0
+                    continue
+                lines[k, e] = sum(b[q] * self.ogradu[q][k, e] for q in range(Je)) - self.ofbuf[k, e]
+        return lines
+
+    def _outflow_u_lines(self, c, lines):
+        """Natural outflow velocity (u or v): (p - extrapolated nu div u +
+        KE* S0 / nu) times n_x or n_y, p the new pressure."""
+        if not self.oedges or c not in self.vel[:2]:
+            return lines
+        P = self.P
+        Je = min(self.step, self.nord)
+        b = EX_COEFF[Je]
+        pc = self.pname
+        nrm = self.nx if c == self.vel[0] else self.ny
+        for k in range(P.nz):
+            if P.nz > 1 and k == 1:
+                lines[k, self.oedges] = 0.0
+                continue
+            pe = self._edges(self.u[pc][k])
+            for e in self.oedges:
+                work = sum(b[q] * self.odivu[q][k, e] for q in range(Je))
+                lines[k, e] = ((1.0 / self.nu) * self.ofbuf[k, e] + (pe[e] - work)) * nrm[e]
+        return lines
+
     def _hopbc_lines(self, lines):
         """BCmgr::evaluateCNBCp (src/bcmgr.cpp:1299-1331): extrapolated
         dp/dn on the high-order pressure edges of the Fourier BC lines."""
@@ -1622,6 +1731,14 @@ class DNS:
         P = self.P
         U = [self.u[c].copy() for c in self.vel]
         Uphys = [self._inverse32(self.u[c]) for c in self.vel]
+        if self.oedges:                  # BCmgr::maintainPhysical (src/bcmgr.cpp:998-1034)
+            if self.dealias:
+                raise NotImplementedError("outflow BCs with DEALIAS")
+            lv = [np.stack([self._edges(Uphys[i][k]) for k in range(P.nz)]) for i in range(self.ncom)]
+            if self.ncom < 3:
+                lv.append(np.zeros_like(lv[0]))
+            self.ouvw = [lv] + self.ouvw[:-1]
+            self.otoggle = True
         if self.advection == 1:
             forms = ("conv",) if self.toggle else ("cons",)
         elif self.advection == 0:
@@ -1776,7 +1893,8 @@ class DNS:
             div /= self.dt
             pc = self.pname
             self.u[pc] = P.solve(pc, div, self.u[pc], self.psys,
-                                 self._hopbc_lines(P.bc_lines(pc, self.time)), tok["TOL_REL"])
+                                 self._outflow_p_lines(self._hopbc_lines(P.bc_lines(pc, self.time))),
+                                 tok["TOL_REL"])
             # -- project (dns/integrate.cpp:260-289)
             a = -1.0 / (self.dt * self.nu)
             b = 1.0 / self.nu
@@ -1795,7 +1913,7 @@ class DNS:
             # -- viscous substep (dns/integrate.cpp:177-193, 328-356); in
             #    cylindrical 3D v and w are solved coupled as v~, w~
             c3d = cyl and self.ncom == 3
-            lines = {c: P.bc_lines(c, self.time) for c in self.vel}
+            lines = {c: self._outflow_u_lines(c, P.bc_lines(c, self.time)) for c in self.vel}
             if c3d:
                 forc[1], forc[2] = self._couple(forc[1], forc[2], 1)
                 self.u[self.vel[1]], self.u[self.vel[2]] = self._couple(self.u[self.vel[1]],

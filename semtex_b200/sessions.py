@@ -12,14 +12,19 @@ import numpy as np
 
 def rect_session(path, nx, ny, x=(0.0, 1.0), y=(0.0, 1.0), tokens=None, fields="c",
                  periodic_x=False, periodic_y=False, bcs=None, user=None, xs=None, ys=None,
-                 wall_group="w", force=None):
+                 wall_group="w", force=None, side_groups=None, group_names=None):
     """Write a session file.
 
     bcs: {group_char: {field: "<D> value" | "<N> value" | "<H>"}} applied to
     every non-periodic boundary side (group `wall_group`), or None for no BCs.
     xs / ys: explicit node coordinates along x / y (length nx+1 / ny+1).
     force: lines of a <FORCE> section ("CONST_X = 0.1", ...), or None.
+    side_groups: {"bottom" | "top" | "left" | "right": group char} overriding
+    `wall_group` on those sides; group_names: {group char: descriptor}
+    ("wall" by default; "outflow" and "axis" are the reserved ones).
     """
+    side_groups = side_groups or {}
+    group_names = group_names or {}
     xs = np.linspace(x[0], x[1], nx + 1) if xs is None else np.asarray(xs, float)
     ys = np.linspace(y[0], y[1], ny + 1) if ys is None else np.asarray(ys, float)
     lines = []
@@ -41,7 +46,7 @@ def rect_session(path, nx, ny, x=(0.0, 1.0), y=(0.0, 1.0), tokens=None, fields="
     if bcs:
         lines.append(f"<GROUPS NUMBER={len(bcs)}>")
         for i, g in enumerate(bcs):
-            lines.append(f"\t{i + 1}\t{g}\twall")
+            lines.append(f"\t{i + 1}\t{g}\t{group_names.get(g, 'wall')}")
         lines.append("</GROUPS>\n")
         lines.append(f"<BCS NUMBER={len(bcs)}>")
         for i, (g, spec) in enumerate(bcs.items()):
@@ -77,14 +82,14 @@ def rect_session(path, nx, ny, x=(0.0, 1.0), y=(0.0, 1.0), tokens=None, fields="
         if periodic_y:
             surf.append((eid(i, 0), 1, f"<P>\t{eid(i, ny - 1)} 3\t</P>"))
         elif bcs:
-            surf.append((eid(i, 0), 1, f"<B>\t{wall_group}\t</B>"))
-            surf.append((eid(i, ny - 1), 3, f"<B>\t{wall_group}\t</B>"))
+            surf.append((eid(i, 0), 1, f"<B>\t{side_groups.get('bottom', wall_group)}\t</B>"))
+            surf.append((eid(i, ny - 1), 3, f"<B>\t{side_groups.get('top', wall_group)}\t</B>"))
     for j in range(ny):
         if periodic_x:
             surf.append((eid(0, j), 4, f"<P>\t{eid(nx - 1, j)} 2\t</P>"))
         elif bcs:
-            surf.append((eid(0, j), 4, f"<B>\t{wall_group}\t</B>"))
-            surf.append((eid(nx - 1, j), 2, f"<B>\t{wall_group}\t</B>"))
+            surf.append((eid(0, j), 4, f"<B>\t{side_groups.get('left', wall_group)}\t</B>"))
+            surf.append((eid(nx - 1, j), 2, f"<B>\t{side_groups.get('right', wall_group)}\t</B>"))
     lines.append(f"<SURFACES NUMBER={len(surf)}>")
     for k, (e, s, body) in enumerate(surf):
         lines.append(f"\t{k + 1}\t{e}\t{s}\t{body}")
