@@ -175,6 +175,10 @@ int stx_context_create(const char* session_path, const char* overrides, int devi
     ctx->S = read_session(session_path, overrides ? overrides : "");
     if (ctx->S.tokens.ivalue("CYLINDRICAL"))
       throw StxError(STX_EUNSUPPORTED, "cylindrical coordinates are not supported");
+    for (const auto& g : ctx->S.bcs)
+      for (const auto& f : g.second)
+        if (f.second.kind == 'O')
+          throw StxError(STX_EUNSUPPORTED, "computed outflow BCs <O> are not supported");
     ctx->M = build_mesh(ctx->S);
     ctx->device = device;
     cuda_check(cudaSetDevice(device), "cudaSetDevice");

@@ -718,12 +718,20 @@ Numbering build_numbering(const Session& S, const Mesh& M, char field, int rcm_r
         bc.kind = axis_kind('A', field, mclass);
         bc.expr = "0.0";
       }
-      if (bc.kind == 'D') {
+      if (bc.kind == 'O') {  // computed outflow (src/bcmgr.cpp:416-431): p essential, u v natural, w c zero natural
+        if (field != 'u' && field != 'v' && field != 'w' && field != 'p' && field != 'c')
+          throw std::runtime_error(std::string("field name '") + field + "' for outflow BC not in 'uvwpc'");
+        if (field == 'w' || field == 'c') {
+          bc.kind = 'N';
+          bc.expr = "0.0";
+        }
+      }
+      if (bc.kind == 'D' || (bc.kind == 'O' && field == 'p')) {
         for (int t = 0; t <= nm; ++t) ess[gid[e * next + (s * nm + t) % next]] = 1;
       } else if (bc.kind == 'H') {
         if (field != 'p')
           throw std::runtime_error(std::string("high-order BC <H> given for field ") + field + ", not pressure");
-      } else if (bc.kind != 'N' && bc.kind != 'M') {
+      } else if (bc.kind != 'N' && bc.kind != 'M' && bc.kind != 'O') {
         throw std::runtime_error(std::string("boundary condition kind <") + bc.kind +
                                  "> is not supported");
       }

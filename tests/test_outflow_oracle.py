@@ -45,3 +45,17 @@ def test_outflow_energy_term_acts(tmp_path):
     y = D.P.M.y[None]
     err = np.abs(D.physical()["u"] - (1 - y * y)).max()
     assert 1e-8 < err < 1e-4
+
+
+@pytest.mark.parametrize("nz", [1, 4])
+def test_outflow_numbering_host_matches_oracle(tmp_path, nz):
+    # the library's host numbering classifies outflow edges as the oracle
+    # does: pressure essential, u and v natural (computed), w natural zero
+    import semtex_b200 as S
+    p = _channel(str(tmp_path / "ch"), nz, 0.05)
+    P = O.Problem(O.read_session(p))
+    for c in P.S.fields:
+        n = S.numbering(p, c)
+        N = P.N[c]
+        assert (n["nglobal"], n["nsolve"], int(n["bmask"].sum())) == (N.nglobal, N.nsolve, int(N.bmask.sum())), c
+    assert S.numbering(p, "p")["nsolve"] < S.numbering(p, "p")["nglobal"]    # the exit pins the pressure
