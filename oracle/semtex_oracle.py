@@ -1414,6 +1414,8 @@ class DNS:
                 if uns and v is not None:
                     domega[i] = v
         F["coriolis"] = (2 if uns else 1) if on else 0
+        if F["coriolis"] and self.P.M.cyl:
+            raise NotImplementedError("Coriolis forcing in cylindrical coordinates")
         F["omega"], F["domega"] = omega, domega
         F["m2o"] = [-2.0 * float(tok.evaluate(o)) for o in omega]
         F["o"], F["mo"], F["dodt"] = [0.0] * 3, [0.0] * 3, [0.0] * 3
@@ -1484,12 +1486,16 @@ class DNS:
             q = F["qbar"][i]
             f = f - F["chi"] * Uphys[i] + F["chi"] * q
             F["qbar"][i] = q * (1.0 - F["rate"]) + F["rate"] * Uphys[i]
+        if M.cyl and i < 2:                              # radius-premultiplied x, r components (:100)
+            f = f * M.y[None]
         return n + f
 
     def _force_fourier(self, i, N):
         """FieldForce::addFourier (dns/fieldforce.cpp:110-137): ConstForce."""
         if self.force is not None and abs(self.force["const"][i]) > EPSDP:
-            N[0] += self.force["const"][i]
+            add = self.force["const"][i]
+            # radius-premultiplied x, r components (dns/fieldforce.cpp:131)
+            N[0] += add * self.P.M.y if (self.P.M.cyl and i < 2) else add
         return N
 
     # -- High-order pressure BCs (BCmgr::buildComputedBCs / maintainFourier /

@@ -167,3 +167,29 @@ def test_cylindrical_laplace_analytic(name):
     P, U = O.elliptic(os.path.join(SESSIONS, name))
     exact = P.evaluate(O.user_functions(P.S)["c"])
     assert np.abs(U - exact).max() < 1e-8 * np.abs(exact).max()
+
+
+@pytest.mark.parametrize("nz", [1, 4])
+def test_cylindrical_pipe_driven_by_constant_force(tmp_path, nz):
+    # pipe Poiseuille flow u = 1 - r^2 driven by CONST_X = 4 KINVIS (nu
+    # (1/r) d/dr (r du/dr) + f = 0) with the axis at r = 0: exact in the
+    # basis, kept to round-off (the x and r forcing premultiplied by r,
+    # dns/fieldforce.cpp:100, 131)
+    from semtex_b200 import sessions
+    fields = "uvwp" if nz > 1 else "uvp"
+    wall = {"u": "<D> 0", "v": "<D> 0", "p": "<H> 0"}
+    axis = {"u": "<A> 0", "v": "<A> 0", "p": "<A> 0"}
+    if nz > 1:
+        wall["w"] = "<D> 0"
+        axis["w"] = "<A> 0"
+    p = sessions.rect_session(str(tmp_path / "pipe"), 3, 2, x=(0.0, 2.0), y=(0.0, 1.0),
+                              tokens={"N_P": 6, "N_Z": nz, "CYLINDRICAL": 1, "N_TIME": 2, "D_T": 0.01,
+                                      "KINVIS": 0.1, "N_STEP": 10, "TOL_REL": 1e-14},
+                              fields=fields, periodic_x=True, bcs={"w": wall, "a": axis},
+                              side_groups={"bottom": "a", "top": "w"}, group_names={"a": "axis"},
+                              user=["u = 1-y*y", "v = 0", "p = 0"] + (["w = 0"] if nz > 1 else []),
+                              force=["CONST_X = 4*KINVIS"])
+    D = O.dns_session(p)
+    ph = D.physical()
+    assert np.abs(ph["u"] - (1 - D.P.M.y[None] ** 2)).max() < 1e-12
+    assert max(np.abs(ph[c]).max() for c in fields[1:-1]) < 1e-12
