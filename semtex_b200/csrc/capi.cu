@@ -60,6 +60,33 @@ int guarded(F&& f) {
   }
 }
 
+// An expression of x, y, z, t evaluated at many points: the compiled
+// program (equal to the interpreter bit for bit), or the interpreter for
+// the forms the compiler does not take (assignments inside the expression).
+struct PointEvaluator {
+  const stx::TokenTable& T;
+  std::string expr;
+  bool compiled = false;
+  stx::ExprProgram P;
+  std::map<std::string, double> vars;
+  PointEvaluator(const stx::TokenTable& tab, const std::string& e) : T(tab), expr(e) {
+    try {
+      P = T.compile(e);
+      compiled = true;
+    } catch (const std::exception&) {
+      compiled = false;
+    }
+  }
+  double operator()(double x, double y, double z, double t) {
+    if (compiled) return P.run(x, y, z, t);
+    vars["x"] = x;
+    vars["y"] = y;
+    vars["z"] = z;
+    vars["t"] = t;
+    return T.eval(expr, &vars);
+  }
+};
+
 }  // namespace
 
 namespace stx {
@@ -400,21 +427,16 @@ int stx_mesh_families(const stx_context* ctx, int* nfamily) {
   });
 }
 
+
 int stx_field_evaluate(const stx_context* ctx, const char* expr, double t, double* h_out) {
   return guarded([&] {
     if (!ctx || !expr || !h_out) throw StxError(STX_EINVAL, "null argument");
     const Mesh& M = ctx->M;
     const double dz = 2.0 * M_PI / ctx->S.tokens.value("BETA") / M.nz;
-    std::map<std::string, double> vars;
-    vars["t"] = t;
-    for (int k = 0; k < M.nz; ++k) {
-      vars["z"] = k * dz;
-      for (int i = 0; i < M.nplane; ++i) {
-        vars["x"] = M.x[i];
-        vars["y"] = M.y[i];
-        h_out[static_cast<size_t>(k) * M.nplane + i] = ctx->S.tokens.eval(expr, &vars);
-      }
-    }
+    PointEvaluator f(ctx->S.tokens, expr);
+    for (int k = 0; k < M.nz; ++k)
+      for (int i = 0; i < M.nplane; ++i)
+        h_out[static_cast<size_t>(k) * M.nplane + i] = f(M.x[i], M.y[i], k * dz, t);
   });
 }
 
@@ -491,19 +513,16 @@ int stx_field_bc_evaluate(stx_context* ctx, char field, double t) {
     if (F.nline == 0) return;
     const double dz = 2.0 * M_PI / ctx->S.tokens.value("BETA") / nz;
     std::vector<double> line(static_cast<size_t>(F.nline) * nz, 0.0);
-    std::map<std::string, double> vars;
-    vars["t"] = t;
+    std::map<std::string, PointEvaluator> evals;  // one per distinct expression
     for (int k = 0; k < nz; ++k) {
-      vars["z"] = k * dz;
       for (size_t b = 0; b < F.N.edges.size(); ++b) {
         const BoundaryEdge& E = F.N.edges[b];
-        for (int q = 0; q < np; ++q) {
-          vars["x"] = E.x[q];
-          vars["y"] = E.y[q];
-          // high-order pressure values are computed on the device each step
-          line[static_cast<size_t>(k) * F.nline + b * np + q] =
-              E.kind == 'H' || E.kind == 'M' ? 0.0 : ctx->S.tokens.eval(E.expr, &vars);
-        }
+        // high-order pressure values are computed on the device each step
+        if (E.kind == 'H' || E.kind == 'M') continue;
+        auto it = evals.find(E.expr);
+        if (it == evals.end()) it = evals.emplace(E.expr, PointEvaluator(ctx->S.tokens, E.expr)).first;
+        for (int q = 0; q < np; ++q)
+          line[static_cast<size_t>(k) * F.nline + b * np + q] = it->second(E.x[q], E.y[q], k * dz, t);
       }
     }
     host_dft_forward(line, nz, F.nline);
