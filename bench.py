@@ -245,7 +245,9 @@ def run_ours(args):
     f, nuniq = forcing_per_unique_node(x, y, ctx.nz, w["seed"])
     sysm = S.ModalMatrixSys(ctx, "c", w["lambda2"], w["beta"])
     setup_s = time.perf_counter() - t0
-    dof = nuniq * ctx.nz
+    # DOF over the solved planes (the Nyquist plane is never solved), counted
+    # as the reference arm counts them
+    dof = nuniq * (ctx.nz - 1 if ctx.nz > 1 else 1)
     F = ctx.new_field("f").load_physical(f).transform(S.FORWARD).zero_nyquist()
     U = ctx.new_field("c")
     stream = ctx.torch_stream()

@@ -156,7 +156,10 @@ int stx_modal_info(const stx_modal* sys, int mode, int* nsolve, int* nband);
  * (and holds the PCG initial guess on entry).  Uses the field's BC values
  * from the last stx_field_bc_evaluate.  For JACPCG, `tol_rel` and
  * `step_max` are TOL_REL / STEP_MAX; `iterations` (nz ints, may be NULL)
- * receives the per-plane iteration counts and the call synchronises. */
+ * receives the per-plane iteration counts and the call synchronises.
+ * A DIRECT solve is asynchronous and does not read the system's device
+ * status word: after synchronising, stx_modal_status tells whether every
+ * bounded wait of its kernels met its copy (else the solution is invalid). */
 int stx_field_solve(stx_modal* sys, const double* d_forcing, double* d_unknown, double tol_rel,
                     int step_max, int* iterations);
 
@@ -185,15 +188,21 @@ int stx_field_solve_profiled(stx_modal* sys, const double* d_forcing, double* d_
  * For callers that cannot let a library call cudaMalloc after start-up --
  * hosts whose device memory is owned by their own allocator, or loops that
  * cannot take the synchronisation an allocation may imply.  The solve
- * scratch lives in a file-scope device array of 2^20 doubles (8 MiB) that
- * every GPU loading the library holds until exit; problems needing more
- * (2 x padded nglobal x nz doubles) are rejected with STX_EINVAL.  The first
- * call on a device looks up the array's device address (cudaGetSymbolAddress)
- * and should come before any stream capture.  All calls on a device share
- * the one array and it keeps the last call's contents (the solve clears what
- * it accumulates into): calls that overlap on the GPU, e.g. issued on
- * different streams, race.  Inputs, outputs and BC values are as for
- * stx_field_solve. */
+ * scratch lives in a file-scope device array of 2^20 doubles (8 MiB);
+ * problems needing more are rejected with STX_EINVAL.  The need is
+ * 3 x nz x (nglobal rounded up to a multiple of 32) doubles for the two-level
+ * skeleton solve, 2 x that for the single banded factor (token
+ * STX_TWOLEVEL = 0).  CUDA loads the library's device code lazily, so the
+ * array is mapped on a device by the first call made there, which looks up
+ * its device address (cudaGetSymbolAddress): that first call may allocate
+ * and synchronise like any module load and must be made at start-up, before
+ * any stream capture; the device then holds the array until the process
+ * exits, and later calls allocate nothing.  All calls on a device share the
+ * one array and it keeps the last call's contents (the solve clears what it
+ * accumulates into): calls that overlap on the GPU, e.g. issued on different
+ * streams or contexts, race.  Asynchronous; the device status word is not
+ * read (query stx_modal_status after synchronising).  Inputs, outputs and BC
+ * values are as for stx_field_solve. */
 int stx_field_solve_noalloc(stx_modal* sys, const double* d_forcing, double* d_unknown);
 
 /* Synchronise and read the system's device status word: 0 when every

@@ -807,6 +807,8 @@ class BoundarySystem:
                 raise ValueError(f"no BC for field {fld} in group {g}")
             kind = axis_kind(bc[0], fld, mclass)
             if kind == "O":      # computed outflow BCs (src/bcmgr.cpp:416-431)
+                if "outflow" not in S.groups.get(g, ""):
+                    raise ValueError("type 'O' BC must belong to group \"outflow\"")
                 kind = {"u": "OU", "v": "OV", "p": "OP"}.get(fld, "N")
             self.edges.append((e, s, kind, "0.0" if bc[0] in "AO" else bc[1]))
         n = M.np

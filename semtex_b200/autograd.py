@@ -81,9 +81,11 @@ def _helmholtz_solve():
         def backward(actx, g):
             system = actx.system
             w = _work(system)
-            if w.offset is None:  # b = solve(0): the BC part of the affine map
-                w.offset = solve_physical(system, torch.zeros_like(g))
-            x = solve_physical(system, g / w.q4) - w.offset
+            # b = solve(0), the BC part of the affine map, taken afresh each
+            # time: stx_field_bc_evaluate may have changed the BC values
+            # (time-dependent BCs) since the forward call
+            offset = solve_physical(system, torch.zeros_like(g))
+            x = solve_physical(system, g / w.q4) - offset
             return w.q4 * x, None
 
     return HelmholtzSolve

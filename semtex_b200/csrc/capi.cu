@@ -22,6 +22,7 @@
 #include "host/mesh.hpp"
 #include "host/session.hpp"
 #include "kernels/helmholtz.cuh"
+#include "kernels/ptx.cuh"
 #include "kernels/element.cuh"
 #include "kernels/symtile.hpp"
 #include "kernels/twolevel.cuh"
@@ -606,6 +607,15 @@ int stx_modal_create(stx_context* ctx, char field, double lambda2, double beta, 
       d.nmodes = num_modes;
       d.method = method;
       d.nfamily = M.nfamily;
+      // bound of the kernels' bounded waits (token STX_WAIT_NS, default 2 s;
+      // 0: one non-blocking probe, which a copy issued just before misses --
+      // the error path's tests use it)
+      d.wait_ns = kWaitNs;
+      if (ctx->S.tokens.has("STX_WAIT_NS")) {
+        const double w = ctx->S.tokens.value("STX_WAIT_NS");
+        if (!(w >= 0.0)) throw StxError(STX_EINVAL, "STX_WAIT_NS must be at least 0");
+        d.wait_ns = static_cast<unsigned long long>(std::min(w, 6.0e10));
+      }
       d.nband = N.nband;
       std::vector<double> lam(num_modes), bk2(num_modes);
       std::vector<int> ns(num_modes);

@@ -719,6 +719,9 @@ Numbering build_numbering(const Session& S, const Mesh& M, char field, int rcm_r
         bc.expr = "0.0";
       }
       if (bc.kind == 'O') {  // computed outflow (src/bcmgr.cpp:416-431): p essential, u v natural, w c zero natural
+        auto gd = S.groups.find(g);
+        if (gd == S.groups.end() || gd->second.find("outflow") == std::string::npos)
+          throw std::runtime_error("type 'O' BC must belong to group \"outflow\"");
         if (field != 'u' && field != 'v' && field != 'w' && field != 'p' && field != 'c')
           throw std::runtime_error(std::string("field name '") + field + "' for outflow BC not in 'uvwpc'");
         if (field == 'w' || field == 'c') {

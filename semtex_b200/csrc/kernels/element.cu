@@ -92,10 +92,11 @@ __device__ __forceinline__ void stage_rows(uint64_t* bar, double* sA, const doub
   }
 }
 
-// All threads: bounded wait for the operator rows; false (uniformly) when the
-// bound expired, after the error is recorded and a second bounded wait.
-__device__ __forceinline__ bool rows_ready(uint64_t* bar, int* status) {
-  const bool ok = __syncthreads_and(mbar_wait(bar, 0));
+// All threads: wait, bounded by `limit_ns`, for the operator rows; false
+// (uniformly) when the bound expired, after the error is recorded and a
+// second wait (bounded by the default 2 s) for the copy still in flight.
+__device__ __forceinline__ bool rows_ready(uint64_t* bar, int* status, unsigned long long limit_ns) {
+  const bool ok = __syncthreads_and(mbar_wait(bar, 0, limit_ns));
   if (!ok) {
     if (threadIdx.x == 0 && status) atomicExch(status, 3);
     mbar_wait(bar, 0);
@@ -335,7 +336,7 @@ __global__ void __launch_bounds__(32 * kMaxWarps, 1)
     lift_columns<false>(g, N, G, gstride, S.lambda2[m] + S.betak2[m], X, cnt, m, ncol, sB, ldb, sQ, sD, sFlag, 0);
     __syncthreads();
   }
-  if (!rows_ready(bar, S.status)) return;
+  if (!rows_ready(bar, S.status, S.wait_ns)) return;
   const int wp = threadIdx.x >> 5, ln = threadIdx.x & 31;
   const int ntile = (ncol + 7) / 8, strips = (rows + 7) / 8;
   const int ncg = (ntile + kUnitTiles - 1) / kUnitTiles;
@@ -403,7 +404,7 @@ __global__ void __launch_bounds__(32 * kMaxWarps, 1)
     lift_columns<true>(g, N, G, gstride, S.lambda2[m] + S.betak2[m], X, cnt, m, ncol, sB, ldb, sQ, sD, sFlag, next);
     __syncthreads();
   }
-  if (!rows_ready(bar, S.status)) return;
+  if (!rows_ready(bar, S.status, S.wait_ns)) return;
   const int wp = threadIdx.x >> 5, ln = threadIdx.x & 31, nwp = blockDim.x >> 5;
   const int ntile = (ncol + 7) / 8, strips = (rows + 7) / 8;
   const int ncg = (ntile + kUnitTiles - 1) / kUnitTiles;

@@ -37,10 +37,26 @@ __device__ __forceinline__ unsigned long long global_ns() {
   return t;
 }
 
-// Bounded wait (about 2 s of wall time) for phase `parity` of an mbarrier;
-// false if the bound expired.
-__device__ __forceinline__ bool mbar_wait(uint64_t* bar, unsigned parity) {
+// Default bound of an mbarrier wait, and of every wait that drains copies
+// still in flight after an expired one: 2 s of wall time.
+constexpr unsigned long long kWaitNs = 2000000000ull;
+
+// Bounded wait (`limit_ns` of wall time) for phase `parity` of an mbarrier;
+// false if the bound expired.  limit_ns = 0 probes once without blocking
+// (the error path's tests use it: a copy issued just before has not landed).
+__device__ __forceinline__ bool mbar_wait(uint64_t* bar, unsigned parity,
+                                          unsigned long long limit_ns = kWaitNs) {
   const uint32_t a = smem_u32(bar);
+  if (limit_ns == 0) {
+    uint32_t done;
+    asm volatile(
+        "{\n .reg .pred p;\n mbarrier.test_wait.parity.shared::cta.b64 p, [%1], %2;\n"
+        " selp.u32 %0, 1, 0, p;\n}\n"
+        : "=r"(done)
+        : "r"(a), "r"(parity)
+        : "memory");
+    return done != 0;
+  }
   const unsigned long long t0 = global_ns();
   for (;;) {
     uint32_t done;
@@ -51,7 +67,7 @@ __device__ __forceinline__ bool mbar_wait(uint64_t* bar, unsigned parity) {
         : "r"(a), "r"(parity)
         : "memory");
     if (done) return true;
-    if (global_ns() - t0 > 2000000000ull) return false;
+    if (global_ns() - t0 > limit_ns) return false;
   }
 }
 

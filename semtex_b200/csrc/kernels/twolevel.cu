@@ -97,7 +97,7 @@ template <class T, int NF>
 __global__ void __launch_bounds__(32 * kSymWarps<NF>)
     k_psymv(const T* __restrict__ pack, const SymProblem* __restrict__ probs, const SymWarp* __restrict__ warps,
             int nwarps, const double* __restrict__ X, double* __restrict__ Y, int rstride, size_t fstride, int nz,
-            int* status) {
+            int* status, unsigned long long wait_ns) {
   extern __shared__ __align__(16) unsigned char sraw[];
   const int wp = threadIdx.x >> 5, ln = threadIdx.x & 31;
   const int gw = blockIdx.x * kSymWarps<NF> + wp;
@@ -165,7 +165,7 @@ __global__ void __launch_bounds__(32 * kSymWarps<NF>)
   int done = 0;
   for (; done < W.count; ++done) {
     const int s = done % kSymStages;
-    if (!__all_sync(0xffffffffu, mbar_wait(&sm.bar[s], (done / kSymStages) & 1))) {
+    if (!__all_sync(0xffffffffu, mbar_wait(&sm.bar[s], (done / kSymStages) & 1, wait_ns))) {
       if (ln == 0 && status) atomicExch(status, 4);
       break;
     }
@@ -254,7 +254,7 @@ __global__ void __launch_bounds__(32 * kSymWarps<NF>)
     if (issued < W.count) issue(s);  // the buffer's reads are complete (syncwarp)
     cc.next(probs, done + 1 < W.count);
   }
-  // leave no copy in flight (only after an expired wait)
+  // leave no copy in flight (only after an expired wait; default bound)
   for (int k = done; k < issued; ++k) mbar_wait(&sm.bar[k % kSymStages], (k / kSymStages) & 1);
 }
 
@@ -267,10 +267,11 @@ void configure_psymv() {
 
 template <class T, int NF>
 void launch_psymv_as(const T* pack, const SymProblem* probs, const SymWarp* warps, int nwarps, const double* X,
-                     double* Y, int rstride, size_t fstride, int nz, int* status, cudaStream_t st) {
+                     double* Y, int rstride, size_t fstride, int nz, int* status, unsigned long long wait_ns,
+                     cudaStream_t st) {
   const int blocks = (nwarps + kSymWarps<NF> - 1) / kSymWarps<NF>;
   k_psymv<T, NF><<<blocks, 32 * kSymWarps<NF>, sym_smem<NF>(), st>>>(pack, probs, warps, nwarps, X, Y, rstride,
-                                                                     fstride, nz, status);
+                                                                     fstride, nz, status, wait_ns);
 }
 
 cudaError_t launch_psymv(const DevModal& S, const SymProblem* probs, const SymWarp* warps, int nwarps,
@@ -279,13 +280,13 @@ cudaError_t launch_psymv(const DevModal& S, const SymProblem* probs, const SymWa
   if (nwarps <= 0) return cudaSuccess;
   configure_psymv();
   if (fp32)
-    launch_psymv_as<float, 1>(S.l2_pack32, probs, warps, nwarps, X, Y, rstride, 0, nz, S.status, st);
+    launch_psymv_as<float, 1>(S.l2_pack32, probs, warps, nwarps, X, Y, rstride, 0, nz, S.status, S.wait_ns, st);
   else if (nf == 3)
-    launch_psymv_as<double, 3>(S.l2_pack, probs, warps, nwarps, X, Y, rstride, fstride, nz, S.status, st);
+    launch_psymv_as<double, 3>(S.l2_pack, probs, warps, nwarps, X, Y, rstride, fstride, nz, S.status, S.wait_ns, st);
   else if (nf == 2)
-    launch_psymv_as<double, 2>(S.l2_pack, probs, warps, nwarps, X, Y, rstride, fstride, nz, S.status, st);
+    launch_psymv_as<double, 2>(S.l2_pack, probs, warps, nwarps, X, Y, rstride, fstride, nz, S.status, S.wait_ns, st);
   else
-    launch_psymv_as<double, 1>(S.l2_pack, probs, warps, nwarps, X, Y, rstride, 0, nz, S.status, st);
+    launch_psymv_as<double, 1>(S.l2_pack, probs, warps, nwarps, X, Y, rstride, 0, nz, S.status, S.wait_ns, st);
   return cudaGetLastError();
 }
 

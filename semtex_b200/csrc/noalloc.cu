@@ -20,8 +20,10 @@
 
 namespace {
 
-// Upper bound of the scratch a call may use: 2^20 doubles (8 MiB).  The array
-// lives in every GPU that loads this library until the process exits.
+// Upper bound of the scratch a call may use: 2^20 doubles (8 MiB).  CUDA loads
+// this file's device code lazily, so a GPU maps the array at the first call
+// made on it (which may allocate and synchronise like any module load: make
+// it at start-up) and holds it until the process exits.
 constexpr size_t kNoAllocScratchDoubles = size_t(1) << 20;
 
 static __device__ __align__(256) double g_noalloc_scratch[kNoAllocScratchDoubles];

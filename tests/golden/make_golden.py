@@ -5,7 +5,7 @@ Copies (verbatim) the reference's regression goldens `regress/*.ok` and
 (test/testregress:14-30) -- into regress_ok.json, and copies the session
 files those tests and the elliptic suite run (mesh/<name>) into sessions/.
 
-Usage:  python tests/golden/make_golden.py [/path/to/reference]
+Usage:  python tests/golden/make_golden.py /path/to/reference
 """
 
 from __future__ import annotations
@@ -44,4 +44,6 @@ def main(ref):
 
 
 if __name__ == "__main__":
-    main(sys.argv[1] if len(sys.argv) > 1 else "/root/reference")
+    if len(sys.argv) != 2:
+        sys.exit("usage: make_golden.py /path/to/reference")
+    main(sys.argv[1])

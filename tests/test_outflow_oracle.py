@@ -59,3 +59,21 @@ def test_outflow_numbering_host_matches_oracle(tmp_path, nz):
         N = P.N[c]
         assert (n["nglobal"], n["nsolve"], int(n["bmask"].sum())) == (N.nglobal, N.nsolve, int(N.bmask.sum())), c
     assert S.numbering(p, "p")["nsolve"] < S.numbering(p, "p")["nglobal"]    # the exit pins the pressure
+
+
+def test_outflow_needs_outflow_group(tmp_path):
+    # BCmgr rejects a type 'O' BC whose group is not described as "outflow"
+    # (src/bcmgr.cpp:418-419); the oracle and the host numbering do the same
+    import semtex_b200 as S
+    fields = "uvp"
+    bcs = {"v": {"u": "<D> 1-y*y", "v": "<D> 0", "p": "<H> 0"},
+           "w": {"u": "<D> 0", "v": "<D> 0", "p": "<H> 0"},
+           "o": {"u": "<O> 0", "v": "<O> 0", "p": "<O> 0"}}
+    p = sessions.rect_session(str(tmp_path / "bad"), 4, 2, x=(0.0, 4.0), y=(-1.0, 1.0),
+                              tokens={"N_P": 5, "N_Z": 1, "N_TIME": 2, "D_T": 0.01, "KINVIS": 0.1},
+                              fields=fields, bcs=bcs, side_groups={"left": "v", "right": "o"},
+                              group_names={"o": "exit"}, user=["u = 1-y*y", "v = 0", "p = 0"])
+    with pytest.raises(ValueError, match="outflow"):
+        O.Problem(O.read_session(p))
+    with pytest.raises(RuntimeError, match="outflow"):
+        S.numbering(p, "p")
