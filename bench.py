@@ -126,6 +126,37 @@ def measured_peaks():
     return 6650.0, "fallback"
 
 
+def c2_parity(ctx, U):
+    """Relative error of the timed solution (Fourier space, device) against
+    the oracle's checksums of the same workload (tests/golden/baseline/c2.npz:
+    norm, seeded Gaussian projections and sampled values of the oracle's
+    physical-space solution), or None when the fixture is absent."""
+    import semtex_b200 as S
+    gold = os.path.join(ROOT, "tests", "golden")
+    if not os.path.exists(os.path.join(gold, "baseline", "c2.npz")):
+        return None
+    sys.path.insert(0, gold)
+    import make_baseline_fixtures as FX
+    W = ctx.new_field("parity")
+    ctx.sync()
+    W.data.copy_(U.data)
+    import torch
+    torch.cuda.synchronize()
+    W.transform(S.INVERSE)
+    e = FX.errors(W.to_numpy(), FX.load("c2")["c"])
+    return {"vs": "oracle checksums of the same forcing (norm, 4 Gaussian projections, 256 samples)",
+            "rel_err": max(e.values()), "detail": e}
+
+
+def load_dns_traffic(workload):
+    """DRAM bytes (read + write) of one steady DNS step, from the committed
+    ncu summary of the same workload (profiles/dns_traffic.json), or None."""
+    p = os.path.join(ROOT, "profiles", "dns_traffic.json")
+    if os.path.exists(p):
+        return json.load(open(p)).get("dram_bytes_per_step", {}).get(workload)
+    return None
+
+
 def load_profile_traffic(phase):
     """DRAM bytes (read + write) of one launch of a solve phase, from the
     committed ncu summary of the same workload (profiles/c2_solve_traffic.json)."""
@@ -165,6 +196,57 @@ def _oracle_plane_worker(args):
                 O.solve_plane(P.M, P.N[c], P.B[c], systems[k], F[k], np.zeros_like(F[k]), bl[k])
             out.append(time.perf_counter() - t0)
     return out
+
+
+def dns_session(d, workload):
+    """The DNS workloads' sessions (the builders and seeds of the tests)."""
+    from semtex_b200 import sessions
+    if workload in ("c3", "c3d"):
+        return sessions.taylor_green_session(os.path.join(d, workload), 24, 9, 96, re=1600.0, dt=1e-3, nstep=200,
+                                             extra={"DEALIAS": 1} if workload == "c3d" else None)
+    return sessions.channel_session(os.path.join(d, "c5"), 16, 8, 9, 32, re=500.0, dt=5e-3, nstep=100)
+
+
+def oracle_dns_sample(workload, modes, nsteps):
+    """CPU baseline of a DNS workload: the oracle restatement of integrate()
+    on one core, at full size, with the Helmholtz solves of the Fourier modes
+    `modes` only (None: every mode).  Matrix setup is excluded, and the
+    N_TIME - 1 start-up steps (whose Jacobi-PCG solves differ from a steady
+    step's) are skipped: the run starts at full order from the initial state,
+    with zero history, which changes the values of a steady step but not its
+    work.  `nsteps` steady steps are timed.  The solve time of the sample is
+    scaled to all solved planes; the rest of the step (nonlinear terms,
+    transforms, waveProp, setPForce, project) runs in full.
+    Returns (seconds per step, description)."""
+    from threadpoolctl import threadpool_limits
+    sys.path.insert(0, os.path.join(ROOT, "oracle"))
+    import semtex_oracle as O
+    from semtex_b200 import sessions
+    with tempfile.TemporaryDirectory() as d:
+        p = dns_session(d, workload)
+        S = O.read_session(p)
+        P = O.Problem(S)
+        if workload == "c5":
+            ic = sessions.channel_initial(P.M.x, P.M.y, np.arange(P.nz) * 2 * np.pi / P.nz)
+        else:
+            funcs = O.user_functions(S)
+            ic = {c: P.evaluate(funcs[c], 0.0) for c in S.fields if c in funcs}
+        D = O.DNS(P, ic, modes=modes)
+        D.step = D.nord - 1
+        with threadpool_limits(1):
+            P.solve_seconds = 0.0
+            t0 = time.perf_counter()
+            D.advance(nsteps)
+            total = time.perf_counter() - t0
+        solved = P.nz - 1 if P.nz > 1 else 1
+        sampled = solved if modes is None else sum(1 if (m == 0 or P.nz == 1) else 2 for m in modes)
+        per_step = ((total - P.solve_seconds) + P.solve_seconds * solved / sampled) / nsteps
+    what = (f"{nsteps} steady steps of the oracle restatement at full size, 1 thread, setup excluded, "
+            "started at full order")
+    if modes is not None:
+        what += (f"; Helmholtz solves of modes {list(modes)} only ({sampled} of {solved} planes per field), "
+                 f"their time scaled to all planes")
+    return per_step, what
 
 
 def cpu_sample(session, planes, workers, seed, nrep=1):
@@ -288,6 +370,7 @@ def run_ours(args):
         phases.append(solve_profiled())
     torch.cuda.synchronize()
     t_total = max_over_ranks(t_total, ws, f"cuda:{local}")
+    parity = c2_parity(ctx, U)
     if ws > 1:
         torch.distributed.barrier()
     # -- end to end through the host-buffer call
@@ -349,13 +432,14 @@ def run_ours(args):
         "sequential_ms": float(sum(phase_ms)),
         "setup_s": setup_s, "families": ctx.families(),
         "gpu_launches": int(launches.value) * args.steps,
-        "clocks": clocks, "cpu_baseline": cpu,
+        "clocks": clocks, "cpu_baseline": cpu, "parity": parity,
     }
     if args.dns_steps > 0 and ws == 1:
         line["mixed"] = run_mixed(ctx, sysm, F, args, flush, stream, dof)
-        line["dns"] = run_dns(args.dns_steps, 3, local, "c3")
-        line["dns_c3_dealiased"] = run_dns(args.dns_steps, 3, local, "c3d")
-        line["dns_c5"] = run_dns(args.dns_steps, 3, local, "c5")
+        cb = not args.no_cpu_baseline
+        line["dns"] = run_dns(args.dns_steps, 3, local, "c3", cb)
+        line["dns_c3_dealiased"] = run_dns(args.dns_steps, 3, local, "c3d", cb)
+        line["dns_c5"] = run_dns(args.dns_steps, 3, local, "c5", cb)
         line["batch_c4"] = run_batch(args.dns_steps, 3, local)
     print(json.dumps(line))
     if ws > 1:
@@ -413,7 +497,7 @@ DNS_WORKLOADS = {
 }
 
 
-def run_dns(steps, warmup=3, local=0, workload="c3"):
+def run_dns(steps, warmup=3, local=0, workload="c3", cpu_baseline=False):
     """Secondary measurement: DNS steps/s, plain FP64 direct solves,
     alternating skew-symmetric advection.  c3: 3D Taylor--Green (24x24
     periodic quads, N_P=9, N_Z=96, Re=1600, D_T=1e-3, N_TIME=3).  c5: plane
@@ -427,11 +511,7 @@ def run_dns(steps, warmup=3, local=0, workload="c3"):
     import semtex_b200 as S
     from semtex_b200 import sessions
     d = tempfile.mkdtemp()
-    if workload in ("c3", "c3d"):
-        p = sessions.taylor_green_session(os.path.join(d, "c3"), 24, 9, 96, re=1600.0, dt=1e-3, nstep=200,
-                                          extra={"DEALIAS": 1} if workload == "c3d" else None)
-    else:
-        p = sessions.channel_session(os.path.join(d, "c5"), 16, 8, 9, 32, re=500.0, dt=5e-3, nstep=100)
+    p = dns_session(d, workload)
     t0 = time.perf_counter()
     ctx = S.Context(p, device=local)
     D = S.DNS(ctx, 1)
@@ -458,11 +538,39 @@ def run_dns(steps, warmup=3, local=0, workload="c3"):
     e1.synchronize()
     ms = e0.elapsed_time(e1) / steps
     period, glaunch = D.graph_info()
+    # roofline: algorithmic bytes of one steady step over its device time.
+    # Field passes (F = one field, nz planes of plane_size doubles):
+    # nonlinear 2 ncom, waveProp (2 N_TIME + 1) ncom, setPForce ndim + 1,
+    # project 2 ncom + 1; plus the solves: the pressure system's
+    # stx_modal_bytes, the velocity system's once (its matrices are read once
+    # for all components) plus 3 F per further component (forcing read by the
+    # condensation and the recovery, solution written)
+    ncom = len(ctx.fields) - 1
+    ndim = 3 if ctx.nz > 1 else 2
+    nord = int(ctx.token("N_TIME"))
+    F = 8.0 * ctx.plane_size * ctx.nz
+    passes = 2 * ncom + (2 * nord + 1) * ncom + (ndim + 1) + (2 * ncom + 1)
+    vb, pb = sum(D.system_bytes(ctx.fields[0])), sum(D.system_bytes(ctx.fields[ncom]))
+    step_bytes = passes * F + pb + vb + (ncom - 1) * 3 * F
+    peak, kind = measured_peaks()
+    achieved = step_bytes / (ms / 1e3) / 1e9
+    traffic = load_dns_traffic(workload)
     out = {"metric": "DNS steps/s", "value": 1e3 / ms, "ms_per_step": ms, "steps": steps,
            "workload": DNS_WORKLOADS[workload], "setup_s": setup,
-           "graph": {"cycle_steps": period, "launches": glaunch}}
+           "graph": {"cycle_steps": period, "launches": glaunch},
+           "roofline": {"bound": "hbm", "kernel": "whole step", "achieved": achieved, "peak": peak,
+                        "unit": "GB/s", "frac": achieved / peak, "peak_kind": kind,
+                        "algorithmic_bytes_per_step": step_bytes,
+                        "model": {"field_bytes": F, "field_passes": passes, "pressure_solve_bytes": pb,
+                                  "velocity_solve_bytes": vb + (ncom - 1) * 3 * F},
+                        "traffic": traffic}}
     D.close()
     ctx.close()
+    if cpu_baseline:
+        modes = (1, 15) if workload == "c5" else (1, 47)
+        sec, what = oracle_dns_sample(workload, modes, 2)
+        out["cpu_baseline"] = {"value": 1.0 / sec, "unit": "steps/s", "cores": 1, "kind": "port",
+                               "sample": what}
     return out
 
 
@@ -570,7 +678,7 @@ def main():
         import torch
         torch.cuda.set_device(0)
         print(json.dumps(run_dns(max(1, args.dns_steps), args.warmup, 0,
-                                 "c3" if args.workload == "dns" else "c5")))
+                                 "c3" if args.workload == "dns" else "c5", not args.no_cpu_baseline)))
     elif args.workload == "batch_c4":
         import torch
         torch.cuda.set_device(0)

@@ -290,6 +290,11 @@ int stx_dns_state(const stx_dns* dns, int* step, double* time);
 int stx_dns_modal_energy(stx_dns* dns, double* h_ek);
 int stx_dns_divergence_energy(stx_dns* dns, double* value);
 int stx_dns_cfl(stx_dns* dns, double* inv_dt);
+/* The ModalMatrixSys a steady step solves `field` with: the viscous system
+ * of a velocity component (dns/integrate.cpp:186-193), the pressure system
+ * (:244-252); owned by the DNS (not to be destroyed).  For stx_modal_bytes
+ * and stx_modal_status. */
+int stx_dns_system(stx_dns* dns, char field, stx_modal** sys);
 /* Device pointer of a field's Fourier-space storage (nz x plane_size). */
 int stx_dns_field_ptr(stx_dns* dns, char field, double** d_ptr);
 

@@ -42,6 +42,7 @@ from __future__ import annotations
 import math
 import os
 import re
+import time
 from dataclasses import dataclass, field as dfield
 
 import numpy as np
@@ -1158,6 +1159,7 @@ class Problem:
                 else:
                     self.NB[(c, mc)] = (self.N[c], self.B[c])
         self.dz = 2 * math.pi / tok["BETA"] / self.nz
+        self.solve_seconds = 0.0   # time spent in solve(), for the CPU timings
 
     def nb(self, c, mode):
         """(Numbering, BoundarySystem) of field c for Fourier mode `mode`."""
@@ -1179,8 +1181,9 @@ class Problem:
                          for k in range(self.nz)])
         return dft_forward(phys)
 
-    def modal_systems(self, c, lambda2, method="DIRECT", cache=None):
-        """ModalMatrixSys (src/matrix.cpp:33-105): one MatrixSys per mode."""
+    def modal_systems(self, c, lambda2, method="DIRECT", cache=None, modes=None):
+        """ModalMatrixSys (src/matrix.cpp:33-105): one MatrixSys per mode
+        (None for a mode outside `modes`, when given: a timing sample)."""
         tok = self.S.tokens
         beta = tok["BETA"]
         nmodes = (self.nz + 1) // 2
@@ -1189,6 +1192,9 @@ class Problem:
               if lambda2 > EPSDP else np.ones(nmodes))
         out = []
         for m in range(nmodes):
+            if modes is not None and m not in modes:
+                out.append(None)
+                continue
             bk2 = mode_constant(self.M, c, m, beta) ** 2 * sz[m]
             key = (c, round(lambda2, 14), round(bk2, 14), method, min(m, 2) if self.axis else 0)
             if cache is not None and key in cache:
@@ -1204,12 +1210,14 @@ class Problem:
     def solve(self, c, forcing, unknown, systems, bclines, tol_rel=1e-8, step_max=500):
         """Field::solve over all planes; forcing in Fourier space."""
         out = unknown.copy()
+        t0 = time.perf_counter()
         for k in range(self.nz):
-            if k == 1:
+            if k == 1 or systems[k >> 1] is None:
                 continue
             N, B = self.nb(c, k >> 1)
             out[k] = solve_plane(self.M, N, B, systems[k >> 1],
                                  forcing[k], unknown[k], bclines[k], tol_rel, step_max)
+        self.solve_seconds += time.perf_counter() - t0
         return out
 
 
@@ -1300,7 +1308,7 @@ class DNS:
     """
 
     def __init__(self, P: Problem, ic: dict | None = None, t0: float = 0.0,
-                 dealias: bool | None = None, advection: int = 1):
+                 dealias: bool | None = None, advection: int = 1, modes=None):
         if dealias is None:   # the session token (the reference's build-time DEALIAS)
             dealias = float(P.S.tokens.get("DEALIAS", 0)) > 0
         self.dealias = bool(dealias) and P.nz > 2
@@ -1334,8 +1342,10 @@ class DNS:
         lam = SS_COEFF[self.nord][0] / (self.dt * self.nu)
         # preSolve (dns/integrate.cpp:292-325): ITERATIVE selects Jacobi-PCG velocity systems
         vmethod = "JACPCG" if tok.ivalue("ITERATIVE") else "DIRECT"
-        self.vsys = {c: P.modal_systems(c, lam, vmethod, self.cache) for c in self.vel}
-        self.psys = P.modal_systems(self.pname, 0.0, "DIRECT", self.cache)
+        # modes: build and solve only these Fourier modes (a CPU timing sample)
+        self.modes = modes
+        self.vsys = {c: P.modal_systems(c, lam, vmethod, self.cache, modes) for c in self.vel}
+        self.psys = P.modal_systems(self.pname, 0.0, "DIRECT", self.cache, modes)
         self._hopbc_setup()
         self._force_setup()
 
@@ -1930,7 +1940,7 @@ class DNS:
             for i, c in enumerate(self.vel):
                 if self.step < self.nord:
                     lam = SS_COEFF[Je][0] / (self.dt * self.nu)
-                    sysi = P.modal_systems(c, lam, "JACPCG", self.cache)
+                    sysi = P.modal_systems(c, lam, "JACPCG", self.cache, self.modes)
                 else:
                     sysi = self.vsys[c]
                 self.u[c] = P.solve(c, forc[i], self.u[c], sysi,

@@ -393,6 +393,15 @@ class DNS:
             check(lib().stx_dns_destroy(self._h))
         self._h = C.c_void_p()
 
+    def system_bytes(self, field: str):
+        """Algorithmic bytes of one direct solve of `field`'s steady-step
+        system, per phase (stx_dns_system + stx_modal_bytes)."""
+        h = C.c_void_p()
+        check(lib().stx_dns_system(self._h, field.encode(), C.byref(h)))
+        b = (C.c_double * 4)()
+        check(lib().stx_modal_bytes(h, b))
+        return list(b)
+
     def __del__(self):
         try:
             self.close()

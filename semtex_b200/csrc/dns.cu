@@ -1239,6 +1239,16 @@ int stx_dns_graph_info(const stx_dns* d, int* period, long long* launches) {
   });
 }
 
+int stx_dns_system(stx_dns* d, char field, stx_modal** sys) {
+  return dns_guarded([&] {
+    if (!d || !sys) throw DnsError(STX_EINVAL, "null argument");
+    const size_t idx = d->names.find(field);
+    if (idx == std::string::npos) throw DnsError(STX_EINVAL, std::string("no field ") + field);
+    if (static_cast<int>(idx) == d->ncom) *sys = d->psys;
+    else *sys = d->vsys.at(idx);
+  });
+}
+
 int stx_dns_field_ptr(stx_dns* d, char field, double** d_ptr) {
   return dns_guarded([&] {
     if (!d || !d_ptr) throw DnsError(STX_EINVAL, "null argument");
