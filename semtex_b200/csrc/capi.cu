@@ -23,6 +23,8 @@
 #include "host/session.hpp"
 #include "kernels/helmholtz.cuh"
 #include "kernels/ptx.cuh"
+#include "kernels/sweep.cuh"
+#include "l2setup.hpp"
 #include "kernels/element.cuh"
 #include "kernels/symtile.hpp"
 #include "kernels/twolevel.cuh"
@@ -241,8 +243,14 @@ int stx_context_create(const char* session_path, const char* overrides, int devi
     g.family = upload(A, M.family);
     {
       // chunks of up to 32 same-family elements (fewer when the recovery
-      // kernel's shared-memory plan would exceed 200 KB)
+      // kernel's shared-memory plan would exceed 200 KB; token STX_CHUNK
+      // caps the count, the autotuner's element-chunk choice)
       int cm = 32;
+      if (ctx->S.tokens.has("STX_CHUNK")) {
+        const int want = ctx->S.tokens.ivalue("STX_CHUNK");
+        if (want < 1 || want > 32) throw StxError(STX_EINVAL, "STX_CHUNK must be in 1..32");
+        cm = want;
+      }
       auto need = [&](int c) {  // shared memory of the batched recovery kernel
         return sizeof(double) * (2 * static_cast<size_t>(c) * (M.npnp | 1) + 2 * static_cast<size_t>(c) * (M.next | 1) +
                                  24 * M.npnp + M.np * M.np);
@@ -578,6 +586,9 @@ int stx_modal_create(stx_context* ctx, char field, double lambda2, double beta, 
         throw StxError(STX_EUNSUPPORTED, "mixed precision needs the two-level skeleton solve");
       std::vector<ModeSystem> modes(num_modes);
       std::vector<std::string> errs(num_modes);
+      // two-level systems form their patch and interface matrices on the
+      // device (token STX_SETUP_HOST = 1: on the host, for comparison)
+      const bool l2_device = P && !(ctx->S.tokens.has("STX_SETUP_HOST") && ctx->S.tokens.ivalue("STX_SETUP_HOST"));
       // viscous systems: beta^2 k^2 scaled by the SVV factors of the modes
       // (src/matrix.cpp:78-83)
       const TokenTable& T = ctx->S.tokens;
@@ -594,7 +605,7 @@ int stx_modal_create(stx_context* ctx, char field, double lambda2, double beta, 
           for (int m = static_cast<int>(w); m < num_modes; m += nth) {
             try {
               const double bk = beta * (base_mode + m);
-              modes[m] = build_mode_system(M, N, P, lambda2, bk * bk * svz[m], method, inner);
+              modes[m] = build_mode_system(M, N, P, lambda2, bk * bk * svz[m], method, inner, l2_device);
             } catch (const std::exception& e) {
               errs[m] = e.what();
             }
@@ -607,6 +618,7 @@ int stx_modal_create(stx_context* ctx, char field, double lambda2, double beta, 
       d.nmodes = num_modes;
       d.method = method;
       d.nfamily = M.nfamily;
+      d.sym_warps = 4;
       // bound of the kernels' bounded waits (token STX_WAIT_NS, default 2 s;
       // 0: one non-blocking probe, which a copy issued just before misses --
       // the error path's tests use it)
@@ -683,6 +695,23 @@ int stx_modal_create(stx_context* ctx, char field, double lambda2, double beta, 
         const size_t nB_max = std::max(1, P->nB_max);
         std::vector<int> pin(num_modes, -1);
         const size_t nI_max = std::max(1, P->nI_max);
+        // packed layout per mode: S_II^-1 of each patch family, G of each
+        // patch family, the interface inverse
+        long long pack_total = 0;
+        for (int m = 0; m < num_modes; ++m) {
+          for (int f = 0; f < P->nfamily; ++f) {
+            fam_off[static_cast<size_t>(m) * P->nfamily + f] = pack_total;
+            pack_total += sym_size(P->nI[P->family_rep[f]]);
+          }
+          for (int f = 0; f < P->nfamily; ++f) {
+            const int rep = P->family_rep[f];
+            g_off[static_cast<size_t>(m) * P->nfamily + f] = pack_total;
+            pack_total += gen_size(P->nI[rep], P->nB[rep]);
+          }
+          if_off[m] = pack_total;
+          pack_total += sym_size(P->niface);
+        }
+        std::vector<double> hbb_dev;
         for (int m = 0; m < num_modes; ++m) {
           hbi.insert(hbi.end(), modes[m].hbi.begin(), modes[m].hbi.end());
           hii.insert(hii.end(), modes[m].hii.begin(), modes[m].hii.end());
@@ -690,6 +719,12 @@ int stx_modal_create(stx_context* ctx, char field, double lambda2, double beta, 
             const double* h = modes[m].hsc.data() + static_cast<size_t>(f) * nx * nx;
             for (int a = 0; a < nx; ++a)
               for (int b = 0; b < ldsc; ++b) sc.push_back(b < nx ? h[static_cast<size_t>(a) * nx + b] : 0.0);
+          }
+          pin[m] = modes[m].pin_iid;
+          if (l2_device) {
+            hbb_dev.insert(hbb_dev.end(), modes[m].hsc.begin(), modes[m].hsc.end());
+            modes[m] = ModeSystem();
+            continue;
           }
           for (int f = 0; f < P->nfamily; ++f) {
             const int n = P->nI[P->family_rep[f]];
@@ -746,12 +781,30 @@ int stx_modal_create(stx_context* ctx, char field, double lambda2, double beta, 
           for (int m = 0; m < num_modes; ++m)
             if (pin[m] >= 0) throw StxError(STX_EUNSUPPORTED, "mixed precision needs a non-singular system");
           if (!N.mixdiag.empty()) throw StxError(STX_EUNSUPPORTED, "mixed precision with mixed (Robin) BCs");
-          std::vector<float> p32(pack.begin(), pack.end());
-          if (p32.empty()) p32.assign(32, 0.0f);
-          d.l2_pack32 = upload(st->arena, p32);
+          if (l2_device) {
+            DeviceArena t64;
+            const size_t np64 = std::max<long long>(pack_total, 32);
+            double* d64 = static_cast<double*>(t64.alloc(sizeof(double) * np64));
+            cuda_check(cudaMemsetAsync(d64, 0, sizeof(double) * np64, ctx->stream), "pack memset");
+            l2_device_setup_guarded(M, N, *P, hbb_dev, num_modes, pin, fam_off, g_off, if_off, d64, ctx->stream);
+            float* d32 = static_cast<float*>(st->arena.alloc(sizeof(float) * np64));
+            cuda_check(to_float(d64, d32, np64, ctx->stream), "pack to FP32");
+            cuda_check(cudaStreamSynchronize(ctx->stream), "pack sync");
+            d.l2_pack32 = d32;
+          } else {
+            std::vector<float> p32(pack.begin(), pack.end());
+            if (p32.empty()) p32.assign(32, 0.0f);
+            d.l2_pack32 = upload(st->arena, p32);
+          }
           d.l2_pack = nullptr;
           d.refine = ctx->S.tokens.has("STX_REFINE") ? ctx->S.tokens.ivalue("STX_REFINE") : 2;
           if (d.refine < 0) throw StxError(STX_EINVAL, "STX_REFINE must be at least 0");
+        } else if (l2_device) {
+          const size_t np64 = std::max<long long>(pack_total, 32);
+          double* d64 = static_cast<double*>(st->arena.alloc(sizeof(double) * np64));
+          cuda_check(cudaMemsetAsync(d64, 0, sizeof(double) * np64, ctx->stream), "pack memset");
+          l2_device_setup_guarded(M, N, *P, hbb_dev, num_modes, pin, fam_off, g_off, if_off, d64, ctx->stream);
+          d.l2_pack = d64;
         } else {
           d.l2_pack = upload(st->arena, pack.empty() ? std::vector<double>(32, 0.0) : pack);
         }
@@ -774,8 +827,17 @@ int stx_modal_create(stx_context* ctx, char field, double lambda2, double beta, 
         if (P->niface > 0)
           for (int m = 0; m < num_modes; ++m)
             pi.push_back(SymProblem{if_off[m], P->niface, m, pin[m], d.skel_of, 0, nullptr, 1.0});
-        const std::vector<SymWarp> wp = sym_schedule(pp, ctx->device), wi = sym_schedule(pi, ctx->device),
-                                   wg = sym_schedule(pg, ctx->device);
+        // products' launch shape: warps per block (token STX_SYM_WARPS,
+        // default 4) and warps scheduled per full wave (STX_SYM_OCC percent,
+        // default 100): autotuner knobs
+        const int wpb = ctx->S.tokens.has("STX_SYM_WARPS") ? ctx->S.tokens.ivalue("STX_SYM_WARPS") : 4;
+        const int occ = ctx->S.tokens.has("STX_SYM_OCC") ? ctx->S.tokens.ivalue("STX_SYM_OCC") : 100;
+        if (wpb < 1 || wpb > 8) throw StxError(STX_EINVAL, "STX_SYM_WARPS must be in 1..8");
+        if (occ < 10 || occ > 800) throw StxError(STX_EINVAL, "STX_SYM_OCC must be in 10..800");
+        d.sym_warps = wpb;
+        const std::vector<SymWarp> wp = sym_schedule(pp, ctx->device, wpb, occ),
+                                   wi = sym_schedule(pi, ctx->device, wpb, occ),
+                                   wg = sym_schedule(pg, ctx->device, wpb, occ);
         d.prob_gen = pg.empty() ? nullptr : upload(st->arena, pg);
         d.warp_gen = wg.empty() ? nullptr : upload(st->arena, wg);
         d.nwarp_gen = static_cast<int>(wg.size());
@@ -802,8 +864,9 @@ int stx_modal_create(stx_context* ctx, char field, double lambda2, double beta, 
             while (ppos < pp.size() && pp[ppos].mode < m1) gp.push_back(pp[ppos++]);
             while (ipos < pi.size() && pi[ipos].mode < m1) gi.push_back(pi[ipos++]);
             while (gpos < pg.size() && pg[gpos].mode < m1) gg.push_back(pg[gpos++]);
-            const std::vector<SymWarp> gwp = sym_schedule(gp, ctx->device), gwi = sym_schedule(gi, ctx->device),
-                                       gwg = sym_schedule(gg, ctx->device);
+            const std::vector<SymWarp> gwp = sym_schedule(gp, ctx->device, wpb, occ),
+                                       gwi = sym_schedule(gi, ctx->device, wpb, occ),
+                                       gwg = sym_schedule(gg, ctx->device, wpb, occ);
             v.prob_gen = gg.empty() ? nullptr : d.prob_gen + q0;
             v.warp_gen = gwg.empty() ? nullptr : upload(st->arena, gwg);
             v.nwarp_gen = static_cast<int>(gwg.size());

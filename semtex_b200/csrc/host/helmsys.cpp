@@ -212,7 +212,7 @@ void spd_inverse(int n, double* A, int nthreads) {
 }
 
 ModeSystem build_mode_system(const Mesh& M, const Numbering& N, const Patching* P, double lambda2,
-                             double betak2, int method, int nthreads) {
+                             double betak2, int method, int nthreads, bool l2_device) {
   ModeSystem S;
   S.lambda2 = lambda2;
   S.betak2 = betak2;
@@ -278,6 +278,13 @@ ModeSystem build_mode_system(const Mesh& M, const Numbering& N, const Patching* 
     }
   }
 
+  if (P && l2_device) {
+    S.hsc = hbb_all;
+    S.pin_iid = S.singular ? P->pin_iid : -1;
+    S.nsolve = P->niface;
+    S.nband = 0;
+    return S;
+  }
   if (P) {
     // -- second level: per patch family, condense the patch-interior
     //    skeleton nodes; assemble the interface Schur complements.

@@ -47,11 +47,13 @@ struct ModeSystem {
 void element_helmholtz(const Mesh& M, int e, double lambda2, double betak2, double* H);
 
 // `P` (may be null) selects the two-level condensation for DIRECT systems.
+// l2_device: stop after the element level (hbi, hii, hsc, pin_iid): the
+// patch and interface matrices are then formed on the device (l2setup.cu).
 // In-place inverse of a symmetric positive-definite n x n matrix (Cholesky,
 // triangular inverse, product) on `nthreads` host threads; throws if the
 // matrix is not positive definite.
 void spd_inverse(int n, double* A, int nthreads = 1);
 ModeSystem build_mode_system(const Mesh& M, const Numbering& N, const Patching* P, double lambda2,
-                             double betak2, int method, int nthreads = 1);
+                             double betak2, int method, int nthreads = 1, bool l2_device = false);
 
 }  // namespace stx

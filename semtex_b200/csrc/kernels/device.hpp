@@ -96,6 +96,7 @@ struct DevModal {
   const double* dinv_fwd;         // [nmodes][dinv_stride]: 16x16 inverse diagonal blocks
   const double* dinv_bwd;
   int* status;                    // device status word (0 = ok)
+  int sym_warps;                  // warps per block of the packed products (token STX_SYM_WARPS)
   unsigned long long wait_ns;     // bound of the element and skeleton kernels' first
                                   // wait per copy (token STX_WAIT_NS, default 2 s)
   const double* pc;               // JACPCG: [nmodes][npts]

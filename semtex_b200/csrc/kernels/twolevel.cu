@@ -29,10 +29,9 @@ namespace stx {
 
 namespace {
 
-// Warps per block of the packed products (for each NF: 4 measured faster
-// than 6 for one field).
-template <int NF>
-constexpr int kSymWarps = 4;
+// Warps per block of the packed products: DevModal::sym_warps (token
+// STX_SYM_WARPS, 1..8, default 4: measured faster than 6 for one field).
+constexpr int kSymWarpsMax = 8;
 constexpr int kSymStages = 1;  // tile buffers per warp
 constexpr int kTileDoubles = kSymTile * kSymLd;
 
@@ -46,7 +45,7 @@ struct SymWarpSmem {
   double tile[kSymStages][kTileDoubles];
 };
 template <int NF>
-constexpr size_t sym_smem() { return kSymWarps<NF> * sizeof(SymWarpSmem<NF>); }
+constexpr size_t sym_smem(int warps) { return warps * sizeof(SymWarpSmem<NF>); }
 
 // Position of a warp in the tiles of its problems.
 struct SymCursor {
@@ -94,13 +93,13 @@ struct SymCursor {
 // added at its end.  Waits are bounded; on expiry `status` is set and the
 // warp stops.
 template <class T, int NF>
-__global__ void __launch_bounds__(32 * kSymWarps<NF>)
+__global__ void __launch_bounds__(32 * kSymWarpsMax)
     k_psymv(const T* __restrict__ pack, const SymProblem* __restrict__ probs, const SymWarp* __restrict__ warps,
             int nwarps, const double* __restrict__ X, double* __restrict__ Y, int rstride, size_t fstride, int nz,
             int* status, unsigned long long wait_ns) {
   extern __shared__ __align__(16) unsigned char sraw[];
   const int wp = threadIdx.x >> 5, ln = threadIdx.x & 31;
-  const int gw = blockIdx.x * kSymWarps<NF> + wp;
+  const int gw = blockIdx.x * (blockDim.x >> 5) + wp;
   if (gw >= nwarps) return;  // the warps of a block never synchronise with each other
   SymWarpSmem<NF>& sm = reinterpret_cast<SymWarpSmem<NF>*>(sraw)[wp];
   const SymWarp W = warps[gw];
@@ -259,19 +258,19 @@ __global__ void __launch_bounds__(32 * kSymWarps<NF>)
 }
 
 void configure_psymv() {
-  raise_smem_limit(reinterpret_cast<const void*>(k_psymv<double, 1>), sym_smem<1>());
-  raise_smem_limit(reinterpret_cast<const void*>(k_psymv<float, 1>), sym_smem<1>());
-  raise_smem_limit(reinterpret_cast<const void*>(k_psymv<double, 2>), sym_smem<2>());
-  raise_smem_limit(reinterpret_cast<const void*>(k_psymv<double, 3>), sym_smem<3>());
+  raise_smem_limit(reinterpret_cast<const void*>(k_psymv<double, 1>), sym_smem<1>(kSymWarpsMax));
+  raise_smem_limit(reinterpret_cast<const void*>(k_psymv<float, 1>), sym_smem<1>(kSymWarpsMax));
+  raise_smem_limit(reinterpret_cast<const void*>(k_psymv<double, 2>), sym_smem<2>(kSymWarpsMax));
+  raise_smem_limit(reinterpret_cast<const void*>(k_psymv<double, 3>), sym_smem<3>(kSymWarpsMax));
 }
 
 template <class T, int NF>
 void launch_psymv_as(const T* pack, const SymProblem* probs, const SymWarp* warps, int nwarps, const double* X,
                      double* Y, int rstride, size_t fstride, int nz, int* status, unsigned long long wait_ns,
-                     cudaStream_t st) {
-  const int blocks = (nwarps + kSymWarps<NF> - 1) / kSymWarps<NF>;
-  k_psymv<T, NF><<<blocks, 32 * kSymWarps<NF>, sym_smem<NF>(), st>>>(pack, probs, warps, nwarps, X, Y, rstride,
-                                                                     fstride, nz, status, wait_ns);
+                     int wpb, cudaStream_t st) {
+  const int blocks = (nwarps + wpb - 1) / wpb;
+  k_psymv<T, NF><<<blocks, 32 * wpb, sym_smem<NF>(wpb), st>>>(pack, probs, warps, nwarps, X, Y, rstride, fstride,
+                                                              nz, status, wait_ns);
 }
 
 cudaError_t launch_psymv(const DevModal& S, const SymProblem* probs, const SymWarp* warps, int nwarps,
@@ -280,13 +279,13 @@ cudaError_t launch_psymv(const DevModal& S, const SymProblem* probs, const SymWa
   if (nwarps <= 0) return cudaSuccess;
   configure_psymv();
   if (fp32)
-    launch_psymv_as<float, 1>(S.l2_pack32, probs, warps, nwarps, X, Y, rstride, 0, nz, S.status, S.wait_ns, st);
+    launch_psymv_as<float, 1>(S.l2_pack32, probs, warps, nwarps, X, Y, rstride, 0, nz, S.status, S.wait_ns, S.sym_warps, st);
   else if (nf == 3)
-    launch_psymv_as<double, 3>(S.l2_pack, probs, warps, nwarps, X, Y, rstride, fstride, nz, S.status, S.wait_ns, st);
+    launch_psymv_as<double, 3>(S.l2_pack, probs, warps, nwarps, X, Y, rstride, fstride, nz, S.status, S.wait_ns, S.sym_warps, st);
   else if (nf == 2)
-    launch_psymv_as<double, 2>(S.l2_pack, probs, warps, nwarps, X, Y, rstride, fstride, nz, S.status, S.wait_ns, st);
+    launch_psymv_as<double, 2>(S.l2_pack, probs, warps, nwarps, X, Y, rstride, fstride, nz, S.status, S.wait_ns, S.sym_warps, st);
   else
-    launch_psymv_as<double, 1>(S.l2_pack, probs, warps, nwarps, X, Y, rstride, 0, nz, S.status, S.wait_ns, st);
+    launch_psymv_as<double, 1>(S.l2_pack, probs, warps, nwarps, X, Y, rstride, 0, nz, S.status, S.wait_ns, S.sym_warps, st);
   return cudaGetLastError();
 }
 
@@ -341,7 +340,7 @@ int twolevel_launches(const DevModal& S) {
 
 static int prob_ntiles(const SymProblem& P) { return P.ncol ? gen_ntiles(P.n, P.ncol) : sym_ntiles(P.n); }
 
-std::vector<SymWarp> sym_schedule(const std::vector<SymProblem>& probs, int device) {
+std::vector<SymWarp> sym_schedule(const std::vector<SymProblem>& probs, int device, int wpb, int occ_pct) {
   std::vector<SymWarp> out;
   long long total = 0;
   for (const auto& P : probs) total += prob_ntiles(P);
@@ -349,11 +348,13 @@ std::vector<SymWarp> sym_schedule(const std::vector<SymProblem>& probs, int devi
   int sms = 148, per_sm = 1;
   cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, device);
   configure_psymv();
-  if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_psymv<double, 1>, 32 * kSymWarps<1>, sym_smem<1>()) !=
+  if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_psymv<double, 1>, 32 * wpb, sym_smem<1>(wpb)) !=
           cudaSuccess ||
       per_sm < 1)
     per_sm = 1;
-  const long long nw = std::min<long long>(total, static_cast<long long>(sms) * per_sm * kSymWarps<1>);
+  // warps of one full wave at the kernel's occupancy, times occ_pct / 100
+  const long long wave = static_cast<long long>(sms) * per_sm * wpb;
+  const long long nw = std::max<long long>(1, std::min<long long>(total, wave * occ_pct / 100));
   size_t p = 0;
   long long before = 0;  // tiles of problems [0, p)
   for (long long w = 0; w < nw; ++w) {

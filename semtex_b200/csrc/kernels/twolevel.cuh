@@ -30,7 +30,9 @@ cudaError_t twolevel_solve_fields(const DevModal& S, const DevGeom& g, const Dev
 int twolevel_launches(const DevModal& S);
 
 // Split the tiles of `probs` (in order) into equal runs, one per warp of a
-// grid that fills `device` once at the product kernel's occupancy.
-std::vector<SymWarp> sym_schedule(const std::vector<SymProblem>& probs, int device);
+// grid of `wpb`-warp blocks that fills `device` occ_pct / 100 times at the
+// product kernel's occupancy (100: one full wave).
+std::vector<SymWarp> sym_schedule(const std::vector<SymProblem>& probs, int device, int wpb = 4,
+                                  int occ_pct = 100);
 
 }  // namespace stx

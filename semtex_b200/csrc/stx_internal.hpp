@@ -81,9 +81,15 @@ struct stx_context {
     if (!F.patch_done) {
       F.patch_done = true;
       const bool want = (!S.tokens.has("STX_TWOLEVEL") || S.tokens.ivalue("STX_TWOLEVEL") != 0) && M.next <= 64;
+      // token STX_PATCH_CAP (8, 16, 36 or 64) fixes the patch size (the
+      // autotuner's choice) instead of the byte model
+      const int fixed = S.tokens.has("STX_PATCH_CAP") ? S.tokens.ivalue("STX_PATCH_CAP") : 0;
+      if (fixed && fixed != 8 && fixed != 16 && fixed != 36 && fixed != 64)
+        throw std::runtime_error("STX_PATCH_CAP must be 8, 16, 36 or 64");
       if (want) {
         double best = 0;
         for (int cap : {8, 16, 36, 64}) {
+          if (fixed && cap != fixed) continue;
           auto P = std::make_unique<stx::Patching>(stx::build_patching(M, F.N, cap));
           if (P->niface > 6000) continue;
           double bytes = static_cast<double>(stx::sym_size(P->niface));

@@ -1,0 +1,43 @@
+"""The autotuner on the device: every knob value it may pick gives the same
+solution (to round-off), and a tuning run records a winner no slower than
+the defaults, which then solves correctly."""
+import numpy as np
+import pytest
+
+import semtex_b200 as S
+from semtex_b200 import autotune as A, sessions
+
+pytestmark = pytest.mark.gpu
+
+
+def _solve(p, ov, f):
+    ctx = S.Context(p, ov or None)
+    sysm = S.ModalMatrixSys(ctx, "c", 1.0)
+    u = sysm.solve_host(f)
+    assert sysm.status() == 0
+    sysm.close()
+    ctx.close()
+    return u
+
+
+@pytest.mark.parametrize("ov", [{"STX_PATCH_CAP": 8}, {"STX_PATCH_CAP": 64}, {"STX_CHUNK": 8},
+                                {"STX_CHUNK": 3}, {"STX_MODE_GROUPS": 3}, {"STX_SYM_WARPS": 1},
+                                {"STX_SYM_WARPS": 8}, {"STX_SYM_OCC": 10}, {"STX_SYM_OCC": 400}])
+def test_knobs_do_not_change_the_solution(tmp_path, ov):
+    p = sessions.helmholtz_session(str(tmp_path / "k"), 8, 7, nz=8, lambda2=1.0, beta=1.0)
+    f = np.random.default_rng(2).uniform(-1, 1, (8, 64, 7, 7))
+    ref = _solve(p, {}, f)
+    got = _solve(p, ov, f)
+    assert np.linalg.norm(got - ref) <= 1e-12 * np.linalg.norm(ref)
+
+
+def test_tune_records_winner(tmp_path):
+    p = sessions.helmholtz_session(str(tmp_path / "t"), 8, 7, nz=8, lambda2=1.0, beta=1.0)
+    table = str(tmp_path / "table.json")
+    space = {"STX_CHUNK": [None, 8], "STX_SYM_WARPS": [None, 2]}
+    e = A.tune(p, "c", 1.0, space=space, reps=3, path=table)
+    assert e["best_ms"] <= e["default_ms"] and len(e["trials"]) == 3
+    ov = A.tuned_overrides(p, "c", 1.0, table)
+    assert ov == e["best"]
+    f = np.random.default_rng(4).uniform(-1, 1, (8, 64, 7, 7))
+    assert np.linalg.norm(_solve(p, ov, f) - _solve(p, {}, f)) <= 1e-12 * np.linalg.norm(_solve(p, {}, f))
