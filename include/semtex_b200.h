@@ -290,6 +290,20 @@ int stx_dns_state(const stx_dns* dns, int* step, double* time);
 int stx_dns_modal_energy(stx_dns* dns, double* h_ek);
 int stx_dns_divergence_energy(stx_dns* dns, double* value);
 int stx_dns_cfl(stx_dns* dns, double* inv_dt);
+/* Full-state checkpoint of the time stepping: the fields, the multi-level
+ * velocity and nonlinear storage Us/Uf of every order (dns/integrate.cpp:
+ * 99-136), the high-order pressure BC levels (BCmgr's _un / _hopbc,
+ * src/bcmgr.cpp:951-993), the alternating form's switch, forcing state (SFD
+ * filter, sponge mask) and running averages, with step and time.  The
+ * reference's Domain::dump / restart (src/domain.cpp:123-215) keep the fields
+ * only and restart at first order; a loaded checkpoint continues exactly as
+ * the uninterrupted run.  _size gives the bytes; _save fills a host buffer
+ * (synchronises); _load restores one into a DNS of the same session
+ * (re-evaluates BCs at the restored time; STX_EINVAL for a buffer of another
+ * layout). */
+int stx_dns_checkpoint_size(stx_dns* dns, unsigned long long* bytes);
+int stx_dns_checkpoint_save(stx_dns* dns, void* h_buf, unsigned long long bytes);
+int stx_dns_checkpoint_load(stx_dns* dns, const void* h_buf, unsigned long long bytes);
 /* The ModalMatrixSys a steady step solves `field` with: the viscous system
  * of a velocity component (dns/integrate.cpp:186-193), the pressure system
  * (:244-252); owned by the DNS (not to be destroyed).  For stx_modal_bytes

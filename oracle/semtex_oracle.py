@@ -459,7 +459,11 @@ class Numbering:
     bmask (1 = essential), solve nodes numbered first, RCM-ordered.
     """
 
-    def __init__(self, M: Mesh, fld: str, rcm: bool = True, mclass: int = 0):
+    def __init__(self, M: Mesh, fld: str, rcm: bool = True, mclass: int = 0, btog=None):
+        """btog: a precomputed map (the `.num` file's contents, as the
+        reference's dns reads it) used instead of this restatement's RCM /
+        `enumerate -O3` ordering; the CPU timings pass one to skip the -O3
+        search, which tries every node as root."""
         S, n, nel = M.S, M.np, M.nel
         nm = n - 1
         next_ = 4 * nm
@@ -531,7 +535,9 @@ class Numbering:
         newid[order] = np.arange(nsolve)
         newid[ess_nodes] = nsolve + np.arange(len(ess_nodes))
         self.btog = newid[gid]
-        if rcm and not len(ess_nodes):
+        if btog is not None:
+            self.btog = np.asarray(btog, int).reshape(nel, next_)
+        elif rcm and not len(ess_nodes):
             # no essential nodes: the k=0 system of this field is singular and
             # its pinned node (the highest number) decides the solution, so
             # the reference's own numbering is used
@@ -910,15 +916,12 @@ class MatrixSys:
                 else:
                     hii_inv, hbi_c = hii, hbi
                 self.hbi[e], self.hii[e] = hbi_c, hii_inv
-                g = N.btog[e]
-                for i in range(next_):
-                    m = g[i]
-                    if m >= ns:
-                        continue
-                    for k in range(next_):
-                        nn = g[k]
-                        if nn < ns and nn >= m:
-                            AB[kd + m - nn, nn] += hbb[i, k]
+                # band assembly (src/matrix.cpp:218-232): entries (m, n),
+                # m <= n < nsolve, of the element's boundary nodes
+                g = np.asarray(N.btog[e])
+                gm, gn = g[:, None], g[None, :]
+                sel = (gm < ns) & (gn < ns) & (gn >= gm)
+                np.add.at(AB, ((kd + gm - gn)[sel], np.broadcast_to(gn, sel.shape)[sel]), hbb[sel])
             if mixdiag is not None:
                 AB[kd, :ns] += mixdiag[:ns]
             self.factor = sla.cholesky_banded(AB, lower=False) if ns else AB
@@ -1133,7 +1136,8 @@ def read_field(path):
 class Problem:
     """Mesh + numbering + boundary systems for every field of a session."""
 
-    def __init__(self, S: Session, rcm: bool = True):
+    def __init__(self, S: Session, rcm: bool = True, numbering: dict | None = None):
+        """numbering: {field: btog} precomputed maps (see Numbering)."""
         self.S = S
         tok = S.tokens
         self.np = tok.ivalue("N_P")
@@ -1144,7 +1148,7 @@ class Problem:
         self.nel = self.M.nel
         self.N, self.B = {}, {}
         for c in S.fields:
-            self.N[c] = Numbering(self.M, c, rcm)
+            self.N[c] = Numbering(self.M, c, rcm, btog=(numbering or {}).get(c))
             self.B[c] = BoundarySystem(self.M, self.N[c], c)
         # cylindrical 3D with axis BCs: numbering and BCs per Fourier mode
         # class 0, 1, 2+ (BCmgr::getNumberSys, src/bcmgr.cpp:550-583)

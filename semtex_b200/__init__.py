@@ -393,6 +393,20 @@ class DNS:
             check(lib().stx_dns_destroy(self._h))
         self._h = C.c_void_p()
 
+    def checkpoint(self) -> np.ndarray:
+        """Full state (fields, multistep history, pressure-BC levels, forcing
+        state, averages, step, time) as a host array (stx_dns_checkpoint_save)."""
+        n = C.c_ulonglong()
+        check(lib().stx_dns_checkpoint_size(self._h, C.byref(n)))
+        buf = np.empty(n.value // 8, dtype=np.float64)
+        check(lib().stx_dns_checkpoint_save(self._h, C.c_void_p(buf.ctypes.data), n.value))
+        return buf
+
+    def restore(self, buf: np.ndarray):
+        """Continue from a checkpoint of the same session (stx_dns_checkpoint_load)."""
+        buf = np.ascontiguousarray(buf, dtype=np.float64)
+        check(lib().stx_dns_checkpoint_load(self._h, C.c_void_p(buf.ctypes.data), buf.nbytes))
+
     def system_bytes(self, field: str):
         """Algorithmic bytes of one direct solve of `field`'s steady-step
         system, per phase (stx_dns_system + stx_modal_bytes)."""

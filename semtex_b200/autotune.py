@@ -5,8 +5,9 @@ library otherwise makes from byte and shared-memory models: the patch size of
 the two-level condensation (session token STX_PATCH_CAP), the elements per
 chunk of the element kernels (STX_CHUNK), the Fourier-mode groups run on
 parallel streams (STX_MODE_GROUPS), the warps per block of the packed
-skeleton products (STX_SYM_WARPS) and how many product warps are scheduled
-per full wave (STX_SYM_OCC, percent).  ``tune`` measures them on the device
+skeleton products (STX_SYM_WARPS), how many product warps are scheduled
+per full wave (STX_SYM_OCC, percent) and whether the products run their
+register-capped build (STX_SYM_REGCAP: more resident warps, a few spills).  ``tune`` measures them on the device
 by coordinate descent -- each knob in turn over its values with the others
 held at the best so far, the device time of stx_field_solve (CUDA events,
 median of several solves of a resident forcing) deciding -- and records every
@@ -37,6 +38,7 @@ SPACE = {
     "STX_MODE_GROUPS": [None, 1, 3, 4],
     "STX_SYM_WARPS": [None, 2, 8],
     "STX_SYM_OCC": [None, 50, 200],
+    "STX_SYM_REGCAP": [None, 1],
 }
 
 

@@ -205,10 +205,6 @@ int stx_context_create(const char* session_path, const char* overrides, int devi
     ctx->S = read_session(session_path, overrides ? overrides : "");
     if (ctx->S.tokens.ivalue("CYLINDRICAL"))
       throw StxError(STX_EUNSUPPORTED, "cylindrical coordinates are not supported");
-    for (const auto& g : ctx->S.bcs)
-      for (const auto& f : g.second)
-        if (f.second.kind == 'O')
-          throw StxError(STX_EUNSUPPORTED, "computed outflow BCs <O> are not supported");
     ctx->M = build_mesh(ctx->S);
     ctx->device = device;
     cuda_check(cudaSetDevice(device), "cudaSetDevice");
@@ -619,6 +615,7 @@ int stx_modal_create(stx_context* ctx, char field, double lambda2, double beta, 
       d.method = method;
       d.nfamily = M.nfamily;
       d.sym_warps = 4;
+      d.sym_regcap = 0;
       // bound of the kernels' bounded waits (token STX_WAIT_NS, default 2 s;
       // 0: one non-blocking probe, which a copy issued just before misses --
       // the error path's tests use it)
@@ -834,10 +831,12 @@ int stx_modal_create(stx_context* ctx, char field, double lambda2, double beta, 
         const int occ = ctx->S.tokens.has("STX_SYM_OCC") ? ctx->S.tokens.ivalue("STX_SYM_OCC") : 100;
         if (wpb < 1 || wpb > 8) throw StxError(STX_EINVAL, "STX_SYM_WARPS must be in 1..8");
         if (occ < 10 || occ > 800) throw StxError(STX_EINVAL, "STX_SYM_OCC must be in 10..800");
+        const int rcap = ctx->S.tokens.has("STX_SYM_REGCAP") ? (ctx->S.tokens.ivalue("STX_SYM_REGCAP") != 0) : 0;
         d.sym_warps = wpb;
-        const std::vector<SymWarp> wp = sym_schedule(pp, ctx->device, wpb, occ),
-                                   wi = sym_schedule(pi, ctx->device, wpb, occ),
-                                   wg = sym_schedule(pg, ctx->device, wpb, occ);
+        d.sym_regcap = rcap;
+        const std::vector<SymWarp> wp = sym_schedule(pp, ctx->device, wpb, occ, rcap),
+                                   wi = sym_schedule(pi, ctx->device, wpb, occ, rcap),
+                                   wg = sym_schedule(pg, ctx->device, wpb, occ, rcap);
         d.prob_gen = pg.empty() ? nullptr : upload(st->arena, pg);
         d.warp_gen = wg.empty() ? nullptr : upload(st->arena, wg);
         d.nwarp_gen = static_cast<int>(wg.size());
@@ -864,9 +863,9 @@ int stx_modal_create(stx_context* ctx, char field, double lambda2, double beta, 
             while (ppos < pp.size() && pp[ppos].mode < m1) gp.push_back(pp[ppos++]);
             while (ipos < pi.size() && pi[ipos].mode < m1) gi.push_back(pi[ipos++]);
             while (gpos < pg.size() && pg[gpos].mode < m1) gg.push_back(pg[gpos++]);
-            const std::vector<SymWarp> gwp = sym_schedule(gp, ctx->device, wpb, occ),
-                                       gwi = sym_schedule(gi, ctx->device, wpb, occ),
-                                       gwg = sym_schedule(gg, ctx->device, wpb, occ);
+            const std::vector<SymWarp> gwp = sym_schedule(gp, ctx->device, wpb, occ, rcap),
+                                       gwi = sym_schedule(gi, ctx->device, wpb, occ, rcap),
+                                       gwg = sym_schedule(gg, ctx->device, wpb, occ, rcap);
             v.prob_gen = gg.empty() ? nullptr : d.prob_gen + q0;
             v.warp_gen = gwg.empty() ? nullptr : upload(st->arena, gwg);
             v.nwarp_gen = static_cast<int>(gwg.size());

@@ -22,6 +22,7 @@
 #include "../../include/semtex_b200.h"
 #include "host/fieldfile.hpp"
 #include "kernels/dns_kernels.cuh"
+#include "kernels/outflow.cuh"
 #include "kernels/force.cuh"
 #include "kernels/helmholtz.cuh"
 #include "stx_internal.hpp"
@@ -106,6 +107,13 @@ struct stx_dns {
   const double* h_ny = nullptr;
   std::vector<double*> un_lvl, hop_lvl;
   size_t hsize = 0;  // doubles per level
+  // Computed outflow BCs <O> (outflow.cuh): edges, and the levels (newest
+  // first, rolled by pointer) of the physical edge velocities, nu div u and
+  // nu n.grad(u).n; o_fb holds KE* S0 of the step.
+  stx::OutflowEdges oe{};
+  std::vector<double*> o_uvw, o_divu, o_gradu;
+  double* o_fb = nullptr;
+  double o_iuzd = 0.0;  // 1 / U0Delta
   // 3/2-rule products (token DEALIAS, N_Z > 2): physical fields on nz32 =
   // 3 N_Z / 2 planes (AuxField::transform32, src/auxfield.cpp:1197-1258).
   int nz32 = 0;
@@ -500,6 +508,8 @@ void nonlinear32(stx_dns* d, int form) {
   }
 }
 
+void rollm_levels(std::vector<double*>& v);
+
 // Nonlinear terms N(u) into Uf[0], copy of u into Us[0] (dns/nonlinear.cpp).
 void nonlinear(stx_dns* d) {
   stx_context* ctx = d->ctx;
@@ -522,6 +532,11 @@ void nonlinear(stx_dns* d) {
     copy(d, d->Us[0][i], d->u[i]);
     copy(d, d->Up[i], d->u[i]);
     transform(d, d->Up[i], STX_INVERSE);
+  }
+  if (d->oe.no) {  // BCmgr::maintainPhysical (src/bcmgr.cpp:998-1034): edge velocities of this step
+    rollm_levels(d->o_uvw);
+    ck(outflow_gather(g, d->oe, d->Up[0], d->Up[1], d->ncom > 2 ? d->Up[2] : nullptr, d->o_uvw[0], st),
+       "outflow edge velocities");
   }
   const DevNumbering& Nm = ctx->fields.at(d->names[0]).dn;
   for (int i = 0; i < d->ncom; ++i) {
@@ -616,6 +631,41 @@ void hopbc(stx_dns* d) {
   rollm_levels(d->un_lvl);
 }
 
+// Computed outflow BCs: BCmgr::maintainFourier's gradient terms (newest
+// level from Us[0]) and the essential pressure of the outflow edges
+// (evaluateCEBCp), written into the pressure's BC lines.
+void outflow_pressure(stx_dns* d) {
+  stx_context* ctx = d->ctx;
+  const DevGeom& g = ctx->dg;
+  cudaStream_t st = ctx->stream;
+  rollm_levels(d->o_divu);
+  rollm_levels(d->o_gradu);
+  ck(outflow_fourier(g, d->oe, d->Us[0][0], d->Us[0][1], d->ncom > 2 ? d->Us[0][2] : nullptr, d->nu, d->beta,
+                     d->o_divu[0], d->o_gradu[0], st),
+     "outflow gradients");
+  const int Jx = std::min(d->step, d->nord);
+  ck(outflow_energy(g, d->oe, d->o_uvw.data(), kEX[Jx], Jx, d->o_iuzd, d->o_fb, st), "outflow energy");
+  if (g.nz > 2)
+    ck(z_transform(d->o_fb, g.nz, d->oe.ostride, STX_FORWARD, ctx->d_twiddle, nullptr, st), "outflow transform");
+  else if (g.nz == 2)
+    ck(cudaMemsetAsync(d->o_fb + d->oe.ostride, 0, sizeof(double) * d->oe.ostride, st), "outflow nyquist");
+  const FieldDev& P = ctx->fields.at(d->names[d->ncom]);
+  ck(outflow_plines(g, d->oe, d->o_gradu.data(), kEX[Jx], Jx, d->o_fb, P.d_lines, P.nline, st), "outflow p");
+}
+
+// Natural u, v values of the outflow edges from the new pressure
+// (evaluateCNBCu), written into their BC lines.
+void outflow_velocity(stx_dns* d) {
+  stx_context* ctx = d->ctx;
+  const int Jx = std::min(d->step, d->nord);
+  for (int i = 0; i < 2 && i < d->ncom; ++i) {
+    FieldDev& F = ctx->fields.at(d->names[i]);
+    ck(outflow_ulines(ctx->dg, d->oe, d->o_divu.data(), kEX[Jx], Jx, d->o_fb, d->u[d->ncom], d->nu, i, F.d_lines,
+                      F.nline, ctx->stream),
+       "outflow velocity");
+  }
+}
+
 void advance_one(stx_dns* d) {
   stx_context* ctx = d->ctx;
   const DevGeom& g = ctx->dg;
@@ -626,6 +676,7 @@ void advance_one(stx_dns* d) {
   const char pc = d->names[d->ncom];
   if (d->tdep[d->ncom]) ckstx(stx_field_bc_evaluate(ctx, pc, d->time));
   if (d->nh) hopbc(d);
+  if (d->oe.no) outflow_pressure(d);
   // -- waveProp (dns/integrate.cpp:204-239)
   const int Je = std::min(d->step, d->nord);
   for (int i = 0; i < d->ncom; ++i) {
@@ -658,6 +709,7 @@ void advance_one(stx_dns* d) {
   // -- velocity BCs, viscous substep (dns/integrate.cpp:177-193, 328-356)
   for (int i = 0; i < d->ncom; ++i)
     if (d->tdep[i]) ckstx(stx_field_bc_evaluate(ctx, d->names[i], d->time));
+  if (d->oe.no) outflow_velocity(d);
   // direct systems sharing their matrices: one skeleton solve for all
   // components (every matrix tile read once)
   bool shared = d->step >= d->nord && d->ncom <= 3 && !d->iterative;
@@ -702,6 +754,9 @@ std::vector<double*> pointer_state(const stx_dns* d) {
   for (const auto& v : d->Uf) k.insert(k.end(), v.begin(), v.end());
   k.insert(k.end(), d->un_lvl.begin(), d->un_lvl.end());
   k.insert(k.end(), d->hop_lvl.begin(), d->hop_lvl.end());
+  k.insert(k.end(), d->o_uvw.begin(), d->o_uvw.end());
+  k.insert(k.end(), d->o_divu.begin(), d->o_divu.end());
+  k.insert(k.end(), d->o_gradu.begin(), d->o_gradu.end());
   return k;
 }
 
@@ -734,6 +789,7 @@ bool capture_steps(stx_dns* d) {
   const auto u = d->u;
   const auto Us = d->Us, Uf = d->Uf;
   const auto un = d->un_lvl, hop = d->hop_lvl;
+  const auto ouvw = d->o_uvw, odiv = d->o_divu, ogr = d->o_gradu;
   const int step = d->step, toggle = d->toggle;
   const double time = d->time;
   const std::vector<double*> key = pointer_state(d);
@@ -761,6 +817,9 @@ bool capture_steps(stx_dns* d) {
     d->Uf = Uf;
     d->un_lvl = un;
     d->hop_lvl = hop;
+    d->o_uvw = ouvw;
+    d->o_divu = odiv;
+    d->o_gradu = ogr;
     d->step = step;
     d->toggle = toggle;
     d->time = time;
@@ -899,6 +958,57 @@ int stx_dns_create(stx_context* ctx, int advection, stx_dns** out) {
           d->un_lvl.push_back(hb + d->hsize * q);
           d->hop_lvl.push_back(hb + d->hsize * (d->nord + q));
         }
+      }
+    }
+    // -- computed outflow edges and storage (BCmgr::buildComputedBCs,
+    //    src/bcmgr.cpp:937-996): the pressure's 'O' edges, which u and v
+    //    carry at the same positions of their BC lines
+    {
+      const FieldDev& P = ctx->fields.at(d->names[d->ncom]);
+      std::vector<int> el, sd, ln;
+      std::vector<double> nx, ny;
+      for (size_t b = 0; b < P.N.edges.size(); ++b) {
+        const BoundaryEdge& E = P.N.edges[b];
+        if (E.kind != 'O') continue;
+        for (int i = 0; i < 2; ++i) {
+          const auto& V = ctx->fields.at(d->names[i]).N.edges;
+          if (b >= V.size() || V[b].elmt != E.elmt || V[b].side != E.side)
+            throw DnsError(STX_EUNSUPPORTED, "outflow edges differ between the velocity and pressure BC lines");
+        }
+        el.push_back(E.elmt);
+        sd.push_back(E.side);
+        ln.push_back(static_cast<int>(b));
+        nx.insert(nx.end(), E.nx.begin(), E.nx.end());
+        ny.insert(ny.end(), E.ny.begin(), E.ny.end());
+      }
+      if (!el.empty()) {
+        if (d->nz32) throw DnsError(STX_EUNSUPPORTED, "computed outflow BCs with DEALIAS");
+        auto up = [&](const auto& v) {
+          using T = typename std::decay_t<decltype(v)>::value_type;
+          T* p = static_cast<T*>(d->arena.alloc(sizeof(T) * v.size()));
+          ck(cudaMemcpy(p, v.data(), sizeof(T) * v.size(), cudaMemcpyHostToDevice), "upload");
+          return p;
+        };
+        OutflowEdges& O = d->oe;
+        O.no = static_cast<int>(el.size());
+        O.ostride = (O.no * g.np + 1) / 2 * 2;
+        O.elmt = up(el);
+        O.side = up(sd);
+        O.line = up(ln);
+        O.nx = up(nx);
+        O.ny = up(ny);
+        const size_t lvl = static_cast<size_t>(g.nz) * O.ostride;
+        const size_t total = lvl * (3 * d->nord + 2 * d->nord + 1);
+        double* ob = static_cast<double*>(d->arena.alloc(sizeof(double) * total));
+        ck(cudaMemset(ob, 0, sizeof(double) * total), "memset");
+        for (int q = 0; q < d->nord; ++q) {
+          d->o_uvw.push_back(ob + 3 * lvl * q);
+          d->o_divu.push_back(ob + 3 * lvl * d->nord + lvl * q);
+          d->o_gradu.push_back(ob + 4 * lvl * d->nord + lvl * q);
+        }
+        d->o_fb = ob + 5 * lvl * d->nord;
+        const TokenTable& T = S.tokens;
+        d->o_iuzd = 1.0 / (T.has("U0Delta") ? T.value("U0Delta") : 0.0);
       }
     }
     // -- preSolve (dns/integrate.cpp:292-325): ITERATIVE = 1 selects
@@ -1236,6 +1346,117 @@ int stx_dns_graph_info(const stx_dns* d, int* period, long long* launches) {
     if (!d) throw DnsError(STX_EINVAL, "null argument");
     if (period) *period = d->gperiod;
     if (launches) *launches = d->graph_launches;
+  });
+}
+
+namespace {
+
+// Full-state checkpoint: a header of kCkptHeader doubles, then the device
+// blocks of ckpt_blocks in order.
+constexpr double kCkptMagic = 1398035523.0;  // "STXC" read as a little-endian int
+constexpr int kCkptHeader = 16;
+
+std::vector<std::pair<double*, size_t>> ckpt_blocks(stx_dns* d) {
+  std::vector<std::pair<double*, size_t>> b;
+  for (int i = 0; i <= d->ncom; ++i) b.emplace_back(d->u[i], d->fsize);
+  for (int q = 0; q < d->nord; ++q)
+    for (int i = 0; i < d->ncom; ++i) {
+      b.emplace_back(d->Us[q][i], d->fsize);
+      b.emplace_back(d->Uf[q][i], d->fsize);
+    }
+  for (size_t q = 0; q < d->un_lvl.size(); ++q) {
+    b.emplace_back(d->un_lvl[q], d->hsize);
+    b.emplace_back(d->hop_lvl[q], d->hsize);
+  }
+  const size_t ol = static_cast<size_t>(d->ctx->M.nz) * d->oe.ostride;
+  for (double* a : d->o_uvw) b.emplace_back(a, 3 * ol);
+  for (double* a : d->o_divu) b.emplace_back(a, ol);
+  for (double* a : d->o_gradu) b.emplace_back(a, ol);
+  const size_t nf = static_cast<size_t>(d->force.nzl) * d->ctx->M.plane_size;
+  for (int i = 0; i < 3; ++i)
+    if (d->force.qbar[i]) b.emplace_back(d->force.qbar[i], nf);
+  if (d->force.mask) b.emplace_back(d->force.mask, nf);
+  for (double* a : d->avg_buf) b.emplace_back(a, d->fsize);
+  return b;
+}
+
+void ckpt_header(stx_dns* d, double* h, size_t nblock) {
+  for (int k = 0; k < kCkptHeader; ++k) h[k] = 0.0;
+  h[0] = kCkptMagic;
+  h[1] = 1.0;  // format version
+  h[2] = d->step;
+  h[3] = d->time;
+  h[4] = d->toggle;
+  h[5] = d->ncom;
+  h[6] = d->nord;
+  h[7] = static_cast<double>(d->fsize);
+  h[8] = static_cast<double>(d->hsize);
+  h[9] = static_cast<double>(nblock);
+  h[10] = d->navg;
+  h[11] = d->force.sfd_started ? 1.0 : 0.0;
+}
+
+}  // namespace
+
+int stx_dns_checkpoint_size(stx_dns* d, unsigned long long* bytes) {
+  return dns_guarded([&] {
+    if (!d || !bytes) throw DnsError(STX_EINVAL, "null argument");
+    size_t n = kCkptHeader;
+    for (const auto& b : ckpt_blocks(d)) n += b.second;
+    *bytes = sizeof(double) * n;
+  });
+}
+
+int stx_dns_checkpoint_save(stx_dns* d, void* h_buf, unsigned long long bytes) {
+  return dns_guarded([&] {
+    if (!d || !h_buf) throw DnsError(STX_EINVAL, "null argument");
+    const auto blocks = ckpt_blocks(d);
+    size_t n = kCkptHeader;
+    for (const auto& b : blocks) n += b.second;
+    if (bytes < sizeof(double) * n) throw DnsError(STX_EINVAL, "checkpoint buffer too small");
+    cudaSetDevice(d->ctx->device);
+    double* h = static_cast<double*>(h_buf);
+    ckpt_header(d, h, blocks.size());
+    size_t off = kCkptHeader;
+    for (const auto& b : blocks) {
+      ck(cudaMemcpyAsync(h + off, b.first, sizeof(double) * b.second, cudaMemcpyDeviceToHost, d->ctx->stream),
+         "checkpoint d2h");
+      off += b.second;
+    }
+    ck(cudaStreamSynchronize(d->ctx->stream), "sync");
+  });
+}
+
+int stx_dns_checkpoint_load(stx_dns* d, const void* h_buf, unsigned long long bytes) {
+  return dns_guarded([&] {
+    if (!d || !h_buf) throw DnsError(STX_EINVAL, "null argument");
+    const auto blocks = ckpt_blocks(d);
+    size_t n = kCkptHeader;
+    for (const auto& b : blocks) n += b.second;
+    const double* h = static_cast<const double*>(h_buf);
+    if (bytes < sizeof(double) * kCkptHeader || h[0] != kCkptMagic || h[1] != 1.0)
+      throw DnsError(STX_EINVAL, "not a DNS checkpoint");
+    double want[kCkptHeader];
+    ckpt_header(d, want, blocks.size());
+    for (int k : {5, 6, 7, 8, 9})
+      if (h[k] != want[k]) throw DnsError(STX_EINVAL, "checkpoint of a different session or layout");
+    if (bytes < sizeof(double) * n) throw DnsError(STX_EINVAL, "checkpoint buffer too small");
+    cudaSetDevice(d->ctx->device);
+    size_t off = kCkptHeader;
+    for (const auto& b : blocks) {
+      ck(cudaMemcpyAsync(b.first, h + off, sizeof(double) * b.second, cudaMemcpyHostToDevice, d->ctx->stream),
+         "checkpoint h2d");
+      off += b.second;
+    }
+    ck(cudaStreamSynchronize(d->ctx->stream), "sync");
+    drop_graph(d);
+    d->eager_steady = 0;
+    d->step = static_cast<int>(h[2]);
+    d->time = h[3];
+    d->toggle = static_cast<int>(h[4]);
+    d->navg = static_cast<int>(h[10]);
+    d->force.sfd_started = h[11] != 0.0;
+    for (char c : d->names) ckstx(stx_field_bc_evaluate(d->ctx, c, d->time));
   });
 }
 

@@ -17,25 +17,12 @@
 // element data in its own shared memory (lanes over nodes, a few nodes per
 // lane loaded together) and synchronises only with itself.
 #include "dns_kernels.cuh"
+#include "elemderiv.cuh"
 #include "launch.hpp"
 
 namespace stx {
 
 namespace {
-
-// x (dir 0) or y (dir 1) derivative at node t of the element held in su.
-__device__ __forceinline__ double elem_deriv(const DevGeom& g, const double* su, const double* sD, int e,
-                                             int t, int dir) {
-  const int np = g.np;
-  const int i = t / np, j = t - (t / np) * np;
-  double ur = 0.0, us = 0.0;
-  for (int k = 0; k < np; ++k) {
-    ur += su[i * np + k] * sD[j * np + k];  // (u D^T)[i][j] = du/dr
-    us += sD[i * np + k] * su[k * np + j];  // (D u)[i][j]   = du/ds
-  }
-  const int q = e * g.npnp + t;
-  return dir == 0 ? ur * g.drdx[q] + us * g.dsdx[q] : ur * g.drdy[q] + us * g.dsdy[q];
-}
 
 // Fourier z-derivative of plane k at offset x (planes 0 and 1 are zero).
 __device__ __forceinline__ double zderiv(const double* a, int k, size_t x, int plane_size, double beta) {

@@ -243,10 +243,11 @@ __device__ __forceinline__ void sym_entry(int n, long long o, int& i, int& j, bo
     J = static_cast<int>(o2 / (rows * kSymLd));
     w = o2 - J * rows * kSymLd;
   }
-  const int r = static_cast<int>(w / kSymLd), c = static_cast<int>(w - static_cast<long long>(r) * kSymLd);
+  int r, c;
+  tile_rc(static_cast<int>(w), r, c);
   i = kSymTile * I + r;
   j = kSymTile * J + c;
-  pad = c >= kSymTile || r >= sym_rows(n, I) || j >= n;
+  pad = r >= sym_rows(n, I) || j >= n;
 }
 
 __global__ void k_pack_sym(const double* __restrict__ A, long long stride, int lda, int n, double sign,
@@ -287,10 +288,11 @@ __global__ void k_pack_gen_t(const double* __restrict__ A, long long stride, int
     J = static_cast<int>(o2 / (rows * kSymLd));
     w = o2 - J * rows * kSymLd;
   }
-  const int r = static_cast<int>(w / kSymLd), c = static_cast<int>(w - static_cast<long long>(r) * kSymLd);
+  int r, c;
+  tile_rc(static_cast<int>(w), r, c);
   const int a = kSymTile * I + r, bcol = kSymTile * J + c;
   double v = 0.0;
-  if (c < kSymTile && r < sym_rows(nr, I) && bcol < nc)
+  if (r < sym_rows(nr, I) && bcol < nc)
     v = A[m * stride + static_cast<size_t>(r0 + bcol) * lda + a];
   out[off[m] + o] = v;
 }

@@ -87,13 +87,19 @@ struct SymCursor {
 // (SymWarp) through a ring of kSymStages buffers.  For a tile, lane 0
 // bulk-copies the tile and every lane copies (cp.async) the x entries of the
 // tile's column and row blocks, all completing on the buffer's mbarrier (count 1 + 32).
-// Per tile (I, J): direct part y_I += A_IJ x_J (lane = tile row), and for
-// J < I the transposed part y_J += A_IJ^T x_I (lane = tile column), four
-// independent partial sums per plane; y_I is accumulated along the row and
-// added at its end.  Waits are bounded; on expiry `status` is set and the
-// warp stops.
-template <class T, int NF>
-__global__ void __launch_bounds__(32 * kSymWarpsMax)
+// Per tile (I, J), on the FP64 tensor cores (mma m8n8k4) with the x entries
+// as an 8-column operand (column 2 f + p = plane p of field f, f < NF, the
+// rest zero): the direct part y_I += A_IJ x_J as D(32 x 8) = A (32 x 32)
+// X_J (32 x 8), and for J < I the transposed part y_J += A_IJ^T x_I as
+// D^T(8 x 32) = X_I^T (8 x 32) A_IJ (32 x 32), the tile read as the B
+// operand.  A lane's X fragment value is the same for both (X[4 kb + t][g]).
+// y_I is accumulated in the fragments along the tile row and added at its
+// end.  Waits are bounded; on expiry `status` is set and the warp stops.
+// MINB: blocks of kSymWarpsMax warps the register allocation must allow per
+// SM (1: as many registers as the code wants; 3: at most 80, a few spilled,
+// more resident warps -- DevModal::sym_regcap chooses).
+template <class T, int NF, int MINB>
+__global__ void __launch_bounds__(32 * kSymWarpsMax, MINB)
     k_psymv(const T* __restrict__ pack, const SymProblem* __restrict__ probs, const SymWarp* __restrict__ warps,
             int nwarps, const double* __restrict__ X, double* __restrict__ Y, int rstride, size_t fstride, int nz,
             int* status, unsigned long long wait_ns) {
@@ -158,9 +164,12 @@ __global__ void __launch_bounds__(32 * kSymWarpsMax)
     if (issued < W.count) prefetch();
   };
   for (int s = 0; s < kSymStages && s < W.count; ++s) issue(s);
-  double d0[NF], d1[NF];  // direct part of row 32 I + ln
+  // fragment coordinates: lane = 4 g + t
+  const int g = ln >> 2, t = ln & 3;
+  const bool xcol = g < 2 * NF;  // this lane's X column is a field's plane
+  double dd[4][2];               // direct part of the tile row, per 8-row block
 #pragma unroll
-  for (int f = 0; f < NF; ++f) d0[f] = d1[f] = 0.0;
+  for (int mb = 0; mb < 4; ++mb) dd[mb][0] = dd[mb][1] = 0.0;
   int done = 0;
   for (; done < W.count; ++done) {
     const int s = done % kSymStages;
@@ -170,84 +179,67 @@ __global__ void __launch_bounds__(32 * kSymWarpsMax)
     }
     const int n = cc.P.n, m = cc.P.mode, I = cc.I, J = cc.J;
     const bool two = nz > 1 && m > 0, sym = cc.P.ncol == 0;
+    const bool trans = sym && J < I;
     const double scale = cc.P.scale;
     const T* A = reinterpret_cast<const T*>(sm.tile[s]);
-    const double2* xs = sm.x[s];
-    const int h = sym_rows(n, I);
+    const double* xs = reinterpret_cast<const double*>(sm.x[s]);
+    const int h = sym_rows(n, I), hs = (h + 3) & ~3;  // rows of the tile, rows stored
     // output positions (column block for the transposed part, row block at a
     // row's end), loaded before the products to overlap their latency
     const bool row_end = cc.row_last() || done + 1 == W.count;
-    const int g_col = (sym && J < I) ? __ldg(cc.P.idx + kSymTile * J + ln) : 0;  // J < T - 1: a full tile column
+    const int g_col = trans ? __ldg(cc.P.idx + kSymTile * J + ln) : 0;  // J < T - 1: a full tile column
     const int g_row = (row_end && ln < h) ? __ldg(cc.P.idx + kSymTile * I + ln) : 0;
-    if (ln < h) {
-      const T* Ar = A + ln * kSymLd;
-      double p0[NF][4], p1[NF][4];
+    double tt[4][2];  // transposed part of this tile, per 8-column block
 #pragma unroll
-      for (int f = 0; f < NF; ++f)
+    for (int nb = 0; nb < 4; ++nb) tt[nb][0] = tt[nb][1] = 0.0;
 #pragma unroll
-        for (int u = 0; u < 4; ++u) p0[f][u] = p1[f][u] = 0.0;
+    for (int kb = 0; kb < kSymTile / 4; ++kb) {
+      // X fragments: column block (direct B operand), row block (transposed
+      // A operand); entry (4 kb + t, column g)
+      const int xo = (4 * kb + t) * NF * 2 + g;
+      const double bx = xcol ? xs[xo] : 0.0;
 #pragma unroll
-      for (int c = 0; c < kSymTile; ++c) {
-        const double a = static_cast<double>(Ar[c]);
-#pragma unroll
-        for (int f = 0; f < NF; ++f) {
-          const double2 x = xs[c * NF + f];
-          p0[f][c & 3] = fma(a, x.x, p0[f][c & 3]);
-          p1[f][c & 3] = fma(a, x.y, p1[f][c & 3]);
+      for (int mb = 0; mb < 4; ++mb) {
+        if (8 * mb < hs) {
+          const int r = 8 * mb + g;
+          const double a = r < hs ? static_cast<double>(A[tile_pos(r, 4 * kb + t)]) : 0.0;
+          dmma_8x8x4(dd[mb][0], dd[mb][1], a, bx);
         }
       }
+      if (trans && 4 * kb < hs) {
+        const double ax = xcol ? xs[kSymTile * NF * 2 + xo] : 0.0;
 #pragma unroll
-      for (int f = 0; f < NF; ++f) {
-        d0[f] += (p0[f][0] + p0[f][1]) + (p0[f][2] + p0[f][3]);
-        d1[f] += (p1[f][0] + p1[f][1]) + (p1[f][2] + p1[f][3]);
+        for (int nb = 0; nb < 4; ++nb) {
+          const double b = static_cast<double>(A[tile_pos(4 * kb + t, 8 * nb + g)]);
+          dmma_8x8x4(tt[nb][0], tt[nb][1], ax, b);
+        }
       }
     }
     double* Y0 = Y + static_cast<size_t>(2 * m) * rstride;
-    double* Y1 = Y0 + rstride;
-    if (sym && J < I) {
-      double p0[NF][4], p1[NF][4];
+    if (trans) {
+      // lane holds D^T[g][8 nb + 2 t + e]: plane g & 1 of field g >> 1 at
+      // column 8 nb + 2 t + e of the tile
 #pragma unroll
-      for (int f = 0; f < NF; ++f)
+      for (int nb = 0; nb < 4; ++nb)
 #pragma unroll
-        for (int u = 0; u < 4; ++u) p0[f][u] = p1[f][u] = 0.0;
-      if (h == kSymTile) {
-#pragma unroll
-        for (int r = 0; r < kSymTile; ++r) {
-          const double a = static_cast<double>(A[r * kSymLd + ln]);
-#pragma unroll
-          for (int f = 0; f < NF; ++f) {
-            const double2 x = xs[(kSymTile + r) * NF + f];
-            p0[f][r & 3] = fma(a, x.x, p0[f][r & 3]);
-            p1[f][r & 3] = fma(a, x.y, p1[f][r & 3]);
-          }
+        for (int e = 0; e < 2; ++e) {
+          const int gi = __shfl_sync(0xffffffffu, g_col, 8 * nb + 2 * t + e);
+          if (xcol && ((g & 1) == 0 || two))
+            atomicAdd(&Y0[(g & 1) * static_cast<size_t>(rstride) + (g >> 1) * fstride + gi], scale * tt[nb][e]);
         }
-      } else {
-        for (int r = 0; r < h; ++r) {
-          const double a = static_cast<double>(A[r * kSymLd + ln]);
-#pragma unroll
-          for (int f = 0; f < NF; ++f) {
-            const double2 x = xs[(kSymTile + r) * NF + f];
-            p0[f][0] = fma(a, x.x, p0[f][0]);
-            p1[f][0] = fma(a, x.y, p1[f][0]);
-          }
-        }
-      }
-#pragma unroll
-      for (int f = 0; f < NF; ++f) {
-        atomicAdd(&Y0[f * fstride + g_col], scale * ((p0[f][0] + p0[f][1]) + (p0[f][2] + p0[f][3])));
-        if (two) atomicAdd(&Y1[f * fstride + g_col], scale * ((p1[f][0] + p1[f][1]) + (p1[f][2] + p1[f][3])));
-      }
     }
     if (row_end) {
-      if (ln < h) {
+      // lane holds D[8 mb + g][2 t + e]: row 8 mb + g, plane e of field t
 #pragma unroll
-        for (int f = 0; f < NF; ++f) {
-          atomicAdd(&Y0[f * fstride + g_row], scale * d0[f]);
-          if (two) atomicAdd(&Y1[f * fstride + g_row], scale * d1[f]);
+      for (int mb = 0; mb < 4; ++mb) {
+        const int r = 8 * mb + g;
+        const int gi = __shfl_sync(0xffffffffu, g_row, r);
+        if (r < h && t < NF) {
+          atomicAdd(&Y0[t * fstride + gi], scale * dd[mb][0]);
+          if (two) atomicAdd(&Y0[rstride + t * fstride + gi], scale * dd[mb][1]);
         }
+        dd[mb][0] = dd[mb][1] = 0.0;
       }
-#pragma unroll
-      for (int f = 0; f < NF; ++f) d0[f] = d1[f] = 0.0;
     }
     __syncwarp();
     if (issued < W.count) issue(s);  // the buffer's reads are complete (syncwarp)
@@ -257,20 +249,30 @@ __global__ void __launch_bounds__(32 * kSymWarpsMax)
   for (int k = done; k < issued; ++k) mbar_wait(&sm.bar[k % kSymStages], (k / kSymStages) & 1);
 }
 
+template <int MINB>
+void configure_psymv_as() {
+  raise_smem_limit(reinterpret_cast<const void*>(k_psymv<double, 1, MINB>), sym_smem<1>(kSymWarpsMax));
+  raise_smem_limit(reinterpret_cast<const void*>(k_psymv<float, 1, MINB>), sym_smem<1>(kSymWarpsMax));
+  raise_smem_limit(reinterpret_cast<const void*>(k_psymv<double, 2, MINB>), sym_smem<2>(kSymWarpsMax));
+  raise_smem_limit(reinterpret_cast<const void*>(k_psymv<double, 3, MINB>), sym_smem<3>(kSymWarpsMax));
+}
+
 void configure_psymv() {
-  raise_smem_limit(reinterpret_cast<const void*>(k_psymv<double, 1>), sym_smem<1>(kSymWarpsMax));
-  raise_smem_limit(reinterpret_cast<const void*>(k_psymv<float, 1>), sym_smem<1>(kSymWarpsMax));
-  raise_smem_limit(reinterpret_cast<const void*>(k_psymv<double, 2>), sym_smem<2>(kSymWarpsMax));
-  raise_smem_limit(reinterpret_cast<const void*>(k_psymv<double, 3>), sym_smem<3>(kSymWarpsMax));
+  configure_psymv_as<1>();
+  configure_psymv_as<3>();
 }
 
 template <class T, int NF>
 void launch_psymv_as(const T* pack, const SymProblem* probs, const SymWarp* warps, int nwarps, const double* X,
                      double* Y, int rstride, size_t fstride, int nz, int* status, unsigned long long wait_ns,
-                     int wpb, cudaStream_t st) {
+                     int wpb, int regcap, cudaStream_t st) {
   const int blocks = (nwarps + wpb - 1) / wpb;
-  k_psymv<T, NF><<<blocks, 32 * wpb, sym_smem<NF>(wpb), st>>>(pack, probs, warps, nwarps, X, Y, rstride, fstride,
-                                                              nz, status, wait_ns);
+  if (regcap)
+    k_psymv<T, NF, 3><<<blocks, 32 * wpb, sym_smem<NF>(wpb), st>>>(pack, probs, warps, nwarps, X, Y, rstride,
+                                                                   fstride, nz, status, wait_ns);
+  else
+    k_psymv<T, NF, 1><<<blocks, 32 * wpb, sym_smem<NF>(wpb), st>>>(pack, probs, warps, nwarps, X, Y, rstride,
+                                                                   fstride, nz, status, wait_ns);
 }
 
 cudaError_t launch_psymv(const DevModal& S, const SymProblem* probs, const SymWarp* warps, int nwarps,
@@ -279,13 +281,13 @@ cudaError_t launch_psymv(const DevModal& S, const SymProblem* probs, const SymWa
   if (nwarps <= 0) return cudaSuccess;
   configure_psymv();
   if (fp32)
-    launch_psymv_as<float, 1>(S.l2_pack32, probs, warps, nwarps, X, Y, rstride, 0, nz, S.status, S.wait_ns, S.sym_warps, st);
+    launch_psymv_as<float, 1>(S.l2_pack32, probs, warps, nwarps, X, Y, rstride, 0, nz, S.status, S.wait_ns, S.sym_warps, S.sym_regcap, st);
   else if (nf == 3)
-    launch_psymv_as<double, 3>(S.l2_pack, probs, warps, nwarps, X, Y, rstride, fstride, nz, S.status, S.wait_ns, S.sym_warps, st);
+    launch_psymv_as<double, 3>(S.l2_pack, probs, warps, nwarps, X, Y, rstride, fstride, nz, S.status, S.wait_ns, S.sym_warps, S.sym_regcap, st);
   else if (nf == 2)
-    launch_psymv_as<double, 2>(S.l2_pack, probs, warps, nwarps, X, Y, rstride, fstride, nz, S.status, S.wait_ns, S.sym_warps, st);
+    launch_psymv_as<double, 2>(S.l2_pack, probs, warps, nwarps, X, Y, rstride, fstride, nz, S.status, S.wait_ns, S.sym_warps, S.sym_regcap, st);
   else
-    launch_psymv_as<double, 1>(S.l2_pack, probs, warps, nwarps, X, Y, rstride, 0, nz, S.status, S.wait_ns, S.sym_warps, st);
+    launch_psymv_as<double, 1>(S.l2_pack, probs, warps, nwarps, X, Y, rstride, 0, nz, S.status, S.wait_ns, S.sym_warps, S.sym_regcap, st);
   return cudaGetLastError();
 }
 
@@ -340,7 +342,8 @@ int twolevel_launches(const DevModal& S) {
 
 static int prob_ntiles(const SymProblem& P) { return P.ncol ? gen_ntiles(P.n, P.ncol) : sym_ntiles(P.n); }
 
-std::vector<SymWarp> sym_schedule(const std::vector<SymProblem>& probs, int device, int wpb, int occ_pct) {
+std::vector<SymWarp> sym_schedule(const std::vector<SymProblem>& probs, int device, int wpb, int occ_pct,
+                                  int regcap) {
   std::vector<SymWarp> out;
   long long total = 0;
   for (const auto& P : probs) total += prob_ntiles(P);
@@ -348,8 +351,9 @@ std::vector<SymWarp> sym_schedule(const std::vector<SymProblem>& probs, int devi
   int sms = 148, per_sm = 1;
   cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, device);
   configure_psymv();
-  if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_psymv<double, 1>, 32 * wpb, sym_smem<1>(wpb)) !=
-          cudaSuccess ||
+  const void* kern = regcap ? reinterpret_cast<const void*>(k_psymv<double, 1, 3>)
+                            : reinterpret_cast<const void*>(k_psymv<double, 1, 1>);
+  if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, kern, 32 * wpb, sym_smem<1>(wpb)) != cudaSuccess ||
       per_sm < 1)
     per_sm = 1;
   // warps of one full wave at the kernel's occupancy, times occ_pct / 100

@@ -33,6 +33,6 @@ int twolevel_launches(const DevModal& S);
 // grid of `wpb`-warp blocks that fills `device` occ_pct / 100 times at the
 // product kernel's occupancy (100: one full wave).
 std::vector<SymWarp> sym_schedule(const std::vector<SymProblem>& probs, int device, int wpb = 4,
-                                  int occ_pct = 100);
+                                  int occ_pct = 100, int regcap = 0);
 
 }  // namespace stx
