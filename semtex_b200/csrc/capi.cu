@@ -301,8 +301,14 @@ int stx_context_create(const char* session_path, const char* overrides, int devi
           area.push_back(E.area[t]);
         }
         // NaturalCBCp::sum is Natural::sum (src/condition.cpp:470-495); Mixed::sum
-        // adds K C w, the line value of an 'M' edge (:315-343)
-        kind.push_back(E.kind == 'H' || E.kind == 'M' ? 'N' : E.kind);
+        // adds K C w, the line value of an 'M' edge (:315-343); a computed
+        // outflow edge is essential for the pressure (EssentialCBCp) and
+        // natural for the velocities (NaturalCBCu), its values computed per
+        // step (src/bcmgr.cpp:416-431)
+        char k = E.kind;
+        if (k == 'H' || k == 'M') k = 'N';
+        if (k == 'O') k = c == 'p' ? 'D' : 'N';
+        kind.push_back(k);
       }
       d.edge_gid = upload(A, gid);
       d.edge_kind = upload(A, kind);
