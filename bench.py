@@ -324,6 +324,11 @@ def run_ours(args):
     session = make_session(d)
     t0 = time.perf_counter()
     over = {"STX_TWOLEVEL": 0} if args.solver == "band" else {}
+    tuning = {}
+    if not args.untuned and args.solver != "band":
+        from semtex_b200 import autotune
+        tuning = autotune.tuned_overrides(session, "c", w["lambda2"])
+        over.update(tuning)
     if args.mode_groups:
         over["STX_MODE_GROUPS"] = args.mode_groups
     ctx = S.Context(session, over or None, device=local)
@@ -437,6 +442,7 @@ def run_ours(args):
         "setup_s": setup_s, "families": ctx.families(),
         "gpu_launches": int(launches.value) * args.steps,
         "clocks": clocks, "cpu_baseline": cpu, "parity": parity,
+        "tuning": {"table": "semtex_b200/autotune_table.json", "tokens": tuning},
     }
     if args.dns_steps > 0 and ws == 1:
         line["mixed"] = run_mixed(ctx, sysm, F, args, flush, stream, dof)
@@ -444,7 +450,7 @@ def run_ours(args):
         line["dns"] = run_dns(args.dns_steps, 3, local, "c3", cb)
         line["dns_c3_dealiased"] = run_dns(args.dns_steps, 3, local, "c3d", cb)
         line["dns_c5"] = run_dns(args.dns_steps, 3, local, "c5", cb)
-        line["batch_c4"] = run_batch(args.dns_steps, 3, local)
+        line["batch_c4"] = run_batch(args.dns_steps, 3, local, not args.untuned)
     print(json.dumps(line))
     if ws > 1:
         torch.distributed.destroy_process_group()
@@ -580,7 +586,7 @@ def run_dns(steps, warmup=3, local=0, workload="c3", cpu_baseline=False):
     return out
 
 
-def run_batch(steps, warmup=3, local=0):
+def run_batch(steps, warmup=3, local=0, tuned=True):
     """Secondary measurement: the uneven batch (64 independent 2D Helmholtz
     problems, n x n quads with n uniform in 4..32, order N uniform in 6..12,
     lambda^2 log-uniform in [0.1, 100], Dirichlet zero, U[-1,1] forcing per
@@ -599,7 +605,11 @@ def run_batch(steps, warmup=3, local=0):
     items, ctxs, dof = [], [], 0
     for i, sp in enumerate(specs):
         path = sessions.helmholtz_session(os.path.join(d, f"p{i}"), sp["n"], sp["np"], lambda2=sp["lambda2"])
-        ctx = S.Context(path, device=local)
+        ov = None
+        if tuned:
+            from semtex_b200 import autotune
+            ov = autotune.tuned_overrides(path, "c", sp["lambda2"]) or None
+        ctx = S.Context(path, ov, device=local)
         x, y = ctx.mesh_coords()
         f, nu = sessions.forcing_per_unique_node(x, y, 1, sp["seed"])
         dof += nu
@@ -673,6 +683,8 @@ def main():
                          "batch c4); 0 skips them")
     ap.add_argument("--mode-groups", type=int, default=0,
                     help="Fourier-mode groups solved on parallel streams (0: library default)")
+    ap.add_argument("--untuned", action="store_true",
+                    help="ignore the autotuner's table (semtex_b200/autotune_table.json)")
     ap.add_argument("--solver", default="twolevel", choices=["twolevel", "band"],
                     help="band: the single banded-Cholesky skeleton solve (for comparison)")
     ap.add_argument("--workload", default="c2", choices=["c2", "dns", "dns_c5", "batch_c4"],
@@ -688,7 +700,7 @@ def main():
     elif args.workload == "batch_c4":
         import torch
         torch.cuda.set_device(0)
-        print(json.dumps(run_batch(max(1, args.dns_steps), args.warmup, 0)))
+        print(json.dumps(run_batch(max(1, args.dns_steps), args.warmup, 0, not args.untuned)))
     else:
         run_ours(args)
 

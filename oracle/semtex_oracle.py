@@ -672,12 +672,23 @@ def _sparspak_rcm(root, adj, deg):
     return perm[::-1]
 
 
+_O3_CACHE = {}
+
+
 def enumerate_o3(bmap):
     """`enumerate -O3` of a field without essential nodes (utility/
     enumerate.cpp:694-831, connectivSC :883-920, globalBandwidth :923-964):
     every node in turn as the RCM root, the first with the least global
     bandwidth kept.  bmap [nel, next] holds Mesh::buildMap numbers; returns
-    the renumbered map (the chosen root becomes the highest number)."""
+    the renumbered map (the chosen root becomes the highest number).  The
+    fields of one mesh often share a map: results are cached by map."""
+    key = (bmap.shape, np.ascontiguousarray(bmap, dtype=np.int64).tobytes())
+    if key not in _O3_CACHE:
+        _O3_CACHE[key] = _enumerate_o3(bmap)
+    return _O3_CACHE[key].copy()
+
+
+def _enumerate_o3(bmap):
     nel, nxt = bmap.shape
     nsolve = int(bmap.max()) + 1
     adj = [[] for _ in range(nsolve)]

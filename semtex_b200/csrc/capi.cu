@@ -838,6 +838,7 @@ int stx_modal_create(stx_context* ctx, char field, double lambda2, double beta, 
         if (wpb < 1 || wpb > 8) throw StxError(STX_EINVAL, "STX_SYM_WARPS must be in 1..8");
         if (occ < 10 || occ > 800) throw StxError(STX_EINVAL, "STX_SYM_OCC must be in 10..800");
         const int rcap = ctx->S.tokens.has("STX_SYM_REGCAP") ? (ctx->S.tokens.ivalue("STX_SYM_REGCAP") != 0) : 0;
+        if (wpb > 4 && !rcap) throw StxError(STX_EINVAL, "STX_SYM_WARPS above 4 needs STX_SYM_REGCAP = 1");
         d.sym_warps = wpb;
         d.sym_regcap = rcap;
         const std::vector<SymWarp> wp = sym_schedule(pp, ctx->device, wpb, occ, rcap),

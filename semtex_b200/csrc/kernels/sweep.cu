@@ -247,7 +247,7 @@ __device__ __forceinline__ void sym_entry(int n, long long o, int& i, int& j, bo
   tile_rc(static_cast<int>(w), r, c);
   i = kSymTile * I + r;
   j = kSymTile * J + c;
-  pad = r >= sym_rows(n, I) || j >= n;
+  pad = c >= kSymTile || r >= sym_rows(n, I) || j >= n;
 }
 
 __global__ void k_pack_sym(const double* __restrict__ A, long long stride, int lda, int n, double sign,
@@ -292,7 +292,7 @@ __global__ void k_pack_gen_t(const double* __restrict__ A, long long stride, int
   tile_rc(static_cast<int>(w), r, c);
   const int a = kSymTile * I + r, bcol = kSymTile * J + c;
   double v = 0.0;
-  if (r < sym_rows(nr, I) && bcol < nc)
+  if (c < kSymTile && r < sym_rows(nr, I) && bcol < nc)
     v = A[m * stride + static_cast<size_t>(r0 + bcol) * lda + a];
   out[off[m] + o] = v;
 }

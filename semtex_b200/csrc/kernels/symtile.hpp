@@ -2,13 +2,13 @@
 // two-level skeleton solve: the lower triangle of 32 x 32 tiles (I >= J),
 // tile-row-major, the last tile row only as tall as the matrix needs
 // (h = n - 32 (T - 1) rows, stored rounded up to a multiple of 4).  Diagonal
-// tiles hold both triangles; columns past n are zero.  Within a tile the
-// entries are stored by 4 x 4 quadrants, quadrant-row-major, each quadrant's
-// 16 entries consecutive (row-major inside: tile_pos).  The products read a
-// tile as FP64 tensor-core fragments (mma m8n8k4): an 8 x 4 fragment of the
-// tile (the direct product) and a 4 x 8 fragment (the transposed product)
-// are each two whole quadrants, so a warp's fragment load touches every
-// shared-memory bank once either way.  Offsets and sizes count entries;
+// tiles hold both triangles; columns past n are zero.  Within a tile, row r
+// occupies 33 entries (entry (r, c) at r*33 + c, the 33rd zero: tile_pos),
+// so that a warp reading a tile row (lanes over c) or a tile column (lanes
+// over r) touches every bank once and every address is a constant offset.
+// (A layout of 4 x 4 quadrants, which FP64 tensor-core fragments read
+// conflict-free, was measured slower: with one or two planes per tile the
+// m8n8k4 products use 2 of their 8 columns.)  Offsets and sizes count entries;
 // with doubles or floats alike every tile is a multiple of 16 bytes and
 // starts on a 16-byte boundary: one bulk copy each.
 #pragma once
@@ -18,16 +18,13 @@
 namespace stx {
 
 constexpr int kSymTile = 32;
-constexpr int kSymLd = kSymTile;  // entries per stored tile row
+constexpr int kSymLd = kSymTile + 1;  // entries per stored tile row
 
-// Entry (r, c) of a tile, and its inverse.
-__host__ __device__ inline int tile_pos(int r, int c) {
-  return (((r >> 2) * (kSymTile / 4) + (c >> 2)) << 4) + ((r & 3) << 2) + (c & 3);
-}
+// Entry (r, c) of a tile, and its inverse (c = 32: the zero padding entry).
+__host__ __device__ inline int tile_pos(int r, int c) { return r * kSymLd + c; }
 __host__ __device__ inline void tile_rc(int w, int& r, int& c) {
-  const int q = w >> 4, e = w & 15;
-  r = (q / (kSymTile / 4)) * 4 + (e >> 2);
-  c = (q % (kSymTile / 4)) * 4 + (e & 3);
+  r = w / kSymLd;
+  c = w - r * kSymLd;
 }
 
 __host__ __device__ inline int sym_tiles(int n) { return (n + kSymTile - 1) / kSymTile; }

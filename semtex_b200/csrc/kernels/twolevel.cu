@@ -87,19 +87,17 @@ struct SymCursor {
 // (SymWarp) through a ring of kSymStages buffers.  For a tile, lane 0
 // bulk-copies the tile and every lane copies (cp.async) the x entries of the
 // tile's column and row blocks, all completing on the buffer's mbarrier (count 1 + 32).
-// Per tile (I, J), on the FP64 tensor cores (mma m8n8k4) with the x entries
-// as an 8-column operand (column 2 f + p = plane p of field f, f < NF, the
-// rest zero): the direct part y_I += A_IJ x_J as D(32 x 8) = A (32 x 32)
-// X_J (32 x 8), and for J < I the transposed part y_J += A_IJ^T x_I as
-// D^T(8 x 32) = X_I^T (8 x 32) A_IJ (32 x 32), the tile read as the B
-// operand.  A lane's X fragment value is the same for both (X[4 kb + t][g]).
-// y_I is accumulated in the fragments along the tile row and added at its
-// end.  Waits are bounded; on expiry `status` is set and the warp stops.
-// MINB: blocks of kSymWarpsMax warps the register allocation must allow per
-// SM (1: as many registers as the code wants; 3: at most 80, a few spilled,
-// more resident warps -- DevModal::sym_regcap chooses).
-template <class T, int NF, int MINB>
-__global__ void __launch_bounds__(32 * kSymWarpsMax, MINB)
+// Per tile (I, J): direct part y_I += A_IJ x_J (lane = tile row), and for
+// J < I the transposed part y_J += A_IJ^T x_I (lane = tile column), four
+// independent partial sums per plane; y_I is accumulated along the row and
+// added at its end.  Waits are bounded; on expiry `status` is set and the
+// warp stops.  Two builds (DevModal::sym_regcap chooses): CAP 0, blocks of
+// up to 4 warps and the registers the code wants (no minimum block count:
+// giving one lets the compiler take up to 255); CAP 1, blocks of up to 8
+// warps and at most 80 registers (three such blocks per SM), a few spilled,
+// more resident warps.
+template <class T, int NF, int CAP>
+__global__ void __launch_bounds__(CAP ? 32 * kSymWarpsMax : 128, CAP ? 3 : 0)
     k_psymv(const T* __restrict__ pack, const SymProblem* __restrict__ probs, const SymWarp* __restrict__ warps,
             int nwarps, const double* __restrict__ X, double* __restrict__ Y, int rstride, size_t fstride, int nz,
             int* status, unsigned long long wait_ns) {
@@ -164,12 +162,9 @@ __global__ void __launch_bounds__(32 * kSymWarpsMax, MINB)
     if (issued < W.count) prefetch();
   };
   for (int s = 0; s < kSymStages && s < W.count; ++s) issue(s);
-  // fragment coordinates: lane = 4 g + t
-  const int g = ln >> 2, t = ln & 3;
-  const bool xcol = g < 2 * NF;  // this lane's X column is a field's plane
-  double dd[4][2];               // direct part of the tile row, per 8-row block
+  double d0[NF], d1[NF];  // direct part of row 32 I + ln
 #pragma unroll
-  for (int mb = 0; mb < 4; ++mb) dd[mb][0] = dd[mb][1] = 0.0;
+  for (int f = 0; f < NF; ++f) d0[f] = d1[f] = 0.0;
   int done = 0;
   for (; done < W.count; ++done) {
     const int s = done % kSymStages;
@@ -179,67 +174,84 @@ __global__ void __launch_bounds__(32 * kSymWarpsMax, MINB)
     }
     const int n = cc.P.n, m = cc.P.mode, I = cc.I, J = cc.J;
     const bool two = nz > 1 && m > 0, sym = cc.P.ncol == 0;
-    const bool trans = sym && J < I;
     const double scale = cc.P.scale;
     const T* A = reinterpret_cast<const T*>(sm.tile[s]);
-    const double* xs = reinterpret_cast<const double*>(sm.x[s]);
-    const int h = sym_rows(n, I), hs = (h + 3) & ~3;  // rows of the tile, rows stored
+    const double2* xs = sm.x[s];
+    const int h = sym_rows(n, I);
     // output positions (column block for the transposed part, row block at a
     // row's end), loaded before the products to overlap their latency
     const bool row_end = cc.row_last() || done + 1 == W.count;
-    const int g_col = trans ? __ldg(cc.P.idx + kSymTile * J + ln) : 0;  // J < T - 1: a full tile column
+    const int g_col = (sym && J < I) ? __ldg(cc.P.idx + kSymTile * J + ln) : 0;  // J < T - 1: a full tile column
     const int g_row = (row_end && ln < h) ? __ldg(cc.P.idx + kSymTile * I + ln) : 0;
-    double tt[4][2];  // transposed part of this tile, per 8-column block
+    if (ln < h) {
+      const T* Ar = A + ln * kSymLd;
+      double p0[NF][4], p1[NF][4];
 #pragma unroll
-    for (int nb = 0; nb < 4; ++nb) tt[nb][0] = tt[nb][1] = 0.0;
+      for (int f = 0; f < NF; ++f)
 #pragma unroll
-    for (int kb = 0; kb < kSymTile / 4; ++kb) {
-      // X fragments: column block (direct B operand), row block (transposed
-      // A operand); entry (4 kb + t, column g)
-      const int xo = (4 * kb + t) * NF * 2 + g;
-      const double bx = xcol ? xs[xo] : 0.0;
+        for (int u = 0; u < 4; ++u) p0[f][u] = p1[f][u] = 0.0;
 #pragma unroll
-      for (int mb = 0; mb < 4; ++mb) {
-        if (8 * mb < hs) {
-          const int r = 8 * mb + g;
-          const double a = r < hs ? static_cast<double>(A[tile_pos(r, 4 * kb + t)]) : 0.0;
-          dmma_8x8x4(dd[mb][0], dd[mb][1], a, bx);
+      for (int c = 0; c < kSymTile; ++c) {
+        const double a = static_cast<double>(Ar[c]);
+#pragma unroll
+        for (int f = 0; f < NF; ++f) {
+          const double2 x = xs[c * NF + f];
+          p0[f][c & 3] = fma(a, x.x, p0[f][c & 3]);
+          p1[f][c & 3] = fma(a, x.y, p1[f][c & 3]);
         }
       }
-      if (trans && 4 * kb < hs) {
-        const double ax = xcol ? xs[kSymTile * NF * 2 + xo] : 0.0;
 #pragma unroll
-        for (int nb = 0; nb < 4; ++nb) {
-          const double b = static_cast<double>(A[tile_pos(4 * kb + t, 8 * nb + g)]);
-          dmma_8x8x4(tt[nb][0], tt[nb][1], ax, b);
-        }
+      for (int f = 0; f < NF; ++f) {
+        d0[f] += (p0[f][0] + p0[f][1]) + (p0[f][2] + p0[f][3]);
+        d1[f] += (p1[f][0] + p1[f][1]) + (p1[f][2] + p1[f][3]);
       }
     }
     double* Y0 = Y + static_cast<size_t>(2 * m) * rstride;
-    if (trans) {
-      // lane holds D^T[g][8 nb + 2 t + e]: plane g & 1 of field g >> 1 at
-      // column 8 nb + 2 t + e of the tile
+    double* Y1 = Y0 + rstride;
+    if (sym && J < I) {
+      double p0[NF][4], p1[NF][4];
 #pragma unroll
-      for (int nb = 0; nb < 4; ++nb)
+      for (int f = 0; f < NF; ++f)
 #pragma unroll
-        for (int e = 0; e < 2; ++e) {
-          const int gi = __shfl_sync(0xffffffffu, g_col, 8 * nb + 2 * t + e);
-          if (xcol && ((g & 1) == 0 || two))
-            atomicAdd(&Y0[(g & 1) * static_cast<size_t>(rstride) + (g >> 1) * fstride + gi], scale * tt[nb][e]);
+        for (int u = 0; u < 4; ++u) p0[f][u] = p1[f][u] = 0.0;
+      if (h == kSymTile) {
+#pragma unroll
+        for (int r = 0; r < kSymTile; ++r) {
+          const double a = static_cast<double>(A[r * kSymLd + ln]);
+#pragma unroll
+          for (int f = 0; f < NF; ++f) {
+            const double2 x = xs[(kSymTile + r) * NF + f];
+            p0[f][r & 3] = fma(a, x.x, p0[f][r & 3]);
+            p1[f][r & 3] = fma(a, x.y, p1[f][r & 3]);
+          }
         }
+      } else {
+        for (int r = 0; r < h; ++r) {
+          const double a = static_cast<double>(A[r * kSymLd + ln]);
+#pragma unroll
+          for (int f = 0; f < NF; ++f) {
+            const double2 x = xs[(kSymTile + r) * NF + f];
+            p0[f][0] = fma(a, x.x, p0[f][0]);
+            p1[f][0] = fma(a, x.y, p1[f][0]);
+          }
+        }
+      }
+#pragma unroll
+      for (int f = 0; f < NF; ++f) {
+        atomicAdd(&Y0[f * fstride + g_col], scale * ((p0[f][0] + p0[f][1]) + (p0[f][2] + p0[f][3])));
+        if (two) atomicAdd(&Y1[f * fstride + g_col], scale * ((p1[f][0] + p1[f][1]) + (p1[f][2] + p1[f][3])));
+      }
     }
     if (row_end) {
-      // lane holds D[8 mb + g][2 t + e]: row 8 mb + g, plane e of field t
+      if (ln < h) {
 #pragma unroll
-      for (int mb = 0; mb < 4; ++mb) {
-        const int r = 8 * mb + g;
-        const int gi = __shfl_sync(0xffffffffu, g_row, r);
-        if (r < h && t < NF) {
-          atomicAdd(&Y0[t * fstride + gi], scale * dd[mb][0]);
-          if (two) atomicAdd(&Y0[rstride + t * fstride + gi], scale * dd[mb][1]);
+        for (int f = 0; f < NF; ++f) {
+          atomicAdd(&Y0[f * fstride + g_row], scale * d0[f]);
+          if (two) atomicAdd(&Y1[f * fstride + g_row], scale * d1[f]);
         }
-        dd[mb][0] = dd[mb][1] = 0.0;
       }
+#pragma unroll
+      for (int f = 0; f < NF; ++f) d0[f] = d1[f] = 0.0;
     }
     __syncwarp();
     if (issued < W.count) issue(s);  // the buffer's reads are complete (syncwarp)
@@ -249,17 +261,17 @@ __global__ void __launch_bounds__(32 * kSymWarpsMax, MINB)
   for (int k = done; k < issued; ++k) mbar_wait(&sm.bar[k % kSymStages], (k / kSymStages) & 1);
 }
 
-template <int MINB>
+template <int CAP>
 void configure_psymv_as() {
-  raise_smem_limit(reinterpret_cast<const void*>(k_psymv<double, 1, MINB>), sym_smem<1>(kSymWarpsMax));
-  raise_smem_limit(reinterpret_cast<const void*>(k_psymv<float, 1, MINB>), sym_smem<1>(kSymWarpsMax));
-  raise_smem_limit(reinterpret_cast<const void*>(k_psymv<double, 2, MINB>), sym_smem<2>(kSymWarpsMax));
-  raise_smem_limit(reinterpret_cast<const void*>(k_psymv<double, 3, MINB>), sym_smem<3>(kSymWarpsMax));
+  raise_smem_limit(reinterpret_cast<const void*>(k_psymv<double, 1, CAP>), sym_smem<1>(kSymWarpsMax));
+  raise_smem_limit(reinterpret_cast<const void*>(k_psymv<float, 1, CAP>), sym_smem<1>(kSymWarpsMax));
+  raise_smem_limit(reinterpret_cast<const void*>(k_psymv<double, 2, CAP>), sym_smem<2>(kSymWarpsMax));
+  raise_smem_limit(reinterpret_cast<const void*>(k_psymv<double, 3, CAP>), sym_smem<3>(kSymWarpsMax));
 }
 
 void configure_psymv() {
+  configure_psymv_as<0>();
   configure_psymv_as<1>();
-  configure_psymv_as<3>();
 }
 
 template <class T, int NF>
@@ -268,10 +280,10 @@ void launch_psymv_as(const T* pack, const SymProblem* probs, const SymWarp* warp
                      int wpb, int regcap, cudaStream_t st) {
   const int blocks = (nwarps + wpb - 1) / wpb;
   if (regcap)
-    k_psymv<T, NF, 3><<<blocks, 32 * wpb, sym_smem<NF>(wpb), st>>>(pack, probs, warps, nwarps, X, Y, rstride,
+    k_psymv<T, NF, 1><<<blocks, 32 * wpb, sym_smem<NF>(wpb), st>>>(pack, probs, warps, nwarps, X, Y, rstride,
                                                                    fstride, nz, status, wait_ns);
   else
-    k_psymv<T, NF, 1><<<blocks, 32 * wpb, sym_smem<NF>(wpb), st>>>(pack, probs, warps, nwarps, X, Y, rstride,
+    k_psymv<T, NF, 0><<<blocks, 32 * wpb, sym_smem<NF>(wpb), st>>>(pack, probs, warps, nwarps, X, Y, rstride,
                                                                    fstride, nz, status, wait_ns);
 }
 
@@ -351,8 +363,8 @@ std::vector<SymWarp> sym_schedule(const std::vector<SymProblem>& probs, int devi
   int sms = 148, per_sm = 1;
   cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, device);
   configure_psymv();
-  const void* kern = regcap ? reinterpret_cast<const void*>(k_psymv<double, 1, 3>)
-                            : reinterpret_cast<const void*>(k_psymv<double, 1, 1>);
+  const void* kern = regcap ? reinterpret_cast<const void*>(k_psymv<double, 1, 1>)
+                            : reinterpret_cast<const void*>(k_psymv<double, 1, 0>);
   if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, kern, 32 * wpb, sym_smem<1>(wpb)) != cudaSuccess ||
       per_sm < 1)
     per_sm = 1;

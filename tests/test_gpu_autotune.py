@@ -22,8 +22,8 @@ def _solve(p, ov, f):
 
 @pytest.mark.parametrize("ov", [{"STX_PATCH_CAP": 8}, {"STX_PATCH_CAP": 64}, {"STX_CHUNK": 8},
                                 {"STX_CHUNK": 3}, {"STX_MODE_GROUPS": 3}, {"STX_SYM_WARPS": 1},
-                                {"STX_SYM_WARPS": 8}, {"STX_SYM_OCC": 10}, {"STX_SYM_OCC": 400},
-                                {"STX_SYM_REGCAP": 1}])
+                                {"STX_SYM_WARPS": 8, "STX_SYM_REGCAP": 1}, {"STX_SYM_OCC": 10},
+                                {"STX_SYM_OCC": 400}, {"STX_SYM_REGCAP": 1}])
 def test_knobs_do_not_change_the_solution(tmp_path, ov):
     p = sessions.helmholtz_session(str(tmp_path / "k"), 8, 7, nz=8, lambda2=1.0, beta=1.0)
     f = np.random.default_rng(2).uniform(-1, 1, (8, 64, 7, 7))
