@@ -65,7 +65,7 @@ def test_outflow_ntime3_graph_and_checkpoint(tmp_path):
     # third-order steps, enough of them for the steady-step graph replay; the
     # outflow levels also travel in a checkpoint
     p = _channel(str(tmp_path / "ch3"), 4, 0.05, True)
-    txt = open(p).read().replace("N_TIME = 2", "N_TIME = 3").replace("N_STEP = 12", "N_STEP = 60")
+    txt = open(p).read().replace("N_TIME = 2", "N_TIME = 3").replace("N_STEP = 12", "N_STEP = 110")
     open(p, "w").write(txt)
     ctx = S.Context(p)
     funcs = S._user_functions(p)
@@ -74,7 +74,7 @@ def test_outflow_ntime3_graph_and_checkpoint(tmp_path):
     A.restart(ic, 0.0)
     A.advance(20)
     buf = A.checkpoint()
-    A.advance(40)
+    A.advance(90)   # the steady cycle (42 steps with pressure-BC and outflow levels) is captured
     gpu = {c: A.field(c) for c in ctx.fields}
     assert A.graph_info()[1] > 0   # steady steps were replayed as a graph
     A.close()
@@ -83,7 +83,7 @@ def test_outflow_ntime3_graph_and_checkpoint(tmp_path):
     B = S.DNS(ctx, 1)
     B.restart(ic, 0.0)
     B.restore(buf)
-    B.advance(40)
+    B.advance(90)
     cont = {c: B.field(c) for c in ctx.fields}
     scale = max(np.linalg.norm(gpu[c]) for c in "uvw")
     for c in "uvw":
