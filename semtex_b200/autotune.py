@@ -10,7 +10,9 @@ per full wave (STX_SYM_OCC, percent) and whether the products run their
 register-capped build (STX_SYM_REGCAP: more resident warps, a few spills).  ``tune`` measures them on the device
 by coordinate descent -- each knob in turn over its values with the others
 held at the best so far, the device time of stx_field_solve (CUDA events,
-median of several solves of a resident forcing) deciding -- and records every
+the least of several solves of a resident forcing: the mean moves between
+processes, e.g. with how two mode-group streams happen to overlap, the
+least time much less) deciding -- and records every
 trial and the winner in a JSON table keyed by the problem's shape.
 ``tuned_overrides`` returns the winner for a session from that table (empty
 when the shape was never tuned), for Context(..., overrides=...).
@@ -25,7 +27,6 @@ from __future__ import annotations
 import argparse
 import json
 import os
-import statistics
 
 import numpy as np
 
@@ -117,10 +118,10 @@ def _overrides(config: dict) -> dict:
     return {k: v for k, v in config.items() if v is not None}
 
 
-def solve_time_ms(session: str, field: str, lambda2: float, overrides: dict, reps: int = 7, device: int = 0,
+def solve_time_ms(session: str, field: str, lambda2: float, overrides: dict, reps: int = 11, device: int = 0,
                   seed: int = 1) -> float:
-    """Median device time (ms) of stx_field_solve with a resident random
-    forcing under `overrides` (a failed configuration: +inf)."""
+    """Least device time (ms) of `reps` stx_field_solve calls with a
+    resident random forcing under `overrides` (a failed configuration: +inf)."""
     import ctypes as C
     import torch
     from . import Context, FORWARD, ModalMatrixSys, StxError
@@ -151,10 +152,10 @@ def solve_time_ms(session: str, field: str, lambda2: float, overrides: dict, rep
     ok = sysm.status() == 0
     sysm.close()
     ctx.close()
-    return statistics.median(times) if ok else float("inf")
+    return min(times) if ok else float("inf")
 
 
-def tune(session: str, field: str, lambda2: float, space: dict = SPACE, reps: int = 7, device: int = 0,
+def tune(session: str, field: str, lambda2: float, space: dict = SPACE, reps: int = 11, device: int = 0,
          path: str | None = TABLE, label: str = "") -> dict:
     """Tune one shape on the device; record it in the table at `path` (None:
     do not record).  Returns the table entry."""
