@@ -296,8 +296,9 @@ int stx_dns_cfl(stx_dns* dns, double* inv_dt);
  * src/bcmgr.cpp:951-993), the alternating form's switch, forcing state (SFD
  * filter, sponge mask) and running averages, with step and time.  The
  * reference's Domain::dump / restart (src/domain.cpp:123-215) keep the fields
- * only and restart at first order; a loaded checkpoint continues exactly as
- * the uninterrupted run.  _size gives the bytes; _save fills a host buffer
+ * only and restart at first order; a loaded checkpoint continues as the
+ * uninterrupted run does (to round-off: the skeleton products sum with
+ * atomics).  _size gives the bytes; _save fills a host buffer
  * (synchronises); _load restores one into a DNS of the same session
  * (re-evaluates BCs at the restored time; STX_EINVAL for a buffer of another
  * layout). */
