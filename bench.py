@@ -586,6 +586,29 @@ def run_dns(steps, warmup=3, local=0, workload="c3", cpu_baseline=False):
     return out
 
 
+def dns_probe(workload):
+    """Two start-up and three steady steps of a DNS workload with the graph
+    replay off (every kernel a plain launch): the run the DNS traffic
+    profile captures."""
+    import semtex_b200 as S
+    from semtex_b200 import sessions
+    d = tempfile.mkdtemp()
+    p = dns_session(d, workload)
+    ctx = S.Context(p, {"STX_DNS_GRAPH": 0})
+    D = S.DNS(ctx, 1)
+    if workload == "c5":
+        x, y = ctx.mesh_coords()
+        ic = sessions.channel_initial(x, y, np.arange(ctx.nz) * 2 * np.pi / ctx.nz)
+    else:
+        funcs = S._user_functions(p)
+        ic = {c: ctx.evaluate(funcs[c], 0.0) for c in ctx.fields if c in funcs}
+    D.restart(ic, 0.0)
+    D.advance(5)
+    ctx.sync()
+    D.close()
+    ctx.close()
+
+
 def run_batch(steps, warmup=3, local=0, tuned=True):
     """Secondary measurement: the uneven batch (64 independent 2D Helmholtz
     problems, n x n quads with n uniform in 4..32, order N uniform in 6..12,
@@ -687,11 +710,16 @@ def main():
                     help="ignore the autotuner's table (semtex_b200/autotune_table.json)")
     ap.add_argument("--solver", default="twolevel", choices=["twolevel", "band"],
                     help="band: the single banded-Cholesky skeleton solve (for comparison)")
-    ap.add_argument("--workload", default="c2", choices=["c2", "dns", "dns_c5", "batch_c4"],
-                    help="dns / dns_c5 / batch_c4: run only that secondary measurement (one JSON line)")
+    ap.add_argument("--workload", default="c2",
+                    choices=["c2", "dns", "dns_c5", "batch_c4", "dns_probe_c3", "dns_probe_c5"],
+                    help="dns / dns_c5 / batch_c4: run only that secondary measurement (one JSON line); "
+                         "dns_probe_c3 / _c5: 2 start-up + 3 steady steps with graph replay off, nothing "
+                         "timed (a run to profile every kernel of a step)")
     args = ap.parse_args()
     if args.impl == "reference":
         run_reference(args)
+    elif args.workload.startswith("dns_probe_"):
+        dns_probe(args.workload[len("dns_probe_"):])
     elif args.workload in ("dns", "dns_c5"):
         import torch
         torch.cuda.set_device(0)
