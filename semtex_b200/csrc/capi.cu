@@ -993,10 +993,15 @@ int stx_field_solve(stx_modal* sys, const double* d_forcing, double* d_unknown, 
         cuda_check(cudaEventRecord(ctx->aux_ev[0], ctx->stream), "fork");
         for (size_t k = 1; k < groups.size(); ++k)
           cuda_check(cudaStreamWaitEvent(ctx->aux[k - 1], ctx->aux_ev[0], 0), "fork wait");
-        for (size_t k = 0; k < groups.size(); ++k)
+        const bool stag = ctx->stagger();
+        if (stag) ctx->ensure_stagger(groups.size());
+        for (size_t k = 0; k < groups.size(); ++k) {
+          cudaStream_t sk = k ? ctx->aux[k - 1] : ctx->stream;
+          if (stag && k) cuda_check(cudaStreamWaitEvent(sk, ctx->stagger_ev[k - 1], 0), "stagger wait");
           cuda_check(helmholtz_direct_solve(ctx->dg, F.dn, groups[k], d_forcing, d_unknown, F.d_lines, F.nline,
-                                            work, k ? ctx->aux[k - 1] : ctx->stream),
+                                            work, sk, nullptr, stag ? ctx->stagger_ev[k] : nullptr),
                      "direct solve");
+        }
         for (size_t k = 1; k < groups.size(); ++k) {
           cuda_check(cudaEventRecord(ctx->aux_ev[k], ctx->aux[k - 1]), "join");
           cuda_check(cudaStreamWaitEvent(ctx->stream, ctx->aux_ev[k], 0), "join wait");
@@ -1057,10 +1062,15 @@ int stx_field_solve_multi(stx_modal* const* systems, int n, const double* const*
       cuda_check(cudaEventRecord(ctx->aux_ev[0], ctx->stream), "fork");
       for (size_t k = 1; k < groups.size(); ++k)
         cuda_check(cudaStreamWaitEvent(ctx->aux[k - 1], ctx->aux_ev[0], 0), "fork wait");
-      for (size_t k = 0; k < groups.size(); ++k)
+      const bool stag = ctx->stagger();
+      if (stag) ctx->ensure_stagger(groups.size());
+      for (size_t k = 0; k < groups.size(); ++k) {
+        cudaStream_t sk = k ? ctx->aux[k - 1] : ctx->stream;
+        if (stag && k) cuda_check(cudaStreamWaitEvent(sk, ctx->stagger_ev[k - 1], 0), "stagger wait");
         cuda_check(helmholtz_direct_solve_fields(ctx->dg, N.data(), groups[k], d_forcing, d_unknown, lines.data(),
-                                                 nline.data(), n, work, k ? ctx->aux[k - 1] : ctx->stream),
+                                                 nline.data(), n, work, sk, stag ? ctx->stagger_ev[k] : nullptr),
                    "multi-field solve");
+      }
       for (size_t k = 1; k < groups.size(); ++k) {
         cuda_check(cudaEventRecord(ctx->aux_ev[k], ctx->aux[k - 1]), "join");
         cuda_check(cudaStreamWaitEvent(ctx->stream, ctx->aux_ev[k], 0), "join wait");

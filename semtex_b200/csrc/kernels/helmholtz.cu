@@ -939,7 +939,7 @@ int helmholtz_direct_launches(const DevNumbering& N, const DevModal& S, int np) 
 
 cudaError_t helmholtz_direct_solve(const DevGeom& g, const DevNumbering& N, const DevModal& S,
                                    const double* F, double* U, const double* lines, int nline,
-                                   double* work, cudaStream_t st, cudaEvent_t* ev) {
+                                   double* work, cudaStream_t st, cudaEvent_t* ev, cudaEvent_t after_condense) {
   const int rstride = (N.nglobal + 31) / 32 * 32;
   double* R = work;
   double* G = work + static_cast<size_t>(rstride) * g.nz;
@@ -982,6 +982,7 @@ cudaError_t helmholtz_direct_solve(const DevGeom& g, const DevNumbering& N, cons
     k_natural<<<grid, 128, 0, st>>>(g, N, lines, nline, R, rstride, nz, k0);
   }
   if (ev) cudaEventRecord(ev[1], st);
+  if (after_condense) cudaEventRecord(after_condense, st);
   const SweepPlan plan = S.l2 ? SweepPlan() : sweep_plan(S.nbp, S.nband);
   const double* Rsol = R;  // skeleton solution
   if (S.l2) {
@@ -1045,7 +1046,8 @@ size_t helmholtz_fields_workspace_doubles(const DevGeom& g, const DevNumbering& 
 
 cudaError_t helmholtz_direct_solve_fields(const DevGeom& g, const DevNumbering* const* N, const DevModal& S,
                                           const double* const* F, double* const* U, const double* const* lines,
-                                          const int* nline, int nf, double* work, cudaStream_t st) {
+                                          const int* nline, int nf, double* work, cudaStream_t st,
+                                          cudaEvent_t after_condense) {
   if (nf < 1 || nf > 3 || !helmholtz_fields_supported(g, *N[0], S)) return cudaErrorInvalidValue;
   const int rstride = (N[0]->nglobal + 31) / 32 * 32;
   const int nz = g.nz;
@@ -1075,6 +1077,7 @@ cudaError_t helmholtz_direct_solve_fields(const DevGeom& g, const DevNumbering* 
       k_natural<<<grid, 128, 0, st>>>(g, *N[f], lines[f], nline[f], Rf, rstride, nz, k0);
     }
   }
+  if (after_condense) cudaEventRecord(after_condense, st);
   err = twolevel_solve_fields(S, g, *N[0], R, Y, fs, nf, rstride, nz, st);
   if (err != cudaSuccess) return err;
   for (int f = 0; f < nf; ++f)

@@ -25,7 +25,7 @@ size_t helmholtz_workspace_doubles(const DevGeom& g, const DevNumbering& N, cons
 cudaError_t helmholtz_direct_solve(const DevGeom& g, const DevNumbering& N, const DevModal& S,
                                    const double* F, double* U, const double* lines, int nline,
                                    double* work, cudaStream_t st,
-                                   cudaEvent_t* phase_events = nullptr);
+                                   cudaEvent_t* phase_events = nullptr, cudaEvent_t after_condense = nullptr);
 
 // The direct solve of nf (1..3) fields whose systems share S (the same
 // matrices: equal constants and numbering; each field its own forcing, BC
@@ -37,7 +37,8 @@ bool helmholtz_fields_supported(const DevGeom& g, const DevNumbering& N, const D
 size_t helmholtz_fields_workspace_doubles(const DevGeom& g, const DevNumbering& N, int nf);
 cudaError_t helmholtz_direct_solve_fields(const DevGeom& g, const DevNumbering* const* N, const DevModal& S,
                                           const double* const* F, double* const* U, const double* const* lines,
-                                          const int* nline, int nf, double* work, cudaStream_t st);
+                                          const int* nline, int nf, double* work, cudaStream_t st,
+                                          cudaEvent_t after_condense = nullptr);
 
 // Number of kernel launches one direct solve issues.
 int helmholtz_direct_launches(const DevNumbering& N, const DevModal& S, int np);

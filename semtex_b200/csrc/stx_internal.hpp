@@ -138,6 +138,20 @@ struct stx_context {
   // that fork them from `stream` and join them back.
   std::vector<cudaStream_t> aux;
   std::vector<cudaEvent_t> aux_ev;  // [0] fork, [i] join of aux[i - 1]
+  // [k]: mode group k has finished its element condensation; group k + 1
+  // starts after it (token STX_STAGGER, default 1), so that one group's
+  // element phase meets the other's skeleton products instead of competing
+  // with its element phase
+  std::vector<cudaEvent_t> stagger_ev;
+  bool stagger() const { return !S.tokens.has("STX_STAGGER") || S.tokens.ivalue("STX_STAGGER") != 0; }
+  void ensure_stagger(size_t n) {
+    while (stagger_ev.size() < n) {
+      cudaEvent_t e;
+      if (cudaEventCreateWithFlags(&e, cudaEventDisableTiming) != cudaSuccess)
+        throw std::runtime_error("event creation failed");
+      stagger_ev.push_back(e);
+    }
+  }
   void ensure_aux(size_t n) {
     if (aux_ev.empty()) {
       aux_ev.resize(1);
@@ -165,6 +179,7 @@ struct stx_context {
   ~stx_context() {
     for (auto s : aux) cudaStreamDestroy(s);
     for (auto e : aux_ev) cudaEventDestroy(e);
+    for (auto e : stagger_ev) cudaEventDestroy(e);
     if (d_work) cudaFree(d_work);
     if (d_scratch) cudaFree(d_scratch);
     if (h_flags) cudaFreeHost(h_flags);
