@@ -231,6 +231,16 @@ int stx_transform(stx_context* ctx, double* d_data, int sign);
  * physical-space solution out.  Synchronises. */
 int stx_elliptic_solve_host(stx_modal* sys, const double* h_forcing, double* h_solution);
 
+/* n whole elliptic solves from host memory, as stx_elliptic_solve_host does
+ * each, pipelined: the forcing of solve i + 1 is copied in and the solution
+ * of solve i - 1 copied out while solve i runs (two device buffer sets, one
+ * copy stream each way).  Host buffers should be pinned (cudaHostAlloc) for
+ * the copies to overlap.  Synchronises; the device status words are read
+ * once at the end.  No counterpart in the reference (one elliptic run is one
+ * solve). */
+int stx_elliptic_solve_host_batch(stx_modal* sys, int n, const double* const* h_forcing,
+                                  double* const* h_solution);
+
 /* The cudaStream_t all of the context's device work runs on. */
 int stx_context_stream(const stx_context* ctx, void** stream);
 

@@ -27,7 +27,7 @@ from .fieldfile import read_field, write_field
 
 DIRECT, JACPCG, MIXED = STX_DIRECT, STX_JACPCG, STX_MIXED
 
-__all__ = ["Context", "ModalMatrixSys", "Field", "DNS", "Batch", "expression", "svv", "numbering", "element_matrix", "solve_multi", "elliptic", "dns", "read_field",
+__all__ = ["Context", "ModalMatrixSys", "Field", "DNS", "Batch", "expression", "svv", "numbering", "element_matrix", "solve_multi", "solve_host_batch", "elliptic", "dns", "read_field",
            "write_field", "FORWARD", "INVERSE", "DIRECT", "JACPCG", "MIXED", "StxError"]
 
 
@@ -230,6 +230,31 @@ class ModalMatrixSys:
         check(lib().stx_elliptic_solve_host(self._h, C.c_void_p(f.ctypes.data),
                                             C.c_void_p(out.ctypes.data)))
         return out
+
+
+def solve_host_batch(system: "ModalMatrixSys", forcings, solutions):
+    """Whole elliptic solves of several host forcings, copies overlapped with
+    the solves (stx_elliptic_solve_host_batch).  forcings / solutions are
+    sequences of [nz, nel, np, np] float64 arrays (pinned host memory, e.g.
+    torch tensors from pin_memory(), lets the copies overlap) or raw host
+    addresses (int)."""
+    n = len(forcings)
+    if len(solutions) != n:
+        raise ValueError("as many solutions as forcings")
+
+    def addr(a):
+        if isinstance(a, int):
+            return a
+        if hasattr(a, "data_ptr"):
+            return a.data_ptr()
+        if not (isinstance(a, np.ndarray) and a.dtype == np.float64 and a.flags.c_contiguous):
+            raise ValueError("forcings and solutions must be C-contiguous float64 arrays")
+        return a.ctypes.data
+
+    fin = (C.c_void_p * n)(*[addr(a) for a in forcings])
+    fout = (C.c_void_p * n)(*[addr(a) for a in solutions])
+    check(lib().stx_elliptic_solve_host_batch(system.handle, n, fin, fout))
+    return solutions
 
 
 def solve_multi(systems, forcings, unknowns):

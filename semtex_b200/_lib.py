@@ -64,6 +64,7 @@ SIGNATURES = {
     "stx_dns_state": (_i, [_p, _pi, _pd]),
     "stx_dns_field_ptr": (_i, [_p, C.c_char, C.POINTER(_p)]),
     "stx_dns_system": (_i, [_p, C.c_char, C.POINTER(_p)]),
+    "stx_elliptic_solve_host_batch": (_i, [_p, _i, C.POINTER(_p), C.POINTER(_p)]),
     "stx_dns_checkpoint_size": (_i, [_p, C.POINTER(C.c_ulonglong)]),
     "stx_dns_checkpoint_save": (_i, [_p, _p, C.c_ulonglong]),
     "stx_dns_checkpoint_load": (_i, [_p, _p, C.c_ulonglong]),

@@ -1228,6 +1228,69 @@ int stx_elliptic_solve_host(stx_modal* sys, const double* h_forcing, double* h_s
   });
 }
 
+int stx_elliptic_solve_host_batch(stx_modal* sys, int n, const double* const* h_forcing,
+                                  double* const* h_solution) {
+  return guarded([&] {
+    if (!sys || n < 0 || (n && (!h_forcing || !h_solution))) throw StxError(STX_EINVAL, "bad argument");
+    for (int i = 0; i < n; ++i)
+      if (!h_forcing[i] || !h_solution[i]) throw StxError(STX_EINVAL, "null host buffer");
+    if (n == 0) return;
+    stx_context* ctx = sys->ctx;
+    const Mesh& M = ctx->M;
+    cudaSetDevice(ctx->device);
+    const size_t nplane = M.nplane, ps = M.plane_size, nz = M.nz;
+    const size_t set = 2 * ps * nz;  // forcing and solution planes of one set
+    ctx->ensure_pipeline(set);
+    const double tol = ctx->S.tokens.value("TOL_REL");
+    const int smax = ctx->S.tokens.ivalue("STEP_MAX");
+    for (int i = 0; i < n; ++i) {
+      const int b = i & 1;
+      double* dF = ctx->d_io2 + set * b;
+      double* dU = dF + ps * nz;
+      // in: set b's forcing is free once solve i - 2 has run
+      cuda_check(cudaStreamWaitEvent(ctx->s_h2d, ctx->ev_comp[b], 0), "wait");
+      cuda_check(cudaMemcpy2DAsync(dF, sizeof(double) * ps, h_forcing[i], sizeof(double) * nplane,
+                                   sizeof(double) * nplane, nz, cudaMemcpyHostToDevice, ctx->s_h2d),
+                 "forcing h2d");
+      cuda_check(cudaEventRecord(ctx->ev_in[b], ctx->s_h2d), "record");
+      // solve: after the forcing landed and set b's solution was read out
+      cuda_check(cudaStreamWaitEvent(ctx->stream, ctx->ev_in[b], 0), "wait");
+      cuda_check(cudaStreamWaitEvent(ctx->stream, ctx->ev_out[b], 0), "wait");
+      cuda_check(z_transform(dF, M.nz, M.plane_size, STX_FORWARD, ctx->d_twiddle, nullptr, ctx->stream),
+                 "forward transform");
+      if (nz > 1) {
+        cuda_check(cudaMemsetAsync(dF + ps, 0, sizeof(double) * ps, ctx->stream), "nyquist");
+        cuda_check(cudaMemsetAsync(dU + ps, 0, sizeof(double) * ps, ctx->stream), "zero nyquist");
+      }
+      const int rc = stx_field_solve(sys, dF, dU, tol, smax, nullptr);
+      if (rc != STX_OK) throw StxError(rc, g_last_error);
+      cuda_check(z_transform(dU, M.nz, M.plane_size, STX_INVERSE, ctx->d_twiddle, nullptr, ctx->stream),
+                 "inverse transform");
+      cuda_check(cudaEventRecord(ctx->ev_comp[b], ctx->stream), "record");
+      // out
+      cuda_check(cudaStreamWaitEvent(ctx->s_d2h, ctx->ev_comp[b], 0), "wait");
+      cuda_check(cudaMemcpy2DAsync(h_solution[i], sizeof(double) * nplane, dU, sizeof(double) * ps,
+                                   sizeof(double) * nplane, nz, cudaMemcpyDeviceToHost, ctx->s_d2h),
+                 "solution d2h");
+      cuda_check(cudaEventRecord(ctx->ev_out[b], ctx->s_d2h), "record");
+    }
+    int* fl = ctx->flags();
+    fl[0] = fl[1] = 0;
+    if (sys->store->dm.status)
+      cuda_check(cudaMemcpyAsync(&fl[0], sys->store->dm.status, sizeof(int), cudaMemcpyDeviceToHost, ctx->stream),
+                 "status d2h");
+    if (const int* ft = fft_timeout_address())
+      cuda_check(cudaMemcpyAsync(&fl[1], ft, sizeof(int), cudaMemcpyDeviceToHost, ctx->stream), "status d2h");
+    cuda_check(cudaStreamSynchronize(ctx->stream), "sync");
+    cuda_check(cudaStreamSynchronize(ctx->s_d2h), "sync");
+    if (fl[0]) {
+      const char* where = fl[0] == 1 ? "banded sweep" : fl[0] == 3 ? "element kernel" : "packed skeleton product";
+      throw StxError(STX_ECUDA, std::string(where) + ": a bounded wait for a bulk copy expired");
+    }
+    if (fl[1]) throw StxError(STX_ECUDA, "z-FFT: a bounded wait for a bulk copy expired");
+  });
+}
+
 int stx_context_stream(const stx_context* ctx, void** stream) {
   return guarded([&] {
     if (!ctx || !stream) throw StxError(STX_EINVAL, "null argument");
