@@ -37,7 +37,7 @@ SPACE = {
     "STX_PATCH_CAP": [None, 8, 16, 36, 64],
     "STX_CHUNK": [None, 16, 8],
     "STX_MODE_GROUPS": [None, 1, 3, 4],
-    "STX_STAGGER": [None, 0],
+    "STX_STAGGER": [None, 1],
     "STX_SYM_REGCAP": [None, 1],
     "STX_SYM_WARPS": [None, 2, 8],
     "STX_SYM_OCC": [None, 50, 200],
