@@ -173,16 +173,19 @@ def tune(session: str, field: str, lambda2: float, space: dict = SPACE, reps: in
     return entry
 
 
-def tune_benchmark_workloads(path: str = TABLE, device: int = 0):
+def tune_benchmark_workloads(path: str = TABLE, device: int = 0, only: str | None = None):
     """Tune the benchmark's Helmholtz workloads into the table: the batched
     2D x Fourier solve (16x16 quads, N_P=11, N_Z=64) and each problem of the
     uneven batch (64 problems, seed 20261203)."""
     import tempfile
     from . import sessions
     with tempfile.TemporaryDirectory() as d:
-        p = sessions.helmholtz_session(os.path.join(d, "c2"), 16, 11, nz=64, lambda2=1.0, beta=1.0)
-        e = tune(p, "c", 1.0, device=device, path=path, label="c2")
-        print("c2", json.dumps({k: e[k] for k in ("best", "best_ms", "default_ms")}), flush=True)
+        if only in (None, "c2"):
+            p = sessions.helmholtz_session(os.path.join(d, "c2"), 16, 11, nz=64, lambda2=1.0, beta=1.0)
+            e = tune(p, "c", 1.0, device=device, path=path, label="c2")
+            print("c2", json.dumps({k: e[k] for k in ("best", "best_ms", "default_ms")}), flush=True)
+        if only not in (None, "c4"):
+            return
         seen = set()
         for i, sp in enumerate(sessions.uneven_batch()):
             p = sessions.helmholtz_session(os.path.join(d, f"p{i}"), sp["n"], sp["np"], lambda2=sp["lambda2"])
@@ -202,9 +205,10 @@ def main():
     ap.add_argument("--label", default="")
     ap.add_argument("--table", default=TABLE)
     ap.add_argument("--benchmark", action="store_true", help="tune the benchmark's Helmholtz workloads")
+    ap.add_argument("--only", choices=["c2", "c4"], help="with --benchmark: one of the two workloads")
     a = ap.parse_args()
     if a.benchmark:
-        tune_benchmark_workloads(a.table)
+        tune_benchmark_workloads(a.table, only=a.only)
         return
     e = tune(a.session, a.field, a.lambda2, path=a.table, label=a.label)
     print(json.dumps({k: e[k] for k in ("best", "best_ms", "default_ms")}))
