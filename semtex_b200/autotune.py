@@ -36,6 +36,7 @@ TABLE = os.path.join(os.path.dirname(os.path.abspath(__file__)), "autotune_table
 SPACE = {
     "STX_PATCH_CAP": [None, 8, 16, 36, 64],
     "STX_CHUNK": [None, 16, 8],
+    "STX_ELEM_TWOBLOCK": [None, 1],
     "STX_MODE_GROUPS": [None, 1, 3, 4],
     "STX_STAGGER": [None, 1],
     "STX_SYM_REGCAP": [None, 1],

@@ -622,6 +622,7 @@ int stx_modal_create(stx_context* ctx, char field, double lambda2, double beta, 
       d.nfamily = M.nfamily;
       d.sym_warps = 4;
       d.sym_regcap = 0;
+      d.elem_twoblock = ctx->S.tokens.has("STX_ELEM_TWOBLOCK") && ctx->S.tokens.ivalue("STX_ELEM_TWOBLOCK") != 0;
       // bound of the kernels' bounded waits (token STX_WAIT_NS, default 2 s;
       // 0: one non-blocking probe, which a copy issued just before misses --
       // the error path's tests use it)

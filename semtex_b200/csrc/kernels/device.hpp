@@ -98,6 +98,7 @@ struct DevModal {
   int* status;                    // device status word (0 = ok)
   int sym_warps;                  // warps per block of the packed products (token STX_SYM_WARPS)
   int sym_regcap;                 // 1: their register-capped build (token STX_SYM_REGCAP)
+  int elem_twoblock;              // 1: element kernels split rows to run two blocks per SM (STX_ELEM_TWOBLOCK)
   unsigned long long wait_ns;     // bound of the element and skeleton kernels' first
                                   // wait per copy (token STX_WAIT_NS, default 2 s)
   const double* pc;               // JACPCG: [nmodes][npts]

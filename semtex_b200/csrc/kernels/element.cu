@@ -547,9 +547,12 @@ ElementPlan element_plan(const DevGeom& g, const DevModal& S, bool lift) {
     threads = 32 * warps;
     return (rows + 7) / 8 * ncg <= warps && smem <= cap;
   };
-  // per kernel: the two-block tier only when it needs no row split
+  // per kernel: the two-block tier only when it needs no row split, unless
+  // S.elem_twoblock asks for it with row blocks (each gathers every column
+  // of its chunk: more blocks and two per SM, for more gather traffic)
   auto choose = [&](int nrow, int ld, int& rows, int& nrb, int& threads, size_t& smem) {
-    if (fit(nrow, ld, kMaxWarps / 2, 113 * 1024, rows, nrb, threads, smem) && nrb == 1) return true;
+    if (fit(nrow, ld, kMaxWarps / 2, 113 * 1024, rows, nrb, threads, smem) && (nrb == 1 || S.elem_twoblock))
+      return true;
     return fit(nrow, ld, kMaxWarps, 227 * 1024, rows, nrb, threads, smem);
   };
   P.ok = choose(g.next, S.eb_ld, P.cond_rows, P.cond_rb, P.cond_threads, P.cond_smem) &&

@@ -32,6 +32,18 @@ def test_knobs_do_not_change_the_solution(tmp_path, ov):
     assert np.linalg.norm(got - ref) <= 1e-12 * np.linalg.norm(ref)
 
 
+@pytest.mark.parametrize("ov", [{"STX_ELEM_TWOBLOCK": 1}, {"STX_ELEM_TWOBLOCK": 1, "STX_CHUNK": 16},
+                                {"STX_STAGGER": 1}])
+def test_element_tiers_do_not_change_the_solution(tmp_path, ov):
+    # N_P = 11 with 32-element chunks: the recovery's operator rows exceed the
+    # two-block tier unless split into row blocks
+    p = sessions.helmholtz_session(str(tmp_path / "t"), 6, 11, nz=4, lambda2=1.0, beta=1.0)
+    f = np.random.default_rng(3).uniform(-1, 1, (4, 36, 11, 11))
+    ref = _solve(p, {}, f)
+    got = _solve(p, ov, f)
+    assert np.linalg.norm(got - ref) <= 1e-12 * np.linalg.norm(ref)
+
+
 def test_tune_records_winner(tmp_path):
     p = sessions.helmholtz_session(str(tmp_path / "t"), 8, 7, nz=8, lambda2=1.0, beta=1.0)
     table = str(tmp_path / "table.json")
