@@ -97,6 +97,7 @@ def coordinate_descent(measure, space: dict = SPACE, rounds: int = 1):
     config maps knob -> value (None = library default, left out of the
     overrides).  Returns (best config, best time, trials [(config, time)])."""
     best = {k: v[0] for k, v in space.items()}
+    measure(dict(best))  # discarded: the first solves of a run start on an idle GPU
     best_t = measure(dict(best))
     trials = [(dict(best), best_t)]
     for _ in range(rounds):

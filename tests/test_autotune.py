@@ -19,7 +19,7 @@ def test_coordinate_descent_finds_separable_minimum():
     assert best == {"a": 2, "b": 20, "c": None}
     assert t == 0.75
     assert trials[0][0] == {"a": None, "b": None, "c": None}
-    assert len(trials) == len(calls)
+    assert len(trials) == len(calls) - 1   # the first measurement warms the device up
 
 
 def test_failed_configurations_are_skipped():
