@@ -635,15 +635,15 @@ def run_batch(steps, warmup=3, local=0, tuned=True):
     from semtex_b200._lib import lib
     d = tempfile.mkdtemp()
     specs = sessions.uneven_batch()
+    batch_tuning = {}
+    if tuned:
+        from semtex_b200 import autotune
+        batch_tuning = autotune.tuned_batch_overrides(specs)
     t0 = time.perf_counter()
     items, ctxs, dof = [], [], 0
     for i, sp in enumerate(specs):
         path = sessions.helmholtz_session(os.path.join(d, f"p{i}"), sp["n"], sp["np"], lambda2=sp["lambda2"])
-        ov = None
-        if tuned:
-            from semtex_b200 import autotune
-            ov = autotune.tuned_overrides(path, "c", sp["lambda2"]) or None
-        ctx = S.Context(path, ov, device=local)
+        ctx = S.Context(path, batch_tuning or None, device=local)
         x, y = ctx.mesh_coords()
         f, nu = sessions.forcing_per_unique_node(x, y, 1, sp["seed"])
         dof += nu
@@ -693,7 +693,7 @@ def run_batch(steps, warmup=3, local=0, tuned=True):
            "unit": "DOF/s", "ms_per_step": ms_graph, "steps": steps,
            "per_problem_calls": {"value": dof / (ms_loop * 1e-3), "ms_per_step": ms_loop},
            "problems": len(specs), "dof": dof, "elements": sum(sp["n"] ** 2 for sp in specs),
-           "kernel_nodes": B.kernel_nodes,
+           "kernel_nodes": B.kernel_nodes, "tuning": batch_tuning,
            "workload": "c4: 64 Dirichlet Helmholtz problems on [0,1]^2, n in 4..32, N in 6..12, "
                        "lambda^2 log-uniform [0.1,100], seed 20261203",
            "setup_s": setup}

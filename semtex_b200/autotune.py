@@ -15,7 +15,11 @@ processes, e.g. with how two mode-group streams happen to overlap, the
 least time much less) deciding -- and records every
 trial and the winner in a JSON table keyed by the problem's shape.
 ``tuned_overrides`` returns the winner for a session from that table (empty
-when the shape was never tuned), for Context(..., overrides=...).
+when the shape was never tuned), for Context(..., overrides=...).  A batch
+of independent problems is tuned as a whole (``tune_batch``: one setting for
+every problem, timed as the batch's graph replay), since problems that run
+side by side compete for the GPU: settings best for each problem alone made
+the 64-problem benchmark batch slower (0.69 against 0.56 ms).
 
 The committed table (semtex_b200/autotune_table.json) holds the
 benchmark workloads' entries; ``python -m semtex_b200.autotune session
@@ -175,10 +179,89 @@ def tune(session: str, field: str, lambda2: float, space: dict = SPACE, reps: in
     return entry
 
 
+# knobs of a batch of single-plane problems (mode groups do not apply)
+BATCH_SPACE = {k: v for k, v in SPACE.items() if k not in ("STX_MODE_GROUPS", "STX_STAGGER")}
+
+
+def batch_signature(specs) -> str:
+    """Key of a batch of problems: their (n, N_P) list in order."""
+    import hashlib
+    key = ";".join(f"{s['n']}x{s['np']}" for s in specs)
+    return "batch-" + hashlib.sha1(key.encode()).hexdigest()[:16] + f"-{len(specs)}"
+
+
+def batch_time_ms(specs, overrides: dict, reps: int = 11, device: int = 0) -> float:
+    """Least device time (ms) of `reps` replays of the batch's CUDA graph
+    (stx_batch_launch) with the same overrides on every problem (+inf when a
+    problem rejects them).  The problems are the uneven-batch dicts of
+    sessions.uneven_batch (n, np, lambda2, seed), Dirichlet zero."""
+    import tempfile
+    import torch
+    from . import Batch, Context, ModalMatrixSys, StxError, sessions
+    items, ctxs = [], []
+    with tempfile.TemporaryDirectory() as d:
+        try:
+            for i, sp in enumerate(specs):
+                p = sessions.helmholtz_session(os.path.join(d, f"p{i}"), sp["n"], sp["np"], lambda2=sp["lambda2"])
+                ctx = Context(p, overrides or None, device=device)
+                ctxs.append(ctx)
+                x, y = ctx.mesh_coords()
+                f, _ = sessions.forcing_per_unique_node(x, y, 1, sp["seed"])
+                items.append((ModalMatrixSys(ctx, "c", sp["lambda2"]), ctx.new_field("f").load_physical(f),
+                              ctx.new_field("u")))
+        except StxError:
+            for c in ctxs:
+                c.close()
+            return float("inf")
+    B = Batch(items)
+    main = torch.cuda.ExternalStream(B.stream, device=f"cuda:{device}")
+    times = []
+    for k in range(reps + 2):
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        e0.record(main)
+        B.launch()
+        e1.record(main)
+        e1.synchronize()
+        if k >= 2:
+            times.append(e0.elapsed_time(e1))
+    ok = all(s.status() == 0 for s, _, _ in items)
+    B.close()
+    for s, _, _ in items:
+        s.close()
+    for c in ctxs:
+        c.close()
+    return min(times) if ok else float("inf")
+
+
+def tune_batch(specs, space: dict = BATCH_SPACE, reps: int = 11, device: int = 0, path: str | None = TABLE,
+               label: str = "") -> dict:
+    """Tune one setting of the knobs for a whole batch, timed as the batch
+    runs (its graph replay: the problems' kernels run side by side, so a
+    setting that is best for a problem alone need not be best in the batch).
+    Recorded under batch_signature(specs)."""
+    def measure(config):
+        return batch_time_ms(specs, _overrides(config), reps, device)
+
+    best, best_t, trials = coordinate_descent(measure, space)
+    entry = {"label": label, "best": _overrides(best), "best_ms": best_t, "default_ms": trials[0][1],
+             "trials": [[_overrides(c), t] for c, t in trials]}
+    if path:
+        table = load_table(path)
+        table["entries"][batch_signature(specs)] = entry
+        save_table(table, path)
+    return entry
+
+
+def tuned_batch_overrides(specs, path: str = TABLE) -> dict:
+    """The tuned tokens of a batch, or {} if it was never tuned."""
+    entry = load_table(path)["entries"].get(batch_signature(specs))
+    return dict(entry["best"]) if entry else {}
+
+
 def tune_benchmark_workloads(path: str = TABLE, device: int = 0, only: str | None = None):
     """Tune the benchmark's Helmholtz workloads into the table: the batched
-    2D x Fourier solve (16x16 quads, N_P=11, N_Z=64) and each problem of the
-    uneven batch (64 problems, seed 20261203)."""
+    2D x Fourier solve (16x16 quads, N_P=11, N_Z=64) and the uneven batch
+    (64 problems, seed 20261203) as one batch."""
     import tempfile
     from . import sessions
     with tempfile.TemporaryDirectory() as d:
@@ -188,15 +271,8 @@ def tune_benchmark_workloads(path: str = TABLE, device: int = 0, only: str | Non
             print("c2", json.dumps({k: e[k] for k in ("best", "best_ms", "default_ms")}), flush=True)
         if only not in (None, "c4"):
             return
-        seen = set()
-        for i, sp in enumerate(sessions.uneven_batch()):
-            p = sessions.helmholtz_session(os.path.join(d, f"p{i}"), sp["n"], sp["np"], lambda2=sp["lambda2"])
-            sig = signature(p, "c", sp["lambda2"])
-            if sig in seen:
-                continue
-            seen.add(sig)
-            e = tune(p, "c", sp["lambda2"], device=device, path=path, label=f"c4 n={sp['n']} N_P={sp['np']}")
-            print(f"c4[{i}]", json.dumps({k: e[k] for k in ("best", "best_ms", "default_ms")}), flush=True)
+        e = tune_batch(sessions.uneven_batch(), device=device, path=path, label="c4 uneven batch")
+        print("c4", json.dumps({k: e[k] for k in ("best", "best_ms", "default_ms")}), flush=True)
 
 
 def main():

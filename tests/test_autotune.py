@@ -50,3 +50,10 @@ def test_committed_table_is_well_formed():
         assert sig.startswith("nel")
         assert set(e["best"]) <= set(A.SPACE)
         assert e["best_ms"] <= e["default_ms"]
+
+
+def test_batch_signature():
+    specs = [{"n": 4, "np": 7, "lambda2": 1.0, "seed": 1}, {"n": 9, "np": 12, "lambda2": 3.0, "seed": 2}]
+    assert A.batch_signature(specs) == A.batch_signature([dict(s, lambda2=5.0) for s in specs])
+    assert A.batch_signature(specs) != A.batch_signature(specs[::-1])
+    assert A.batch_signature(specs).endswith("-2")

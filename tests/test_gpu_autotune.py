@@ -54,3 +54,13 @@ def test_tune_records_winner(tmp_path):
     assert ov == e["best"]
     f = np.random.default_rng(4).uniform(-1, 1, (8, 64, 7, 7))
     assert np.linalg.norm(_solve(p, ov, f) - _solve(p, {}, f)) <= 1e-12 * np.linalg.norm(_solve(p, {}, f))
+
+
+def test_tune_batch_records_one_setting(tmp_path):
+    specs = [{"n": 3, "np": 6, "lambda2": 1.0, "seed": 1}, {"n": 5, "np": 8, "lambda2": 10.0, "seed": 2},
+             {"n": 4, "np": 7, "lambda2": 0.5, "seed": 3}]
+    table = str(tmp_path / "table.json")
+    e = A.tune_batch(specs, space={"STX_CHUNK": [None, 8]}, reps=3, path=table)
+    assert e["best_ms"] <= e["default_ms"] and len(e["trials"]) == 2
+    assert A.tuned_batch_overrides(specs, table) == e["best"]
+    assert A.tuned_batch_overrides(specs[:2], table) == {}
