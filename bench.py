@@ -462,6 +462,7 @@ def run_ours(args):
         line["dns_c3_dealiased"] = run_dns(args.dns_steps, 3, local, "c3d", cb)
         line["dns_c5"] = run_dns(args.dns_steps, 3, local, "c5", cb)
         line["batch_c4"] = run_batch(args.dns_steps, 3, local, not args.untuned)
+        line["adjoint_c5"] = run_adjoint(local)
     print(json.dumps(line))
     if ws > 1:
         torch.distributed.destroy_process_group()
@@ -597,6 +598,78 @@ def run_dns(steps, warmup=3, local=0, workload="c3", cpu_baseline=False):
     return out
 
 
+def run_adjoint(local=0, steps=100, every=10):
+    """Secondary measurement: the discrete adjoint of the c5 channel
+    workload (16x8 quads, N_P=9, N_Z=32, Re=500, D_T=5e-3, N_TIME=3): a
+    100-step recorded run with full-state checkpoints every 10 steps, then
+    the gradient of the perturbation kinetic energy at the end w.r.t. the
+    initial velocity (stx_dns_adjoint_backward: segments recomputed from
+    their checkpoints, steps transposed), and the tangent-linear derivative
+    along a second seeded perturbation (stx_dns_adjoint_tangent).  Device
+    time by CUDA events on the library stream around each C-ABI call (the
+    calls include their host copies of the seed and gradient, 3 fields
+    each).  The gradient's directional derivative is compared with the
+    tangent-linear one (they agree to round-off when the adjoint is the
+    exact transpose)."""
+    import torch
+    import semtex_b200 as S
+    from semtex_b200 import sessions
+    import ctypes as C
+    from semtex_b200 import _lib
+    d = tempfile.mkdtemp()
+    p = dns_session(d, "c5")
+    ctx = S.Context(p, device=local)
+    x, y = ctx.mesh_coords()
+    z = np.arange(ctx.nz) * 2 * np.pi / ctx.nz
+    u0 = {c: v for c, v in sessions.channel_initial(x, y, z).items() if c != "p"}
+    alt = sessions.channel_initial(x, y, z, seed=7)
+    shape = (ctx.nz, ctx.nel, ctx.np, ctx.np)
+    base = {"u": np.broadcast_to(1 - y * y, shape), "v": np.zeros(shape), "w": np.zeros(shape)}
+    dirn = {c: alt[c] - base[c] for c in "uvw"}
+    q4 = np.empty(ctx.nel * ctx.np * ctx.np)
+    _lib.check(_lib.lib().stx_mesh_mass(ctx.handle, C.c_void_p(q4.ctypes.data)))
+    q4 = q4.reshape(1, ctx.nel, ctx.np, ctx.np)
+    stream = ctx.torch_stream()
+
+    def timed(fn):
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        ctx.sync()
+        e0.record(stream)
+        r = fn()
+        e1.record(stream)
+        e1.synchronize()
+        return r, e0.elapsed_time(e1)
+
+    D = S.DNS(ctx, 1)
+    A = S.DNSAdjoint(D, checkpoint_every=every)
+    res = {}
+    for rep in range(2):  # the first pass sets up the start-up systems
+        D.restart(u0, 0.0)
+        _, fwd_ms = timed(lambda: D.advance(steps))
+        D.restart(u0, 0.0)
+        _, rec_ms = timed(lambda: A.record(steps))
+        uT = {c: D.field(c) for c in "uvw"}
+        dE = {c: q4 * (uT[c] - base[c]) for c in "uvw"}
+        grad, bwd_ms = timed(lambda: A.backward(dE))
+        tl, tan_ms = timed(lambda: A.tangent(dirn))
+        res = {"forward_ms": fwd_ms, "record_ms": rec_ms, "backward_ms": bwd_ms, "tangent_ms": tan_ms,
+               "grad": grad, "tl": tl}
+    dot = sum(float(np.vdot(res["grad"][c], dirn[c])) for c in "uvw")
+    tld = sum(float(np.vdot(dE[c], res["tl"][c])) for c in "uvw")
+    _, _, ck_bytes = A.info()
+    A.close()
+    D.close()
+    ctx.close()
+    return {"metric": "adjoint gradient time", "workload": DNS_WORKLOADS["c5"] + "; 100 steps, checkpoints every 10",
+            "objective": "perturbation kinetic energy at the end (Q4-weighted, about u = 1 - y^2)",
+            "forward_ms": res["forward_ms"], "record_ms": res["record_ms"], "backward_ms": res["backward_ms"],
+            "tangent_ms": res["tangent_ms"],
+            "gradient_ms": res["record_ms"] + res["backward_ms"],
+            "backward_over_forward": res["backward_ms"] / res["forward_ms"],
+            "checkpoint_bytes": ck_bytes,
+            "adjoint_vs_tangent_rel": abs(dot - tld) / abs(tld)}
+
+
 def dns_probe(workload):
     """Two start-up and three steady steps of a DNS workload with the graph
     replay off (every kernel a plain launch): the run the DNS traffic
@@ -722,7 +795,7 @@ def main():
     ap.add_argument("--solver", default="twolevel", choices=["twolevel", "band"],
                     help="band: the single banded-Cholesky skeleton solve (for comparison)")
     ap.add_argument("--workload", default="c2",
-                    choices=["c2", "dns", "dns_c5", "batch_c4", "dns_probe_c3", "dns_probe_c5"],
+                    choices=["c2", "dns", "dns_c5", "batch_c4", "adjoint_c5", "dns_probe_c3", "dns_probe_c5"],
                     help="dns / dns_c5 / batch_c4: run only that secondary measurement (one JSON line); "
                          "dns_probe_c3 / _c5: 2 start-up + 3 steady steps with graph replay off, nothing "
                          "timed (a run to profile every kernel of a step)")
@@ -736,6 +809,10 @@ def main():
         torch.cuda.set_device(0)
         print(json.dumps(run_dns(max(1, args.dns_steps), args.warmup, 0,
                                  "c3" if args.workload == "dns" else "c5", not args.no_cpu_baseline)))
+    elif args.workload == "adjoint_c5":
+        import torch
+        torch.cuda.set_device(0)
+        print(json.dumps(run_adjoint(0)))
     elif args.workload == "batch_c4":
         import torch
         torch.cuda.set_device(0)

@@ -323,6 +323,44 @@ int stx_dns_system(stx_dns* dns, char field, stx_modal** sys);
 /* Device pointer of a field's Fourier-space storage (nz x plane_size). */
 int stx_dns_field_ptr(stx_dns* dns, char field, double** d_ptr);
 
+/* ---- Discrete adjoint and tangent-linear model of the time step ---------
+ * The reference has no derivative code; these differentiate the discrete
+ * map its integrate() computes (dns/integrate.cpp:138-200): the velocity
+ * given to stx_dns_set_field at the start of a recorded run -> the velocity
+ * stx_dns_get_field reads at its end.  Checkpoints of the full state
+ * (stx_dns_checkpoint_* blocks) are kept on the device every
+ * `checkpoint_every` steps; the backward sweep recomputes one segment at a
+ * time from its checkpoint and transposes its steps, so the memory is one
+ * state per checkpoint plus one velocity per step of a segment.  The
+ * transposed step reuses the step's symmetric condensed solves (with zero
+ * BC data), transposes the projection, the high-order pressure BC terms
+ * (src/bcmgr.cpp:1036-1331) and the z transforms, and linearises the
+ * advection at the recorded velocity (dns/nonlinear.cpp:198-381).  Solves
+ * that the forward run did by Jacobi-PCG (start-up orders, ITERATIVE) are
+ * exact (DIRECT) in the derivatives.
+ * Not differentiated (STX_EUNSUPPORTED at _create): DEALIAS, computed
+ * outflow BCs, SVV, velocity-dependent forcing (sponge, drag, Coriolis,
+ * SFD); other forcing and time-dependent BC values are data.
+ * Host buffers of _backward and _tangent hold the velocity components one
+ * after the other, each nz x nplane physical values as stx_dns_set_field
+ * takes them.
+ *   _record:   runs nsteps from the current state, keeping checkpoints;
+ *   _backward: h_seed = d(objective)/d(final velocity) -> h_grad =
+ *              d(objective)/d(initial velocity); the DNS is left at the
+ *              end of the recorded run;
+ *   _tangent:  h_dir (initial velocity direction) -> h_out, the derivative
+ *              of the final velocity along it (the forward-mode check of
+ *              _backward: <tangent(x), y> = <x, backward(y)>);
+ *   _info:     first and last step of the record, checkpoint bytes. */
+typedef struct stx_dns_adjoint stx_dns_adjoint;
+int stx_dns_adjoint_create(stx_dns* dns, int checkpoint_every, stx_dns_adjoint** out);
+int stx_dns_adjoint_destroy(stx_dns_adjoint* adj);
+int stx_dns_adjoint_record(stx_dns_adjoint* adj, int nsteps);
+int stx_dns_adjoint_backward(stx_dns_adjoint* adj, const double* h_seed, double* h_grad);
+int stx_dns_adjoint_tangent(stx_dns_adjoint* adj, const double* h_dir, double* h_out);
+int stx_dns_adjoint_info(const stx_dns_adjoint* adj, int* first_step, int* last_step,
+                         unsigned long long* checkpoint_bytes);
+
 /* ---- Batches of independent solves --------------------------------------
  * The reference solves one problem per `elliptic` run (elliptic/drive.cpp:
  * 61-96: one Field::solve).  stx_batch_create captures n DIRECT (or MIXED)

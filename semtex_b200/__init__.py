@@ -27,7 +27,7 @@ from .fieldfile import read_field, write_field
 
 DIRECT, JACPCG, MIXED = STX_DIRECT, STX_JACPCG, STX_MIXED
 
-__all__ = ["Context", "ModalMatrixSys", "Field", "DNS", "Batch", "expression", "svv", "numbering", "element_matrix", "solve_multi", "solve_host_batch", "elliptic", "dns", "read_field",
+__all__ = ["Context", "ModalMatrixSys", "Field", "DNS", "DNSAdjoint", "Batch", "expression", "svv", "numbering", "element_matrix", "solve_multi", "solve_host_batch", "elliptic", "dns", "read_field",
            "write_field", "FORWARD", "INVERSE", "DIRECT", "JACPCG", "MIXED", "StxError"]
 
 
@@ -513,6 +513,66 @@ class DNS:
         v = C.c_double()
         check(lib().stx_dns_cfl(self._h, C.byref(v)))
         return v.value
+
+
+class DNSAdjoint:
+    """Discrete adjoint and tangent-linear model of a DNS's time steps over
+    the C ABI (stx_dns_adjoint_*): :meth:`record` runs steps keeping
+    full-state checkpoints on the device every ``checkpoint_every`` steps;
+    :meth:`backward` maps d(objective)/d(final velocity) to
+    d(objective)/d(initial velocity) (segments recomputed from their
+    checkpoints, steps transposed last to first); :meth:`tangent` maps an
+    initial-velocity direction to the final velocity's derivative along it.
+    Velocities are dicts {component: [nz, nel, np, np]} in physical space,
+    as :meth:`DNS.restart` and :meth:`DNS.field` use them."""
+
+    def __init__(self, dns: DNS, checkpoint_every: int = 10):
+        self.dns = dns
+        self._h = C.c_void_p()
+        check(lib().stx_dns_adjoint_create(dns._h, checkpoint_every, C.byref(self._h)))
+        names = dns.ctx.fields
+        self.components = names[:-1]
+
+    def close(self):
+        if self._h and self.dns._h:
+            check(lib().stx_dns_adjoint_destroy(self._h))
+        self._h = C.c_void_p()
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    def record(self, nsteps: int):
+        check(lib().stx_dns_adjoint_record(self._h, nsteps))
+
+    def info(self):
+        """(first step, last step, checkpoint bytes on the device)."""
+        a, b, n = C.c_int(), C.c_int(), C.c_ulonglong()
+        check(lib().stx_dns_adjoint_info(self._h, C.byref(a), C.byref(b), C.byref(n)))
+        return a.value, b.value, n.value
+
+    def _pack(self, fields: dict) -> np.ndarray:
+        ctx = self.dns.ctx
+        shape = (ctx.nz, ctx.nel, ctx.np, ctx.np)
+        return np.ascontiguousarray(np.stack([np.broadcast_to(np.asarray(fields[c], dtype=np.float64), shape)
+                                              for c in self.components]))
+
+    def _unpack(self, a: np.ndarray) -> dict:
+        return {c: a[i] for i, c in enumerate(self.components)}
+
+    def backward(self, seed: dict) -> dict:
+        x = self._pack(seed)
+        out = np.empty_like(x)
+        check(lib().stx_dns_adjoint_backward(self._h, C.c_void_p(x.ctypes.data), C.c_void_p(out.ctypes.data)))
+        return self._unpack(out)
+
+    def tangent(self, direction: dict) -> dict:
+        x = self._pack(direction)
+        out = np.empty_like(x)
+        check(lib().stx_dns_adjoint_tangent(self._h, C.c_void_p(x.ctypes.data), C.c_void_p(out.ctypes.data)))
+        return self._unpack(out)
 
 
 def _user_functions(session: str):

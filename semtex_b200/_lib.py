@@ -77,6 +77,12 @@ SIGNATURES = {
     "stx_dns_stats_info": (_i, [_p, _s, _i, _pi, _i]),
     "stx_dns_stats_get": (_i, [_p, C.c_char, _p]),
     "stx_dns_stats_set": (_i, [_p, C.c_char, _p]),
+    "stx_dns_adjoint_create": (_i, [_p, _i, C.POINTER(_p)]),
+    "stx_dns_adjoint_destroy": (_i, [_p]),
+    "stx_dns_adjoint_record": (_i, [_p, _i]),
+    "stx_dns_adjoint_backward": (_i, [_p, _p, _p]),
+    "stx_dns_adjoint_tangent": (_i, [_p, _p, _p]),
+    "stx_dns_adjoint_info": (_i, [_p, _pi, _pi, C.POINTER(C.c_ulonglong)]),
     "stx_elliptic_solve_host": (_i, [_p, _p, _p]),
     "stx_sync": (_i, [_p]),
     "stx_context_stream": (_i, [_p, C.POINTER(_p)]),

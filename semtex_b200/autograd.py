@@ -1,7 +1,8 @@
-"""Differentiable Field::solve: the elliptic map forcing -> solution as a
-torch.autograd.Function over the C ABI.
+"""Differentiable Field::solve (the elliptic map forcing -> solution) and
+DNS time steps (the discrete adjoint over the C ABI), as
+torch.autograd.Functions.
 
-The map (src/field.cpp:598-809 with the z transforms of elliptic/helmholtz.cpp:
+Field::solve.  The map (src/field.cpp:598-809 with the z transforms of elliptic/helmholtz.cpp:
 29-52) is affine, u = A f + b: b comes from the boundary conditions and
 A = I S F, with F / I the packed real DFT pair and S, per plane, the
 condensed Helmholtz solve S = -P H^-1 P^T M (P: global -> element-local
@@ -100,3 +101,46 @@ def helmholtz_solve(f, system):
     if _FN is None:
         _FN = _helmholtz_solve()
     return _FN.apply(f, system)
+
+
+def _dns_steps():
+    torch = _torch()
+
+    class DNSSteps(torch.autograd.Function):
+        @staticmethod
+        def forward(actx, u0, adjoint, nsteps, t0):
+            dns = adjoint.dns
+            a = u0.detach().to("cpu", torch.float64).numpy()
+            dns.restart({c: a[i] for i, c in enumerate(adjoint.components)}, t0)
+            adjoint.record(nsteps)
+            out = np.stack([dns.field(c) for c in adjoint.components])
+            actx.adjoint = adjoint
+            actx.device = u0.device
+            return torch.from_numpy(out).to(u0.device)
+
+        @staticmethod
+        def backward(actx, g):
+            adj = actx.adjoint
+            gn = g.detach().to("cpu", torch.float64).numpy()
+            r = adj.backward({c: gn[i] for i, c in enumerate(adj.components)})
+            grad = torch.from_numpy(np.stack([r[c] for c in adj.components])).to(actx.device)
+            return grad, None, None, None
+
+    return DNSSteps
+
+
+_DNS_FN = None
+
+
+def dns_steps(u0, adjoint, nsteps: int, t0: float = 0.0):
+    """Differentiable final velocity of `nsteps` DNS time steps (integrate(),
+    dns/integrate.cpp:138-200) from the initial velocity u0 (tensor
+    [ncom, nz, nel, np, np], float64, physical; the DNS restarts from it at
+    time t0 with empty history).  `adjoint` is a semtex_b200.DNSAdjoint of
+    the DNS: the forward call records the run (checkpoints every
+    checkpoint_every steps on the device), backward runs its discrete
+    adjoint, whose solves reuse the step's condensed factors."""
+    global _DNS_FN
+    if _DNS_FN is None:
+        _DNS_FN = _dns_steps()
+    return _DNS_FN.apply(u0, adjoint, nsteps, t0)

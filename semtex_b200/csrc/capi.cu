@@ -977,6 +977,61 @@ int stx_modal_info(const stx_modal* sys, int mode, int* nsolve, int* nband) {
   });
 }
 
+namespace {
+
+// A DIRECT (or MIXED) solve of every plane with the BC values `lines` in
+// place of the field's own (same [nz][nline] layout).
+void direct_solve_lines(stx_modal* sys, const double* d_forcing, double* d_unknown, const double* lines) {
+  stx_context* ctx = sys->ctx;
+  FieldDev& F = ctx->fields.at(sys->field);
+  double* work = ctx->workspace(helmholtz_workspace_doubles(ctx->dg, F.dn, sys->store->dm));
+  const auto& groups = sys->store->groups;
+  if (groups.size() > 1) {
+    // mode groups on parallel streams, forked from and joined back into
+    // the context stream
+    ctx->ensure_aux(groups.size() - 1);
+    cuda_check(cudaEventRecord(ctx->aux_ev[0], ctx->stream), "fork");
+    for (size_t k = 1; k < groups.size(); ++k)
+      cuda_check(cudaStreamWaitEvent(ctx->aux[k - 1], ctx->aux_ev[0], 0), "fork wait");
+    const bool stag = ctx->stagger();
+    if (stag) ctx->ensure_stagger(groups.size());
+    for (size_t k = 0; k < groups.size(); ++k) {
+      cudaStream_t sk = k ? ctx->aux[k - 1] : ctx->stream;
+      if (stag && k) cuda_check(cudaStreamWaitEvent(sk, ctx->stagger_ev[k - 1], 0), "stagger wait");
+      cuda_check(helmholtz_direct_solve(ctx->dg, F.dn, groups[k], d_forcing, d_unknown, lines, F.nline, work, sk,
+                                        nullptr, stag ? ctx->stagger_ev[k] : nullptr),
+                 "direct solve");
+    }
+    for (size_t k = 1; k < groups.size(); ++k) {
+      cuda_check(cudaEventRecord(ctx->aux_ev[k], ctx->aux[k - 1]), "join");
+      cuda_check(cudaStreamWaitEvent(ctx->stream, ctx->aux_ev[k], 0), "join wait");
+    }
+  } else {
+    cuda_check(helmholtz_direct_solve(ctx->dg, F.dn, sys->store->dm, d_forcing, d_unknown, lines, F.nline, work,
+                                      ctx->stream),
+               "direct solve");
+  }
+}
+
+}  // namespace
+
+}  // extern "C"
+
+namespace stx {
+
+int field_solve_with_lines(stx_modal* sys, const double* d_forcing, double* d_unknown, const double* d_lines) {
+  return guarded([&] {
+    if (!sys || !d_forcing || !d_unknown || !d_lines) throw StxError(STX_EINVAL, "null argument");
+    if (sys->method == STX_JACPCG) throw StxError(STX_EINVAL, "solve with given BC values: DIRECT systems only");
+    cudaSetDevice(sys->ctx->device);
+    direct_solve_lines(sys, d_forcing, d_unknown, d_lines);
+  });
+}
+
+}  // namespace stx
+
+extern "C" {
+
 int stx_field_solve(stx_modal* sys, const double* d_forcing, double* d_unknown, double tol_rel,
                     int step_max, int* iterations) {
   return guarded([&] {
@@ -985,33 +1040,7 @@ int stx_field_solve(stx_modal* sys, const double* d_forcing, double* d_unknown, 
     FieldDev& F = ctx->fields.at(sys->field);
     cudaSetDevice(ctx->device);
     if (sys->method != STX_JACPCG) {
-      double* work = ctx->workspace(helmholtz_workspace_doubles(ctx->dg, F.dn, sys->store->dm));
-      const auto& groups = sys->store->groups;
-      if (groups.size() > 1) {
-        // mode groups on parallel streams, forked from and joined back into
-        // the context stream
-        ctx->ensure_aux(groups.size() - 1);
-        cuda_check(cudaEventRecord(ctx->aux_ev[0], ctx->stream), "fork");
-        for (size_t k = 1; k < groups.size(); ++k)
-          cuda_check(cudaStreamWaitEvent(ctx->aux[k - 1], ctx->aux_ev[0], 0), "fork wait");
-        const bool stag = ctx->stagger();
-        if (stag) ctx->ensure_stagger(groups.size());
-        for (size_t k = 0; k < groups.size(); ++k) {
-          cudaStream_t sk = k ? ctx->aux[k - 1] : ctx->stream;
-          if (stag && k) cuda_check(cudaStreamWaitEvent(sk, ctx->stagger_ev[k - 1], 0), "stagger wait");
-          cuda_check(helmholtz_direct_solve(ctx->dg, F.dn, groups[k], d_forcing, d_unknown, F.d_lines, F.nline,
-                                            work, sk, nullptr, stag ? ctx->stagger_ev[k] : nullptr),
-                     "direct solve");
-        }
-        for (size_t k = 1; k < groups.size(); ++k) {
-          cuda_check(cudaEventRecord(ctx->aux_ev[k], ctx->aux[k - 1]), "join");
-          cuda_check(cudaStreamWaitEvent(ctx->stream, ctx->aux_ev[k], 0), "join wait");
-        }
-      } else {
-        cuda_check(helmholtz_direct_solve(ctx->dg, F.dn, sys->store->dm, d_forcing, d_unknown,
-                                          F.d_lines, F.nline, work, ctx->stream),
-                   "direct solve");
-      }
+      direct_solve_lines(sys, d_forcing, d_unknown, F.d_lines);
     } else {
       double* work = ctx->workspace(jacpcg_workspace_doubles(ctx->dg, F.dn));
       std::vector<int> it(ctx->M.nz, -1);

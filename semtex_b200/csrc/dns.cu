@@ -25,14 +25,19 @@
 #include "kernels/outflow.cuh"
 #include "kernels/force.cuh"
 #include "kernels/helmholtz.cuh"
+#include "dns_internal.hpp"
 #include "stx_internal.hpp"
 
 using namespace stx;
 
-namespace {
+namespace stx {
 
 const double kSS[4][4] = {{0, 0, 0, 0}, {1.0, -1.0, 0, 0}, {1.5, -2.0, 0.5, 0}, {11.0 / 6.0, -3.0, 1.5, -1.0 / 3.0}};
 const double kEX[4][3] = {{0, 0, 0}, {1.0, 0, 0}, {2.0, -1.0, 0}, {3.0, -3.0, 1.0}};
+
+}  // namespace stx
+
+namespace {
 
 struct DnsError : std::runtime_error {
   int code;
@@ -72,109 +77,6 @@ int dns_guarded(F&& f) {
 
 }  // namespace
 
-struct stx_dns {
-  stx_context* ctx = nullptr;
-  int ncom = 0, ndim = 0, nord = 0, form = 1;
-  double dt = 0, nu = 0, beta = 0, tol = 0;
-  int step_max = 0;
-  bool iterative = false;  // ITERATIVE: Jacobi-PCG velocity systems at every step
-  int step = 0;
-  double time = 0;
-  int toggle = 1;  // altSkewSymmetric's static switch (dns/nonlinear.cpp:254)
-  std::string names;  // velocity components then pressure
-  DeviceArena arena;
-  size_t fsize = 0;  // doubles per field
-  std::vector<double*> u;                 // [ncom+1] Domain fields (Fourier)
-  std::vector<std::vector<double*>> Us, Uf;  // [nord][ncom]
-  std::vector<double*> Up;                // [ncom] physical velocities
-  double* tmp0 = nullptr;
-  double* tmp1 = nullptr;
-  double* tmp2 = nullptr;
-  double* dsswork = nullptr;
-  std::vector<stx_modal*> vsys;           // DIRECT velocity systems
-  stx_modal* psys = nullptr;
-  std::map<std::pair<char, int>, stx_modal*> pcg;  // temporary JACPCG systems
-  std::vector<char> tdep;                 // per field: BCs depend on t
-  std::vector<int> last_iters;
-  // High-order pressure BCs: edge tables and the multi-level storage of u.n
-  // and of the BC terms (BCmgr::_un / _hopbc), levels newest first and
-  // rolled by pointer like rollv (src/sem.h:98-106).
-  int nh = 0;
-  const int* h_elmt = nullptr;
-  const int* h_side = nullptr;
-  const int* h_line = nullptr;
-  const double* h_nx = nullptr;
-  const double* h_ny = nullptr;
-  std::vector<double*> un_lvl, hop_lvl;
-  size_t hsize = 0;  // doubles per level
-  // Computed outflow BCs <O> (outflow.cuh): edges, and the levels (newest
-  // first, rolled by pointer) of the physical edge velocities, nu div u and
-  // nu n.grad(u).n; o_fb holds KE* S0 of the step.
-  stx::OutflowEdges oe{};
-  std::vector<double*> o_uvw, o_divu, o_gradu;
-  double* o_fb = nullptr;
-  double o_iuzd = 0.0;  // 1 / U0Delta
-  // 3/2-rule products (token DEALIAS, N_Z > 2): physical fields on nz32 =
-  // 3 N_Z / 2 planes (AuxField::transform32, src/auxfield.cpp:1197-1258).
-  int nz32 = 0;
-  double* twiddle32 = nullptr;
-  std::vector<double*> Up32;               // [ncom] padded physical velocities
-  double* A32 = nullptr;                   // padded nonlinear terms
-  double* B32 = nullptr;                   // padded z-derivative term (convective)
-  double* C32 = nullptr;                   // padded product / z-derivative term (conservative)
-  double* part = nullptr;                  // analysis partials: blocks x max(modes, 3)
-  // Steady steps replayed as a CUDA graph (token STX_DNS_GRAPH, default 1):
-  // the steps from one pointer state back to the same state (the multi-level
-  // storage rolls by pointer, the alternating form toggles) captured once.
-  bool use_graph = true;
-  cudaGraphExec_t gexec = nullptr;
-  int gperiod = 0;
-  std::vector<double*> gkey;  // pointer state the captured steps start from and return to
-  int gtoggle = 0;
-  int eager_steady = 0;       // steady steps run directly since the last restart
-  long long graph_launches = 0;
-  // Running averages (Statistics, src/statistics.cpp:94-466; token AVERAGE
-  // 1 or 2): buffers named as the reference names them, in its order (the
-  // sorted keys of its map): the raw fields held in Fourier space and, for
-  // AVERAGE 2, the velocity products A = uu, B = uv, C = vv, D = uw, E = vw,
-  // F = ww held in physical space.
-  int avg_level = 0;
-  int navg = 0;
-  std::string avg_names;
-  std::vector<double*> avg_buf;
-  // Body forcing (<FORCE>; FieldForce and its classes, dns/fieldforce.cpp),
-  // on the grid of the nonlinear products (nzl planes: N_Z, or 3 N_Z / 2
-  // with DEALIAS).  Fields are device arrays of nzl planes, null when a term
-  // is absent; time-dependent scalars are evaluated on the host each step.
-  struct Force {
-    bool on = false;        // FORCE section present
-    bool physical = false;  // some physical-space term present
-    bool tdep = false;      // some term changes from step to step
-    double cst[3] = {0.0, 0.0, 0.0};  // ConstForce
-    int nzl = 0;
-    double dz = 0.0;
-    double* x = nullptr;  // node coordinates [nplane]
-    double* y = nullptr;
-    double* mask = nullptr;  // SpongeForce
-    double* uref[3] = {nullptr, nullptr, nullptr};
-    int sponge_update = 0;
-    ExprOp* mask_prog = nullptr;
-    int nmask = 0;
-    int coriolis = 0;  // CoriolisForce: 0 off, 1 steady, 2 unsteady
-    std::string omega[3], domega[3];
-    double m2o[3] = {0.0, 0.0, 0.0}, o[3] = {0.0, 0.0, 0.0}, mo[3] = {0.0, 0.0, 0.0},
-           dodt[3] = {0.0, 0.0, 0.0};
-    double* steady[3] = {nullptr, nullptr, nullptr};  // SteadyForce
-    std::string alpha[3];                              // ModulatedForce
-    double* moda[3] = {nullptr, nullptr, nullptr};
-    ExprOp* st[3] = {nullptr, nullptr, nullptr};  // SpatioTemporalForce
-    int nst[3] = {0, 0, 0};
-    double* drag = nullptr;  // DragForce
-    double* qbar[3] = {nullptr, nullptr, nullptr};  // SFDForce
-    double chi = 0.0, rate = 0.0;
-    bool sfd_started = false;
-  } force;
-};
 
 namespace {
 
@@ -511,18 +413,21 @@ void nonlinear32(stx_dns* d, int form) {
 void rollm_levels(std::vector<double*>& v);
 
 // Nonlinear terms N(u) into Uf[0], copy of u into Us[0] (dns/nonlinear.cpp).
+int next_form(const stx_dns* d) {
+  switch (d->form) {
+    case 0: return 0;
+    case 1: return d->toggle ? 1 : 2;
+    case 2: return 1;
+    default: return -1;
+  }
+}
+
 void nonlinear(stx_dns* d) {
   stx_context* ctx = d->ctx;
   const DevGeom& g = ctx->dg;
   cudaStream_t st = ctx->stream;
   const bool z3 = d->ndim == 3;
-  int form;  // 0 skew, 1 convective, 2 conservative, -1 Stokes
-  switch (d->form) {
-    case 0: form = 0; break;
-    case 1: form = d->toggle ? 1 : 2; break;
-    case 2: form = 1; break;
-    default: form = -1; break;
-  }
+  const int form = next_form(d);  // 0 skew, 1 convective, 2 conservative, -1 Stokes
   if (d->nz32) {
     nonlinear32(d, form);
     if (d->form == 1) d->toggle = 1 - d->toggle;
@@ -742,6 +647,19 @@ void advance_one(stx_dns* d) {
 }
 
 }  // namespace
+
+namespace stx {
+
+void dns_advance_one(stx_dns* d) { advance_one(d); }
+
+int dns_next_form(const stx_dns* d) { return next_form(d); }
+
+int dns_error_code(const std::exception& e) {
+  if (const auto* de = dynamic_cast<const DnsError*>(&e)) return de->code;
+  return STX_ESESSION;
+}
+
+}  // namespace stx
 
 namespace {
 
@@ -1397,6 +1315,37 @@ void ckpt_header(stx_dns* d, double* h, size_t nblock) {
 }
 
 }  // namespace
+
+}  // extern "C"
+
+namespace stx {
+
+std::vector<std::pair<double*, size_t>> dns_state_blocks(stx_dns* d) { return ckpt_blocks(d); }
+
+DnsHostState dns_host_state(const stx_dns* d) {
+  DnsHostState s;
+  s.step = d->step;
+  s.toggle = d->toggle;
+  s.navg = d->navg;
+  s.time = d->time;
+  s.sfd_started = d->force.sfd_started;
+  return s;
+}
+
+void dns_set_host_state(stx_dns* d, const DnsHostState& s) {
+  drop_graph(d);
+  d->eager_steady = 0;
+  d->step = s.step;
+  d->time = s.time;
+  d->toggle = s.toggle;
+  d->navg = s.navg;
+  d->force.sfd_started = s.sfd_started;
+  for (char c : d->names) ckstx(stx_field_bc_evaluate(d->ctx, c, d->time));
+}
+
+}  // namespace stx
+
+extern "C" {
 
 int stx_dns_checkpoint_size(stx_dns* d, unsigned long long* bytes) {
   return dns_guarded([&] {

@@ -221,3 +221,12 @@ struct stx_modal {
   double lambda2 = 0, beta = 0;
   std::shared_ptr<stx::ModalStore> store;
 };
+
+namespace stx {
+
+// Field::solve DIRECT (or MIXED) over every plane, with the Fourier BC
+// values `d_lines` ([nz][nline] of the field) in place of the field's own;
+// asynchronous on the context stream.  Returns an STX_* status.
+int field_solve_with_lines(stx_modal* sys, const double* d_forcing, double* d_unknown, const double* d_lines);
+
+}  // namespace stx
