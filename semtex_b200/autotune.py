@@ -46,6 +46,7 @@ SPACE = {
     "STX_SYM_REGCAP": [None, 1],
     "STX_SYM_WARPS": [None, 2, 8],
     "STX_SYM_OCC": [None, 50, 200],
+    "STX_PDL": [None, 0],
 }
 
 

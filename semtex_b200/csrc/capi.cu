@@ -225,6 +225,10 @@ int stx_context_create(const char* session_path, const char* overrides, int devi
     g.next = M.next;
     g.nint = M.nint;
     g.plane_size = M.plane_size;
+    // the DNS step's own kernels launch programmatically dependent only on
+    // request (token STX_PDL_STEP = 1; measured slower on the 24x24x96
+    // Taylor-Green step); the solves' kernels do by default (STX_PDL)
+    g.pdl = ctx->S.tokens.has("STX_PDL_STEP") && ctx->S.tokens.ivalue("STX_PDL_STEP") != 0;
     g.D = upload(A, M.q.D);
     g.Q1 = upload(A, M.Q1);
     g.Q2 = upload(A, M.Q2);
@@ -310,6 +314,8 @@ int stx_context_create(const char* session_path, const char* overrides, int devi
         if (k == 'O') k = c == 'p' ? 'D' : 'N';
         kind.push_back(k);
       }
+      d.ness = static_cast<int>(std::count(kind.begin(), kind.end(), static_cast<int>('D')));
+      d.nnat = static_cast<int>(std::count(kind.begin(), kind.end(), static_cast<int>('N')));
       d.edge_gid = upload(A, gid);
       d.edge_kind = upload(A, kind);
       d.mixdiag = F.N.mixdiag.empty() ? nullptr : upload(A, F.N.mixdiag);
@@ -623,6 +629,7 @@ int stx_modal_create(stx_context* ctx, char field, double lambda2, double beta, 
       d.sym_warps = 4;
       d.sym_regcap = 0;
       d.elem_twoblock = ctx->S.tokens.has("STX_ELEM_TWOBLOCK") && ctx->S.tokens.ivalue("STX_ELEM_TWOBLOCK") != 0;
+      d.pdl = !ctx->S.tokens.has("STX_PDL") || ctx->S.tokens.ivalue("STX_PDL") != 0;
       // bound of the kernels' bounded waits (token STX_WAIT_NS, default 2 s;
       // 0: one non-blocking probe, which a copy issued just before misses --
       // the error path's tests use it)

@@ -32,6 +32,7 @@ struct DevGeom {
   const int* chunk_count;
   const int* elem_sorted;
   const int4* chunk_desc;  // [nchunk] (chunk_start, chunk_count, family, 0): one load per block
+  int pdl;                 // 1: the DNS step's kernels launch programmatically dependent (token STX_PDL_STEP)
 };
 
 struct DevNumbering {
@@ -45,6 +46,7 @@ struct DevNumbering {
   const int* edge_kind; // [nedge]  'D' or 'N'
   const double* edge_area;  // [nedge*np]
   const double* mixdiag;    // [nglobal] mixed-BC diagonal (K x side weights), or null
+  int ness, nnat;           // edges of kind 'D' / 'N' (kernels with nothing to do are not launched)
 };
 
 // One tiled product y += scale A x for the planes of a Fourier mode, the
@@ -99,6 +101,7 @@ struct DevModal {
   int sym_warps;                  // warps per block of the packed products (token STX_SYM_WARPS)
   int sym_regcap;                 // 1: their register-capped build (token STX_SYM_REGCAP)
   int elem_twoblock;              // 1: element kernels split rows to run two blocks per SM (STX_ELEM_TWOBLOCK)
+  int pdl;                        // 1: the solve's kernels launch programmatically dependent (STX_PDL)
   unsigned long long wait_ns;     // bound of the element and skeleton kernels' first
                                   // wait per copy (token STX_WAIT_NS, default 2 s)
   const double* pc;               // JACPCG: [nmodes][npts]

@@ -19,6 +19,8 @@
 #include "dns_kernels.cuh"
 #include "elemderiv.cuh"
 #include "launch.hpp"
+#include "ptx.cuh"
+#include "twolevel.cuh"
 
 namespace stx {
 
@@ -64,6 +66,8 @@ __device__ __forceinline__ void ep_load(const double* __restrict__ src, double* 
 }
 
 __global__ void k_grad_xy(DevGeom g, const double* __restrict__ in, double* __restrict__ out, int dir) {
+  pdl_trigger();
+  pdl_wait();
   extern __shared__ double sm[];
   double* su;
   const int k = ep_setup(g, sm, 1, su);
@@ -86,6 +90,8 @@ __global__ void k_grad_xy(DevGeom g, const double* __restrict__ in, double* __re
 // extrapolated pressure BC value  sum_q ex[q] hop_q.  The Nyquist plane is
 // never touched (its lines stay zero).
 __global__ void k_hopbc(DevGeom g, HopbcArgs a) {
+  pdl_trigger();
+  pdl_wait();
   extern __shared__ double sm[];
   const int np = g.np, nn = g.npnp;
   const int h = blockIdx.x, m = blockIdx.y;
@@ -215,6 +221,8 @@ __global__ void __launch_bounds__(kAnaThreads) k_cfl(DevGeom g, const double* __
 
 __global__ void k_grad_z(const double* __restrict__ in, double* __restrict__ out, int nz, int plane_size,
                          double beta) {
+  pdl_trigger();
+  pdl_wait();
   const size_t n = static_cast<size_t>(nz) * plane_size;
   for (size_t x = blockIdx.x * static_cast<size_t>(blockDim.x) + threadIdx.x; x < n;
        x += static_cast<size_t>(gridDim.x) * blockDim.x) {
@@ -225,6 +233,8 @@ __global__ void k_grad_z(const double* __restrict__ in, double* __restrict__ out
 
 __global__ void k_product(const double* __restrict__ a, const double* __restrict__ b, double* __restrict__ out,
                           size_t n) {
+  pdl_trigger();
+  pdl_wait();
   for (size_t x = blockIdx.x * static_cast<size_t>(blockDim.x) + threadIdx.x; x < n;
        x += static_cast<size_t>(gridDim.x) * blockDim.x)
     out[x] = a[x] * b[x];
@@ -234,6 +244,8 @@ __global__ void k_product(const double* __restrict__ a, const double* __restrict
 //            cons: -(d(Ui U0)/dx + d(Ui U1)/dy + Tk) ] , form 0 skew (sc=1/2,
 // both), 1 convective, 2 conservative.  Tc / Tk / U2 may be null (2D).
 __global__ void __launch_bounds__(32 * kEpPlanes, 3) k_nonlinear(DevGeom g, NonlinearArgs a) {
+  pdl_trigger();
+  pdl_wait();
   extern __shared__ double sm[];
   double* ws;
   const int k = ep_setup(g, sm, 5, ws);
@@ -286,6 +298,8 @@ __global__ void __launch_bounds__(32 * kEpPlanes, 3) k_nonlinear(DevGeom g, Nonl
 
 __global__ void k_dss_accum(DevGeom g, DevNumbering N, const double* __restrict__ in, double* __restrict__ ds,
                             int gstride) {
+  pdl_trigger();
+  pdl_wait();
   const int e = blockIdx.x, k = blockIdx.y * kEpPlanes + (threadIdx.x >> 5), ln = threadIdx.x & 31;
   if (k >= g.nz) return;
   const double* src = in + static_cast<size_t>(k) * g.plane_size + static_cast<size_t>(e) * g.npnp;
@@ -297,6 +311,8 @@ __global__ void k_dss_accum(DevGeom g, DevNumbering N, const double* __restrict_
 
 __global__ void k_dss_insert(DevGeom g, DevNumbering N, double* __restrict__ io, const double* __restrict__ ds,
                              int gstride) {
+  pdl_trigger();
+  pdl_wait();
   const int e = blockIdx.x, k = blockIdx.y * kEpPlanes + (threadIdx.x >> 5), ln = threadIdx.x & 31;
   if (k >= g.nz) return;
   double* dst = io + static_cast<size_t>(k) * g.plane_size + static_cast<size_t>(e) * g.npnp;
@@ -307,6 +323,8 @@ __global__ void k_dss_insert(DevGeom g, DevNumbering N, double* __restrict__ io,
 }
 
 __global__ void k_combine(CombineArgs a, size_t n) {
+  pdl_trigger();
+  pdl_wait();
   for (size_t x = blockIdx.x * static_cast<size_t>(blockDim.x) + threadIdx.x; x < n;
        x += static_cast<size_t>(gridDim.x) * blockDim.x) {
     double v = 0.0;
@@ -319,6 +337,8 @@ __global__ void k_combine(CombineArgs a, size_t n) {
 __global__ void k_divergence(DevGeom g, const double* __restrict__ a0, const double* __restrict__ a1,
                              const double* __restrict__ a2, double* __restrict__ out, double inv_dt,
                              double beta) {
+  pdl_trigger();
+  pdl_wait();
   extern __shared__ double sm[];
   double* ws;
   const int k = ep_setup(g, sm, 2, ws);
@@ -340,6 +360,8 @@ __global__ void k_divergence(DevGeom g, const double* __restrict__ a0, const dou
 // io = alpha * io + b * d p / dx_dir  (dir 0, 1 element; 2 Fourier z; -1 none)
 __global__ void k_project(DevGeom g, double* __restrict__ io, const double* __restrict__ p, int dir,
                           double alpha, double b, double beta) {
+  pdl_trigger();
+  pdl_wait();
   extern __shared__ double sm[];
   double* sp;
   const int k = ep_setup(g, sm, 1, sp);
@@ -376,35 +398,35 @@ inline unsigned stream_blocks(size_t n) {
 cudaError_t dns_grad_xy(const DevGeom& g, const double* in, double* out, int dir, cudaStream_t st) {
   if (!ep_fits(g)) return cudaErrorInvalidValue;
   raise_smem_limit(reinterpret_cast<const void*>(k_grad_xy), ep_smem(g, 1));
-  k_grad_xy<<<ep_grid(g), kEpThreads, ep_smem(g, 1), st>>>(g, in, out, dir);
+  launch_ex(g.pdl != 0, k_grad_xy, ep_grid(g), dim3(kEpThreads), ep_smem(g, 1), st, g, in, out, dir);
   return cudaGetLastError();
 }
 
 cudaError_t dns_grad_z(const DevGeom& g, const double* in, double* out, double beta, cudaStream_t st) {
   const size_t n = static_cast<size_t>(g.nz) * g.plane_size;
-  k_grad_z<<<stream_blocks(n), 256, 0, st>>>(in, out, g.nz, g.plane_size, beta);
+  launch_ex(g.pdl != 0, k_grad_z, dim3(stream_blocks(n)), dim3(256), 0, st, in, out, g.nz, g.plane_size, beta);
   return cudaGetLastError();
 }
 
 cudaError_t dns_product(const DevGeom& g, const double* a, const double* b, double* out, cudaStream_t st) {
   const size_t n = static_cast<size_t>(g.nz) * g.plane_size;
-  k_product<<<stream_blocks(n), 256, 0, st>>>(a, b, out, n);
+  launch_ex(g.pdl != 0, k_product, dim3(stream_blocks(n)), dim3(256), 0, st, a, b, out, n);
   return cudaGetLastError();
 }
 
 cudaError_t dns_nonlinear(const DevGeom& g, const NonlinearArgs& a, cudaStream_t st) {
   if (!ep_fits(g)) return cudaErrorInvalidValue;
   raise_smem_limit(reinterpret_cast<const void*>(k_nonlinear), ep_smem(g, 5));
-  k_nonlinear<<<ep_grid(g), kEpThreads, ep_smem(g, 5), st>>>(g, a);
+  launch_ex(g.pdl != 0, k_nonlinear, ep_grid(g), dim3(kEpThreads), ep_smem(g, 5), st, g, a);
   return cudaGetLastError();
 }
 
 cudaError_t dns_smooth(const DevGeom& g, const DevNumbering& N, double* io, double* work, cudaStream_t st) {
   const int gstride = (N.nglobal + 31) / 32 * 32;
-  cudaError_t e = cudaMemsetAsync(work, 0, sizeof(double) * gstride * static_cast<size_t>(g.nz), st);
+  cudaError_t e = zero_ranges(g.pdl != 0, work, static_cast<size_t>(gstride) * g.nz, nullptr, 0, st);
   if (e != cudaSuccess) return e;
-  k_dss_accum<<<ep_grid(g), kEpThreads, 0, st>>>(g, N, io, work, gstride);
-  k_dss_insert<<<ep_grid(g), kEpThreads, 0, st>>>(g, N, io, work, gstride);
+  launch_ex(g.pdl != 0, k_dss_accum, ep_grid(g), dim3(kEpThreads), 0, st, g, N, io, work, gstride);
+  launch_ex(g.pdl != 0, k_dss_insert, ep_grid(g), dim3(kEpThreads), 0, st, g, N, io, work, gstride);
   return cudaGetLastError();
 }
 
@@ -431,13 +453,12 @@ cudaError_t dns_hopbc(const DevGeom& g, const HopbcArgs& a, cudaStream_t st) {
   if (a.nh == 0) return cudaSuccess;
   if (2 * g.np > 128 || a.Je < 0 || a.Je > 3 || a.Jx < 1 || a.Jx > 3) return cudaErrorInvalidValue;
   const dim3 grid(a.nh, g.nz > 1 ? g.nz / 2 : 1);
-  k_hopbc<<<grid, 128, dns_hopbc_smem(g), st>>>(g, a);
-  return cudaGetLastError();
+  return launch_ex(g.pdl != 0, k_hopbc, grid, dim3(128), dns_hopbc_smem(g), st, g, a);
 }
 
 cudaError_t dns_combine(const DevGeom& g, const CombineArgs& a, cudaStream_t st) {
   const size_t n = static_cast<size_t>(g.nz) * g.plane_size;
-  k_combine<<<stream_blocks(n), 256, 0, st>>>(a, n);
+  launch_ex(g.pdl != 0, k_combine, dim3(stream_blocks(n)), dim3(256), 0, st, a, n);
   return cudaGetLastError();
 }
 
@@ -445,7 +466,7 @@ cudaError_t dns_divergence(const DevGeom& g, const double* a0, const double* a1,
                            double dt, double beta, cudaStream_t st) {
   if (!ep_fits(g)) return cudaErrorInvalidValue;
   raise_smem_limit(reinterpret_cast<const void*>(k_divergence), ep_smem(g, 2));
-  k_divergence<<<ep_grid(g), kEpThreads, ep_smem(g, 2), st>>>(g, a0, a1, a2, out, 1.0 / dt, beta);
+  launch_ex(g.pdl != 0, k_divergence, ep_grid(g), dim3(kEpThreads), ep_smem(g, 2), st, g, a0, a1, a2, out, 1.0 / dt, beta);
   return cudaGetLastError();
 }
 
@@ -453,7 +474,7 @@ cudaError_t dns_project(const DevGeom& g, double* io, const double* p, int dir, 
                         double beta, cudaStream_t st) {
   if (!ep_fits(g)) return cudaErrorInvalidValue;
   raise_smem_limit(reinterpret_cast<const void*>(k_project), ep_smem(g, 1));
-  k_project<<<ep_grid(g), kEpThreads, ep_smem(g, 1), st>>>(g, io, p, dir, alpha, b, beta);
+  launch_ex(g.pdl != 0, k_project, ep_grid(g), dim3(kEpThreads), ep_smem(g, 1), st, g, io, p, dir, alpha, b, beta);
   return cudaGetLastError();
 }
 

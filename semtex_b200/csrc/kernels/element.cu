@@ -303,6 +303,7 @@ __global__ void __launch_bounds__(32 * kMaxWarps, 1)
     k_elem_condense(DevGeom g, DevNumbering N, DevModal S, const double* __restrict__ F, const double* __restrict__ G,
                     int gstride, double* __restrict__ R, int rstride, int rb_rows) {
   extern __shared__ __align__(16) unsigned char sraw[];
+  pdl_trigger();
   const int c = blockIdx.x, m = S.mode0 + blockIdx.y;
   const int nr = (g.nz > 1 && m > 0) ? 2 : 1;
   const int nn = g.npnp, next = g.next;
@@ -324,6 +325,7 @@ __global__ void __launch_bounds__(32 * kMaxWarps, 1)
   const ElemIdx X = load_idx(g, sraw, L, el, cnt);
   for (int w = threadIdx.x; w < g.np * g.np; w += blockDim.x) sD[w] = S.D[w];
   __syncthreads();
+  pdl_wait();  // the operator rows are set-up data; F, G and R come from earlier kernels
   // boundary-major columns: the product takes the interior rows, F_b stays
   issue_forcing<false>(g, F, X, cnt, m, ncol, sB, ldb, sQ, 0);
   if (G)
@@ -366,6 +368,7 @@ __global__ void __launch_bounds__(32 * kMaxWarps, 1)
     k_elem_recover(DevGeom g, DevNumbering N, DevModal S, const double* __restrict__ F, const double* __restrict__ G,
                    int gstride, const double* __restrict__ R, int rstride, double* __restrict__ U, int rb_rows) {
   extern __shared__ __align__(16) unsigned char sraw[];
+  pdl_trigger();
   const int c = blockIdx.x, m = S.mode0 + blockIdx.y;
   const int nr = (g.nz > 1 && m > 0) ? 2 : 1;
   const int nn = g.npnp, next = g.next, nint = g.nint;
@@ -389,6 +392,7 @@ __global__ void __launch_bounds__(32 * kMaxWarps, 1)
   const ElemIdx X = load_idx(g, sraw, L, el, cnt);
   for (int w = threadIdx.x; w < g.np * g.np; w += blockDim.x) sD[w] = S.D[w];
   __syncthreads();
+  pdl_wait();  // F, G, R (and U's other writers) belong to earlier kernels
   // interior forcing only: the boundary rows carry u_b
   issue_forcing<true>(g, F, X, cnt, m, ncol, sB, ldb, sQ, next);
   const int nsolve = S.nsolve[m];
@@ -452,6 +456,7 @@ __global__ void __launch_bounds__(256)
     k_elem_schur(int dir, DevGeom g, DevNumbering N, DevModal S, const double* __restrict__ src,
                  double* __restrict__ dst, int rstride) {
   extern __shared__ __align__(16) unsigned char sraw[];
+  pdl_trigger();
   const int c = blockIdx.x, m = S.mode0 + blockIdx.y;
   const int nr = (g.nz > 1 && m > 0) ? 2 : 1;
   // this block's part of the chunk: elements [e0, e0 + cnt)
@@ -470,6 +475,7 @@ __global__ void __launch_bounds__(256)
   const int* code = S.l2_ncode + static_cast<size_t>(cd.x + e0) * next;
   for (int i = threadIdx.x; i < cnt * next; i += blockDim.x) sN[i] = __ldg(code + i);
   __syncthreads();
+  pdl_wait();  // S_e and the node codes are set-up data; src and dst are not
   // input columns, loads of kColBatch columns per warp in flight together
   for (int c0 = wp; c0 < ncol; c0 += nwp * kColBatch) {
     double v[kColBatch][2];
@@ -563,16 +569,16 @@ ElementPlan element_plan(const DevGeom& g, const DevModal& S, bool lift) {
 void element_condense(const ElementPlan& P, const DevGeom& g, const DevNumbering& N, const DevModal& S,
                       const double* F, const double* G, int gstride, double* R, int rstride, cudaStream_t st) {
   raise_smem_limit(reinterpret_cast<const void*>(k_elem_condense), P.cond_smem);
-  k_elem_condense<<<dim3(g.nchunk, S.nmodes, P.cond_rb), P.cond_threads, P.cond_smem, st>>>(g, N, S, F, G, gstride,
-                                                                                            R, rstride, P.cond_rows);
+  launch_ex(S.pdl != 0, k_elem_condense, dim3(g.nchunk, S.nmodes, P.cond_rb), dim3(P.cond_threads), P.cond_smem, st,
+            g, N, S, F, G, gstride, R, rstride, P.cond_rows);
 }
 
 void element_recover(const ElementPlan& P, const DevGeom& g, const DevNumbering& N, const DevModal& S,
                      const double* F, const double* G, int gstride, const double* R, int rstride, double* U,
                      cudaStream_t st) {
   raise_smem_limit(reinterpret_cast<const void*>(k_elem_recover), P.rec_smem);
-  k_elem_recover<<<dim3(g.nchunk, S.nmodes, P.rec_rb), P.rec_threads, P.rec_smem, st>>>(g, N, S, F, G, gstride, R,
-                                                                                        rstride, U, P.rec_rows);
+  launch_ex(S.pdl != 0, k_elem_recover, dim3(g.nchunk, S.nmodes, P.rec_rb), dim3(P.rec_threads), P.rec_smem, st, g,
+            N, S, F, G, gstride, R, rstride, U, P.rec_rows);
 }
 
 void element_schur_apply(int dir, const DevGeom& g, const DevNumbering& N, const DevModal& S, const double* src,
@@ -582,7 +588,8 @@ void element_schur_apply(int dir, const DevGeom& g, const DevNumbering& N, const
                       sizeof(int) * static_cast<size_t>(g.chunk_max) * g.next;
   raise_smem_limit(reinterpret_cast<const void*>(k_elem_schur), smem);
   // two blocks per chunk and mode: the work is latency-bound
-  k_elem_schur<<<dim3(g.nchunk, S.nmodes, 2), 256, smem, st>>>(dir, g, N, S, src, dst, rstride);
+  launch_ex(S.pdl != 0, k_elem_schur, dim3(g.nchunk, S.nmodes, 2), dim3(256), smem, st, dir, g, N, S, src, dst,
+            rstride);
 }
 
 }  // namespace stx

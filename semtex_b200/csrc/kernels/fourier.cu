@@ -22,6 +22,8 @@ constexpr int kTP = 32;  // points per block
 
 __global__ void k_dft(double* __restrict__ data, int nz, int plane_size, int sign,
                       const double* __restrict__ twiddle) {
+  pdl_trigger();
+  pdl_wait();
   extern __shared__ double sm[];
   double* x = sm;             // [nz][kTP]
   double* tw = sm + nz * kTP; // [2][nz]
@@ -212,6 +214,8 @@ namespace {
 template <int TPL>
 __global__ void k_fft(double* __restrict__ data, int nz, int plane_size, int sign, const double* __restrict__ twiddle,
                       FftPlan plan, int bulk) {
+  pdl_trigger();
+  pdl_wait();
   constexpr int TPC = TPL / 2, LD = TPL;
   extern __shared__ __align__(16) double sm[];
   uint64_t* bar = reinterpret_cast<uint64_t*>(sm);
@@ -321,6 +325,8 @@ __global__ void k_fft(double* __restrict__ data, int nz, int plane_size, int sig
 }
 
 __global__ void k_nz2(double* data, int plane_size, int sign) {
+  pdl_trigger();
+  pdl_wait();
   const int p = blockIdx.x * blockDim.x + threadIdx.x;
   if (p >= plane_size) return;
   data[plane_size + p] = sign > 0 ? 0.0 : data[p];
@@ -329,10 +335,10 @@ __global__ void k_nz2(double* data, int plane_size, int sign) {
 }  // namespace
 
 cudaError_t z_transform(double* data, int nz, int plane_size, int sign, const double* twiddle,
-                        double* /*work*/, cudaStream_t st) {
+                        double* /*work*/, cudaStream_t st, bool pdl) {
   if (nz < 2) return cudaSuccess;
   if (nz == 2) {
-    k_nz2<<<(plane_size + 255) / 256, 256, 0, st>>>(data, plane_size, sign);
+    launch_ex(pdl, k_nz2, dim3((plane_size + 255) / 256), dim3(256), 0, st, data, plane_size, sign);
     return cudaGetLastError();
   }
   // Stockham FFT when nz factors into 2, 3, 5 (radix 4 first)
@@ -360,15 +366,18 @@ cudaError_t z_transform(double* data, int nz, int plane_size, int sign, const do
     const int bulk = (reinterpret_cast<uintptr_t>(data) % 16 == 0 && plane_size % 2 == 0 && tp % 2 == 0) ? 1 : 0;
     if (fshm <= 200 * 1024) {
       const int nb = (plane_size + tp - 1) / tp;
-      if (tp == 32) k_fft<32><<<nb, 256, fshm, st>>>(data, nz, plane_size, sign, twiddle, plan, bulk);
-      else if (tp == 16) k_fft<16><<<nb, 256, fshm, st>>>(data, nz, plane_size, sign, twiddle, plan, bulk);
-      else if (tp == 8) k_fft<8><<<nb, 256, fshm, st>>>(data, nz, plane_size, sign, twiddle, plan, bulk);
-      else k_fft<4><<<nb, 256, fshm, st>>>(data, nz, plane_size, sign, twiddle, plan, bulk);
+      auto go = [&](auto kernel) {
+        launch_ex(pdl, kernel, dim3(nb), dim3(256), fshm, st, data, nz, plane_size, sign, twiddle, plan, bulk);
+      };
+      if (tp == 32) go(k_fft<32>);
+      else if (tp == 16) go(k_fft<16>);
+      else if (tp == 8) go(k_fft<8>);
+      else go(k_fft<4>);
       return cudaGetLastError();
     }
   }
   const size_t shm = sizeof(double) * (2 * static_cast<size_t>(nz) * kTP + 2 * nz);
-  k_dft<<<(plane_size + kTP - 1) / kTP, 256, shm, st>>>(data, nz, plane_size, sign, twiddle);
+  launch_ex(pdl, k_dft, dim3((plane_size + kTP - 1) / kTP), dim3(256), shm, st, data, nz, plane_size, sign, twiddle);
   return cudaGetLastError();
 }
 

@@ -72,6 +72,8 @@ __device__ void constrained_forcing(const DevGeom& g, const DevNumbering& N,
 
 __global__ void k_essential(DevGeom g, DevNumbering N, const double* __restrict__ lines,
                             int nline, double* __restrict__ G, int gstride, int nz, int k0) {
+  pdl_trigger();
+  pdl_wait();
   const int idx = blockIdx.x * blockDim.x + threadIdx.x;
   const int k = k0 + blockIdx.y;
   if (k >= nz || idx >= N.nedge * g.np) return;
@@ -89,6 +91,8 @@ __global__ void k_add(double* __restrict__ y, const double* __restrict__ x, size
 
 __global__ void k_natural(DevGeom g, DevNumbering N, const double* __restrict__ lines,
                           int nline, double* __restrict__ R, int rstride, int nz, int k0) {
+  pdl_trigger();
+  pdl_wait();
   const int idx = blockIdx.x * blockDim.x + threadIdx.x;
   const int k = k0 + blockIdx.y;
   if (k >= nz || (nz > 1 && k == 1) || idx >= N.nedge * g.np) return;
@@ -948,14 +952,15 @@ cudaError_t helmholtz_direct_solve(const DevGeom& g, const DevNumbering& N, cons
   const int k0 = nz > 1 ? 2 * S.mode0 : 0, k1 = nz > 1 ? std::min(nz, 2 * (S.mode0 + S.nmodes)) : 1;
   const size_t pz = static_cast<size_t>(rstride) * (k1 - k0);
   if (ev) cudaEventRecord(ev[0], st);
-  cudaError_t err = cudaMemsetAsync(R + static_cast<size_t>(rstride) * k0, 0, sizeof(double) * pz, st);
-  if (err == cudaSuccess) err = cudaMemsetAsync(G + static_cast<size_t>(rstride) * k0, 0, sizeof(double) * pz, st);
+  const bool pdl = S.pdl != 0;
+  cudaError_t err = zero_ranges(pdl, R + static_cast<size_t>(rstride) * k0, pz,
+                                G + static_cast<size_t>(rstride) * k0, pz, st);
   if (err != cudaSuccess) return err;
   const bool has_ess = N.nglobal > N.nsolve;
   const int nedge_nodes = N.nedge * g.np;
-  if (has_ess && nedge_nodes) {
+  if (has_ess && nedge_nodes && N.ness) {
     dim3 grid((nedge_nodes + 127) / 128, k1 - k0);
-    k_essential<<<grid, 128, 0, st>>>(g, N, lines, nline, G, rstride, nz, k0);
+    launch_ex(pdl, k_essential, grid, dim3(128), 0, st, g, N, lines, nline, G, rstride, nz, k0);
   }
   const int threads = ((g.npnp + 31) / 32) * 32 < 64 ? 64 : ((g.npnp + 31) / 32) * 32;
   const size_t shm = sizeof(double) * (static_cast<size_t>(g.np) * g.np + 5 * g.npnp);
@@ -977,9 +982,9 @@ cudaError_t helmholtz_direct_solve(const DevGeom& g, const DevNumbering& N, cons
   } else {
     k_condense<<<egrid, threads, shm, st>>>(g, N, S, F, has_ess ? G : nullptr, rstride, R, rstride);
   }
-  if (nedge_nodes) {
+  if (nedge_nodes && N.nnat) {
     dim3 grid((nedge_nodes + 127) / 128, k1 - k0);
-    k_natural<<<grid, 128, 0, st>>>(g, N, lines, nline, R, rstride, nz, k0);
+    launch_ex(pdl && ep.ok, k_natural, grid, dim3(128), 0, st, g, N, lines, nline, R, rstride, nz, k0);
   }
   if (ev) cudaEventRecord(ev[1], st);
   if (after_condense) cudaEventRecord(after_condense, st);
@@ -1063,18 +1068,18 @@ cudaError_t helmholtz_direct_solve_fields(const DevGeom& g, const DevNumbering* 
   for (int f = 0; f < nf; ++f) {
     double* Rf = R + f * fs;
     double* Gf = G + f * fs;
-    err = cudaMemsetAsync(Rf + off, 0, sizeof(double) * pz, st);
-    if (err == cudaSuccess) err = cudaMemsetAsync(Gf + off, 0, sizeof(double) * pz, st);
+    const bool pdl = S.pdl != 0;
+    err = zero_ranges(pdl, Rf + off, pz, Gf + off, pz, st);
     if (err != cudaSuccess) return err;
     const int nedge_nodes = N[f]->nedge * g.np;
-    if (has_ess && nedge_nodes) {
+    if (has_ess && nedge_nodes && N[f]->ness) {
       dim3 grid((nedge_nodes + 127) / 128, k1 - k0);
-      k_essential<<<grid, 128, 0, st>>>(g, *N[f], lines[f], nline[f], Gf, rstride, nz, k0);
+      launch_ex(pdl, k_essential, grid, dim3(128), 0, st, g, *N[f], lines[f], nline[f], Gf, rstride, nz, k0);
     }
     element_condense(ep, g, *N[f], S, F[f], has_ess ? Gf : nullptr, rstride, Rf, rstride, st);
-    if (nedge_nodes) {
+    if (nedge_nodes && N[f]->nnat) {
       dim3 grid((nedge_nodes + 127) / 128, k1 - k0);
-      k_natural<<<grid, 128, 0, st>>>(g, *N[f], lines[f], nline[f], Rf, rstride, nz, k0);
+      launch_ex(pdl, k_natural, grid, dim3(128), 0, st, g, *N[f], lines[f], nline[f], Rf, rstride, nz, k0);
     }
   }
   if (after_condense) cudaEventRecord(after_condense, st);

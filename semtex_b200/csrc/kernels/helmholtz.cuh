@@ -61,8 +61,9 @@ const int* fft_timeout_address();
 
 // AuxField::transform (src/auxfield.cpp:1157-1194, femlib/fourier.c:40-165)
 // of nz planes in place: sign +1 forward (scaled by 1/nz), -1 inverse.
-// `twiddle` holds cos/sin(2 pi m / nz), m < nz, as [2][nz].
+// `twiddle` holds cos/sin(2 pi m / nz), m < nz, as [2][nz].  pdl: launched
+// programmatically dependent on the stream's previous kernel.
 cudaError_t z_transform(double* data, int nz, int plane_size, int sign, const double* twiddle,
-                        double* work, cudaStream_t st);
+                        double* work, cudaStream_t st, bool pdl = false);
 
 }  // namespace stx

@@ -31,6 +31,14 @@ __device__ __forceinline__ void bulk_g2s(void* dst, const void* src, unsigned by
       : "memory");
 }
 
+// Programmatic dependent launch (a kernel launched with the programmatic
+// stream serialisation attribute may start while the previous kernel of its
+// stream finishes): pdl_wait blocks until that kernel has completed and its
+// writes are visible (a no-op for a kernel launched without the attribute);
+// pdl_trigger lets the next such kernel start launching its blocks.
+__device__ __forceinline__ void pdl_wait() { asm volatile("griddepcontrol.wait;" ::: "memory"); }
+__device__ __forceinline__ void pdl_trigger() { asm volatile("griddepcontrol.launch_dependents;" ::: "memory"); }
+
 __device__ __forceinline__ unsigned long long global_ns() {
   unsigned long long t;
   asm volatile("mov.u64 %0, %%globaltimer;" : "=l"(t));

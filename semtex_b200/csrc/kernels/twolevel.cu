@@ -102,9 +102,13 @@ __global__ void __launch_bounds__(CAP ? 32 * kSymWarpsMax : 128, CAP ? 3 : 0)
             int nwarps, const double* __restrict__ X, double* __restrict__ Y, int rstride, size_t fstride, int nz,
             int* status, unsigned long long wait_ns) {
   extern __shared__ __align__(16) unsigned char sraw[];
+  pdl_trigger();
   const int wp = threadIdx.x >> 5, ln = threadIdx.x & 31;
   const int gw = blockIdx.x * (blockDim.x >> 5) + wp;
-  if (gw >= nwarps) return;  // the warps of a block never synchronise with each other
+  if (gw >= nwarps) {  // the warps of a block never synchronise with each other
+    pdl_wait();
+    return;
+  }
   SymWarpSmem<NF>& sm = reinterpret_cast<SymWarpSmem<NF>*>(sraw)[wp];
   const SymWarp W = warps[gw];
   SymCursor ic, cc;  // issue and consume cursors
@@ -139,6 +143,9 @@ __global__ void __launch_bounds__(CAP ? 32 * kSymWarpsMax : 128, CAP ? 3 : 0)
       mbar_expect_tx(&sm.bar[s], bytes);
       bulk_g2s(sm.tile[s], pack + ic.P.moff + ic.offset(), bytes, &sm.bar[s]);
     }
+    // the matrix tiles are set-up data; the x entries (and the y atomics
+    // after them) depend on the previous kernel
+    if (issued == 0) pdl_wait();
     const double* X0 = X + static_cast<size_t>(2 * m) * rstride;
     const double* X1 = X0 + rstride;
 #pragma unroll
@@ -162,6 +169,7 @@ __global__ void __launch_bounds__(CAP ? 32 * kSymWarpsMax : 128, CAP ? 3 : 0)
     if (issued < W.count) prefetch();
   };
   for (int s = 0; s < kSymStages && s < W.count; ++s) issue(s);
+  if (W.count == 0) pdl_wait();
   double d0[NF], d1[NF];  // direct part of row 32 I + ln
 #pragma unroll
   for (int f = 0; f < NF; ++f) d0[f] = d1[f] = 0.0;
@@ -277,14 +285,14 @@ void configure_psymv() {
 template <class T, int NF>
 void launch_psymv_as(const T* pack, const SymProblem* probs, const SymWarp* warps, int nwarps, const double* X,
                      double* Y, int rstride, size_t fstride, int nz, int* status, unsigned long long wait_ns,
-                     int wpb, int regcap, cudaStream_t st) {
+                     int wpb, int regcap, bool pdl, cudaStream_t st) {
   const int blocks = (nwarps + wpb - 1) / wpb;
   if (regcap)
-    k_psymv<T, NF, 1><<<blocks, 32 * wpb, sym_smem<NF>(wpb), st>>>(pack, probs, warps, nwarps, X, Y, rstride,
-                                                                   fstride, nz, status, wait_ns);
+    launch_ex(pdl, k_psymv<T, NF, 1>, dim3(blocks), dim3(32 * wpb), sym_smem<NF>(wpb), st, pack, probs, warps,
+              nwarps, X, Y, rstride, fstride, nz, status, wait_ns);
   else
-    k_psymv<T, NF, 0><<<blocks, 32 * wpb, sym_smem<NF>(wpb), st>>>(pack, probs, warps, nwarps, X, Y, rstride,
-                                                                   fstride, nz, status, wait_ns);
+    launch_ex(pdl, k_psymv<T, NF, 0>, dim3(blocks), dim3(32 * wpb), sym_smem<NF>(wpb), st, pack, probs, warps,
+              nwarps, X, Y, rstride, fstride, nz, status, wait_ns);
 }
 
 cudaError_t launch_psymv(const DevModal& S, const SymProblem* probs, const SymWarp* warps, int nwarps,
@@ -293,17 +301,39 @@ cudaError_t launch_psymv(const DevModal& S, const SymProblem* probs, const SymWa
   if (nwarps <= 0) return cudaSuccess;
   configure_psymv();
   if (fp32)
-    launch_psymv_as<float, 1>(S.l2_pack32, probs, warps, nwarps, X, Y, rstride, 0, nz, S.status, S.wait_ns, S.sym_warps, S.sym_regcap, st);
+    launch_psymv_as<float, 1>(S.l2_pack32, probs, warps, nwarps, X, Y, rstride, 0, nz, S.status, S.wait_ns, S.sym_warps, S.sym_regcap, S.pdl != 0, st);
   else if (nf == 3)
-    launch_psymv_as<double, 3>(S.l2_pack, probs, warps, nwarps, X, Y, rstride, fstride, nz, S.status, S.wait_ns, S.sym_warps, S.sym_regcap, st);
+    launch_psymv_as<double, 3>(S.l2_pack, probs, warps, nwarps, X, Y, rstride, fstride, nz, S.status, S.wait_ns, S.sym_warps, S.sym_regcap, S.pdl != 0, st);
   else if (nf == 2)
-    launch_psymv_as<double, 2>(S.l2_pack, probs, warps, nwarps, X, Y, rstride, fstride, nz, S.status, S.wait_ns, S.sym_warps, S.sym_regcap, st);
+    launch_psymv_as<double, 2>(S.l2_pack, probs, warps, nwarps, X, Y, rstride, fstride, nz, S.status, S.wait_ns, S.sym_warps, S.sym_regcap, S.pdl != 0, st);
   else
-    launch_psymv_as<double, 1>(S.l2_pack, probs, warps, nwarps, X, Y, rstride, 0, nz, S.status, S.wait_ns, S.sym_warps, S.sym_regcap, st);
+    launch_psymv_as<double, 1>(S.l2_pack, probs, warps, nwarps, X, Y, rstride, 0, nz, S.status, S.wait_ns, S.sym_warps, S.sym_regcap, S.pdl != 0, st);
   return cudaGetLastError();
 }
 
 }  // namespace
+
+namespace {
+
+__global__ void k_zero_ranges(double* __restrict__ a, size_t na, double* __restrict__ b, size_t nb) {
+  pdl_trigger();
+  pdl_wait();
+  for (size_t i = blockIdx.x * static_cast<size_t>(blockDim.x) + threadIdx.x; i < na + nb;
+       i += static_cast<size_t>(gridDim.x) * blockDim.x) {
+    if (i < na) a[i] = 0.0;
+    else b[i - na] = 0.0;
+  }
+}
+
+}  // namespace
+
+cudaError_t zero_ranges(bool pdl, double* a, size_t na, double* b, size_t nb, cudaStream_t st) {
+  if (!b) nb = 0;
+  const size_t n = na + nb;
+  if (n == 0) return cudaSuccess;
+  const unsigned blocks = static_cast<unsigned>(std::min<size_t>((n + 255) / 256, 148 * 8));
+  return launch_ex(pdl, k_zero_ranges, dim3(blocks), dim3(256), 0, st, a, na, b, nb);
+}
 
 size_t twolevel_workspace_doubles(int rstride, int nz) { return static_cast<size_t>(rstride) * nz; }
 
@@ -312,8 +342,8 @@ cudaError_t twolevel_solve(const DevModal& S, const DevGeom& g, const DevNumberi
   double* Yv = twolevel_solution(work, rstride, nz);  // y_I, then the whole skeleton solution
   // planes of the launch's modes
   const int k0 = nz > 1 ? 2 * S.mode0 : 0, k1 = nz > 1 ? std::min(nz, 2 * (S.mode0 + S.nmodes)) : 1;
-  cudaError_t err = cudaMemsetAsync(Yv + static_cast<size_t>(rstride) * k0, 0,
-                                    sizeof(double) * rstride * (k1 - k0), st);
+  cudaError_t err = zero_ranges(S.pdl != 0, Yv + static_cast<size_t>(rstride) * k0,
+                                static_cast<size_t>(rstride) * (k1 - k0), nullptr, 0, st);
   if (err != cudaSuccess) return err;
   // y_I = S_II^-1 R_I; r_B = R_B - S_BI y_I
   err = launch_psymv(S, S.prob_patch, S.warp_patch, S.nwarp_patch, R, Yv, rstride, nz, fp32, st);
@@ -335,8 +365,8 @@ cudaError_t twolevel_solve_fields(const DevModal& S, const DevGeom& g, const Dev
   const int k0 = nz > 1 ? 2 * S.mode0 : 0, k1 = nz > 1 ? std::min(nz, 2 * (S.mode0 + S.nmodes)) : 1;
   cudaError_t err = cudaSuccess;
   for (int f = 0; f < nf && err == cudaSuccess; ++f)
-    err = cudaMemsetAsync(Y + f * fstride + static_cast<size_t>(rstride) * k0, 0,
-                          sizeof(double) * rstride * (k1 - k0), st);
+    err = zero_ranges(S.pdl != 0, Y + f * fstride + static_cast<size_t>(rstride) * k0,
+                      static_cast<size_t>(rstride) * (k1 - k0), nullptr, 0, st);
   if (err != cudaSuccess) return err;
   err = launch_psymv(S, S.prob_patch, S.warp_patch, S.nwarp_patch, R, Y, rstride, nz, false, st, nf, fstride);
   if (err != cudaSuccess) return err;

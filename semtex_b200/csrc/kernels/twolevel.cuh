@@ -29,6 +29,11 @@ cudaError_t twolevel_solve_fields(const DevModal& S, const DevGeom& g, const Dev
 
 int twolevel_launches(const DevModal& S);
 
+// a[0..na) = 0 and b[0..nb) = 0 (b may be null) in one kernel, launched
+// programmatically dependent when `pdl` is set (it waits for the previous
+// kernel before writing).
+cudaError_t zero_ranges(bool pdl, double* a, size_t na, double* b, size_t nb, cudaStream_t st);
+
 // Split the tiles of `probs` (in order) into equal runs, one per warp of a
 // grid of `wpb`-warp blocks that fills `device` occ_pct / 100 times at the
 // product kernel's occupancy (100: one full wave).
