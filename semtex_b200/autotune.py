@@ -10,9 +10,10 @@ per full wave (STX_SYM_OCC, percent) and whether the products run their
 register-capped build (STX_SYM_REGCAP: more resident warps, a few spills).  ``tune`` measures them on the device
 by coordinate descent -- each knob in turn over its values with the others
 held at the best so far, the device time of stx_field_solve (CUDA events,
-the least of several solves of a resident forcing: the mean moves between
-processes, e.g. with how two mode-group streams happen to overlap, the
-least time much less) deciding -- and records every
+the least of several solves of a resident forcing, each after a 256 MB
+write that flushes L2, as the benchmark times its solves: the mean moves
+between processes, e.g. with how two mode-group streams happen to overlap,
+the least time much less) deciding -- and records every
 trial and the winner in a JSON table keyed by the problem's shape.
 ``tuned_overrides`` returns the winner for a session from that table (empty
 when the shape was never tuned), for Context(..., overrides=...).  A batch
@@ -126,10 +127,17 @@ def _overrides(config: dict) -> dict:
     return {k: v for k, v in config.items() if v is not None}
 
 
+def _l2_flush_buffer(device: int):
+    """A 256 MB device buffer whose write evicts L2 (126 MB) between timed solves."""
+    import torch
+    return torch.empty(256 * 1024 * 1024 // 4, dtype=torch.float32, device=f"cuda:{device}")
+
+
 def solve_time_ms(session: str, field: str, lambda2: float, overrides: dict, reps: int = 11, device: int = 0,
                   seed: int = 1) -> float:
     """Least device time (ms) of `reps` stx_field_solve calls with a
-    resident random forcing under `overrides` (a failed configuration: +inf)."""
+    resident random forcing under `overrides`, L2 flushed before each (a
+    failed configuration: +inf)."""
     import ctypes as C
     import torch
     from . import Context, FORWARD, ModalMatrixSys, StxError
@@ -148,9 +156,12 @@ def solve_time_ms(session: str, field: str, lambda2: float, overrides: dict, rep
     F = ctx.new_field("f").load_physical(f).transform(FORWARD).zero_nyquist()
     U = ctx.new_field("u")
     stream = ctx.torch_stream()
+    flush = _l2_flush_buffer(device)
     times = []
     for k in range(reps + 2):
         e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        with torch.cuda.stream(stream):
+            flush.fill_(float(k))
         e0.record(stream)
         check(lib().stx_field_solve(sysm.handle, F.ptr(), U.ptr(), C.c_double(0.0), 0, None))
         e1.record(stream)
@@ -193,7 +204,7 @@ def batch_signature(specs) -> str:
 
 def batch_time_ms(specs, overrides: dict, reps: int = 11, device: int = 0) -> float:
     """Least device time (ms) of `reps` replays of the batch's CUDA graph
-    (stx_batch_launch) with the same overrides on every problem (+inf when a
+    (stx_batch_launch, L2 flushed before each) with the same overrides on every problem (+inf when a
     problem rejects them).  The problems are the uneven-batch dicts of
     sessions.uneven_batch (n, np, lambda2, seed), Dirichlet zero."""
     import tempfile
@@ -216,9 +227,12 @@ def batch_time_ms(specs, overrides: dict, reps: int = 11, device: int = 0) -> fl
             return float("inf")
     B = Batch(items)
     main = torch.cuda.ExternalStream(B.stream, device=f"cuda:{device}")
+    flush = _l2_flush_buffer(device)
     times = []
     for k in range(reps + 2):
         e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        with torch.cuda.stream(main):
+            flush.fill_(float(k))
         e0.record(main)
         B.launch()
         e1.record(main)
