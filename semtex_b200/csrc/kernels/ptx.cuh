@@ -87,6 +87,11 @@ __device__ __forceinline__ void cp_async8(void* dst, const void* src) {
 
 __device__ __forceinline__ void cp_async_wait_all() { asm volatile("cp.async.wait_all;" ::: "memory"); }
 
+// Close the group of this thread's cp.async copies issued so far; wait until
+// at most one group (the newest) is still in flight.
+__device__ __forceinline__ void cp_async_commit() { asm volatile("cp.async.commit_group;" ::: "memory"); }
+__device__ __forceinline__ void cp_async_wait_group1() { asm volatile("cp.async.wait_group 1;" ::: "memory"); }
+
 // Arrive on `bar` once all of this thread's earlier cp.async copies have
 // landed (the arrival is not added to the expected count: the barrier's
 // initial count must include it).

@@ -18,7 +18,7 @@
 namespace stx {
 
 constexpr int kSymTile = 32;
-constexpr int kSymLd = kSymTile + 1;  // entries per stored tile row
+constexpr int kSymLd = kSymTile;  // entries per stored tile row
 
 // Entry (r, c) of a tile, and its inverse (c = 32: the zero padding entry).
 __host__ __device__ inline int tile_pos(int r, int c) { return r * kSymLd + c; }

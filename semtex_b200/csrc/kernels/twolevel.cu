@@ -82,22 +82,88 @@ struct SymCursor {
   }
 };
 
+// Column of a tile held in position q (0..3) by a lane of column group cq
+// (0..7): two 16-byte pairs, 2 cq and 16 + 2 cq, so that the eight lanes
+// reading one tile row cover it in one conflict-free 128-byte access each.
+__host__ __device__ inline int col_of(int cq, int q) { return 16 * (q >> 1) + 2 * cq + (q & 1); }
+
+// The lane's four entries of a tile row in shared memory (zero when the row
+// is past the matrix).
+__device__ __forceinline__ void tile_row4(const double* row, int cq, bool ok, double (&e)[4]) {
+  if (ok) {
+    const double2 u = *reinterpret_cast<const double2*>(row + 2 * cq);
+    const double2 v = *reinterpret_cast<const double2*>(row + 16 + 2 * cq);
+    e[0] = u.x;
+    e[1] = u.y;
+    e[2] = v.x;
+    e[3] = v.y;
+  } else {
+    e[0] = e[1] = e[2] = e[3] = 0.0;
+  }
+}
+__device__ __forceinline__ void tile_row4(const float* row, int cq, bool ok, double (&e)[4]) {
+  if (ok) {
+    const float2 u = *reinterpret_cast<const float2*>(row + 2 * cq);
+    const float2 v = *reinterpret_cast<const float2*>(row + 16 + 2 * cq);
+    e[0] = u.x;
+    e[1] = u.y;
+    e[2] = v.x;
+    e[3] = v.y;
+  } else {
+    e[0] = e[1] = e[2] = e[3] = 0.0;
+  }
+}
+
+// The last two halving exchanges (lane bits 1, 0) of a sum over the 8 lanes
+// that share (lane >> 3): v[i] holds, after the first exchange (bit 2), the
+// pair sums of row group i (lanes with bit 2 set: the upper row of the
+// pair); lane l ends with the sum for position l & 7.
+__device__ __forceinline__ double reduce_scatter4_low(const double (&w)[4], int ln) {
+  double u[2];
+  const bool h1 = ln & 2, h0 = ln & 1;
+#pragma unroll
+  for (int i = 0; i < 2; ++i) {
+    const double send = h1 ? w[i] : w[2 + i], keep = h1 ? w[2 + i] : w[i];
+    u[i] = keep + __shfl_xor_sync(0xffffffffu, send, 2);
+  }
+  const double send = h0 ? u[0] : u[1], keep = h0 ? u[1] : u[0];
+  return keep + __shfl_xor_sync(0xffffffffu, send, 1);
+}
+
+// Sum over the 4 lanes that share (lane & 7) of v[q], q = 0..3: lane l ends
+// with the sum for q = l >> 3 (halving exchanges over lane bits 4, 3).
+__device__ __forceinline__ double reduce_scatter4_high(const double (&v)[4], int ln) {
+  double w[2];
+  const bool h4 = ln & 16, h3 = ln & 8;
+#pragma unroll
+  for (int i = 0; i < 2; ++i) {
+    const double send = h4 ? v[i] : v[2 + i], keep = h4 ? v[2 + i] : v[i];
+    w[i] = keep + __shfl_xor_sync(0xffffffffu, send, 16);
+  }
+  const double send = h3 ? w[0] : w[1], keep = h3 ? w[1] : w[0];
+  return keep + __shfl_xor_sync(0xffffffffu, send, 8);
+}
+
 // y[idx] += scale A x[idx] for every problem (and each of NF fields whose
 // vectors are fstride doubles apart): each warp streams its run of tiles
 // (SymWarp) through a ring of kSymStages buffers.  For a tile, lane 0
 // bulk-copies the tile and every lane copies (cp.async) the x entries of the
 // tile's column and row blocks, all completing on the buffer's mbarrier (count 1 + 32).
-// Per tile (I, J): direct part y_I += A_IJ x_J (lane = tile row), and for
-// J < I the transposed part y_J += A_IJ^T x_I (lane = tile column), four
-// independent partial sums per plane; y_I is accumulated along the row and
-// added at its end.  Waits are bounded; on expiry `status` is set and the
+// Per tile (I, J) every lane reads its 8 x 4 entries of the tile once from
+// shared memory (eight lanes cover a tile row with 16-byte reads) and forms
+// both products from registers: the direct part y_I += A_IJ x_J as partial
+// row sums over its four columns, summed over the eight lanes of a row by a
+// halving exchange of warp shuffles (one row per lane, accumulated along the
+// tile row and added at its end), and for J < I the transposed part
+// y_J += A_IJ^T x_I as partial column sums over its eight rows, summed over
+// the four lanes of a column the same way.  Waits are bounded; on expiry `status` is set and the
 // warp stops.  Two builds (DevModal::sym_regcap chooses): CAP 0, blocks of
 // up to 4 warps and the registers the code wants (no minimum block count:
 // giving one lets the compiler take up to 255); CAP 1, blocks of up to 8
 // warps and at most 80 registers (three such blocks per SM), a few spilled,
 // more resident warps.
 template <class T, int NF, int CAP>
-__global__ void __launch_bounds__(CAP ? 32 * kSymWarpsMax : 128, CAP ? 3 : 0)
+__global__ void __launch_bounds__(CAP ? 32 * kSymWarpsMax : 128, CAP ? 2 : 4)
     k_psymv(const T* __restrict__ pack, const SymProblem* __restrict__ probs, const SymWarp* __restrict__ warps,
             int nwarps, const double* __restrict__ X, double* __restrict__ Y, int rstride, size_t fstride, int nz,
             int* status, unsigned long long wait_ns) {
@@ -170,7 +236,12 @@ __global__ void __launch_bounds__(CAP ? 32 * kSymWarpsMax : 128, CAP ? 3 : 0)
   };
   for (int s = 0; s < kSymStages && s < W.count; ++s) issue(s);
   if (W.count == 0) pdl_wait();
-  double d0[NF], d1[NF];  // direct part of row 32 I + ln
+  // lane (rho, cq) = (lane >> 3, lane & 7): rows 4 t + rho (t = 0..7) and
+  // columns col_of(cq, q) (q = 0..3) of every tile; it collects row
+  // 4 cq + rho of the direct part and column col_of(cq, rho) of the
+  // transposed part
+  const int rho = ln >> 3, cq = ln & 7;
+  double d0[NF], d1[NF];  // direct part of row 32 I + 4 cq + rho
 #pragma unroll
   for (int f = 0; f < NF; ++f) d0[f] = d1[f] = 0.0;
   int done = 0;
@@ -181,77 +252,61 @@ __global__ void __launch_bounds__(CAP ? 32 * kSymWarpsMax : 128, CAP ? 3 : 0)
       break;
     }
     const int n = cc.P.n, m = cc.P.mode, I = cc.I, J = cc.J;
-    const bool two = nz > 1 && m > 0, sym = cc.P.ncol == 0;
+    const bool two = nz > 1 && m > 0, sym = cc.P.ncol == 0, trans = sym && J < I;
     const double scale = cc.P.scale;
     const T* A = reinterpret_cast<const T*>(sm.tile[s]);
     const double2* xs = sm.x[s];
     const int h = sym_rows(n, I);
-    // output positions (column block for the transposed part, row block at a
-    // row's end), loaded before the products to overlap their latency
+    // output positions (the column this lane collects for the transposed
+    // part, the row it collects where the tile row ends), loaded before the
+    // products to overlap their latency
     const bool row_end = cc.row_last() || done + 1 == W.count;
-    const int g_col = (sym && J < I) ? __ldg(cc.P.idx + kSymTile * J + ln) : 0;  // J < T - 1: a full tile column
-    const int g_row = (row_end && ln < h) ? __ldg(cc.P.idx + kSymTile * I + ln) : 0;
-    if (ln < h) {
-      const T* Ar = A + ln * kSymLd;
-      double p0[NF][4], p1[NF][4];
-#pragma unroll
-      for (int f = 0; f < NF; ++f)
-#pragma unroll
-        for (int u = 0; u < 4; ++u) p0[f][u] = p1[f][u] = 0.0;
-#pragma unroll
-      for (int c = 0; c < kSymTile; ++c) {
-        const double a = static_cast<double>(Ar[c]);
-#pragma unroll
-        for (int f = 0; f < NF; ++f) {
-          const double2 x = xs[c * NF + f];
-          p0[f][c & 3] = fma(a, x.x, p0[f][c & 3]);
-          p1[f][c & 3] = fma(a, x.y, p1[f][c & 3]);
-        }
-      }
-#pragma unroll
-      for (int f = 0; f < NF; ++f) {
-        d0[f] += (p0[f][0] + p0[f][1]) + (p0[f][2] + p0[f][3]);
-        d1[f] += (p1[f][0] + p1[f][1]) + (p1[f][2] + p1[f][3]);
-      }
-    }
+    const int rrow = 4 * cq + rho;
+    const int g_col = trans ? __ldg(cc.P.idx + kSymTile * J + col_of(cq, rho)) : 0;  // J < I: a full block
+    const int g_row = (row_end && rrow < h) ? __ldg(cc.P.idx + kSymTile * I + rrow) : 0;
     double* Y0 = Y + static_cast<size_t>(2 * m) * rstride;
     double* Y1 = Y0 + rstride;
-    if (sym && J < I) {
-      double p0[NF][4], p1[NF][4];
 #pragma unroll
-      for (int f = 0; f < NF; ++f)
+    for (int f = 0; f < NF; ++f) {
+      double2 xc[4];  // x of the lane's four columns (column block)
 #pragma unroll
-        for (int u = 0; u < 4; ++u) p0[f][u] = p1[f][u] = 0.0;
-      if (h == kSymTile) {
+      for (int q = 0; q < 4; ++q) xc[q] = xs[col_of(cq, q) * NF + f];
+      double w0[4], w1[4], tp0[4] = {0.0, 0.0, 0.0, 0.0}, tp1[4] = {0.0, 0.0, 0.0, 0.0};
+      const bool h2 = ln & 4;
 #pragma unroll
-        for (int r = 0; r < kSymTile; ++r) {
-          const double a = static_cast<double>(A[r * kSymLd + ln]);
+      for (int i = 0; i < 4; ++i) {
+        // rows 4 i + rho and 16 + 4 i + rho, their direct partial sums
+        // combined at once over lane bit 2 (the first halving exchange)
+        double dp[2][2];
 #pragma unroll
-          for (int f = 0; f < NF; ++f) {
-            const double2 x = xs[(kSymTile + r) * NF + f];
-            p0[f][r & 3] = fma(a, x.x, p0[f][r & 3]);
-            p1[f][r & 3] = fma(a, x.y, p1[f][r & 3]);
+        for (int k = 0; k < 2; ++k) {
+          const int r = 16 * k + 4 * i + rho;
+          double e[4];
+          tile_row4(A + r * kSymLd, cq, r < h, e);
+          dp[k][0] = fma(e[0], xc[0].x, fma(e[1], xc[1].x, fma(e[2], xc[2].x, e[3] * xc[3].x)));
+          dp[k][1] = fma(e[0], xc[0].y, fma(e[1], xc[1].y, fma(e[2], xc[2].y, e[3] * xc[3].y)));
+          if (trans) {
+            const double2 xr = xs[(kSymTile + r) * NF + f];
+#pragma unroll
+            for (int q = 0; q < 4; ++q) {
+              tp0[q] = fma(e[q], xr.x, tp0[q]);
+              tp1[q] = fma(e[q], xr.y, tp1[q]);
+            }
           }
         }
-      } else {
-        for (int r = 0; r < h; ++r) {
-          const double a = static_cast<double>(A[r * kSymLd + ln]);
-#pragma unroll
-          for (int f = 0; f < NF; ++f) {
-            const double2 x = xs[(kSymTile + r) * NF + f];
-            p0[f][0] = fma(a, x.x, p0[f][0]);
-            p1[f][0] = fma(a, x.y, p1[f][0]);
-          }
-        }
+        w0[i] = (h2 ? dp[1][0] : dp[0][0]) + __shfl_xor_sync(0xffffffffu, h2 ? dp[0][0] : dp[1][0], 4);
+        w1[i] = (h2 ? dp[1][1] : dp[0][1]) + __shfl_xor_sync(0xffffffffu, h2 ? dp[0][1] : dp[1][1], 4);
       }
-#pragma unroll
-      for (int f = 0; f < NF; ++f) {
-        atomicAdd(&Y0[f * fstride + g_col], scale * ((p0[f][0] + p0[f][1]) + (p0[f][2] + p0[f][3])));
-        if (two) atomicAdd(&Y1[f * fstride + g_col], scale * ((p1[f][0] + p1[f][1]) + (p1[f][2] + p1[f][3])));
+      d0[f] += reduce_scatter4_low(w0, ln);
+      d1[f] += reduce_scatter4_low(w1, ln);
+      if (trans) {
+        const double s0 = reduce_scatter4_high(tp0, ln), s1 = reduce_scatter4_high(tp1, ln);
+        atomicAdd(&Y0[f * fstride + g_col], scale * s0);
+        if (two) atomicAdd(&Y1[f * fstride + g_col], scale * s1);
       }
     }
     if (row_end) {
-      if (ln < h) {
+      if (rrow < h) {
 #pragma unroll
         for (int f = 0; f < NF; ++f) {
           atomicAdd(&Y0[f * fstride + g_row], scale * d0[f]);

@@ -156,9 +156,13 @@ def _c5(tmp_path):
     vel = {c: ic[c] for c in "uvw"}
     shape = (ctx.nz, ctx.nel, ctx.np, ctx.np)
     base = {"u": np.broadcast_to(1 - y * y, shape), "v": np.zeros(shape), "w": np.zeros(shape)}
-    # a second divergence-free perturbation of the same family as the direction
+    # a second divergence-free perturbation of the same family as the
+    # direction, scaled to unit amplitude (max |d| = 1), so that the central
+    # difference step h = 1e-6 perturbs the initial velocity by 1e-6
     alt = sessions.channel_initial(x, y, np.arange(ctx.nz) * 2 * np.pi / ctx.nz, seed=7)
     direction = {c: alt[c] - base[c] for c in "uvw"}
+    amp = max(float(np.abs(v).max()) for v in direction.values())
+    direction = {c: v / amp for c, v in direction.items()}
     return ctx, vel, base, direction
 
 
