@@ -48,6 +48,8 @@ __device__ __forceinline__ unsigned long long global_ns() {
 // Default bound of an mbarrier wait, and of every wait that drains copies
 // still in flight after an expired one: 2 s of wall time.
 constexpr unsigned long long kWaitNs = 2000000000ull;
+// Longest sleep of one try_wait (the bound above is checked between them).
+constexpr unsigned kWaitHintNs = 100000u;
 
 // Bounded wait (`limit_ns` of wall time) for phase `parity` of an mbarrier;
 // false if the bound expired.  limit_ns = 0 probes once without blocking
@@ -67,12 +69,15 @@ __device__ __forceinline__ bool mbar_wait(uint64_t* bar, unsigned parity,
   }
   const unsigned long long t0 = global_ns();
   for (;;) {
+    // the thread may sleep in try_wait until the phase completes, for at
+    // most the hint (ns): waiting warps then take no issue slots and no
+    // shared-memory cycles from the warps that compute
     uint32_t done;
     asm volatile(
-        "{\n .reg .pred p;\n mbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2;\n"
+        "{\n .reg .pred p;\n mbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2, %3;\n"
         " selp.u32 %0, 1, 0, p;\n}\n"
         : "=r"(done)
-        : "r"(a), "r"(parity)
+        : "r"(a), "r"(parity), "r"(kWaitHintNs)
         : "memory");
     if (done) return true;
     if (global_ns() - t0 > limit_ns) return false;
