@@ -102,7 +102,7 @@ struct stx_dns_adjoint {
   // recorded run
   int s0 = -1, s1 = -1;
   size_t state_doubles = 0;
-  std::vector<DevBuf> ckpt;  // state at s0 + j * every, and at s1 last
+  std::vector<DevBuf> ckpt;  // state at s0 + j * every, and at s1 last (ckpt_host.size() in use)
   std::vector<DnsHostState> ckpt_host;
   // level rings (level l at l mod (nord + 1)): adjoint (or tangent) of the
   // velocity and nonlinear terms of level l, of its pressure-BC level and u.n
@@ -532,7 +532,7 @@ void download(stx_dns* d, const double* f, double* h) {
 }
 
 void require_recorded(const stx_dns_adjoint* a) {
-  if (a->s0 < 0 || a->ckpt.empty()) throw AdjError(STX_EINVAL, "no recorded run (stx_dns_adjoint_record)");
+  if (a->s0 < 0 || a->ckpt_host.empty()) throw AdjError(STX_EINVAL, "no recorded run (stx_dns_adjoint_record)");
 }
 
 }  // namespace
@@ -615,13 +615,15 @@ int stx_dns_adjoint_record(stx_dns_adjoint* a, int nsteps) {
     stx_dns* d = a->d;
     cudaSetDevice(d->ctx->device);
     ck(cudaStreamSynchronize(d->ctx->stream), "sync");
-    a->ckpt.clear();
+    // checkpoint buffers are kept from record to record (allocated only
+    // when a longer run needs more of them)
     a->ckpt_host.clear();
     a->s0 = a->s1 = -1;
     const int s0 = d->step;
     auto keep = [&] {
-      a->ckpt.emplace_back(a->state_doubles);
-      save_state(a, a->ckpt.back());
+      const size_t j = a->ckpt_host.size();
+      if (j == a->ckpt.size()) a->ckpt.emplace_back(a->state_doubles);
+      save_state(a, a->ckpt[j]);
       a->ckpt_host.push_back(dns_host_state(d));
     };
     keep();
@@ -655,7 +657,7 @@ int stx_dns_adjoint_backward(stx_dns_adjoint* a, const double* h_seed, double* h
       inverse_t(d, f);
       zero_nyquist(d, f);
     }
-    const int nseg = static_cast<int>(a->ckpt.size()) - 1;
+    const int nseg = static_cast<int>(a->ckpt_host.size()) - 1;
     for (int j = nseg - 1; j >= 0; --j) {
       const int sa = a->s0 + j * a->every, sb = std::min(sa + a->every, a->s1);
       load_state(a, j);
@@ -718,7 +720,7 @@ int stx_dns_adjoint_tangent(stx_dns_adjoint* a, const double* h_dir, double* h_o
       download(d, a->X, h_out + nphys * c);
     }
     ck(cudaStreamSynchronize(d->ctx->stream), "sync");
-    load_state(a, static_cast<int>(a->ckpt.size()) - 1);
+    load_state(a, static_cast<int>(a->ckpt_host.size()) - 1);
     ck(cudaStreamSynchronize(d->ctx->stream), "sync");
   });
 }
@@ -729,7 +731,7 @@ int stx_dns_adjoint_info(const stx_dns_adjoint* a, int* first_step, int* last_st
     if (!a) throw AdjError(STX_EINVAL, "null argument");
     if (first_step) *first_step = a->s0;
     if (last_step) *last_step = a->s1;
-    if (checkpoint_bytes) *checkpoint_bytes = sizeof(double) * a->state_doubles * a->ckpt.size();
+    if (checkpoint_bytes) *checkpoint_bytes = sizeof(double) * a->state_doubles * a->ckpt_host.size();
   });
 }
 
