@@ -37,6 +37,7 @@
 #include <cmath>
 #include <cstring>
 #include <map>
+#include <set>
 #include <stdexcept>
 #include <string>
 #include <vector>
@@ -117,6 +118,14 @@ struct stx_dns_adjoint {
   double* dlines = nullptr;      // tangent pressure BC lines [nz][nline of p]
   std::vector<double*> seg;      // [every][ncom] recorded u^n of a segment
   std::vector<int> seg_form;
+  std::vector<double*> ucur;     // [ncom] u^n of the step being transposed
+  // steady transposed steps (all orders at N_TIME) replayed as CUDA graphs,
+  // one per (level ring position, nonlinear form); a class runs directly
+  // once (work buffers, systems, launch attributes settle), is captured the
+  // second time
+  bool use_graph = true;
+  std::map<int, cudaGraphExec_t> rgraph;
+  std::set<int> rseen;
   std::map<int, stx_modal*> vel_sys;  // DIRECT velocity systems by order (start-up, ITERATIVE)
   std::vector<stx_modal*> own_sys;
 };
@@ -382,6 +391,52 @@ void reverse_step(stx_dns_adjoint* a, int s, const double* const* un, int form) 
   }
 }
 
+// The transpose of step s on u^n in a->ucur: directly, or as the replay of
+// the captured graph of its class (steady steps: every order at N_TIME).
+void run_reverse(stx_dns_adjoint* a, int s, int form) {
+  stx_dns* d = a->d;
+  cudaStream_t st = d->ctx->stream;
+  if (!a->use_graph || s <= d->nord) {
+    reverse_step(a, s, a->ucur.data(), form);
+    return;
+  }
+  const int key = ring(a, s) * 4 + (form + 1);
+  const auto it = a->rgraph.find(key);
+  if (it != a->rgraph.end()) {
+    ck(cudaGraphLaunch(it->second, st), "graph launch");
+    return;
+  }
+  if (a->rseen.insert(key).second) {
+    reverse_step(a, s, a->ucur.data(), form);
+    return;
+  }
+  if (cudaStreamBeginCapture(st, cudaStreamCaptureModeThreadLocal) != cudaSuccess) {
+    cudaGetLastError();
+    a->use_graph = false;
+    reverse_step(a, s, a->ucur.data(), form);
+    return;
+  }
+  bool ok = true;
+  try {
+    reverse_step(a, s, a->ucur.data(), form);
+  } catch (const std::exception&) {
+    ok = false;
+  }
+  cudaGraph_t graph = nullptr;
+  const cudaError_t e = cudaStreamEndCapture(st, &graph);
+  cudaGraphExec_t exec = nullptr;
+  ok = ok && e == cudaSuccess && graph && cudaGraphInstantiate(&exec, graph, 0) == cudaSuccess;
+  if (graph) cudaGraphDestroy(graph);
+  cudaGetLastError();  // clear a capture error: the step runs directly instead
+  if (!ok) {
+    a->use_graph = false;
+    reverse_step(a, s, a->ucur.data(), form);
+    return;
+  }
+  a->rgraph[key] = exec;
+  ck(cudaGraphLaunch(exec, st), "graph launch");
+}
+
 // -- the tangent-linear step s along the trajectory (u^n given) -------------
 void tangent_step(stx_dns_adjoint* a, int s, const double* const* un, int form) {
   stx_dns* d = a->d;
@@ -565,7 +620,7 @@ int stx_dns_adjoint_create(stx_dns* d, int checkpoint_every, stx_dns_adjoint** o
     a->nring = d->nord + 1;
     const int ncom = d->ncom;
     const size_t fs = d->fsize;
-    const int nwork = 2 * a->nring * ncom + 5 * ncom + 9;
+    const int nwork = 2 * a->nring * ncom + 6 * ncom + 9;
     double* base = static_cast<double*>(a->arena.alloc(sizeof(double) * fs * nwork));
     ck(cudaMemset(base, 0, sizeof(double) * fs * nwork), "memset");
     int k = 0;
@@ -576,7 +631,7 @@ int stx_dns_adjoint_create(stx_dns* d, int checkpoint_every, stx_dns_adjoint** o
         a->Au[r].push_back(base + fs * k++);
         a->AN[r].push_back(base + fs * k++);
       }
-    for (auto* v : {&a->Uh, &a->Fb, &a->Up, &a->A, &a->dUp})
+    for (auto* v : {&a->Uh, &a->Fb, &a->Up, &a->A, &a->dUp, &a->ucur})
       for (int c = 0; c < ncom; ++c) v->push_back(base + fs * k++);
     for (double** p : {&a->pb, &a->sp, &a->T1, &a->Pb, &a->Tc, &a->Tcb, &a->Bz, &a->X, &a->Y}) *p = base + fs * k++;
     if (d->nh) {
@@ -595,6 +650,7 @@ int stx_dns_adjoint_create(stx_dns* d, int checkpoint_every, stx_dns_adjoint** o
     double* sb = static_cast<double*>(a->arena.alloc(sizeof(double) * fs * ncom * checkpoint_every));
     for (int j = 0; j < ncom * checkpoint_every; ++j) a->seg.push_back(sb + fs * j);
     a->seg_form.assign(checkpoint_every, 0);
+    a->use_graph = d->use_graph;
     *out = guard.release();
   });
 }
@@ -604,6 +660,7 @@ int stx_dns_adjoint_destroy(stx_dns_adjoint* a) {
     if (!a) return;
     cudaSetDevice(a->d->ctx->device);
     cudaStreamSynchronize(a->d->ctx->stream);
+    for (auto& g : a->rgraph) cudaGraphExecDestroy(g.second);
     for (stx_modal* m : a->own_sys) stx_modal_destroy(m);
     delete a;
   });
@@ -669,7 +726,8 @@ int stx_dns_adjoint_backward(stx_dns_adjoint* a, const double* h_seed, double* h
       }
       for (int s = sb; s > sa; --s) {
         const int slot = s - sa - 1;
-        reverse_step(a, s, &a->seg[slot * ncom], a->seg_form[slot]);
+        for (int c = 0; c < ncom; ++c) copyf(d, a->ucur[c], a->seg[slot * ncom + c]);
+        run_reverse(a, s, a->seg_form[slot]);
       }
     }
     // gradient w.r.t. the physical velocity given to stx_dns_set_field
