@@ -953,8 +953,14 @@ cudaError_t helmholtz_direct_solve(const DevGeom& g, const DevNumbering& N, cons
   const size_t pz = static_cast<size_t>(rstride) * (k1 - k0);
   if (ev) cudaEventRecord(ev[0], st);
   const bool pdl = S.pdl != 0;
-  cudaError_t err = zero_ranges(pdl, R + static_cast<size_t>(rstride) * k0, pz,
-                                G + static_cast<size_t>(rstride) * k0, pz, st);
+  // R, G and (two-level) the skeleton solution zeroed in one kernel
+  ZeroRanges zr;
+  zr.add(R + static_cast<size_t>(rstride) * k0, pz);
+  zr.add(G + static_cast<size_t>(rstride) * k0, pz);
+  if (S.l2) zr.add(twolevel_solution(work + 2 * static_cast<size_t>(rstride) * nz, rstride, nz) +
+                       static_cast<size_t>(rstride) * k0,
+                   pz);
+  cudaError_t err = zero_ranges(pdl, zr, st);
   if (err != cudaSuccess) return err;
   const bool has_ess = N.nglobal > N.nsolve;
   const int nedge_nodes = N.nedge * g.np;
@@ -1002,7 +1008,8 @@ cudaError_t helmholtz_direct_solve(const DevGeom& g, const DevNumbering& N, cons
     double* w3 = rr + static_cast<size_t>(rstride) * nz;
     if (mixed && S.refine > 0)
       err = cudaMemcpyAsync(R0 + off, R + off, sizeof(double) * pz, cudaMemcpyDeviceToDevice, st);
-    if (err == cudaSuccess) err = twolevel_solve(S, g, N, R, rstride, w2, nz, st, ev ? ev[2] : nullptr, mixed);
+    if (err == cudaSuccess)
+      err = twolevel_solve(S, g, N, R, rstride, w2, nz, st, ev ? ev[2] : nullptr, mixed, /*y_zeroed=*/true);
     if (err != cudaSuccess) return err;
     double* Y = twolevel_solution(w2, rstride, nz);
     for (int it = 0; it < S.refine; ++it) {
@@ -1064,13 +1071,19 @@ cudaError_t helmholtz_direct_solve_fields(const DevGeom& g, const DevNumbering* 
   const size_t pz = static_cast<size_t>(rstride) * (k1 - k0), off = static_cast<size_t>(rstride) * k0;
   const bool has_ess = N[0]->nglobal > N[0]->nsolve;
   const ElementPlan ep = element_plan(g, S, has_ess);
-  cudaError_t err = cudaSuccess;
+  const bool pdl = S.pdl != 0;
+  // every field's R, G and skeleton solution zeroed in one kernel
+  ZeroRanges zr;
+  for (int f = 0; f < nf; ++f) {
+    zr.add(R + f * fs + off, pz);
+    zr.add(G + f * fs + off, pz);
+    zr.add(Y + f * fs + off, pz);
+  }
+  cudaError_t err = zero_ranges(pdl, zr, st);
+  if (err != cudaSuccess) return err;
   for (int f = 0; f < nf; ++f) {
     double* Rf = R + f * fs;
     double* Gf = G + f * fs;
-    const bool pdl = S.pdl != 0;
-    err = zero_ranges(pdl, Rf + off, pz, Gf + off, pz, st);
-    if (err != cudaSuccess) return err;
     const int nedge_nodes = N[f]->nedge * g.np;
     if (has_ess && nedge_nodes && N[f]->ness) {
       dim3 grid((nedge_nodes + 127) / 128, k1 - k0);
@@ -1083,7 +1096,7 @@ cudaError_t helmholtz_direct_solve_fields(const DevGeom& g, const DevNumbering* 
     }
   }
   if (after_condense) cudaEventRecord(after_condense, st);
-  err = twolevel_solve_fields(S, g, *N[0], R, Y, fs, nf, rstride, nz, st);
+  err = twolevel_solve_fields(S, g, *N[0], R, Y, fs, nf, rstride, nz, st, /*y_zeroed=*/true);
   if (err != cudaSuccess) return err;
   for (int f = 0; f < nf; ++f)
     element_recover(ep, g, *N[f], S, F[f], has_ess ? G + f * fs : nullptr, rstride, Y + f * fs, rstride, U[f], st);

@@ -370,35 +370,45 @@ cudaError_t launch_psymv(const DevModal& S, const SymProblem* probs, const SymWa
 
 namespace {
 
-__global__ void k_zero_ranges(double* __restrict__ a, size_t na, double* __restrict__ b, size_t nb) {
+__global__ void k_zero_ranges(ZeroRanges z, size_t total) {
   pdl_trigger();
   pdl_wait();
-  for (size_t i = blockIdx.x * static_cast<size_t>(blockDim.x) + threadIdx.x; i < na + nb;
+  for (size_t i = blockIdx.x * static_cast<size_t>(blockDim.x) + threadIdx.x; i < total;
        i += static_cast<size_t>(gridDim.x) * blockDim.x) {
-    if (i < na) a[i] = 0.0;
-    else b[i - na] = 0.0;
+    size_t j = i;
+    int r = 0;
+    while (r + 1 < z.count && j >= z.n[r]) j -= z.n[r++];
+    z.p[r][j] = 0.0;
   }
 }
 
 }  // namespace
 
-cudaError_t zero_ranges(bool pdl, double* a, size_t na, double* b, size_t nb, cudaStream_t st) {
-  if (!b) nb = 0;
-  const size_t n = na + nb;
+cudaError_t zero_ranges(bool pdl, const ZeroRanges& z, cudaStream_t st) {
+  size_t n = 0;
+  for (int r = 0; r < z.count; ++r) n += z.n[r];
   if (n == 0) return cudaSuccess;
   const unsigned blocks = static_cast<unsigned>(std::min<size_t>((n + 255) / 256, 148 * 8));
-  return launch_ex(pdl, k_zero_ranges, dim3(blocks), dim3(256), 0, st, a, na, b, nb);
+  return launch_ex(pdl, k_zero_ranges, dim3(blocks), dim3(256), 0, st, z, n);
+}
+
+cudaError_t zero_ranges(bool pdl, double* a, size_t na, double* b, size_t nb, cudaStream_t st) {
+  ZeroRanges z;
+  z.add(a, na);
+  z.add(b, nb);
+  return zero_ranges(pdl, z, st);
 }
 
 size_t twolevel_workspace_doubles(int rstride, int nz) { return static_cast<size_t>(rstride) * nz; }
 
 cudaError_t twolevel_solve(const DevModal& S, const DevGeom& g, const DevNumbering& N, double* R, int rstride,
-                           double* work, int nz, cudaStream_t st, cudaEvent_t mid, bool fp32) {
+                           double* work, int nz, cudaStream_t st, cudaEvent_t mid, bool fp32, bool y_zeroed) {
   double* Yv = twolevel_solution(work, rstride, nz);  // y_I, then the whole skeleton solution
   // planes of the launch's modes
   const int k0 = nz > 1 ? 2 * S.mode0 : 0, k1 = nz > 1 ? std::min(nz, 2 * (S.mode0 + S.nmodes)) : 1;
-  cudaError_t err = zero_ranges(S.pdl != 0, Yv + static_cast<size_t>(rstride) * k0,
-                                static_cast<size_t>(rstride) * (k1 - k0), nullptr, 0, st);
+  cudaError_t err = y_zeroed ? cudaSuccess
+                             : zero_ranges(S.pdl != 0, Yv + static_cast<size_t>(rstride) * k0,
+                                           static_cast<size_t>(rstride) * (k1 - k0), nullptr, 0, st);
   if (err != cudaSuccess) return err;
   // y_I = S_II^-1 R_I; r_B = R_B - S_BI y_I
   err = launch_psymv(S, S.prob_patch, S.warp_patch, S.nwarp_patch, R, Yv, rstride, nz, fp32, st);
@@ -415,13 +425,17 @@ cudaError_t twolevel_solve(const DevModal& S, const DevGeom& g, const DevNumberi
 }
 
 cudaError_t twolevel_solve_fields(const DevModal& S, const DevGeom& g, const DevNumbering& N, double* R,
-                                  double* Y, size_t fstride, int nf, int rstride, int nz, cudaStream_t st) {
+                                  double* Y, size_t fstride, int nf, int rstride, int nz, cudaStream_t st,
+                                  bool y_zeroed) {
   if (nf < 1 || nf > 3 || S.refine > 0 || S.l2_pack32) return cudaErrorInvalidValue;
   const int k0 = nz > 1 ? 2 * S.mode0 : 0, k1 = nz > 1 ? std::min(nz, 2 * (S.mode0 + S.nmodes)) : 1;
   cudaError_t err = cudaSuccess;
-  for (int f = 0; f < nf && err == cudaSuccess; ++f)
-    err = zero_ranges(S.pdl != 0, Y + f * fstride + static_cast<size_t>(rstride) * k0,
-                      static_cast<size_t>(rstride) * (k1 - k0), nullptr, 0, st);
+  if (!y_zeroed) {
+    ZeroRanges z;
+    for (int f = 0; f < nf; ++f)
+      z.add(Y + f * fstride + static_cast<size_t>(rstride) * k0, static_cast<size_t>(rstride) * (k1 - k0));
+    err = zero_ranges(S.pdl != 0, z, st);
+  }
   if (err != cudaSuccess) return err;
   err = launch_psymv(S, S.prob_patch, S.warp_patch, S.nwarp_patch, R, Y, rstride, nz, false, st, nf, fstride);
   if (err != cudaSuccess) return err;
