@@ -1281,10 +1281,10 @@ int stx_elliptic_solve_host_batch(stx_modal* sys, int n, const double* const* h_
     const double tol = ctx->S.tokens.value("TOL_REL");
     const int smax = ctx->S.tokens.ivalue("STEP_MAX");
     for (int i = 0; i < n; ++i) {
-      const int b = i & 1;
+      const int b = i % stx_context::kIoSets;
       double* dF = ctx->d_io2 + set * b;
       double* dU = dF + ps * nz;
-      // in: set b's forcing is free once solve i - 2 has run
+      // in: set b's forcing is free once solve i - kIoSets has run
       cuda_check(cudaStreamWaitEvent(ctx->s_h2d, ctx->ev_comp[b], 0), "wait");
       cuda_check(cudaMemcpy2DAsync(dF, sizeof(double) * ps, h_forcing[i], sizeof(double) * nplane,
                                    sizeof(double) * nplane, nz, cudaMemcpyHostToDevice, ctx->s_h2d),

@@ -168,23 +168,26 @@ struct stx_context {
       aux_ev.push_back(e);
     }
   }
-  // Pipelined host-buffer solves: two sets of device forcing / solution
-  // planes, the copy streams (host -> device, device -> host) and the
-  // events that hand a set from stage to stage.
-  double* d_io2 = nullptr;  // [2][2][nz][plane_size]
+  // Pipelined host-buffer solves: kIoSets sets of device forcing / solution
+  // planes (a third set, so that the copy in of solve i + 1, solve i and the
+  // copy out of solve i - 1 never share one, measured no faster: the two
+  // PCIe directions bound the pipeline), the copy streams (host -> device,
+  // device -> host) and the events that hand a set from stage to stage.
+  static constexpr int kIoSets = 2;
+  double* d_io2 = nullptr;  // [kIoSets][2][nz][plane_size]
   cudaStream_t s_h2d = nullptr, s_d2h = nullptr;
-  cudaEvent_t ev_in[2] = {nullptr, nullptr}, ev_comp[2] = {nullptr, nullptr}, ev_out[2] = {nullptr, nullptr};
+  cudaEvent_t ev_in[kIoSets] = {}, ev_comp[kIoSets] = {}, ev_out[kIoSets] = {};
   void ensure_pipeline(size_t doubles_per_set) {
     if (!d_io2) {
-      d_io2 = static_cast<double*>(arena.alloc(sizeof(double) * 2 * doubles_per_set));
-      if (cudaMemset(d_io2, 0, sizeof(double) * 2 * doubles_per_set) != cudaSuccess)
+      d_io2 = static_cast<double*>(arena.alloc(sizeof(double) * kIoSets * doubles_per_set));
+      if (cudaMemset(d_io2, 0, sizeof(double) * kIoSets * doubles_per_set) != cudaSuccess)
         throw std::runtime_error("memset of the pipeline buffers failed");
     }
     if (!s_h2d) {
       if (cudaStreamCreateWithFlags(&s_h2d, cudaStreamNonBlocking) != cudaSuccess ||
           cudaStreamCreateWithFlags(&s_d2h, cudaStreamNonBlocking) != cudaSuccess)
         throw std::runtime_error("stream creation failed");
-      for (int b = 0; b < 2; ++b)
+      for (int b = 0; b < kIoSets; ++b)
         if (cudaEventCreateWithFlags(&ev_in[b], cudaEventDisableTiming) != cudaSuccess ||
             cudaEventCreateWithFlags(&ev_comp[b], cudaEventDisableTiming) != cudaSuccess ||
             cudaEventCreateWithFlags(&ev_out[b], cudaEventDisableTiming) != cudaSuccess)
@@ -205,7 +208,7 @@ struct stx_context {
     for (auto e : stagger_ev) cudaEventDestroy(e);
     if (s_h2d) cudaStreamDestroy(s_h2d);
     if (s_d2h) cudaStreamDestroy(s_d2h);
-    for (int b = 0; b < 2; ++b)
+    for (int b = 0; b < kIoSets; ++b)
       for (cudaEvent_t e : {ev_in[b], ev_comp[b], ev_out[b]})
         if (e) cudaEventDestroy(e);
     if (d_work) cudaFree(d_work);
