@@ -26,11 +26,11 @@ constexpr int kMaxWarps = 32;
 constexpr int kUnitTiles = 4;  // 8x8 tiles per warp unit of the product: 8 rows x 32 columns
 
 struct ElemSmem {
-  size_t a, b, d, q, flag, bits, idx, bytes;
+  size_t a, b, d, q, flag, bits, idx, num, bytes;
 };
 
 // [mbarrier | A rows | B columns | D | Q4 / lift scratch | column flags |
-//  override bits | pmap, emap, chunk elements]
+//  override bits | pmap, emap, chunk elements | the chunk's btog, bmask]
 __host__ __device__ inline ElemSmem elem_layout(int a_doubles, int cm, int ldb, int np, int nn, int next, bool lift) {
   ElemSmem L;
   L.a = 16;
@@ -43,29 +43,42 @@ __host__ __device__ inline ElemSmem elem_layout(int a_doubles, int cm, int ldb, 
   L.bits = L.flag + sizeof(int) * 2 * static_cast<size_t>(cm);
   const int nwords = (next + 31) / 32;
   L.idx = L.bits + sizeof(unsigned) * 2 * static_cast<size_t>(cm) * nwords;
-  L.bytes = (L.idx + sizeof(int) * (static_cast<size_t>(nn) + nn + cm) + 15) / 16 * 16;
+  L.num = L.idx + sizeof(int) * (static_cast<size_t>(nn) + nn + cm);
+  L.bytes = (L.num + sizeof(int) * 2 * static_cast<size_t>(cm) * next + 15) / 16 * 16;
   return L;
 }
 
 // Small index tables in shared memory (the asynchronous copies stream
-// through L1, so global index reads would go back to L2 every time).
+// through L1, so global index reads would go back to L2 every time), the
+// chunk's numbering included: set-up data, loaded before the kernel waits
+// for its predecessor.
 struct ElemIdx {
-  const int* pmap;  // [nn] boundary-major position of node t
-  const int* emap;  // [nn] node at boundary-major position p
-  const int* el;    // [cnt] the chunk's elements
+  const int* pmap;   // [nn] boundary-major position of node t
+  const int* emap;   // [nn] node at boundary-major position p
+  const int* el;     // [cnt] the chunk's elements
+  const int* btog;   // [cnt][next] global number of boundary node a of chunk element l
+  const int* bmask;  // [cnt][next] its essential flag
 };
 
-__device__ __forceinline__ ElemIdx load_idx(const DevGeom& g, unsigned char* sraw, const ElemSmem& L, const int* el,
-                                            int cnt) {
+__device__ __forceinline__ ElemIdx load_idx(const DevGeom& g, const DevNumbering& N, unsigned char* sraw,
+                                            const ElemSmem& L, const int* el, int cnt) {
   int* sp = reinterpret_cast<int*>(sraw + L.idx);
   int* se = sp + g.npnp;
   int* sl = se + g.npnp;
+  int* sb = reinterpret_cast<int*>(sraw + L.num);
+  int* sm = sb + static_cast<size_t>(cnt) * g.next;
   for (int t = threadIdx.x; t < g.npnp; t += blockDim.x) {
     sp[t] = __ldg(g.pmap + t);
     se[t] = __ldg(g.emap + t);
   }
   for (int l = threadIdx.x; l < cnt; l += blockDim.x) sl[l] = __ldg(el + l);
-  return ElemIdx{sp, se, sl};
+  for (int q = threadIdx.x; q < cnt * g.next; q += blockDim.x) {
+    const int l = q / g.next, a = q - l * g.next;
+    const int e = __ldg(el + l);
+    sb[q] = __ldg(N.btog + e * g.next + a);
+    sm[q] = __ldg(N.bmask + e * g.next + a);
+  }
+  return ElemIdx{sp, se, sl, sb, sm};
 }
 
 // Row of node t of a column: natural node order or boundary-major order.
@@ -170,13 +183,13 @@ __device__ void scan_boundary(const DevGeom& g, const DevNumbering& N, const dou
         const int col = c0 + j * nwp;
         int slot, l;
         col_slot(min(col, ncol - 1), cnt, slot, l);
-        const int eb = X.el[l] * next;
+        const int eb = l * next;
 #pragma unroll
         for (int h = 0; h < 2; ++h) {
           const int a = a0 + 32 * h + ln;
           const bool ok = col < ncol && a < next;
-          gi[j][h] = ok ? __ldg(N.btog + eb + a) : -1;
-          bm[j][h] = (ok && G) ? __ldg(N.bmask + eb + a) : 0;
+          gi[j][h] = ok ? X.btog[eb + a] : -1;
+          bm[j][h] = (ok && G) ? X.bmask[eb + a] : 0;
         }
       }
       double gv[kColBatch][2];
@@ -249,7 +262,7 @@ __device__ void lift_columns(const DevGeom& g, const DevNumbering& N, const doub
     for (int q = lane; q < nn; q += 32) su[q] = 0.0;
     __syncwarp();
     for (int q = lane; q < next; q += 32)
-      if (__ldg(N.bmask + e * next + q)) su[X.emap[q]] = Gp[__ldg(N.btog + e * next + q)];
+      if (X.bmask[l * next + q]) su[X.emap[q]] = Gp[X.btog[l * next + q]];
     __syncwarp();
     for (int q = lane; q < nn; q += 32) {
       const int i = q / np, j = q - (q / np) * np;
@@ -322,7 +335,7 @@ __global__ void __launch_bounds__(32 * kMaxWarps, 1)
   int* sFlag = reinterpret_cast<int*>(sraw + L.flag);
   const size_t fm = static_cast<size_t>(m) * S.nfamily + cd.z;
   stage_rows(bar, sA, S.eb + (fm * next + r_lo) * lda, static_cast<unsigned>(sizeof(double) * rows * lda));
-  const ElemIdx X = load_idx(g, sraw, L, el, cnt);
+  const ElemIdx X = load_idx(g, N, sraw, L, el, cnt);
   for (int w = threadIdx.x; w < g.np * g.np; w += blockDim.x) sD[w] = S.D[w];
   __syncthreads();
   pdl_wait();  // the operator rows are set-up data; F, G and R come from earlier kernels
@@ -333,8 +346,8 @@ __global__ void __launch_bounds__(32 * kMaxWarps, 1)
   cp_async_wait_all();
   __syncthreads();
   scale_forcing<false>(g, X, cnt, ncol, sB, ldb, sQ, 0);
-  __syncthreads();
-  if (G) {
+  // lift terms only where some column carries a nonzero essential value
+  if (__syncthreads_or(G && threadIdx.x < ncol && sFlag[threadIdx.x])) {
     lift_columns<false>(g, N, G, gstride, S.lambda2[m] + S.betak2[m], X, cnt, m, ncol, sB, ldb, sQ, sD, sFlag, 0);
     __syncthreads();
   }
@@ -357,7 +370,7 @@ __global__ void __launch_bounds__(32 * kMaxWarps, 1)
           int slot, l;
           col_slot(col, cnt, slot, l);
           const int b = r_lo + row;
-          atomicAdd(&R[static_cast<size_t>(2 * m + slot) * rstride + __ldg(N.btog + X.el[l] * next + b)],
+          atomicAdd(&R[static_cast<size_t>(2 * m + slot) * rstride + X.btog[l * next + b]],
                     sB[col * ldb + b] - acc[j][i]);
         }
       }
@@ -389,7 +402,7 @@ __global__ void __launch_bounds__(32 * kMaxWarps, 1)
   const int nwords = (next + 31) / 32;
   const size_t fm = static_cast<size_t>(m) * S.nfamily + cd.z;
   stage_rows(bar, sA, S.ew + (fm * nint + r_lo) * lda, static_cast<unsigned>(sizeof(double) * rows * lda));
-  const ElemIdx X = load_idx(g, sraw, L, el, cnt);
+  const ElemIdx X = load_idx(g, N, sraw, L, el, cnt);
   for (int w = threadIdx.x; w < g.np * g.np; w += blockDim.x) sD[w] = S.D[w];
   __syncthreads();
   pdl_wait();  // F, G, R (and U's other writers) belong to earlier kernels
@@ -403,8 +416,8 @@ __global__ void __launch_bounds__(32 * kMaxWarps, 1)
   cp_async_wait_all();
   __syncthreads();
   scale_forcing<true>(g, X, cnt, ncol, sB, ldb, sQ, next);
-  __syncthreads();
-  if (G) {
+  // lift terms only where some column carries a nonzero essential value
+  if (__syncthreads_or(G && threadIdx.x < ncol && sFlag[threadIdx.x])) {
     lift_columns<true>(g, N, G, gstride, S.lambda2[m] + S.betak2[m], X, cnt, m, ncol, sB, ldb, sQ, sD, sFlag, next);
     __syncthreads();
   }
