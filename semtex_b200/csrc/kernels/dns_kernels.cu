@@ -16,6 +16,8 @@
 // element per block: D is staged once per block, each warp holds its plane's
 // element data in its own shared memory (lanes over nodes, a few nodes per
 // lane loaded together) and synchronises only with itself.
+#include <type_traits>
+
 #include "dns_kernels.cuh"
 #include "elemderiv.cuh"
 #include "launch.hpp"
@@ -65,6 +67,23 @@ __device__ __forceinline__ void ep_load(const double* __restrict__ src, double* 
   }
 }
 
+// The nodes of an ElemMma result fragment held by this lane: f(node, m, n, c)
+// for every node (8 m + g, 8 n + 2 t + c) inside the np x np element.
+template <int MT, class F>
+__device__ __forceinline__ void for_frag_nodes(int np, F&& f) {
+  const int ln = threadIdx.x & 31, g8 = ln >> 2, t4 = ln & 3;
+#pragma unroll
+  for (int m = 0; m < MT; ++m)
+#pragma unroll
+    for (int n = 0; n < MT; ++n)
+#pragma unroll
+      for (int c = 0; c < 2; ++c) {
+        const int i = 8 * m + g8, j = 8 * n + 2 * t4 + c;
+        if (i < np && j < np) f(i * np + j, m, n, c);
+      }
+}
+
+template <int MT, int KS>
 __global__ void k_grad_xy(DevGeom g, const double* __restrict__ in, double* __restrict__ out, int dir) {
   pdl_trigger();
   pdl_wait();
@@ -72,11 +91,20 @@ __global__ void k_grad_xy(DevGeom g, const double* __restrict__ in, double* __re
   double* su;
   const int k = ep_setup(g, sm, 1, su);
   if (k < 0) return;
-  const int e = blockIdx.x, ln = threadIdx.x & 31;
+  const int e = blockIdx.x, np = g.np;
   const size_t base = static_cast<size_t>(k) * g.plane_size + static_cast<size_t>(e) * g.npnp;
   ep_load(in + base, su, g.npnp);
   __syncwarp();
-  for (int t = ln; t < g.npnp; t += 32) out[base + t] = elem_deriv(g, su, sm, e, t, dir);
+  ElemMma<MT, KS> M;
+  M.load_d(sm, np);
+  double ur[MT][MT][2], us[MT][MT][2];
+  M.grad(su, np, ur, us);
+  const double* fr = dir == 0 ? g.drdx : g.drdy;
+  const double* fs = dir == 0 ? g.dsdx : g.dsdy;
+  for_frag_nodes<MT>(np, [&](int t, int m, int n, int c) {
+    const int q = e * g.npnp + t;
+    out[base + t] = ur[m][n][c] * fr[q] + us[m][n][c] * fs[q];
+  });
 }
 
 // One block per (high-order edge h, Fourier mode m): planes 0 (m = 0) or
@@ -242,8 +270,11 @@ __global__ void k_product(const double* __restrict__ a, const double* __restrict
 
 // N = sc * [ conv: -(U0 dUi/dx + U1 dUi/dy + U2 Tc)
 //            cons: -(d(Ui U0)/dx + d(Ui U1)/dy + Tk) ] , form 0 skew (sc=1/2,
-// both), 1 convective, 2 conservative.  Tc / Tk / U2 may be null (2D).
-__global__ void __launch_bounds__(32 * kEpPlanes, 3) k_nonlinear(DevGeom g, NonlinearArgs a) {
+// both), 1 convective, 2 conservative.  Tc / Tk / U2 may be null (2D).  The
+// element derivatives run on the FP64 tensor cores (ElemMma), the products
+// Ui U0, Ui U1 staged in shared memory first.
+template <int MT, int KS>
+__global__ void __launch_bounds__(32 * kEpPlanes, 2) k_nonlinear(DevGeom g, NonlinearArgs a) {
   pdl_trigger();
   pdl_wait();
   extern __shared__ double sm[];
@@ -267,33 +298,41 @@ __global__ void __launch_bounds__(32 * kEpPlanes, 3) k_nonlinear(DevGeom g, Nonl
   }
   __syncwarp();
   const bool conv_on = a.form != 2, cons_on = a.form != 1;
-  for (int t = ln; t < npnp; t += 32) {
-    const int i = t / np, j = t - i * np;
-    // reference (r, s) derivatives of Ui, Ui U0, Ui U1 in one pass
-    double ur = 0.0, us = 0.0, p0r = 0.0, p0s = 0.0, p1r = 0.0, p1s = 0.0;
-    for (int kk = 0; kk < np; ++kk) {
-      const double dj = sm[j * np + kk], di = sm[i * np + kk];
-      const int row = i * np + kk, col = kk * np + j;
-      ur = fma(sUi[row], dj, ur);
-      us = fma(di, sUi[col], us);
-      p0r = fma(sP0[row], dj, p0r);
-      p0s = fma(di, sP0[col], p0s);
-      p1r = fma(sP1[row], dj, p1r);
-      p1s = fma(di, sP1[col], p1s);
-    }
-    const int q = e * npnp + t;
-    const double rx = g.drdx[q], ry = g.drdy[q], sx = g.dsdx[q], sy = g.dsdy[q];
-    double conv = 0.0, cons = 0.0;
-    if (conv_on) {
-      conv = -(sU0[t] * (ur * rx + us * sx) + sU1[t] * (ur * ry + us * sy));
-      if (a.U2 && a.Tc) conv -= a.U2[base + t] * a.Tc[base + t];
-    }
-    if (cons_on) {
-      cons = -((p0r * rx + p0s * sx) + (p1r * ry + p1s * sy));
-      if (a.Tk) cons -= a.Tk[base + t];
-    }
-    a.N[base + t] = a.form == 0 ? 0.5 * (conv + cons) : (a.form == 1 ? conv : cons);
+  const double wconv = a.form == 0 ? 0.5 : 1.0, wcons = a.form == 0 ? 0.5 : 1.0;
+  ElemMma<MT, KS> M;
+  M.load_d(sm, np);
+  double acc[MT][MT][2];
+#pragma unroll
+  for (int m = 0; m < MT; ++m)
+#pragma unroll
+    for (int n = 0; n < MT; ++n) acc[m][n][0] = acc[m][n][1] = 0.0;
+  double ur[MT][MT][2], us[MT][MT][2];
+  if (conv_on) {  // -(U0 dUi/dx + U1 dUi/dy + U2 Tc)
+    M.grad(sUi, np, ur, us);
+    for_frag_nodes<MT>(np, [&](int t, int m, int n, int c) {
+      const int q = e * npnp + t;
+      const double dx = ur[m][n][c] * g.drdx[q] + us[m][n][c] * g.dsdx[q];
+      const double dy = ur[m][n][c] * g.drdy[q] + us[m][n][c] * g.dsdy[q];
+      double v = -(sU0[t] * dx + sU1[t] * dy);
+      if (a.U2 && a.Tc) v -= a.U2[base + t] * a.Tc[base + t];
+      acc[m][n][c] += wconv * v;
+    });
   }
+  if (cons_on) {  // -(d(Ui U0)/dx + d(Ui U1)/dy + Tk)
+    M.grad(sP0, np, ur, us);
+    for_frag_nodes<MT>(np, [&](int t, int m, int n, int c) {
+      const int q = e * npnp + t;
+      acc[m][n][c] -= wcons * (ur[m][n][c] * g.drdx[q] + us[m][n][c] * g.dsdx[q]);
+    });
+    M.grad(sP1, np, ur, us);
+    for_frag_nodes<MT>(np, [&](int t, int m, int n, int c) {
+      const int q = e * npnp + t;
+      double v = ur[m][n][c] * g.drdy[q] + us[m][n][c] * g.dsdy[q];
+      if (a.Tk) v += a.Tk[base + t];
+      acc[m][n][c] -= wcons * v;
+    });
+  }
+  for_frag_nodes<MT>(np, [&](int t, int m, int n, int c) { a.N[base + t] = acc[m][n][c]; });
 }
 
 __global__ void k_dss_accum(DevGeom g, DevNumbering N, const double* __restrict__ in, double* __restrict__ ds,
@@ -333,7 +372,9 @@ __global__ void k_combine(CombineArgs a, size_t n) {
   }
 }
 
-// out = (du0/dx + du1/dy + [dz u2]) / dt  (setPForce)
+// out = (du0/dx + du1/dy + [dz u2]) / dt  (setPForce), element derivatives
+// on the FP64 tensor cores
+template <int MT, int KS>
 __global__ void k_divergence(DevGeom g, const double* __restrict__ a0, const double* __restrict__ a1,
                              const double* __restrict__ a2, double* __restrict__ out, double inv_dt,
                              double beta) {
@@ -343,21 +384,33 @@ __global__ void k_divergence(DevGeom g, const double* __restrict__ a0, const dou
   double* ws;
   const int k = ep_setup(g, sm, 2, ws);
   if (k < 0) return;
-  const int e = blockIdx.x, ln = threadIdx.x & 31;
+  const int e = blockIdx.x, np = g.np;
   double* s0 = ws;
   double* s1 = ws + g.npnp;
   const size_t base = static_cast<size_t>(k) * g.plane_size + static_cast<size_t>(e) * g.npnp;
   ep_load(a0 + base, s0, g.npnp);
   ep_load(a1 + base, s1, g.npnp);
   __syncwarp();
-  for (int t = ln; t < g.npnp; t += 32) {
-    double v = elem_deriv(g, s0, sm, e, t, 0) + elem_deriv(g, s1, sm, e, t, 1);
+  ElemMma<MT, KS> M;
+  M.load_d(sm, np);
+  double acc[MT][MT][2], ur[MT][MT][2], us[MT][MT][2];
+  M.grad(s0, np, ur, us);
+  for_frag_nodes<MT>(np, [&](int t, int m, int n, int c) {
+    const int q = e * g.npnp + t;
+    acc[m][n][c] = ur[m][n][c] * g.drdx[q] + us[m][n][c] * g.dsdx[q];
+  });
+  M.grad(s1, np, ur, us);
+  for_frag_nodes<MT>(np, [&](int t, int m, int n, int c) {
+    const int q = e * g.npnp + t;
+    double v = acc[m][n][c] + ur[m][n][c] * g.drdy[q] + us[m][n][c] * g.dsdy[q];
     if (a2) v += zderiv(a2, k, base + t - static_cast<size_t>(k) * g.plane_size, g.plane_size, beta);
     out[base + t] = v * inv_dt;
-  }
+  });
 }
 
-// io = alpha * io + b * d p / dx_dir  (dir 0, 1 element; 2 Fourier z; -1 none)
+// io = alpha * io + b * d p / dx_dir  (dir 0, 1 element, on the FP64 tensor
+// cores; 2 Fourier z; -1 none)
+template <int MT, int KS>
 __global__ void k_project(DevGeom g, double* __restrict__ io, const double* __restrict__ p, int dir,
                           double alpha, double b, double beta) {
   pdl_trigger();
@@ -366,18 +419,44 @@ __global__ void k_project(DevGeom g, double* __restrict__ io, const double* __re
   double* sp;
   const int k = ep_setup(g, sm, 1, sp);
   if (k < 0) return;
-  const int e = blockIdx.x, ln = threadIdx.x & 31;
+  const int e = blockIdx.x, ln = threadIdx.x & 31, np = g.np;
   const size_t base = static_cast<size_t>(k) * g.plane_size + static_cast<size_t>(e) * g.npnp;
   if (dir == 0 || dir == 1) {
     ep_load(p + base, sp, g.npnp);
     __syncwarp();
+    ElemMma<MT, KS> M;
+    M.load_d(sm, np);
+    double ur[MT][MT][2], us[MT][MT][2];
+    M.grad(sp, np, ur, us);
+    const double* fr = dir == 0 ? g.drdx : g.drdy;
+    const double* fs = dir == 0 ? g.dsdx : g.dsdy;
+    for_frag_nodes<MT>(np, [&](int t, int m, int n, int c) {
+      const int q = e * g.npnp + t;
+      io[base + t] = alpha * io[base + t] + b * (ur[m][n][c] * fr[q] + us[m][n][c] * fs[q]);
+    });
+    return;
   }
   for (int t = ln; t < g.npnp; t += 32) {
     double v = alpha * io[base + t];
-    if (dir == 0 || dir == 1) v += b * elem_deriv(g, sp, sm, e, t, dir);
     if (dir == 2) v += b * zderiv(p, k, base + t - static_cast<size_t>(k) * g.plane_size, g.plane_size, beta);
     io[base + t] = v;
   }
+}
+
+// Call f(MT, KS) (std::integral_constant arguments) for the ElemMma instance
+// that covers np (np <= 16).
+template <class F>
+cudaError_t mma_dispatch(int np, F&& f) {
+  using I1 = std::integral_constant<int, 1>;
+  using I2 = std::integral_constant<int, 2>;
+  using I3 = std::integral_constant<int, 3>;
+  using I4 = std::integral_constant<int, 4>;
+  const int mt = mma_tiles(np), ks = mma_ksteps(np);
+  if (mt == 1 && ks == 1) return f(I1{}, I1{});
+  if (mt == 1 && ks == 2) return f(I1{}, I2{});
+  if (mt == 2 && ks == 3) return f(I2{}, I3{});
+  if (mt == 2 && ks == 4) return f(I2{}, I4{});
+  return cudaErrorInvalidValue;
 }
 
 inline dim3 ep_grid(const DevGeom& g) { return dim3(g.nel, (g.nz + kEpPlanes - 1) / kEpPlanes); }
@@ -397,9 +476,12 @@ inline unsigned stream_blocks(size_t n) {
 
 cudaError_t dns_grad_xy(const DevGeom& g, const double* in, double* out, int dir, cudaStream_t st) {
   if (!ep_fits(g)) return cudaErrorInvalidValue;
-  raise_smem_limit(reinterpret_cast<const void*>(k_grad_xy), ep_smem(g, 1));
-  launch_ex(g.pdl != 0, k_grad_xy, ep_grid(g), dim3(kEpThreads), ep_smem(g, 1), st, g, in, out, dir);
-  return cudaGetLastError();
+  return mma_dispatch(g.np, [&](auto mt_, auto ks_) {
+    constexpr int MT = decltype(mt_)::value, KS = decltype(ks_)::value;
+    raise_smem_limit(reinterpret_cast<const void*>(k_grad_xy<MT, KS>), ep_smem(g, 1));
+    launch_ex(g.pdl != 0, k_grad_xy<MT, KS>, ep_grid(g), dim3(kEpThreads), ep_smem(g, 1), st, g, in, out, dir);
+    return cudaGetLastError();
+  });
 }
 
 cudaError_t dns_grad_z(const DevGeom& g, const double* in, double* out, double beta, cudaStream_t st) {
@@ -416,9 +498,12 @@ cudaError_t dns_product(const DevGeom& g, const double* a, const double* b, doub
 
 cudaError_t dns_nonlinear(const DevGeom& g, const NonlinearArgs& a, cudaStream_t st) {
   if (!ep_fits(g)) return cudaErrorInvalidValue;
-  raise_smem_limit(reinterpret_cast<const void*>(k_nonlinear), ep_smem(g, 5));
-  launch_ex(g.pdl != 0, k_nonlinear, ep_grid(g), dim3(kEpThreads), ep_smem(g, 5), st, g, a);
-  return cudaGetLastError();
+  return mma_dispatch(g.np, [&](auto mt_, auto ks_) {
+    constexpr int MT = decltype(mt_)::value, KS = decltype(ks_)::value;
+    raise_smem_limit(reinterpret_cast<const void*>(k_nonlinear<MT, KS>), ep_smem(g, 5));
+    launch_ex(g.pdl != 0, k_nonlinear<MT, KS>, ep_grid(g), dim3(kEpThreads), ep_smem(g, 5), st, g, a);
+    return cudaGetLastError();
+  });
 }
 
 cudaError_t dns_smooth(const DevGeom& g, const DevNumbering& N, double* io, double* work, cudaStream_t st) {
@@ -465,17 +550,25 @@ cudaError_t dns_combine(const DevGeom& g, const CombineArgs& a, cudaStream_t st)
 cudaError_t dns_divergence(const DevGeom& g, const double* a0, const double* a1, const double* a2, double* out,
                            double dt, double beta, cudaStream_t st) {
   if (!ep_fits(g)) return cudaErrorInvalidValue;
-  raise_smem_limit(reinterpret_cast<const void*>(k_divergence), ep_smem(g, 2));
-  launch_ex(g.pdl != 0, k_divergence, ep_grid(g), dim3(kEpThreads), ep_smem(g, 2), st, g, a0, a1, a2, out, 1.0 / dt, beta);
-  return cudaGetLastError();
+  return mma_dispatch(g.np, [&](auto mt_, auto ks_) {
+    constexpr int MT = decltype(mt_)::value, KS = decltype(ks_)::value;
+    raise_smem_limit(reinterpret_cast<const void*>(k_divergence<MT, KS>), ep_smem(g, 2));
+    launch_ex(g.pdl != 0, k_divergence<MT, KS>, ep_grid(g), dim3(kEpThreads), ep_smem(g, 2), st, g, a0, a1, a2, out,
+              1.0 / dt, beta);
+    return cudaGetLastError();
+  });
 }
 
 cudaError_t dns_project(const DevGeom& g, double* io, const double* p, int dir, double alpha, double b,
                         double beta, cudaStream_t st) {
   if (!ep_fits(g)) return cudaErrorInvalidValue;
-  raise_smem_limit(reinterpret_cast<const void*>(k_project), ep_smem(g, 1));
-  launch_ex(g.pdl != 0, k_project, ep_grid(g), dim3(kEpThreads), ep_smem(g, 1), st, g, io, p, dir, alpha, b, beta);
-  return cudaGetLastError();
+  return mma_dispatch(g.np, [&](auto mt_, auto ks_) {
+    constexpr int MT = decltype(mt_)::value, KS = decltype(ks_)::value;
+    raise_smem_limit(reinterpret_cast<const void*>(k_project<MT, KS>), ep_smem(g, 1));
+    launch_ex(g.pdl != 0, k_project<MT, KS>, ep_grid(g), dim3(kEpThreads), ep_smem(g, 1), st, g, io, p, dir, alpha,
+              b, beta);
+    return cudaGetLastError();
+  });
 }
 
 }  // namespace stx
