@@ -101,6 +101,16 @@ int stx_mesh_coords(const stx_context* ctx, double* h_x, double* h_y);
 /* Element mass weights (quadrature weight x Jacobian, Element::_Q4), host
  * buffer of nel*np*np. */
 int stx_mesh_mass(const stx_context* ctx, double* h_q4);
+/* Locate points in the mesh (HistoryPoint::locate, src/history.cpp:45-63,
+ * over Element::locate, src/element.cpp:1061-1183, tokens TOL_POS and
+ * NR_MAX): for each (xy[2i], xy[2i+1]) the first element whose Newton
+ * iteration from its nearest node converges inside the element, in
+ * h_elmt[i] (-1 when no element holds the point) with its canonical
+ * coordinates (r, s) in h_rs[2i], h_rs[2i+1].  Host work, set-up. */
+int stx_mesh_locate(const stx_context* ctx, int npts, const double* xy, int* h_elmt, double* h_rs);
+/* The same from a session file, without a context or device. */
+int stx_mesh_locate_host(const char* session_path, const char* overrides, int npts, const double* xy, int* h_elmt,
+                         double* h_rs);
 /* Number of geometry families (elements sharing condensed matrices). */
 int stx_mesh_families(const stx_context* ctx, int* nfamily);
 
@@ -300,6 +310,20 @@ int stx_dns_state(const stx_dns* dns, int* step, double* time);
 int stx_dns_modal_energy(stx_dns* dns, double* h_ek);
 int stx_dns_divergence_energy(stx_dns* dns, double* value);
 int stx_dns_cfl(stx_dns* dns, double* inv_dt);
+/* History-point values (HistoryPoint::extract, src/history.cpp:66-78, over
+ * AuxField::probe, src/auxfield.cpp:1621-1700), computed on the device from
+ * the current (Fourier) fields: for points on elements h_elmt at (r, s) =
+ * (h_rs[2i], h_rs[2i+1]) (from stx_mesh_locate) and z = h_z[i] (ignored with
+ * fewer than 3 planes; null for z = 0), h_out[i * nfields + f] is the
+ * physical-space value of field f, in FIELDS order. */
+int stx_dns_probe(stx_dns* dns, int npts, const int* h_elmt, const double* h_rs, const double* h_z, double* h_out);
+/* Forces on the edges of the boundary group named "wall" (DNSAnalyser::
+ * analyse, dns/dnsanalysis.cpp:97-113: Field::normTraction and
+ * tangTraction, src/field.cpp:392-458), from the mean (plane 0) fields on
+ * the device: pressure[3] the pressure force, viscous[3] the viscous force
+ * (-RHO KINVIS times the traction sums; z from the wall flux of w in 3D).
+ * Zero without wall edges. */
+int stx_dns_wall_forces(stx_dns* dns, double* pressure, double* viscous);
 /* Full-state checkpoint of the time stepping: the fields, the multi-level
  * velocity and nonlinear storage Us/Uf of every order (dns/integrate.cpp:
  * 99-136), the high-order pressure BC levels (BCmgr's _un / _hopbc,

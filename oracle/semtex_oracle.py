@@ -22,6 +22,10 @@ CUDA library accelerates:
   src/field.cpp:1127-1227, src/bcmgr.cpp:153-180, src/edge.cpp:98-256)
 * computed outflow BCs                         (src/bcmgr.cpp:998-1633;
   parity unpinned: the reference has no golden for them)
+* history points and wall forces               (src/history.cpp:45-78,
+  src/element.cpp:1061-1203, src/auxfield.cpp:1621-1700,
+  src/field.cpp:392-458, src/edge.cpp:259-378; parity unpinned: no
+  reference golden holds them)
 
 The banded factorisation and solve call LAPACK dpbtrf/dpbtrs through scipy,
 the same routines the reference calls (src/matrix.cpp:252, src/field.cpp:693).
@@ -778,6 +782,56 @@ def helmholtz_op(M: Mesh, u, lambda2, betak2):
     R2 = M.Q1 * R + M.Q3 * S
     S2 = M.Q2 * S + M.Q3 * R
     return M.Q4 * u * _hcon(M, None, lambda2, betak2) + D.T @ S2 + R2 @ D
+
+
+def lagrange_interpolants(z, x):
+    """Lagrange interpolants h_j(x) of the points z and their derivatives
+    (intmat_g / dermat_g as intp uses them, femlib/operators.c:250-300)."""
+    n = len(z)
+    h, dh = np.ones(n), np.zeros(n)
+    for j in range(n):
+        others = [m for m in range(n) if m != j]
+        f = np.array([(x - z[m]) / (z[j] - z[m]) for m in others])
+        h[j] = np.prod(f)
+        dh[j] = sum(np.prod(np.delete(f, i)) / (z[j] - z[m]) for i, m in enumerate(others))
+    return h, dh
+
+
+def locate(M: Mesh, x: float, y: float, tol: float = 1e-5, maxit: int = 20):
+    """HistoryPoint::locate (src/history.cpp:45-63) over Element::locate
+    (src/element.cpp:1061-1183): (element, r, s) of the first element where
+    Newton's iteration from the nearest node converges inside, else None."""
+    n = M.np
+    for e in range(M.nel):
+        X, Y = M.x[e].ravel(), M.y[e].ravel()
+        diag = max(math.hypot(X[-1] - X[0], Y[-1] - Y[0]),
+                   math.hypot(X[n * (n - 1)] - X[n - 1], Y[n * (n - 1)] - Y[n - 1]))
+        d2 = (x - X) ** 2 + (y - Y) ** 2
+        i = int(np.argmin(d2))
+        if d2[i] - diag * diag > 0.0:
+            continue
+        r, s = M.z[i % n], M.z[i // n]
+        Xm, Ym = M.x[e], M.y[e]
+        it, ok = 0, True
+        while True:
+            ir, dr = lagrange_interpolants(M.z, r)
+            is_, ds = lagrange_interpolants(M.z, s)
+            F0 = x - is_ @ Xm @ ir
+            F1 = y - is_ @ Ym @ ir
+            J = [dr @ Xm.T @ is_, dr @ Ym.T @ is_, ds @ Xm @ ir, ds @ Ym @ ir]
+            det = J[0] * J[3] - J[1] * J[2]
+            idet = 1.0 / EPSDP if abs(det) < EPSDP else 1.0 / det
+            r += (F0 * J[3] - F1 * J[2]) * idet
+            s += (F1 * J[0] - F0 * J[1]) * idet
+            if abs(r) > 20.0 and abs(s) > 20.0:
+                ok = False
+                break
+            it += 1
+            if not (it < maxit and (abs(F0) > tol or abs(F1) > tol)):
+                break
+        if ok and it < maxit and abs(r) < 1.0 + tol and abs(s) < 1.0 + tol:
+            return e, r, s
+    return None
 
 
 def grad(M: Mesh, u, direction):
@@ -2040,6 +2094,75 @@ class DNS:
         if self.ncom == 3:
             out = max(out, np.abs(self.u[self.vel[2]][0]).max() / (2 * math.pi / P.S.tokens["BETA"] / P.nz))
         return out
+
+    def probe(self, points):
+        """History-point values (HistoryPoint::extract, src/history.cpp:66-78;
+        AuxField::probe, src/auxfield.cpp:1621-1700): [n, nfields] in FIELDS
+        order at physical (x, y, z), the Fourier series of the held half
+        spectrum summed at z (non-zero modes doubled)."""
+        P, M = self.P, self.P.M
+        tok = P.S.tokens
+        out = np.zeros((len(points), len(P.S.fields)))
+        for i, (x, y, z) in enumerate(points):
+            loc = locate(M, x, y, tok["TOL_POS"], tok.ivalue("NR_MAX"))
+            if loc is None:
+                raise ValueError("history point not in mesh")
+            e, r, s = loc
+            ir, _ = lagrange_interpolants(M.z, r)
+            is_, _ = lagrange_interpolants(M.z, s)
+            for f, c in enumerate(P.S.fields):
+                vals = np.array([is_ @ self.u[c][k, e] @ ir for k in range(P.nz)])
+                if P.nz < 3:
+                    out[i, f] = vals[0]
+                    continue
+                bz = z * tok["BETA"]
+                nzh = P.nz // 2
+                v = vals[0] + vals[1] * math.cos(nzh * bz)
+                for k in range(1, nzh):
+                    v += 2.0 * vals[2 * k] * math.cos(k * bz) - 2.0 * vals[2 * k + 1] * math.sin(k * bz)
+                out[i, f] = v
+        return out
+
+    def wall_forces(self):
+        """DNSAnalyser::analyse's forces (dns/dnsanalysis.cpp:97-113):
+        Field::normTraction / tangTraction (src/field.cpp:392-458) over the
+        edges of the group named "wall" (Edge::normTraction / tangTraction /
+        scalarFlux, src/edge.cpp:259-378), on the mean (plane 0) data.
+        Returns (pressure[3], viscous[3])."""
+        P, M = self.P, self.P.M
+        S, tok = P.S, P.S.tokens
+        names = S.fields
+        B = P.B[names[0]]
+        mu = tok["RHO"] * tok["KINVIS"]
+        pf, vf = np.zeros(3), np.zeros(3)
+        pres = self.u[names[self.ndim]][0]          # field DIM: p, or w for 2D "uvwp"
+        u, v = self.u[names[0]][0], self.u[names[1]][0]
+        w = self.u[names[2]][0] if self.ndim == 3 else None
+        grads = {id(a): (grad(M, a, 0), grad(M, a, 1)) for a in [u, v] + ([w] if w is not None else [])}
+        for b, (e, s, _, _) in enumerate(B.edges):
+            if S.groups.get(M.group[(e, s)], "") != "wall":
+                continue
+            idx = M.side_nodes(s)
+            sgn, (a, c) = {0: (-1, ("dsdx", "dsdy")), 1: (1, ("drdx", "drdy")),
+                           2: (1, ("dsdx", "dsdy")), 3: (-1, ("drdx", "drdy"))}[s]
+            nx = sgn * getattr(M, a)[e].ravel()[idx]
+            ny = sgn * getattr(M, c)[e].ravel()[idx]
+            ln = np.hypot(nx, ny)
+            nx, ny = nx / ln, ny / ln
+            area = B.area[b]
+            pv = pres[e].ravel()[idx]
+            pf[0] += np.sum(nx * pv * area)
+            pf[1] += np.sum(ny * pv * area)
+            ux, uy = (t[e].ravel()[idx] for t in grads[id(u)])
+            vx, vy = (t[e].ravel()[idx] for t in grads[id(v)])
+            sx = np.sum((2.0 * ux * nx + uy * ny) * area) + np.sum(vx * ny * area)
+            sy = np.sum(uy * nx * area) + np.sum((2.0 * vy * ny + vx * nx) * area)
+            vf[0] -= mu * sx
+            vf[1] -= mu * sy
+            if w is not None:
+                wx, wy = (t[e].ravel()[idx] for t in grads[id(w)])
+                vf[2] -= mu * np.sum((wx * nx + wy * ny) * area)
+        return pf, vf
 
     def physical(self):
         out = {}

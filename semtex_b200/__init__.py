@@ -105,6 +105,16 @@ class Context:
         s = (self.nel, self.np, self.np)
         return x.reshape(s), y.reshape(s)
 
+    def locate(self, xy) -> tuple[np.ndarray, np.ndarray]:
+        """Elements (-1 outside the mesh) and canonical (r, s) of points
+        [n, 2] (HistoryPoint::locate / Element::locate)."""
+        pts = np.ascontiguousarray(np.asarray(xy, dtype=np.float64).reshape(-1, 2))
+        n = pts.shape[0]
+        el = np.empty(n, dtype=np.int32)
+        rs = np.empty((n, 2))
+        check(lib().stx_mesh_locate(self._h, n, pts.ctypes.data, el.ctypes.data, rs.ctypes.data))
+        return el, rs
+
     def evaluate(self, expr: str, t: float = 0.0) -> np.ndarray:
         """AuxField = "function" in physical space, [nz, nel, np, np]."""
         out = np.empty((self.nz, self.nel, self.np, self.np))
@@ -513,6 +523,27 @@ class DNS:
         v = C.c_double()
         check(lib().stx_dns_cfl(self._h, C.byref(v)))
         return v.value
+
+    def probe(self, points) -> np.ndarray:
+        """Field values at history points [n, 3] (x, y, z), [n, nfields] in
+        FIELDS order (HistoryPoint::extract); points outside the mesh are
+        rejected."""
+        pts = np.asarray(points, dtype=np.float64).reshape(-1, 3)
+        el, rs = self.ctx.locate(pts[:, :2])
+        if (el < 0).any():
+            raise ValueError(f"history point {pts[int(np.argmin(el))]} not in mesh")
+        z = np.ascontiguousarray(pts[:, 2])
+        out = np.empty((pts.shape[0], len(self.ctx.fields)))
+        check(lib().stx_dns_probe(self._h, pts.shape[0], el.ctypes.data, rs.ctypes.data, z.ctypes.data,
+                                  out.ctypes.data))
+        return out
+
+    def wall_forces(self) -> tuple[np.ndarray, np.ndarray]:
+        """(pressure, viscous) forces [3] on the "wall" group
+        (Field::normTraction / tangTraction)."""
+        p, v = np.zeros(3), np.zeros(3)
+        check(lib().stx_dns_wall_forces(self._h, p.ctypes.data, v.ctypes.data))
+        return p, v
 
 
 class DNSAdjoint:

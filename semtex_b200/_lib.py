@@ -39,6 +39,8 @@ SIGNATURES = {
     "stx_mesh_coords": (_i, [_p, _p, _p]),
     "stx_mesh_families": (_i, [_p, _pi]),
     "stx_mesh_mass": (_i, [_p, _p]),
+    "stx_mesh_locate": (_i, [_p, _i, _p, _p, _p]),
+    "stx_mesh_locate_host": (_i, [_s, _s, _i, _p, _p, _p]),
     "stx_field_evaluate": (_i, [_p, _s, _d, _p]),
     "stx_expression_eval": (_i, [_s, _s, _i, _i, _p, _p, _p, _d, _p, _pi]),
     "stx_svv": (_i, [_i, _d, _i, _i, _d, _i, _d, _p, _p]),
@@ -71,6 +73,8 @@ SIGNATURES = {
     "stx_dns_modal_energy": (_i, [_p, _p]),
     "stx_dns_divergence_energy": (_i, [_p, _pd]),
     "stx_dns_cfl": (_i, [_p, _pd]),
+    "stx_dns_probe": (_i, [_p, _i, _p, _p, _p, _p]),
+    "stx_dns_wall_forces": (_i, [_p, _p, _p]),
     "stx_dns_graph_info": (_i, [_p, _pi, C.POINTER(C.c_longlong)]),
     "stx_dns_status": (_i, [_p, _pi]),
     "stx_dns_stats_update": (_i, [_p]),

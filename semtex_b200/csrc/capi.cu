@@ -437,6 +437,38 @@ int stx_mesh_mass(const stx_context* ctx, double* h_q4) {
   });
 }
 
+namespace {
+
+void locate_points(const Session& S, const Mesh& M, int npts, const double* xy, int* h_elmt, double* h_rs) {
+  if (npts < 0 || (npts > 0 && (!xy || !h_elmt || !h_rs))) throw StxError(STX_EINVAL, "null argument");
+  const double tol = S.tokens.value("TOL_POS");
+  const int maxit = S.tokens.ivalue("NR_MAX");
+  for (int i = 0; i < npts; ++i) {
+    double r = 0.0, s = 0.0;
+    h_elmt[i] = locate_point(M, xy[2 * i], xy[2 * i + 1], tol, maxit, r, s);
+    h_rs[2 * i] = h_elmt[i] >= 0 ? r : 0.0;
+    h_rs[2 * i + 1] = h_elmt[i] >= 0 ? s : 0.0;
+  }
+}
+
+}  // namespace
+
+int stx_mesh_locate(const stx_context* ctx, int npts, const double* xy, int* h_elmt, double* h_rs) {
+  return guarded([&] {
+    if (!ctx) throw StxError(STX_EINVAL, "null context");
+    locate_points(ctx->S, ctx->M, npts, xy, h_elmt, h_rs);
+  });
+}
+
+int stx_mesh_locate_host(const char* session_path, const char* overrides, int npts, const double* xy, int* h_elmt,
+                         double* h_rs) {
+  return guarded([&] {
+    if (!session_path) throw StxError(STX_EINVAL, "null argument");
+    const Session S = read_session(session_path, overrides ? overrides : "");
+    locate_points(S, build_mesh(S), npts, xy, h_elmt, h_rs);
+  });
+}
+
 int stx_mesh_families(const stx_context* ctx, int* nfamily) {
   return guarded([&] {
     if (!ctx || !nfamily) throw StxError(STX_EINVAL, "null argument");

@@ -11,16 +11,23 @@
 // Every IO_CFL steps the CFL estimate and divergence energy are printed
 // (Analyser::estimateCFL / divergence, src/analysis.cpp:382-443); with
 // AVERAGE > 0 running averages are updated every IO_HIS steps and written
-// to session.avg with each dump (Statistics, src/statistics.cpp).
+// to session.avg with each dump (Statistics, src/statistics.cpp).  Every
+// IO_HIS and IO_FLD steps and at the end the HISTORY points go to
+// session.his (Analyser::analyse, src/analysis.cpp:275-304) and the forces
+// on the "wall" group to session.flx (DNSAnalyser, dns/dnsanalysis.cpp:
+// 44-127); every IO_MDL steps the modal energies go to session.mdl
+// (Analyser::modalEnergy, src/analysis.cpp:329-375).
 #include <cmath>
 #include <cstdio>
 #include <cstring>
 #include <fstream>
+#include <iomanip>
 #include <string>
 #include <vector>
 
 #include "../../../include/semtex_b200.h"
 #include "host/fieldfile.hpp"
+#include "host/session.hpp"
 
 namespace {
 
@@ -122,6 +129,50 @@ int main(int argc, char** argv) {
       check(stx_dns_stats_info(dns, nullptr, 0, nullptr, A.step), "statistics");
     }
   }
+  // -- Analyser::Analyser (src/analysis.cpp:106-184) and DNSAnalyser::
+  //    DNSAnalyser (dns/dnsanalysis.cpp:30-52): history points located in
+  //    the mesh (shifted and scaled as X_SHIFT, X_SCALE, ... ask), files
+  const int io_mdl = static_cast<int>(std::lround(token(ctx, "IO_MDL")));
+  std::vector<int> his_id, his_el;
+  std::vector<double> his_rs, his_z;
+  {
+    const stx::Session S = stx::read_session(session);
+    const double xs = token(ctx, "X_SHIFT"), ys = token(ctx, "Y_SHIFT");
+    const double xc = token(ctx, "X_SCALE"), yc = token(ctx, "Y_SCALE");
+    for (const auto& h : S.history) {
+      const double xy[2] = {(h.x + xs) * xc, (h.y + ys) * yc};
+      int el = -1;
+      double rs[2];
+      check(stx_mesh_locate(ctx, 1, xy, &el, rs), "history");
+      if (el < 0) {
+        std::fprintf(stderr, "Analyser::Analyser: History point at (%f, %f, %f) not in mesh\n", xy[0], xy[1], h.z);
+        continue;
+      }
+      his_id.push_back(h.id);
+      his_el.push_back(el);
+      his_rs.insert(his_rs.end(), rs, rs + 2);
+      his_z.push_back(h.z);
+    }
+  }
+  std::ofstream his, mdl;
+  if (!his_id.empty()) {
+    his.open(session + ".his");
+    if (!his) fail("can't open history file");
+    his.setf(std::ios::scientific, std::ios::floatfield);
+    his.precision(6);
+  }
+  if (io_mdl) {
+    mdl.open(session + ".mdl");
+    if (!mdl) fail("can't open modal energy file");
+    mdl << "#     Time Mode         Energy" << std::endl << "# ----------------------------" << std::endl;
+  }
+  std::ofstream flx(session + ".flx");
+  if (!flx) fail("can't open flux file");
+  flx << "# DNS state information file" << std::endl
+      << "# Step Time [Fpre Fvis Ftot]-axis" << std::endl
+      << "# -------------------------------" << std::endl;
+  std::vector<double> his_val(his_id.size() * fields.size());
+  std::vector<double> ek((nz + 1) / 2);
   const double dt = token(ctx, "D_T");
   const bool chkpoint = !no_chk && token(ctx, "CHKPOINT") != 0.0;
   stx::FieldFile out;
@@ -139,7 +190,8 @@ int main(int argc, char** argv) {
   while (step < nstep) {
     int next = std::min(nstep, (step / io_fld + 1) * io_fld);
     if (io_cfl > 0) next = std::min(next, (step / io_cfl + 1) * io_cfl);
-    if (averaging) next = std::min(next, (step / io_his + 1) * io_his);
+    next = std::min(next, (step / io_his + 1) * io_his);
+    if (io_mdl > 0) next = std::min(next, (step / io_mdl + 1) * io_mdl);
     if (verbose) {  // the step line of DNSAnalyser::analyse, one step at a time
       for (; step < next; ++step) {
         check(stx_dns_advance(dns, 1), "integrate");
@@ -162,7 +214,35 @@ int main(int argc, char** argv) {
                   static_cast<int>(100.0 * dt / dt_max));
       std::printf("------- Divergence Energy: %g\n", div);
     }
+    // -- history points and wall forces at IO_HIS / IO_FLD steps and at
+    //    the end (Analyser::analyse, DNSAnalyser::analyse)
+    if (step % io_his == 0 || step % io_fld == 0 || step == nstep) {
+      if (!his_id.empty()) {
+        const int nf = static_cast<int>(fields.size());
+        check(stx_dns_probe(dns, static_cast<int>(his_id.size()), his_el.data(), his_rs.data(), his_z.data(),
+                            his_val.data()),
+              "history");
+        for (size_t i = 0; i < his_id.size(); ++i) {
+          his << std::setw(4) << his_id[i] << std::setprecision(8) << std::setw(15) << time << std::setprecision(6);
+          for (int j = 0; j < nf - 1; ++j) his << std::setw(14) << his_val[i * nf + j];
+          his << std::setprecision(11) << std::setw(19) << his_val[i * nf + nf - 1] << std::setprecision(6)
+              << std::endl;
+        }
+      }
+      double pf[3], vf[3];
+      check(stx_dns_wall_forces(dns, pf, vf), "wall forces");
+      char line[256];
+      std::snprintf(line, sizeof(line),
+                    "%6d %#10.6g %#10.6g %#10.6g %#10.6g %#10.6g %#10.6g %#10.6g %#10.6g %#10.6g %#10.6g", step,
+                    time, pf[0], vf[0], pf[0] + vf[0], pf[1], vf[1], pf[1] + vf[1], pf[2], vf[2], pf[2] + vf[2]);
+      flx << line << std::endl;
+    }
     if (averaging && step % io_his == 0) check(stx_dns_stats_update(dns), "statistics");
+    if (io_mdl > 0 && step % io_mdl == 0) {  // Analyser::modalEnergy
+      check(stx_dns_modal_energy(dns, ek.data()), "modal energy");
+      for (size_t m = 0; m < ek.size(); ++m)
+        mdl << std::setw(10) << time << std::setw(5) << m << std::setw(15) << ek[m] << std::endl;
+    }
     const bool periodic = step % io_fld == 0, initial = step == io_fld, final = step == nstep;
     if (periodic || final) {
       for (size_t k = 0; k < fields.size(); ++k)

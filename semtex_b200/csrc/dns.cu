@@ -881,6 +881,39 @@ int stx_dns_create(stx_context* ctx, int advection, stx_dns** out) {
         }
       }
     }
+    // -- edges of the boundary group "wall" (the group string compared as
+    //    Edge::normTraction does, src/edge.cpp:259-289), for the forces
+    {
+      const FieldDev& U = ctx->fields.at(d->names[0]);
+      std::vector<int> el, nd;
+      std::vector<double> nx, ny, area;
+      std::vector<int> idx(g.np);
+      for (const BoundaryEdge& E : U.N.edges) {
+        const auto gi = S.groups.find(E.group);
+        if (gi == S.groups.end() || gi->second != "wall") continue;
+        el.push_back(E.elmt);
+        ctx->M.side_nodes(E.side, idx.data());
+        nd.insert(nd.end(), idx.begin(), idx.end());
+        nx.insert(nx.end(), E.nx.begin(), E.nx.end());
+        ny.insert(ny.end(), E.ny.begin(), E.ny.end());
+        area.insert(area.end(), E.area.begin(), E.area.end());
+      }
+      d->nwall = static_cast<int>(el.size());
+      if (d->nwall) {
+        auto up = [&](const auto& v) {
+          using T = typename std::decay_t<decltype(v)>::value_type;
+          T* p = static_cast<T*>(d->arena.alloc(sizeof(T) * v.size()));
+          ck(cudaMemcpy(p, v.data(), sizeof(T) * v.size(), cudaMemcpyHostToDevice), "upload");
+          return p;
+        };
+        d->w_elmt = up(el);
+        d->w_node = up(nd);
+        d->w_nx = up(nx);
+        d->w_ny = up(ny);
+        d->w_area = up(area);
+        d->w_out = static_cast<double*>(d->arena.alloc(sizeof(double) * 5 * d->nwall));
+      }
+    }
     // -- computed outflow edges and storage (BCmgr::buildComputedBCs,
     //    src/bcmgr.cpp:937-996): the pressure's 'O' edges, which u and v
     //    carry at the same positions of their BC lines
@@ -957,6 +990,7 @@ int stx_dns_destroy(stx_dns* d) {
     for (auto* m : d->vsys) stx_modal_destroy(m);
     if (d->psys) stx_modal_destroy(d->psys);
     for (auto& kv : d->pcg) stx_modal_destroy(kv.second);
+    if (d->probe_buf) cudaFree(d->probe_buf);
     delete d;
   });
 }
@@ -1135,6 +1169,103 @@ int stx_dns_cfl(stx_dns* d, double* inv_dt) {
       c = std::max(c, m);
     }
     *inv_dt = c;
+  });
+}
+
+int stx_dns_probe(stx_dns* d, int npts, const int* elmt, const double* rs, const double* z, double* out) {
+  return dns_guarded([&] {
+    if (!d || npts < 0 || (npts > 0 && (!elmt || !rs || !out))) throw DnsError(STX_EINVAL, "null argument");
+    if (npts == 0) return;
+    stx_context* ctx = d->ctx;
+    const Mesh& M = ctx->M;
+    cudaSetDevice(ctx->device);
+    const int np = M.np, nf = static_cast<int>(d->names.size());
+    // 2D (fewer than 3 planes): plane 0 alone (src/auxfield.cpp:1668-1669)
+    const int nzc = M.nz < 3 ? 1 : M.nz;
+    const int stride = 2 * np + nzc;
+    std::vector<double> w(static_cast<size_t>(npts) * stride);
+    for (int p = 0; p < npts; ++p) {
+      if (elmt[p] < 0 || elmt[p] >= M.nel) throw DnsError(STX_EINVAL, "history point element out of range");
+      double* wp = w.data() + static_cast<size_t>(p) * stride;
+      gll_interpolants(M.q, rs[2 * p + 1], wp, nullptr);
+      gll_interpolants(M.q, rs[2 * p], wp + np, nullptr);
+      double* c = wp + 2 * np;
+      c[0] = 1.0;
+      if (nzc > 1) {
+        // the Fourier series at z of the packed half spectrum, non-zero
+        // modes doubled (src/auxfield.cpp:1681-1695)
+        const double bz = (z ? z[p] : 0.0) * d->beta;
+        c[1] = std::cos((M.nz / 2) * bz);
+        for (int k = 1; k < M.nz / 2; ++k) {
+          c[2 * k] = 2.0 * std::cos(k * bz);
+          c[2 * k + 1] = -2.0 * std::sin(k * bz);
+        }
+      }
+    }
+    const size_t wbytes = sizeof(double) * w.size(), ebytes = (sizeof(int) * npts + 15) / 16 * 16;
+    const size_t obytes = sizeof(double) * static_cast<size_t>(npts) * nf;
+    const size_t need = wbytes + ebytes + obytes;
+    if (need > d->probe_bytes) {
+      ck(cudaStreamSynchronize(ctx->stream), "sync");
+      if (d->probe_buf) cudaFree(d->probe_buf);
+      d->probe_buf = nullptr;
+      d->probe_bytes = 0;
+      ck(cudaMalloc(&d->probe_buf, need), "history point scratch");
+      d->probe_bytes = need;
+    }
+    char* base = static_cast<char*>(d->probe_buf);
+    ProbeArgs a{};
+    a.npts = npts;
+    a.nf = nf;
+    a.nzc = nzc;
+    a.w = reinterpret_cast<double*>(base);
+    a.elmt = reinterpret_cast<int*>(base + wbytes);
+    a.out = reinterpret_cast<double*>(base + wbytes + ebytes);
+    for (int f = 0; f < nf; ++f) a.f[f] = d->u[f];
+    ck(cudaMemcpyAsync(base, w.data(), wbytes, cudaMemcpyHostToDevice, ctx->stream), "upload");
+    ck(cudaMemcpyAsync(base + wbytes, elmt, sizeof(int) * npts, cudaMemcpyHostToDevice, ctx->stream), "upload");
+    ck(dns_probe(ctx->dg, a, ctx->stream), "probe");
+    ck(cudaMemcpyAsync(out, a.out, obytes, cudaMemcpyDeviceToHost, ctx->stream), "download");
+    ck(cudaStreamSynchronize(ctx->stream), "sync");
+  });
+}
+
+int stx_dns_wall_forces(stx_dns* d, double* pressure, double* viscous) {
+  return dns_guarded([&] {
+    if (!d || !pressure || !viscous) throw DnsError(STX_EINVAL, "null argument");
+    stx_context* ctx = d->ctx;
+    cudaSetDevice(ctx->device);
+    for (int i = 0; i < 3; ++i) pressure[i] = viscous[i] = 0.0;
+    if (!d->nwall) return;
+    // DNSAnalyser::analyse (dns/dnsanalysis.cpp:97-113) takes field DIM as
+    // the pressure and field 2 as w in 3D only: with N_Z = 1 and fields
+    // "uvwp" the third field (w) stands in the pressure's place there too
+    WallArgs a{};
+    a.nw = d->nwall;
+    a.elmt = d->w_elmt;
+    a.node = d->w_node;
+    a.nx = d->w_nx;
+    a.ny = d->w_ny;
+    a.area = d->w_area;
+    a.p = d->u[d->ndim];
+    a.u = d->u[0];
+    a.v = d->u[1];
+    a.w = d->ndim == 3 ? d->u[2] : nullptr;
+    a.out = d->w_out;
+    std::vector<double> h(static_cast<size_t>(5) * d->nwall);
+    ck(dns_wall_forces(ctx->dg, a, ctx->stream), "wall forces");
+    ck(cudaMemcpyAsync(h.data(), d->w_out, sizeof(double) * h.size(), cudaMemcpyDeviceToHost, ctx->stream),
+       "download");
+    ck(cudaStreamSynchronize(ctx->stream), "sync");
+    const double mu = ctx->S.tokens.value("RHO") * d->nu;
+    for (int b = 0; b < d->nwall; ++b) {  // per edge, in order (Field::normTraction / tangTraction)
+      const double* e = h.data() + 5 * b;
+      pressure[0] += e[0];
+      pressure[1] += e[1];
+      viscous[0] -= mu * e[2];
+      viscous[1] -= mu * e[3];
+      if (d->ndim == 3) viscous[2] -= mu * e[4];
+    }
   });
 }
 

@@ -66,6 +66,21 @@ struct stx_dns {
   double* B32 = nullptr;                   // padded z-derivative term (convective)
   double* C32 = nullptr;                   // padded product / z-derivative term (conservative)
   double* part = nullptr;                  // analysis partials: blocks x max(modes, 3)
+  // Edges of the boundary group named "wall" (Field::normTraction /
+  // tangTraction, src/field.cpp:392-458): element, side nodes in the side
+  // traverse, unit outward normal and quadrature-weighted length per node,
+  // and the per-edge sums of stx_dns_wall_forces.
+  int nwall = 0;
+  const int* w_elmt = nullptr;
+  const int* w_node = nullptr;
+  const double* w_nx = nullptr;
+  const double* w_ny = nullptr;
+  const double* w_area = nullptr;
+  double* w_out = nullptr;
+  // History-point scratch (stx_dns_probe), grown on demand: per-point
+  // weights, elements and results.
+  void* probe_buf = nullptr;
+  size_t probe_bytes = 0;
   // Steady steps replayed as a CUDA graph (token STX_DNS_GRAPH, default 1):
   // the steps from one pointer state back to the same state (the multi-level
   // storage rolls by pointer, the alternating form toggles) captured once.

@@ -742,6 +742,7 @@ Numbering build_numbering(const Session& S, const Mesh& M, char field, int rcm_r
       E.elmt = e;
       E.side = s;
       E.kind = bc.kind;
+      E.group = g;
       E.expr = bc.expr;
       if (bc.kind == 'M') {  // "K;C" or "K,C" (Mixed::Mixed, src/condition.cpp:295-312)
         const size_t cut = bc.expr.find_first_of(";,");
@@ -858,6 +859,84 @@ Numbering build_numbering(const Session& S, const Mesh& M, char field, int rcm_r
     }
   for (auto& v : N.imass) v = 1.0 / v;
   return N;
+}
+
+void gll_interpolants(const Quadrature& q, double x, double* h, double* dh) {
+  const int n = q.np;
+  const double* z = q.z.data();
+  for (int j = 0; j < n; ++j) {
+    // h_j(x) = prod_{m != j} (x - z_m) / (z_j - z_m); its derivative the
+    // sum over l != j of the same product with factor l replaced by
+    // 1 / (z_j - z_l)
+    double v = 1.0, d = 0.0;
+    for (int m = 0; m < n; ++m) {
+      if (m == j) continue;
+      const double f = (x - z[m]) / (z[j] - z[m]);
+      d = d * f + v / (z[j] - z[m]);
+      v *= f;
+    }
+    if (h) h[j] = v;
+    if (dh) dh[j] = d;
+  }
+}
+
+int locate_point(const Mesh& M, double x, double y, double tol, int maxit, double& r, double& s) {
+  const int np = M.np, nn = M.npnp;
+  const double kDiverge = 20.0;
+  std::vector<double> ir(np), is(np), dr(np), ds(np), tp(np);
+  for (int e = 0; e < M.nel; ++e) {
+    const double* X = M.x.data() + static_cast<size_t>(e) * nn;
+    const double* Y = M.y.data() + static_cast<size_t>(e) * nn;
+    // initial guess: the element node nearest (x, y), if within the
+    // element's longer diagonal
+    const double diag = std::max(std::hypot(X[nn - 1] - X[0], Y[nn - 1] - Y[0]),
+                                 std::hypot(X[np * (np - 1)] - X[np - 1], Y[np * (np - 1)] - Y[np - 1]));
+    int best = 0;
+    double dmin = 0.0;
+    for (int t = 0; t < nn; ++t) {
+      const double dx = x - X[t], dy = y - Y[t];
+      const double d2 = dx * dx + dy * dy;
+      if (t == 0 || d2 < dmin) {
+        dmin = d2;
+        best = t;
+      }
+    }
+    if (dmin - diag * diag > 0.0) continue;
+    r = M.q.z[best % np];
+    s = M.q.z[best / np];
+    int it = 0;
+    double F0, F1;
+    bool diverged = false;
+    do {
+      gll_interpolants(M.q, r, ir.data(), dr.data());
+      gll_interpolants(M.q, s, is.data(), ds.data());
+      // x(r, s) = is^T X ir and its partials
+      auto form = [&](const double* A, const double* w, const double* v) {
+        for (int i = 0; i < np; ++i) {
+          double a = 0.0;
+          for (int j = 0; j < np; ++j) a += A[i * np + j] * w[j];
+          tp[i] = a;
+        }
+        double a = 0.0;
+        for (int i = 0; i < np; ++i) a += v[i] * tp[i];
+        return a;
+      };
+      F0 = x - form(X, ir.data(), is.data());
+      F1 = y - form(Y, ir.data(), is.data());
+      const double J2 = form(X, ir.data(), ds.data()), J3 = form(Y, ir.data(), ds.data());
+      const double J0 = form(X, dr.data(), is.data()), J1 = form(Y, dr.data(), is.data());
+      double idet = J0 * J3 - J1 * J2;
+      idet = std::fabs(idet) < kEpsDP ? 1.0 / kEpsDP : 1.0 / idet;
+      r += (F0 * J3 - F1 * J2) * idet;
+      s += (F1 * J0 - F0 * J1) * idet;
+      if (std::fabs(r) > kDiverge && std::fabs(s) > kDiverge) {
+        diverged = true;
+        break;
+      }
+    } while (++it < maxit && (std::fabs(F0) > tol || std::fabs(F1) > tol));
+    if (!diverged && it < maxit && std::fabs(r) < 1.0 + tol && std::fabs(s) < 1.0 + tol) return e;
+  }
+  return -1;
 }
 
 }  // namespace stx

@@ -62,9 +62,21 @@ struct Mesh {
 
 Mesh build_mesh(const Session& S);
 
+// Lagrange interpolants of the GLL points q.z at x and their derivatives
+// (the intmat_g / dermat_g vectors of intp, femlib/operators.c:250-300);
+// either output may be null.
+void gll_interpolants(const Quadrature& q, double x, double* h, double* dh);
+
+// HistoryPoint::locate (src/history.cpp:45-63) with Element::locate
+// (src/element.cpp:1061-1183): the first element, in order, where Newton's
+// iteration from the nearest element node converges (|F| <= tol within
+// maxit steps) to |r|, |s| < 1 + tol.  Returns the element, -1 when none.
+int locate_point(const Mesh& M, double x, double y, double tol, int maxit, double& r, double& s);
+
 struct BoundaryEdge {
   int elmt = 0, side = 0;
   char kind = 0;              // 'D', 'N', 'M' (mixed) or 'H' (pressure only); others rejected
+  char group = 0;             // boundary group
   std::string expr;
   double mix_K = 0.0, mix_C = 0.0;  // 'M': dc/dn + K (c - C) = 0
   std::vector<double> area;   // np quadrature-weighted side lengths

@@ -2,6 +2,7 @@
 
 #include <algorithm>
 #include <cctype>
+#include <cstdlib>
 #include <fstream>
 #include <sstream>
 #include <stdexcept>
@@ -39,6 +40,25 @@ bool section(const std::string& text, const std::string& name, std::string& body
     throw std::runtime_error("FEML: unterminated section " + name);
   body = text.substr(gt + 1, end - gt - 1);
   return true;
+}
+
+// Integer attribute `attr=` of the opening tag of section NAME
+// (FEML::attribute, src/feml.cpp:258-300); -1 when the tag lacks it.
+int attribute(const std::string& text, const std::string& name, const std::string& attr) {
+  const std::string U = upper(text);
+  const std::string open = "<" + name;
+  size_t p = 0;
+  while ((p = U.find(open, p)) != std::string::npos) {
+    size_t q = p + open.size();
+    if (q < U.size() && (U[q] == '>' || std::isspace(static_cast<unsigned char>(U[q])))) break;
+    p = q;
+  }
+  if (p == std::string::npos) return -1;
+  const size_t gt = U.find('>', p);
+  const std::string tag = U.substr(p, gt == std::string::npos ? std::string::npos : gt - p);
+  const size_t a = tag.find(upper(attr) + "=");
+  if (a == std::string::npos) return -1;
+  return std::atoi(tag.c_str() + a + attr.size() + 1);
 }
 
 std::vector<std::string> lines(const std::string& body) {
@@ -124,6 +144,18 @@ Session read_session(const std::string& path, const std::string& overrides) {
       std::string g, d;
       is >> id >> g >> d;
       S.groups[g[0]] = d;
+    }
+  }
+  // HISTORY (Analyser::Analyser, src/analysis.cpp:108-134): NUMBER
+  // points read as "id x y z" from the section's start
+  if (section(text, "HISTORY", body)) {
+    const int n = attribute(text, "HISTORY", "NUMBER");
+    if (n < 0) throw std::runtime_error("FEML: HISTORY needs NUMBER=");
+    std::istringstream is(body);
+    for (int i = 0; i < n; ++i) {
+      HistoryPoint h;
+      if (!(is >> h.id >> h.x >> h.y >> h.z)) throw std::runtime_error("FEML: short HISTORY section");
+      S.history.push_back(h);
     }
   }
   if (section(text, "BCS", body)) {

@@ -2,7 +2,7 @@
 //
 // Reads the sections the reference reads for the dns / elliptic hot path
 // (src/feml.cpp:64-330, src/mesh.cpp:129-470, src/bcmgr.cpp:100-110):
-// TOKENS, FIELDS, GROUPS, BCS, NODES, ELEMENTS (<Q> quads), SURFACES
+// TOKENS, FIELDS, GROUPS, HISTORY, BCS, NODES, ELEMENTS (<Q> quads), SURFACES
 // (<B> boundary group or <P> periodic mate), USER, FORCE (dns/fieldforce.cpp:
 // 31-73).  CURVES are recorded as present and rejected by the mesh builder
 // (straight sides only).
@@ -29,6 +29,13 @@ struct Surface {
   int mate_elmt = -1, mate_side = -1;  // for 'P'
 };
 
+// A history point of the HISTORY section (Analyser::Analyser,
+// src/analysis.cpp:108-134): tag and location.
+struct HistoryPoint {
+  int id = 0;
+  double x = 0.0, y = 0.0, z = 0.0;
+};
+
 struct Session {
   std::string path, name;
   TokenTable tokens;
@@ -42,6 +49,7 @@ struct Session {
   bool has_curves = false;
   bool has_force = false;                            // <FORCE> section present
   std::vector<std::string> force;                    // its raw lines
+  std::vector<HistoryPoint> history;                 // HISTORY section, in order
 
   // FEML::valueFromSection (src/feml.cpp:430-560) on the FORCE section: the
   // text after `token` on the first line whose first word is `token` (words

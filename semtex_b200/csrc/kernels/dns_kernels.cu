@@ -247,6 +247,76 @@ __global__ void __launch_bounds__(kAnaThreads) k_cfl(DevGeom g, const double* __
   block_store(s, part, blockIdx.x, true);
 }
 
+// History-point values (AuxField::probe, src/auxfield.cpp:1621-1700, over
+// Element::probe, src/element.cpp:1186-1203): block (point, field); the
+// point's interpolants is (rows) and ir (columns) and Fourier coefficients
+// c_k in w[point][2 np + nz], so that value = sum_k c_k is^T F_k ir on the
+// point's element (c_0 = 1, c_1 = cos(nz/2 beta z), 2 cos / -2 sin of
+// k beta z on the Re / Im planes of mode k).
+__global__ void __launch_bounds__(kAnaThreads) k_probe(DevGeom g, ProbeArgs a) {
+  const int p = blockIdx.x, f = blockIdx.y;
+  const int np = g.np, nn = g.npnp;
+  const double* w = a.w + static_cast<size_t>(p) * (2 * np + a.nzc);
+  const double* is = w;
+  const double* ir = w + np;
+  const double* c = w + 2 * np;
+  const double* src = a.f[f] + static_cast<size_t>(a.elmt[p]) * nn;
+  double v = 0.0;
+  for (int q = threadIdx.x; q < a.nzc * nn; q += blockDim.x) {
+    const int k = q / nn, t = q - k * nn;
+    const int i = t / np, j = t - i * np;
+    v += c[k] * is[i] * ir[j] * src[static_cast<size_t>(k) * g.plane_size + t];
+  }
+  block_store(v, a.out, p * a.nf + f, false);
+}
+
+// Forces on the wall edges (Edge::normTraction / tangTraction / scalarFlux,
+// src/edge.cpp:259-378, with Element::sideGrad, :621-700 of
+// src/element.cpp): one warp per edge on plane 0 (the mean mode); per edge
+// out[5 e ..] = sum of n p area (x, y), of the viscous traction sums
+// (2 ux nx + uy ny + vx ny, uy nx + 2 vy ny + vx nx) area and of
+// (wx nx + wy ny) area.  The gradients are the element's at the side nodes.
+__global__ void __launch_bounds__(32) k_wall_forces(DevGeom g, WallArgs a) {
+  const int b = blockIdx.x, ln = threadIdx.x;
+  const int np = g.np, nn = g.npnp;
+  const int e = a.elmt[b];
+  double acc[5] = {0.0, 0.0, 0.0, 0.0, 0.0};
+  if (ln < np) {
+    const int t = a.node[b * np + ln];
+    const int i = t / np, j = t - i * np;
+    const size_t o = static_cast<size_t>(e) * nn;
+    const double nx = a.nx[b * np + ln], ny = a.ny[b * np + ln], area = a.area[b * np + ln];
+    auto grad = [&](const double* f, double& fx, double& fy) {
+      double dr = 0.0, ds = 0.0;
+      for (int k = 0; k < np; ++k) {
+        dr += g.D[j * np + k] * f[o + i * np + k];
+        ds += g.D[i * np + k] * f[o + k * np + j];
+      }
+      fx = g.drdx[o + t] * dr + g.dsdx[o + t] * ds;
+      fy = g.drdy[o + t] * dr + g.dsdy[o + t] * ds;
+    };
+    const double pv = a.p[o + t];
+    acc[0] = nx * pv * area;
+    acc[1] = ny * pv * area;
+    double ux, uy, vx, vy;
+    grad(a.u, ux, uy);
+    grad(a.v, vx, vy);
+    acc[2] = (2.0 * ux * nx + uy * ny) * area + vx * ny * area;
+    acc[3] = uy * nx * area + (2.0 * vy * ny + vx * nx) * area;
+    if (a.w) {
+      double wx, wy;
+      grad(a.w, wx, wy);
+      acc[4] = (wx * nx + wy * ny) * area;
+    }
+  }
+#pragma unroll
+  for (int q = 0; q < 5; ++q) {
+    double v = acc[q];
+    for (int o = 16; o; o >>= 1) v += __shfl_xor_sync(0xffffffffu, v, o);
+    if (ln == 0) a.out[5 * b + q] = v;
+  }
+}
+
 __global__ void k_grad_z(const double* __restrict__ in, double* __restrict__ out, int nz, int plane_size,
                          double beta) {
   pdl_trigger();
@@ -529,6 +599,20 @@ cudaError_t dns_mode_energy_partials(const DevGeom& g, const double* f, double* 
 
 cudaError_t dns_cfl_partials(const DevGeom& g, const double* u, int dir, double d, double* part, cudaStream_t st) {
   k_cfl<<<dns_analysis_blocks(), kAnaThreads, 0, st>>>(g, u, dir, d, part);
+  return cudaGetLastError();
+}
+
+cudaError_t dns_probe(const DevGeom& g, const ProbeArgs& a, cudaStream_t st) {
+  if (a.npts <= 0) return cudaSuccess;
+  if (a.nf < 1 || a.nf > 8) return cudaErrorInvalidValue;
+  k_probe<<<dim3(a.npts, a.nf), kAnaThreads, 0, st>>>(g, a);
+  return cudaGetLastError();
+}
+
+cudaError_t dns_wall_forces(const DevGeom& g, const WallArgs& a, cudaStream_t st) {
+  if (a.nw <= 0) return cudaSuccess;
+  if (g.np > 32) return cudaErrorInvalidValue;
+  k_wall_forces<<<a.nw, 32, 0, st>>>(g, a);
   return cudaGetLastError();
 }
 

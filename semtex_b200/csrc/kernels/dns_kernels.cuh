@@ -66,6 +66,37 @@ int dns_analysis_blocks();
 cudaError_t dns_mode_energy_partials(const DevGeom& g, const double* f, double* part, cudaStream_t st);
 cudaError_t dns_cfl_partials(const DevGeom& g, const double* u, int dir, double d, double* part, cudaStream_t st);
 
+// History-point values: out[p * nf + f] for fields f[0..nf) at points
+// p < npts on elements elmt[p], with per-point weights w[p][2 np + nzc]
+// (interpolants in s, in r, then nzc Fourier coefficients).
+struct ProbeArgs {
+  int npts, nf, nzc;
+  const int* elmt;
+  const double* w;
+  const double* f[8];
+  double* out;
+};
+cudaError_t dns_probe(const DevGeom& g, const ProbeArgs& a, cudaStream_t st);
+
+// Wall forces: per edge b (element elmt[b], side nodes node[b][np] in the
+// side traverse, unit normal and quadrature-weighted length per node) the
+// five sums out[5 b ..] of the plane-0 data (pressure x, y; viscous x, y;
+// flux of w, 0 when w is null).
+struct WallArgs {
+  int nw;
+  const int* elmt;
+  const int* node;
+  const double* nx;
+  const double* ny;
+  const double* area;
+  const double* p;
+  const double* u;
+  const double* v;
+  const double* w;
+  double* out;
+};
+cudaError_t dns_wall_forces(const DevGeom& g, const WallArgs& a, cudaStream_t st);
+
 cudaError_t dns_grad_xy(const DevGeom& g, const double* in, double* out, int dir, cudaStream_t st);
 cudaError_t dns_grad_z(const DevGeom& g, const double* in, double* out, double beta, cudaStream_t st);
 cudaError_t dns_product(const DevGeom& g, const double* a, const double* b, double* out, cudaStream_t st);

@@ -12,7 +12,7 @@ import numpy as np
 
 def rect_session(path, nx, ny, x=(0.0, 1.0), y=(0.0, 1.0), tokens=None, fields="c",
                  periodic_x=False, periodic_y=False, bcs=None, user=None, xs=None, ys=None,
-                 wall_group="w", force=None, side_groups=None, group_names=None):
+                 wall_group="w", force=None, side_groups=None, group_names=None, history=None):
     """Write a session file.
 
     bcs: {group_char: {field: "<D> value" | "<N> value" | "<H>"}} applied to
@@ -22,6 +22,7 @@ def rect_session(path, nx, ny, x=(0.0, 1.0), y=(0.0, 1.0), tokens=None, fields="
     side_groups: {"bottom" | "top" | "left" | "right": group char} overriding
     `wall_group` on those sides; group_names: {group char: descriptor}
     ("wall" by default; "outflow" and "axis" are the reserved ones).
+    history: (id, x, y, z) points of a <HISTORY> section, or None.
     """
     side_groups = side_groups or {}
     group_names = group_names or {}
@@ -43,6 +44,10 @@ def rect_session(path, nx, ny, x=(0.0, 1.0), y=(0.0, 1.0), tokens=None, fields="
         lines.append("<FORCE>")
         lines += [f"\t{f}" for f in force]
         lines.append("</FORCE>\n")
+    if history:
+        lines.append(f"<HISTORY NUMBER={len(history)}>")
+        lines += [f"\t{i}\t{hx:.17g}\t{hy:.17g}\t{hz:.17g}" for (i, hx, hy, hz) in history]
+        lines.append("</HISTORY>\n")
     if bcs:
         lines.append(f"<GROUPS NUMBER={len(bcs)}>")
         for i, g in enumerate(bcs):
@@ -118,7 +123,7 @@ def taylor_green_session(path, n, np_, nz, re=1600.0, dt=1e-3, nstep=200, extra=
 
 
 def channel_session(path, nx=16, ny=8, np_=9, nz=32, re=500.0, dt=5e-3, nstep=100, ntime=3, extra=None,
-                    force=None):
+                    force=None, history=None):
     """Plane channel [0, 2 pi] x [-1, 1] x [0, 2 pi), periodic in x and z,
     no-slip walls at y = +-1 with high-order pressure BCs (config c5)."""
     tok = {"N_P": np_, "N_Z": nz, "BETA": 1, "KINVIS": f"1.0/{re}", "D_T": dt, "N_TIME": ntime,
@@ -129,7 +134,7 @@ def channel_session(path, nx=16, ny=8, np_=9, nz=32, re=500.0, dt=5e-3, nstep=10
     if nz > 1:
         bc["w"] = "<D> 0"
     return rect_session(path, nx, ny, x=(0.0, 2 * np.pi), y=(-1.0, 1.0), tokens=tok, fields=fields,
-                        periodic_x=True, bcs={"w": bc}, force=force)
+                        periodic_x=True, bcs={"w": bc}, force=force, history=history)
 
 
 def channel_initial(x, y, z, seed=20261203, amplitude=1e-3, modes=3):
