@@ -461,6 +461,7 @@ def run_ours(args):
         line["dns"] = run_dns(args.dns_steps, 3, local, "c3", cb)
         line["dns_c3_dealiased"] = run_dns(args.dns_steps, 3, local, "c3d", cb)
         line["dns_c5"] = run_dns(args.dns_steps, 3, local, "c5", cb)
+        line["dns_mixed_c3_dealiased"] = run_dns_mixed(args.dns_steps, 3, local, "c3d")
         line["batch_c4"] = run_batch(args.dns_steps, 3, local, not args.untuned)
         line["adjoint_c5"] = run_adjoint(local)
     print(json.dumps(line))
@@ -596,6 +597,48 @@ def run_dns(steps, warmup=3, local=0, workload="c3", cpu_baseline=False):
         out["cpu_baseline"] = {"value": 1.0 / sec, "unit": "steps/s", "cores": 1, "kind": "port",
                                "sample": what}
     return out
+
+
+def run_dns_mixed(steps, warmup=3, local=0, workload="c3d"):
+    """Secondary measurement: the DNS with mixed-precision steady velocity
+    solves (token STX_DNS_MIXED = 1: FP32 packed skeleton inverses, sums in
+    FP64, two FP64 refinements; pressure solves, field passes, FFTs and the
+    time integration in FP64) against the plain FP64 DNS on the same
+    workload and schedule.  Both run 2 start-up + warm-up + 84 graph-capture
+    steps, then `steps` timed steps (device time, CUDA events on the library
+    stream); the error is the relative L2 difference of every field from the
+    FP64 run after the same steps (the FP64 run matches the oracle)."""
+    import torch
+    import semtex_b200 as S
+    d = tempfile.mkdtemp()
+    p = dns_session(d, workload)
+    res = {}
+    fields = {}
+    for name, ov in (("fp64", None), ("mixed", {"STX_DNS_MIXED": 1})):
+        ctx = S.Context(p, overrides=ov, device=local)
+        D = S.DNS(ctx, 1)
+        funcs = S._user_functions(p)
+        D.restart({c: ctx.evaluate(funcs[c], 0.0) for c in ctx.fields if c in funcs}, 0.0)
+        D.advance(2 + warmup)
+        D.advance(84)
+        stream = ctx.torch_stream()
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        ctx.sync()
+        e0.record(stream)
+        D.advance(steps)
+        e1.record(stream)
+        e1.synchronize()
+        res[name] = e0.elapsed_time(e1) / steps
+        fields[name] = {c: D.field(c) for c in ctx.fields}
+        D.close()
+        ctx.close()
+    err = {c: float(np.linalg.norm(fields["mixed"][c] - fields["fp64"][c]) /
+                    max(np.linalg.norm(fields["fp64"][c]), 1e-300)) for c in fields["fp64"]}
+    return {"metric": "DNS steps/s", "value": 1e3 / res["mixed"], "ms_per_step": res["mixed"],
+            "steps": steps, "workload": DNS_WORKLOADS[workload],
+            "dtype": "f32 skeleton inverses of the velocity systems; f64 everything else",
+            "fp64_ms_per_step": res["fp64"], "ratio_to_fp64": res["fp64"] / res["mixed"],
+            "rel_l2_vs_fp64": err, "after_steps": 2 + warmup + 84 + steps}
 
 
 def run_adjoint(local=0, steps=100, every=10):
@@ -795,8 +838,10 @@ def main():
     ap.add_argument("--solver", default="twolevel", choices=["twolevel", "band"],
                     help="band: the single banded-Cholesky skeleton solve (for comparison)")
     ap.add_argument("--workload", default="c2",
-                    choices=["c2", "dns", "dns_c5", "batch_c4", "adjoint_c5", "dns_probe_c3", "dns_probe_c5"],
-                    help="dns / dns_c5 / batch_c4: run only that secondary measurement (one JSON line); "
+                    choices=["c2", "dns", "dns_c5", "dns_mixed", "batch_c4", "adjoint_c5", "dns_probe_c3",
+                             "dns_probe_c5"],
+                    help="dns / dns_c5 / dns_mixed / batch_c4: run only that secondary measurement (one JSON "
+                         "line); "
                          "dns_probe_c3 / _c5: 2 start-up + 3 steady steps with graph replay off, nothing "
                          "timed (a run to profile every kernel of a step)")
     args = ap.parse_args()
@@ -809,6 +854,10 @@ def main():
         torch.cuda.set_device(0)
         print(json.dumps(run_dns(max(1, args.dns_steps), args.warmup, 0,
                                  "c3" if args.workload == "dns" else "c5", not args.no_cpu_baseline)))
+    elif args.workload == "dns_mixed":
+        import torch
+        torch.cuda.set_device(0)
+        print(json.dumps(run_dns_mixed(max(1, args.dns_steps), args.warmup, 0, "c3d")))
     elif args.workload == "adjoint_c5":
         import torch
         torch.cuda.set_device(0)

@@ -603,6 +603,7 @@ int stx_dns_adjoint_create(stx_dns* d, int checkpoint_every, stx_dns_adjoint** o
     const TokenTable& T = S.tokens;
     if (d->nz32) throw AdjError(STX_EUNSUPPORTED, "adjoint: 3/2-rule products (DEALIAS) are not differentiated");
     if (d->oe.no) throw AdjError(STX_EUNSUPPORTED, "adjoint: computed outflow BCs are not differentiated");
+    if (d->mixed) throw AdjError(STX_EUNSUPPORTED, "adjoint: mixed-precision velocity solves (STX_DNS_MIXED)");
     if (T.value("SVV_EPSN") > 6.0e-14 || T.value("SVV_EPSZ") > 6.0e-14)
       throw AdjError(STX_EUNSUPPORTED, "adjoint: spectral vanishing viscosity is not differentiated");
     const auto& F = d->force;

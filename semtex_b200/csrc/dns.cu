@@ -966,14 +966,18 @@ int stx_dns_create(stx_context* ctx, int advection, stx_dns** out) {
       }
     }
     // -- preSolve (dns/integrate.cpp:292-325): ITERATIVE = 1 selects
-    //    Jacobi-PCG velocity systems; the pressure system is always direct
+    //    Jacobi-PCG velocity systems; the pressure system is always direct.
+    //    Token STX_DNS_MIXED = 1 gives the steady velocity systems the
+    //    mixed-precision form (FP32 skeleton inverses, FP64 refinement); the
+    //    pressure system stays FP64 (its mode 0 is singular)
     const double lam = kSS[d->nord][0] / (d->dt * d->nu);
     const int nmodes = (ctx->M.nz + 1) / 2;
     d->iterative = S.tokens.ivalue("ITERATIVE") != 0;
+    d->mixed = !d->iterative && S.tokens.has("STX_DNS_MIXED") && S.tokens.ivalue("STX_DNS_MIXED") != 0;
     for (int i = 0; i < d->ncom; ++i) {
       stx_modal* m = nullptr;
-      ckstx(stx_modal_create(ctx, d->names[i], lam, d->beta, 0, nmodes, d->iterative ? STX_JACPCG : STX_DIRECT,
-                             &m));
+      ckstx(stx_modal_create(ctx, d->names[i], lam, d->beta, 0, nmodes,
+                             d->iterative ? STX_JACPCG : d->mixed ? STX_MIXED : STX_DIRECT, &m));
       d->vsys.push_back(m);
     }
     ckstx(stx_modal_create(ctx, d->names[d->ncom], 0.0, d->beta, 0, nmodes, STX_DIRECT, &d->psys));

@@ -21,6 +21,7 @@ struct stx_dns {
   double dt = 0, nu = 0, beta = 0, tol = 0;
   int step_max = 0;
   bool iterative = false;  // ITERATIVE: Jacobi-PCG velocity systems at every step
+  bool mixed = false;      // STX_DNS_MIXED: mixed-precision steady velocity systems
   int step = 0;
   double time = 0;
   int toggle = 1;  // altSkewSymmetric's static switch (dns/nonlinear.cpp:254)
