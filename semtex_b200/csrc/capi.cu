@@ -185,6 +185,14 @@ static void check_sweep_status(const stx_modal* sys) {
   throw StxError(STX_ECUDA, std::string(where) + ": a bounded wait for a bulk copy expired");
 }
 
+// Planes between host and device: one linear copy when both sides are
+// packed (plane size = points per plane), else a pitched copy.
+static cudaError_t copy_planes(void* dst, size_t dpitch, const void* src, size_t spitch, size_t width, size_t rows,
+                               cudaMemcpyKind kind, cudaStream_t st) {
+  if (dpitch == width && spitch == width) return cudaMemcpyAsync(dst, src, width * rows, kind, st);
+  return cudaMemcpy2DAsync(dst, dpitch, src, spitch, width, rows, kind, st);
+}
+
 template <class T>
 static T* upload(DeviceArena& A, const std::vector<T>& v) {
   T* p = static_cast<T*>(A.alloc(sizeof(T) * v.size()));
@@ -1261,10 +1269,10 @@ int stx_elliptic_solve_host(stx_modal* sys, const double* h_forcing, double* h_s
     }
     double* dF = ctx->d_io;
     double* dU = ctx->d_io + ps * nz;
-    // one pitched copy per direction: host planes are nplane doubles apart,
-    // device planes plane_size
-    cuda_check(cudaMemcpy2DAsync(dF, sizeof(double) * ps, h_forcing, sizeof(double) * nplane,
-                                 sizeof(double) * nplane, nz, cudaMemcpyHostToDevice, ctx->stream),
+    // one copy per direction: host planes are nplane doubles apart, device
+    // planes plane_size
+    cuda_check(copy_planes(dF, sizeof(double) * ps, h_forcing, sizeof(double) * nplane, sizeof(double) * nplane,
+                           nz, cudaMemcpyHostToDevice, ctx->stream),
                "forcing h2d");
     cuda_check(z_transform(dF, M.nz, M.plane_size, STX_FORWARD, ctx->d_twiddle, nullptr, ctx->stream),
                "forward transform");
@@ -1277,8 +1285,8 @@ int stx_elliptic_solve_host(stx_modal* sys, const double* h_forcing, double* h_s
     if (rc != STX_OK) throw StxError(rc, g_last_error);
     cuda_check(z_transform(dU, M.nz, M.plane_size, STX_INVERSE, ctx->d_twiddle, nullptr, ctx->stream),
                "inverse transform");
-    cuda_check(cudaMemcpy2DAsync(h_solution, sizeof(double) * nplane, dU, sizeof(double) * ps,
-                                 sizeof(double) * nplane, nz, cudaMemcpyDeviceToHost, ctx->stream),
+    cuda_check(copy_planes(h_solution, sizeof(double) * nplane, dU, sizeof(double) * ps, sizeof(double) * nplane,
+                           nz, cudaMemcpyDeviceToHost, ctx->stream),
                "solution d2h");
     // the status words travel with the solution (no extra synchronisation)
     int* fl = ctx->flags();
@@ -1318,8 +1326,8 @@ int stx_elliptic_solve_host_batch(stx_modal* sys, int n, const double* const* h_
       double* dU = dF + ps * nz;
       // in: set b's forcing is free once solve i - kIoSets has run
       cuda_check(cudaStreamWaitEvent(ctx->s_h2d, ctx->ev_comp[b], 0), "wait");
-      cuda_check(cudaMemcpy2DAsync(dF, sizeof(double) * ps, h_forcing[i], sizeof(double) * nplane,
-                                   sizeof(double) * nplane, nz, cudaMemcpyHostToDevice, ctx->s_h2d),
+      cuda_check(copy_planes(dF, sizeof(double) * ps, h_forcing[i], sizeof(double) * nplane,
+                             sizeof(double) * nplane, nz, cudaMemcpyHostToDevice, ctx->s_h2d),
                  "forcing h2d");
       cuda_check(cudaEventRecord(ctx->ev_in[b], ctx->s_h2d), "record");
       // solve: after the forcing landed and set b's solution was read out
@@ -1338,8 +1346,8 @@ int stx_elliptic_solve_host_batch(stx_modal* sys, int n, const double* const* h_
       cuda_check(cudaEventRecord(ctx->ev_comp[b], ctx->stream), "record");
       // out
       cuda_check(cudaStreamWaitEvent(ctx->s_d2h, ctx->ev_comp[b], 0), "wait");
-      cuda_check(cudaMemcpy2DAsync(h_solution[i], sizeof(double) * nplane, dU, sizeof(double) * ps,
-                                   sizeof(double) * nplane, nz, cudaMemcpyDeviceToHost, ctx->s_d2h),
+      cuda_check(copy_planes(h_solution[i], sizeof(double) * nplane, dU, sizeof(double) * ps,
+                             sizeof(double) * nplane, nz, cudaMemcpyDeviceToHost, ctx->s_d2h),
                  "solution d2h");
       cuda_check(cudaEventRecord(ctx->ev_out[b], ctx->s_d2h), "record");
     }
