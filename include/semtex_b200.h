@@ -324,6 +324,15 @@ int stx_dns_probe(stx_dns* dns, int npts, const int* h_elmt, const double* h_rs,
  * (-RHO KINVIS times the traction sums; z from the wall flux of w in 3D).
  * Zero without wall edges. */
 int stx_dns_wall_forces(stx_dns* dns, double* pressure, double* viscous);
+/* Tractions along the edges of the "wall" group, in physical space
+ * (DNSAnalyser::analyse's session.wss data, dns/dnsanalysis.cpp:130-250:
+ * Field::traction, src/field.cpp:533-593, per Fourier mode, then the inverse
+ * z transform): *nline (if not null) receives N_P x the number of wall
+ * edges; h_out (if not null; 3 x N_Z x nline doubles) receives the normal
+ * (pressure), in-plane and out-of-plane viscous tractions, each as N_Z
+ * planes of the wall lines, edges in the SURFACES section's order and
+ * nodes along each side. */
+int stx_dns_wall_traction(stx_dns* dns, int* nline, double* h_out);
 /* Full-state checkpoint of the time stepping: the fields, the multi-level
  * velocity and nonlinear storage Us/Uf of every order (dns/integrate.cpp:
  * 99-136), the high-order pressure BC levels (BCmgr's _un / _hopbc,

@@ -2164,6 +2164,62 @@ class DNS:
                 vf[2] -= mu * np.sum((wx * nx + wy * ny) * area)
         return pf, vf
 
+    def wall_traction(self):
+        """Field::traction (src/field.cpp:533-593; Edge::traction,
+        src/edge.cpp:381-540) per Fourier mode over the edges of the group
+        named "wall" in SURFACES order, then the inverse z transform (plane 0
+        copied when N_Z = 2): [3, nz, np * nwall] normal, in-plane and
+        out-of-plane tractions in physical space."""
+        P, M = self.P, self.P.M
+        S, tok = P.S, P.S.tokens
+        names = S.fields
+        mu = tok["RHO"] * tok["KINVIS"]
+        beta = tok["BETA"]
+        nz = P.nz
+        pres, u, v = self.u[names[self.ncom]], self.u[names[0]], self.u[names[1]]
+        w = self.u[names[2]] if self.ncom == 3 else None
+        walls = [(e, s) for (e, s, kind, g) in S.surfaces if kind == "B" and S.groups.get(g, "") == "wall"]
+        npn = P.np
+        out = np.zeros((3, nz, npn * len(walls)))
+        for b, (e, s) in enumerate(walls):
+            idx = M.side_nodes(s)
+            sgn, (a, c) = {0: (-1, ("dsdx", "dsdy")), 1: (1, ("drdx", "drdy")),
+                           2: (1, ("dsdx", "dsdy")), 3: (-1, ("drdx", "drdy"))}[s]
+            nx = sgn * getattr(M, a)[e].ravel()[idx]
+            ny = sgn * getattr(M, c)[e].ravel()[idx]
+            ln = np.hypot(nx, ny)
+            nx, ny = nx / ln, ny / ln
+            sl = slice(b * npn, (b + 1) * npn)
+
+            def gr(f):
+                return grad(M, f, 0)[e].ravel()[idx], grad(M, f, 1)[e].ravel()[idx]
+
+            def tang(U, V):
+                ux, uy = gr(U)
+                vx, vy = gr(V)
+                return (-2 * ux * nx * ny - uy * ny * ny + uy * nx * nx) + (2 * vy * nx * ny - vx * ny * ny + vx * nx * nx)
+
+            out[0, 0, sl] = pres[0][e].ravel()[idx]
+            out[1, 0, sl] = -mu * tang(u[0], v[0])
+            if w is not None:
+                wx, wy = gr(w[0])
+                out[2, 0, sl] = -mu * (wx * nx + wy * ny)
+            for m in range(1, nz // 2 if nz > 2 else 1):
+                bk, re, im = m * beta, 2 * m, 2 * m + 1
+                side = lambda f: f[e].ravel()[idx]
+                out[0, re, sl], out[0, im, sl] = side(pres[re]), side(pres[im])
+                out[1, re, sl] = -mu * tang(u[re], v[re])
+                out[1, im, sl] = -mu * tang(u[im], v[im])
+                wx, wy = gr(w[re])
+                out[2, re, sl] = -mu * ((wx - bk * side(u[im])) * nx + (wy - bk * side(v[im])) * ny)
+                wx, wy = gr(w[im])
+                out[2, im, sl] = -mu * ((wx + bk * side(u[re])) * nx + (wy + bk * side(v[re])) * ny)
+        if nz == 2:
+            out[:, 1] = out[:, 0]
+        elif nz > 2:
+            out = np.stack([dft_inverse(out[c]) for c in range(3)])
+        return out
+
     def physical(self):
         out = {}
         for c, v in self.u.items():

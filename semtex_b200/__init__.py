@@ -545,6 +545,17 @@ class DNS:
         check(lib().stx_dns_wall_forces(self._h, p.ctypes.data, v.ctypes.data))
         return p, v
 
+    def wall_traction(self) -> np.ndarray:
+        """Normal, in-plane and out-of-plane tractions along the "wall"
+        group in physical space, [3, nz, N_P x wall edges] (Field::traction,
+        the data of session.wss)."""
+        n = C.c_int()
+        check(lib().stx_dns_wall_traction(self._h, C.byref(n), None))
+        out = np.zeros((3, self.ctx.nz, n.value))
+        if n.value:
+            check(lib().stx_dns_wall_traction(self._h, C.byref(n), out.ctypes.data))
+        return out
+
 
 class DNSAdjoint:
     """Discrete adjoint and tangent-linear model of a DNS's time steps over

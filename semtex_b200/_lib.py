@@ -75,6 +75,7 @@ SIGNATURES = {
     "stx_dns_cfl": (_i, [_p, _pd]),
     "stx_dns_probe": (_i, [_p, _i, _p, _p, _p, _p]),
     "stx_dns_wall_forces": (_i, [_p, _p, _p]),
+    "stx_dns_wall_traction": (_i, [_p, _pi, _p]),
     "stx_dns_graph_info": (_i, [_p, _pi, C.POINTER(C.c_longlong)]),
     "stx_dns_status": (_i, [_p, _pi]),
     "stx_dns_stats_update": (_i, [_p]),

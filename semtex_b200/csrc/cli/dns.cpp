@@ -16,10 +16,15 @@
 // session.his (Analyser::analyse, src/analysis.cpp:275-304) and the forces
 // on the "wall" group to session.flx (DNSAnalyser, dns/dnsanalysis.cpp:
 // 44-127); every IO_MDL steps the modal energies go to session.mdl
-// (Analyser::modalEnergy, src/analysis.cpp:329-375).
+// (Analyser::modalEnergy, src/analysis.cpp:329-375); with IO_WSS > 0 and a
+// "wall" group, every IO_WSS and IO_FLD steps and at the end the wall
+// tractions are appended to session.wss (a header like a field file's, then
+// the normal, in-plane and out-of-plane tractions, N_Z planes each,
+// dns/dnsanalysis.cpp:130-250).
 #include <cmath>
 #include <cstdio>
 #include <cstring>
+#include <ctime>
 #include <fstream>
 #include <iomanip>
 #include <string>
@@ -171,6 +176,17 @@ int main(int argc, char** argv) {
   flx << "# DNS state information file" << std::endl
       << "# Step Time [Fpre Fvis Ftot]-axis" << std::endl
       << "# -------------------------------" << std::endl;
+  // wall tractions (DNSAnalyser::DNSAnalyser, dns/dnsanalysis.cpp:53-81)
+  const int io_wss = static_cast<int>(std::lround(token(ctx, "IO_WSS")));
+  int wss_line = 0;
+  check(stx_dns_wall_traction(dns, &wss_line, nullptr), "wall traction");
+  std::ofstream wss;
+  std::vector<double> wss_val;
+  if (io_wss > 0 && wss_line > 0) {
+    wss.open(session + ".wss", std::ios::binary);
+    if (!wss) fail("can't open WSS file");
+    wss_val.resize(static_cast<size_t>(3) * nz * wss_line);
+  }
   std::vector<double> his_val(his_id.size() * fields.size());
   std::vector<double> ek((nz + 1) / 2);
   const double dt = token(ctx, "D_T");
@@ -192,6 +208,7 @@ int main(int argc, char** argv) {
     if (io_cfl > 0) next = std::min(next, (step / io_cfl + 1) * io_cfl);
     next = std::min(next, (step / io_his + 1) * io_his);
     if (io_mdl > 0) next = std::min(next, (step / io_mdl + 1) * io_mdl);
+    if (wss.is_open()) next = std::min(next, (step / io_wss + 1) * io_wss);
     if (verbose) {  // the step line of DNSAnalyser::analyse, one step at a time
       for (; step < next; ++step) {
         check(stx_dns_advance(dns, 1), "integrate");
@@ -238,6 +255,34 @@ int main(int argc, char** argv) {
       flx << line << std::endl;
     }
     if (averaging && step % io_his == 0) check(stx_dns_stats_update(dns), "statistics");
+    if (wss.is_open() && (step % io_wss == 0 || step % io_fld == 0 || step == nstep)) {
+      check(stx_dns_wall_traction(dns, &wss_line, wss_val.data()), "wall traction");
+      char created[64];
+      const std::time_t now = std::time(nullptr);
+      std::strftime(created, sizeof(created), "%a %b %d %H:%M:%S %Y", std::localtime(&now));
+      const bool little = [] {
+        const unsigned one = 1;
+        return *reinterpret_cast<const unsigned char*>(&one) == 1;
+      }();
+      const std::string fmt = std::string("binary IEEE ") + (little ? "little-endian" : "big-endian");
+      char h[1024];
+      int n = 0;
+      n += std::snprintf(h + n, sizeof(h) - n, "%-25s Session\n", out.session.c_str());
+      n += std::snprintf(h + n, sizeof(h) - n, "%-25s Created\n", created);
+      n += std::snprintf(h + n, sizeof(h) - n, "%-5d1    %-5d %-10dNr, Ns, Nz, Elements\n", np, nz, wss_line / np);
+      n += std::snprintf(h + n, sizeof(h) - n, "%-25d Step\n", step);
+      n += std::snprintf(h + n, sizeof(h) - n, "%-25.6g Time\n", time);
+      n += std::snprintf(h + n, sizeof(h) - n, "%-25.6g Time step\n", dt);
+      n += std::snprintf(h + n, sizeof(h) - n, "%-25.6g Kinvis\n", out.kinvis);
+      n += std::snprintf(h + n, sizeof(h) - n, "%-25.6g Beta\n", out.beta);
+      n += std::snprintf(h + n, sizeof(h) - n, "%-25s Fields written\n", "nts");
+      n += std::snprintf(h + n, sizeof(h) - n, "%-25s Format\n", fmt.c_str());
+      wss.write(h, n);
+      wss.write(reinterpret_cast<const char*>(wss_val.data()),
+                static_cast<std::streamsize>(sizeof(double) * wss_val.size()));
+      wss.flush();
+      if (!wss) fail("unable to write WSS output");
+    }
     if (io_mdl > 0 && step % io_mdl == 0) {  // Analyser::modalEnergy
       check(stx_dns_modal_energy(dns, ek.data()), "modal energy");
       for (size_t m = 0; m < ek.size(); ++m)

@@ -882,15 +882,22 @@ int stx_dns_create(stx_context* ctx, int advection, stx_dns** out) {
       }
     }
     // -- edges of the boundary group "wall" (the group string compared as
-    //    Edge::normTraction does, src/edge.cpp:259-289), for the forces
+    //    Edge::normTraction does, src/edge.cpp:259-289), for the forces and
+    //    tractions, in the order of the SURFACES section (BCmgr::buildsurf,
+    //    src/bcmgr.cpp:827-870: the order of the tractions in session.wss)
     {
       const FieldDev& U = ctx->fields.at(d->names[0]);
+      std::map<std::pair<int, int>, const BoundaryEdge*> by_side;
+      for (const BoundaryEdge& E : U.N.edges) by_side[{E.elmt, E.side}] = &E;
       std::vector<int> el, nd;
       std::vector<double> nx, ny, area;
       std::vector<int> idx(g.np);
-      for (const BoundaryEdge& E : U.N.edges) {
-        const auto gi = S.groups.find(E.group);
-        if (gi == S.groups.end() || gi->second != "wall") continue;
+      for (const Surface& sf : S.surfaces) {
+        if (sf.kind != 'B') continue;
+        const auto gi = S.groups.find(sf.group);
+        const auto be = by_side.find({sf.elmt, sf.side});
+        if (gi == S.groups.end() || gi->second != "wall" || be == by_side.end()) continue;
+        const BoundaryEdge& E = *be->second;
         el.push_back(E.elmt);
         ctx->M.side_nodes(E.side, idx.data());
         nd.insert(nd.end(), idx.begin(), idx.end());
@@ -912,6 +919,11 @@ int stx_dns_create(stx_context* ctx, int advection, stx_dns** out) {
         d->w_ny = up(ny);
         d->w_area = up(area);
         d->w_out = static_cast<double*>(d->arena.alloc(sizeof(double) * 5 * d->nwall));
+        // tractions: nz planes of the three components' wall lines, padded
+        // to an even length (DNSAnalyser::DNSAnalyser, dns/dnsanalysis.cpp:55-72)
+        const int nline = g.np * d->nwall;
+        d->w_npad = 3 * nline + (3 * nline) % 2;
+        d->w_buf = static_cast<double*>(d->arena.alloc(sizeof(double) * d->w_npad * g.nz));
       }
     }
     // -- computed outflow edges and storage (BCmgr::buildComputedBCs,
@@ -1270,6 +1282,46 @@ int stx_dns_wall_forces(stx_dns* d, double* pressure, double* viscous) {
       viscous[1] -= mu * e[3];
       if (d->ndim == 3) viscous[2] -= mu * e[4];
     }
+  });
+}
+
+int stx_dns_wall_traction(stx_dns* d, int* nline, double* h_out) {
+  return dns_guarded([&] {
+    if (!d) throw DnsError(STX_EINVAL, "null argument");
+    stx_context* ctx = d->ctx;
+    const Mesh& M = ctx->M;
+    const int nl = M.np * d->nwall;
+    if (nline) *nline = nl;
+    if (!h_out || !d->nwall) return;
+    cudaSetDevice(ctx->device);
+    TractionArgs a{};
+    a.nw = d->nwall;
+    a.nline = nl;
+    a.npad = d->w_npad;
+    a.nz = M.nz;
+    a.elmt = d->w_elmt;
+    a.node = d->w_node;
+    a.nx = d->w_nx;
+    a.ny = d->w_ny;
+    // Field::traction's fields (dns/dnsanalysis.cpp:145-150): the pressure,
+    // u, v, and w when the session has three velocity components
+    a.p = d->u[d->ncom];
+    a.u = d->u[0];
+    a.v = d->u[1];
+    a.w = d->ncom == 3 ? d->u[2] : nullptr;
+    a.mu = ctx->S.tokens.value("RHO") * d->nu;
+    a.beta = d->beta;
+    a.out = d->w_buf;
+    ck(cudaMemsetAsync(d->w_buf, 0, sizeof(double) * d->w_npad * M.nz, ctx->stream), "zero");
+    ck(dns_wall_traction(ctx->dg, a, ctx->stream), "wall traction");
+    // to physical space along z (Femlib::DFTr inverse, as Field::bTransform)
+    ck(z_transform(d->w_buf, M.nz, d->w_npad, STX_INVERSE, ctx->d_twiddle, nullptr, ctx->stream), "transform");
+    for (int c = 0; c < 3; ++c)
+      ck(cudaMemcpy2DAsync(h_out + static_cast<size_t>(c) * M.nz * nl, sizeof(double) * nl, d->w_buf + c * nl,
+                           sizeof(double) * d->w_npad, sizeof(double) * nl, M.nz, cudaMemcpyDeviceToHost,
+                           ctx->stream),
+         "download");
+    ck(cudaStreamSynchronize(ctx->stream), "sync");
   });
 }
 

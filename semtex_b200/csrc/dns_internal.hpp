@@ -78,6 +78,8 @@ struct stx_dns {
   const double* w_ny = nullptr;
   const double* w_area = nullptr;
   double* w_out = nullptr;
+  int w_npad = 0;            // traction plane length: 3 np nwall rounded up to even
+  double* w_buf = nullptr;   // [nz][w_npad] tractions (stx_dns_wall_traction)
   // History-point scratch (stx_dns_probe), grown on demand: per-point
   // weights, elements and results.
   void* probe_buf = nullptr;

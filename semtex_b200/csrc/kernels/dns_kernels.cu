@@ -317,6 +317,67 @@ __global__ void __launch_bounds__(32) k_wall_forces(DevGeom g, WallArgs a) {
   }
 }
 
+// Wall tractions (Field::traction, src/field.cpp:533-593, over
+// Edge::traction, src/edge.cpp:381-540): block (edge b, mode m), one lane
+// per side node.  Mode 0 (plane 0; plane 1 left zero): n = p,
+// t = -mu [(-2 ux nx ny - uy ny^2 + uy nx^2) + (2 vy nx ny - vx ny^2 + vx nx^2)],
+// s = -mu (wx nx + wy ny).  Mode m > 0, planes 2m (Re), 2m + 1 (Im): n and t
+// of each part alike, s_Re = -mu ((wx - bk u_Im) nx + (wy - bk v_Im) ny),
+// s_Im = -mu ((wx + bk u_Re) nx + (wy + bk v_Re) ny) with the w gradients
+// of the same part and bk = m BETA.
+__global__ void __launch_bounds__(32) k_wall_traction(DevGeom g, TractionArgs a) {
+  const int b = blockIdx.x, m = blockIdx.y, ln = threadIdx.x;
+  const int np = g.np, nn = g.npnp;
+  if (ln >= np) return;
+  const int t = a.node[b * np + ln];
+  const int i = t / np, j = t - i * np;
+  const size_t o = static_cast<size_t>(a.elmt[b]) * nn;
+  const double nx = a.nx[b * np + ln], ny = a.ny[b * np + ln];
+  auto grad = [&](const double* f, double& fx, double& fy) {
+    double dr = 0.0, ds = 0.0;
+    for (int k = 0; k < np; ++k) {
+      dr += g.D[j * np + k] * f[o + i * np + k];
+      ds += g.D[i * np + k] * f[o + k * np + j];
+    }
+    fx = g.drdx[o + t] * dr + g.dsdx[o + t] * ds;
+    fy = g.drdy[o + t] * dr + g.dsdy[o + t] * ds;
+  };
+  auto tang = [&](const double* U, const double* V) {
+    double ux, uy, vx, vy;
+    grad(U, ux, uy);
+    grad(V, vx, vy);
+    return (-2.0 * ux * nx * ny - uy * ny * ny + uy * nx * nx) + (2.0 * vy * nx * ny - vx * ny * ny + vx * nx * nx);
+  };
+  const int q = b * np + ln;
+  const size_t ps = g.plane_size;
+  if (m == 0) {
+    double* o0 = a.out;
+    o0[q] = a.p[o + t];
+    o0[a.nline + q] = -a.mu * tang(a.u, a.v);
+    double sv = 0.0;
+    if (a.w) {
+      double wx, wy;
+      grad(a.w, wx, wy);
+      sv = -a.mu * (wx * nx + wy * ny);
+    }
+    o0[2 * a.nline + q] = sv;
+    return;
+  }
+  const double bk = m * a.beta;
+  const size_t re = 2 * m * ps, im = re + ps;
+  double* orr = a.out + static_cast<size_t>(2 * m) * a.npad;
+  double* oi = orr + a.npad;
+  orr[q] = a.p[re + o + t];
+  oi[q] = a.p[im + o + t];
+  orr[a.nline + q] = -a.mu * tang(a.u + re, a.v + re);
+  oi[a.nline + q] = -a.mu * tang(a.u + im, a.v + im);
+  double wx, wy;
+  grad(a.w + re, wx, wy);
+  orr[2 * a.nline + q] = -a.mu * ((wx - bk * a.u[im + o + t]) * nx + (wy - bk * a.v[im + o + t]) * ny);
+  grad(a.w + im, wx, wy);
+  oi[2 * a.nline + q] = -a.mu * ((wx + bk * a.u[re + o + t]) * nx + (wy + bk * a.v[re + o + t]) * ny);
+}
+
 __global__ void k_grad_z(const double* __restrict__ in, double* __restrict__ out, int nz, int plane_size,
                          double beta) {
   pdl_trigger();
@@ -613,6 +674,13 @@ cudaError_t dns_wall_forces(const DevGeom& g, const WallArgs& a, cudaStream_t st
   if (a.nw <= 0) return cudaSuccess;
   if (g.np > 32) return cudaErrorInvalidValue;
   k_wall_forces<<<a.nw, 32, 0, st>>>(g, a);
+  return cudaGetLastError();
+}
+
+cudaError_t dns_wall_traction(const DevGeom& g, const TractionArgs& a, cudaStream_t st) {
+  if (a.nw <= 0) return cudaSuccess;
+  if (g.np > 32 || (g.nz > 2 && !a.w)) return cudaErrorInvalidValue;
+  k_wall_traction<<<dim3(a.nw, g.nz > 2 ? g.nz / 2 : 1), 32, 0, st>>>(g, a);
   return cudaGetLastError();
 }
 

@@ -97,6 +97,25 @@ struct WallArgs {
 };
 cudaError_t dns_wall_forces(const DevGeom& g, const WallArgs& a, cudaStream_t st);
 
+// Wall tractions of every Fourier mode: plane k of out (npad doubles a
+// plane) holds the normal (pressure) values of the wall lines at [0, nline),
+// the in-plane viscous traction at [nline, 2 nline) and the out-of-plane one
+// at [2 nline, 3 nline) (zero when w is null), edges as in WallArgs.
+struct TractionArgs {
+  int nw, nline, npad, nz;
+  const int* elmt;
+  const int* node;
+  const double* nx;
+  const double* ny;
+  const double* p;
+  const double* u;
+  const double* v;
+  const double* w;
+  double mu, beta;
+  double* out;
+};
+cudaError_t dns_wall_traction(const DevGeom& g, const TractionArgs& a, cudaStream_t st);
+
 cudaError_t dns_grad_xy(const DevGeom& g, const double* in, double* out, int dir, cudaStream_t st);
 cudaError_t dns_grad_z(const DevGeom& g, const double* in, double* out, double beta, cudaStream_t st);
 cudaError_t dns_product(const DevGeom& g, const double* a, const double* b, double* out, cudaStream_t st);

@@ -1,12 +1,16 @@
-"""History points, wall forces and the analyser's files on the device
-(stx_mesh_locate, stx_dns_probe, stx_dns_wall_forces; the `dns` program's
-session.his, session.mdl and session.flx).
+"""History points, wall forces, wall tractions and the analyser's files on
+the device (stx_mesh_locate, stx_dns_probe, stx_dns_wall_forces,
+stx_dns_wall_traction; the `dns` program's session.his, session.mdl,
+session.flx and session.wss).
 
 - Probes and forces against the oracle's restatement (HistoryPoint::extract
   over AuxField::probe, src/auxfield.cpp:1621-1700; Field::normTraction /
   tangTraction, src/field.cpp:392-458) evaluated on the DNS's own Fourier
   fields after a few steps: the plane channel in 3D (N_Z = 8) and 2D, and
   the periodic Taylor-Green box (no wall: zero forces).
+- Wall tractions (Field::traction, src/field.cpp:533-593) against the
+  oracle on the channel with 8, 2 and 1 planes: every mode's normal,
+  in-plane and out-of-plane traction, then the inverse z transform.
 - The `dns` program's files against the same values through the Python
   API, line for line in the reference's formats (src/analysis.cpp:275-375,
   dns/dnsanalysis.cpp:44-127).
@@ -84,6 +88,24 @@ def test_channel_probe_and_wall_forces_match_oracle(tmp_path, nz):
     D.close()
 
 
+@pytest.mark.parametrize("nz", [8, 2, 1])
+def test_channel_wall_traction_matches_oracle(tmp_path, nz):
+    path, ctx, ic = _channel(tmp_path, f"wt{nz}", nz)
+    D = S.DNS(ctx, 1)
+    D.restart(ic, 0.0)
+    D.advance(6)
+    got = D.wall_traction()
+    want = _oracle_on(D, path).wall_traction()
+    assert got.shape == want.shape == (3, ctx.nz, 2 * 4 * ctx.np)   # 4 wall edges top and bottom
+    for c in range(3):
+        scale = max(np.abs(want[c]).max(), 1e-300)
+        assert np.abs(got[c] - want[c]).max() <= 1e-11 * scale, c
+    assert np.abs(got[1]).max() > 1e-4
+    if nz == 1:
+        assert not got[2].any()
+    D.close()
+
+
 def test_taylor_green_probe_and_no_wall(tmp_path):
     path = sessions.taylor_green_session(str(tmp_path / "tg"), 3, 6, 8, re=100.0, dt=2e-3)
     ctx = S.Context(path)
@@ -111,7 +133,7 @@ def test_dns_program_writes_history_modal_and_flux_files(tmp_path):
     hist = [(1, 0.3, -0.95, 0.0), (2, 3.0, 0.5, 1.5), (7, 9.0, 0.0, 0.0)]   # the last is outside
     nstep = 6
     path, ctx, ic = _channel(tmp_path, "chf", 8, history=hist,
-                             extra={"N_STEP": nstep, "IO_HIS": 2, "IO_MDL": 3, "IO_FLD": nstep})
+                             extra={"N_STEP": nstep, "IO_HIS": 2, "IO_MDL": 3, "IO_FLD": nstep, "IO_WSS": 3})
     write_field(path + ".rst", "chf", ctx.np, ctx.nz, ctx.nel, 0, 0.0, 5e-3, 1.0 / 200.0, 1.0,
                 {**ic, "p": np.zeros_like(ic["u"])})
     r = subprocess.run([os.path.join(BIN, "dns"), path], capture_output=True, text=True, timeout=600)
@@ -120,10 +142,12 @@ def test_dns_program_writes_history_modal_and_flux_files(tmp_path):
     # the same run through the Python API, formatted as the reference formats
     D = S.DNS(ctx, 1)
     D.restart(ic, 0.0)
-    his, mdl, flx = [], [], []
+    his, mdl, flx, wss = [], [], [], []
     for step in range(1, nstep + 1):
         D.advance(1)
         t = D.state()[1]
+        if step % 3 == 0:
+            wss.append((step, D.wall_traction()))
         if step % 2 == 0 or step == nstep:
             vals = D.probe([h[1:] for h in hist[:2]])
             for (i, *_), v in zip(hist[:2], vals):
@@ -142,6 +166,24 @@ def test_dns_program_writes_history_modal_and_flux_files(tmp_path):
                 ["# DNS state information file", "# Step Time [Fpre Fvis Ftot]-axis",
                  "# -------------------------------"] + flx)
     assert len(his) == 2 * 3 and len(mdl) == 2 * 4 and len(flx) == 3
+    # session.wss: per output step a ten-line header and 3 x N_Z planes of
+    # the wall lines
+    raw = open(path + ".wss", "rb").read()
+    pos = 0
+    for step, want in wss:
+        hdr = []
+        for _ in range(10):
+            end = raw.index(b"\n", pos)
+            hdr.append(raw[pos:end].decode())
+            pos = end + 1
+        assert hdr[0].split()[0] == "chf" and hdr[8].split()[0] == "nts"
+        assert hdr[2].split()[:4] == [str(ctx.np), "1", str(ctx.nz), "8"]
+        assert int(hdr[3].split()[0]) == step and "binary IEEE" in hdr[9]
+        got = np.frombuffer(raw[pos:pos + want.nbytes], dtype=np.float64).reshape(want.shape)
+        pos += want.nbytes
+        for c in range(3):
+            assert np.abs(got[c] - want[c]).max() <= 1e-9 * max(np.abs(want[c]).max(), 1e-300)
+    assert pos == len(raw)
 
 
 def _same_lines(got, want):
