@@ -2024,6 +2024,8 @@ class DNS:
         names = list(self.P.S.fields)
         if level > 1:
             names += [chr(ord("A") + i) for i in range(self.ncom * (self.ncom + 1) // 2)]
+        if level > 2:      # energy-equation correlations (src/statistics.cpp:128-175)
+            names += list("qdmnortsabcGHIJKL" if self.ncom == 3 else "qdmnrsabGHI")
         shape = (self.P.nz, self.P.nel, self.P.np, self.P.np)
         self.avg = {c: np.zeros(shape) for c in sorted(names)}
         self.avg_level, self.navg = level, 0
@@ -2044,9 +2046,44 @@ class DNS:
                 i, j = pairs[k]
                 c = chr(ord("A") + k)
                 self.avg[c] = self.avg[c] + ph[i] * ph[j]
+        if self.avg_level > 2:
+            self._stats_energy(ph)
         for c in self.avg:
             self.avg[c] = smooth(self.P, self.vel[0], self.avg[c]) / (n + 1)
         self.navg += 1
+
+    def _stats_energy(self, ph):
+        """AVERAGE 3 (Statistics::update, src/statistics.cpp:247-391,
+        Cartesian): p u_i, q = |u|^2 / 2, q u_i, the rate-of-strain tensor
+        from gradients of the Fourier fields (then to physical space), S_ij
+        u_j and S_ij S_ij."""
+        P, nv, A = self.P, self.ncom, self.avg
+        pp = dft_inverse(self.u[self.pname])
+        for i, c in enumerate("mno"[:nv]):
+            A[c] = A[c] + pp * ph[i]
+        q = 0.5 * sum(ph[i] * ph[i] for i in range(nv))
+        A["q"] = A["q"] + q
+        for i, c in enumerate("rst"[:nv]):
+            A[c] = A[c] + ph[i] * q
+        off = {}
+        for i in range(nv):
+            for j in range(nv):
+                if j == i:
+                    continue
+                gij = plane_grad(P, self.u[self.vel[i]], j)
+                off[i + j - 1] = gij if j > i else off[i + j - 1] + gij
+        So = [dft_inverse(0.5 * off[k]) for k in range(nv * (nv - 1) // 2)]
+        Sd = [dft_inverse(plane_grad(P, self.u[self.vel[i]], i)) for i in range(nv)]
+        A["G"], A["H"], A["I"] = A["G"] + Sd[0], A["H"] + So[0], A["I"] + Sd[1]
+        A["a"] = A["a"] + Sd[0] * ph[0] + So[0] * ph[1]
+        A["b"] = A["b"] + So[0] * ph[0] + Sd[1] * ph[1]
+        A["d"] = A["d"] + Sd[0] ** 2 + 2 * So[0] ** 2 + Sd[1] ** 2
+        if nv == 3:
+            A["J"], A["K"], A["L"] = A["J"] + So[1], A["K"] + So[2], A["L"] + Sd[2]
+            A["a"] = A["a"] + So[1] * ph[2]
+            A["b"] = A["b"] + So[2] * ph[2]
+            A["c"] = A["c"] + So[1] * ph[0] + So[2] * ph[1] + Sd[2] * ph[2]
+            A["d"] = A["d"] + 2 * So[1] ** 2 + 2 * So[2] ** 2 + Sd[2] ** 2
 
     def stats_physical(self):
         out = {}

@@ -813,12 +813,20 @@ int stx_dns_create(stx_context* ctx, int advection, stx_dns** out) {
     }
     // -- running averages (Statistics::Statistics)
     d->avg_level = S.tokens.has("AVERAGE") ? S.tokens.ivalue("AVERAGE") : 0;
-    if (d->avg_level < 0 || d->avg_level > 2)
-      throw DnsError(STX_EUNSUPPORTED, "AVERAGE must be 0, 1 or 2 (energy-equation correlations are not built)");
+    if (d->avg_level < 0 || d->avg_level > 3) throw DnsError(STX_EINVAL, "AVERAGE token out of [0,3]");
     if (d->avg_level > 0) {
       std::string names = d->names;
       if (d->avg_level > 1)
         for (int i = 0; i < d->ncom * (d->ncom + 1) / 2; ++i) names.push_back(static_cast<char>('A' + i));
+      if (d->avg_level > 2) {
+        // energy-equation correlations (Statistics::Statistics,
+        // src/statistics.cpp:128-175): q, d; p u_i (m n o); q u_i (r s t);
+        // S_ij u_j (a b c); S_ij (G H I, J K L)
+        names += d->ncom == 3 ? "qdmnortsabcGHIJKL" : "qdmnrsabGHI";
+        // work fields: p and q in physical space, then the strain-rate
+        // components and a gradient
+        d->avg_work = static_cast<double*>(d->arena.alloc(sizeof(double) * d->fsize * 7));
+      }
       std::sort(names.begin(), names.end());
       d->avg_names = names;
       double* ab = static_cast<double*>(d->arena.alloc(sizeof(double) * d->fsize * names.size()));
@@ -1361,6 +1369,99 @@ double* avg_buffer(stx_dns* d, char name) {
   return d->avg_buf[k];
 }
 
+// The energy-equation correlations of AVERAGE 3 (Statistics::update,
+// src/statistics.cpp:247-391, Cartesian): with the velocities in physical
+// space in Up, add p u_i, q = |u|^2 / 2, q u_i, the rate-of-strain tensor
+// S_ij = (du_i/dx_j + du_j/dx_i) / 2 (gradients of the Fourier fields,
+// then to physical space), S_ij u_j and S_ij S_ij to the averages.
+void stats_energy(stx_dns* d) {
+  stx_context* ctx = d->ctx;
+  const DevGeom& g = ctx->dg;
+  cudaStream_t st = ctx->stream;
+  const int nv = d->ncom;
+  double* W[7];
+  for (int k = 0; k < 7; ++k) W[k] = d->avg_work + d->fsize * k;
+  auto add_product = [&](char name, const double* a, const double* b) {
+    ck(dns_product(g, a, b, d->tmp0, st), "product");
+    double* avg = avg_buffer(d, name);
+    combine2(d, avg, 1.0, avg, 1.0, d->tmp0);
+  };
+  auto add_field = [&](char name, const double* f) {
+    double* avg = avg_buffer(d, name);
+    combine2(d, avg, 1.0, avg, 1.0, f);
+  };
+  // -- pressure--velocity terms
+  double* P = W[0];
+  copy(d, P, d->u[d->ncom]);
+  transform(d, P, STX_INVERSE);
+  const char pu[3] = {'m', 'n', 'o'}, qu[3] = {'r', 's', 't'};
+  for (int i = 0; i < nv; ++i) add_product(pu[i], P, d->Up[i]);
+  // -- q and q u_i
+  double* Q = W[1];
+  ck(dns_product(g, d->Up[0], d->Up[0], Q, st), "product");
+  for (int i = 1; i < nv; ++i) {
+    ck(dns_product(g, d->Up[i], d->Up[i], d->tmp0, st), "product");
+    combine2(d, Q, 1.0, Q, 1.0, d->tmp0);
+  }
+  combine2(d, Q, 0.5, Q, 0.0, nullptr);
+  add_field('q', Q);
+  for (int i = 0; i < nv; ++i) add_product(qu[i], d->Up[i], Q);
+  // -- rate of strain: off-diagonal k = i + j - 1 (xy, xz, yz), diagonal
+  double* Sd[3] = {W[0], W[1], W[2]};
+  double* So[3] = {W[3], W[4], W[5]};
+  double* T = W[6];
+  auto grad = [&](int i, int j, double* out) {
+    if (j < 2) ck(dns_grad_xy(g, d->u[i], out, j, st), "gradient");
+    else ck(dns_grad_z(g, d->u[i], out, d->beta, st), "gradient");
+  };
+  for (int i = 0; i < nv; ++i)
+    for (int j = 0; j < nv; ++j) {
+      if (j == i) continue;
+      const int k = i + j - 1;
+      if (j > i) {
+        grad(i, j, So[k]);
+      } else {
+        grad(i, j, T);
+        combine2(d, So[k], 1.0, So[k], 1.0, T);
+      }
+    }
+  const int noff = nv * (nv - 1) / 2;
+  for (int k = 0; k < noff; ++k) combine2(d, So[k], 0.5, So[k], 0.0, nullptr);
+  for (int i = 0; i < nv; ++i) grad(i, i, Sd[i]);
+  for (int i = 0; i < nv; ++i) transform(d, Sd[i], STX_INVERSE);
+  for (int k = 0; k < noff; ++k) transform(d, So[k], STX_INVERSE);
+  add_field('G', Sd[0]);
+  add_field('H', So[0]);
+  add_field('I', Sd[1]);
+  if (nv == 3) {
+    add_field('J', So[1]);
+    add_field('K', So[2]);
+    add_field('L', Sd[2]);
+  }
+  // -- S_ij u_j
+  add_product('a', Sd[0], d->Up[0]);
+  add_product('a', So[0], d->Up[1]);
+  if (nv == 3) add_product('a', So[1], d->Up[2]);
+  add_product('b', So[0], d->Up[0]);
+  add_product('b', Sd[1], d->Up[1]);
+  if (nv == 3) add_product('b', So[2], d->Up[2]);
+  if (nv == 3) {
+    add_product('c', So[1], d->Up[0]);
+    add_product('c', So[2], d->Up[1]);
+    add_product('c', Sd[2], d->Up[2]);
+  }
+  // -- S_ij S_ij, the off-diagonal terms twice (scaled by sqrt 2)
+  for (int k = 0; k < noff; ++k) combine2(d, So[k], std::sqrt(2.0), So[k], 0.0, nullptr);
+  add_product('d', Sd[0], Sd[0]);
+  add_product('d', So[0], So[0]);
+  add_product('d', Sd[1], Sd[1]);
+  if (nv == 3) {
+    add_product('d', So[1], So[1]);
+    add_product('d', So[2], So[2]);
+    add_product('d', Sd[2], Sd[2]);
+  }
+}
+
 }  // namespace
 
 int stx_dns_stats_update(stx_dns* d) {
@@ -1390,6 +1491,7 @@ int stx_dns_stats_update(stx_dns* d) {
         combine2(d, b, 1.0, b, 1.0, d->tmp0);
       }
     }
+    if (d->avg_level > 2) stats_energy(d);
     const DevNumbering& Nm = ctx->fields.at(d->names[0]).dn;
     for (double* b : d->avg_buf) {
       ck(dns_smooth(ctx->dg, Nm, b, d->dsswork, ctx->stream), "smooth");

@@ -103,6 +103,7 @@ struct stx_dns {
   int navg = 0;
   std::string avg_names;
   std::vector<double*> avg_buf;
+  double* avg_work = nullptr;  // AVERAGE 3: seven work fields
   // Body forcing (<FORCE>; FieldForce and its classes, dns/fieldforce.cpp),
   // on the grid of the nonlinear products (nzl planes: N_Z, or 3 N_Z / 2
   // with DEALIAS).  Fields are device arrays of nzl planes, null when a term

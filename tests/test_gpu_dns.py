@@ -302,16 +302,17 @@ def test_high_order_elements(tmp_path):
     _compare(p, gpu, D)
 
 
-@pytest.mark.parametrize("nz", [8, 1])
-def test_running_statistics(tmp_path, nz):
+@pytest.mark.parametrize("nz,level", [(8, 2), (1, 2), (8, 3), (1, 3)])
+def test_running_statistics(tmp_path, nz, level):
     # Statistics (token AVERAGE = 2): running averages of u, v, (w,) p and
-    # the velocity products, updated every 3 steps, against the oracle.
+    # the velocity products, updated every 3 steps, against the oracle;
+    # AVERAGE = 3 adds the energy-equation correlations.
     if nz > 1:
         p = sessions.taylor_green_session(str(tmp_path / "tgs"), 3, 6, nz, re=100.0, dt=2e-3, nstep=12,
-                                          extra={"TOL_REL": 1e-14, "AVERAGE": 2})
+                                          extra={"TOL_REL": 1e-14, "AVERAGE": level})
     else:
         p = sessions.channel_session(str(tmp_path / "chs"), 4, 2, 6, 1, nstep=12,
-                                     extra={"TOL_REL": 1e-14, "AVERAGE": 2})
+                                     extra={"TOL_REL": 1e-14, "AVERAGE": level})
     ctx = S.Context(p)
     x, y = ctx.mesh_coords()
     if nz > 1:
@@ -322,7 +323,7 @@ def test_running_statistics(tmp_path, nz):
     D = S.DNS(ctx, 1)
     D.restart(ic, 0.0)
     Do = O.DNS(O.Problem(O.read_session(p)), ic)
-    Do.stats_init(2)
+    Do.stats_init(level)
     for _ in range(4):
         D.advance(3)
         D.stats_update()
@@ -335,8 +336,10 @@ def test_running_statistics(tmp_path, nz):
     assert n == 4 and sorted(avg) == sorted(ref)
     for c in ref:
         scale = max(np.linalg.norm(ref[c]), 1e-300)
-        tol = 1e-9 if c == "p" else 1e-10
+        tol = 1e-9 if c in "pmno" else 1e-10   # the pressure and its products
         assert np.linalg.norm(avg[c] - ref[c]) / scale < tol, (c, np.linalg.norm(avg[c] - ref[c]) / scale)
+    if level == 3:
+        assert len(ref) == (4 + 6 + 17 if nz > 1 else 3 + 3 + 11)
 
 
 @pytest.mark.parametrize("nz", [1, 4])
