@@ -111,6 +111,15 @@ int stx_mesh_locate(const stx_context* ctx, int npts, const double* xy, int* h_e
 /* The same from a session file, without a context or device. */
 int stx_mesh_locate_host(const char* session_path, const char* overrides, int npts, const double* xy, int* h_elmt,
                          double* h_rs);
+/* Relocate moved points (FluidParticle::integrate's search,
+ * src/particle.cpp:155-175): for each point, Newton's iteration in its
+ * element h_elmt[i] from its previous (r, s) in h_rs (Element::locate
+ * without a guess); when that fails, or h_elmt[i] < 0, the search of
+ * stx_mesh_locate.  h_elmt and h_rs are updated (-1 outside the mesh).
+ * Host work. */
+int stx_mesh_relocate(const stx_context* ctx, int npts, const double* xy, int* h_elmt, double* h_rs);
+int stx_mesh_relocate_host(const char* session_path, const char* overrides, int npts, const double* xy,
+                           int* h_elmt, double* h_rs);
 /* Number of geometry families (elements sharing condensed matrices). */
 int stx_mesh_families(const stx_context* ctx, int* nfamily);
 

@@ -797,41 +797,129 @@ def lagrange_interpolants(z, x):
     return h, dh
 
 
-def locate(M: Mesh, x: float, y: float, tol: float = 1e-5, maxit: int = 20):
-    """HistoryPoint::locate (src/history.cpp:45-63) over Element::locate
-    (src/element.cpp:1061-1183): (element, r, s) of the first element where
-    Newton's iteration from the nearest node converges inside, else None."""
+def element_locate(M: Mesh, e: int, x: float, y: float, r: float = 0.0, s: float = 0.0, guess: bool = True,
+                   tol: float = 1e-5, maxit: int = 20):
+    """Element::locate (src/element.cpp:1061-1183) in element e: (r, s) of
+    (x, y) by Newton's iteration from the nearest element node (guess) or
+    from the given (r, s); None when it does not converge inside."""
     n = M.np
-    for e in range(M.nel):
-        X, Y = M.x[e].ravel(), M.y[e].ravel()
+    X, Y = M.x[e].ravel(), M.y[e].ravel()
+    if guess:
         diag = max(math.hypot(X[-1] - X[0], Y[-1] - Y[0]),
                    math.hypot(X[n * (n - 1)] - X[n - 1], Y[n * (n - 1)] - Y[n - 1]))
         d2 = (x - X) ** 2 + (y - Y) ** 2
         i = int(np.argmin(d2))
         if d2[i] - diag * diag > 0.0:
-            continue
+            return None
         r, s = M.z[i % n], M.z[i // n]
-        Xm, Ym = M.x[e], M.y[e]
-        it, ok = 0, True
-        while True:
-            ir, dr = lagrange_interpolants(M.z, r)
-            is_, ds = lagrange_interpolants(M.z, s)
-            F0 = x - is_ @ Xm @ ir
-            F1 = y - is_ @ Ym @ ir
-            J = [dr @ Xm.T @ is_, dr @ Ym.T @ is_, ds @ Xm @ ir, ds @ Ym @ ir]
-            det = J[0] * J[3] - J[1] * J[2]
-            idet = 1.0 / EPSDP if abs(det) < EPSDP else 1.0 / det
-            r += (F0 * J[3] - F1 * J[2]) * idet
-            s += (F1 * J[0] - F0 * J[1]) * idet
-            if abs(r) > 20.0 and abs(s) > 20.0:
-                ok = False
-                break
-            it += 1
-            if not (it < maxit and (abs(F0) > tol or abs(F1) > tol)):
-                break
-        if ok and it < maxit and abs(r) < 1.0 + tol and abs(s) < 1.0 + tol:
-            return e, r, s
+    Xm, Ym = M.x[e], M.y[e]
+    it = 0
+    while True:
+        ir, dr = lagrange_interpolants(M.z, r)
+        is_, ds = lagrange_interpolants(M.z, s)
+        F0 = x - is_ @ Xm @ ir
+        F1 = y - is_ @ Ym @ ir
+        J = [dr @ Xm.T @ is_, dr @ Ym.T @ is_, ds @ Xm @ ir, ds @ Ym @ ir]
+        det = J[0] * J[3] - J[1] * J[2]
+        idet = 1.0 / EPSDP if abs(det) < EPSDP else 1.0 / det
+        r += (F0 * J[3] - F1 * J[2]) * idet
+        s += (F1 * J[0] - F0 * J[1]) * idet
+        if abs(r) > 20.0 and abs(s) > 20.0:
+            return None
+        it += 1
+        if not (it < maxit and (abs(F0) > tol or abs(F1) > tol)):
+            break
+    if it < maxit and abs(r) < 1.0 + tol and abs(s) < 1.0 + tol:
+        return r, s
     return None
+
+
+def locate(M: Mesh, x: float, y: float, tol: float = 1e-5, maxit: int = 20):
+    """HistoryPoint::locate (src/history.cpp:45-63) over Element::locate:
+    (element, r, s) of the first element where Newton's iteration from the
+    nearest node converges inside, else None."""
+    for e in range(M.nel):
+        rs = element_locate(M, e, x, y, guess=True, tol=tol, maxit=maxit)
+        if rs is not None:
+            return e, rs[0], rs[1]
+    return None
+
+
+def relocate(M: Mesh, x: float, y: float, e: int, r: float, s: float, tol: float = 1e-5, maxit: int = 20):
+    """FluidParticle::integrate's search (src/particle.cpp:155-175): Newton
+    in element e from (r, s), else the full search; None outside."""
+    if e is not None and e >= 0:
+        rs = element_locate(M, e, x, y, r, s, guess=False, tol=tol, maxit=maxit)
+        if rs is not None:
+            return e, rs[0], rs[1]
+    return locate(M, x, y, tol, maxit)
+
+
+class FluidParticles:
+    """Massless particles (FluidParticle, src/particle.cpp:37-281, and the
+    Analyser's handling, src/analysis.cpp:63-104, 206-226, 252-272): made
+    where located, moved by an Adams-Bashforth predictor and Adams-Moulton
+    corrector (Integration::AdamsBashforth / AdamsMoulton,
+    src/integration.cpp:37-96) of order min(steps, N_TIME) on velocities from
+    `probe(e, r, s, z) -> (u, v, w)`, relocated from their element (else a
+    full search); those that leave stop.  z wraps into one period in 3D."""
+
+    AB = {1: [1.0], 2: [1.5, -0.5], 3: [23 / 12, -16 / 12, 5 / 12]}
+    AM = {2: [0.5, 0.5], 3: [5 / 12, 8 / 12, -1 / 12], 4: [9 / 24, 19 / 24, -5 / 24, 1 / 24]}
+
+    def __init__(self, M: Mesh, tok, nfields: int):
+        self.M = M
+        self.ncom = 3 if nfields > 3 else 2
+        self.dt, self.tord = tok["D_T"], tok.ivalue("N_TIME")
+        self.lz = 2 * math.pi / tok["BETA"]
+        self.tol, self.maxit = tok["TOL_POS"], tok.ivalue("NR_MAX")
+        self.parts, self.initial = [], []
+
+    def _wrap(self, z):
+        return self.lz - math.fmod(abs(z), self.lz) if z < 0 else math.fmod(z, self.lz)
+
+    def make(self, pid, p, t):
+        loc = locate(self.M, p[0], p[1], self.tol, self.maxit)
+        if loc is None:
+            return False
+        z = 0.0 if self.ncom == 2 else self._wrap(p[2])
+        self.parts.append(dict(id=pid, ctime=t, x=p[0], y=p[1], z=z, e=loc[0], r=loc[1], s=loc[2], step=0,
+                               u=[0.0] * self.tord, v=[0.0] * self.tord, w=[0.0] * self.tord))
+        return True
+
+    def _move(self, q, x, y):
+        loc = relocate(self.M, x, y, q["e"], q["r"], q["s"], self.tol, self.maxit)
+        if loc is None:
+            q["e"] = None
+            return False
+        q["e"], q["r"], q["s"] = loc
+        return True
+
+    def integrate(self, probe):
+        for q in self.parts:
+            if q["e"] is None:
+                continue
+            q["step"] += 1
+            N = min(q["step"], self.tord)
+            pred = [self.dt * c for c in self.AB[N]]
+            corr = [self.dt * c for c in self.AM[N + 1]]
+            q["u"][0], q["v"][0], q["w"][0] = probe(q["e"], q["r"], q["s"], q["z"])
+            xp = q["x"] + sum(pred[i] * q["u"][i] for i in range(N))
+            yp = q["y"] + sum(pred[i] * q["v"][i] for i in range(N))
+            zp = q["z"] + (sum(pred[i] * q["w"][i] for i in range(N)) if self.ncom == 3 else 0.0)
+            if not self._move(q, xp, yp):
+                continue
+            up, vp, wp = probe(q["e"], q["r"], q["s"], zp)
+            q["x"] += corr[0] * up + sum(corr[i] * q["u"][i - 1] for i in range(1, N + 1))
+            q["y"] += corr[0] * vp + sum(corr[i] * q["v"][i - 1] for i in range(1, N + 1))
+            if self.ncom == 3:
+                q["z"] += corr[0] * wp + sum(corr[i] * q["w"][i - 1] for i in range(1, N + 1))
+            if not self._move(q, q["x"], q["y"]):
+                continue
+            if self.ncom == 3:
+                q["z"] = self._wrap(q["z"])
+            for c in "uvw":
+                q[c] = [q[c][-1]] + q[c][:-1]
 
 
 def grad(M: Mesh, u, direction):

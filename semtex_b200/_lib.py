@@ -41,6 +41,8 @@ SIGNATURES = {
     "stx_mesh_mass": (_i, [_p, _p]),
     "stx_mesh_locate": (_i, [_p, _i, _p, _p, _p]),
     "stx_mesh_locate_host": (_i, [_s, _s, _i, _p, _p, _p]),
+    "stx_mesh_relocate": (_i, [_p, _i, _p, _p, _p]),
+    "stx_mesh_relocate_host": (_i, [_s, _s, _i, _p, _p, _p]),
     "stx_field_evaluate": (_i, [_p, _s, _d, _p]),
     "stx_expression_eval": (_i, [_s, _s, _i, _i, _p, _p, _p, _d, _p, _pi]),
     "stx_svv": (_i, [_i, _d, _i, _i, _d, _i, _d, _p, _p]),

@@ -459,7 +459,44 @@ void locate_points(const Session& S, const Mesh& M, int npts, const double* xy, 
   }
 }
 
+// FluidParticle::integrate's search (src/particle.cpp:155-175): Newton's
+// iteration in the point's element from its (r, s), else the full search.
+void relocate_points(const Session& S, const Mesh& M, int npts, const double* xy, int* h_elmt, double* h_rs) {
+  if (npts < 0 || (npts > 0 && (!xy || !h_elmt || !h_rs))) throw StxError(STX_EINVAL, "null argument");
+  const double tol = S.tokens.value("TOL_POS");
+  const int maxit = S.tokens.ivalue("NR_MAX");
+  for (int i = 0; i < npts; ++i) {
+    const int e = h_elmt[i];
+    if (e >= M.nel) throw StxError(STX_EINVAL, "element out of range");
+    double r = h_rs[2 * i], s = h_rs[2 * i + 1];
+    if (e >= 0 && element_locate(M, e, xy[2 * i], xy[2 * i + 1], tol, maxit, false, r, s)) {
+      h_rs[2 * i] = r;
+      h_rs[2 * i + 1] = s;
+      continue;
+    }
+    h_elmt[i] = locate_point(M, xy[2 * i], xy[2 * i + 1], tol, maxit, r, s);
+    h_rs[2 * i] = h_elmt[i] >= 0 ? r : 0.0;
+    h_rs[2 * i + 1] = h_elmt[i] >= 0 ? s : 0.0;
+  }
+}
+
 }  // namespace
+
+int stx_mesh_relocate(const stx_context* ctx, int npts, const double* xy, int* h_elmt, double* h_rs) {
+  return guarded([&] {
+    if (!ctx) throw StxError(STX_EINVAL, "null context");
+    relocate_points(ctx->S, ctx->M, npts, xy, h_elmt, h_rs);
+  });
+}
+
+int stx_mesh_relocate_host(const char* session_path, const char* overrides, int npts, const double* xy,
+                           int* h_elmt, double* h_rs) {
+  return guarded([&] {
+    if (!session_path) throw StxError(STX_EINVAL, "null argument");
+    const Session S = read_session(session_path, overrides ? overrides : "");
+    relocate_points(S, build_mesh(S), npts, xy, h_elmt, h_rs);
+  });
+}
 
 int stx_mesh_locate(const stx_context* ctx, int npts, const double* xy, int* h_elmt, double* h_rs) {
   return guarded([&] {

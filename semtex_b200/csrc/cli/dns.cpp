@@ -20,7 +20,11 @@
 // "wall" group, every IO_WSS and IO_FLD steps and at the end the wall
 // tractions are appended to session.wss (a header like a field file's, then
 // the normal, in-plane and out-of-plane tractions, N_Z planes each,
-// dns/dnsanalysis.cpp:130-250).
+// dns/dnsanalysis.cpp:130-250).  Particles listed in session.par are tracked
+// every step (FluidParticle, src/particle.cpp; new ones at the listed places
+// every SPAWN steps) and written to session.trk with the history points.
+#include <algorithm>
+#include <array>
 #include <cmath>
 #include <cstdio>
 #include <cstring>
@@ -58,6 +62,151 @@ double token(const stx_context* ctx, const char* name) {
   check(stx_token(ctx, name, &v), name);
   return v;
 }
+
+// Massless fluid particles (FluidParticle, src/particle.cpp:37-281, and the
+// Analyser's handling of them, src/analysis.cpp:63-104, 206-226, 252-272):
+// located in the mesh when made, moved every step by an Adams-Bashforth
+// predictor and Adams-Moulton corrector of order min(steps, N_TIME) on the
+// velocities probed on the device, relocated from their element (else by a
+// full search); a particle that leaves the mesh stops.  z wraps into one
+// period in 3D.
+struct Particles {
+  struct P {
+    int id = 0, elmt = -1, step = 0;
+    double ctime = 0.0, x = 0.0, y = 0.0, z = 0.0, r = 0.0, s = 0.0;
+    std::vector<double> u, v, w;  // velocity levels, newest first
+  };
+  std::vector<P> all;
+  std::vector<std::array<double, 3>> initial;  // places new particles start from
+  int ncom = 2, tord = 1, nf = 1;
+  double dt = 0.0, lz = 0.0;
+
+  void setup(const stx_context* ctx, int nfields) {
+    ncom = nfields > 3 ? 3 : 2;
+    nf = nfields;
+    tord = static_cast<int>(std::lround(token(ctx, "N_TIME")));
+    dt = token(ctx, "D_T");
+    lz = 2.0 * M_PI / token(ctx, "BETA");
+  }
+  double wrap(double z) const { return z < 0.0 ? lz - std::fmod(std::fabs(z), lz) : std::fmod(z, lz); }
+  // FluidParticle::FluidParticle: false when the place is not in the mesh
+  bool make(const stx_context* ctx, int id, const std::array<double, 3>& p, double t) {
+    P q;
+    q.id = id;
+    q.ctime = t;
+    q.x = p[0];
+    q.y = p[1];
+    double rs[2];
+    check(stx_mesh_locate(ctx, 1, p.data(), &q.elmt, rs), "particle");
+    if (q.elmt < 0) return false;
+    q.r = rs[0];
+    q.s = rs[1];
+    q.z = ncom == 2 ? 0.0 : wrap(p[2]);
+    q.u.assign(tord, 0.0);
+    q.v.assign(tord, 0.0);
+    q.w.assign(tord, 0.0);
+    all.push_back(q);
+    return true;
+  }
+  // velocities of the listed particles at (elmt, r, s, z)
+  void probe(stx_dns* dns, const std::vector<int>& ix, const std::vector<double>& zs, std::vector<double>& vel) {
+    const int n = static_cast<int>(ix.size());
+    std::vector<int> el(n);
+    std::vector<double> rs(2 * n), out(static_cast<size_t>(n) * nf);
+    for (int k = 0; k < n; ++k) {
+      el[k] = all[ix[k]].elmt;
+      rs[2 * k] = all[ix[k]].r;
+      rs[2 * k + 1] = all[ix[k]].s;
+    }
+    check(stx_dns_probe(dns, n, el.data(), rs.data(), zs.data(), out.data()), "particle");
+    vel.assign(static_cast<size_t>(n) * 3, 0.0);
+    for (int k = 0; k < n; ++k)
+      for (int c = 0; c < ncom; ++c) vel[3 * k + c] = out[static_cast<size_t>(k) * nf + c];
+  }
+  void relocate(const stx_context* ctx, const std::vector<int>& ix, const std::vector<double>& xy) {
+    const int n = static_cast<int>(ix.size());
+    std::vector<int> el(n);
+    std::vector<double> rs(2 * n);
+    for (int k = 0; k < n; ++k) {
+      el[k] = all[ix[k]].elmt;
+      rs[2 * k] = all[ix[k]].r;
+      rs[2 * k + 1] = all[ix[k]].s;
+    }
+    check(stx_mesh_relocate(ctx, n, xy.data(), el.data(), rs.data()), "particle");
+    for (int k = 0; k < n; ++k) {
+      all[ix[k]].elmt = el[k];
+      all[ix[k]].r = rs[2 * k];
+      all[ix[k]].s = rs[2 * k + 1];
+    }
+  }
+  // FluidParticle::integrate for every particle still in the mesh
+  void integrate(const stx_context* ctx, stx_dns* dns) {
+    static const double kAB[3][3] = {{1.0, 0.0, 0.0}, {1.5, -0.5, 0.0}, {23.0 / 12.0, -16.0 / 12.0, 5.0 / 12.0}};
+    static const double kAM[3][4] = {
+        {0.5, 0.5, 0.0, 0.0}, {5.0 / 12.0, 8.0 / 12.0, -1.0 / 12.0, 0.0},
+        {9.0 / 24.0, 19.0 / 24.0, -5.0 / 24.0, 1.0 / 24.0}};  // Integration::AdamsMoulton orders 2..4
+    std::vector<int> ix;
+    for (size_t k = 0; k < all.size(); ++k)
+      if (all[k].elmt >= 0) ix.push_back(static_cast<int>(k));
+    if (ix.empty()) return;
+    const int n = static_cast<int>(ix.size());
+    std::vector<double> zs(n), vel, xy(2 * n), zp(n);
+    for (int k = 0; k < n; ++k) zs[k] = all[ix[k]].z;
+    probe(dns, ix, zs, vel);  // predictor: the velocities where the particles are
+    for (int k = 0; k < n; ++k) {
+      P& q = all[ix[k]];
+      const int N = std::min(++q.step, tord);
+      q.u[0] = vel[3 * k];
+      q.v[0] = vel[3 * k + 1];
+      q.w[0] = vel[3 * k + 2];
+      double x = q.x, y = q.y, z = q.z;
+      for (int i = 0; i < N; ++i) {
+        const double c = dt * kAB[N - 1][i];
+        x += c * q.u[i];
+        y += c * q.v[i];
+        if (ncom == 3) z += c * q.w[i];
+      }
+      xy[2 * k] = x;
+      xy[2 * k + 1] = y;
+      zp[k] = z;
+    }
+    relocate(ctx, ix, xy);
+    std::vector<int> in;  // still in the mesh
+    std::vector<double> zin;
+    for (int k = 0; k < n; ++k)
+      if (all[ix[k]].elmt >= 0) {
+        in.push_back(ix[k]);
+        zin.push_back(zp[k]);
+      }
+    if (in.empty()) return;
+    probe(dns, in, zin, vel);  // corrector: the velocities at the predicted places
+    std::vector<double> xy2(2 * in.size());
+    for (size_t k = 0; k < in.size(); ++k) {
+      P& q = all[in[k]];
+      const int N = std::min(q.step, tord);
+      const double* c = kAM[N - 1];
+      q.x += dt * c[0] * vel[3 * k];
+      q.y += dt * c[0] * vel[3 * k + 1];
+      if (ncom == 3) q.z += dt * c[0] * vel[3 * k + 2];
+      for (int i = 1; i < N + 1; ++i) {
+        q.x += dt * c[i] * q.u[i - 1];
+        q.y += dt * c[i] * q.v[i - 1];
+        if (ncom == 3) q.z += dt * c[i] * q.w[i - 1];
+      }
+      xy2[2 * k] = q.x;
+      xy2[2 * k + 1] = q.y;
+    }
+    relocate(ctx, in, xy2);
+    for (int k : in) {
+      P& q = all[k];
+      if (q.elmt >= 0 && ncom == 3) q.z = wrap(q.z);
+      // rollv: every level one older, the oldest slot reused for the next
+      std::rotate(q.u.rbegin(), q.u.rbegin() + 1, q.u.rend());
+      std::rotate(q.v.rbegin(), q.v.rbegin() + 1, q.v.rend());
+      std::rotate(q.w.rbegin(), q.w.rbegin() + 1, q.w.rend());
+    }
+  }
+};
 
 }  // namespace
 
@@ -159,6 +308,36 @@ int main(int argc, char** argv) {
       his_z.push_back(h.z);
     }
   }
+  // particles (Analyser::Analyser, src/analysis.cpp:63-104): session.par
+  // lines "id time ctime x y z", placed as given (shifted and scaled)
+  Particles parts;
+  std::ofstream trk;
+  const int spawn = static_cast<int>(std::lround(token(ctx, "SPAWN")));
+  {
+    std::ifstream pf(session + ".par");
+    if (pf) {
+      parts.setup(ctx, static_cast<int>(fields.size()));
+      const double xs = token(ctx, "X_SHIFT"), ys = token(ctx, "Y_SHIFT");
+      const double xc = token(ctx, "X_SCALE"), yc = token(ctx, "Y_SCALE");
+      double t0 = 0.0;
+      check(stx_dns_state(dns, nullptr, &t0), "state");
+      trk.open(session + ".trk");
+      if (!trk) fail("can't open particle track file");
+      trk.setf(std::ios::scientific, std::ios::floatfield);
+      trk.precision(6);
+      int id, i = 0;
+      double tm, ct;
+      std::array<double, 3> p;
+      while (pf >> id >> tm >> ct >> p[0] >> p[1] >> p[2]) {
+        p[0] = (p[0] + xs) * xc;
+        p[1] = (p[1] + ys) * yc;
+        if (!parts.make(ctx, ++i, p, t0))
+          std::fprintf(stderr, "Analyser::Analyser: Particle at (%f, %f, %f) not in mesh\n", p[0], p[1], p[2]);
+        else if (spawn)
+          parts.initial.push_back(p);
+      }
+    }
+  }
   std::ofstream his, mdl;
   if (!his_id.empty()) {
     his.open(session + ".his");
@@ -209,6 +388,7 @@ int main(int argc, char** argv) {
     next = std::min(next, (step / io_his + 1) * io_his);
     if (io_mdl > 0) next = std::min(next, (step / io_mdl + 1) * io_mdl);
     if (wss.is_open()) next = std::min(next, (step / io_wss + 1) * io_wss);
+    if (trk.is_open()) next = step + 1;  // particles move every step
     if (verbose) {  // the step line of DNSAnalyser::analyse, one step at a time
       for (; step < next; ++step) {
         check(stx_dns_advance(dns, 1), "integrate");
@@ -222,6 +402,13 @@ int main(int argc, char** argv) {
     }
     double time;
     check(stx_dns_state(dns, nullptr, &time), "state");
+    if (trk.is_open()) {  // Analyser::analyse: new particles, then every particle moves
+      if (spawn && step % spawn == 0) {
+        int i = 0;
+        for (const auto& p : parts.initial) parts.make(ctx, ++i, p, time);
+      }
+      parts.integrate(ctx, dns);
+    }
     if (io_cfl > 0 && step % io_cfl == 0) {
       double inv = 0.0, div = 0.0;
       check(stx_dns_cfl(dns, &inv), "CFL");
@@ -234,6 +421,10 @@ int main(int argc, char** argv) {
     // -- history points and wall forces at IO_HIS / IO_FLD steps and at
     //    the end (Analyser::analyse, DNSAnalyser::analyse)
     if (step % io_his == 0 || step % io_fld == 0 || step == nstep) {
+      for (const auto& q : parts.all)
+        if (q.elmt >= 0)
+          trk << std::setw(6) << q.id << std::setw(14) << time << std::setw(14) << q.ctime << std::setw(14) << q.x
+              << std::setw(14) << q.y << std::setw(14) << q.z << std::endl;
       if (!his_id.empty()) {
         const int nf = static_cast<int>(fields.size());
         check(stx_dns_probe(dns, static_cast<int>(his_id.size()), his_el.data(), his_rs.data(), his_z.data(),

@@ -880,13 +880,14 @@ void gll_interpolants(const Quadrature& q, double x, double* h, double* dh) {
   }
 }
 
-int locate_point(const Mesh& M, double x, double y, double tol, int maxit, double& r, double& s) {
+bool element_locate(const Mesh& M, int e, double x, double y, double tol, int maxit, bool guess, double& r,
+                    double& s) {
   const int np = M.np, nn = M.npnp;
   const double kDiverge = 20.0;
   std::vector<double> ir(np), is(np), dr(np), ds(np), tp(np);
-  for (int e = 0; e < M.nel; ++e) {
-    const double* X = M.x.data() + static_cast<size_t>(e) * nn;
-    const double* Y = M.y.data() + static_cast<size_t>(e) * nn;
+  const double* X = M.x.data() + static_cast<size_t>(e) * nn;
+  const double* Y = M.y.data() + static_cast<size_t>(e) * nn;
+  if (guess) {
     // initial guess: the element node nearest (x, y), if within the
     // element's longer diagonal
     const double diag = std::max(std::hypot(X[nn - 1] - X[0], Y[nn - 1] - Y[0]),
@@ -901,40 +902,43 @@ int locate_point(const Mesh& M, double x, double y, double tol, int maxit, doubl
         best = t;
       }
     }
-    if (dmin - diag * diag > 0.0) continue;
+    if (dmin - diag * diag > 0.0) return false;
     r = M.q.z[best % np];
     s = M.q.z[best / np];
-    int it = 0;
-    double F0, F1;
-    bool diverged = false;
-    do {
-      gll_interpolants(M.q, r, ir.data(), dr.data());
-      gll_interpolants(M.q, s, is.data(), ds.data());
-      // x(r, s) = is^T X ir and its partials
-      auto form = [&](const double* A, const double* w, const double* v) {
-        for (int i = 0; i < np; ++i) {
-          double a = 0.0;
-          for (int j = 0; j < np; ++j) a += A[i * np + j] * w[j];
-          tp[i] = a;
-        }
+  }
+  int it = 0;
+  double F0, F1;
+  do {
+    gll_interpolants(M.q, r, ir.data(), dr.data());
+    gll_interpolants(M.q, s, is.data(), ds.data());
+    // x(r, s) = is^T X ir and its partials
+    auto form = [&](const double* A, const double* w, const double* v) {
+      for (int i = 0; i < np; ++i) {
         double a = 0.0;
-        for (int i = 0; i < np; ++i) a += v[i] * tp[i];
-        return a;
-      };
-      F0 = x - form(X, ir.data(), is.data());
-      F1 = y - form(Y, ir.data(), is.data());
-      const double J2 = form(X, ir.data(), ds.data()), J3 = form(Y, ir.data(), ds.data());
-      const double J0 = form(X, dr.data(), is.data()), J1 = form(Y, dr.data(), is.data());
-      double idet = J0 * J3 - J1 * J2;
-      idet = std::fabs(idet) < kEpsDP ? 1.0 / kEpsDP : 1.0 / idet;
-      r += (F0 * J3 - F1 * J2) * idet;
-      s += (F1 * J0 - F0 * J1) * idet;
-      if (std::fabs(r) > kDiverge && std::fabs(s) > kDiverge) {
-        diverged = true;
-        break;
+        for (int j = 0; j < np; ++j) a += A[i * np + j] * w[j];
+        tp[i] = a;
       }
-    } while (++it < maxit && (std::fabs(F0) > tol || std::fabs(F1) > tol));
-    if (!diverged && it < maxit && std::fabs(r) < 1.0 + tol && std::fabs(s) < 1.0 + tol) return e;
+      double a = 0.0;
+      for (int i = 0; i < np; ++i) a += v[i] * tp[i];
+      return a;
+    };
+    F0 = x - form(X, ir.data(), is.data());
+    F1 = y - form(Y, ir.data(), is.data());
+    const double J2 = form(X, ir.data(), ds.data()), J3 = form(Y, ir.data(), ds.data());
+    const double J0 = form(X, dr.data(), is.data()), J1 = form(Y, dr.data(), is.data());
+    double idet = J0 * J3 - J1 * J2;
+    idet = std::fabs(idet) < kEpsDP ? 1.0 / kEpsDP : 1.0 / idet;
+    r += (F0 * J3 - F1 * J2) * idet;
+    s += (F1 * J0 - F0 * J1) * idet;
+    if (std::fabs(r) > kDiverge && std::fabs(s) > kDiverge) return false;
+  } while (++it < maxit && (std::fabs(F0) > tol || std::fabs(F1) > tol));
+  return it < maxit && std::fabs(r) < 1.0 + tol && std::fabs(s) < 1.0 + tol;
+}
+
+int locate_point(const Mesh& M, double x, double y, double tol, int maxit, double& r, double& s) {
+  for (int e = 0; e < M.nel; ++e) {
+    r = s = 0.0;
+    if (element_locate(M, e, x, y, tol, maxit, true, r, s)) return e;
   }
   return -1;
 }

@@ -67,6 +67,14 @@ Mesh build_mesh(const Session& S);
 // either output may be null.
 void gll_interpolants(const Quadrature& q, double x, double* h, double* dh);
 
+// Element::locate (src/element.cpp:1061-1183) in element e: Newton's
+// iteration for (r, s) with x(r, s) = (x, y), from the element node nearest
+// the point (guess; false when the point is farther than the element's
+// longer diagonal) or from the given (r, s); true when it converges
+// (|F| <= tol within maxit steps) to |r|, |s| < 1 + tol.
+bool element_locate(const Mesh& M, int e, double x, double y, double tol, int maxit, bool guess, double& r,
+                    double& s);
+
 // HistoryPoint::locate (src/history.cpp:45-63) with Element::locate
 // (src/element.cpp:1061-1183): the first element, in order, where Newton's
 // iteration from the nearest element node converges (|F| <= tol within

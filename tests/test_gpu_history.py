@@ -11,6 +11,10 @@ session.flx and session.wss).
 - Wall tractions (Field::traction, src/field.cpp:533-593) against the
   oracle on the channel with 8, 2 and 1 planes: every mode's normal,
   in-plane and out-of-plane traction, then the inverse z transform.
+- The `dns` program's particle tracks (session.par in, session.trk out,
+  FluidParticle, src/particle.cpp) against the oracle's particle integrator
+  moving on the device DNS's own fields, step by step, with new particles
+  every SPAWN steps.
 - The `dns` program's files against the same values through the Python
   API, line for line in the reference's formats (src/analysis.cpp:275-375,
   dns/dnsanalysis.cpp:44-127).
@@ -205,3 +209,64 @@ def _same_lines(got, want):
                 assert a == b
             else:
                 assert abs(float(a) - float(b)) <= 2e-6 * abs(float(b)) + 1e-12 * scale, (g, w)
+
+
+def _probe_at(F, M, e, r, s, z, beta):
+    """Physical velocity of Fourier fields F [ncom][nz, nel, np, np] at
+    (element e, r, s, z) (AuxField::probe)."""
+    ir, _ = O.lagrange_interpolants(M.z, r)
+    is_, _ = O.lagrange_interpolants(M.z, s)
+    out = []
+    for f in F:
+        vals = np.array([is_ @ f[k, e] @ ir for k in range(f.shape[0])])
+        if f.shape[0] < 3:
+            out.append(vals[0])
+            continue
+        nzh, bz = f.shape[0] // 2, z * beta
+        v = vals[0] + vals[1] * np.cos(nzh * bz)
+        for k in range(1, nzh):
+            v += 2 * vals[2 * k] * np.cos(k * bz) - 2 * vals[2 * k + 1] * np.sin(k * bz)
+        out.append(v)
+    return out + [0.0] * (3 - len(out))
+
+
+def test_dns_program_tracks_particles(tmp_path):
+    nstep = 6
+    path, ctx, ic = _channel(tmp_path, "chp", 8, extra={"N_STEP": nstep, "IO_HIS": 2, "IO_FLD": nstep,
+                                                       "SPAWN": 3, "D_T": 0.05})
+    write_field(path + ".rst", "chp", ctx.np, ctx.nz, ctx.nel, 0, 0.0, 0.05, 1.0 / 200.0, 1.0,
+                {**ic, "p": np.zeros_like(ic["u"])})
+    places = [(0.4, -0.5, 0.3), (3.0, 0.2, 6.0), (5.8, 0.9, -1.0), (9.0, 0.0, 0.0)]   # the last is outside
+    with open(path + ".par", "w") as f:
+        for i, (x, y, z) in enumerate(places):
+            f.write(f"{i + 1} 0.0 0.0 {x} {y} {z}\n")
+    r = subprocess.run([os.path.join(BIN, "dns"), path], capture_output=True, text=True, timeout=600)
+    assert r.returncode == 0, r.stderr
+    assert "Particle at (9.000000, 0.000000, 0.000000) not in mesh" in r.stderr
+    # the same particles on the device DNS's fields, through the oracle
+    Sn = O.read_session(path)
+    M = O.Problem(Sn).M
+    T = O.FluidParticles(M, Sn.tokens, 4)
+    for i, pl in enumerate(places):
+        if T.make(i + 1, pl, 0.0):
+            T.initial.append(pl)
+    D = S.DNS(ctx, 1)
+    D.restart(ic, 0.0)
+    want = []
+    for step in range(1, nstep + 1):
+        D.advance(1)
+        t = D.state()[1]
+        if step % 3 == 0:
+            for i, pl in enumerate(T.initial):
+                T.make(i + 1, pl, t)
+        F = [_fourier(D, c) for c in "uvw"]
+        T.integrate(lambda e, r_, s_, z: _probe_at(F, M, e, r_, s_, z, 1.0))
+        if step % 2 == 0:
+            want += [(q["id"], t, q["ctime"], q["x"], q["y"], q["z"]) for q in T.parts if q["e"] is not None]
+    D.close()
+    got = [ln.split() for ln in open(path + ".trk").read().splitlines()]
+    assert len(got) == len(want) == 3 + 6 + 9   # three particles, three more every 3 steps
+    for g, w in zip(got, want):
+        assert int(g[0]) == w[0]
+        for a, b in zip(g[1:], w[1:]):
+            assert abs(float(a) - b) <= 2e-6 * abs(b) + 1e-9, (g, w)

@@ -1,7 +1,9 @@
 """History-point location on the host (stx_mesh_locate_host; HistoryPoint::
 locate / Element::locate, src/history.cpp:45-63, src/element.cpp:
-1061-1183) against the oracle's restatement, on a mesh of skewed quads,
-and the oracle's Lagrange interpolants against polynomials."""
+1061-1183) and the relocation of moved particles (stx_mesh_relocate_host;
+src/particle.cpp:155-175) against the oracle's restatement, on a mesh of
+skewed quads; the oracle's Lagrange interpolants against polynomials and
+its particle integrator on a uniform flow."""
 import ctypes as C
 import re
 
@@ -67,3 +69,46 @@ def test_locate_matches_oracle_on_skewed_quads(tmp_path):
         is_, _ = O.lagrange_interpolants(M.z, rs[i, 1])
         assert abs(is_ @ M.x[e] @ ir - x) < 1e-9 and abs(is_ @ M.y[e] @ ir - y) < 1e-9
     assert (el[:40] >= 0).all() and (el[40:] == -1).all()
+
+
+def test_relocate_matches_oracle(tmp_path):
+    path = _skewed_session(str(tmp_path / "skew"))
+    S = O.read_session(path)
+    M = O.Problem(S).M
+    rng = np.random.default_rng(4)
+    start = rng.uniform(0.05, 0.95, (30, 2))
+    moved = np.clip(start + rng.uniform(-0.08, 0.08, start.shape), 0.0, 1.0)
+    moved[0] = (1.2, 0.5)   # left the mesh
+    moved = np.ascontiguousarray(moved)
+    el = np.empty(len(start), dtype=np.int32)
+    rs = np.empty((len(start), 2))
+    lib = _lib.lib()
+    _lib.check(lib.stx_mesh_locate_host(path.encode(), None, len(start), C.c_void_p(np.ascontiguousarray(start).ctypes.data),
+                                        C.c_void_p(el.ctypes.data), C.c_void_p(rs.ctypes.data)))
+    want = [O.relocate(M, x, y, int(e), r, s) for (x, y), e, (r, s) in zip(moved, el, rs)]
+    _lib.check(lib.stx_mesh_relocate_host(path.encode(), None, len(start), C.c_void_p(moved.ctypes.data),
+                                          C.c_void_p(el.ctypes.data), C.c_void_p(rs.ctypes.data)))
+    for i, w in enumerate(want):
+        if w is None:
+            assert el[i] == -1
+            continue
+        assert el[i] == w[0]
+        assert abs(rs[i, 0] - w[1]) < 1e-12 and abs(rs[i, 1] - w[2]) < 1e-12
+    assert (el[1:] >= 0).all() and el[0] == -1
+
+
+def test_particles_follow_a_uniform_flow(tmp_path):
+    # the predictor and corrector weights of every order sum to one: a
+    # particle in a uniform flow moves by dt * velocity each step
+    path = sessions.rect_session(str(tmp_path / "uf"), 4, 4, x=(0.0, 4.0), y=(0.0, 4.0),
+                                 tokens={"N_P": 5, "N_Z": 4, "D_T": 0.01, "N_TIME": 3}, fields="uvwp",
+                                 periodic_x=True, periodic_y=True)
+    S = O.read_session(path)
+    M = O.Problem(S).M
+    T = O.FluidParticles(M, S.tokens, 4)
+    assert T.make(1, (0.5, 0.7, 6.2), 0.0) and not T.make(2, (5.0, 1.0, 0.0), 0.0)
+    for _ in range(5):
+        T.integrate(lambda e, r, s, z: (1.0, 0.5, 0.25))
+    q = T.parts[0]
+    assert abs(q["x"] - (0.5 + 0.05)) < 1e-12 and abs(q["y"] - (0.7 + 0.025)) < 1e-12
+    assert abs(q["z"] - ((6.2 + 0.0125) % (2 * np.pi))) < 1e-12 and q["e"] is not None
