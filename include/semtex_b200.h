@@ -295,7 +295,8 @@ int stx_dns_get_field(stx_dns* dns, char field, double* h_phys);
 int stx_dns_advance(stx_dns* dns, int nsteps);
 /* Running averages (Statistics, src/statistics.cpp; session token AVERAGE
  * 1: the raw fields, 2: also the velocity products A=uu B=uv C=vv D=uw E=vw
- * F=ww).  stx_dns_stats_update is Statistics::update (the caller chooses
+ * F=ww, 3: also the energy-equation correlations q d m n o r s t a b c
+ * G-L).  stx_dns_stats_update is Statistics::update (the caller chooses
  * when: the dns program every IO_HIS steps).  stx_dns_stats_info returns the
  * averages' names in file order (NUL terminated) and the number of updates,
  * and sets that number when set_navg >= 0; get / set move one average in
@@ -304,6 +305,12 @@ int stx_dns_stats_update(stx_dns* dns);
 int stx_dns_stats_info(stx_dns* dns, char* names, int len, int* navg, int set_navg);
 int stx_dns_stats_get(stx_dns* dns, char name, double* h_phys);
 int stx_dns_stats_set(stx_dns* dns, char name, const double* h_phys);
+/* Exchange the running averages with a second set of the same names (made,
+ * zero, at the first call), with its own number of updates: the phase
+ * averages (Statistics::phaseUpdate, src/statistics.cpp:587-611) are loaded
+ * into it, updated and read out between two exchanges while the main
+ * averages stay on the device unchanged. */
+int stx_dns_stats_swap(stx_dns* dns);
 /* stx_modal_status over every system of the time stepping (0: all valid). */
 int stx_dns_status(stx_dns* dns, int* status);
 /* Length of the captured step cycle (0: none) and the number of graph

@@ -84,6 +84,7 @@ SIGNATURES = {
     "stx_dns_stats_info": (_i, [_p, _s, _i, _pi, _i]),
     "stx_dns_stats_get": (_i, [_p, C.c_char, _p]),
     "stx_dns_stats_set": (_i, [_p, C.c_char, _p]),
+    "stx_dns_stats_swap": (_i, [_p]),
     "stx_dns_adjoint_create": (_i, [_p, _i, C.POINTER(_p)]),
     "stx_dns_adjoint_destroy": (_i, [_p]),
     "stx_dns_adjoint_record": (_i, [_p, _i]),

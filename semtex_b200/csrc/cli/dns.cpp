@@ -23,6 +23,9 @@
 // dns/dnsanalysis.cpp:130-250).  Particles listed in session.par are tracked
 // every step (FluidParticle, src/particle.cpp; new ones at the listed places
 // every SPAWN steps) and written to session.trk with the history points.
+// With N_PHASE > 0 the phase averages are updated every STEPS_P / N_PHASE
+// steps in session.<phase>.phs (Statistics::phaseUpdate,
+// src/statistics.cpp:587-611; checks of src/analysis.cpp:141-172).
 #include <algorithm>
 #include <array>
 #include <cmath>
@@ -283,6 +286,18 @@ int main(int argc, char** argv) {
       check(stx_dns_stats_info(dns, nullptr, 0, nullptr, A.step), "statistics");
     }
   }
+  // -- phase averaging (Analyser::Analyser, src/analysis.cpp:141-172)
+  const int n_phase = static_cast<int>(std::lround(token(ctx, "N_PHASE")));
+  int steps_p = 0;
+  if (n_phase > 0) {
+    double v = 0.0;
+    if (stx_token(ctx, "STEPS_P", &v) == STX_OK) steps_p = static_cast<int>(std::lround(v));
+    if (!averaging) fail("if N_PHASE is set, AVERAGE > 0 also required");
+    if (!steps_p) fail("phase averaging is on but STEPS_P not set");
+    if (steps_p % n_phase) fail("STEPS_P / N_PHASE non-integer");
+    if (nstep % n_phase) fail("N_STEP / N_PHASE non-integer");
+    if (io_fld != steps_p / n_phase) fail("phase averaging: IO_FLD != STEPS_P / N_PHASE");
+  }
   // -- Analyser::Analyser (src/analysis.cpp:106-184) and DNSAnalyser::
   //    DNSAnalyser (dns/dnsanalysis.cpp:30-52): history points located in
   //    the mesh (shifted and scaled as X_SHIFT, X_SCALE, ... ask), files
@@ -417,6 +432,38 @@ int main(int argc, char** argv) {
       std::printf("-- CFL: %g, dt (max): %g, dt (set): %g (%d%%)\n", inv * dt, dt_max, dt,
                   static_cast<int>(100.0 * dt / dt_max));
       std::printf("------- Divergence Energy: %g\n", div);
+    }
+    // -- phase averages (Statistics::phaseUpdate): the second set of
+    //    averages on the device takes session.<phase>.phs (or zero), is
+    //    updated and written back; the running averages stay untouched
+    if (n_phase > 0 && step % (steps_p / n_phase) == 0) {
+      const int iphase = (step % steps_p) / (steps_p / n_phase);
+      const std::string fn = session + "." + std::to_string(iphase) + ".phs";
+      check(stx_dns_stats_swap(dns), "statistics");
+      int nphs = 0;
+      if (std::ifstream(fn)) {
+        const stx::FieldFile A = stx::read_field(fn);
+        if (A.names != avg_names) fail(fn + " holds other averages than AVERAGE asks for");
+        for (size_t k = 0; k < avg_names.size(); ++k) {
+          if (A.data[k].size() != n) fail(fn + " does not match the session");
+          check(stx_dns_stats_set(dns, avg_names[k], A.data[k].data()), "statistics");
+        }
+        nphs = A.step;
+      } else {
+        for (size_t k = 0; k < avg_names.size(); ++k)
+          check(stx_dns_stats_set(dns, avg_names[k], zero.data()), "statistics");
+      }
+      check(stx_dns_stats_info(dns, nullptr, 0, nullptr, nphs), "statistics");
+      check(stx_dns_stats_update(dns), "statistics");
+      stx::FieldFile A = out;
+      A.time = time;
+      A.names = avg_names;
+      A.data.assign(avg_names.size(), std::vector<double>(n));
+      check(stx_dns_stats_info(dns, nullptr, 0, &A.step, -1), "statistics");
+      for (size_t k = 0; k < avg_names.size(); ++k)
+        check(stx_dns_stats_get(dns, avg_names[k], A.data[k].data()), "statistics");
+      stx::write_field(fn, A);
+      check(stx_dns_stats_swap(dns), "statistics");
     }
     // -- history points and wall forces at IO_HIS / IO_FLD steps and at
     //    the end (Analyser::analyse, DNSAnalyser::analyse)

@@ -1502,6 +1502,23 @@ int stx_dns_stats_update(stx_dns* d) {
   });
 }
 
+int stx_dns_stats_swap(stx_dns* d) {
+  return dns_guarded([&] {
+    if (!d) throw DnsError(STX_EINVAL, "null argument");
+    if (!d->avg_level) throw DnsError(STX_EINVAL, "no averaging (token AVERAGE)");
+    if (d->avg_alt.empty()) {
+      const size_t nb = d->avg_buf.size();
+      double* ab = static_cast<double*>(d->arena.alloc(sizeof(double) * d->fsize * nb));
+      cudaSetDevice(d->ctx->device);
+      ck(cudaMemset(ab, 0, sizeof(double) * d->fsize * nb), "memset");
+      for (size_t k = 0; k < nb; ++k) d->avg_alt.push_back(ab + d->fsize * k);
+      d->navg_alt = 0;
+    }
+    std::swap(d->avg_buf, d->avg_alt);
+    std::swap(d->navg, d->navg_alt);
+  });
+}
+
 int stx_dns_stats_info(stx_dns* d, char* names, int len, int* navg, int set_navg) {
   return dns_guarded([&] {
     if (!d) throw DnsError(STX_EINVAL, "null argument");

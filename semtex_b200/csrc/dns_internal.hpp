@@ -104,6 +104,8 @@ struct stx_dns {
   std::string avg_names;
   std::vector<double*> avg_buf;
   double* avg_work = nullptr;  // AVERAGE 3: seven work fields
+  std::vector<double*> avg_alt; // the second set of averages (stx_dns_stats_swap)
+  int navg_alt = 0;
   // Body forcing (<FORCE>; FieldForce and its classes, dns/fieldforce.cpp),
   // on the grid of the nonlinear products (nzl planes: N_Z, or 3 N_Z / 2
   // with DEALIAS).  Fields are device arrays of nzl planes, null when a term

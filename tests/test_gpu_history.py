@@ -11,6 +11,9 @@ session.flx and session.wss).
 - Wall tractions (Field::traction, src/field.cpp:533-593) against the
   oracle on the channel with 8, 2 and 1 planes: every mode's normal,
   in-plane and out-of-plane traction, then the inverse z transform.
+- Phase averages (N_PHASE, STEPS_P: Statistics::phaseUpdate) in
+  session.<phase>.phs and the running averages beside them, against the
+  oracle's statistics on the device DNS's fields.
 - The `dns` program's particle tracks (session.par in, session.trk out,
   FluidParticle, src/particle.cpp) against the oracle's particle integrator
   moving on the device DNS's own fields, step by step, with new particles
@@ -270,3 +273,46 @@ def test_dns_program_tracks_particles(tmp_path):
         assert int(g[0]) == w[0]
         for a, b in zip(g[1:], w[1:]):
             assert abs(float(a) - b) <= 2e-6 * abs(b) + 1e-9, (g, w)
+
+
+def test_dns_program_phase_averages(tmp_path):
+    from semtex_b200.fieldfile import read_field
+    nstep = 8
+    path = sessions.taylor_green_session(str(tmp_path / "tgp"), 3, 6, 8, re=100.0, dt=2e-3, nstep=nstep,
+                                         extra={"TOL_REL": 1e-14, "AVERAGE": 2, "N_PHASE": 2, "STEPS_P": 4,
+                                                "IO_FLD": 2, "IO_HIS": 4})
+    ctx = S.Context(path)
+    funcs = S._user_functions(path)
+    ic = {c: ctx.evaluate(funcs[c], 0.0) for c in ctx.fields if c in funcs}
+    write_field(path + ".rst", "tgp", ctx.np, ctx.nz, ctx.nel, 0, 0.0, 2e-3, 1.0 / 100.0, 1.0,
+                {c: ic.get(c, np.zeros_like(ic["u"])) for c in ctx.fields})
+    r = subprocess.run([os.path.join(BIN, "dns"), path], capture_output=True, text=True, timeout=600)
+    assert r.returncode == 0, r.stderr
+    # the oracle's statistics, two phase sets and the running set, on the
+    # device DNS's fields of the same steps
+    P = O.Problem(O.read_session(path))
+    sets = {}
+    for key in ("0", "1", "avg"):
+        sets[key] = O.DNS(P)
+        sets[key].stats_init(2)
+    D = S.DNS(ctx, 1)
+    D.restart(ic, 0.0)
+    for step in range(1, nstep + 1):
+        D.advance(1)
+        upd = []
+        if step % 2 == 0:
+            upd.append(str((step % 4) // 2))
+        if step % 4 == 0:
+            upd.append("avg")
+        for key in upd:
+            for c in ctx.fields:
+                sets[key].u[c] = _fourier(D, c)
+            sets[key].stats_update()
+    D.close()
+    for key, fn in (("0", path + ".0.phs"), ("1", path + ".1.phs"), ("avg", path + ".avg")):
+        hdr, got = read_field(fn)
+        ref = sets[key].stats_physical()
+        assert hdr["step"] == 2 and sorted(got) == sorted(ref), (key, hdr["step"], sorted(got))
+        for c in ref:
+            scale = max(np.linalg.norm(ref[c]), 1e-300)
+            assert np.linalg.norm(got[c] - ref[c]) / scale < (1e-9 if c == "p" else 1e-10), (key, c)
