@@ -1,10 +1,11 @@
-// dns [-h] [-S|-C|-N] [-chk] [-v] session
+// dns [-h] [-i] [-S|-C|-N] [-chk] [-v] session
 //
 // The `dns` program (dns/drive.cpp:56-160) on the device: the session's
 // fields start from session.rst if present, else zero (Domain::restart,
 // src/domain.cpp:123-156); N_STEP velocity-correction steps of integrate()
 // (dns/integrate.cpp:66-200) with the advection form of -S (skew-symmetric),
-// default (alternating skew-symmetric), -C (convective) or -N (Stokes).
+// default (alternating skew-symmetric), -C (convective) or -N (Stokes); -i
+// solves the viscous steps iteratively (token ITERATIVE = 1).
 // Field dumps follow Domain::dump (src/domain.cpp:158-215): every IO_FLD
 // steps and at the end, to session.chk (previous one kept as .chk.bak) with
 // the final dump to session.fld, or with -chk all appended to session.fld.
@@ -56,6 +57,7 @@ const char* kUsage =
     "Usage: dns [options] session-file\n"
     "  [options]:\n"
     "  -h       ... print this message\n"
+    "  -i       ... use iterative solver for viscous steps\n"
     "  -v[v...] ... increase verbosity level\n"
     "  -chk     ... turn off checkpoint field dumps [default: selected]\n"
     "  -S|C|N   ... regular skew-symm || convective || Stokes advection\n";
@@ -215,7 +217,7 @@ struct Particles {
 
 int main(int argc, char** argv) {
   int advection = 1, verbose = 0;
-  bool no_chk = false;
+  bool no_chk = false, iterative = false;
   int a = 1;
   for (; a < argc && argv[a][0] == '-'; ++a) {
     const std::string o = argv[a];
@@ -230,6 +232,8 @@ int main(int argc, char** argv) {
       advection = 3;
     } else if (o == "-chk") {
       no_chk = true;
+    } else if (o.find_first_not_of('i', 1) == std::string::npos) {  // -i[i...]: viscous steps only
+      iterative = true;
     } else if (o[1] == 'v') {
       verbose += static_cast<int>(o.size()) - 1;
     } else {
@@ -240,7 +244,7 @@ int main(int argc, char** argv) {
   if (a != argc - 1) fail("no session definition file");
   const std::string session = argv[a];
   stx_context* ctx = nullptr;
-  check(stx_context_create(session.c_str(), nullptr, 0, nullptr, &ctx), "session");
+  check(stx_context_create(session.c_str(), iterative ? "ITERATIVE=1" : nullptr, 0, nullptr, &ctx), "session");
   int np = 0, nz = 0, nel = 0, ps = 0;
   check(stx_context_geometry(ctx, &np, &nz, &nel, &ps), "geometry");
   char fbuf[64];

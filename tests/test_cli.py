@@ -88,3 +88,30 @@ def test_dns_program_writes_averages(tmp_path):
     hdr, fld = read_field(path + ".fld")
     assert hdr["step"] == 12
     assert np.all(np.isfinite(avg["A"])) and np.abs(avg["A"]).max() > 0.1
+
+
+@pytest.mark.gpu
+def test_dns_program_iterative_option(tmp_path):
+    # -i: Jacobi-PCG viscous steps (token ITERATIVE = 1), as the library
+    # runs them with the token set
+    import semtex_b200 as S
+    from semtex_b200 import sessions
+    path = sessions.channel_session(str(tmp_path / "chi"), 4, 2, 6, 4, re=200.0, dt=5e-3, nstep=6,
+                                    extra={"TOL_REL": 1e-12})
+    ctx = S.Context(path, overrides={"ITERATIVE": 1})
+    x, y = ctx.mesh_coords()
+    ic = sessions.channel_initial(x, y, np.arange(ctx.nz) * 2 * np.pi / ctx.nz, amplitude=0.05)
+    ic = {c: ic[c] for c in ctx.fields[:-1]}
+    write_field(path + ".rst", "chi", ctx.np, ctx.nz, ctx.nel, 0, 0.0, 5e-3, 1.0 / 200.0, 1.0,
+                {**ic, "p": np.zeros_like(ic["u"])})
+    r = subprocess.run([os.path.join(BIN, "dns"), "-i", "-chk", path], capture_output=True, text=True, timeout=600)
+    assert r.returncode == 0, r.stderr
+    hdr, flds = read_field(path + ".fld")
+    D = S.DNS(ctx, 1)
+    D.restart(ic, 0.0)
+    D.advance(6)
+    for c in ctx.fields:
+        want = D.field(c)
+        tol = 1e-8 if c == "p" else 1e-10
+        assert np.linalg.norm(flds[c] - want) <= tol * np.linalg.norm(want), c
+    D.close()

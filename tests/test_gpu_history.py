@@ -44,6 +44,7 @@ def _fourier(D, c):
     """The DNS's Fourier-space storage of field c, [nz, nel, np, np]."""
     from cuda.bindings import runtime as rt
     ctx = D.ctx
+    ctx.sync()   # the DNS runs on the context's own stream: its step must be done before the copy
     p = C.c_void_p()
     _lib.check(_lib.lib().stx_dns_field_ptr(D._h, c.encode(), C.byref(p)))
     buf = np.empty((ctx.nz, ctx.plane_size))
