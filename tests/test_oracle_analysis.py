@@ -1,8 +1,9 @@
 """The oracle's analysis restatements on flows with known answers (CPU):
 the wall forces and tractions of plane Poiseuille flow (Field::
-normTraction / tangTraction / traction, src/field.cpp:392-593) and the
+normTraction / tangTraction / traction, src/field.cpp:392-593), the
 AVERAGE 3 correlations of a uniform shear (Statistics::update,
-src/statistics.cpp:247-391).  The device paths are checked against these
+src/statistics.cpp:247-391) and history-point probes of a smooth field
+(AuxField::probe, src/auxfield.cpp:1621-1700).  The device paths are checked against these
 restatements by the GPU tests."""
 import numpy as np
 
@@ -65,3 +66,25 @@ def test_uniform_shear_energy_correlations(tmp_path):
               "A": y * y, "m": 0 * y}
     for c, v in expect.items():
         assert np.abs(A[c] - v).max() < 1e-10, c
+
+
+def test_probe_reproduces_a_smooth_field(tmp_path):
+    # AuxField::probe on u = sin(x) cos(y) (cos z + 0.5 sin 2z): the
+    # interpolants and the Fourier series reproduce it to the resolution
+    p = sessions.taylor_green_session(str(tmp_path / "tgp"), 4, 11, 8)
+    S = O.read_session(p)
+    P = O.Problem(S)
+    D = O.DNS(P)
+    x, y = P.M.x, P.M.y
+    z = (np.arange(P.nz) * 2 * np.pi / P.nz)[:, None, None, None]
+    u = np.sin(x) * np.cos(y) * (np.cos(z) + 0.5 * np.sin(2 * z))
+    for c in S.fields:
+        f = O.dft_forward(u if c == "u" else 0 * u)
+        f[1] = 0.0
+        D.u[c] = f
+    rng = np.random.default_rng(3)
+    pts = np.column_stack([rng.uniform(0, 2 * np.pi, 12), rng.uniform(0, 2 * np.pi, 12), rng.uniform(-3, 9, 12)])
+    got = D.probe(pts)
+    want = np.sin(pts[:, 0]) * np.cos(pts[:, 1]) * (np.cos(pts[:, 2]) + 0.5 * np.sin(2 * pts[:, 2]))
+    assert np.abs(got[:, 0] - want).max() < 1e-6
+    assert np.abs(got[:, 1:]).max() == 0.0
